@@ -1,0 +1,98 @@
+"""Build the synx CUDA library (libsynx.so) and the antsRegistration-compatible host binary.
+
+Everything is compiled in-tree for sm_100a with nvcc; no JIT cache is involved, so the built
+files travel with the source tree.
+
+    python -m ants_b200.build            # build what is out of date
+    python -m ants_b200.build --force    # rebuild everything
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+              "--expt-relaxed-constexpr"]
+
+LIB = os.path.join(HERE, "libsynx.so")
+CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
+
+LIB_SOURCES = ["synx_kernels.cu", "synx_ctx.cu"]
+LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh"]
+CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
+CLI_HEADERS = ["nifti_io.h", "ants_registration.h"]
+
+
+def _nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return cand
+
+
+def _host_cxx() -> str:
+    # the system g++ (some environments point CXX at a toolchain without libgomp)
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in LIB_HEADERS] + [os.path.join(INCLUDE, "synx.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *srcs, "-lcudart"]
+    if verbose_ptxas:
+        cmd.insert(1, "-Xptxas=-v")
+    _run(cmd)
+    return LIB
+
+
+def build_cli(force: bool = False) -> str | None:
+    srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES]
+    if not all(os.path.exists(s) for s in srcs):
+        return None
+    deps = srcs + [os.path.join(CSRC, h) for h in CLI_HEADERS] + [LIB]
+    if not force and not _stale(CLI, deps):
+        return CLI
+    cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", "/usr/local/cuda/include", "-o", CLI,
+           *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN", "-lz"]
+    _run(cmd)
+    return CLI
+
+
+def build_all(force: bool = False) -> None:
+    build_lib(force)
+    build_cli(force)
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas", action="store_true", help="print ptxas register/smem usage")
+    a = ap.parse_args(argv)
+    build_lib(a.force or a.ptxas, verbose_ptxas=a.ptxas)
+    build_cli(a.force)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1192 @@
+// synx C ABI: registration context, level loop and step entry points.
+//
+// One context = one fixed/moving pair on one GPU.  All pair state (images, the pyramid
+// level images, the four half-fields and the iteration work buffers) lives in one device
+// arena allocated at synx_set_images; a level is enqueued without host synchronisation (the
+// convergence test and the fixed-point loop bounds are evaluated on the device), and is
+// optionally captured once as a CUDA graph and replayed per iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/synx.h"
+#include "synx_kernels.cuh"
+
+using namespace synx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+// ---- discrete Gaussian kernel --------------------------------------------------------------
+// Lindeberg's discrete Gaussian k(n) = e^{-t} I_n(t) with I_0, I_1 from the polynomial
+// approximations of Abramowitz & Stegun (9.8.1-9.8.4) and the recurrence
+// I_n = I_{n-2} - 2 (n-1) I_{n-1} / t, grown until the two-sided mass reaches 1 - max_error
+// or the half-kernel exceeds max_width, then normalised and mirrored (the construction of
+// ITK's GaussianOperator that SyN's field smoothing and the level pyramid use).
+double as_i0(double y) {
+  double ay = std::fabs(y);
+  if (ay < 3.75) {
+    double t = (y / 3.75) * (y / 3.75);
+    return 1.0 + t * (3.5156229 + t * (3.0899424 + t * (1.2067492 + t * (0.2659732 + t * (0.0360768 + t * 0.0045813)))));
+  }
+  double t = 3.75 / ay;
+  return (std::exp(ay) / std::sqrt(ay)) *
+         (0.39894228 + t * (0.01328592 + t * (0.00225319 + t * (-0.00157565 + t * (0.00916281 +
+          t * (-0.02057706 + t * (0.02635537 + t * (-0.01647633 + t * 0.00392377))))))));
+}
+double as_i1(double y) {
+  double ay = std::fabs(y), r;
+  if (ay < 3.75) {
+    double t = (y / 3.75) * (y / 3.75);
+    r = ay * (0.5 + t * (0.87890594 + t * (0.51498869 + t * (0.15084934 + t * (0.02658733 + t * (0.00301532 + t * 0.00032411))))));
+  } else {
+    double t = 3.75 / ay;
+    r = 0.02282967 + t * (-0.02895312 + t * (0.01787654 - t * 0.00420059));
+    r = 0.39894228 + t * (-0.03988024 + t * (-0.00362018 + t * (0.00163801 + t * (-0.01031555 + t * r))));
+    r *= std::exp(ay) / std::sqrt(ay);
+  }
+  return y < 0 ? -r : r;
+}
+std::vector<double> gauss_kernel(double variance, double max_error, size_t max_width) {
+  std::vector<double> h;
+  const double et = std::exp(-variance), cap = 1.0 - max_error;
+  double sum = 0.0;
+  h.push_back(et * as_i0(variance));
+  sum += h[0];
+  h.push_back(et * as_i1(variance));
+  sum += 2.0 * h[1];
+  for (int i = 2; sum < cap; ++i) {
+    h.push_back(h[i - 2] - 2.0 * (i - 1) * h[i - 1] / variance);
+    sum += 2.0 * h[i];
+    if (h[i] <= 0.0) break;
+    if (h.size() > max_width) break;
+  }
+  for (double& c : h) c /= sum;
+  const size_t R = h.size() - 1;
+  std::vector<double> k(2 * R + 1);
+  for (size_t i = 0; i <= R; ++i) k[R + i] = k[R - i] = h[i];
+  return k;
+}
+
+// ---- level geometry (CalculateShrinkFactorsPerDimension + ShrinkImageFilter) ----------------
+void shrink_factors(int dim, unsigned factor, const double sp[3], unsigned out[3]) {
+  double minSp = sp[0];
+  int minIdx = 0;
+  for (int n = 1; n < dim; ++n)
+    if (minSp > sp[n]) {
+      minSp = sp[n];
+      minIdx = n;
+    }
+  out[0] = out[1] = out[2] = 0;
+  out[minIdx] = factor;
+  const double target = sp[minIdx] * factor;
+  for (int n = 0; n < dim; ++n) {
+    if (out[n]) continue;
+    double best = std::fabs(sp[n] * factor - target);
+    unsigned bf = factor;
+    for (unsigned f = factor - 1; f > 0; --f) {
+      double dd = std::fabs(sp[n] * f - target);
+      if (dd <= best) {
+        best = dd;
+        bf = f;
+      }
+    }
+    out[n] = bf;
+  }
+  if (dim == 2) out[2] = 1;
+}
+
+void geom_to_grid(const synx_geom& g, GridInfo& gi) {
+  gi = make_grid(g.dim, g.size, g.spacing, g.origin, g.direction);
+}
+
+synx_geom shrink(const synx_geom& in, unsigned factor) {
+  unsigned f[3];
+  shrink_factors(in.dim, factor, in.spacing, f);
+  synx_geom out = in;
+  for (int d = 0; d < in.dim; ++d) {
+    out.spacing[d] = in.spacing[d] * f[d];
+    int64_t s = (int64_t)std::floor((double)in.size[d] / (double)f[d]);
+    out.size[d] = s < 1 ? 1 : s;
+  }
+  if (in.dim == 2) out.size[2] = 1;
+  GridInfo gin, gout;
+  geom_to_grid(in, gin);
+  geom_to_grid(out, gout);
+  double ci[3] = {0, 0, 0}, co[3] = {0, 0, 0};
+  for (int d = 0; d < in.dim; ++d) {
+    ci[d] = (in.size[d] - 1) / 2.0;
+    co[d] = (out.size[d] - 1) / 2.0;
+  }
+  for (int r = 0; r < 3; ++r) {
+    double pin = gin.org[r], pout = gout.org[r];
+    for (int c = 0; c < 3; ++c) {
+      pin += gin.i2p[r * 3 + c] * ci[c];
+      pout += gout.i2p[r * 3 + c] * co[c];
+    }
+    out.origin[r] = in.origin[r] + (pin - pout);
+  }
+  if (in.dim == 2) out.origin[2] = in.origin[2];
+  return out;
+}
+
+bool check_geom(const synx_geom* g, int dim) {
+  if (!g || g->dim != dim) return false;
+  for (int d = 0; d < dim; ++d)
+    if (g->size[d] < 1 || !(g->spacing[d] > 0)) return false;
+  if (dim == 2 && g->size[2] != 1) return false;
+  long long n = (long long)g->size[0] * g->size[1] * g->size[2];
+  if (n * 3 >= (1LL << 31)) return false;
+  return true;
+}
+
+int set_err(synx_ctx* c, int code, const std::string& msg);
+
+}  // namespace
+
+struct synx_ctx {
+  synx_params P;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  bool images_set = false;
+  synx_geom geF{}, geM{};
+  GridInfo gF{}, gM{};
+  std::vector<synx_geom> lgeom;
+  std::vector<GridInfo> lv;
+  long long Nmax = 0, NF = 0, NM = 0;
+  int D = 3;
+  // arena
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  float *F0 = nullptr, *M0 = nullptr, *Fs = nullptr, *Ms = nullptr, *tmpI = nullptr;
+  float *phiF = nullptr, *psiF = nullptr, *phiM = nullptr, *psiM = nullptr;
+  float *Ft = nullptr, *Mt = nullptr;
+  float *gFu = nullptr, *gMu = nullptr, *t1F = nullptr, *t1M = nullptr, *t2F = nullptr, *t2M = nullptr;
+  double* cc_partials = nullptr;
+  int cc_cap = 0;
+  double* inv_psum = nullptr;
+  float* inv_pmax = nullptr;
+  int inv_cap = 0;
+  float* coeff_upd = nullptr;   // [3][cap]
+  float* coeff_tot = nullptr;   // [3][cap]
+  double* coeff_img = nullptr;  // [3][cap]
+  int coeff_cap = 0;
+  int R_upd[3] = {0, 0, 0}, R_tot[3] = {0, 0, 0};
+  IterCtl* ctl = nullptr;
+  LogDev logdev{};
+  unsigned* hist = nullptr;  // 256 bins + 2 min/max
+  // host mirrors
+  std::vector<float> h_coeff_upd, h_coeff_tot;
+  std::vector<double> h_coeff_img;
+  int cur_level = -1;
+  GridInfo cur_grid{};
+  std::vector<int32_t> log_level, log_iter, log_inv;
+  std::vector<double> log_metric, log_conv;
+  // graphs
+  cudaGraphExec_t gexec = nullptr;
+  // profiling
+  double prof_inv_ms = 0, prof_cc_ms = 0;
+  long long prof_inv_launches = 0, prof_inv_vox = 0, prof_cc_launches = 0, prof_cc_vox = 0;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_pairs_inv, ev_pairs_cc;  // indices into ev_pool
+  size_t ev_used = 0;
+};
+
+namespace {
+
+int set_err(synx_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return set_err(ctx, SYNX_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+  } while (0)
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+void free_arena(synx_ctx* c) {
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  if (c->arena) cudaFree(c->arena);
+  c->arena = nullptr;
+  c->arena_bytes = 0;
+}
+
+int build_levels(synx_ctx* c) {
+  c->lgeom.clear();
+  c->lv.clear();
+  c->Nmax = 0;
+  for (int l = 0; l < c->P.n_levels; ++l) {
+    synx_geom g = shrink(c->geF, (unsigned)c->P.shrink_factors[l]);
+    GridInfo gi;
+    geom_to_grid(g, gi);
+    c->lgeom.push_back(g);
+    c->lv.push_back(gi);
+    c->Nmax = std::max(c->Nmax, gi.d.N);
+  }
+  return SYNX_OK;
+}
+
+int allocate(synx_ctx* c) {
+  const int D = c->D;
+  const long long Nmax = c->Nmax, NI = std::max(c->NF, c->NM);
+  int ccb = 0, invb = 0;
+  for (auto& g : c->lv) {
+    ccb = std::max(ccb, cc_blocks(g, c->P.cc_radius));
+    invb = std::max(invb, inv_blocks(g));
+  }
+  // step entry points on arbitrary grids reuse nothing from here
+  const int coeff_cap = 1024;
+  int max_iters = 1;
+  for (int l = 0; l < c->P.n_levels; ++l) max_iters = std::max(max_iters, c->P.iterations[l]);
+  size_t sz = 0;
+  auto add = [&](size_t bytes) {
+    size_t o = sz;
+    sz += align_up(bytes);
+    return o;
+  };
+  size_t oF0 = add(4 * c->NF), oM0 = add(4 * c->NM), oFs = add(4 * c->NF), oMs = add(4 * c->NM), oTmp = add(4 * NI);
+  size_t oField[4];
+  for (int k = 0; k < 4; ++k) oField[k] = add(4 * (size_t)D * Nmax);
+  size_t oFt = add(4 * Nmax), oMt = add(4 * Nmax);
+  size_t oWork[6];
+  for (int k = 0; k < 6; ++k) oWork[k] = add(4 * (size_t)D * Nmax);
+  size_t oCC = add(8 * (size_t)ccb), oIS = add(8 * 2 * (size_t)invb), oIM = add(4 * 2 * (size_t)invb);
+  size_t oCu = add(4 * 3 * coeff_cap), oCt = add(4 * 3 * coeff_cap), oCi = add(8 * 3 * coeff_cap);
+  size_t oCtl = add(sizeof(IterCtl));
+  size_t oLm = add(8 * (size_t)max_iters), oLc = add(8 * (size_t)max_iters), oLi = add(4 * (size_t)max_iters);
+  size_t oH = add(4 * 258);
+  if (c->arena && c->arena_bytes >= sz) {
+    // reuse
+  } else {
+    free_arena(c);
+    cudaError_t e = cudaMalloc((void**)&c->arena, sz);
+    if (e != cudaSuccess) {
+      c->arena = nullptr;
+      cudaGetLastError();
+      return set_err(c, SYNX_E_NOMEM, std::string("device arena of ") + std::to_string(sz) + " bytes: " +
+                                          cudaGetErrorString(e));
+    }
+    c->arena_bytes = sz;
+  }
+  char* a = c->arena;
+  c->F0 = (float*)(a + oF0);
+  c->M0 = (float*)(a + oM0);
+  c->Fs = (float*)(a + oFs);
+  c->Ms = (float*)(a + oMs);
+  c->tmpI = (float*)(a + oTmp);
+  c->phiF = (float*)(a + oField[0]);
+  c->psiF = (float*)(a + oField[1]);
+  c->phiM = (float*)(a + oField[2]);
+  c->psiM = (float*)(a + oField[3]);
+  c->Ft = (float*)(a + oFt);
+  c->Mt = (float*)(a + oMt);
+  c->gFu = (float*)(a + oWork[0]);
+  c->gMu = (float*)(a + oWork[1]);
+  c->t1F = (float*)(a + oWork[2]);
+  c->t1M = (float*)(a + oWork[3]);
+  c->t2F = (float*)(a + oWork[4]);
+  c->t2M = (float*)(a + oWork[5]);
+  c->cc_partials = (double*)(a + oCC);
+  c->cc_cap = ccb;
+  c->inv_psum = (double*)(a + oIS);
+  c->inv_pmax = (float*)(a + oIM);
+  c->inv_cap = invb;
+  c->coeff_upd = (float*)(a + oCu);
+  c->coeff_tot = (float*)(a + oCt);
+  c->coeff_img = (double*)(a + oCi);
+  c->coeff_cap = coeff_cap;
+  c->ctl = (IterCtl*)(a + oCtl);
+  c->logdev.metric = (double*)(a + oLm);
+  c->logdev.conv = (double*)(a + oLc);
+  c->logdev.inv_iters = (int*)(a + oLi);
+  c->logdev.cap = max_iters;
+  c->hist = (unsigned*)(a + oH);
+  CUDA_TRY(c, cudaMemsetAsync(c->ctl, 0, sizeof(IterCtl), c->stream));
+  return SYNX_OK;
+}
+
+// Preprocess one image in place on the device: histogram quantiles -> window -> [0, 1].
+int preprocess(synx_ctx* c, float* img, long long n) {
+  unsigned init[2] = {float_to_ordered(FLT_MAX), float_to_ordered(-FLT_MAX)};
+  unsigned* mm = c->hist + 256;
+  CUDA_TRY(c, cudaMemcpyAsync(mm, init, 8, cudaMemcpyHostToDevice, c->stream));
+  launch_minmax(img, n, mm, c->stream);
+  unsigned hm[2];
+  CUDA_TRY(c, cudaMemcpyAsync(hm, mm, 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const float mn = ordered_to_float(hm[0]), mx = ordered_to_float(hm[1]);
+  const int nb = 256;
+  const float margin = ((mx - mn) / (float)nb) / 10.0f;
+  const float hi = mx + margin;
+  CUDA_TRY(c, cudaMemsetAsync(c->hist, 0, 4 * nb, c->stream));
+  launch_histogram(img, n, mn, hi, nb, c->hist, c->stream);
+  std::vector<unsigned> hh(nb);
+  CUDA_TRY(c, cudaMemcpyAsync(hh.data(), c->hist, 4 * nb, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const double bw = ((double)hi - (double)mn) / nb;
+  auto bmin = [&](int b) { return (double)mn + b * bw; };
+  auto bmax = [&](int b) { return (double)mn + (b + 1) * bw; };
+  auto quantile = [&](double p) -> double {
+    double total = (double)n, cum = 0, pn = 0, pprev = 0, fn = 0;
+    if (p < 0.5) {
+      int k = 0;
+      do {
+        fn = hh[k];
+        cum += fn;
+        pprev = pn;
+        pn = cum / total;
+        ++k;
+      } while (k < nb && pn < p);
+      return bmin(k - 1) + ((p - pprev) / (fn / total)) * (bmax(k - 1) - bmin(k - 1));
+    }
+    int k = nb - 1, m = 0;
+    pn = 1.0;
+    do {
+      fn = hh[k];
+      cum += fn;
+      pprev = pn;
+      pn = 1.0 - cum / total;
+      --k;
+      ++m;
+    } while (m < nb && pn > p);
+    return bmax(k + 1) - ((pprev - p) / (fn / total)) * (bmax(k + 1) - bmin(k + 1));
+  };
+  const float wlo = (float)quantile(c->P.winsor_lower), whi = (float)quantile(c->P.winsor_upper);
+  const double scale = 1.0 / ((double)whi - (double)wlo);
+  const double shift = -(double)wlo * scale;
+  launch_window(img, img, n, wlo, whi, scale, shift, c->stream);
+  return SYNX_OK;
+}
+
+// Kernels for the current level: pyramid (per image axis) and field smoothing (per field
+// axis, width limited by the level size).
+int upload_level_kernels(synx_ctx* c, int level) {
+  const GridInfo& g = c->lv[level];
+  c->h_coeff_upd.assign(3 * c->coeff_cap, 0.0f);
+  c->h_coeff_tot.assign(3 * c->coeff_cap, 0.0f);
+  for (int a = 0; a < c->D; ++a) {
+    const int n = a == 0 ? g.d.nx : (a == 1 ? g.d.ny : g.d.nz);
+    auto ku = gauss_kernel(c->P.update_variance, 0.001, (size_t)n);
+    auto kt = gauss_kernel(c->P.total_variance, 0.001, (size_t)n);
+    if ((int)ku.size() > c->coeff_cap || (int)kt.size() > c->coeff_cap)
+      return set_err(c, SYNX_E_UNSUPPORTED, "field smoothing kernel wider than 1024 taps");
+    c->R_upd[a] = (int)ku.size() / 2;
+    c->R_tot[a] = (int)kt.size() / 2;
+    for (size_t j = 0; j < ku.size(); ++j) c->h_coeff_upd[a * c->coeff_cap + j] = (float)ku[j];
+    for (size_t j = 0; j < kt.size(); ++j) c->h_coeff_tot[a * c->coeff_cap + j] = (float)kt[j];
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->coeff_upd, c->h_coeff_upd.data(), 4 * 3 * c->coeff_cap, cudaMemcpyHostToDevice,
+                              c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->coeff_tot, c->h_coeff_tot.data(), 4 * 3 * c->coeff_cap, cudaMemcpyHostToDevice,
+                              c->stream));
+  return SYNX_OK;
+}
+
+int smooth_images_for_level(synx_ctx* c, int level) {
+  const double sigma = c->P.smoothing_sigmas[level];
+  struct Img {
+    const float* src;
+    float* dst;
+    const GridInfo* g;
+  } imgs[2] = {{c->F0, c->Fs, &c->gF}, {c->M0, c->Ms, &c->gM}};
+  for (auto& im : imgs) {
+    const GridInfo& g = *im.g;
+    if (sigma <= 0.0) {
+      CUDA_TRY(c, cudaMemcpyAsync(im.dst, im.src, 4 * g.d.N, cudaMemcpyDeviceToDevice, c->stream));
+      continue;
+    }
+    // per-axis kernels, last axis first (chained as DiscreteGaussianImageFilter does)
+    std::vector<double> hk(3 * c->coeff_cap, 0.0);
+    int R[3] = {0, 0, 0};
+    for (int a = 0; a < c->D; ++a) {
+      double var = sigma * sigma;
+      if (c->P.sigmas_in_mm) var /= g.sp[a] * g.sp[a];
+      auto k = gauss_kernel(var, 0.01, 32);
+      R[a] = (int)k.size() / 2;
+      for (size_t j = 0; j < k.size(); ++j) hk[a * c->coeff_cap + j] = k[j];
+    }
+    c->h_coeff_img = hk;
+    CUDA_TRY(c, cudaMemcpyAsync(c->coeff_img, c->h_coeff_img.data(), 8 * 3 * c->coeff_cap, cudaMemcpyHostToDevice,
+                                c->stream));
+    // ping-pong between dst and tmpI so the final pass (axis 0) lands in dst
+    const float* src = im.src;
+    int passes = c->D;
+    for (int p = 0; p < passes; ++p) {
+      const int axis = c->D - 1 - p;
+      float* out = ((passes - 1 - p) % 2 == 0) ? im.dst : c->tmpI;
+      launch_conv_image_axis(src, out, g, axis, c->coeff_img + axis * c->coeff_cap, R[axis], c->stream);
+      src = out;
+    }
+    // the host kernel buffer must outlive the async copy: synchronise before reuse
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  return SYNX_OK;
+}
+
+// One SyN iteration on the current level (all launches asynchronous, stop-aware).
+void enqueue_iteration(synx_ctx* c, bool profile) {
+  const GridInfo& g = c->cur_grid;
+  cudaStream_t s = c->stream;
+  const int D = c->D;
+  auto ev = [&](void) -> int {
+    if (c->ev_used >= c->ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      c->ev_pool.push_back(e);
+    }
+    int idx = (int)c->ev_used++;
+    cudaEventRecord(c->ev_pool[idx], s);
+    return idx;
+  };
+  launch_warp_pair(c->Fs, c->gF, c->psiF, c->Ms, c->gM, c->psiM, g, c->Ft, c->Mt, c->ctl, s);
+  int e0 = profile ? ev() : -1;
+  launch_cc(c->Ft, c->Mt, g, c->P.cc_radius, c->gFu, c->gMu, c->cc_partials, c->ctl, s);
+  if (profile) c->ev_pairs_cc.push_back({e0, ev()});
+  // update-field smoothing, SyN epilogue (boundary zero, blend) and max ||u/spacing||
+  const float* upd[2];
+  const double var = c->P.update_variance;
+  if (var > 0.0) {
+    const float w1 = var < 0.5 ? (float)(1.0 - var / 0.5) : 1.0f;
+    const float w2 = 1.0f - w1;
+    const float* orig[2] = {c->gFu, c->gMu};
+    if (D == 3) {
+      const float* i0[2] = {c->gFu, c->gMu};
+      float* o0[2] = {c->t1F, c->t1M};
+      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, false, c->ctl, s);
+      const float* i1[2] = {c->t1F, c->t1M};
+      float* o1[2] = {c->t2F, c->t2M};
+      launch_smooth_field_pass(i1, o1, nullptr, 2, g, 1, c->coeff_upd + c->coeff_cap, c->R_upd[1], false, 1.f, 0.f,
+                               false, c->ctl, s);
+      const float* i2[2] = {c->t2F, c->t2M};
+      float* o2[2] = {c->t1F, c->t1M};
+      launch_smooth_field_pass(i2, o2, orig, 2, g, 2, c->coeff_upd + 2 * c->coeff_cap, c->R_upd[2], true, w1, w2,
+                               true, c->ctl, s);
+      upd[0] = c->t1F;
+      upd[1] = c->t1M;
+    } else {
+      const float* i0[2] = {c->gFu, c->gMu};
+      float* o0[2] = {c->t1F, c->t1M};
+      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, false, c->ctl, s);
+      const float* i1[2] = {c->t1F, c->t1M};
+      float* o1[2] = {c->t2F, c->t2M};
+      launch_smooth_field_pass(i1, o1, orig, 2, g, 1, c->coeff_upd + c->coeff_cap, c->R_upd[1], true, w1, w2, true,
+                               c->ctl, s);
+      upd[0] = c->t2F;
+      upd[1] = c->t2M;
+    }
+  } else {
+    // no smoothing (the kernel is [0 1 0]): a copy plus the max norm, boundary untouched
+    const float* i0[2] = {c->gFu, c->gMu};
+    float* o0[2] = {c->t1F, c->t1M};
+    launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, true, c->ctl, s);
+    upd[0] = c->t1F;
+    upd[1] = c->t1M;
+  }
+  // scale + compose into the forward half-fields, in place
+  {
+    const float* w[2] = {c->phiF, c->phiM};
+    float* o[2] = {c->phiF, c->phiM};
+    launch_compose(upd, w, o, 2, g, (float)c->P.learning_rate, c->ctl, s);
+  }
+  // total-field smoothing (only when its variance is positive)
+  if (c->P.total_variance > 0.0) {
+    const double vt = c->P.total_variance;
+    const float w1 = vt < 0.5 ? (float)(1.0 - vt / 0.5) : 1.0f, w2 = 1.0f - w1;
+    const float* orig[2] = {c->phiF, c->phiM};
+    if (D == 3) {
+      const float* i0[2] = {c->phiF, c->phiM};
+      float* o0[2] = {c->gFu, c->gMu};
+      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_tot, c->R_tot[0], false, 1.f, 0.f, false, c->ctl, s);
+      const float* i1[2] = {c->gFu, c->gMu};
+      float* o1[2] = {c->t2F, c->t2M};
+      launch_smooth_field_pass(i1, o1, nullptr, 2, g, 1, c->coeff_tot + c->coeff_cap, c->R_tot[1], false, 1.f, 0.f,
+                               false, c->ctl, s);
+      const float* i2[2] = {c->t2F, c->t2M};
+      float* o2[2] = {c->phiF, c->phiM};
+      launch_smooth_field_pass(i2, o2, orig, 2, g, 2, c->coeff_tot + 2 * c->coeff_cap, c->R_tot[2], true, w1, w2,
+                               false, c->ctl, s);
+    } else {
+      const float* i0[2] = {c->phiF, c->phiM};
+      float* o0[2] = {c->gFu, c->gMu};
+      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_tot, c->R_tot[0], false, 1.f, 0.f, false, c->ctl, s);
+      const float* i1[2] = {c->gFu, c->gMu};
+      float* o1[2] = {c->phiF, c->phiM};
+      launch_smooth_field_pass(i1, o1, orig, 2, g, 1, c->coeff_tot + c->coeff_cap, c->R_tot[1], true, w1, w2, false,
+                               c->ctl, s);
+    }
+  }
+  // fixed-point inverses: psi <- inv(phi) warm from psi, then phi <- inv(psi) warm from phi
+  PartialBufs pb{c->inv_psum, c->inv_pmax, c->inv_cap};
+  const int mi = c->P.inv_max_iter;
+  int e1 = profile ? ev() : -1;
+  {
+    const float* phi[2] = {c->phiF, c->phiM};
+    float* psi[2] = {c->psiF, c->psiM};
+    for (int k = 0; k <= mi; ++k)
+      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 0, pb, s);
+  }
+  {
+    const float* phi[2] = {c->psiF, c->psiM};
+    float* psi[2] = {c->phiF, c->phiM};
+    for (int k = 0; k <= mi; ++k)
+      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 1, pb, s);
+  }
+  if (profile) c->ev_pairs_inv.push_back({e1, ev()});
+  launch_converge(c->ctl, c->logdev, c->P.convergence_threshold, c->P.convergence_window, s);
+}
+
+int run_level_impl(synx_ctx* c, int level) {
+  if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_run_level: images not set");
+  if (level != c->cur_level + 1 || level >= c->P.n_levels)
+    return set_err(c, SYNX_E_STATE, "synx_run_level: levels must run in order 0.." + std::to_string(c->P.n_levels - 1));
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const GridInfo& gl = c->lv[level];
+  const int D = c->D;
+  int rc = smooth_images_for_level(c, level);
+  if (rc) return rc;
+  rc = upload_level_kernels(c, level);
+  if (rc) return rc;
+  if (level == 0) {
+    for (float* f : {c->phiF, c->psiF, c->phiM, c->psiM})
+      CUDA_TRY(c, cudaMemsetAsync(f, 0, 4 * (size_t)D * gl.d.N, c->stream));
+  } else {
+    const float* in[4] = {c->phiF, c->psiF, c->phiM, c->psiM};
+    float* out[4] = {c->gFu, c->gMu, c->t1F, c->t1M};
+    launch_resample_fields(in, c->cur_grid, out, gl, 4, c->stream);
+    std::swap(c->phiF, c->gFu);
+    std::swap(c->psiF, c->gMu);
+    std::swap(c->phiM, c->t1F);
+    std::swap(c->psiM, c->t1M);
+  }
+  c->cur_grid = gl;
+  c->cur_level = level;
+  launch_zero_ctl_level(c->ctl, c->stream);
+  CUDA_TRY(c, cudaGetLastError());
+  const int iters = c->P.iterations[level];
+  const bool profile = (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0;
+  const bool graphs = (c->P.flags & SYNX_F_USE_GRAPHS) != 0 && !profile;
+  c->ev_used = 0;
+  c->ev_pairs_inv.clear();
+  c->ev_pairs_cc.clear();
+  if (graphs && iters > 0) {
+    cudaGraph_t graph;
+    const long long before = launch_count();
+    CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration(c, false);
+    CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
+    // capture recorded one iteration's kernels; the replays below launch them `iters` times
+    add_launch_count((launch_count() - before) * (long long)(iters - 1));
+    if (c->gexec) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
+    cudaError_t e = cudaGraphInstantiate(&c->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_err(c, SYNX_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    for (int k = 0; k < iters; ++k) CUDA_TRY(c, cudaGraphLaunch(c->gexec, c->stream));
+  } else {
+    for (int k = 0; k < iters; ++k) enqueue_iteration(c, profile);
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  // collect the level's log
+  IterCtl hctl;
+  CUDA_TRY(c, cudaMemcpyAsync(&hctl, c->ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<double> lm(std::max(iters, 1)), lc(std::max(iters, 1));
+  std::vector<int> li(std::max(iters, 1));
+  if (iters > 0) {
+    CUDA_TRY(c, cudaMemcpyAsync(lm.data(), c->logdev.metric, 8 * iters, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(lc.data(), c->logdev.conv, 8 * iters, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(li.data(), c->logdev.inv_iters, 4 * iters, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const int done = std::min(hctl.iter, iters);
+  long long sub_iters = 0;
+  for (int k = 0; k < done; ++k) {
+    c->log_level.push_back(level);
+    c->log_iter.push_back(k + 1);
+    c->log_metric.push_back(lm[k]);
+    c->log_conv.push_back(lc[k]);
+    c->log_inv.push_back(li[k]);
+    sub_iters += li[k];
+  }
+  if (profile) {
+    for (auto& pr : c->ev_pairs_inv) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev_pool[pr.first], c->ev_pool[pr.second]);
+      c->prof_inv_ms += ms;
+    }
+    for (auto& pr : c->ev_pairs_cc) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev_pool[pr.first], c->ev_pool[pr.second]);
+      c->prof_cc_ms += ms;
+      c->prof_cc_launches += 1;
+      c->prof_cc_vox += gl.d.N;
+    }
+    // each executed fixed-point iteration is one working launch over one half-field
+    c->prof_inv_launches += sub_iters;
+    c->prof_inv_vox += sub_iters * gl.d.N;
+  }
+  return SYNX_OK;
+}
+
+bool valid_ctx(const synx_ctx* c) { return c != nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+int synx_params_default(synx_params* p, int dim) {
+  if (!p) return set_err(nullptr, SYNX_E_ARG, "synx_params_default: null");
+  if (dim != 2 && dim != 3) return set_err(nullptr, SYNX_E_ARG, "synx_params_default: dim must be 2 or 3");
+  memset(p, 0, sizeof(*p));
+  p->dim = dim;
+  p->n_levels = 1;
+  p->learning_rate = 0.1;
+  p->update_variance = 3.0;
+  p->total_variance = 0.0;
+  p->cc_radius = 4;
+  p->sigmas_in_mm = 0;
+  p->iterations[0] = 1;
+  p->shrink_factors[0] = 1;
+  p->smoothing_sigmas[0] = 0.0;
+  p->convergence_threshold = 1e-6;
+  p->convergence_window = 10;
+  p->preprocess = 1;
+  p->winsor_lower = 0.0f;
+  p->winsor_upper = 1.0f;
+  p->inv_max_iter = 20;
+  p->inv_mean_tol = 0.001;
+  p->inv_max_tol = 0.1;
+  p->flags = 0;
+  return SYNX_OK;
+}
+
+const char* synx_last_error(const synx_ctx* ctx) {
+  if (ctx) return ctx->err.c_str();
+  return g_last_error.c_str();
+}
+
+int synx_create(const synx_params* params, int device, void* cuda_stream, synx_ctx** out) {
+  if (!params || !out) return set_err(nullptr, SYNX_E_ARG, "synx_create: null argument");
+  *out = nullptr;
+  const synx_params& p = *params;
+  if (p.dim != 2 && p.dim != 3) return set_err(nullptr, SYNX_E_ARG, "synx_create: dim must be 2 or 3");
+  if (p.n_levels < 1 || p.n_levels > SYNX_MAX_LEVELS)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: n_levels must be in 1..8");
+  for (int l = 0; l < p.n_levels; ++l) {
+    if (p.iterations[l] < 0) return set_err(nullptr, SYNX_E_ARG, "synx_create: negative iteration count");
+    if (p.shrink_factors[l] < 1) return set_err(nullptr, SYNX_E_ARG, "synx_create: shrink factors must be >= 1");
+    if (p.smoothing_sigmas[l] < 0) return set_err(nullptr, SYNX_E_ARG, "synx_create: negative smoothing sigma");
+  }
+  if (!cc_radius_supported(p.dim, p.cc_radius))
+    return set_err(nullptr, SYNX_E_UNSUPPORTED, "synx_create: CC radius must be in 1..7");
+  if (!(p.learning_rate > 0)) return set_err(nullptr, SYNX_E_ARG, "synx_create: learning rate must be > 0");
+  if (p.convergence_window < 2 || p.convergence_window > kMaxWindow)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: convergence window must be in 2..64");
+  if (p.inv_max_iter < 1 || p.inv_max_iter > 1000)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: inverse iteration cap must be in 1..1000");
+  if (p.update_variance < 0 || p.total_variance < 0)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: negative smoothing variance");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_err(nullptr, SYNX_E_CUDA, "synx_create: no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return set_err(nullptr, SYNX_E_ARG, "synx_create: bad device index");
+  synx_ctx* c = new synx_ctx();
+  c->P = p;
+  c->D = p.dim;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return set_err(nullptr, SYNX_E_CUDA, "synx_create: cudaSetDevice failed");
+  }
+  if (cuda_stream) {
+    c->stream = (cudaStream_t)cuda_stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return set_err(nullptr, SYNX_E_CUDA, "synx_create: stream creation failed");
+    }
+    c->own_stream = true;
+  }
+  cudaError_t e = cc_prepare(p.dim, p.cc_radius);
+  if (e != cudaSuccess) {
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return set_err(nullptr, SYNX_E_CUDA, std::string("synx_create: CC kernel setup: ") + cudaGetErrorString(e));
+  }
+  *out = c;
+  return SYNX_OK;
+}
+
+int synx_destroy(synx_ctx* ctx) {
+  if (!ctx) return SYNX_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_arena(ctx);
+  for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return SYNX_OK;
+}
+
+static int set_images_common(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm,
+                             cudaMemcpyKind kind) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (!F || !M) return set_err(c, SYNX_E_ARG, "synx_set_images: null image pointer");
+  if (!check_geom(gf, c->D) || !check_geom(gm, c->D))
+    return set_err(c, SYNX_E_ARG, "synx_set_images: image geometry does not match the stage dimension or is invalid");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->geF = *gf;
+  c->geM = *gm;
+  geom_to_grid(c->geF, c->gF);
+  geom_to_grid(c->geM, c->gM);
+  c->NF = c->gF.d.N;
+  c->NM = c->gM.d.N;
+  int rc = build_levels(c);
+  if (rc) return rc;
+  rc = allocate(c);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaMemcpyAsync(c->F0, F, 4 * c->NF, kind, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->M0, M, 4 * c->NM, kind, c->stream));
+  if (c->P.preprocess) {
+    rc = preprocess(c, c->F0, c->NF);
+    if (rc) return rc;
+    rc = preprocess(c, c->M0, c->NM);
+    if (rc) return rc;
+  }
+  c->images_set = true;
+  c->cur_level = -1;
+  c->log_level.clear();
+  c->log_iter.clear();
+  c->log_metric.clear();
+  c->log_conv.clear();
+  c->log_inv.clear();
+  CUDA_TRY(c, cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_set_images(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm) {
+  return set_images_common(c, F, gf, M, gm, cudaMemcpyHostToDevice);
+}
+int synx_set_images_device(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm) {
+  return set_images_common(c, F, gf, M, gm, cudaMemcpyDeviceToDevice);
+}
+
+int synx_run_level(synx_ctx* c, int level) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  return run_level_impl(c, level);
+}
+
+int synx_run(synx_ctx* c) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_run: images not set");
+  for (int l = c->cur_level + 1; l < c->P.n_levels; ++l) {
+    int rc = run_level_impl(c, l);
+    if (rc) return rc;
+  }
+  return SYNX_OK;
+}
+
+int synx_get_output_geom(const synx_ctx* c, synx_geom* out) {
+  if (!valid_ctx(c) || !out) return set_err(nullptr, SYNX_E_ARG, "synx_get_output_geom: null argument");
+  if (c->cur_level < 0) return set_err(const_cast<synx_ctx*>(c), SYNX_E_STATE, "no level has run");
+  *out = c->lgeom[c->cur_level];
+  return SYNX_OK;
+}
+
+static int final_fields(synx_ctx* c, float* fwd_planes, float* inv_planes) {
+  const GridInfo& g = c->cur_grid;
+  {
+    const float* d[1] = {c->psiM};
+    const float* w[1] = {c->phiF};
+    float* o[1] = {fwd_planes};
+    launch_compose(d, w, o, 1, g, -1.0f, nullptr, c->stream);
+  }
+  {
+    const float* d[1] = {c->psiF};
+    const float* w[1] = {c->phiM};
+    float* o[1] = {inv_planes};
+    launch_compose(d, w, o, 1, g, -1.0f, nullptr, c->stream);
+  }
+  return SYNX_OK;
+}
+
+static int get_fields_common(synx_ctx* c, float* fwd, float* inv, bool host) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (c->cur_level < 0) return set_err(c, SYNX_E_STATE, "synx_get_fields: no level has run");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const GridInfo& g = c->cur_grid;
+  const size_t n = (size_t)c->D * g.d.N;
+  // final composition into work buffers, then interleave
+  final_fields(c, c->t2F, c->t2M);
+  launch_interleave(c->t2F, c->gFu, g.d.N, c->D, c->stream);
+  launch_interleave(c->t2M, c->gMu, g.d.N, c->D, c->stream);
+  const cudaMemcpyKind kind = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  if (fwd) CUDA_TRY(c, cudaMemcpyAsync(fwd, c->gFu, 4 * n, kind, c->stream));
+  if (inv) CUDA_TRY(c, cudaMemcpyAsync(inv, c->gMu, 4 * n, kind, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return SYNX_OK;
+}
+
+int synx_get_fields(synx_ctx* c, float* fwd, float* inv) { return get_fields_common(c, fwd, inv, true); }
+int synx_get_fields_device(synx_ctx* c, float* fwd, float* inv) { return get_fields_common(c, fwd, inv, false); }
+
+int synx_get_half_fields(synx_ctx* c, float* phi_f, float* psi_f, float* phi_m, float* psi_m) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (c->cur_level < 0) return set_err(c, SYNX_E_STATE, "synx_get_half_fields: no level has run");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const GridInfo& g = c->cur_grid;
+  const size_t n = (size_t)c->D * g.d.N;
+  float* outs[4] = {phi_f, psi_f, phi_m, psi_m};
+  const float* srcs[4] = {c->phiF, c->psiF, c->phiM, c->psiM};
+  for (int k = 0; k < 4; ++k) {
+    if (!outs[k]) continue;
+    launch_interleave(srcs[k], c->t2F, g.d.N, c->D, c->stream);
+    CUDA_TRY(c, cudaMemcpyAsync(outs[k], c->t2F, 4 * n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  return SYNX_OK;
+}
+
+int synx_set_half_fields(synx_ctx* c, const float* phi_f, const float* psi_f, const float* phi_m, const float* psi_m,
+                         const synx_geom* grid) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_set_half_fields: images not set");
+  if (!phi_f || !psi_f || !phi_m || !psi_m || !check_geom(grid, c->D))
+    return set_err(c, SYNX_E_ARG, "synx_set_half_fields: bad arguments");
+  // the grid must be one of the level grids; the next level to run is the one after it
+  int lvl = -1;
+  for (int l = 0; l < (int)c->lgeom.size(); ++l) {
+    const synx_geom& g = c->lgeom[l];
+    bool same = true;
+    for (int d = 0; d < 3; ++d) same = same && g.size[d] == grid->size[d];
+    if (same) {
+      lvl = l;
+      break;
+    }
+  }
+  if (lvl < 0) return set_err(c, SYNX_E_ARG, "synx_set_half_fields: grid is not a level grid of this stage");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const GridInfo& g = c->lv[lvl];
+  const size_t n = (size_t)c->D * g.d.N;
+  const float* ins[4] = {phi_f, psi_f, phi_m, psi_m};
+  float* dsts[4] = {c->phiF, c->psiF, c->phiM, c->psiM};
+  for (int k = 0; k < 4; ++k) {
+    CUDA_TRY(c, cudaMemcpyAsync(c->t2F, ins[k], 4 * n, cudaMemcpyHostToDevice, c->stream));
+    launch_deinterleave(c->t2F, dsts[k], g.d.N, c->D, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  c->cur_grid = g;
+  c->cur_level = lvl;
+  return SYNX_OK;
+}
+
+int synx_get_log(synx_ctx* c, int32_t* level, int32_t* iteration, double* metric, double* convergence,
+                 int32_t* inverse_iterations, int64_t capacity, int64_t* count) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  const int64_t n = (int64_t)c->log_metric.size();
+  if (count) *count = n;
+  for (int64_t i = 0; i < n && i < capacity; ++i) {
+    if (level) level[i] = c->log_level[i];
+    if (iteration) iteration[i] = c->log_iter[i];
+    if (metric) metric[i] = c->log_metric[i];
+    if (convergence) convergence[i] = c->log_conv[i];
+    if (inverse_iterations) inverse_iterations[i] = c->log_inv[i];
+  }
+  return SYNX_OK;
+}
+
+int synx_get_profile(synx_ctx* c, double* inv_ms, int64_t* inv_launches, int64_t* inv_vox, double* cc_ms,
+                     int64_t* cc_launches, int64_t* cc_vox) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (inv_ms) *inv_ms = c->prof_inv_ms;
+  if (inv_launches) *inv_launches = c->prof_inv_launches;
+  if (inv_vox) *inv_vox = c->prof_inv_vox;
+  if (cc_ms) *cc_ms = c->prof_cc_ms;
+  if (cc_launches) *cc_launches = c->prof_cc_launches;
+  if (cc_vox) *cc_vox = c->prof_cc_vox;
+  return SYNX_OK;
+}
+
+int synx_reset_profile(synx_ctx* c) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  c->prof_inv_ms = c->prof_cc_ms = 0;
+  c->prof_inv_launches = c->prof_inv_vox = c->prof_cc_launches = c->prof_cc_vox = 0;
+  return SYNX_OK;
+}
+
+int synx_get_launch_count(int64_t* count) {
+  if (!count) return set_err(nullptr, SYNX_E_ARG, "synx_get_launch_count: null");
+  *count = (int64_t)launch_count();
+  return SYNX_OK;
+}
+
+int synx_get_device_bytes(const synx_ctx* c, int64_t* bytes) {
+  if (!valid_ctx(c) || !bytes) return set_err(nullptr, SYNX_E_ARG, "null argument");
+  *bytes = (int64_t)c->arena_bytes;
+  return SYNX_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Step entry points
+// ------------------------------------------------------------------------------------------
+int synx_gaussian_kernel(double variance, double max_error, int max_width, double* coeffs, int cap, int* len) {
+  if (max_width < 1 || !(max_error > 0) || max_error >= 1)
+    return set_err(nullptr, SYNX_E_ARG, "synx_gaussian_kernel: bad arguments");
+  auto k = gauss_kernel(variance, max_error, (size_t)max_width);
+  if (len) *len = (int)k.size();
+  for (int i = 0; i < (int)k.size() && i < cap && coeffs; ++i) coeffs[i] = k[i];
+  return SYNX_OK;
+}
+
+int synx_shrink_geom(const synx_geom* in, int factor, synx_geom* out) {
+  if (!in || !out || factor < 1 || (in->dim != 2 && in->dim != 3))
+    return set_err(nullptr, SYNX_E_ARG, "synx_shrink_geom: bad arguments");
+  *out = shrink(*in, (unsigned)factor);
+  return SYNX_OK;
+}
+
+namespace {
+struct TempCtl {
+  IterCtl* ctl = nullptr;
+  double* part = nullptr;
+  float* pmax = nullptr;
+  int cap = 0;
+  cudaError_t alloc(int partials) {
+    cap = partials;
+    cudaError_t e = cudaMalloc((void**)&ctl, sizeof(IterCtl));
+    if (e) return e;
+    e = cudaMalloc((void**)&part, 8 * 2 * (size_t)std::max(partials, 1));
+    if (e) return e;
+    e = cudaMalloc((void**)&pmax, 4 * 2 * (size_t)std::max(partials, 1));
+    return e;
+  }
+  ~TempCtl() {
+    if (ctl) cudaFree(ctl);
+    if (part) cudaFree(part);
+    if (pmax) cudaFree(pmax);
+  }
+};
+}  // namespace
+
+#define STEP_TRY(call)                                                                              \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess)                                                                          \
+      return set_err(nullptr, SYNX_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+int synx_smooth_image(const float* in, float* out, const synx_geom* gg, double sigma, int mm, void* stream) {
+  if (!in || !out || !gg || (gg->dim != 2 && gg->dim != 3) || !check_geom(gg, gg->dim) || sigma < 0)
+    return set_err(nullptr, SYNX_E_ARG, "synx_smooth_image: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  GridInfo g;
+  geom_to_grid(*gg, g);
+  if (sigma == 0.0) {
+    STEP_TRY(cudaMemcpyAsync(out, in, 4 * g.d.N, cudaMemcpyDeviceToDevice, s));
+    return SYNX_OK;
+  }
+  double* dk = nullptr;
+  float* tmp = nullptr;
+  STEP_TRY(cudaMalloc((void**)&dk, 8 * 3 * 64));
+  STEP_TRY(cudaMalloc((void**)&tmp, 4 * g.d.N));
+  std::vector<double> hk(3 * 64, 0.0);
+  int R[3] = {0, 0, 0};
+  for (int a = 0; a < gg->dim; ++a) {
+    double var = sigma * sigma;
+    if (mm) var /= g.sp[a] * g.sp[a];
+    auto k = gauss_kernel(var, 0.01, 32);
+    R[a] = (int)k.size() / 2;
+    for (size_t j = 0; j < k.size(); ++j) hk[a * 64 + j] = k[j];
+  }
+  STEP_TRY(cudaMemcpyAsync(dk, hk.data(), 8 * 3 * 64, cudaMemcpyHostToDevice, s));
+  const float* src = in;
+  const int D = gg->dim;
+  for (int p = 0; p < D; ++p) {
+    const int axis = D - 1 - p;
+    float* o = ((D - 1 - p) % 2 == 0) ? out : tmp;
+    launch_conv_image_axis(src, o, g, axis, dk + axis * 64, R[axis], s);
+    src = o;
+  }
+  STEP_TRY(cudaStreamSynchronize(s));
+  cudaFree(dk);
+  cudaFree(tmp);
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_warp_image(const float* img, const synx_geom* gi, const float* u, const synx_geom* gv, float* out,
+                    void* stream) {
+  if (!img || !u || !out || !gi || !gv || !check_geom(gi, gi->dim) || !check_geom(gv, gi->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_warp_image: bad arguments");
+  GridInfo a, b;
+  geom_to_grid(*gi, a);
+  geom_to_grid(*gv, b);
+  launch_warp_image(img, a, u, b, out, (cudaStream_t)stream);
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_cc_metric(const float* F, const float* M, const synx_geom* gg, int radius, float* gF, float* gM,
+                   double* value, void* stream) {
+  if (!F || !M || !gF || !gM || !gg || !check_geom(gg, gg->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_cc_metric: bad arguments");
+  if (!cc_radius_supported(gg->dim, radius)) return set_err(nullptr, SYNX_E_UNSUPPORTED, "synx_cc_metric: radius");
+  cudaStream_t s = (cudaStream_t)stream;
+  GridInfo g;
+  geom_to_grid(*gg, g);
+  STEP_TRY(cc_prepare(gg->dim, radius));
+  TempCtl t;
+  STEP_TRY(t.alloc(cc_blocks(g, radius)));
+  STEP_TRY(cudaMemsetAsync(t.ctl, 0, sizeof(IterCtl), s));
+  launch_cc(F, M, g, radius, gF, gM, t.part, t.ctl, s);
+  IterCtl h;
+  STEP_TRY(cudaMemcpyAsync(&h, t.ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, s));
+  STEP_TRY(cudaStreamSynchronize(s));
+  if (value) *value = h.metric;
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_smooth_field(const float* in, float* out, const synx_geom* gg, double variance, double* max_norm,
+                      void* stream) {
+  if (!in || !out || !gg || !check_geom(gg, gg->dim) || variance < 0)
+    return set_err(nullptr, SYNX_E_ARG, "synx_smooth_field: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  GridInfo g;
+  geom_to_grid(*gg, g);
+  const int D = gg->dim;
+  const size_t n = (size_t)D * g.d.N;
+  TempCtl t;
+  STEP_TRY(t.alloc(1));
+  STEP_TRY(cudaMemsetAsync(t.ctl, 0, sizeof(IterCtl), s));
+  float* coeff = nullptr;
+  float *ta = nullptr, *tb = nullptr;
+  STEP_TRY(cudaMalloc((void**)&coeff, 4 * 3 * 1024));
+  STEP_TRY(cudaMalloc((void**)&ta, 4 * n));
+  STEP_TRY(cudaMalloc((void**)&tb, 4 * n));
+  std::vector<float> hk(3 * 1024, 0.0f);
+  int R[3] = {0, 0, 0};
+  for (int a = 0; a < D; ++a) {
+    const int len = a == 0 ? g.d.nx : (a == 1 ? g.d.ny : g.d.nz);
+    auto k = gauss_kernel(variance, 0.001, (size_t)len);
+    if (k.size() > 1024) return set_err(nullptr, SYNX_E_UNSUPPORTED, "synx_smooth_field: kernel too wide");
+    R[a] = (int)k.size() / 2;
+    for (size_t j = 0; j < k.size(); ++j) hk[a * 1024 + j] = (float)k[j];
+  }
+  STEP_TRY(cudaMemcpyAsync(coeff, hk.data(), 4 * 3 * 1024, cudaMemcpyHostToDevice, s));
+  if (variance <= 0.0) {
+    const float* i0[1] = {in};
+    float* o0[1] = {out};
+    launch_smooth_field_pass(i0, o0, nullptr, 1, g, 0, coeff, R[0], false, 1.f, 0.f, true, t.ctl, s);
+  } else {
+    const float w1 = variance < 0.5 ? (float)(1.0 - variance / 0.5) : 1.0f, w2 = 1.0f - w1;
+    const float* orig[1] = {in};
+    const float* src = in;
+    for (int a = 0; a < D; ++a) {
+      const bool last = a == D - 1;
+      float* dst = last ? out : (a % 2 == 0 ? ta : tb);
+      const float* i0[1] = {src};
+      float* o0[1] = {dst};
+      launch_smooth_field_pass(i0, o0, last ? orig : nullptr, 1, g, a, coeff + a * 1024, R[a], last, w1, w2, last,
+                               t.ctl, s);
+      src = dst;
+    }
+  }
+  IterCtl h;
+  STEP_TRY(cudaMemcpyAsync(&h, t.ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, s));
+  STEP_TRY(cudaStreamSynchronize(s));
+  if (max_norm) {
+    float f;
+    memcpy(&f, &h.maxnorm[0], 4);
+    *max_norm = f;
+  }
+  cudaFree(coeff);
+  cudaFree(ta);
+  cudaFree(tb);
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_compose(const float* d, const float* w, const synx_geom* gg, float scale, float* out, void* stream) {
+  if (!d || !w || !out || !gg || !check_geom(gg, gg->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_compose: bad arguments");
+  GridInfo g;
+  geom_to_grid(*gg, g);
+  const float* dd[1] = {d};
+  const float* ww[1] = {w};
+  float* oo[1] = {out};
+  if (scale == 1.0f) {
+    launch_compose(dd, ww, oo, 1, g, -1.0f, nullptr, (cudaStream_t)stream);
+  } else {
+    // scale via a constant max-norm: maxnorm = 1 / scale with eta = 1 gives scale
+    TempCtl t;
+    STEP_TRY(t.alloc(1));
+    IterCtl h;
+    memset(&h, 0, sizeof(h));
+    float inv = 1.0f / scale;
+    memcpy(&h.maxnorm[0], &inv, 4);
+    STEP_TRY(cudaMemcpyAsync(t.ctl, &h, sizeof(IterCtl), cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    launch_compose(dd, ww, oo, 1, g, 1.0f, t.ctl, (cudaStream_t)stream);
+    STEP_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  }
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_invert_field(const float* phi, float* psi, const synx_geom* gg, int max_iter, double mean_tol, double max_tol,
+                      int* iterations, void* stream) {
+  if (!phi || !psi || !gg || !check_geom(gg, gg->dim) || max_iter < 1)
+    return set_err(nullptr, SYNX_E_ARG, "synx_invert_field: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  GridInfo g;
+  geom_to_grid(*gg, g);
+  TempCtl t;
+  const int nb = inv_blocks(g);
+  STEP_TRY(t.alloc(nb));
+  STEP_TRY(cudaMemsetAsync(t.ctl, 0, sizeof(IterCtl), s));
+  PartialBufs pb{t.part, t.pmax, nb};
+  const float* pp[1] = {phi};
+  float* ps[1] = {psi};
+  for (int k = 0; k <= max_iter; ++k) launch_invert_step(pp, ps, 1, g, k, max_iter, mean_tol, max_tol, t.ctl, 0, pb, s);
+  IterCtl h;
+  STEP_TRY(cudaMemcpyAsync(&h, t.ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, s));
+  STEP_TRY(cudaStreamSynchronize(s));
+  if (iterations) *iterations = h.inv[0][0].iters;
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+int synx_resample_field(const float* in, const synx_geom* gi, float* out, const synx_geom* go, void* stream) {
+  if (!in || !out || !gi || !go || !check_geom(gi, gi->dim) || !check_geom(go, gi->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_resample_field: bad arguments");
+  GridInfo a, b;
+  geom_to_grid(*gi, a);
+  geom_to_grid(*go, b);
+  const float* ii[1] = {in};
+  float* oo[1] = {out};
+  launch_resample_fields(ii, a, oo, b, 1, (cudaStream_t)stream);
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
+}  // extern "C"

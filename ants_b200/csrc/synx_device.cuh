@@ -1,0 +1,136 @@
+// Device-side building blocks shared by the synx kernels: grid descriptors, ITK's linear
+// interpolation buffer rule, deterministic block reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace synx {
+
+// Voxel counts of one grid.  nz = 1 for 2-D.
+struct Dims {
+  int nx, ny, nz;
+  int dim;
+  long long N;
+};
+
+// Continuous index into a target grid of a source-grid voxel i displaced by u (physical):
+// c = t + B * i + A * u.  For a single grid (composition, inversion) t = 0, B = I and
+// A = inverse(direction * diag(spacing)).
+struct Affine {
+  float t[3];
+  float B[9];
+  float A[9];
+};
+
+// ITK ImageFunction::IsInsideBuffer: start-0.5 <= c < end+0.5 per axis (NaN is outside).
+template <int DIM>
+__device__ __forceinline__ bool inside_buffer(const Dims& d, float cx, float cy, float cz) {
+  bool ok = (cx >= -0.5f) && (cx < (float)d.nx - 0.5f) && (cy >= -0.5f) && (cy < (float)d.ny - 0.5f);
+  if (DIM == 3) ok = ok && (cz >= -0.5f) && (cz < (float)d.nz - 0.5f);
+  return ok;
+}
+
+// Clamp-to-edge cell of ITK's (Vector)LinearInterpolateImageFunction for c inside the buffer.
+__device__ __forceinline__ void axis_cell(float c, int n, int& i0, int& i1, float& w) {
+  float f = floorf(c);
+  int b = (int)f;
+  w = c - f;
+  if (b < 0) {
+    b = 0;
+    w = 0.0f;
+  }
+  int u = b + 1;
+  if (u > n - 1) {
+    u = n - 1;
+    w = 0.0f;
+  }
+  i0 = b;
+  i1 = u;
+}
+
+struct Cell {
+  long long o000, dx, dy, dz;  // base offset and the per-axis offset to the upper neighbour
+  float wx, wy, wz;
+};
+
+template <int DIM>
+__device__ __forceinline__ Cell make_cell(const Dims& d, float cx, float cy, float cz) {
+  Cell c;
+  int x0, x1, y0, y1, z0 = 0, z1 = 0;
+  axis_cell(cx, d.nx, x0, x1, c.wx);
+  axis_cell(cy, d.ny, y0, y1, c.wy);
+  c.wz = 0.0f;
+  if (DIM == 3) axis_cell(cz, d.nz, z0, z1, c.wz);
+  const long long sy = d.nx, sz = (long long)d.nx * d.ny;
+  c.o000 = (long long)z0 * sz + (long long)y0 * sy + x0;
+  c.dx = x1 - x0;
+  c.dy = (long long)(y1 - y0) * sy;
+  c.dz = (long long)(z1 - z0) * sz;
+  return c;
+}
+
+// Multilinear interpolation in the lerp form a + (b - a) w, x then y then z.
+template <int DIM>
+__device__ __forceinline__ float lerp_at(const float* __restrict__ a, const Cell& c) {
+  const float* p = a + c.o000;
+  float v00 = __ldg(p), v10 = __ldg(p + c.dx);
+  float v01 = __ldg(p + c.dy), v11 = __ldg(p + c.dy + c.dx);
+  float a0 = fmaf(v10 - v00, c.wx, v00);
+  float a1 = fmaf(v11 - v01, c.wx, v01);
+  float b0 = fmaf(a1 - a0, c.wy, a0);
+  if (DIM == 2) return b0;
+  const float* q = p + c.dz;
+  float u00 = __ldg(q), u10 = __ldg(q + c.dx);
+  float u01 = __ldg(q + c.dy), u11 = __ldg(q + c.dy + c.dx);
+  float c0 = fmaf(u10 - u00, c.wx, u00);
+  float c1 = fmaf(u11 - u01, c.wx, u01);
+  float b1 = fmaf(c1 - c0, c.wy, c0);
+  return fmaf(b1 - b0, c.wz, b0);
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Fixed-order block sum (valid in thread 0).  blockDim.x must be a multiple of 32, <= 1024.
+__device__ __forceinline__ double block_sum_d(double v, double* sh /* >= 32 */) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = warp_sum_d(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = lane < nw ? sh[lane] : 0.0;
+    r = warp_sum_d(r);
+  }
+  return r;
+}
+__device__ __forceinline__ float block_max_f(float v, float* sh /* >= 32 */) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = warp_max_f(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  float r = 0.0f;
+  if (w == 0) {
+    r = lane < nw ? sh[lane] : 0.0f;
+    r = warp_max_f(r);
+  }
+  return r;
+}
+
+// Non-negative floats order like their bit patterns: atomicMax on the bits is a float max.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned int* addr, float v) {
+  atomicMax(addr, __float_as_uint(fmaxf(v, 0.0f)));
+}
+
+}  // namespace synx

@@ -1,0 +1,123 @@
+// Host-side launch interface of the synx kernels (C++ linkage, internal to libsynx).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "synx_device.cuh"
+
+namespace synx {
+
+// Fixed-point inverse control block, one per (phase, half).  Slot k%2 holds the decision
+// and statistics consumed by launch k; launch k writes slot (k+1)%2.
+struct InvCtl {
+  int exec[2];
+  float maxv[2];
+  double mean[2];
+  int iters;
+  unsigned counter;
+  int pad[2];
+};
+
+constexpr int kMaxWindow = 64;
+
+// Device-resident control block of one registration context.
+struct IterCtl {
+  int stop;                   // 1 once the level converged: iteration kernels return at once
+  int iter;                   // iterations completed in the current level
+  unsigned maxnorm[2];        // float bits of max ||u / spacing|| per half (fixed, moving)
+  unsigned cc_counter;        // block arrival counter of the CC reduction
+  int pad0;
+  double cc_sum;              // sum of local cc of the last evaluation
+  double metric;              // -mean cc of the last evaluation
+  double total_abs;           // running sum of |metric| over the level
+  double energies[kMaxWindow];
+  InvCtl inv[2][2];           // [phase A (psi), phase B (phi)][half]
+};
+
+struct LogDev {
+  double* metric;
+  double* conv;
+  int* inv_iters;
+  int cap;
+};
+
+// Geometry helpers (host).
+struct GridInfo {
+  Dims d;
+  double sp[3], org[3], dir[9], i2p[9], p2i[9];
+};
+
+GridInfo make_grid(int dim, const int64_t size[3], const double sp[3], const double org[3], const double dir[9]);
+// c = t + B i + A u mapping voxel i of `src` displaced by u into continuous index of `dst`.
+Affine make_affine(const GridInfo& src, const GridInfo& dst);
+
+struct PartialBufs {
+  double* sum;       // per-block partial sums
+  float* maxv;       // per-block partial max
+  int capacity;      // entries per half
+};
+
+// ---- launchers (all asynchronous on `s`) -----------------------------------------------
+void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s);
+
+void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, const float* M, const GridInfo& gM,
+                      const float* psiM, const GridInfo& gv, float* Ft, float* Mt, IterCtl* ctl, cudaStream_t s);
+void launch_warp_image(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
+                       cudaStream_t s);
+
+// Returns the number of blocks the CC launch uses (partials needed).
+int cc_blocks(const GridInfo& g, int radius);
+size_t cc_smem_bytes(int dim, int radius);
+bool cc_radius_supported(int dim, int radius);
+// Raise the dynamic shared-memory limit of the CC kernel (once per device, outside capture).
+cudaError_t cc_prepare(int dim, int radius);
+void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
+               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr);
+
+// Separable smoothing of `halves` fields (each dim components) along one axis.
+// `last` applies the SyN epilogue: zero boundary, blend with `orig` (w2 != 0), and the max
+// ||u/spacing|| reduction into ctl->maxnorm when `maxnorm` is set.
+void launch_smooth_field_pass(const float* const* in, float* const* out, const float* const* orig, int halves,
+                              const GridInfo& g, int axis, const float* coeffs, int R, bool last, float w1, float w2,
+                              bool maxnorm, IterCtl* ctl, cudaStream_t s);
+
+// out = w + scale * d(x + w); scale = eta / maxnorm[h] when eta > 0, else 1.  In place when
+// out == w.
+void launch_compose(const float* const* d, const float* const* w, float* const* out, int halves, const GridInfo& g,
+                    float eta, IterCtl* ctl, cudaStream_t s);
+
+// One launch of the fused fixed-point inverse (k = 0 .. max_iter) for `halves` pairs.
+int inv_blocks(const GridInfo& g);
+void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
+                        double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
+                        bool stop_aware = true);
+
+void launch_converge(IterCtl* ctl, LogDev log, double threshold, int window, cudaStream_t s);
+
+void launch_resample_fields(const float* const* in, const GridInfo& gi, float* const* out, const GridInfo& go,
+                            int nfields, cudaStream_t s);
+
+// Image pyramid: one axis pass, double accumulation.
+void launch_conv_image_axis(const float* in, float* out, const GridInfo& g, int axis, const double* coeffs, int R,
+                            cudaStream_t s);
+
+// Intensity statistics / window.
+void launch_minmax(const float* x, long long n, unsigned* mm /* [2]: ordered-int min, max */, cudaStream_t s);
+void launch_histogram(const float* x, long long n, float lo, float hi, int nbins, unsigned* hist, cudaStream_t s);
+void launch_window(const float* in, float* out, long long n, float wlo, float whi, double scale, double shift,
+                   cudaStream_t s);
+
+// Layout conversion: interleaved (x,y,z per voxel) <-> component planes.
+void launch_interleave(const float* planes, float* inter, long long N, int D, cudaStream_t s);
+void launch_deinterleave(const float* inter, float* planes, long long N, int D, cudaStream_t s);
+
+// Process-wide kernel launch counter (graph replays are added by the caller).
+long long launch_count();
+void add_launch_count(long long n);
+
+// Ordered-int encoding of floats for atomic min/max.
+unsigned float_to_ordered(float f);
+float ordered_to_float(unsigned u);
+
+}  // namespace synx

@@ -1,0 +1,433 @@
+"""ctypes binding of the synx C ABI (include/synx.h).
+
+This is the Python mirror of the reference's stage interface: a `SyNStage` is configured
+with the values antsRegistration parses from `-t SyN[...] -m CC[...] -c ... -f ... -s ...`
+(Examples/antsRegistrationTemplateHeader.h:545-651, :801-815, :1081-1087) and run on one
+fixed/moving pair; it returns the forward (prefix0Warp) and inverse (prefix0InverseWarp)
+displacement fields.  Every call goes through libsynx.so; there is no CPU path.  Loading the
+library fails loudly if it has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsynx.so")
+
+SYNX_MAX_LEVELS = 8
+SYNX_F_PROFILE_EVENTS = 0x1
+SYNX_F_USE_GRAPHS = 0x2
+
+ERRORS = {-1: "invalid argument", -2: "bad state", -3: "CUDA error", -4: "out of device memory", -5: "unsupported"}
+
+
+class SynxGeom(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("size", C.c_int64 * 3),
+        ("spacing", C.c_double * 3),
+        ("origin", C.c_double * 3),
+        ("direction", C.c_double * 9),
+    ]
+
+
+class SynxParams(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32),
+        ("n_levels", C.c_int32),
+        ("learning_rate", C.c_double),
+        ("update_variance", C.c_double),
+        ("total_variance", C.c_double),
+        ("cc_radius", C.c_int32),
+        ("sigmas_in_mm", C.c_int32),
+        ("iterations", C.c_int32 * SYNX_MAX_LEVELS),
+        ("shrink_factors", C.c_int32 * SYNX_MAX_LEVELS),
+        ("smoothing_sigmas", C.c_double * SYNX_MAX_LEVELS),
+        ("convergence_threshold", C.c_double),
+        ("convergence_window", C.c_int32),
+        ("preprocess", C.c_int32),
+        ("winsor_lower", C.c_float),
+        ("winsor_upper", C.c_float),
+        ("inv_max_iter", C.c_int32),
+        ("flags", C.c_int32),
+        ("inv_mean_tol", C.c_double),
+        ("inv_max_tol", C.c_double),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+# ---- geometry --------------------------------------------------------------------------------
+@dataclass
+class Geom:
+    """ITK image information: p = origin + direction @ diag(spacing) @ index (index x-fastest)."""
+
+    size: tuple  # (nx, ny) or (nx, ny, nz)
+    spacing: tuple = None
+    origin: tuple = None
+    direction: np.ndarray = None
+
+    def __post_init__(self):
+        d = len(self.size)
+        if d not in (2, 3):
+            raise ValueError("size must have 2 or 3 entries")
+        self.size = tuple(int(s) for s in self.size)
+        self.spacing = tuple(float(s) for s in (self.spacing or (1.0,) * d))
+        self.origin = tuple(float(s) for s in (self.origin or (0.0,) * d))
+        if self.direction is None:
+            self.direction = np.eye(d)
+        self.direction = np.asarray(self.direction, dtype=np.float64).reshape(d, d)
+
+    @property
+    def dim(self) -> int:
+        return len(self.size)
+
+    @property
+    def count(self) -> int:
+        return int(np.prod(self.size))
+
+    @property
+    def shape(self) -> tuple:
+        """numpy shape of an image on this grid (z, y, x) / (y, x)."""
+        return tuple(reversed(self.size))
+
+    def to_c(self) -> SynxGeom:
+        g = SynxGeom()
+        d = self.dim
+        g.dim = d
+        for k in range(3):
+            g.size[k] = self.size[k] if k < d else 1
+            g.spacing[k] = self.spacing[k] if k < d else 1.0
+            g.origin[k] = self.origin[k] if k < d else 0.0
+        m = np.eye(3)
+        m[:d, :d] = self.direction
+        for k in range(9):
+            g.direction[k] = float(m.flat[k])
+        return g
+
+    @staticmethod
+    def from_c(g: SynxGeom) -> "Geom":
+        d = g.dim
+        m = np.array(list(g.direction), dtype=np.float64).reshape(3, 3)[:d, :d]
+        return Geom(tuple(g.size[k] for k in range(d)), tuple(g.spacing[k] for k in range(d)),
+                    tuple(g.origin[k] for k in range(d)), m)
+
+
+# ---- library loading -------------------------------------------------------------------------
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libsynx.so; raises if it is missing (build it with `python -m ants_b200.build`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libsynx.so not built at {path}; run `python -m ants_b200.build`")
+    lib = C.CDLL(path)
+    P, I, D, F, V = C.POINTER, C.c_int, C.c_double, C.c_float, C.c_void_p
+    sig = {
+        "synx_params_default": (I, [P(SynxParams), I]),
+        "synx_create": (I, [P(SynxParams), I, V, P(V)]),
+        "synx_destroy": (I, [V]),
+        "synx_last_error": (C.c_char_p, [V]),
+        "synx_set_images": (I, [V, V, P(SynxGeom), V, P(SynxGeom)]),
+        "synx_set_images_device": (I, [V, V, P(SynxGeom), V, P(SynxGeom)]),
+        "synx_run": (I, [V]),
+        "synx_run_level": (I, [V, I]),
+        "synx_get_output_geom": (I, [V, P(SynxGeom)]),
+        "synx_get_fields": (I, [V, V, V]),
+        "synx_get_fields_device": (I, [V, V, V]),
+        "synx_get_half_fields": (I, [V, V, V, V, V]),
+        "synx_set_half_fields": (I, [V, V, V, V, V, P(SynxGeom)]),
+        "synx_get_log": (I, [V, V, V, V, V, V, C.c_int64, P(C.c_int64)]),
+        "synx_get_profile": (I, [V, P(D), P(C.c_int64), P(C.c_int64), P(D), P(C.c_int64), P(C.c_int64)]),
+        "synx_reset_profile": (I, [V]),
+        "synx_get_device_bytes": (I, [V, P(C.c_int64)]),
+        "synx_get_launch_count": (I, [P(C.c_int64)]),
+        "synx_gaussian_kernel": (I, [D, D, I, V, I, P(I)]),
+        "synx_smooth_image": (I, [V, V, P(SynxGeom), D, I, V]),
+        "synx_warp_image": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
+        "synx_cc_metric": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
+        "synx_smooth_field": (I, [V, V, P(SynxGeom), D, P(D), V]),
+        "synx_compose": (I, [V, V, P(SynxGeom), F, V, V]),
+        "synx_invert_field": (I, [V, V, P(SynxGeom), I, D, D, P(I), V]),
+        "synx_resample_field": (I, [V, P(SynxGeom), V, P(SynxGeom), V]),
+        "synx_shrink_geom": (I, [P(SynxGeom), I, P(SynxGeom)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class SynxError(RuntimeError):
+    pass
+
+
+def _check(rc: int, ctx=None) -> None:
+    if rc != 0:
+        lib = load_library()
+        msg = lib.synx_last_error(ctx).decode(errors="replace") if lib else ""
+        raise SynxError(f"synx error {rc} ({ERRORS.get(rc, '?')}): {msg}")
+
+
+def _ptr(a) -> int:
+    """Raw pointer of a numpy array or torch tensor (device pointers for CUDA tensors)."""
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+# ---- stage parameters --------------------------------------------------------------------------
+@dataclass
+class SyNParams:
+    """A SyN stage with the CC metric, as antsRegistration's -t/-m/-c/-f/-s options give it."""
+
+    dim: int = 3
+    learning_rate: float = 0.1
+    update_variance: float = 3.0
+    total_variance: float = 0.0
+    cc_radius: int = 4
+    iterations: Sequence[int] = (1,)
+    shrink_factors: Sequence[int] = (1,)
+    smoothing_sigmas: Sequence[float] = (0.0,)
+    sigmas_in_mm: bool = False
+    convergence_threshold: float = 1e-6
+    convergence_window: int = 10
+    preprocess: bool = True
+    winsor_lower: float = 0.0
+    winsor_upper: float = 1.0
+    inv_max_iter: int = 20
+    inv_mean_tol: float = 0.001
+    inv_max_tol: float = 0.1
+    flags: int = 0
+
+    def to_c(self) -> SynxParams:
+        n = len(self.iterations)
+        if not (len(self.shrink_factors) == n and len(self.smoothing_sigmas) == n):
+            raise ValueError("iterations, shrink factors and smoothing sigmas must have one entry per level")
+        if n < 1 or n > SYNX_MAX_LEVELS:
+            raise ValueError("between 1 and 8 levels")
+        p = SynxParams()  # zero-initialised; every field is set below
+        p.dim = self.dim
+        p.n_levels = n
+        p.learning_rate = self.learning_rate
+        p.update_variance = self.update_variance
+        p.total_variance = self.total_variance
+        p.cc_radius = self.cc_radius
+        p.sigmas_in_mm = int(self.sigmas_in_mm)
+        for i in range(n):
+            p.iterations[i] = int(self.iterations[i])
+            p.shrink_factors[i] = int(self.shrink_factors[i])
+            p.smoothing_sigmas[i] = float(self.smoothing_sigmas[i])
+        p.convergence_threshold = self.convergence_threshold
+        p.convergence_window = self.convergence_window
+        p.preprocess = int(self.preprocess)
+        p.winsor_lower = self.winsor_lower
+        p.winsor_upper = self.winsor_upper
+        p.inv_max_iter = self.inv_max_iter
+        p.inv_mean_tol = self.inv_mean_tol
+        p.inv_max_tol = self.inv_max_tol
+        p.flags = self.flags
+        return p
+
+
+@dataclass
+class LogRecord:
+    level: int
+    iteration: int
+    metric: float
+    convergence: float
+    inverse_iterations: int
+
+
+class SyNStage:
+    """One registration context on one GPU (synx_create ... synx_destroy)."""
+
+    def __init__(self, params: SyNParams, device: int = 0, stream: int | None = None):
+        self.lib = load_library()
+        self.params = params
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        _check(self.lib.synx_create(C.byref(self._cp), device, C.c_void_p(stream or 0), C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.synx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, rc):
+        _check(rc, self.h)
+
+    def set_images(self, fixed, fixed_geom: Geom, moving, moving_geom: Geom) -> None:
+        """Host numpy float32 arrays (copied host->device) or CUDA tensors (device->device)."""
+        gf, gm = fixed_geom.to_c(), moving_geom.to_c()
+        if isinstance(fixed, np.ndarray):
+            f = np.ascontiguousarray(fixed, dtype=np.float32)
+            m = np.ascontiguousarray(moving, dtype=np.float32)
+            self._keep = (f, m)
+            self._ck(self.lib.synx_set_images(self.h, _ptr(f), C.byref(gf), _ptr(m), C.byref(gm)))
+        else:
+            self._ck(self.lib.synx_set_images_device(self.h, _ptr(fixed), C.byref(gf), _ptr(moving), C.byref(gm)))
+
+    def run(self) -> None:
+        self._ck(self.lib.synx_run(self.h))
+
+    def run_level(self, level: int) -> None:
+        self._ck(self.lib.synx_run_level(self.h, level))
+
+    def output_geom(self) -> Geom:
+        g = SynxGeom()
+        self._ck(self.lib.synx_get_output_geom(self.h, C.byref(g)))
+        return Geom.from_c(g)
+
+    def fields(self, fwd: np.ndarray | None = None, inv: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """Forward and inverse fields, interleaved: shape grid.shape + (dim,) (optionally into
+        caller-provided, e.g. pinned, host arrays)."""
+        g = self.output_geom()
+        shp = g.shape + (g.dim,)
+        if fwd is None:
+            fwd = np.empty(shp, np.float32)
+        if inv is None:
+            inv = np.empty(shp, np.float32)
+        assert fwd.shape == shp and inv.shape == shp and fwd.dtype == np.float32 and inv.dtype == np.float32
+        self._ck(self.lib.synx_get_fields(self.h, _ptr(fwd), _ptr(inv)))
+        return fwd, inv
+
+    def fields_device(self, fwd, inv) -> None:
+        self._ck(self.lib.synx_get_fields_device(self.h, _ptr(fwd), _ptr(inv)))
+
+    def half_fields(self) -> tuple:
+        g = self.output_geom()
+        shp = g.shape + (g.dim,)
+        out = [np.empty(shp, np.float32) for _ in range(4)]
+        self._ck(self.lib.synx_get_half_fields(self.h, *[_ptr(a) for a in out]))
+        return tuple(out)
+
+    def set_half_fields(self, phi_f, psi_f, phi_m, psi_m, grid: Geom) -> None:
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (phi_f, psi_f, phi_m, psi_m)]
+        g = grid.to_c()
+        self._ck(self.lib.synx_set_half_fields(self.h, *[_ptr(a) for a in arrs], C.byref(g)))
+
+    def log(self) -> list[LogRecord]:
+        n = C.c_int64()
+        self._ck(self.lib.synx_get_log(self.h, None, None, None, None, None, 0, C.byref(n)))
+        k = n.value
+        lv = np.zeros(k, np.int32)
+        it = np.zeros(k, np.int32)
+        me = np.zeros(k, np.float64)
+        cv = np.zeros(k, np.float64)
+        ii = np.zeros(k, np.int32)
+        if k:
+            self._ck(self.lib.synx_get_log(self.h, _ptr(lv), _ptr(it), _ptr(me), _ptr(cv), _ptr(ii), k, C.byref(n)))
+        return [LogRecord(int(lv[i]), int(it[i]), float(me[i]), float(cv[i]), int(ii[i])) for i in range(k)]
+
+    def profile(self) -> dict:
+        a, b, c_, d, e, f = C.c_double(), C.c_int64(), C.c_int64(), C.c_double(), C.c_int64(), C.c_int64()
+        self._ck(self.lib.synx_get_profile(self.h, C.byref(a), C.byref(b), C.byref(c_), C.byref(d), C.byref(e),
+                                           C.byref(f)))
+        return {"inverse_ms": a.value, "inverse_launches": b.value, "inverse_voxels": c_.value, "cc_ms": d.value,
+                "cc_launches": e.value, "cc_voxels": f.value}
+
+    def reset_profile(self) -> None:
+        self._ck(self.lib.synx_reset_profile(self.h))
+
+    def device_bytes(self) -> int:
+        n = C.c_int64()
+        self._ck(self.lib.synx_get_device_bytes(self.h, C.byref(n)))
+        return n.value
+
+
+def launch_count() -> int:
+    """Kernel launches issued by libsynx in this process so far."""
+    n = C.c_int64()
+    _check(load_library().synx_get_launch_count(C.byref(n)))
+    return n.value
+
+
+# ---- step entry points (device tensors, component-plane fields) --------------------------------
+def gaussian_kernel(variance: float, max_error: float, max_width: int) -> np.ndarray:
+    lib = load_library()
+    n = C.c_int()
+    _check(lib.synx_gaussian_kernel(variance, max_error, max_width, None, 0, C.byref(n)))
+    out = np.zeros(n.value, np.float64)
+    _check(lib.synx_gaussian_kernel(variance, max_error, max_width, _ptr(out), n.value, C.byref(n)))
+    return out
+
+
+def shrink_geom(g: Geom, factor: int) -> Geom:
+    lib = load_library()
+    o = SynxGeom()
+    gi = g.to_c()
+    _check(lib.synx_shrink_geom(C.byref(gi), factor, C.byref(o)))
+    return Geom.from_c(o)
+
+
+def _stream(stream) -> C.c_void_p:
+    return C.c_void_p(stream or 0)
+
+
+def smooth_image(img, out, g: Geom, sigma: float, sigma_in_mm: bool = False, stream=None) -> None:
+    gc = g.to_c()
+    _check(load_library().synx_smooth_image(_ptr(img), _ptr(out), C.byref(gc), sigma, int(sigma_in_mm),
+                                            _stream(stream)))
+
+
+def warp_image(img, img_geom: Geom, u, grid: Geom, out, stream=None) -> None:
+    a, b = img_geom.to_c(), grid.to_c()
+    _check(load_library().synx_warp_image(_ptr(img), C.byref(a), _ptr(u), C.byref(b), _ptr(out), _stream(stream)))
+
+
+def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
+    gc = g.to_c()
+    v = C.c_double()
+    _check(load_library().synx_cc_metric(_ptr(F), _ptr(M), C.byref(gc), radius, _ptr(gF), _ptr(gM), C.byref(v),
+                                         _stream(stream)))
+    return v.value
+
+
+def smooth_field(u, out, g: Geom, variance: float, stream=None) -> float:
+    gc = g.to_c()
+    mx = C.c_double()
+    _check(load_library().synx_smooth_field(_ptr(u), _ptr(out), C.byref(gc), variance, C.byref(mx), _stream(stream)))
+    return mx.value
+
+
+def compose(d, w, g: Geom, out, scale: float = 1.0, stream=None) -> None:
+    gc = g.to_c()
+    _check(load_library().synx_compose(_ptr(d), _ptr(w), C.byref(gc), scale, _ptr(out), _stream(stream)))
+
+
+def invert_field(phi, psi, g: Geom, max_iter=20, mean_tol=0.001, max_tol=0.1, stream=None) -> int:
+    gc = g.to_c()
+    it = C.c_int()
+    _check(load_library().synx_invert_field(_ptr(phi), _ptr(psi), C.byref(gc), max_iter, mean_tol, max_tol,
+                                            C.byref(it), _stream(stream)))
+    return it.value
+
+
+def resample_field(u, gi: Geom, out, go: Geom, stream=None) -> None:
+    a, b = gi.to_c(), go.to_c()
+    _check(load_library().synx_resample_field(_ptr(u), C.byref(a), _ptr(out), C.byref(b), _stream(stream)))

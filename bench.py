@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""SyN-CC throughput on the 3-D 182x218x182 workload (voxel-iterations per second).
+
+One step = one complete SyN stage on one fixed/moving pair:
+  SyN[0.1,3,0], CC radius 4, shrink 8x4x2x1, smoothing 3x2x1x0 vox, iterations 100x70x50x20,
+  convergence [.., 1e-12, 10] (the fixed-schedule setting; the actual iterations run per level
+  are counted from the stage log and reported).
+A voxel-iteration is one voxel of a level grid processed by one full SyN iteration.
+
+  value  -- inputs already resident in HBM (device-to-device image upload, device field output),
+            CUDA events on the stage's stream, L2 flushed between steps.
+  e2e    -- the same stage through the C ABI with pinned host buffers: host->device images,
+            device->host forward and inverse fields inside the timed region.
+  --impl reference -- the CPU path (the oracle restatement of the reference's arithmetic, all
+            host threads) on a bounded sample of the same workload: one full-resolution
+            iteration per step.
+
+Multi-GPU (torchrun): independent replicas, one pair per rank (no data-path collective);
+value = voxel-iterations of all ranks / max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SyN-CC voxel-iters/s at 182x218x182"
+UNIT = "voxel-iter/s"
+SIZE = (182, 218, 182)
+STAGE = dict(cc_radius=4, iterations=(100, 70, 50, 20), shrink_factors=(8, 4, 2, 1), smoothing_sigmas=(3.0, 2.0, 1.0, 0.0),
+             learning_rate=0.1, update_variance=3.0, total_variance=0.0, convergence_threshold=1e-12,
+             convergence_window=10)
+WORKLOAD = ("3-D SyN[0.1,3,0] + CC[r=4], 182x218x182 at 1 mm, shrink 8x4x2x1, sigmas 3x2x1x0 vox, "
+            "iterations 100x70x50x20, convergence [1e-12,10]")
+BYTES_PER_INV_VOXEL = 36  # fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi (3 x 12 B)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = open(os.path.join("/tmp", f"synx_clocks_{os.getpid()}.csv"), "w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.out is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def level_sizes(g):
+    from ants_b200.synx import shrink_geom
+    return [shrink_geom(g, f).count for f in STAGE["shrink_factors"]]
+
+
+def voxel_iterations(log, sizes) -> int:
+    return int(sum(sizes[r.level] for r in log))
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_sample(fixed, moving, g, threads: int):
+    """One full-resolution SyN iteration of the CPU path (oracle restatement, `threads` host
+    threads) from zero fields on the preprocessed, unsmoothed images (sigma = 0 at level 4)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ants_b200.synx import SyNParams
+    O.set_threads(threads)
+    P = SyNParams(dim=3, **STAGE)
+    Fp, Mp = O.preprocess(fixed), O.preprocess(moving)
+    z = np.zeros((3,) + g.shape, np.float32)
+    t0 = time.perf_counter()
+    O.syn_iteration(Fp, g, Mp, g, P, g, z, z, z, z)
+    dt = time.perf_counter() - t0
+    return g.count / dt, dt
+
+
+def run_reference(args, fixed, moving, g):
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(fixed, moving, g, threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_sample(fixed, moving, g, threads)
+        times.append(dt)
+    total = sum(times)
+    value = g.count * args.steps / total
+    sample = "one full-resolution (182x218x182) SyN-CC iteration from zero fields per step"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="synx", choices=["synx", "reference"])
+    ap.add_argument("--graphs", type=int, default=1, help="replay each level's iteration as a CUDA graph")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+
+    ws, rank, local = dist_env()
+    from ants_b200 import phantoms
+    from ants_b200.synx import Geom
+
+    g = Geom(SIZE)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        fixed, moving = phantoms.pair_3d(SIZE, seed=phantoms.SEED_BASE)
+        run_reference(args, fixed, moving, g)
+        return 0
+
+    import torch
+    from ants_b200 import synx as S
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    fixed, moving = phantoms.pair_3d(SIZE, seed=phantoms.SEED_BASE + rank)
+    sizes = level_sizes(g)
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flags = S.SYNX_F_PROFILE_EVENTS if not args.graphs else S.SYNX_F_USE_GRAPHS
+    P = S.SyNParams(dim=3, flags=flags, **STAGE)
+    stage = S.SyNStage(P, device=local, stream=stream.cuda_stream)
+    Fd = torch.from_numpy(fixed).to(f"cuda:{local}")
+    Md = torch.from_numpy(moving).to(f"cuda:{local}")
+    fwd_d = torch.empty((3,) + g.shape, device=f"cuda:{local}")
+    inv_d = torch.empty_like(fwd_d)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
+
+    def step_device():
+        stage.set_images(Fd, g, Md, g)
+        stage.run()
+        stage.fields_device(fwd_d, inv_d)
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+
+    # ---- timed region (device-resident inputs) ----
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stage.reset_profile()
+    launches0 = S.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    vox_iters = 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            step_device()
+            ev[k][1].record(stream)
+            vox_iters += voxel_iterations(stage.log(), sizes)
+        torch.cuda.synchronize()
+    launches = S.launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_total = sum(step_ms) / 1000.0
+    prof = stage.profile()
+    if dist:
+        t = torch.tensor([t_total], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+        vi = torch.tensor([float(vox_iters)], device=f"cuda:{local}")
+        dist.all_reduce(vi)
+        vox_iters_all = int(vi.item())
+    else:
+        vox_iters_all = vox_iters
+    value = vox_iters_all / t_total
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    Fh = torch.from_numpy(fixed).pin_memory().numpy()
+    Mh = torch.from_numpy(moving).pin_memory().numpy()
+    shp = g.shape + (3,)
+    fwd_h = torch.empty(shp, dtype=torch.float32).pin_memory().numpy()
+    inv_h = torch.empty(shp, dtype=torch.float32).pin_memory().numpy()
+    e2e_ms = []
+    e2e_vi = 0
+    if dist:
+        dist.barrier()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        stage.set_images(Fh, g, Mh, g)
+        stage.run()
+        stage.fields(fwd_h, inv_h)
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+        e2e_vi += voxel_iterations(stage.log(), sizes)
+    t_e2e = sum(e2e_ms) / 1000.0
+    if dist:
+        t = torch.tensor([t_e2e], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+        vi = torch.tensor([float(e2e_vi)], device=f"cuda:{local}")
+        dist.all_reduce(vi)
+        e2e_vi = int(vi.item())
+    e2e_value = e2e_vi / t_e2e
+
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        roof = None
+        if prof["inverse_ms"] > 0:
+            bytes_alg = prof["inverse_voxels"] * BYTES_PER_INV_VOXEL
+            achieved = bytes_alg / (prof["inverse_ms"] / 1000.0) / 1e9
+            roof = {"kernel": "k_invert_step (fused fixed-point inverse sub-iteration)", "bound": "hbm",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": peak_kind, "traffic": None,
+                    "algorithmic_bytes_per_half_field_voxel": BYTES_PER_INV_VOXEL,
+                    "inverse_share_of_step": prof["inverse_ms"] / sum(step_ms),
+                    "cc_ms_share": prof["cc_ms"] / sum(step_ms)}
+        cpu = None
+        if not args.no_cpu_baseline and ws == 1:
+            threads = os.cpu_count() or 1
+            v_cpu, dt = cpu_sample(fixed, moving, g, threads)
+            cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"one full-resolution SyN-CC iteration from zero fields ({dt:.1f} s)"}
+        its = {}
+        for r in stage.log():
+            its[r.level] = its.get(r.level, 0) + 1
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field",
+            "config": {"workload": WORKLOAD, "iterations_run_per_level": [its.get(l, 0) for l in range(4)],
+                       "voxel_iterations_per_step": vox_iters // args.steps, "l2": "flushed between steps (256 MB)",
+                       "parallelism": f"replicas x{ws}", "cuda_graphs": bool(args.graphs)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(Fh.nbytes + Mh.nbytes),
+                    "d2h_bytes_per_step": int(fwd_h.nbytes + inv_h.nbytes),
+                    "ms_per_step": 1000.0 * t_e2e / args.steps},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    stage.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,200 @@
+/*
+ * synx.h -- C ABI of the B200 SyN + neighbourhood-CC registration stage.
+ *
+ * This is the boundary a host binds to: plain C types, opaque handles, int status codes,
+ * no exceptions and no C++ or torch types.  It replaces the reference's stage object,
+ * itk::SyNImageRegistrationMethod configured with
+ * itk::ANTSNeighborhoodCorrelationImageToImageMetricv4, which antsRegistration builds and runs
+ * in Examples/itkantsRegistrationHelper.hxx:1983-2220 (construct :2001-2008, configure
+ * :2138-2164, run `Update()` :2198, harvest :2207-2218).  The command line front end
+ * (Examples/antsRegistration.cxx:554, library entry
+ * `int ants::antsRegistration(std::vector<std::string>, std::ostream*)` in
+ * Examples/include/antsRegistration.h:7-9) is provided by the C++ host in
+ * ants_b200/csrc/ants_registration.cpp on top of these calls.
+ *
+ * Conventions
+ *   - Return value 0 = success, negative = error class (SYNX_E_*); synx_last_error() gives
+ *     the message of the last failing call on that context (or the thread's last global
+ *     error when ctx is NULL).
+ *   - Images are float32, x fastest.  Displacement fields are physical-space vectors (mm)
+ *     and are exchanged in ITK's interleaved layout (x,y[,z] per voxel, voxel order x
+ *     fastest), which is also the layout of the vector NIfTI written as prefix0Warp.nii.gz.
+ *   - "host" pointers are ordinary CPU memory; "dev" pointers are CUDA device memory on the
+ *     context's device.  Every call is ordered on the context's CUDA stream.
+ *   - A context is used by one host thread at a time; several contexts may run concurrently.
+ */
+#ifndef SYNX_H
+#define SYNX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SYNX_OK 0
+#define SYNX_E_ARG -1       /* invalid argument (size, dimension, pointer, option) */
+#define SYNX_E_STATE -2     /* call out of order (e.g. run before set_images) */
+#define SYNX_E_CUDA -3      /* CUDA runtime error */
+#define SYNX_E_NOMEM -4     /* device allocation failed / budget exceeded */
+#define SYNX_E_UNSUPPORTED -5
+
+#define SYNX_MAX_LEVELS 8
+
+/* Image grid: ITK image information.  p = origin + direction * diag(spacing) * index. */
+typedef struct synx_geom {
+  int32_t dim;          /* 2 or 3 */
+  int32_t reserved0;
+  int64_t size[3];      /* size[2] = 1 for 2-D */
+  double spacing[3];
+  double origin[3];
+  double direction[9];  /* row-major direction cosines */
+} synx_geom;
+
+/* Stage parameters, the values antsRegistration parses from
+ *   -t SyN[learningRate, updateFieldVariance, totalFieldVariance]
+ *      (Examples/antsRegistrationTemplateHeader.h:801-815, defaults 3 and 0)
+ *   -m CC[fixed, moving, weight, radius]   (radius default 4, :1013, :1081-1087)
+ *   -c [iterations, threshold, window]     (defaults 1e-6 / 10, :545-592)
+ *   -f shrink factors, -s sigmas[vox|mm]   (:622-651)
+ *   --winsorize-image-intensities [lo,hi]  (:440-458)                                   */
+typedef struct synx_params {
+  int32_t dim;
+  int32_t n_levels;
+  double learning_rate;
+  double update_variance;
+  double total_variance;
+  int32_t cc_radius;
+  int32_t sigmas_in_mm;
+  int32_t iterations[SYNX_MAX_LEVELS];
+  int32_t shrink_factors[SYNX_MAX_LEVELS];
+  double smoothing_sigmas[SYNX_MAX_LEVELS];
+  double convergence_threshold;
+  int32_t convergence_window;
+  int32_t preprocess;        /* 1: rescale both images to [0,1] as antsRegistration does */
+  float winsor_lower;        /* quantiles of the intensity window (0 and 1 by default) */
+  float winsor_upper;
+  int32_t inv_max_iter;      /* fixed-point inverse: 20 / 0.001 / 0.1 in SyN */
+  int32_t flags;             /* SYNX_F_* */
+  double inv_mean_tol;
+  double inv_max_tol;
+  int32_t reserved[8];
+} synx_params;
+
+#define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
+#define SYNX_F_USE_GRAPHS 0x2     /* capture each iteration as a CUDA graph and replay it */
+
+/* Fill *p with antsRegistration's defaults for a SyN stage of dimension dim
+ * (SyN[0.1,3,0], CC radius 4, one level, 1 iteration, shrink 1, sigma 0 vox). */
+int synx_params_default(synx_params* p, int dim);
+
+typedef struct synx_ctx synx_ctx;
+
+/* Context lifetime.  stream may be NULL (the context creates its own). */
+int synx_create(const synx_params* params, int device, void* cuda_stream, synx_ctx** out);
+int synx_destroy(synx_ctx* ctx);
+const char* synx_last_error(const synx_ctx* ctx);
+
+/* Inputs from host memory (copied host->device on the context stream). The fixed image grid
+ * is the virtual domain of the stage, as in antsRegistration (hxx:1154). */
+int synx_set_images(synx_ctx* ctx, const float* fixed_host, const synx_geom* fixed_geom,
+                    const float* moving_host, const synx_geom* moving_geom);
+/* Same with device-resident inputs (copied device->device into the context arena). */
+int synx_set_images_device(synx_ctx* ctx, const float* fixed_dev, const synx_geom* fixed_geom,
+                           const float* moving_dev, const synx_geom* moving_geom);
+
+/* Run every level (synx_run) or one level (levels must be run in order 0..L-1). */
+int synx_run(synx_ctx* ctx);
+int synx_run_level(synx_ctx* ctx, int level);
+
+/* Geometry of the grid the output fields live on (the last level run). */
+int synx_get_output_geom(const synx_ctx* ctx, synx_geom* out);
+/* Final forward (prefix0Warp) and inverse (prefix0InverseWarp) fields, interleaved, host. */
+int synx_get_fields(synx_ctx* ctx, float* forward_host, float* inverse_host);
+/* Same into device memory. */
+int synx_get_fields_device(synx_ctx* ctx, float* forward_dev, float* inverse_dev);
+/* The four half-fields (fixed-to-middle, its inverse, moving-to-middle, its inverse) on the
+ * current level grid, interleaved, host; any pointer may be NULL. */
+int synx_get_half_fields(synx_ctx* ctx, float* phi_f, float* psi_f, float* phi_m, float* psi_m);
+/* Replace the four half-fields on the current level grid (resume / test hook). */
+int synx_set_half_fields(synx_ctx* ctx, const float* phi_f, const float* psi_f, const float* phi_m,
+                         const float* psi_m, const synx_geom* grid);
+
+/* Per-iteration log of everything run so far: level, iteration, metric value, convergence
+ * value, fixed-point sub-iterations (sum over the four inversions).  Returns the number of
+ * records through *count; arrays may be NULL to query the count. */
+int synx_get_log(synx_ctx* ctx, int32_t* level, int32_t* iteration, double* metric, double* convergence,
+                 int32_t* inverse_iterations, int64_t capacity, int64_t* count);
+
+/* Device time of the dominant kernel class (fixed-point inverse sub-iterations) recorded
+ * with CUDA events when SYNX_F_PROFILE_EVENTS is set: total ms, launches, voxels processed. */
+int synx_get_profile(synx_ctx* ctx, double* inverse_ms, int64_t* inverse_launches, int64_t* inverse_voxels,
+                     double* cc_ms, int64_t* cc_launches, int64_t* cc_voxels);
+int synx_reset_profile(synx_ctx* ctx);
+
+/* Device memory held by the context, bytes. */
+int synx_get_device_bytes(const synx_ctx* ctx, int64_t* bytes);
+
+/* Kernel launches issued by this library in this process so far (all contexts; each node
+ * of a replayed CUDA graph counts once per replay).  Instrumentation, no reference
+ * counterpart. */
+int synx_get_launch_count(int64_t* count);
+
+/* ---------------------------------------------------------------------------------------
+ * Step entry points (device pointers, component-plane fields: component c of voxel i at
+ * f[c*N + i]).  These are the per-step hooks of the stage, used for parity checks; each
+ * names the reference behaviour it replaces.  All take a CUDA stream (NULL = default).
+ * --------------------------------------------------------------------------------------- */
+
+/* Discrete Gaussian kernel (ITK GaussianOperator: e^-t I_n(t), max error, max width).
+ * Writes up to cap coefficients of the full symmetric kernel; returns its length in *len. */
+int synx_gaussian_kernel(double variance, double max_error, int max_width, double* coeffs, int cap, int* len);
+
+/* Pyramid smoothing of an image (ITK DiscreteGaussianImageFilter, per level of
+ * ImageRegistrationMethodv4; max error 0.01, width 32). */
+int synx_smooth_image(const float* in_dev, float* out_dev, const synx_geom* g, double sigma, int sigma_in_mm,
+                      void* stream);
+
+/* out(i) = img(x_i + u(x_i)), linear, 0 outside (ResampleImageFilter through a
+ * displacement field; itkantsRegistrationHelper.hxx:2138, observer .h:342-381). */
+int synx_warp_image(const float* img_dev, const synx_geom* img_geom, const float* u_dev, const synx_geom* grid,
+                    float* out_dev, void* stream);
+
+/* Windowed CC on two images on the same grid: value (-mean cc), the fixed-to-middle update
+ * direction (uses grad of `moving`) and the moving-to-middle one (uses grad of `fixed`)
+ * (ITK ANTSNeighborhoodCorrelationImageToImageMetricv4; in-tree twin
+ * ImageRegistration/itkCrossCorrelationRegistrationFunction.cxx:179-504). */
+int synx_cc_metric(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
+                   float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
+
+/* Gaussian smoothing of a displacement field as SyN does it (Examples/SmoothDisplacementField
+ * .cxx:70-125 twin).  If max_norm_host is not NULL, also returns max ||u/spacing||. */
+int synx_smooth_field(const float* in_dev, float* out_dev, const synx_geom* g, double variance,
+                      double* max_norm_host, void* stream);
+
+/* out = w + scale * d(x + w)  (ITK ComposeDisplacementFieldsImageFilter; twin
+ * Utilities/itkComposeDiffeomorphismsImageFilter.hxx:70-105). */
+int synx_compose(const float* d_dev, const float* w_dev, const synx_geom* g, float scale, float* out_dev,
+                 void* stream);
+
+/* Fixed-point inverse of phi, warm-started from psi_inout (ITK
+ * InvertDisplacementFieldImageFilter; twin itkANTSImageRegistrationOptimizer.h:1845-1988).
+ * Returns the number of iterations run in *iterations (may be NULL). */
+int synx_invert_field(const float* phi_dev, float* psi_inout_dev, const synx_geom* g, int max_iter,
+                      double mean_tol, double max_tol, int* iterations, void* stream);
+
+/* Linear resampling of a field onto another grid, 0 outside (DisplacementFieldTransform
+ * ParametersAdaptor, itkantsRegistrationHelper.hxx:2028-2055). */
+int synx_resample_field(const float* in_dev, const synx_geom* in_geom, float* out_dev, const synx_geom* out_geom,
+                        void* stream);
+
+/* Level grid for a shrink factor (CalculateShrinkFactorsPerDimension hxx:593-641 +
+ * ShrinkImageFilter output information hxx:16-39). */
+int synx_shrink_geom(const synx_geom* in, int factor, synx_geom* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYNX_H */

@@ -1,0 +1,126 @@
+"""Whole-stage parity: the CUDA SyN stage (through the C ABI, host buffers in and out)
+against the CPU oracle on seeded phantom pairs.
+
+* One iteration from zero fields: the four half-fields must agree to 1e-4 mm.
+* A multi-level schedule: the per-iteration metric log agrees to 2e-3 and the final forward
+  and inverse fields agree to an RMS of 0.05 voxel (the stage-level tolerance).  Exact
+  agreement is not expected over many iterations: the fixed-point inverse stops on
+  `mean > 0.001` / `max > 0.1`, and a rounding-level difference can change its iteration count
+  (the same holds between the reference's float and double builds).
+* Graph replay and plain launches give identical bits; repeated runs are deterministic.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from ants_b200 import phantoms
+from ants_b200.synx import SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage
+
+pytestmark = pytest.mark.gpu
+
+
+def planes(interleaved: np.ndarray) -> np.ndarray:
+    return np.moveaxis(interleaved, -1, 0)
+
+
+def rms_vox(a: np.ndarray, b: np.ndarray, spacing) -> float:
+    sp = np.asarray(spacing, dtype=np.float64).reshape((-1,) + (1,) * (a.ndim - 1))
+    return float(np.sqrt((((a - b) / sp) ** 2).sum(0).mean()))
+
+
+def make_pair(dim, size, seed):
+    return phantoms.pair_2d(size, seed=seed) if dim == 2 else phantoms.pair_3d(size, seed=seed)
+
+
+@pytest.mark.parametrize("dim,size,radius,sigma", [(2, (64, 64), 2, 1.0), (3, (32, 30, 28), 4, 1.0),
+                                                   (3, (31, 33, 27), 2, 0.0)])
+def test_single_iteration_half_fields(cuda, dim, size, radius, sigma):
+    f, m = make_pair(dim, size, seed=1)
+    g = Geom(size)
+    P = SyNParams(dim=dim, cc_radius=radius, iterations=(1,), shrink_factors=(1,), smoothing_sigmas=(sigma,))
+    with SyNStage(P) as st:
+        st.set_images(f, g, m, g)
+        st.run()
+        got = [planes(a) for a in st.half_fields()]
+        log = st.log()
+    fp, mp = O.preprocess(f), O.preprocess(m)
+    Fs, Ms = O.smooth_image(fp, g, sigma), O.smooth_image(mp, g, sigma)
+    z = np.zeros((dim,) + g.shape, np.float32)
+    v, ref, kinv = O.syn_iteration(Fs, g, Ms, g, P, g, z, z, z, z)
+    assert len(log) == 1 and abs(log[0].metric - v) < 1e-7
+    assert log[0].inverse_iterations == kinv
+    for a, b in zip(got, ref):
+        np.testing.assert_allclose(a, b, atol=1e-4, rtol=0)
+
+
+SCHEDULES = [
+    (2, (96, 96), 2, (30, 15, 8), (4, 2, 1), (2.0, 1.0, 0.0)),
+    (3, (40, 44, 36), 4, (12, 6), (2, 1), (1.0, 0.0)),
+]
+
+
+@pytest.mark.parametrize("dim,size,radius,iters,shrink,sigmas", SCHEDULES)
+def test_multilevel_matches_oracle(cuda, dim, size, radius, iters, shrink, sigmas):
+    f, m = make_pair(dim, size, seed=7)
+    g = Geom(size)
+    P = SyNParams(dim=dim, cc_radius=radius, iterations=iters, shrink_factors=shrink, smoothing_sigmas=sigmas,
+                  convergence_threshold=1e-12)
+    with SyNStage(P) as st:
+        st.set_images(f, g, m, g)
+        st.run()
+        fwd, inv = (planes(a) for a in st.fields())
+        go = st.output_geom()
+        log = st.log()
+    rf, ri, rg, rlog = O.syn_register(f, g, m, g, P)
+    assert go.size == rg.size
+    assert [(r.level, r.iteration) for r in log] == [(r["level"], r["iteration"]) for r in rlog]
+    np.testing.assert_allclose([r.metric for r in log], [r["metric"] for r in rlog], atol=2e-3)
+    assert rms_vox(fwd, rf, go.spacing) <= 0.05
+    assert rms_vox(inv, ri, go.spacing) <= 0.05
+    # the registration did something: the final fields are far from zero
+    assert rms_vox(fwd, np.zeros_like(fwd), go.spacing) > 0.2
+
+
+def test_graph_replay_is_bit_identical_and_deterministic(cuda):
+    f, m = make_pair(3, (36, 34, 32), seed=3)
+    g = Geom((36, 34, 32))
+    outs = []
+    for flags in (0, SYNX_F_USE_GRAPHS, SYNX_F_USE_GRAPHS):
+        P = SyNParams(dim=3, cc_radius=3, iterations=(6, 4), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0),
+                      flags=flags)
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.run()
+            outs.append((st.fields(), [r.metric for r in st.log()]))
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o[0][0], outs[0][0][0])
+        np.testing.assert_array_equal(o[0][1], outs[0][0][1])
+        assert o[1] == outs[0][1]
+
+
+def test_convergence_stops_level_early(cuda):
+    # a pair that is already aligned stops as soon as the window fills (slope >= 0)
+    f, _ = make_pair(2, (64, 64), seed=5)
+    g = Geom((64, 64))
+    P = SyNParams(dim=2, cc_radius=2, iterations=(40,), shrink_factors=(1,), smoothing_sigmas=(0.0,),
+                  convergence_threshold=1e-6, convergence_window=10)
+    with SyNStage(P) as st:
+        st.set_images(f, g, f, g)
+        st.run()
+        log = st.log()
+    rf, ri, rg, rlog = O.syn_register(f, g, f, g, P)
+    assert len(log) == len(rlog) < 40
+
+
+def test_run_level_order_enforced(cuda):
+    f, m = make_pair(2, (32, 32), seed=2)
+    g = Geom((32, 32))
+    P = SyNParams(dim=2, cc_radius=2, iterations=(2, 2), shrink_factors=(2, 1), smoothing_sigmas=(0.0, 0.0))
+    from ants_b200.synx import SynxError
+    with SyNStage(P) as st:
+        st.set_images(f, g, m, g)
+        with pytest.raises(SynxError):
+            st.run_level(1)
+        st.run_level(0)
+        st.run_level(1)
+        assert st.output_geom().size == (32, 32)
