@@ -149,6 +149,11 @@ bool check_geom(const synx_geom* g, int dim) {
 
 int set_err(synx_ctx* c, int code, const std::string& msg);
 
+struct LevelProf {
+  double setup_ms = 0, iterate_ms = 0, inv_ms = 0, cc_ms = 0;
+  long long iterations = 0, inv_sub = 0, voxels = 0;
+};
+
 }  // namespace
 
 struct synx_ctx {
@@ -191,9 +196,14 @@ struct synx_ctx {
   GridInfo cur_grid{};
   std::vector<int32_t> log_level, log_iter, log_inv;
   std::vector<double> log_metric, log_conv;
-  // graphs
-  cudaGraphExec_t gexec = nullptr;
+  // canonical buffer assignment (level changes swap field and work buffers)
+  float* canon[8] = {};
+  // graphs: one executable per level, valid while the arena and grids are unchanged
+  cudaGraphExec_t gexec_lv[SYNX_MAX_LEVELS] = {};
+  long long graph_nodes[SYNX_MAX_LEVELS] = {};
   // profiling
+  cudaEvent_t lev_ev[3] = {};
+  LevelProf lprof[SYNX_MAX_LEVELS];
   double prof_inv_ms = 0, prof_cc_ms = 0;
   long long prof_inv_launches = 0, prof_inv_vox = 0, prof_cc_launches = 0, prof_cc_vox = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -218,11 +228,15 @@ int set_err(synx_ctx* c, int code, const std::string& msg) {
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-void free_arena(synx_ctx* c) {
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
+void drop_graphs(synx_ctx* c) {
+  for (auto& g : c->gexec_lv) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
   }
+}
+
+void free_arena(synx_ctx* c) {
+  drop_graphs(c);
   if (c->arena) cudaFree(c->arena);
   c->arena = nullptr;
   c->arena_bytes = 0;
@@ -559,6 +573,7 @@ int run_level_impl(synx_ctx* c, int level) {
   CUDA_TRY(c, cudaSetDevice(c->device));
   const GridInfo& gl = c->lv[level];
   const int D = c->D;
+  CUDA_TRY(c, cudaEventRecord(c->lev_ev[0], c->stream));
   int rc = smooth_images_for_level(c, level);
   if (rc) return rc;
   rc = upload_level_kernels(c, level);
@@ -585,25 +600,32 @@ int run_level_impl(synx_ctx* c, int level) {
   c->ev_used = 0;
   c->ev_pairs_inv.clear();
   c->ev_pairs_cc.clear();
+  CUDA_TRY(c, cudaEventRecord(c->lev_ev[1], c->stream));
   if (graphs && iters > 0) {
-    cudaGraph_t graph;
-    const long long before = launch_count();
-    CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_iteration(c, false);
-    CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
-    // capture recorded one iteration's kernels; the replays below launch them `iters` times
-    add_launch_count((launch_count() - before) * (long long)(iters - 1));
-    if (c->gexec) {
-      cudaGraphExecDestroy(c->gexec);
-      c->gexec = nullptr;
+    // one iteration is captured once per level and context (all its launch arguments are fixed
+    // for a given level: the buffers are reset to the same assignment by synx_set_images) and
+    // replayed `iters` times; the device-side stop flag ends a converged level early
+    if (!c->gexec_lv[level]) {
+      cudaGraph_t graph;
+      const long long before = launch_count();
+      CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_iteration(c, false);
+      CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
+      c->graph_nodes[level] = launch_count() - before;
+      add_launch_count(-c->graph_nodes[level]);  // capture launches nothing
+      cudaError_t e = cudaGraphInstantiate(&c->gexec_lv[level], graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        c->gexec_lv[level] = nullptr;
+        return set_err(c, SYNX_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      }
     }
-    cudaError_t e = cudaGraphInstantiate(&c->gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return set_err(c, SYNX_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    for (int k = 0; k < iters; ++k) CUDA_TRY(c, cudaGraphLaunch(c->gexec, c->stream));
+    for (int k = 0; k < iters; ++k) CUDA_TRY(c, cudaGraphLaunch(c->gexec_lv[level], c->stream));
+    add_launch_count(c->graph_nodes[level] * (long long)iters);
   } else {
     for (int k = 0; k < iters; ++k) enqueue_iteration(c, profile);
   }
+  CUDA_TRY(c, cudaEventRecord(c->lev_ev[2], c->stream));
   CUDA_TRY(c, cudaGetLastError());
   // collect the level's log
   IterCtl hctl;
@@ -626,16 +648,29 @@ int run_level_impl(synx_ctx* c, int level) {
     c->log_inv.push_back(li[k]);
     sub_iters += li[k];
   }
+  LevelProf& lp = c->lprof[level];
+  {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, c->lev_ev[0], c->lev_ev[1]);
+    cudaEventElapsedTime(&b, c->lev_ev[1], c->lev_ev[2]);
+    lp.setup_ms += a;
+    lp.iterate_ms += b;
+    lp.iterations += done;
+    lp.inv_sub += sub_iters;
+    lp.voxels = gl.d.N;
+  }
   if (profile) {
     for (auto& pr : c->ev_pairs_inv) {
       float ms = 0;
       cudaEventElapsedTime(&ms, c->ev_pool[pr.first], c->ev_pool[pr.second]);
       c->prof_inv_ms += ms;
+      lp.inv_ms += ms;
     }
     for (auto& pr : c->ev_pairs_cc) {
       float ms = 0;
       cudaEventElapsedTime(&ms, c->ev_pool[pr.first], c->ev_pool[pr.second]);
       c->prof_cc_ms += ms;
+      lp.cc_ms += ms;
       c->prof_cc_launches += 1;
       c->prof_cc_vox += gl.d.N;
     }
@@ -728,6 +763,8 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     c->own_stream = true;
   }
   cudaError_t e = cc_prepare(p.dim, p.cc_radius);
+  for (auto& ev : c->lev_ev)
+    if (e == cudaSuccess) e = cudaEventCreate(&ev);
   if (e != cudaSuccess) {
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -743,6 +780,8 @@ int synx_destroy(synx_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_arena(ctx);
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+  for (auto e : ctx->lev_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return SYNX_OK;
@@ -755,6 +794,7 @@ static int set_images_common(synx_ctx* c, const float* F, const synx_geom* gf, c
   if (!check_geom(gf, c->D) || !check_geom(gm, c->D))
     return set_err(c, SYNX_E_ARG, "synx_set_images: image geometry does not match the stage dimension or is invalid");
   CUDA_TRY(c, cudaSetDevice(c->device));
+  if (memcmp(&c->geF, gf, sizeof(synx_geom)) != 0 || memcmp(&c->geM, gm, sizeof(synx_geom)) != 0) drop_graphs(c);
   c->geF = *gf;
   c->geM = *gm;
   geom_to_grid(c->geF, c->gF);
@@ -931,6 +971,22 @@ int synx_reset_profile(synx_ctx* c) {
   if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
   c->prof_inv_ms = c->prof_cc_ms = 0;
   c->prof_inv_launches = c->prof_inv_vox = c->prof_cc_launches = c->prof_cc_vox = 0;
+  for (auto& l : c->lprof) l = LevelProf();
+  return SYNX_OK;
+}
+
+int synx_get_level_profile(synx_ctx* c, int level, double* setup_ms, double* iterate_ms, double* inverse_ms,
+                           double* cc_ms, int64_t* iterations, int64_t* inverse_subiterations, int64_t* voxels) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (level < 0 || level >= SYNX_MAX_LEVELS) return set_err(c, SYNX_E_ARG, "synx_get_level_profile: bad level");
+  const LevelProf& l = c->lprof[level];
+  if (setup_ms) *setup_ms = l.setup_ms;
+  if (iterate_ms) *iterate_ms = l.iterate_ms;
+  if (inverse_ms) *inverse_ms = l.inv_ms;
+  if (cc_ms) *cc_ms = l.cc_ms;
+  if (iterations) *iterations = l.iterations;
+  if (inverse_subiterations) *inverse_subiterations = l.inv_sub;
+  if (voxels) *voxels = l.voxels;
   return SYNX_OK;
 }
 

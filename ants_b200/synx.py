@@ -148,6 +148,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_get_log": (I, [V, V, V, V, V, V, C.c_int64, P(C.c_int64)]),
         "synx_get_profile": (I, [V, P(D), P(C.c_int64), P(C.c_int64), P(D), P(C.c_int64), P(C.c_int64)]),
         "synx_reset_profile": (I, [V]),
+        "synx_get_level_profile": (I, [V, I, P(D), P(D), P(D), P(D), P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
         "synx_get_device_bytes": (I, [V, P(C.c_int64)]),
         "synx_get_launch_count": (I, [P(C.c_int64)]),
         "synx_gaussian_kernel": (I, [D, D, I, V, I, P(I)]),
@@ -353,6 +354,17 @@ class SyNStage:
 
     def reset_profile(self) -> None:
         self._ck(self.lib.synx_reset_profile(self.h))
+
+    def level_profile(self) -> list[dict]:
+        out = []
+        for lv in range(len(self.params.iterations)):
+            d = [C.c_double() for _ in range(4)]
+            n = [C.c_int64() for _ in range(3)]
+            self._ck(self.lib.synx_get_level_profile(self.h, lv, *[C.byref(x) for x in d], *[C.byref(x) for x in n]))
+            out.append({"level": lv, "setup_ms": d[0].value, "iterate_ms": d[1].value, "inverse_ms": d[2].value,
+                        "cc_ms": d[3].value, "iterations": n[0].value, "inverse_subiterations": n[1].value,
+                        "voxels": n[2].value})
+        return out
 
     def device_bytes(self) -> int:
         n = C.c_int64()

@@ -132,6 +132,12 @@ int synx_get_log(synx_ctx* ctx, int32_t* level, int32_t* iteration, double* metr
 int synx_get_profile(synx_ctx* ctx, double* inverse_ms, int64_t* inverse_launches, int64_t* inverse_voxels,
                      double* cc_ms, int64_t* cc_launches, int64_t* cc_voxels);
 int synx_reset_profile(synx_ctx* ctx);
+/* Per-level device times (CUDA events on the context stream) accumulated since the last
+ * reset: level set-up (pyramid smoothing, field resampling), the iterations, and in
+ * SYNX_F_PROFILE_EVENTS mode the inverse and CC shares; iterations run, fixed-point
+ * sub-iterations (sum over the four inversions) and grid voxels. */
+int synx_get_level_profile(synx_ctx* ctx, int level, double* setup_ms, double* iterate_ms, double* inverse_ms,
+                           double* cc_ms, int64_t* iterations, int64_t* inverse_subiterations, int64_t* voxels);
 
 /* Device memory held by the context, bytes. */
 int synx_get_device_bytes(const synx_ctx* ctx, int64_t* bytes);
