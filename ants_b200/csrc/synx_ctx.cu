@@ -454,11 +454,34 @@ int smooth_images_for_level(synx_ctx* c, int level) {
   return SYNX_OK;
 }
 
+// Smooth both halves: the fused all-axes kernel when its shared-memory tile fits, otherwise
+// one pass per axis through `tmp` (in != out; orig is read only at each output voxel).
+void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const float* const* orig,
+                   float* const* tmp, const float* coeff_base, const float* host_base, const int R[3], bool epilogue,
+                   float w1, float w2, bool maxnorm) {
+  const GridInfo& g = c->cur_grid;
+  const float* k[3] = {coeff_base, coeff_base + c->coeff_cap, coeff_base + 2 * c->coeff_cap};
+  if (smooth3_supported(c->D, R)) {
+    const float* kh[3] = {host_base, host_base + c->coeff_cap, host_base + 2 * c->coeff_cap};
+    launch_smooth_field(in, out, orig, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream);
+    return;
+  }
+  const int D = c->D;
+  const float* src[2] = {in[0], in[1]};
+  for (int a = 0; a < D; ++a) {
+    const bool last = a == D - 1;
+    float* const* dst = last ? out : (((D - 1 - a) % 2 == 0) ? out : tmp);
+    launch_smooth_field_pass(src, dst, last ? orig : nullptr, 2, g, a, k[a], R[a], last && epilogue, w1, w2,
+                             last && maxnorm, c->ctl, c->stream);
+    src[0] = dst[0];
+    src[1] = dst[1];
+  }
+}
+
 // One SyN iteration on the current level (all launches asynchronous, stop-aware).
 void enqueue_iteration(synx_ctx* c, bool profile) {
   const GridInfo& g = c->cur_grid;
   cudaStream_t s = c->stream;
-  const int D = c->D;
   auto ev = [&](void) -> int {
     if (c->ev_used >= c->ev_pool.size()) {
       cudaEvent_t e;
@@ -474,77 +497,37 @@ void enqueue_iteration(synx_ctx* c, bool profile) {
   launch_cc(c->Ft, c->Mt, g, c->P.cc_radius, c->gFu, c->gMu, c->cc_partials, c->ctl, s);
   if (profile) c->ev_pairs_cc.push_back({e0, ev()});
   // update-field smoothing, SyN epilogue (boundary zero, blend) and max ||u/spacing||
-  const float* upd[2];
+  const float* upd[2] = {c->t1F, c->t1M};
   const double var = c->P.update_variance;
-  if (var > 0.0) {
-    const float w1 = var < 0.5 ? (float)(1.0 - var / 0.5) : 1.0f;
-    const float w2 = 1.0f - w1;
-    const float* orig[2] = {c->gFu, c->gMu};
-    if (D == 3) {
-      const float* i0[2] = {c->gFu, c->gMu};
-      float* o0[2] = {c->t1F, c->t1M};
-      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, false, c->ctl, s);
-      const float* i1[2] = {c->t1F, c->t1M};
-      float* o1[2] = {c->t2F, c->t2M};
-      launch_smooth_field_pass(i1, o1, nullptr, 2, g, 1, c->coeff_upd + c->coeff_cap, c->R_upd[1], false, 1.f, 0.f,
-                               false, c->ctl, s);
-      const float* i2[2] = {c->t2F, c->t2M};
-      float* o2[2] = {c->t1F, c->t1M};
-      launch_smooth_field_pass(i2, o2, orig, 2, g, 2, c->coeff_upd + 2 * c->coeff_cap, c->R_upd[2], true, w1, w2,
-                               true, c->ctl, s);
-      upd[0] = c->t1F;
-      upd[1] = c->t1M;
-    } else {
-      const float* i0[2] = {c->gFu, c->gMu};
-      float* o0[2] = {c->t1F, c->t1M};
-      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, false, c->ctl, s);
-      const float* i1[2] = {c->t1F, c->t1M};
-      float* o1[2] = {c->t2F, c->t2M};
-      launch_smooth_field_pass(i1, o1, orig, 2, g, 1, c->coeff_upd + c->coeff_cap, c->R_upd[1], true, w1, w2, true,
-                               c->ctl, s);
-      upd[0] = c->t2F;
-      upd[1] = c->t2M;
-    }
-  } else {
-    // no smoothing (the kernel is [0 1 0]): a copy plus the max norm, boundary untouched
-    const float* i0[2] = {c->gFu, c->gMu};
-    float* o0[2] = {c->t1F, c->t1M};
-    launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, true, c->ctl, s);
-    upd[0] = c->t1F;
-    upd[1] = c->t1M;
-  }
-  // scale + compose into the forward half-fields, in place
   {
+    const float* in[2] = {c->gFu, c->gMu};
+    float* out[2] = {c->t1F, c->t1M};
+    float* tmp[2] = {c->t2F, c->t2M};
+    if (var > 0.0) {
+      const float w1 = var < 0.5 ? (float)(1.0 - var / 0.5) : 1.0f;
+      smooth_halves(c, in, out, in, tmp, c->coeff_upd, c->h_coeff_upd.data(), c->R_upd, true, w1, 1.0f - w1, true);
+    } else {
+      // no smoothing (the kernel is [0 1 0]): a copy plus the max norm, boundary untouched
+      launch_smooth_field_pass(in, out, nullptr, 2, g, 0, c->coeff_upd, c->R_upd[0], false, 1.f, 0.f, true, c->ctl,
+                               s);
+    }
+  }
+  // scale + compose into the forward half-fields (in place), or into t2 followed by the
+  // total-field smoothing back into the half-fields when its variance is positive
+  if (c->P.total_variance > 0.0) {
+    const double vt = c->P.total_variance;
+    const float w1 = vt < 0.5 ? (float)(1.0 - vt / 0.5) : 1.0f;
+    const float* w[2] = {c->phiF, c->phiM};
+    float* t2[2] = {c->t2F, c->t2M};
+    launch_compose(upd, w, t2, 2, g, (float)c->P.learning_rate, c->ctl, s);
+    const float* in[2] = {c->t2F, c->t2M};
+    float* out[2] = {c->phiF, c->phiM};
+    float* tmp[2] = {c->gFu, c->gMu};
+    smooth_halves(c, in, out, in, tmp, c->coeff_tot, c->h_coeff_tot.data(), c->R_tot, true, w1, 1.0f - w1, false);
+  } else {
     const float* w[2] = {c->phiF, c->phiM};
     float* o[2] = {c->phiF, c->phiM};
     launch_compose(upd, w, o, 2, g, (float)c->P.learning_rate, c->ctl, s);
-  }
-  // total-field smoothing (only when its variance is positive)
-  if (c->P.total_variance > 0.0) {
-    const double vt = c->P.total_variance;
-    const float w1 = vt < 0.5 ? (float)(1.0 - vt / 0.5) : 1.0f, w2 = 1.0f - w1;
-    const float* orig[2] = {c->phiF, c->phiM};
-    if (D == 3) {
-      const float* i0[2] = {c->phiF, c->phiM};
-      float* o0[2] = {c->gFu, c->gMu};
-      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_tot, c->R_tot[0], false, 1.f, 0.f, false, c->ctl, s);
-      const float* i1[2] = {c->gFu, c->gMu};
-      float* o1[2] = {c->t2F, c->t2M};
-      launch_smooth_field_pass(i1, o1, nullptr, 2, g, 1, c->coeff_tot + c->coeff_cap, c->R_tot[1], false, 1.f, 0.f,
-                               false, c->ctl, s);
-      const float* i2[2] = {c->t2F, c->t2M};
-      float* o2[2] = {c->phiF, c->phiM};
-      launch_smooth_field_pass(i2, o2, orig, 2, g, 2, c->coeff_tot + 2 * c->coeff_cap, c->R_tot[2], true, w1, w2,
-                               false, c->ctl, s);
-    } else {
-      const float* i0[2] = {c->phiF, c->phiM};
-      float* o0[2] = {c->gFu, c->gMu};
-      launch_smooth_field_pass(i0, o0, nullptr, 2, g, 0, c->coeff_tot, c->R_tot[0], false, 1.f, 0.f, false, c->ctl, s);
-      const float* i1[2] = {c->gFu, c->gMu};
-      float* o1[2] = {c->phiF, c->phiM};
-      launch_smooth_field_pass(i1, o1, orig, 2, g, 1, c->coeff_tot + c->coeff_cap, c->R_tot[1], true, w1, w2, false,
-                               c->ctl, s);
-    }
   }
   // fixed-point inverses: psi <- inv(phi) warm from psi, then phi <- inv(psi) warm from phi
   PartialBufs pb{c->inv_psum, c->inv_pmax, c->inv_cap};
@@ -763,6 +746,7 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     c->own_stream = true;
   }
   cudaError_t e = cc_prepare(p.dim, p.cc_radius);
+  if (e == cudaSuccess) e = smooth3_prepare();
   for (auto& ev : c->lev_ev)
     if (e == cudaSuccess) e = cudaEventCreate(&ev);
   if (e != cudaSuccess) {
@@ -1154,6 +1138,13 @@ int synx_smooth_field(const float* in, float* out, const synx_geom* gg, double v
     const float* i0[1] = {in};
     float* o0[1] = {out};
     launch_smooth_field_pass(i0, o0, nullptr, 1, g, 0, coeff, R[0], false, 1.f, 0.f, true, t.ctl, s);
+  } else if (smooth3_supported(D, R)) {
+    const float w1 = variance < 0.5 ? (float)(1.0 - variance / 0.5) : 1.0f, w2 = 1.0f - w1;
+    STEP_TRY(smooth3_prepare());
+    const float* i0[1] = {in};
+    float* o0[1] = {out};
+    const float* k[3] = {hk.data(), hk.data() + 1024, hk.data() + 2048};
+    launch_smooth_field(i0, o0, i0, 1, g, k, R, true, w1, w2, true, t.ctl, s);
   } else {
     const float w1 = variance < 0.5 ? (float)(1.0 - variance / 0.5) : 1.0f, w2 = 1.0f - w1;
     const float* orig[1] = {in};

@@ -1,12 +1,16 @@
-// synx kernels for sm_100a: the per-voxel steps of one SyN + neighbourhood-CC iteration.
+// synx kernels for sm_100a: the per-voxel steps of one SyN + neighbourhood-CC iteration
+// (the CC kernel itself is in synx_cc.cu).
 //
 // Everything here is memory-bound stencil / gather work (no contraction), so the design goals
 // are coalesced component-plane access, shared-memory staging of stencil halos, FP64 only
-// where the arithmetic needs it (CC window sums, global means), and device-side loop control
-// so that a whole level can be enqueued (or graph-replayed) without host round trips.
+// where the arithmetic needs it (global means), 32-bit index arithmetic with a 3-D launch
+// mapping (a block covers 32 x 8 voxels in x, y and a chunk of z slices, so no thread divides
+// a linear index), and device-side loop control so that a whole level can be enqueued (or
+// graph-replayed) without host round trips.
+#include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
-#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -101,11 +105,43 @@ static inline int grid_for(long long n, int threads, int cap = 148 * 16) {
   return (int)b;
 }
 
-__device__ __forceinline__ void voxel_xyz(long long i, const Dims& d, int& x, int& y, int& z) {
-  x = (int)(i % d.nx);
-  long long r = i / d.nx;
-  y = (int)(r % d.ny);
-  z = (int)(r / d.ny);
+// 3-D launch mapping: 32 x 8 threads per block, each thread walks `zb` consecutive slices.
+struct Map3 {
+  dim3 grid;
+  int zb;
+  int nblocks;  // blocks per field (per half)
+};
+static Map3 map3(const Dims& d, int halves = 1, int target = 148 * 8) {
+  Map3 m;
+  const int gx = (d.nx + 31) / 32, gy = (d.ny + 7) / 8;
+  int per = target / (gx * gy * halves);
+  if (per < 1) per = 1;
+  int zb = (d.nz + per - 1) / per;
+  if (zb < 1) zb = 1;
+  const int gz = (d.nz + zb - 1) / zb;
+  m.grid = dim3(gx, gy, gz * halves);
+  m.zb = zb;
+  m.nblocks = gx * gy * gz;
+  return m;
+}
+
+// Thread coordinates of a 3-D mapped block; h = half selected by blockIdx.z.
+struct Coord3 {
+  int x, y, z0, z1, h, bid;
+  bool ok;
+};
+__device__ __forceinline__ Coord3 coord3(const Dims& d, int zb, int halves) {
+  Coord3 c;
+  const int gz = gridDim.z / halves;
+  c.h = blockIdx.z / gz;
+  const int zc = blockIdx.z - c.h * gz;
+  c.x = blockIdx.x * 32 + (threadIdx.x & 31);
+  c.y = blockIdx.y * 8 + (threadIdx.x >> 5);
+  c.z0 = zc * zb;
+  c.z1 = min(c.z0 + zb, d.nz);
+  c.ok = c.x < d.nx && c.y < d.ny;
+  c.bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * zc);
+  return c;
 }
 
 template <int DIM>
@@ -146,36 +182,33 @@ void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s) {
 // Warp of both images through their inverse half-fields onto the level grid.
 // ------------------------------------------------------------------------------------------
 template <int DIM>
+__device__ __forceinline__ float sample(const float* __restrict__ img, const Dims& di, const Affine& m, float fx,
+                                        float fy, float fz, float ux, float uy, float uz) {
+  float cx, cy, cz;
+  map_point<DIM>(m, fx, fy, fz, ux, uy, uz, cx, cy, cz);
+  if (!inside_buffer<DIM>(di, cx, cy, cz)) return 0.0f;
+  return lerp_at<DIM>(img, make_cell<DIM>(di, cx, cy, cz));
+}
+
+template <int DIM>
 __global__ void __launch_bounds__(256)
     k_warp_pair(const float* __restrict__ F, Dims dF, Affine mF, const float* __restrict__ psiF,
-                const float* __restrict__ M, Dims dM, Affine mM, const float* __restrict__ psiM, Dims dv,
+                const float* __restrict__ M, Dims dM, Affine mM, const float* __restrict__ psiM, Dims dv, int zb,
                 float* __restrict__ Ft, float* __restrict__ Mt, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0 && ctl != nullptr) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && ctl != nullptr) {
     ctl->maxnorm[0] = 0u;
     ctl->maxnorm[1] = 0u;
   }
-  const long long N = dv.N, stride = (long long)gridDim.x * blockDim.x;
-  for (; i < N; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, dv, x, y, z);
-    const float fx = (float)x, fy = (float)y, fz = (float)z;
-    float cx, cy, cz;
-    {
-      float ux = psiF[i], uy = psiF[N + i], uz = DIM == 3 ? psiF[2 * N + i] : 0.0f;
-      map_point<DIM>(mF, fx, fy, fz, ux, uy, uz, cx, cy, cz);
-      float v = 0.0f;
-      if (inside_buffer<DIM>(dF, cx, cy, cz)) v = lerp_at<DIM>(F, make_cell<DIM>(dF, cx, cy, cz));
-      Ft[i] = v;
-    }
-    {
-      float ux = psiM[i], uy = psiM[N + i], uz = DIM == 3 ? psiM[2 * N + i] : 0.0f;
-      map_point<DIM>(mM, fx, fy, fz, ux, uy, uz, cx, cy, cz);
-      float v = 0.0f;
-      if (inside_buffer<DIM>(dM, cx, cy, cz)) v = lerp_at<DIM>(M, make_cell<DIM>(dM, cx, cy, cz));
-      Mt[i] = v;
-    }
+  const Coord3 c = coord3(dv, zb, 1);
+  if (!c.ok) return;
+  const int N = (int)dv.N, nxy = dv.nx * dv.ny;
+  const float fx = (float)c.x, fy = (float)c.y;
+  for (int z = c.z0; z < c.z1; ++z) {
+    const int i = z * nxy + c.y * dv.nx + c.x;
+    const float fz = (float)z;
+    Ft[i] = sample<DIM>(F, dF, mF, fx, fy, fz, psiF[i], psiF[N + i], DIM == 3 ? psiF[2 * N + i] : 0.0f);
+    Mt[i] = sample<DIM>(M, dM, mM, fx, fy, fz, psiM[i], psiM[N + i], DIM == 3 ? psiM[2 * N + i] : 0.0f);
   }
 }
 
@@ -183,390 +216,47 @@ void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, con
                       const float* psiM, const GridInfo& gv, float* Ft, float* Mt, IterCtl* ctl, cudaStream_t s) {
   count_launch();
   Affine mF = make_affine(gv, gF), mM = make_affine(gv, gM);
-  int blocks = grid_for(gv.d.N, 256);
+  const Map3 m = map3(gv.d);
   if (gv.d.dim == 3)
-    k_warp_pair<3><<<blocks, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, Ft, Mt, ctl);
+    k_warp_pair<3><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
   else
-    k_warp_pair<2><<<blocks, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, Ft, Mt, ctl);
+    k_warp_pair<2><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
 }
 
 template <int DIM>
 __global__ void __launch_bounds__(256) k_warp_image(const float* __restrict__ img, Dims di, Affine m,
-                                                    const float* __restrict__ u, Dims dv, float* __restrict__ out) {
-  const long long N = dv.N, stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, dv, x, y, z);
-    float ux = u[i], uy = u[N + i], uz = DIM == 3 ? u[2 * N + i] : 0.0f;
-    float cx, cy, cz;
-    map_point<DIM>(m, (float)x, (float)y, (float)z, ux, uy, uz, cx, cy, cz);
-    float v = 0.0f;
-    if (inside_buffer<DIM>(di, cx, cy, cz)) v = lerp_at<DIM>(img, make_cell<DIM>(di, cx, cy, cz));
-    out[i] = v;
+                                                    const float* __restrict__ u, Dims dv, int zb,
+                                                    float* __restrict__ out) {
+  const Coord3 c = coord3(dv, zb, 1);
+  if (!c.ok) return;
+  const int N = (int)dv.N, nxy = dv.nx * dv.ny;
+  for (int z = c.z0; z < c.z1; ++z) {
+    const int i = z * nxy + c.y * dv.nx + c.x;
+    out[i] = sample<DIM>(img, di, m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f);
   }
 }
 
 void launch_warp_image(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
                        cudaStream_t s) {
   count_launch();
-  Affine m = make_affine(gv, gi);
-  int blocks = grid_for(gv.d.N, 256);
+  Affine a = make_affine(gv, gi);
+  const Map3 m = map3(gv.d);
   if (gv.d.dim == 3)
-    k_warp_image<3><<<blocks, 256, 0, s>>>(img, gi.d, m, u, gv.d, out);
+    k_warp_image<3><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
   else
-    k_warp_image<2><<<blocks, 256, 0, s>>>(img, gi.d, m, u, gv.d, out);
+    k_warp_image<2><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
 }
 
 // ------------------------------------------------------------------------------------------
-// Neighbourhood cross-correlation: value and both update directions.
+// Gaussian smoothing of displacement fields, all axes in one pass.
 //
-// A block owns a 32 x 8 tile of output columns and marches along z over a chunk of ZC
-// slices.  Each thread keeps FP64 running z-window sums of F, M, F^2, M^2, FM for up to CPT
-// halo columns; the raw (F, M) values of the last 2R+1 slices sit in a shared-memory ring so
-// the leaving slice is subtracted without a second global read.  Per slice the column sums
-// are box-summed along x and then y in shared memory (FP64), giving the five window sums of
-// each output voxel, from which the CC terms and derivatives follow.  The in-bounds count is
-// separable (cx*cy*cz) and computed analytically.
-// ------------------------------------------------------------------------------------------
-struct CCParams {
-  float h[3];      // spacing
-  float dir[9];    // direction cosines
-  int identity_dir;
-  double eps;
-  int ZC;          // z-chunk per block
-};
-
-__device__ __forceinline__ int pmod(int a, int m) {
-  int r = a % m;
-  return r < 0 ? r + m : r;
-}
-
-__device__ __forceinline__ float grad1(float vm, float v0, float vp, int pos, int n, float h) {
-  if (n < 2 || pos == n - 1) return 0.0f;
-  if (pos == 0) return 0.5f * (vp - v0) / h;
-  return (vp - vm) / (2.0f * h);
-}
-
-template <int R, int DIM>
-struct CCShape {
-  static constexpr int TX = 32, TY = 8;
-  static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HC = HX * HY;
-  static constexpr int RZ = DIM == 3 ? R : 0;
-  static constexpr int RD = 2 * RZ + 1;
-  static constexpr int CPT = (HC + 255) / 256;
-  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)5 * HC * sizeof(double) +
-                                 (size_t)5 * HY * TX * sizeof(double);
-};
-
-template <int R, int DIM>
-__global__ void __launch_bounds__(256)
-    k_cc(const float* __restrict__ Ft, const float* __restrict__ Mt, Dims d, CCParams P, float* __restrict__ gF,
-         float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out) {
-  using S = CCShape<R, DIM>;
-  constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
-  if (ctl != nullptr && ctl->stop) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* ring = reinterpret_cast<float2*>(smem_raw);
-  double* cs = reinterpret_cast<double*>(ring + RD * HC);
-  double* xs = cs + 5 * HC;
-  __shared__ double red[32];
-  __shared__ int am_last;
-
-  const int tid = threadIdx.x;
-  const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const long long nxy = (long long)nx * ny, N = d.N;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * S::TY;
-  const int z0 = blockIdx.z * P.ZC;
-  const int z1 = min(z0 + P.ZC, nz);
-
-  // owned halo columns
-  int gofs[CPT];
-  bool gval[CPT];
-#pragma unroll
-  for (int c = 0; c < CPT; ++c) {
-    int col = tid + c * 256;
-    int hx = col % HX, hy = col / HX;
-    int gx = x0 - R + hx, gy = y0 - R + hy;
-    gval[c] = col < HC && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
-    gofs[c] = gval[c] ? gy * nx + gx : 0;
-  }
-  double acc[CPT][5];
-#pragma unroll
-  for (int c = 0; c < CPT; ++c)
-#pragma unroll
-    for (int q = 0; q < 5; ++q) acc[c][q] = 0.0;
-
-  // warm-up: slices z0-RZ .. z0+RZ-1
-  for (int zs = z0 - RZ; zs < z0 + RZ; ++zs) {
-    const bool zin = zs >= 0 && zs < nz;
-    const int slot = pmod(zs, RD);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      int col = tid + c * 256;
-      if (col < HC) {
-        float2 v = make_float2(0.0f, 0.0f);
-        if (zin && gval[c]) {
-          long long o = (long long)zs * nxy + gofs[c];
-          v.x = __ldg(Ft + o);
-          v.y = __ldg(Mt + o);
-          double f = v.x, m = v.y;
-          acc[c][0] += f;
-          acc[c][1] += m;
-          acc[c][2] += f * f;
-          acc[c][3] += m * m;
-          acc[c][4] += f * m;
-        }
-        ring[slot * HC + col] = v;
-      }
-    }
-  }
-
-  double cc_acc = 0.0;
-  const int tx = tid & 31, ty = tid >> 5;
-  const int ox = x0 + tx, oy = y0 + ty;
-  const bool out_ok = ox < nx && oy < ny;
-  const double cxn = (double)(min(ox + R, nx - 1) - max(ox - R, 0) + 1);
-  const double cyn = (double)(min(oy + R, ny - 1) - max(oy - R, 0) + 1);
-
-  for (int zc = z0; zc < z1; ++zc) {
-    // slide the z window: subtract slice zc-RZ-1 (if it was added), add slice zc+RZ
-    const int ze = zc + RZ, zl = zc - RZ - 1;
-    const int slot = pmod(ze, RD);
-    const bool sub = zc > z0 && zl >= 0;
-    const bool zin = ze < nz;
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      int col = tid + c * 256;
-      if (col < HC) {
-        if (sub && gval[c]) {
-          float2 o = ring[slot * HC + col];
-          double f = o.x, m = o.y;
-          acc[c][0] -= f;
-          acc[c][1] -= m;
-          acc[c][2] -= f * f;
-          acc[c][3] -= m * m;
-          acc[c][4] -= f * m;
-        }
-        float2 v = make_float2(0.0f, 0.0f);
-        if (zin && gval[c]) {
-          long long o = (long long)ze * nxy + gofs[c];
-          v.x = __ldg(Ft + o);
-          v.y = __ldg(Mt + o);
-          double f = v.x, m = v.y;
-          acc[c][0] += f;
-          acc[c][1] += m;
-          acc[c][2] += f * f;
-          acc[c][3] += m * m;
-          acc[c][4] += f * m;
-        }
-        ring[slot * HC + col] = v;
-#pragma unroll
-        for (int q = 0; q < 5; ++q) cs[q * HC + col] = acc[c][q];
-      }
-    }
-    __syncthreads();
-    // x box sums: HY rows x TX outputs
-    for (int p = tid; p < HY * TX; p += 256) {
-      const int hy = p / TX, px = p % TX;
-      const double* src = cs + hy * HX + px;
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j <= 2 * R; ++j) s += src[q * HC + j];
-        xs[q * HY * TX + p] = s;
-      }
-    }
-    __syncthreads();
-    if (out_ok) {
-      double Sq[5];
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j <= 2 * R; ++j) s += xs[q * HY * TX + (ty + j) * TX + tx];
-        Sq[q] = s;
-      }
-      const double czn = (double)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
-      const double n = cxn * cyn * czn;
-      const double inv_n = __drcp_rn(n);
-      const double mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
-      const double sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
-      const double sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
-      const double sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
-      const int cidx = (ty + R) * HX + (tx + R);
-      const float2* rc = ring + pmod(zc, RD) * HC;
-      const float2 v0 = rc[cidx];
-      const double fh = (double)v0.x - mF, mh = (double)v0.y - mM;
-      double cc = 1.0, aF = 0.0, aM = 0.0;
-      if (sFF > P.eps && sMM > P.eps) {
-        const double prod = sFF * sMM;
-        const double ip = __drcp_rn(prod);
-        cc = sFM * sFM * ip;
-        const double coef = 2.0 * sFM * ip;
-        aF = coef * (fh - sFM * sFF * ip * mh);
-        aM = coef * (mh - sFM * sMM * ip * fh);
-      }
-      cc_acc += cc;
-      // central differences of both warped images (index axes)
-      float gMi[3], gFi[3];
-      {
-        const float2 xm = rc[cidx - 1], xp = rc[cidx + 1];
-        gMi[0] = grad1(xm.y, v0.y, xp.y, ox, nx, P.h[0]);
-        gFi[0] = grad1(xm.x, v0.x, xp.x, ox, nx, P.h[0]);
-        const float2 ym = rc[cidx - HX], yp = rc[cidx + HX];
-        gMi[1] = grad1(ym.y, v0.y, yp.y, oy, ny, P.h[1]);
-        gFi[1] = grad1(ym.x, v0.x, yp.x, oy, ny, P.h[1]);
-        gMi[2] = gFi[2] = 0.0f;
-        if (DIM == 3) {
-          const float2 zm = ring[pmod(zc - 1, RD) * HC + cidx], zp = ring[pmod(zc + 1, RD) * HC + cidx];
-          gMi[2] = grad1(zm.y, v0.y, zp.y, zc, nz, P.h[2]);
-          gFi[2] = grad1(zm.x, v0.x, zp.x, zc, nz, P.h[2]);
-        }
-      }
-      const long long oi = (long long)zc * nxy + (long long)oy * nx + ox;
-#pragma unroll
-      for (int dd = 0; dd < DIM; ++dd) {
-        float pm, pf;
-        if (P.identity_dir) {
-          pm = gMi[dd];
-          pf = gFi[dd];
-        } else {
-          pm = 0.0f;
-          pf = 0.0f;
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) {
-            pm += P.dir[dd * 3 + a] * gMi[a];
-            pf += P.dir[dd * 3 + a] * gFi[a];
-          }
-        }
-        gF[dd * N + oi] = (float)(aF * (double)pm);
-        gM[dd * N + oi] = (float)(aM * (double)pf);
-      }
-      if (cc_out != nullptr) cc_out[oi] = (float)cc;
-    }
-    __syncthreads();
-  }
-
-  // deterministic reduction of sum(cc): block partials, the last block sums them in order
-  const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
-  const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  double bs = block_sum_d(cc_acc, red);
-  if (tid == 0) {
-    partials[bid] = bs;
-    __threadfence();
-    unsigned t = atomicAdd(&ctl->cc_counter, 1u);
-    am_last = (t == nblocks - 1);
-  }
-  __syncthreads();
-  if (am_last) {
-    __threadfence();
-    double s = 0.0;
-    for (unsigned b = tid; b < nblocks; b += 256) s += __ldcg(partials + b);
-    s = block_sum_d(s, red);
-    if (tid == 0) {
-      ctl->cc_sum = s;
-      ctl->metric = -s / (double)N;
-      ctl->cc_counter = 0u;
-    }
-  }
-}
-
-template <int R, int DIM>
-static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, float* gF, float* gM, double* partials,
-                        IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P) {
-  using S = CCShape<R, DIM>;
-  k_cc<R, DIM><<<grid, 256, S::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
-}
-
-static int cc_zchunk(const GridInfo& g, int radius) {
-  if (g.d.dim == 2) return 1;
-  const int bx = (g.d.nx + 31) / 32, by = (g.d.ny + 7) / 8;
-  const int target = 148 * 6;
-  int chunks = (target + bx * by - 1) / (bx * by);
-  int zc = (g.d.nz + chunks - 1) / chunks;
-  zc = zc < 4 * radius ? 4 * radius : zc;
-  if (zc > g.d.nz) zc = g.d.nz;
-  if (zc < 1) zc = 1;
-  return zc;
-}
-
-int cc_blocks(const GridInfo& g, int radius) {
-  const int bx = (g.d.nx + 31) / 32, by = (g.d.ny + 7) / 8;
-  const int zc = cc_zchunk(g, radius);
-  return bx * by * ((g.d.nz + zc - 1) / zc);
-}
-
-size_t cc_smem_bytes(int dim, int radius) {
-  const size_t TX = 32, TY = 8, HX = TX + 2 * radius, HY = TY + 2 * radius, HC = HX * HY;
-  const size_t RD = dim == 3 ? 2 * radius + 1 : 1;
-  return RD * HC * 8 + 5 * HC * 8 + 5 * HY * TX * 8;
-}
-
-template <int R, int DIM>
-static cudaError_t cc_prepare_t() {
-  return cudaFuncSetAttribute(k_cc<R, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CCShape<R, DIM>::smem);
-}
-
-cudaError_t cc_prepare(int dim, int radius) {
-#define SYNX_CC_PREP(RR) \
-  case RR:               \
-    return dim == 3 ? cc_prepare_t<RR, 3>() : cc_prepare_t<RR, 2>();
-  switch (radius) {
-    SYNX_CC_PREP(1)
-    SYNX_CC_PREP(2)
-    SYNX_CC_PREP(3)
-    SYNX_CC_PREP(4)
-    SYNX_CC_PREP(5)
-    SYNX_CC_PREP(6)
-    SYNX_CC_PREP(7)
-    default:
-      return cudaErrorInvalidValue;
-  }
-#undef SYNX_CC_PREP
-}
-
-bool cc_radius_supported(int dim, int radius) {
-  return radius >= 1 && radius <= 7 && cc_smem_bytes(dim, radius) <= 227 * 1024;
-}
-
-void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out) {
-  count_launch();
-  CCParams P;
-  for (int k = 0; k < 3; ++k) P.h[k] = (float)g.sp[k];
-  bool ident = true;
-  for (int k = 0; k < 9; ++k) {
-    P.dir[k] = (float)g.dir[k];
-    if (g.dir[k] != ((k % 4) == 0 ? 1.0 : 0.0)) ident = false;
-  }
-  P.identity_dir = ident ? 1 : 0;
-  P.eps = 1.1920928955078125e-07;  // FLT_EPSILON: the reference metric's float guard
-  P.ZC = cc_zchunk(g, radius);
-  dim3 grid((g.d.nx + 31) / 32, (g.d.ny + 7) / 8, (g.d.nz + P.ZC - 1) / P.ZC);
-#define SYNX_CC_CASE(RR)                                                                         \
-  case RR:                                                                                       \
-    if (g.d.dim == 3)                                                                            \
-      cc_launch_t<RR, 3>(Ft, Mt, g, gF, gM, partials, ctl, s, cc_out, grid, P);                  \
-    else                                                                                         \
-      cc_launch_t<RR, 2>(Ft, Mt, g, gF, gM, partials, ctl, s, cc_out, grid, P);                  \
-    break;
-  switch (radius) {
-    SYNX_CC_CASE(1)
-    SYNX_CC_CASE(2)
-    SYNX_CC_CASE(3)
-    SYNX_CC_CASE(4)
-    SYNX_CC_CASE(5)
-    SYNX_CC_CASE(6)
-    SYNX_CC_CASE(7)
-    default:
-      break;
-  }
-#undef SYNX_CC_CASE
-}
-
-// ------------------------------------------------------------------------------------------
-// Separable Gaussian smoothing of displacement fields (both halves per launch, blockIdx.y).
+// A block owns a 32 x 8 tile of output columns of one field and marches along z.  For each
+// input slice it stages the (32+2Rx) x (8+2Ry) halo tile of every component in shared
+// memory (replicate-edge indices), convolves along x, then y (each thread its own column),
+// and keeps the xy-smoothed slices of the last 2Rz+1 z positions in a per-thread shared
+// ring; the z convolution of that ring gives the output.  The pass order (x, y, z) and the
+// float rounding after each axis follow the separable filter.  The epilogue applies SyN's
+// boundary zeroing and blend, and reduces max ||u / spacing|| for the update scaling.
 // ------------------------------------------------------------------------------------------
 struct Ptr2c {
   const float* p[2];
@@ -575,52 +265,272 @@ struct Ptr2 {
   float* p[2];
 };
 
+constexpr int kSmoothRMax = 12;
+
+struct Smooth3Args {
+  Ptr2c in, orig;
+  Ptr2 out;
+  float k[3][2 * kSmoothRMax + 1];  // per-axis kernels, zero-padded and centred to radius R
+  int ZC, halves, epilogue, do_max;
+  float w1, w2;
+  float ih[3];
+};
+
+__host__ __device__ inline size_t smooth3_smem_floats(int dim, int R) {
+  const int HX = 32 + 2 * R, HY = 8 + 2 * R, RD = dim == 3 ? 2 * R + 1 : 1;
+  return (size_t)dim * HY * HX + (size_t)dim * HY * 32 + (size_t)RD * dim * 256;
+}
+
+template <int DIM, int R>
+__global__ void __launch_bounds__(256) k_smooth3(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  if (ctl != nullptr && ctl->stop) return;
+  constexpr int RZ = DIM == 3 ? R : 0;
+  constexpr int HX = 32 + 2 * R, HY = 8 + 2 * R, RD = 2 * RZ + 1, K = 2 * R + 1;
+  extern __shared__ __align__(16) float sm3[];
+  __shared__ float red[32];
+  float* tile = sm3;                   // [DIM][HY][HX]
+  float* xsum = tile + DIM * HY * HX;  // [DIM][HY][32]
+  float* ring = xsum + DIM * HY * 32;  // [RD][DIM][256]
+  const int nzc = gridDim.z / a.halves;
+  const int h = blockIdx.z / nzc;
+  const int zc = blockIdx.z - h * nzc;
+  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
+  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+  const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
+  float kx[K], ky[K], kz[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    kx[j] = a.k[0][j];
+    ky[j] = a.k[1][j];
+    kz[j] = a.k[2][j];
+  }
+
+  // xy-smoothed slice clamp(s) -> ring slot of s (each thread writes its own column)
+  auto xy_slice = [&](int s) {
+    const int zs = min(max(s, 0), nz - 1);
+    const float* plane = src + zs * nxy;
+    for (int row = ty; row < DIM * HY; row += 8) {
+      const int c = row / HY, hy = row - c * HY;
+      const int gy = min(max(y0 - R + hy, 0), ny - 1);
+      const float* line = plane + c * N + gy * nx;
+      float* trow = tile + row * HX;
+#pragma unroll
+      for (int hx = tx; hx < HX; hx += 32) trow[hx] = __ldg(line + min(max(x0 - R + hx, 0), nx - 1));
+    }
+    __syncthreads();
+    for (int row = ty; row < DIM * HY; row += 8) {
+      const float* t = tile + row * HX + tx;
+      float acc = 0.0f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc = fmaf(kx[j], t[j], acc);
+      xsum[row * 32 + tx] = acc;
+    }
+    __syncthreads();
+    const int slot = ((s % RD) + RD) % RD;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const float* col = xsum + (c * HY + ty) * 32 + tx;
+      float acc = 0.0f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc = fmaf(ky[j], col[j * 32], acc);
+      ring[(slot * DIM + c) * 256 + tid] = acc;
+    }
+    __syncthreads();  // tile and xsum are reused by the next slice
+  };
+
+  for (int s = z0 - RZ; s < z0 + RZ; ++s) xy_slice(s);
+  const int ox = x0 + tx, oy = y0 + ty;
+  const bool ok = ox < nx && oy < ny;
+  float mx = 0.0f;
+  for (int z = z0; z < z1; ++z) {
+    xy_slice(z + RZ);
+    if (ok) {
+      const int i = z * nxy + oy * nx + ox;
+      const bool edge = a.epilogue && (ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1 ||
+                                       (DIM == 3 && (z == 0 || z == nz - 1)));
+      const int base = (((z - RZ) % RD) + RD) % RD;
+      float nrm2 = 0.0f;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        float v;
+        if (DIM == 3) {
+          v = 0.0f;
+#pragma unroll
+          for (int j = 0; j < K; ++j) {
+            int sl = base + j;
+            sl = sl >= RD ? sl - RD : sl;
+            v = fmaf(kz[j], ring[(sl * DIM + c) * 256 + tid], v);
+          }
+        } else {
+          v = ring[c * 256 + tid];
+        }
+        if (a.epilogue) {
+          if (edge) v = 0.0f;
+          else if (a.w2 != 0.0f) v = v * a.w1 + org[c * N + i] * a.w2;
+        }
+        if (a.do_max) {
+          const float q = v * a.ih[c];
+          nrm2 += q * q;
+        }
+        dst[c * N + i] = v;
+      }
+      if (a.do_max) mx = fmaxf(mx, sqrtf(nrm2));
+    }
+  }
+  if (a.do_max) {
+    const float bm = block_max_f(mx, red);
+    if (tid == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
+  }
+}
+
+static int smooth3_radius(int dim, const int R[3]) {
+  int r = 0;
+  for (int a = 0; a < dim; ++a) r = std::max(r, R[a]);
+  return std::max(r, 1);
+}
+
+bool smooth3_supported(int dim, const int R[3]) { return smooth3_radius(dim, R) <= kSmoothRMax; }
+
+template <int DIM, int R>
+static cudaError_t smooth3_attr() {
+  return cudaFuncSetAttribute(k_smooth3<DIM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(smooth3_smem_floats(DIM, R) * 4));
+}
+
+template <int R>
+static cudaError_t smooth3_attr_both() {
+  cudaError_t e = smooth3_attr<3, R>();
+  return e == cudaSuccess ? smooth3_attr<2, R>() : e;
+}
+
+cudaError_t smooth3_prepare() {
+  cudaError_t e = cudaSuccess;
+  e = e ? e : smooth3_attr_both<1>();
+  e = e ? e : smooth3_attr_both<2>();
+  e = e ? e : smooth3_attr_both<3>();
+  e = e ? e : smooth3_attr_both<4>();
+  e = e ? e : smooth3_attr_both<5>();
+  e = e ? e : smooth3_attr_both<6>();
+  e = e ? e : smooth3_attr_both<7>();
+  e = e ? e : smooth3_attr_both<8>();
+  e = e ? e : smooth3_attr_both<9>();
+  e = e ? e : smooth3_attr_both<10>();
+  e = e ? e : smooth3_attr_both<11>();
+  e = e ? e : smooth3_attr_both<12>();
+  return e;
+}
+
+void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, int halves,
+                         const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
+                         float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s) {
+  count_launch();
+  const int dim = g.d.dim;
+  const int RR = smooth3_radius(dim, R);
+  Smooth3Args a;
+  memset(&a, 0, sizeof(a));
+  a.in = Ptr2c{{in[0], halves > 1 ? in[1] : in[0]}};
+  a.out = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
+  a.orig = Ptr2c{{orig ? orig[0] : nullptr, orig ? (halves > 1 ? orig[1] : orig[0]) : nullptr}};
+  for (int ax = 0; ax < 3; ++ax) {
+    a.ih[ax] = (float)(1.0 / g.sp[ax]);
+    if (ax < dim) {
+      for (int j = 0; j <= 2 * R[ax]; ++j) a.k[ax][RR - R[ax] + j] = khost[ax][j];
+    } else {
+      a.k[ax][RR] = 1.0f;
+    }
+  }
+  a.halves = halves;
+  a.epilogue = epilogue ? 1 : 0;
+  a.do_max = maxnorm ? 1 : 0;
+  a.w1 = w1;
+  a.w2 = w2;
+  const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
+  int zc = g.d.nz;
+  if (dim == 3) {
+    const int target = 148 * 6;
+    const int chunks = (target + gx * gy * halves - 1) / (gx * gy * halves);
+    zc = (g.d.nz + chunks - 1) / chunks;
+    zc = std::max(zc, std::max(4 * RR, 8));
+    zc = std::min(zc, g.d.nz);
+  }
+  a.ZC = zc;
+  const int nzc = (g.d.nz + zc - 1) / zc;
+  const dim3 grid(gx, gy, nzc * halves);
+  const size_t smem = smooth3_smem_floats(dim, RR) * 4;
+#define SYNX_SM3(RV)                                          \
+  case RV:                                                    \
+    if (dim == 3)                                             \
+      k_smooth3<3, RV><<<grid, 256, smem, s>>>(a, g.d, ctl);  \
+    else                                                      \
+      k_smooth3<2, RV><<<grid, 256, smem, s>>>(a, g.d, ctl);  \
+    break;
+  switch (RR) {
+    SYNX_SM3(1)
+    SYNX_SM3(2)
+    SYNX_SM3(3)
+    SYNX_SM3(4)
+    SYNX_SM3(5)
+    SYNX_SM3(6)
+    SYNX_SM3(7)
+    SYNX_SM3(8)
+    SYNX_SM3(9)
+    SYNX_SM3(10)
+    SYNX_SM3(11)
+    SYNX_SM3(12)
+    default:
+      break;
+  }
+#undef SYNX_SM3
+}
+
+// Single-axis fallback for kernels too wide for the fused pass.
 template <int DIM>
 __global__ void __launch_bounds__(256)
-    k_smooth_pass(Ptr2c in, Ptr2 out, Ptr2c orig, Dims d, int axis, const float* __restrict__ coeffs, int R, int last,
-                  float w1, float w2, int do_max, float ihx, float ihy, float ihz, IterCtl* ctl) {
+    k_smooth_pass(Ptr2c in, Ptr2 out, Ptr2c orig, Dims d, int zb, int axis, const float* __restrict__ coeffs, int R,
+                  int last, float w1, float w2, int do_max, float ihx, float ihy, float ihz, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
   __shared__ float red[32];
-  const int h = blockIdx.y;
+  const Coord3 c3 = coord3(d, zb, gridDim.z / ((d.nz + zb - 1) / zb));
+  const int h = c3.h;
   const float* __restrict__ src = in.p[h];
   float* __restrict__ dst = out.p[h];
   const float* __restrict__ org = orig.p[h];
-  const long long N = d.N, stride = (long long)gridDim.x * blockDim.x;
+  const int N = (int)d.N, nxy = d.nx * d.ny;
   const int len = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
-  const long long astride = axis == 0 ? 1 : (axis == 1 ? d.nx : (long long)d.nx * d.ny);
+  const int astride = axis == 0 ? 1 : (axis == 1 ? d.nx : nxy);
   const float ih[3] = {ihx, ihy, ihz};
   float mx = 0.0f;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, d, x, y, z);
-    const int pos = axis == 0 ? x : (axis == 1 ? y : z);
-    const bool edge = last && (x == 0 || x == d.nx - 1 || y == 0 || y == d.ny - 1 ||
-                               (DIM == 3 && (z == 0 || z == d.nz - 1)));
-    float nrm2 = 0.0f;
+  if (c3.ok) {
+    for (int z = c3.z0; z < c3.z1; ++z) {
+      const int i = z * nxy + c3.y * d.nx + c3.x;
+      const int pos = axis == 0 ? c3.x : (axis == 1 ? c3.y : z);
+      const bool edge = last && (c3.x == 0 || c3.x == d.nx - 1 || c3.y == 0 || c3.y == d.ny - 1 ||
+                                 (DIM == 3 && (z == 0 || z == d.nz - 1)));
+      float nrm2 = 0.0f;
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      const float* line = src + c * N + i - pos * astride;
-      float s = 0.0f;
-      if (pos >= R && pos + R < len) {
-        const float* q = line + (long long)(pos - R) * astride;
-        for (int j = 0; j <= 2 * R; ++j) s = fmaf(__ldg(coeffs + j), __ldg(q + j * astride), s);
-      } else {
+      for (int c = 0; c < DIM; ++c) {
+        const float* line = src + c * N + i - pos * astride;
+        float s = 0.0f;
         for (int j = 0; j <= 2 * R; ++j) {
-          int qq = min(max(pos + j - R, 0), len - 1);
-          s = fmaf(__ldg(coeffs + j), __ldg(line + (long long)qq * astride), s);
+          const int qq = min(max(pos + j - R, 0), len - 1);
+          s = fmaf(__ldg(coeffs + j), __ldg(line + qq * astride), s);
         }
+        if (last) {
+          if (edge) s = 0.0f;
+          else if (w2 != 0.0f) s = s * w1 + org[c * N + i] * w2;
+        }
+        if (do_max) {
+          const float v = s * ih[c];
+          nrm2 += v * v;
+        }
+        dst[c * N + i] = s;
       }
-      if (last) {
-        if (edge) s = 0.0f;
-        else if (w2 != 0.0f) s = s * w1 + org[c * N + i] * w2;
-      }
-      if (do_max) {
-        const float v = s * ih[c];
-        nrm2 += v * v;
-      }
-      dst[c * N + i] = s;
+      if (do_max) mx = fmaxf(mx, sqrtf(nrm2));
     }
-    if (do_max) mx = fmaxf(mx, sqrtf(nrm2));
   }
   if (do_max) {
     float bm = block_max_f(mx, red);
@@ -635,14 +545,14 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
   Ptr2c pi{{in[0], halves > 1 ? in[1] : in[0]}};
   Ptr2 po{{out[0], halves > 1 ? out[1] : out[0]}};
   Ptr2c pg{{orig ? orig[0] : nullptr, orig ? (halves > 1 ? orig[1] : orig[0]) : nullptr}};
-  dim3 grid(grid_for(g.d.N, 256), halves);
+  const Map3 m = map3(g.d, halves);
   float ih[3] = {(float)(1.0 / g.sp[0]), (float)(1.0 / g.sp[1]), (float)(1.0 / g.sp[2])};
   if (g.d.dim == 3)
-    k_smooth_pass<3><<<grid, 256, 0, s>>>(pi, po, pg, g.d, axis, coeffs, R, last ? 1 : 0, w1, w2, maxnorm ? 1 : 0,
-                                          ih[0], ih[1], ih[2], ctl);
+    k_smooth_pass<3><<<m.grid, 256, 0, s>>>(pi, po, pg, g.d, m.zb, axis, coeffs, R, last ? 1 : 0, w1, w2,
+                                            maxnorm ? 1 : 0, ih[0], ih[1], ih[2], ctl);
   else
-    k_smooth_pass<2><<<grid, 256, 0, s>>>(pi, po, pg, g.d, axis, coeffs, R, last ? 1 : 0, w1, w2, maxnorm ? 1 : 0,
-                                          ih[0], ih[1], ih[2], ctl);
+    k_smooth_pass<2><<<m.grid, 256, 0, s>>>(pi, po, pg, g.d, m.zb, axis, coeffs, R, last ? 1 : 0, w1, w2,
+                                            maxnorm ? 1 : 0, ih[0], ih[1], ih[2], ctl);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -650,10 +560,12 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
 // Reads w only at its own voxel, so it runs in place (out == w).
 // ------------------------------------------------------------------------------------------
 template <int DIM>
-__global__ void __launch_bounds__(256) k_compose(Ptr2c dd, Ptr2c ww, Ptr2 oo, Dims d, Affine m, double eta,
-                                                 IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_compose(Ptr2c dd, Ptr2c ww, Ptr2 oo, Dims d, int zb, int halves, Affine m,
+                                                 double eta, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
-  const int h = blockIdx.y;
+  const Coord3 c3 = coord3(d, zb, halves);
+  if (!c3.ok) return;
+  const int h = c3.h;
   const float* __restrict__ D = dd.p[h];
   const float* W = ww.p[h];
   float* O = oo.p[h];
@@ -662,13 +574,13 @@ __global__ void __launch_bounds__(256) k_compose(Ptr2c dd, Ptr2c ww, Ptr2 oo, Di
     const float mx = __uint_as_float(ctl->maxnorm[h]);
     scale = mx > 0.0f ? (float)(eta / (double)mx) : (float)eta;
   }
-  const long long N = d.N, stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, d, x, y, z);
+  const int N = (int)d.N, nxy = d.nx * d.ny;
+  const float fx = (float)c3.x, fy = (float)c3.y;
+  for (int z = c3.z0; z < c3.z1; ++z) {
+    const int i = z * nxy + c3.y * d.nx + c3.x;
     const float w0 = W[i], w1 = W[N + i], w2 = DIM == 3 ? W[2 * N + i] : 0.0f;
     float cx, cy, cz;
-    map_point<DIM>(m, (float)x, (float)y, (float)z, w0, w1, w2, cx, cy, cz);
+    map_point<DIM>(m, fx, fy, (float)z, w0, w1, w2, cx, cy, cz);
     if (inside_buffer<DIM>(d, cx, cy, cz)) {
       const Cell c = make_cell<DIM>(d, cx, cy, cz);
       O[i] = fmaf(scale, lerp_at<DIM>(D, c), w0);
@@ -688,12 +600,12 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
   Ptr2c pd{{d[0], halves > 1 ? d[1] : d[0]}};
   Ptr2c pw{{w[0], halves > 1 ? w[1] : w[0]}};
   Ptr2 po{{out[0], halves > 1 ? out[1] : out[0]}};
-  Affine m = make_affine(g, g);
-  dim3 grid(grid_for(g.d.N, 256), halves);
+  Affine a = make_affine(g, g);
+  const Map3 m = map3(g.d, halves);
   if (g.d.dim == 3)
-    k_compose<3><<<grid, 256, 0, s>>>(pd, pw, po, g.d, m, (double)eta, ctl);
+    k_compose<3><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
   else
-    k_compose<2><<<grid, 256, 0, s>>>(pd, pw, po, g.d, m, (double)eta, ctl);
+    k_compose<2><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -706,33 +618,32 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
 struct InvParams {
   float A[9];
   float ih[3];
-  int k, max_iter, phase, stop_aware;
+  int k, max_iter, phase, stop_aware, zb, halves;
   double mean_tol, max_tol;
 };
 
 template <int DIM>
-__device__ __forceinline__ void residual(const float* __restrict__ phi, const Dims& d, const float* A, int x, int y,
-                                         int z, long long i, const float p[3], float e[3]) {
+__device__ __forceinline__ void residual(const float* __restrict__ phi, const Dims& d, const float* A, float fx,
+                                         float fy, float fz, const float p[3], float e[3]) {
   float cx, cy, cz;
-  cx = (float)x + A[0] * p[0] + A[1] * p[1];
-  cy = (float)y + A[3] * p[0] + A[4] * p[1];
+  cx = fx + A[0] * p[0] + A[1] * p[1];
+  cy = fy + A[3] * p[0] + A[4] * p[1];
   cz = 0.0f;
   if (DIM == 3) {
     cx += A[2] * p[2];
     cy += A[5] * p[2];
-    cz = (float)z + A[6] * p[0] + A[7] * p[1] + A[8] * p[2];
+    cz = fz + A[6] * p[0] + A[7] * p[1] + A[8] * p[2];
   }
   e[0] = p[0];
   e[1] = p[1];
   e[2] = DIM == 3 ? p[2] : 0.0f;
   if (inside_buffer<DIM>(d, cx, cy, cz)) {
     const Cell c = make_cell<DIM>(d, cx, cy, cz);
-    const long long N = d.N;
+    const int N = (int)d.N;
     e[0] += lerp_at<DIM>(phi, c);
     e[1] += lerp_at<DIM>(phi + N, c);
     if (DIM == 3) e[2] += lerp_at<DIM>(phi + 2 * N, c);
   }
-  (void)i;
 }
 
 template <int DIM>
@@ -742,7 +653,8 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
   __shared__ double redd[32];
   __shared__ float redf[32];
   __shared__ int am_last;
-  const int h = blockIdx.y;
+  const Coord3 c3 = coord3(d, P.zb, P.halves);
+  const int h = c3.h;
   InvCtl& C = ctl->inv[P.phase][h];
   const float* __restrict__ phi = phis.p[h];
   float* __restrict__ psi = psis.p[h];
@@ -752,7 +664,7 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
   if (k > 0) {
     const int s = k & 1;
     if (!C.exec[s]) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) C.exec[s ^ 1] = 0;
+      if (c3.bid == 0 && threadIdx.x == 0) C.exec[s ^ 1] = 0;
       return;
     }
     apply = true;
@@ -761,70 +673,74 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
     const double mean = C.mean[s];
     lim = eps * mx;
     stats = (k + 1 <= P.max_iter) && ((double)mx > P.max_tol) && (mean > P.mean_tol);
-    if (!stats) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
-        C.exec[s ^ 1] = 0;
-        C.iters = k;
-      }
+    if (!stats && c3.bid == 0 && threadIdx.x == 0) {
+      C.exec[s ^ 1] = 0;
+      C.iters = k;
     }
   }
-  const long long N = d.N, stride = (long long)gridDim.x * blockDim.x;
+  if (!stats && !c3.ok) return;
+  const int N = (int)d.N, nxy = d.nx * d.ny;
   double acc = 0.0;
   float mxl = 0.0f;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, d, x, y, z);
-    float p[3];
-    p[0] = psi[i];
-    p[1] = psi[N + i];
-    p[2] = DIM == 3 ? psi[2 * N + i] : 0.0f;
-    float e[3];
-    if (apply) {
-      residual<DIM>(phi, d, P.A, x, y, z, i, p, e);
-      float s2 = 0.0f;
+  if (c3.ok) {
+    const float fx = (float)c3.x, fy = (float)c3.y;
+    const bool xyedge = c3.x == 0 || c3.x == d.nx - 1 || c3.y == 0 || c3.y == d.ny - 1;
+    for (int z = c3.z0; z < c3.z1; ++z) {
+      const int i = z * nxy + c3.y * d.nx + c3.x;
+      const float fz = (float)z;
+      float p[3];
+      p[0] = psi[i];
+      p[1] = psi[N + i];
+      p[2] = DIM == 3 ? psi[2 * N + i] : 0.0f;
+      float e[3];
+      if (apply) {
+        residual<DIM>(phi, d, P.A, fx, fy, fz, p, e);
+        float s2 = 0.0f;
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        const float v = e[c] * P.ih[c];
-        s2 += v * v;
+        for (int c = 0; c < DIM; ++c) {
+          const float v = e[c] * P.ih[c];
+          s2 += v * v;
+        }
+        const float nrm = sqrtf(s2);
+        const float f = nrm > lim ? lim / nrm : 1.0f;
+        const bool edge = xyedge || (DIM == 3 && (z == 0 || z == d.nz - 1));
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) p[c] = edge ? 0.0f : p[c] + ((-e[c]) * f) * eps;
+        psi[i] = p[0];
+        psi[N + i] = p[1];
+        if (DIM == 3) psi[2 * N + i] = p[2];
       }
-      const float nrm = sqrtf(s2);
-      const float f = nrm > lim ? lim / nrm : 1.0f;
-      const bool edge = x == 0 || x == d.nx - 1 || y == 0 || y == d.ny - 1 || (DIM == 3 && (z == 0 || z == d.nz - 1));
+      if (stats) {
+        residual<DIM>(phi, d, P.A, fx, fy, fz, p, e);
+        float s2 = 0.0f;
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) p[c] = edge ? 0.0f : p[c] + ((-e[c]) * f) * eps;
-      psi[i] = p[0];
-      psi[N + i] = p[1];
-      if (DIM == 3) psi[2 * N + i] = p[2];
-    }
-    if (stats) {
-      residual<DIM>(phi, d, P.A, x, y, z, i, p, e);
-      float s2 = 0.0f;
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        const float v = e[c] * P.ih[c];
-        s2 += v * v;
+        for (int c = 0; c < DIM; ++c) {
+          const float v = e[c] * P.ih[c];
+          s2 += v * v;
+        }
+        const float nrm = sqrtf(s2);
+        acc += (double)nrm;
+        mxl = fmaxf(mxl, nrm);
       }
-      const float nrm = sqrtf(s2);
-      acc += (double)nrm;
-      mxl = fmaxf(mxl, nrm);
     }
   }
   if (!stats) return;
   const double bs = block_sum_d(acc, redd);
   const float bm = block_max_f(mxl, redf);
+  const int nb = gridDim.x * gridDim.y * (gridDim.z / P.halves);
   if (threadIdx.x == 0) {
-    psum[h * pcap + blockIdx.x] = bs;
-    pmax[h * pcap + blockIdx.x] = bm;
+    psum[h * pcap + c3.bid] = bs;
+    pmax[h * pcap + c3.bid] = bm;
     __threadfence();
     const unsigned t = atomicAdd(&C.counter, 1u);
-    am_last = (t == gridDim.x - 1);
+    am_last = (t == (unsigned)nb - 1);
   }
   __syncthreads();
   if (am_last) {
     __threadfence();
     double s = 0.0;
     float m = 0.0f;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
       s += __ldcg(psum + h * pcap + b);
       m = fmaxf(m, __ldcg(pmax + h * pcap + b));
     }
@@ -841,7 +757,7 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
   }
 }
 
-int inv_blocks(const GridInfo& g) { return grid_for(g.d.N, 256, 148 * 8); }
+int inv_blocks(const GridInfo& g) { return map3(g.d, 2).nblocks; }
 
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
@@ -850,20 +766,26 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
   Ptr2c pp{{phi[0], halves > 1 ? phi[1] : phi[0]}};
   Ptr2 ps{{psi[0], halves > 1 ? psi[1] : psi[0]}};
   InvParams P;
-  Affine m = make_affine(g, g);
-  for (int j = 0; j < 9; ++j) P.A[j] = m.A[j];
+  Affine a = make_affine(g, g);
+  for (int j = 0; j < 9; ++j) P.A[j] = a.A[j];
   for (int j = 0; j < 3; ++j) P.ih[j] = (float)(1.0 / g.sp[j]);
+  // the block decomposition is the same for one or two halves, so the partial buffers sized
+  // by inv_blocks() fit either
+  const Map3 m2 = map3(g.d, 2);
+  Map3 m = m2;
+  m.grid.z = (m2.grid.z / 2) * halves;
   P.k = k;
   P.max_iter = max_iter;
   P.phase = phase;
   P.stop_aware = stop_aware ? 1 : 0;
+  P.zb = m.zb;
+  P.halves = halves;
   P.mean_tol = mean_tol;
   P.max_tol = max_tol;
-  dim3 grid(inv_blocks(g), halves);
   if (g.d.dim == 3)
-    k_invert_step<3><<<grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+    k_invert_step<3><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
   else
-    k_invert_step<2><<<grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+    k_invert_step<2><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -917,15 +839,16 @@ struct Ptr4 {
 };
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_resample(Ptr4c in, Dims di, Ptr4 out, Dims dout, Affine m, int nf) {
-  const long long No = dout.N, Ni = di.N, stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < No; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, dout, x, y, z);
+__global__ void __launch_bounds__(256) k_resample(Ptr4c in, Dims di, Ptr4 out, Dims dout, int zb, Affine m, int nf) {
+  const Coord3 c3 = coord3(dout, zb, 1);
+  if (!c3.ok) return;
+  const int No = (int)dout.N, Ni = (int)di.N, nxy = dout.nx * dout.ny;
+  for (int z = c3.z0; z < c3.z1; ++z) {
+    const int i = z * nxy + c3.y * dout.nx + c3.x;
     float cx, cy, cz;
-    map_point<DIM>(m, (float)x, (float)y, (float)z, 0.0f, 0.0f, 0.0f, cx, cy, cz);
+    map_point<DIM>(m, (float)c3.x, (float)c3.y, (float)z, 0.0f, 0.0f, 0.0f, cx, cy, cz);
     const bool ok = inside_buffer<DIM>(di, cx, cy, cz);
-    Cell c;
+    Cell c{};
     if (ok) c = make_cell<DIM>(di, cx, cy, cz);
     for (int f = 0; f < nf; ++f)
 #pragma unroll
@@ -942,31 +865,32 @@ void launch_resample_fields(const float* const* in, const GridInfo& gi, float* c
     pi.p[f] = in[f];
     po.p[f] = out[f];
   }
-  Affine m = make_affine(go, gi);
-  int blocks = grid_for(go.d.N, 256);
+  Affine a = make_affine(go, gi);
+  const Map3 m = map3(go.d);
   if (go.d.dim == 3)
-    k_resample<3><<<blocks, 256, 0, s>>>(pi, gi.d, po, go.d, m, nfields);
+    k_resample<3><<<m.grid, 256, 0, s>>>(pi, gi.d, po, go.d, m.zb, a, nfields);
   else
-    k_resample<2><<<blocks, 256, 0, s>>>(pi, gi.d, po, go.d, m, nfields);
+    k_resample<2><<<m.grid, 256, 0, s>>>(pi, gi.d, po, go.d, m.zb, a, nfields);
 }
 
 // ------------------------------------------------------------------------------------------
 // Image pyramid: one separable pass, replicate-edge boundary, FP64 accumulation.
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_conv_image_axis(const float* __restrict__ in, float* __restrict__ out, Dims d,
-                                                         int axis, const double* __restrict__ coeffs, int R) {
-  const long long N = d.N, stride = (long long)gridDim.x * blockDim.x;
+                                                         int zb, int axis, const double* __restrict__ coeffs, int R) {
+  const Coord3 c3 = coord3(d, zb, 1);
+  if (!c3.ok) return;
+  const int nxy = d.nx * d.ny;
   const int len = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
-  const long long astride = axis == 0 ? 1 : (axis == 1 ? d.nx : (long long)d.nx * d.ny);
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-    int x, y, z;
-    voxel_xyz(i, d, x, y, z);
-    const int pos = axis == 0 ? x : (axis == 1 ? y : z);
+  const int astride = axis == 0 ? 1 : (axis == 1 ? d.nx : nxy);
+  for (int z = c3.z0; z < c3.z1; ++z) {
+    const int i = z * nxy + c3.y * d.nx + c3.x;
+    const int pos = axis == 0 ? c3.x : (axis == 1 ? c3.y : z);
     const float* line = in + i - pos * astride;
     double s = 0.0;
     for (int j = 0; j <= 2 * R; ++j) {
       const int q = min(max(pos + j - R, 0), len - 1);
-      s += __ldg(coeffs + j) * (double)__ldg(line + (long long)q * astride);
+      s += __ldg(coeffs + j) * (double)__ldg(line + q * astride);
     }
     out[i] = (float)s;
   }
@@ -975,7 +899,8 @@ __global__ void __launch_bounds__(256) k_conv_image_axis(const float* __restrict
 void launch_conv_image_axis(const float* in, float* out, const GridInfo& g, int axis, const double* coeffs, int R,
                             cudaStream_t s) {
   count_launch();
-  k_conv_image_axis<<<grid_for(g.d.N, 256), 256, 0, s>>>(in, out, g.d, axis, coeffs, R);
+  const Map3 m = map3(g.d);
+  k_conv_image_axis<<<m.grid, 256, 0, s>>>(in, out, g.d, m.zb, axis, coeffs, R);
 }
 
 // ------------------------------------------------------------------------------------------

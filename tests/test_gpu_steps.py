@@ -106,6 +106,16 @@ def test_smooth_field(cuda, gi, variance):
     assert abs(mx - mx_ref) <= 1e-6 * mx_ref
 
 
+def test_smooth_field_wide_kernel_fallback(cuda):
+    # variance 300 gives a kernel too wide for the fused all-axes tile: the per-axis path runs
+    g = Geom((70, 66, 64))
+    u = np.random.default_rng(250).standard_normal((3,) + g.shape).astype(np.float32)
+    ref = O.smooth_field(u, g, 300.0)
+    out = empty(u.shape, cuda)
+    synx.smooth_field(dev(u, cuda), out, g, 300.0)
+    np.testing.assert_allclose(host(out), ref, atol=2e-6, rtol=0)
+
+
 @pytest.mark.parametrize("gi", range(3))
 def test_compose(cuda, gi):
     g = GEOMS[gi]

@@ -81,6 +81,25 @@ def test_multilevel_matches_oracle(cuda, dim, size, radius, iters, shrink, sigma
     assert rms_vox(fwd, np.zeros_like(fwd), go.spacing) > 0.02
 
 
+@pytest.mark.parametrize("dim,size,uvar,tvar", [(2, (72, 70), 0.25, 0.5), (3, (30, 32, 28), 2.0, 1.0)])
+def test_total_field_smoothing_and_blend(cuda, dim, size, uvar, tvar):
+    # SyN[eta, varU, varT] with varT > 0 smooths the composed total field; varU < 0.5 blends
+    f, m = make_pair(dim, size, seed=9)
+    g = Geom(size)
+    P = SyNParams(dim=dim, cc_radius=2, learning_rate=0.2, update_variance=uvar, total_variance=tvar,
+                  iterations=(6, 3), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12)
+    with SyNStage(P) as st:
+        st.set_images(f, g, m, g)
+        st.run()
+        fwd, inv = (planes(a) for a in st.fields())
+        go = st.output_geom()
+        log = st.log()
+    rf, ri, rg, rlog = O.syn_register(f, g, m, g, P)
+    np.testing.assert_allclose([r.metric for r in log], [r["metric"] for r in rlog], atol=2e-3)
+    assert rms_vox(fwd, rf, go.spacing) <= 0.05
+    assert rms_vox(inv, ri, go.spacing) <= 0.05
+
+
 def test_graph_replay_is_bit_identical_and_deterministic(cuda):
     f, m = make_pair(3, (36, 34, 32), seed=3)
     g = Geom((36, 34, 32))
