@@ -463,7 +463,7 @@ void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const
   const float* k[3] = {coeff_base, coeff_base + c->coeff_cap, coeff_base + 2 * c->coeff_cap};
   if (smooth3_supported(c->D, R)) {
     const float* kh[3] = {host_base, host_base + c->coeff_cap, host_base + 2 * c->coeff_cap};
-    launch_smooth_field(in, out, orig, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream);
+    launch_smooth_field(in, out, orig, tmp, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream);
     return;
   }
   const int D = c->D;
@@ -1144,7 +1144,8 @@ int synx_smooth_field(const float* in, float* out, const synx_geom* gg, double v
     const float* i0[1] = {in};
     float* o0[1] = {out};
     const float* k[3] = {hk.data(), hk.data() + 1024, hk.data() + 2048};
-    launch_smooth_field(i0, o0, i0, 1, g, k, R, true, w1, w2, true, t.ctl, s);
+    float* tt[1] = {ta};
+    launch_smooth_field(i0, o0, i0, tt, 1, g, k, R, true, w1, w2, true, t.ctl, s);
   } else {
     const float w1 = variance < 0.5 ? (float)(1.0 - variance / 0.5) : 1.0f, w2 = 1.0f - w1;
     const float* orig[1] = {in};

@@ -49,8 +49,10 @@ __device__ __forceinline__ void axis_cell(float c, int n, int& i0, int& i1, floa
   i1 = u;
 }
 
+// Grids hold fewer than 2^31 values per component plane (checked on the host), so cell
+// offsets are 32-bit.
 struct Cell {
-  long long o000, dx, dy, dz;  // base offset and the per-axis offset to the upper neighbour
+  int o000, dx, dy, dz;  // base offset and the per-axis offset to the upper neighbour
   float wx, wy, wz;
 };
 
@@ -62,11 +64,11 @@ __device__ __forceinline__ Cell make_cell(const Dims& d, float cx, float cy, flo
   axis_cell(cy, d.ny, y0, y1, c.wy);
   c.wz = 0.0f;
   if (DIM == 3) axis_cell(cz, d.nz, z0, z1, c.wz);
-  const long long sy = d.nx, sz = (long long)d.nx * d.ny;
-  c.o000 = (long long)z0 * sz + (long long)y0 * sy + x0;
+  const int sy = d.nx, sz = d.nx * d.ny;
+  c.o000 = z0 * sz + y0 * sy + x0;
   c.dx = x1 - x0;
-  c.dy = (long long)(y1 - y0) * sy;
-  c.dz = (long long)(z1 - z0) * sz;
+  c.dy = (y1 - y0) * sy;
+  c.dz = (z1 - z0) * sz;
   return c;
 }
 

@@ -111,7 +111,7 @@ struct Map3 {
   int zb;
   int nblocks;  // blocks per field (per half)
 };
-static Map3 map3(const Dims& d, int halves = 1, int target = 148 * 8) {
+static Map3 map3(const Dims& d, int halves = 1, int target = 148 * 24) {
   Map3 m;
   const int gx = (d.nx + 31) / 32, gy = (d.ny + 7) / 8;
   int per = target / (gx * gy * halves);
@@ -144,9 +144,24 @@ __device__ __forceinline__ Coord3 coord3(const Dims& d, int zb, int halves) {
   return c;
 }
 
-template <int DIM>
+static bool affine_diag(const Affine& m) {
+  const int off[6] = {1, 2, 3, 5, 6, 7};
+  for (int k : off)
+    if (m.B[k] != 0.0f || m.A[k] != 0.0f) return false;
+  return true;
+}
+
+// DIAG: the grids share axis directions (no rotation between them), the common case; the
+// map is then one FMA pair per axis.
+template <int DIM, bool DIAG = false>
 __device__ __forceinline__ void map_point(const Affine& m, float fx, float fy, float fz, float ux, float uy, float uz,
                                           float& cx, float& cy, float& cz) {
+  if (DIAG) {
+    cx = fmaf(m.A[0], ux, fmaf(m.B[0], fx, m.t[0]));
+    cy = fmaf(m.A[4], uy, fmaf(m.B[4], fy, m.t[1]));
+    cz = DIM == 3 ? fmaf(m.A[8], uz, fmaf(m.B[8], fz, m.t[2])) : 0.0f;
+    return;
+  }
   cx = m.t[0] + m.B[0] * fx + m.B[1] * fy + m.A[0] * ux + m.A[1] * uy;
   cy = m.t[1] + m.B[3] * fx + m.B[4] * fy + m.A[3] * ux + m.A[4] * uy;
   cz = 0.0f;
@@ -181,16 +196,16 @@ void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s) {
 // ------------------------------------------------------------------------------------------
 // Warp of both images through their inverse half-fields onto the level grid.
 // ------------------------------------------------------------------------------------------
-template <int DIM>
+template <int DIM, bool DIAG>
 __device__ __forceinline__ float sample(const float* __restrict__ img, const Dims& di, const Affine& m, float fx,
                                         float fy, float fz, float ux, float uy, float uz) {
   float cx, cy, cz;
-  map_point<DIM>(m, fx, fy, fz, ux, uy, uz, cx, cy, cz);
+  map_point<DIM, DIAG>(m, fx, fy, fz, ux, uy, uz, cx, cy, cz);
   if (!inside_buffer<DIM>(di, cx, cy, cz)) return 0.0f;
   return lerp_at<DIM>(img, make_cell<DIM>(di, cx, cy, cz));
 }
 
-template <int DIM>
+template <int DIM, bool DIAG>
 __global__ void __launch_bounds__(256)
     k_warp_pair(const float* __restrict__ F, Dims dF, Affine mF, const float* __restrict__ psiF,
                 const float* __restrict__ M, Dims dM, Affine mM, const float* __restrict__ psiM, Dims dv, int zb,
@@ -204,11 +219,31 @@ __global__ void __launch_bounds__(256)
   if (!c.ok) return;
   const int N = (int)dv.N, nxy = dv.nx * dv.ny;
   const float fx = (float)c.x, fy = (float)c.y;
+  const int i0 = c.z0 * nxy + c.y * dv.nx + c.x;
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
+  if (c.z0 < c.z1) {
+    a0 = psiF[i0];
+    a1 = psiF[N + i0];
+    a2 = DIM == 3 ? psiF[2 * N + i0] : 0.0f;
+    b0 = psiM[i0];
+    b1 = psiM[N + i0];
+    b2 = DIM == 3 ? psiM[2 * N + i0] : 0.0f;
+  }
   for (int z = c.z0; z < c.z1; ++z) {
     const int i = z * nxy + c.y * dv.nx + c.x;
     const float fz = (float)z;
-    Ft[i] = sample<DIM>(F, dF, mF, fx, fy, fz, psiF[i], psiF[N + i], DIM == 3 ? psiF[2 * N + i] : 0.0f);
-    Mt[i] = sample<DIM>(M, dM, mM, fx, fy, fz, psiM[i], psiM[N + i], DIM == 3 ? psiM[2 * N + i] : 0.0f);
+    const float u0 = a0, u1 = a1, u2 = a2, v0 = b0, v1 = b1, v2 = b2;
+    if (z + 1 < c.z1) {  // next slice's displacements, loaded ahead of this slice's gathers
+      const int j = i + nxy;
+      a0 = psiF[j];
+      a1 = psiF[N + j];
+      a2 = DIM == 3 ? psiF[2 * N + j] : 0.0f;
+      b0 = psiM[j];
+      b1 = psiM[N + j];
+      b2 = DIM == 3 ? psiM[2 * N + j] : 0.0f;
+    }
+    Ft[i] = sample<DIM, DIAG>(F, dF, mF, fx, fy, fz, u0, u1, u2);
+    Mt[i] = sample<DIM, DIAG>(M, dM, mM, fx, fy, fz, v0, v1, v2);
   }
 }
 
@@ -217,10 +252,18 @@ void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, con
   count_launch();
   Affine mF = make_affine(gv, gF), mM = make_affine(gv, gM);
   const Map3 m = map3(gv.d);
-  if (gv.d.dim == 3)
-    k_warp_pair<3><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
-  else
-    k_warp_pair<2><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+  const bool dg = affine_diag(mF) && affine_diag(mM);
+  if (gv.d.dim == 3) {
+    if (dg)
+      k_warp_pair<3, true><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+    else
+      k_warp_pair<3, false><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+  } else {
+    if (dg)
+      k_warp_pair<2, true><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+    else
+      k_warp_pair<2, false><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+  }
 }
 
 template <int DIM>
@@ -232,7 +275,7 @@ __global__ void __launch_bounds__(256) k_warp_image(const float* __restrict__ im
   const int N = (int)dv.N, nxy = dv.nx * dv.ny;
   for (int z = c.z0; z < c.z1; ++z) {
     const int i = z * nxy + c.y * dv.nx + c.x;
-    out[i] = sample<DIM>(img, di, m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f);
+    out[i] = sample<DIM, false>(img, di, m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f);
   }
 }
 
@@ -277,113 +320,171 @@ struct Smooth3Args {
 };
 
 __host__ __device__ inline size_t smooth3_smem_floats(int dim, int R) {
-  const int HX = 32 + 2 * R, HY = 8 + 2 * R, RD = dim == 3 ? 2 * R + 1 : 1;
-  return (size_t)dim * HY * HX + (size_t)dim * HY * 32 + (size_t)RD * dim * 256;
+  const int HXP = (32 + 2 * R + 3) & ~3, HY = 8 + 2 * R;
+  return (size_t)dim * HY * HXP + (size_t)dim * HY * 32;
 }
 
+// xy part: one block per (32 x 8 tile, slice, field).  The halo tile of every component is
+// staged in shared memory with replicate-edge indices, convolved along x (each work item makes
+// four consecutive outputs from float4 loads) and then along y.  In 2-D this is the whole
+// filter and the SyN epilogue runs here; in 3-D the xy-smoothed slice goes to `out` for the z
+// kernel.
 template <int DIM, int R>
-__global__ void __launch_bounds__(256) k_smooth3(const Smooth3Args a, Dims d, IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
-  constexpr int RZ = DIM == 3 ? R : 0;
-  constexpr int HX = 32 + 2 * R, HY = 8 + 2 * R, RD = 2 * RZ + 1, K = 2 * R + 1;
+  constexpr int K = 2 * R + 1;
+  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = 8 + 2 * R;
+  constexpr int NQ = (2 * R + 3) / 4 + 1;  // float4 loads covering 4 + 2R taps
   extern __shared__ __align__(16) float sm3[];
   __shared__ float red[32];
-  float* tile = sm3;                   // [DIM][HY][HX]
-  float* xsum = tile + DIM * HY * HX;  // [DIM][HY][32]
-  float* ring = xsum + DIM * HY * 32;  // [RD][DIM][256]
+  float* tile = sm3;                    // [DIM][HY][HXP]
+  float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
+  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
+  const int h = blockIdx.z / nz;
+  const int z = blockIdx.z - h * nz;
+  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
+  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+  const float* plane = src + z * nxy;
+  for (int row = ty; row < DIM * HY; row += 8) {
+    const int c = row / HY, hy = row - c * HY;
+    const int gy = min(max(y0 - R + hy, 0), ny - 1);
+    const float* line = plane + c * N + gy * nx;
+    float* trow = tile + row * HXP;
+#pragma unroll
+    for (int hx = tx; hx < HX; hx += 32) trow[hx] = __ldg(line + min(max(x0 - R + hx, 0), nx - 1));
+  }
+  __syncthreads();
+  for (int it = tid; it < DIM * HY * 8; it += 256) {
+    const int row = it >> 3, q = it & 7;
+    const float4* t4 = reinterpret_cast<const float4*>(tile + row * HXP) + q;
+    float w[4 * NQ];
+#pragma unroll
+    for (int m = 0; m < NQ; ++m) {
+      const float4 v = t4[m];
+      w[4 * m] = v.x;
+      w[4 * m + 1] = v.y;
+      w[4 * m + 2] = v.z;
+      w[4 * m + 3] = v.w;
+    }
+    float o[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc = fmaf(a.k[0][j], w[i + j], acc);
+      o[i] = acc;
+    }
+    reinterpret_cast<float4*>(xsum + row * 32)[q] = make_float4(o[0], o[1], o[2], o[3]);
+  }
+  __syncthreads();
+  const int ox = x0 + tx, oy = y0 + ty;
+  const bool ok = ox < nx && oy < ny;
+  float y[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    const float* col = xsum + (c * HY + ty) * 32 + tx;
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc = fmaf(a.k[1][j], col[j * 32], acc);
+    y[c] = acc;
+  }
+  if (DIM == 3) {
+    if (ok) {
+      const int i = z * nxy + oy * nx + ox;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) dst[c * N + i] = y[c];
+    }
+    return;
+  }
+  // 2-D: SyN epilogue and max norm
+  float mx = 0.0f;
+  if (ok) {
+    const int i = oy * nx + ox;
+    const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+    const bool edge = a.epilogue && (ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1);
+    float nrm2 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      float r = y[c];
+      if (a.epilogue) {
+        if (edge) r = 0.0f;
+        else if (a.w2 != 0.0f) r = r * a.w1 + org[c * N + i] * a.w2;
+      }
+      const float q = r * a.ih[c];
+      nrm2 += q * q;
+      dst[c * N + i] = r;
+    }
+    mx = sqrtf(nrm2);
+  }
+  if (a.do_max) {
+    const float bm = block_max_f(mx, red);
+    if (tid == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
+  }
+}
+
+// z part (3-D): each thread owns one (x, y) column of one field over a chunk of slices and
+// keeps the last 2R+1 xy-smoothed values per component in registers; the z loop is unrolled
+// by 2R+1 so every ring index is a compile-time constant.  No shared memory, no barriers in
+// the loop.  Applies the SyN epilogue and reduces the max norm.
+template <int R>
+__global__ void __launch_bounds__(256) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  if (ctl != nullptr && ctl->stop) return;
+  constexpr int K = 2 * R + 1, RD = K;
+  __shared__ float red[32];
+  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
   const int nzc = gridDim.z / a.halves;
   const int h = blockIdx.z / nzc;
   const int zc = blockIdx.z - h * nzc;
   const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
   float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
   const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
-  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+  const int ox = blockIdx.x * 32 + (threadIdx.x & 31), oy = blockIdx.y * 8 + (threadIdx.x >> 5);
   const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
-  float kx[K], ky[K], kz[K];
-#pragma unroll
-  for (int j = 0; j < K; ++j) {
-    kx[j] = a.k[0][j];
-    ky[j] = a.k[1][j];
-    kz[j] = a.k[2][j];
-  }
-
-  // xy-smoothed slice clamp(s) -> ring slot of s (each thread writes its own column)
-  auto xy_slice = [&](int s) {
-    const int zs = min(max(s, 0), nz - 1);
-    const float* plane = src + zs * nxy;
-    for (int row = ty; row < DIM * HY; row += 8) {
-      const int c = row / HY, hy = row - c * HY;
-      const int gy = min(max(y0 - R + hy, 0), ny - 1);
-      const float* line = plane + c * N + gy * nx;
-      float* trow = tile + row * HX;
-#pragma unroll
-      for (int hx = tx; hx < HX; hx += 32) trow[hx] = __ldg(line + min(max(x0 - R + hx, 0), nx - 1));
-    }
-    __syncthreads();
-    for (int row = ty; row < DIM * HY; row += 8) {
-      const float* t = tile + row * HX + tx;
-      float acc = 0.0f;
-#pragma unroll
-      for (int j = 0; j < K; ++j) acc = fmaf(kx[j], t[j], acc);
-      xsum[row * 32 + tx] = acc;
-    }
-    __syncthreads();
-    const int slot = ((s % RD) + RD) % RD;
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      const float* col = xsum + (c * HY + ty) * 32 + tx;
-      float acc = 0.0f;
-#pragma unroll
-      for (int j = 0; j < K; ++j) acc = fmaf(ky[j], col[j * 32], acc);
-      ring[(slot * DIM + c) * 256 + tid] = acc;
-    }
-    __syncthreads();  // tile and xsum are reused by the next slice
-  };
-
-  for (int s = z0 - RZ; s < z0 + RZ; ++s) xy_slice(s);
-  const int ox = x0 + tx, oy = y0 + ty;
-  const bool ok = ox < nx && oy < ny;
   float mx = 0.0f;
-  for (int z = z0; z < z1; ++z) {
-    xy_slice(z + RZ);
-    if (ok) {
-      const int i = z * nxy + oy * nx + ox;
-      const bool edge = a.epilogue && (ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1 ||
-                                       (DIM == 3 && (z == 0 || z == nz - 1)));
-      const int base = (((z - RZ) % RD) + RD) % RD;
-      float nrm2 = 0.0f;
+  if (ox < nx && oy < ny) {
+    const float* col = src + oy * nx + ox;
+    float ring[3][RD];
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        float v;
-        if (DIM == 3) {
-          v = 0.0f;
+    for (int u = 0; u < 2 * R; ++u) {
+      const int zs = min(max(z0 - R + u, 0), nz - 1);
 #pragma unroll
-          for (int j = 0; j < K; ++j) {
-            int sl = base + j;
-            sl = sl >= RD ? sl - RD : sl;
-            v = fmaf(kz[j], ring[(sl * DIM + c) * 256 + tid], v);
+      for (int c = 0; c < 3; ++c) ring[c][u] = __ldg(col + c * N + zs * nxy);
+    }
+    const bool xyedge = ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1;
+    for (int zb = z0; zb < z1; zb += RD) {
+#pragma unroll
+      for (int u = 0; u < RD; ++u) {
+        const int z = zb + u;
+        if (z < z1) {
+          const int zs = min(z + R, nz - 1);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) ring[c][(u + 2 * R) % RD] = __ldg(col + c * N + zs * nxy);
+          const int i = z * nxy + oy * nx + ox;
+          const bool edge = a.epilogue && (xyedge || z == 0 || z == nz - 1);
+          float nrm2 = 0.0f;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int j = 0; j < K; ++j) acc = fmaf(a.k[2][j], ring[c][(u + j) % RD], acc);
+            if (a.epilogue) {
+              if (edge) acc = 0.0f;
+              else if (a.w2 != 0.0f) acc = acc * a.w1 + org[c * N + i] * a.w2;
+            }
+            const float q = acc * a.ih[c];
+            nrm2 += q * q;
+            dst[c * N + i] = acc;
           }
-        } else {
-          v = ring[c * 256 + tid];
+          mx = fmaxf(mx, sqrtf(nrm2));
         }
-        if (a.epilogue) {
-          if (edge) v = 0.0f;
-          else if (a.w2 != 0.0f) v = v * a.w1 + org[c * N + i] * a.w2;
-        }
-        if (a.do_max) {
-          const float q = v * a.ih[c];
-          nrm2 += q * q;
-        }
-        dst[c * N + i] = v;
       }
-      if (a.do_max) mx = fmaxf(mx, sqrtf(nrm2));
     }
   }
   if (a.do_max) {
     const float bm = block_max_f(mx, red);
-    if (tid == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
+    if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
   }
 }
 
@@ -395,16 +496,14 @@ static int smooth3_radius(int dim, const int R[3]) {
 
 bool smooth3_supported(int dim, const int R[3]) { return smooth3_radius(dim, R) <= kSmoothRMax; }
 
-template <int DIM, int R>
-static cudaError_t smooth3_attr() {
-  return cudaFuncSetAttribute(k_smooth3<DIM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(smooth3_smem_floats(DIM, R) * 4));
-}
-
 template <int R>
 static cudaError_t smooth3_attr_both() {
-  cudaError_t e = smooth3_attr<3, R>();
-  return e == cudaSuccess ? smooth3_attr<2, R>() : e;
+  cudaError_t e = cudaFuncSetAttribute(k_smooth_xy<3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(smooth3_smem_floats(3, R) * 4));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_smooth_xy<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(smooth3_smem_floats(2, R) * 4));
+  return e;
 }
 
 cudaError_t smooth3_prepare() {
@@ -424,16 +523,13 @@ cudaError_t smooth3_prepare() {
   return e;
 }
 
-void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, int halves,
-                         const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
-                         float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s) {
-  count_launch();
+void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
+                         int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
+                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s) {
   const int dim = g.d.dim;
   const int RR = smooth3_radius(dim, R);
   Smooth3Args a;
   memset(&a, 0, sizeof(a));
-  a.in = Ptr2c{{in[0], halves > 1 ? in[1] : in[0]}};
-  a.out = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
   a.orig = Ptr2c{{orig ? orig[0] : nullptr, orig ? (halves > 1 ? orig[1] : orig[0]) : nullptr}};
   for (int ax = 0; ax < 3; ++ax) {
     a.ih[ax] = (float)(1.0 / g.sp[ax]);
@@ -449,42 +545,69 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   a.w1 = w1;
   a.w2 = w2;
   const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
-  int zc = g.d.nz;
-  if (dim == 3) {
-    const int target = 148 * 6;
-    const int chunks = (target + gx * gy * halves - 1) / (gx * gy * halves);
-    zc = (g.d.nz + chunks - 1) / chunks;
-    zc = std::max(zc, std::max(4 * RR, 8));
-    zc = std::min(zc, g.d.nz);
-  }
-  a.ZC = zc;
-  const int nzc = (g.d.nz + zc - 1) / zc;
-  const dim3 grid(gx, gy, nzc * halves);
+  // xy pass: in -> (3-D: tmp, 2-D: out)
+  a.in = Ptr2c{{in[0], halves > 1 ? in[1] : in[0]}};
+  float* const* xyout = dim == 3 ? tmp : out;
+  a.out = Ptr2{{xyout[0], halves > 1 ? xyout[1] : xyout[0]}};
+  const dim3 gxy(gx, gy, g.d.nz * halves);
   const size_t smem = smooth3_smem_floats(dim, RR) * 4;
-#define SYNX_SM3(RV)                                          \
-  case RV:                                                    \
-    if (dim == 3)                                             \
-      k_smooth3<3, RV><<<grid, 256, smem, s>>>(a, g.d, ctl);  \
-    else                                                      \
-      k_smooth3<2, RV><<<grid, 256, smem, s>>>(a, g.d, ctl);  \
+  count_launch();
+#define SYNX_SXY(RV)                                             \
+  case RV:                                                       \
+    if (dim == 3)                                                \
+      k_smooth_xy<3, RV><<<gxy, 256, smem, s>>>(a, g.d, ctl);    \
+    else                                                         \
+      k_smooth_xy<2, RV><<<gxy, 256, smem, s>>>(a, g.d, ctl);    \
     break;
   switch (RR) {
-    SYNX_SM3(1)
-    SYNX_SM3(2)
-    SYNX_SM3(3)
-    SYNX_SM3(4)
-    SYNX_SM3(5)
-    SYNX_SM3(6)
-    SYNX_SM3(7)
-    SYNX_SM3(8)
-    SYNX_SM3(9)
-    SYNX_SM3(10)
-    SYNX_SM3(11)
-    SYNX_SM3(12)
+    SYNX_SXY(1)
+    SYNX_SXY(2)
+    SYNX_SXY(3)
+    SYNX_SXY(4)
+    SYNX_SXY(5)
+    SYNX_SXY(6)
+    SYNX_SXY(7)
+    SYNX_SXY(8)
+    SYNX_SXY(9)
+    SYNX_SXY(10)
+    SYNX_SXY(11)
+    SYNX_SXY(12)
     default:
       break;
   }
-#undef SYNX_SM3
+#undef SYNX_SXY
+  if (dim != 3) return;
+  // z pass: tmp -> out with the epilogue
+  a.in = Ptr2c{{tmp[0], halves > 1 ? tmp[1] : tmp[0]}};
+  a.out = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
+  const int target = 148 * 8;
+  const int chunks = std::max(1, (target + gx * gy * halves - 1) / (gx * gy * halves));
+  int zc = (g.d.nz + chunks - 1) / chunks;
+  zc = std::min(std::max(zc, 2 * RR + 1), g.d.nz);
+  a.ZC = zc;
+  const dim3 gz(gx, gy, ((g.d.nz + zc - 1) / zc) * halves);
+  count_launch();
+#define SYNX_SZ(RV)                                    \
+  case RV:                                             \
+    k_smooth_z<RV><<<gz, 256, 0, s>>>(a, g.d, ctl);    \
+    break;
+  switch (RR) {
+    SYNX_SZ(1)
+    SYNX_SZ(2)
+    SYNX_SZ(3)
+    SYNX_SZ(4)
+    SYNX_SZ(5)
+    SYNX_SZ(6)
+    SYNX_SZ(7)
+    SYNX_SZ(8)
+    SYNX_SZ(9)
+    SYNX_SZ(10)
+    SYNX_SZ(11)
+    SYNX_SZ(12)
+    default:
+      break;
+  }
+#undef SYNX_SZ
 }
 
 // Single-axis fallback for kernels too wide for the fused pass.
@@ -496,9 +619,9 @@ __global__ void __launch_bounds__(256)
   __shared__ float red[32];
   const Coord3 c3 = coord3(d, zb, gridDim.z / ((d.nz + zb - 1) / zb));
   const int h = c3.h;
-  const float* __restrict__ src = in.p[h];
-  float* __restrict__ dst = out.p[h];
-  const float* __restrict__ org = orig.p[h];
+  const float* __restrict__ src = (h ? in.p[1] : in.p[0]);
+  float* __restrict__ dst = (h ? out.p[1] : out.p[0]);
+  const float* __restrict__ org = (h ? orig.p[1] : orig.p[0]);
   const int N = (int)d.N, nxy = d.nx * d.ny;
   const int len = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
   const int astride = axis == 0 ? 1 : (axis == 1 ? d.nx : nxy);
@@ -559,16 +682,16 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
 // Composition out = w + s * d(x + w), s = eta / max||d/spacing|| (SyN's update scaling fused).
 // Reads w only at its own voxel, so it runs in place (out == w).
 // ------------------------------------------------------------------------------------------
-template <int DIM>
+template <int DIM, bool DIAG>
 __global__ void __launch_bounds__(256) k_compose(Ptr2c dd, Ptr2c ww, Ptr2 oo, Dims d, int zb, int halves, Affine m,
                                                  double eta, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
   const Coord3 c3 = coord3(d, zb, halves);
   if (!c3.ok) return;
   const int h = c3.h;
-  const float* __restrict__ D = dd.p[h];
-  const float* W = ww.p[h];
-  float* O = oo.p[h];
+  const float* __restrict__ D = (h ? dd.p[1] : dd.p[0]);
+  const float* W = (h ? ww.p[1] : ww.p[0]);
+  float* O = (h ? oo.p[1] : oo.p[0]);
   float scale = 1.0f;
   if (eta > 0.0) {
     const float mx = __uint_as_float(ctl->maxnorm[h]);
@@ -576,11 +699,23 @@ __global__ void __launch_bounds__(256) k_compose(Ptr2c dd, Ptr2c ww, Ptr2 oo, Di
   }
   const int N = (int)d.N, nxy = d.nx * d.ny;
   const float fx = (float)c3.x, fy = (float)c3.y;
+  const int i0 = c3.z0 * nxy + c3.y * d.nx + c3.x;
+  float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+  if (c3.z0 < c3.z1) {
+    n0 = W[i0];
+    n1 = W[N + i0];
+    n2 = DIM == 3 ? W[2 * N + i0] : 0.0f;
+  }
   for (int z = c3.z0; z < c3.z1; ++z) {
     const int i = z * nxy + c3.y * d.nx + c3.x;
-    const float w0 = W[i], w1 = W[N + i], w2 = DIM == 3 ? W[2 * N + i] : 0.0f;
+    const float w0 = n0, w1 = n1, w2 = n2;
+    if (z + 1 < c3.z1) {  // next slice's warp vector, loaded ahead of this slice's gathers
+      n0 = W[i + nxy];
+      n1 = W[N + i + nxy];
+      n2 = DIM == 3 ? W[2 * N + i + nxy] : 0.0f;
+    }
     float cx, cy, cz;
-    map_point<DIM>(m, fx, fy, (float)z, w0, w1, w2, cx, cy, cz);
+    map_point<DIM, DIAG>(m, fx, fy, (float)z, w0, w1, w2, cx, cy, cz);
     if (inside_buffer<DIM>(d, cx, cy, cz)) {
       const Cell c = make_cell<DIM>(d, cx, cy, cz);
       O[i] = fmaf(scale, lerp_at<DIM>(D, c), w0);
@@ -602,10 +737,18 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
   Ptr2 po{{out[0], halves > 1 ? out[1] : out[0]}};
   Affine a = make_affine(g, g);
   const Map3 m = map3(g.d, halves);
-  if (g.d.dim == 3)
-    k_compose<3><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
-  else
-    k_compose<2><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+  const bool dg = affine_diag(a);
+  if (g.d.dim == 3) {
+    if (dg)
+      k_compose<3, true><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+    else
+      k_compose<3, false><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+  } else {
+    if (dg)
+      k_compose<2, true><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+    else
+      k_compose<2, false><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -622,10 +765,15 @@ struct InvParams {
   double mean_tol, max_tol;
 };
 
-template <int DIM>
+template <int DIM, bool DIAG>
 __device__ __forceinline__ void residual(const float* __restrict__ phi, const Dims& d, const float* A, float fx,
                                          float fy, float fz, const float p[3], float e[3]) {
   float cx, cy, cz;
+  if (DIAG) {
+    cx = fmaf(A[0], p[0], fx);
+    cy = fmaf(A[4], p[1], fy);
+    cz = DIM == 3 ? fmaf(A[8], p[2], fz) : 0.0f;
+  } else {
   cx = fx + A[0] * p[0] + A[1] * p[1];
   cy = fy + A[3] * p[0] + A[4] * p[1];
   cz = 0.0f;
@@ -633,6 +781,7 @@ __device__ __forceinline__ void residual(const float* __restrict__ phi, const Di
     cx += A[2] * p[2];
     cy += A[5] * p[2];
     cz = fz + A[6] * p[0] + A[7] * p[1] + A[8] * p[2];
+  }
   }
   e[0] = p[0];
   e[1] = p[1];
@@ -646,8 +795,8 @@ __device__ __forceinline__ void residual(const float* __restrict__ phi, const Di
   }
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims d, InvParams P, IterCtl* ctl,
+template <int DIM, bool DIAG>
+__global__ void __launch_bounds__(256, 4) k_invert_step(Ptr2c phis, Ptr2 psis, Dims d, InvParams P, IterCtl* ctl,
                                                      double* __restrict__ psum, float* __restrict__ pmax, int pcap) {
   if (P.stop_aware && ctl->stop) return;
   __shared__ double redd[32];
@@ -656,8 +805,8 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
   const Coord3 c3 = coord3(d, P.zb, P.halves);
   const int h = c3.h;
   InvCtl& C = ctl->inv[P.phase][h];
-  const float* __restrict__ phi = phis.p[h];
-  float* __restrict__ psi = psis.p[h];
+  const float* __restrict__ phi = (h ? phis.p[1] : phis.p[0]);
+  float* __restrict__ psi = (h ? psis.p[1] : psis.p[0]);
   const int k = P.k;
   bool apply = false, stats = true;
   float eps = 0.0f, lim = 0.0f;
@@ -685,16 +834,27 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
   if (c3.ok) {
     const float fx = (float)c3.x, fy = (float)c3.y;
     const bool xyedge = c3.x == 0 || c3.x == d.nx - 1 || c3.y == 0 || c3.y == d.ny - 1;
+    // the iterate of the next slice is loaded before this slice's gathers (one dependent
+    // memory round trip per slice instead of two)
+    const int i0 = c3.z0 * nxy + c3.y * d.nx + c3.x;
+    float pn[3] = {0.0f, 0.0f, 0.0f};
+    if (c3.z0 < c3.z1) {
+      pn[0] = psi[i0];
+      pn[1] = psi[N + i0];
+      pn[2] = DIM == 3 ? psi[2 * N + i0] : 0.0f;
+    }
     for (int z = c3.z0; z < c3.z1; ++z) {
       const int i = z * nxy + c3.y * d.nx + c3.x;
       const float fz = (float)z;
-      float p[3];
-      p[0] = psi[i];
-      p[1] = psi[N + i];
-      p[2] = DIM == 3 ? psi[2 * N + i] : 0.0f;
+      float p[3] = {pn[0], pn[1], pn[2]};
+      if (z + 1 < c3.z1) {
+        pn[0] = psi[i + nxy];
+        pn[1] = psi[N + i + nxy];
+        pn[2] = DIM == 3 ? psi[2 * N + i + nxy] : 0.0f;
+      }
       float e[3];
       if (apply) {
-        residual<DIM>(phi, d, P.A, fx, fy, fz, p, e);
+        residual<DIM, DIAG>(phi, d, P.A, fx, fy, fz, p, e);
         float s2 = 0.0f;
 #pragma unroll
         for (int c = 0; c < DIM; ++c) {
@@ -711,7 +871,7 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
         if (DIM == 3) psi[2 * N + i] = p[2];
       }
       if (stats) {
-        residual<DIM>(phi, d, P.A, fx, fy, fz, p, e);
+        residual<DIM, DIAG>(phi, d, P.A, fx, fy, fz, p, e);
         float s2 = 0.0f;
 #pragma unroll
         for (int c = 0; c < DIM; ++c) {
@@ -757,7 +917,8 @@ __global__ void __launch_bounds__(256) k_invert_step(Ptr2c phis, Ptr2 psis, Dims
   }
 }
 
-int inv_blocks(const GridInfo& g) { return map3(g.d, 2).nblocks; }
+constexpr int kInvTarget = 148 * 24;  // blocks: short per-thread z walks, small last-wave tail
+int inv_blocks(const GridInfo& g) { return map3(g.d, 2, kInvTarget).nblocks; }
 
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
@@ -771,7 +932,7 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
   for (int j = 0; j < 3; ++j) P.ih[j] = (float)(1.0 / g.sp[j]);
   // the block decomposition is the same for one or two halves, so the partial buffers sized
   // by inv_blocks() fit either
-  const Map3 m2 = map3(g.d, 2);
+  const Map3 m2 = map3(g.d, 2, kInvTarget);
   Map3 m = m2;
   m.grid.z = (m2.grid.z / 2) * halves;
   P.k = k;
@@ -782,10 +943,18 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
   P.halves = halves;
   P.mean_tol = mean_tol;
   P.max_tol = max_tol;
-  if (g.d.dim == 3)
-    k_invert_step<3><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
-  else
-    k_invert_step<2><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+  const bool dg = affine_diag(a);
+  if (g.d.dim == 3) {
+    if (dg)
+      k_invert_step<3, true><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+    else
+      k_invert_step<3, false><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+  } else {
+    if (dg)
+      k_invert_step<2, true><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+    else
+      k_invert_step<2, false><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+  }
 }
 
 // ------------------------------------------------------------------------------------------

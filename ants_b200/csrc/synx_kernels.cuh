@@ -75,15 +75,16 @@ cudaError_t cc_prepare(int dim, int radius);
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
                IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr);
 
-// Gaussian smoothing of `halves` fields along every axis in one z-marching pass (host kernels
-// khost[a] of radius R[a] per axis, passed by value in the launch parameters).  `epilogue`
-// applies SyN's boundary zeroing and the blend with `orig` (w2 != 0); `maxnorm` reduces
-// max ||u/spacing|| into ctl->maxnorm[h].  Supported for radii up to 12.
+// Gaussian smoothing of `halves` fields along every axis: an xy-tile kernel and, in 3-D, a
+// z-column kernel (host kernels khost[a] of radius R[a] per axis, passed by value in the
+// launch parameters).  `epilogue` applies SyN's boundary zeroing and the blend with `orig`
+// (w2 != 0); `maxnorm` reduces max ||u/spacing|| into ctl->maxnorm[h].  Radii up to 12.
 bool smooth3_supported(int dim, const int R[3]);
 cudaError_t smooth3_prepare();
-void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, int halves,
-                         const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
-                         float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s);
+// In 3-D the xy pass writes `tmp` (same shape as `out`), which the z pass reads.
+void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
+                         int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
+                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s);
 
 // Separable smoothing of `halves` fields (each dim components) along one axis.
 // `last` applies the SyN epilogue: zero boundary, blend with `orig` (w2 != 0), and the max
