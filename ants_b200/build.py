@@ -26,7 +26,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 LIB = os.path.join(HERE, "libsynx.so")
 CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
 
-LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_ctx.cu"]
+LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_ctx.cu", "synx_noalloc.cu"]
 LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
 CLI_HEADERS = ["nifti_io.h", "ants_registration.h"]

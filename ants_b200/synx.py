@@ -155,6 +155,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_smooth_image": (I, [V, V, P(SynxGeom), D, I, V]),
         "synx_warp_image": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
         "synx_cc_metric": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
+        "synx_cc_metric_noalloc": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
+        "synx_noalloc_last_error": (C.c_char_p, []),
         "synx_smooth_field": (I, [V, V, P(SynxGeom), D, P(D), V]),
         "synx_compose": (I, [V, V, P(SynxGeom), F, V, V]),
         "synx_invert_field": (I, [V, V, P(SynxGeom), I, D, D, P(I), V]),
@@ -417,6 +419,20 @@ def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
     v = C.c_double()
     _check(load_library().synx_cc_metric(_ptr(F), _ptr(M), C.byref(gc), radius, _ptr(gF), _ptr(gM), C.byref(v),
                                          _stream(stream)))
+    return v.value
+
+
+def cc_metric_noalloc(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
+    """cc_metric without any device allocation: the kernel's scratch is a fixed device array
+    inside libsynx (for callers that cannot allocate, e.g. inside graph capture).  Calls on one
+    device share that array, so calls that overlap on the GPU race."""
+    lib = load_library()
+    gc = g.to_c()
+    v = C.c_double()
+    rc = lib.synx_cc_metric_noalloc(_ptr(F), _ptr(M), C.byref(gc), radius, _ptr(gF), _ptr(gM), C.byref(v),
+                                    _stream(stream))
+    if rc != 0:
+        raise SynxError(f"synx error {rc} ({ERRORS.get(rc, '?')}): {lib.synx_noalloc_last_error().decode()}")
     return v.value
 
 

@@ -174,6 +174,21 @@ int synx_warp_image(const float* img_dev, const synx_geom* img_geom, const float
 int synx_cc_metric(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
                    float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
 
+/* Same computation as synx_cc_metric, for callers that cannot allocate device memory (a
+ * pipeline being captured into a CUDA graph, a host whose device memory is owned by another
+ * allocator, a loop that must not stall on an allocation).  No counterpart in the reference.
+ * It calls no cudaMalloc/cudaFree: the kernel's scratch (control block and per-block partial
+ * sums, about 260 KB) is a fixed array in device memory that each GPU using the library holds
+ * until the process exits.  Limit: grids needing more than 32768 CC blocks (for example more
+ * than 8192 x 1024 voxels per slice) are rejected with SYNX_E_ARG.  The first call on a device
+ * looks the array's device address up (make it before any stream capture).  All calls on a
+ * device share the array: calls that overlap on the GPU (other streams, other host threads)
+ * race.  value_host may be NULL; otherwise the call waits for its stream to read the value.
+ * Errors are reported by synx_noalloc_last_error(). */
+int synx_cc_metric_noalloc(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
+                           float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
+const char* synx_noalloc_last_error(void);
+
 /* Gaussian smoothing of a displacement field as SyN does it (Examples/SmoothDisplacementField
  * .cxx:70-125 twin).  If max_norm_host is not NULL, also returns max ||u/spacing||. */
 int synx_smooth_field(const float* in_dev, float* out_dev, const synx_geom* g, double variance,

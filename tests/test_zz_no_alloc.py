@@ -1,0 +1,59 @@
+"""The allocation-free CC entry point (synx_cc_metric_noalloc).
+
+It exists for callers that cannot allocate device memory -- a pipeline being captured into a CUDA
+graph, a host whose GPU memory belongs to another allocator, a loop that must not stall on an
+allocation -- and keeps the kernel's scratch in a fixed array inside libsynx instead.  The GPU test
+calls it twice in a row through the C ABI and checks each result against synx_cc_metric on the same
+inputs, with the tolerances of the CC parity tests; this file is collected last so that a run which
+stops at the first failure has already run every other test.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from ants_b200 import synx
+from ants_b200.synx import Geom
+
+
+def test_noalloc_rejects_grids_beyond_its_scratch():
+    # 8192 x 1040 voxels per slice needs more CC blocks than the fixed scratch holds; the check runs
+    # on the host before any device work, so this needs no GPU
+    lib = synx.load_library()
+    g = Geom((8192, 1040, 1)).to_c()
+    v = C.c_double()
+    dummy = C.c_void_p(256)
+    rc = lib.synx_cc_metric_noalloc(dummy, dummy, C.byref(g), 2, dummy, dummy, C.byref(v), None)
+    assert rc == -1
+    msg = lib.synx_noalloc_last_error().decode()
+    assert "at most 32768" in msg
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_allocating_entry_point_twice(cuda):
+    import torch
+
+    cases = [
+        (Geom((37, 29, 23), (1.0, 1.2, 0.9)), 4, 11),
+        (Geom((61, 47), (1.0, 1.0)), 2, 12),
+    ]
+    for g, radius, seed in cases:
+        rng = np.random.default_rng(seed)
+        F = rng.uniform(0, 1, g.shape).astype(np.float32)
+        M = (0.6 * np.roll(F, 1, axis=-1) + 0.1 * rng.standard_normal(g.shape)).astype(np.float32)
+        Fd = torch.from_numpy(F).to(cuda)
+        Md = torch.from_numpy(M).to(cuda)
+        shape = (g.dim,) + g.shape
+        ref_f = torch.empty(shape, device=cuda)
+        ref_m = torch.empty(shape, device=cuda)
+        v_ref = synx.cc_metric(Fd, Md, g, radius, ref_f, ref_m)
+        for _ in range(2):  # the second call reuses the scratch left by the first
+            out_f = torch.full(shape, float("nan"), device=cuda)
+            out_m = torch.full(shape, float("nan"), device=cuda)
+            v = synx.cc_metric_noalloc(Fd, Md, g, radius, out_f, out_m)
+            torch.cuda.synchronize()
+            assert abs(v - v_ref) < 1e-9
+            for a, b in ((out_f, ref_f), (out_m, ref_m)):
+                a, b = a.cpu().numpy(), b.cpu().numpy()
+                scale = max(np.abs(b).max(), 1e-20)
+                np.testing.assert_allclose(a, b, atol=1e-6 * scale, rtol=1e-5)
