@@ -74,7 +74,8 @@ def build_cli(force: bool = False) -> str | None:
     if not force and not _stale(CLI, deps):
         return CLI
     cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", "/usr/local/cuda/include", "-o", CLI,
-           *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN", "-lz"]
+           *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN", "-L", "/usr/local/cuda/lib64", "-lcudart",
+           "-Wl,-rpath,/usr/local/cuda/lib64", "-lz"]
     _run(cmd)
     return CLI
 

@@ -1,0 +1,351 @@
+// antsRegistration-compatible command line for a single SyN + CC stage, on the synx C ABI.
+//
+// Accepted options (the reference's syntax, Examples/antsRegistration.cxx:30-548, parsed as in
+// Examples/antsRegistrationTemplateHeader.h:545-651, :801-815, :1081-1087):
+//   -d/--dimensionality 2|3        --float 0|1 (computation is float32 either way)
+//   -m/--metric CC[fixed,moving,weight,radius]
+//   -t/--transform SyN[gradientStep,updateFieldVariance,totalFieldVariance]
+//   -c/--convergence [NxNx...,threshold,window] or NxNx...
+//   -f/--shrink-factors NxNx...     -s/--smoothing-sigmas NxNx...[vox|mm]
+//   -o/--output prefix | [prefix,warpedImage,inverseWarpedImage]
+//   -w/--winsorize-image-intensities [lower,upper]   -u/--use-histogram-matching 0
+//   -v/--verbose 0|1   --random-seed N (accepted, no effect: the stage is deterministic)
+//   --gpu N (device index; not a reference option)
+// Output: prefix0Warp.nii.gz and prefix0InverseWarp.nii.gz (antsRegistrationTemplateHeader.cxx:74-90
+// names for SyN), plus the warped images when requested.  Other stages, metrics, masks and
+// initial transforms are rejected with EXIT_FAILURE.
+#include "ants_registration.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nifti_io.h"
+#include "synx.h"
+
+namespace ants_b200 {
+namespace {
+
+struct OptionCall {
+  std::string name;                 // text before '[' (or the whole value)
+  std::vector<std::string> params;  // comma-separated parameters inside [...]
+};
+
+// name[p0,p1,...] -> {name, params}; "[a,b]" -> {"", {a, b}}
+OptionCall parse_call(const std::string& v) {
+  OptionCall c;
+  const size_t lb = v.find('[');
+  if (lb == std::string::npos) {
+    c.name = v;
+    return c;
+  }
+  const size_t rb = v.rfind(']');
+  if (rb == std::string::npos || rb < lb) throw std::runtime_error("unbalanced brackets in '" + v + "'");
+  c.name = v.substr(0, lb);
+  std::string inner = v.substr(lb + 1, rb - lb - 1);
+  std::stringstream ss(inner);
+  std::string item;
+  while (std::getline(ss, item, ',')) c.params.push_back(item);
+  return c;
+}
+
+template <class T>
+std::vector<T> parse_x_vector(const std::string& s) {
+  std::vector<T> out;
+  std::stringstream ss(s);
+  std::string item;
+  while (std::getline(ss, item, 'x')) {
+    if (item.empty()) continue;
+    std::stringstream is(item);
+    T v;
+    is >> v;
+    if (is.fail()) throw std::runtime_error("cannot parse '" + s + "' as an x-separated vector");
+    out.push_back(v);
+  }
+  return out;
+}
+
+std::string lower(std::string s) {
+  std::transform(s.begin(), s.end(), s.begin(), ::tolower);
+  return s;
+}
+
+synx_geom to_geom(const nifti::Image& im, int dim) {
+  synx_geom g;
+  std::memset(&g, 0, sizeof(g));
+  g.dim = dim;
+  for (int k = 0; k < 3; ++k) {
+    g.size[k] = k < dim ? im.size[k] : 1;
+    g.spacing[k] = k < dim ? im.spacing[k] : 1.0;
+    g.origin[k] = k < dim ? im.origin[k] : 0.0;
+  }
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      g.direction[r * 3 + c] = (r < dim && c < dim) ? im.direction[r * 3 + c] : (r == c ? 1.0 : 0.0);
+  return g;
+}
+
+nifti::Image field_image(const synx_geom& g, const std::vector<float>& interleaved) {
+  nifti::Image im;
+  im.dim = g.dim;
+  im.components = g.dim;
+  for (int k = 0; k < 3; ++k) {
+    im.size[k] = g.size[k];
+    im.spacing[k] = g.spacing[k];
+    im.origin[k] = g.origin[k];
+  }
+  for (int k = 0; k < 9; ++k) im.direction[k] = g.direction[k];
+  const long long N = im.voxels();
+  im.data.resize((size_t)N * g.dim);
+  for (long long i = 0; i < N; ++i)
+    for (int c = 0; c < g.dim; ++c) im.data[(size_t)c * N + i] = interleaved[(size_t)i * g.dim + c];
+  return im;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// out(x) = img(x + u(x)) on grid `grid` (u interleaved on that grid), through synx_warp_image.
+std::vector<float> warp_on_device(const nifti::Image& img, const synx_geom& gimg, const std::vector<float>& u_inter,
+                                  const synx_geom& grid) {
+  const long long Ni = img.voxels(), No = grid.size[0] * grid.size[1] * grid.size[2];
+  const int D = grid.dim;
+  std::vector<float> planes((size_t)No * D);
+  for (long long i = 0; i < No; ++i)
+    for (int c = 0; c < D; ++c) planes[(size_t)c * No + i] = u_inter[(size_t)i * D + c];
+  float *di = nullptr, *du = nullptr, *dout = nullptr;
+  CK(cudaMalloc(&di, 4 * Ni));
+  CK(cudaMalloc(&du, 4 * No * D));
+  CK(cudaMalloc(&dout, 4 * No));
+  CK(cudaMemcpy(di, img.data.data(), 4 * Ni, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(du, planes.data(), 4 * No * D, cudaMemcpyHostToDevice));
+  int rc = synx_warp_image(di, &gimg, du, &grid, dout, nullptr);
+  std::vector<float> out((size_t)No);
+  if (rc == 0) CK(cudaMemcpy(out.data(), dout, 4 * No, cudaMemcpyDeviceToHost));
+  cudaFree(di);
+  cudaFree(du);
+  cudaFree(dout);
+  if (rc) throw std::runtime_error(std::string("synx_warp_image: ") + synx_last_error(nullptr));
+  return out;
+}
+
+// u (interleaved, on grid a) resampled onto grid b, through synx_resample_field.
+std::vector<float> resample_on_device(const std::vector<float>& u_inter, const synx_geom& a, const synx_geom& b) {
+  const int D = a.dim;
+  const long long Na = a.size[0] * a.size[1] * a.size[2], Nb = b.size[0] * b.size[1] * b.size[2];
+  std::vector<float> planes((size_t)Na * D), out_planes((size_t)Nb * D), out((size_t)Nb * D);
+  for (long long i = 0; i < Na; ++i)
+    for (int c = 0; c < D; ++c) planes[(size_t)c * Na + i] = u_inter[(size_t)i * D + c];
+  float *din = nullptr, *dout = nullptr;
+  CK(cudaMalloc(&din, 4 * Na * D));
+  CK(cudaMalloc(&dout, 4 * Nb * D));
+  CK(cudaMemcpy(din, planes.data(), 4 * Na * D, cudaMemcpyHostToDevice));
+  int rc = synx_resample_field(din, &a, dout, &b, nullptr);
+  if (rc == 0) CK(cudaMemcpy(out_planes.data(), dout, 4 * Nb * D, cudaMemcpyDeviceToHost));
+  cudaFree(din);
+  cudaFree(dout);
+  if (rc) throw std::runtime_error(std::string("synx_resample_field: ") + synx_last_error(nullptr));
+  for (long long i = 0; i < Nb; ++i)
+    for (int c = 0; c < D; ++c) out[(size_t)i * D + c] = out_planes[(size_t)c * Nb + i];
+  return out;
+}
+
+nifti::Image like(const nifti::Image& geom_src, std::vector<float> data) {
+  nifti::Image im = geom_src;
+  im.components = 1;
+  im.data = std::move(data);
+  return im;
+}
+
+int run(const std::vector<std::string>& args, std::ostream& out) {
+  std::map<std::string, std::vector<std::string>> opt;  // long name -> values in order
+  const std::map<std::string, std::string> alias = {
+      {"-d", "dimensionality"}, {"-m", "metric"}, {"-t", "transform"}, {"-c", "convergence"},
+      {"-f", "shrink-factors"}, {"-s", "smoothing-sigmas"}, {"-o", "output"}, {"-v", "verbose"},
+      {"-w", "winsorize-image-intensities"}, {"-u", "use-histogram-matching"}, {"-x", "masks"},
+      {"-r", "initial-moving-transform"}, {"-q", "initial-fixed-transform"}, {"-n", "interpolation"},
+      {"-a", "collapse-output-transforms"}, {"-z", "collapse-output-transforms"}, {"-h", "help"}};
+  for (size_t i = 0; i < args.size(); ++i) {
+    std::string k = args[i];
+    std::string name;
+    if (k.rfind("--", 0) == 0) name = k.substr(2);
+    else if (alias.count(k)) name = alias.at(k);
+    else throw std::runtime_error("unexpected argument '" + k + "'");
+    if (name == "help") {
+      out << "antsRegistrationSyN_b200: antsRegistration options for one SyN + CC stage on a B200\n";
+      return EXIT_SUCCESS;
+    }
+    if (i + 1 >= args.size()) throw std::runtime_error("option --" + name + " needs a value");
+    opt[name].push_back(args[++i]);
+  }
+  auto one = [&](const std::string& n, const std::string& def) -> std::string {
+    auto it = opt.find(n);
+    return it == opt.end() ? def : it->second.back();
+  };
+  for (const char* bad : {"masks", "initial-moving-transform", "initial-fixed-transform", "restore-state",
+                          "save-state", "write-composite-transform", "restrict-deformation"})
+    if (opt.count(bad) && !(std::string(bad) == "masks" && opt[bad].back() == "[NULL,NULL]"))
+      throw std::runtime_error(std::string("option --") + bad + " is not supported by this SyN+CC stage");
+  if (opt.count("use-histogram-matching") && (one("use-histogram-matching", "0") == "1" ||
+                                              lower(one("use-histogram-matching", "0")) == "true"))
+    throw std::runtime_error("--use-histogram-matching 1 is not supported");
+  if (opt.count("interpolation") && lower(one("interpolation", "Linear")) != "linear")
+    throw std::runtime_error("only Linear interpolation is supported for the warped outputs");
+
+  const int dim = std::atoi(one("dimensionality", "3").c_str());
+  if (dim != 2 && dim != 3) throw std::runtime_error("--dimensionality must be 2 or 3");
+  const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
+  const int gpu = std::atoi(one("gpu", "0").c_str());
+  if (opt["transform"].size() != 1 || opt["metric"].size() != 1)
+    throw std::runtime_error("exactly one stage (one --transform and one --metric) is supported");
+  OptionCall t = parse_call(opt["transform"][0]);
+  if (lower(t.name) != "syn") throw std::runtime_error("only the SyN transform is supported, got '" + t.name + "'");
+  OptionCall m = parse_call(opt["metric"][0]);
+  if (lower(m.name) != "cc") throw std::runtime_error("only the CC metric is supported, got '" + m.name + "'");
+  if (m.params.size() < 2) throw std::runtime_error("CC[fixed,moving,weight,radius] needs the two images");
+
+  synx_params p;
+  synx_params_default(&p, dim);
+  if (t.params.empty()) throw std::runtime_error("SyN[gradientStep,...] needs a gradient step");
+  p.learning_rate = std::atof(t.params[0].c_str());
+  if (t.params.size() > 1) p.update_variance = std::atof(t.params[1].c_str());
+  if (t.params.size() > 2) p.total_variance = std::atof(t.params[2].c_str());
+  if (m.params.size() > 3) p.cc_radius = std::atoi(m.params[3].c_str());
+  // -c [iterations,threshold,window]
+  OptionCall c = parse_call(one("convergence", ""));
+  std::vector<int> iters;
+  if (!c.params.empty()) {
+    iters = parse_x_vector<int>(c.params[0]);
+    if (c.params.size() > 1) p.convergence_threshold = std::atof(c.params[1].c_str());
+    if (c.params.size() > 2) p.convergence_window = std::atoi(c.params[2].c_str());
+  } else if (!c.name.empty()) {
+    iters = parse_x_vector<int>(c.name);
+  }
+  if (iters.empty()) throw std::runtime_error("no convergence criteria (-c) were given");
+  const int L = (int)iters.size();
+  if (L > SYNX_MAX_LEVELS) throw std::runtime_error("at most 8 levels are supported");
+  std::vector<int> shrink = parse_x_vector<int>(one("shrink-factors", ""));
+  std::string sig = one("smoothing-sigmas", "");
+  if (sig.find("mm") != std::string::npos) {
+    p.sigmas_in_mm = 1;
+    sig.replace(sig.find("mm"), 2, "");
+  } else if (sig.find("vox") != std::string::npos) {
+    sig.replace(sig.find("vox"), 3, "");
+  }
+  std::vector<double> sigmas = parse_x_vector<double>(sig);
+  if (sigmas.size() == 1) sigmas.resize(L, sigmas[0]);
+  if ((int)shrink.size() != L || (int)sigmas.size() != L)
+    throw std::runtime_error("the number of shrink factors and smoothing sigmas must match the levels of -c");
+  p.n_levels = L;
+  for (int l = 0; l < L; ++l) {
+    p.iterations[l] = iters[l];
+    p.shrink_factors[l] = shrink[l];
+    p.smoothing_sigmas[l] = sigmas[l];
+  }
+  if (opt.count("winsorize-image-intensities")) {
+    OptionCall w = parse_call(one("winsorize-image-intensities", ""));
+    if (w.params.size() > 0) p.winsor_lower = (float)std::atof(w.params[0].c_str());
+    if (w.params.size() > 1) p.winsor_upper = (float)std::atof(w.params[1].c_str());
+  }
+  OptionCall o = parse_call(one("output", ""));
+  std::string prefix = o.params.empty() ? o.name : o.params[0];
+  if (prefix.empty()) throw std::runtime_error("no output prefix (-o) was given");
+  const std::string warped = o.params.size() > 1 ? o.params[1] : "";
+  const std::string inv_warped = o.params.size() > 2 ? o.params[2] : "";
+
+  nifti::Image fixed = nifti::read(m.params[0]);
+  nifti::Image moving = nifti::read(m.params[1]);
+  if (fixed.components != 1 || moving.components != 1) throw std::runtime_error("scalar images expected");
+  synx_geom gf = to_geom(fixed, dim), gm = to_geom(moving, dim);
+  if (verbose) {
+    out << "  Stage 0: SyN[" << p.learning_rate << "," << p.update_variance << "," << p.total_variance
+        << "], CC[radius " << p.cc_radius << "], " << L << " levels on GPU " << gpu << std::endl;
+  }
+  synx_ctx* ctx = nullptr;
+  if (synx_create(&p, gpu, nullptr, &ctx) != 0) throw std::runtime_error(std::string("synx_create: ") + synx_last_error(nullptr));
+  struct Guard {
+    synx_ctx* c;
+    ~Guard() { synx_destroy(c); }
+  } guard{ctx};
+  auto t0 = std::chrono::steady_clock::now();
+  if (synx_set_images(ctx, fixed.data.data(), &gf, moving.data.data(), &gm) != 0)
+    throw std::runtime_error(std::string("synx_set_images: ") + synx_last_error(ctx));
+  int64_t printed = 0;
+  for (int l = 0; l < L; ++l) {
+    auto tl = std::chrono::steady_clock::now();
+    if (synx_run_level(ctx, l) != 0) throw std::runtime_error(std::string("synx_run_level: ") + synx_last_error(ctx));
+    const double level_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl).count();
+    if (verbose) {
+      int64_t n = 0;
+      synx_get_log(ctx, nullptr, nullptr, nullptr, nullptr, nullptr, 0, &n);
+      std::vector<int32_t> lv(n), it(n), ki(n);
+      std::vector<double> me(n), cv(n);
+      synx_get_log(ctx, lv.data(), it.data(), me.data(), cv.data(), ki.data(), n, &n);
+      const double t_level0 = std::chrono::duration<double>(tl - t0).count();
+      const int64_t k_level = n - printed;
+      out << "  Current level = " << l + 1 << " of " << L << "\n    number of iterations = " << iters[l]
+          << "\n    shrink factors = " << shrink[l] << "\n    smoothing sigmas = " << sigmas[l]
+          << (p.sigmas_in_mm ? " mm" : " vox") << "\n";
+      out << "XXDIAGNOSTIC,Iteration,metricValue,convergenceValue,ITERATION_TIME_INDEX,SINCE_LAST\n";
+      for (int64_t k = printed; k < n; ++k) {
+        const double dt = level_s / std::max<int64_t>(k_level, 1);
+        out << " 1DIAGNOSTIC, " << std::setw(5) << it[k] << ", " << std::scientific << std::setprecision(12)
+            << me[k] << ", " << std::setprecision(12) << cv[k] << ", " << std::setprecision(4)
+            << t_level0 + dt * (double)(k - printed + 1) << ", " << std::setprecision(4) << dt << ", " << std::endl;
+        out.unsetf(std::ios::scientific);
+      }
+      printed = n;
+    }
+  }
+  synx_geom go;
+  synx_get_output_geom(ctx, &go);
+  const long long No = go.size[0] * go.size[1] * go.size[2];
+  std::vector<float> fwd((size_t)No * dim), inv((size_t)No * dim);
+  if (synx_get_fields(ctx, fwd.data(), inv.data()) != 0)
+    throw std::runtime_error(std::string("synx_get_fields: ") + synx_last_error(ctx));
+  nifti::write(prefix + "0Warp.nii.gz", field_image(go, fwd));
+  nifti::write(prefix + "0InverseWarp.nii.gz", field_image(go, inv));
+  if (!warped.empty()) nifti::write(warped, like(fixed, warp_on_device(moving, gm, fwd, go)));
+  if (!inv_warped.empty()) {
+    std::vector<float> inv_on_moving = resample_on_device(inv, go, gm);
+    nifti::write(inv_warped, like(moving, warp_on_device(fixed, gf, inv_on_moving, gm)));
+  }
+  if (verbose) {
+    const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    out << "  Elapsed time (stage 0): " << total << std::endl;
+  }
+  return EXIT_SUCCESS;
+}
+
+}  // namespace
+
+int antsRegistration(std::vector<std::string> args, std::ostream* out) {
+  std::ostream& os = out ? *out : std::cout;
+  try {
+    return run(args, os);
+  } catch (const std::exception& e) {
+    std::cerr << "antsRegistrationSyN_b200: " << e.what() << std::endl;
+    return EXIT_FAILURE;
+  }
+}
+
+}  // namespace ants_b200
+
+int main(int argc, char** argv) {
+  std::vector<std::string> args(argv + 1, argv + argc);
+  return ants_b200::antsRegistration(args, &std::cout);
+}

@@ -3,17 +3,20 @@
 
 One step = one complete SyN stage on one fixed/moving pair:
   SyN[0.1,3,0], CC radius 4, shrink 8x4x2x1, smoothing 3x2x1x0 vox, iterations 100x70x50x20,
-  convergence [.., 1e-12, 10] (the fixed-schedule setting; the actual iterations run per level
+  convergence [.., 1e-12, 10] (the fixed-schedule setting; the iterations actually run per level
   are counted from the stage log and reported).
 A voxel-iteration is one voxel of a level grid processed by one full SyN iteration.
 
-  value  -- inputs already resident in HBM (device-to-device image upload, device field output),
-            CUDA events on the stage's stream, L2 flushed between steps.
-  e2e    -- the same stage through the C ABI with pinned host buffers: host->device images,
-            device->host forward and inverse fields inside the timed region.
-  --impl reference -- the CPU path (the oracle restatement of the reference's arithmetic, all
-            host threads) on a bounded sample of the same workload: one full-resolution
-            iteration per step.
+  value    -- inputs resident in HBM (device-to-device image upload, device field output), each
+              level's iteration replayed as a CUDA graph, CUDA events on the stage's stream, L2
+              flushed (256 MB write) between steps.
+  e2e      -- the same stage through the C ABI with pinned host buffers: host->device images and
+              device->host forward and inverse fields inside the timed region.
+  roofline -- the fixed-point inverse (the largest kernel class) timed with CUDA events around its
+              launches in a second, event-instrumented pass over the same K steps; algorithmic bytes
+              = executed sub-iterations x voxels x 36 B.
+  --impl reference -- the CPU path (the oracle restatement of the reference arithmetic, all host
+              threads) on a bounded sample of the same workload: one full-resolution iteration per step.
 
 Multi-GPU (torchrun): independent replicas, one pair per rank (no data-path collective);
 value = voxel-iterations of all ranks / max over ranks of the timed region.
@@ -41,14 +44,14 @@ STAGE = dict(cc_radius=4, iterations=(100, 70, 50, 20), shrink_factors=(8, 4, 2,
              convergence_window=10)
 WORKLOAD = ("3-D SyN[0.1,3,0] + CC[r=4], 182x218x182 at 1 mm, shrink 8x4x2x1, sigmas 3x2x1x0 vox, "
             "iterations 100x70x50x20, convergence [1e-12,10]")
-BYTES_PER_INV_VOXEL = 36  # fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi (3 x 12 B)
+BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi
+# DRAM bytes per full-resolution k_invert_step launch (apply + statistics, both halves) from the
+# ncu capture summarised in profiles/k_invert_step_182x218x182.md
+INV_TRAFFIC_BYTES = None
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
 class ClockSampler:
@@ -162,19 +165,18 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="synx", choices=["synx", "reference"])
-    ap.add_argument("--graphs", type=int, default=1, help="replay each level's iteration as a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
 
     ws, rank, local = dist_env()
-    from ants_b200 import phantoms
+    from ants_b200 import phantoms, replicas
     from ants_b200.synx import Geom
 
     g = Geom(SIZE)
     if args.impl == "reference":
         if rank != 0:
             return 0
-        fixed, moving = phantoms.pair_3d(SIZE, seed=phantoms.SEED_BASE)
+        fixed, moving = phantoms.pair_3d(SIZE, seed=replicas.pair_seed(0))
         run_reference(args, fixed, moving, g)
         return 0
 
@@ -182,65 +184,74 @@ def main(argv=None) -> int:
     from ants_b200 import synx as S
 
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     dist = None
     if ws > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    fixed, moving = phantoms.pair_3d(SIZE, seed=phantoms.SEED_BASE + rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    fixed, moving = phantoms.pair_3d(SIZE, seed=replicas.pair_seed(rank))
     sizes = level_sizes(g)
 
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    flags = S.SYNX_F_PROFILE_EVENTS if not args.graphs else S.SYNX_F_USE_GRAPHS
-    P = S.SyNParams(dim=3, flags=flags, **STAGE)
-    stage = S.SyNStage(P, device=local, stream=stream.cuda_stream)
-    Fd = torch.from_numpy(fixed).to(f"cuda:{local}")
-    Md = torch.from_numpy(moving).to(f"cuda:{local}")
-    fwd_d = torch.empty((3,) + g.shape, device=f"cuda:{local}")
+    stage = S.SyNStage(S.SyNParams(dim=3, flags=S.SYNX_F_USE_GRAPHS, **STAGE), device=local,
+                       stream=stream.cuda_stream)
+    Fd = torch.from_numpy(fixed).to(dev)
+    Md = torch.from_numpy(moving).to(dev)
+    fwd_d = torch.empty((3,) + g.shape, device=dev)
     inv_d = torch.empty_like(fwd_d)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
 
-    def step_device():
-        stage.set_images(Fd, g, Md, g)
-        stage.run()
-        stage.fields_device(fwd_d, inv_d)
+    def step_device(st):
+        st.set_images(Fd, g, Md, g)
+        st.run()
+        st.fields_device(fwd_d, inv_d)
 
     for _ in range(args.warmup):
-        step_device()
+        step_device(stage)
     torch.cuda.synchronize()
 
-    # ---- timed region (device-resident inputs) ----
+    # ---- timed region (device-resident inputs, graph replay) ----
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    stage.reset_profile()
     launches0 = S.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     vox_iters = 0
+    its = {}
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
-            step_device()
+            step_device(stage)
             ev[k][1].record(stream)
-            vox_iters += voxel_iterations(stage.log(), sizes)
+            log = stage.log()
+            vox_iters += voxel_iterations(log, sizes)
         torch.cuda.synchronize()
+    for r in log:
+        its[r.level] = its.get(r.level, 0) + 1
     launches = S.launch_count() - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    t_total = sum(step_ms) / 1000.0
-    prof = stage.profile()
-    if dist:
-        t = torch.tensor([t_total], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
-        vi = torch.tensor([float(vox_iters)], device=f"cuda:{local}")
-        dist.all_reduce(vi)
-        vox_iters_all = int(vi.item())
-    else:
-        vox_iters_all = vox_iters
-    value = vox_iters_all / t_total
+    t_total, vox_all = replicas.aggregate(sum(step_ms) / 1000.0, vox_iters, dev)
+    value = vox_all / t_total
+
+    # ---- event-instrumented pass over the same workload: time of the fixed-point inverse ----
+    pstage = S.SyNStage(S.SyNParams(dim=3, flags=S.SYNX_F_PROFILE_EVENTS, **STAGE), device=local,
+                        stream=stream.cuda_stream)
+    step_device(pstage)
+    pstage.reset_profile()
+    pev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    pev[0].record(stream)
+    for k in range(args.steps):
+        step_device(pstage)
+    pev[1].record(stream)
+    torch.cuda.synchronize()
+    prof = pstage.profile()
+    prof_levels = pstage.level_profile()
+    prof_total_ms = pev[0].elapsed_time(pev[1])
+    pstage.close()
 
     # ---- end to end through the C ABI with pinned host buffers ----
     Fh = torch.from_numpy(fixed).pin_memory().numpy()
@@ -248,8 +259,7 @@ def main(argv=None) -> int:
     shp = g.shape + (3,)
     fwd_h = torch.empty(shp, dtype=torch.float32).pin_memory().numpy()
     inv_h = torch.empty(shp, dtype=torch.float32).pin_memory().numpy()
-    e2e_ms = []
-    e2e_vi = 0
+    e2e_ms, e2e_vi = [], 0
     if dist:
         dist.barrier()
     for k in range(args.steps):
@@ -264,14 +274,7 @@ def main(argv=None) -> int:
         b.synchronize()
         e2e_ms.append(a.elapsed_time(b))
         e2e_vi += voxel_iterations(stage.log(), sizes)
-    t_e2e = sum(e2e_ms) / 1000.0
-    if dist:
-        t = torch.tensor([t_e2e], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-        vi = torch.tensor([float(e2e_vi)], device=f"cuda:{local}")
-        dist.all_reduce(vi)
-        e2e_vi = int(vi.item())
+    t_e2e, e2e_vi = replicas.aggregate(sum(e2e_ms) / 1000.0, e2e_vi, dev)
     e2e_value = e2e_vi / t_e2e
 
     if rank == 0:
@@ -280,21 +283,24 @@ def main(argv=None) -> int:
         if prof["inverse_ms"] > 0:
             bytes_alg = prof["inverse_voxels"] * BYTES_PER_INV_VOXEL
             achieved = bytes_alg / (prof["inverse_ms"] / 1000.0) / 1e9
-            roof = {"kernel": "k_invert_step (fused fixed-point inverse sub-iteration)", "bound": "hbm",
+            full = prof_levels[-1]
+            full_ach = (full["inverse_subiterations"] * full["voxels"] * BYTES_PER_INV_VOXEL /
+                        (full["inverse_ms"] / 1000.0) / 1e9) if full["inverse_ms"] > 0 else None
+            roof = {"kernel": "k_invert_step (fixed-point inverse sub-iteration, all levels)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_source": peak_kind, "traffic": None,
+                    "peak_source": peak_kind, "traffic": INV_TRAFFIC_BYTES,
                     "algorithmic_bytes_per_half_field_voxel": BYTES_PER_INV_VOXEL,
-                    "inverse_share_of_step": prof["inverse_ms"] / sum(step_ms),
-                    "cc_ms_share": prof["cc_ms"] / sum(step_ms)}
+                    "achieved_full_resolution_level": full_ach,
+                    "frac_full_resolution_level": (full_ach / peak) if full_ach else None,
+                    "share_of_instrumented_step": prof["inverse_ms"] / prof_total_ms,
+                    "cc_share_of_instrumented_step": prof["cc_ms"] / prof_total_ms,
+                    "level_ms_per_step": [round(l["iterate_ms"] / args.steps, 3) for l in prof_levels]}
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
             threads = os.cpu_count() or 1
             v_cpu, dt = cpu_sample(fixed, moving, g, threads)
             cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"one full-resolution SyN-CC iteration from zero fields ({dt:.1f} s)"}
-        its = {}
-        for r in stage.log():
-            its[r.level] = its.get(r.level, 0) + 1
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_total / args.steps, "higher_is_better": True,
@@ -302,7 +308,7 @@ def main(argv=None) -> int:
             "data": "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field",
             "config": {"workload": WORKLOAD, "iterations_run_per_level": [its.get(l, 0) for l in range(4)],
                        "voxel_iterations_per_step": vox_iters // args.steps, "l2": "flushed between steps (256 MB)",
-                       "parallelism": f"replicas x{ws}", "cuda_graphs": bool(args.graphs)},
+                       "parallelism": f"replicas x{ws}", "cuda_graphs": True},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(Fh.nbytes + Mh.nbytes),
                     "d2h_bytes_per_step": int(fwd_h.nbytes + inv_h.nbytes),
                     "ms_per_step": 1000.0 * t_e2e / args.steps},
