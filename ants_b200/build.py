@@ -26,8 +26,9 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 LIB = os.path.join(HERE, "libsynx.so")
 CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
 
-LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_ctx.cu", "synx_noalloc.cu"]
-LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh"]
+LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu"]
+LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh", "synx_phases.cuh", "synx_cc_tile.cuh", "synx_level.cuh",
+               "synx_level_body.cuh"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
 CLI_HEADERS = ["nifti_io.h", "ants_registration.h"]
 
@@ -54,15 +55,36 @@ def _run(cmd: list[str]) -> None:
     subprocess.run(cmd, check=True)
 
 
+BUILD_DIR = os.path.join(HERE, "_build")
+LEVEL_RADII = range(1, 8)  # the persistent level kernel is instantiated once per CC radius
+
+
+def _objects() -> list[tuple[str, str, list[str]]]:
+    """(source, object, extra flags) for every compile unit of libsynx.so."""
+    units = [(os.path.join(CSRC, s), os.path.join(BUILD_DIR, s.replace(".cu", ".o")), []) for s in LIB_SOURCES]
+    inst = os.path.join(CSRC, "synx_level_inst.cu")
+    units += [(inst, os.path.join(BUILD_DIR, f"synx_level_r{r}.o"), [f"-DSYNX_RCC={r}"]) for r in LEVEL_RADII]
+    return units
+
+
 def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
-    srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in LIB_HEADERS] + [os.path.join(INCLUDE, "synx.h")]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *srcs, "-lcudart"]
-    if verbose_ptxas:
-        cmd.insert(1, "-Xptxas=-v")
-    _run(cmd)
+    from concurrent.futures import ThreadPoolExecutor
+
+    headers = [os.path.join(CSRC, h) for h in LIB_HEADERS] + [os.path.join(INCLUDE, "synx.h")]
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    jobs = []
+    for src, obj, extra in _objects():
+        if force or _stale(obj, [src] + headers):
+            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-ccbin", _host_cxx(), *extra, "-c", "-o", obj, src]
+            if verbose_ptxas:
+                cmd.insert(1, "-Xptxas=-v")
+            jobs.append(cmd)
+    if jobs:
+        with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+            list(ex.map(_run, jobs))
+    objs = [o for _, o, _ in _objects()]
+    if force or jobs or _stale(LIB, objs):
+        _run([_nvcc(), *ARCH, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *objs, "-lcudart"])
     return LIB
 
 

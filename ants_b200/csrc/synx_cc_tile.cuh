@@ -1,0 +1,245 @@
+// Neighbourhood cross-correlation tile (value and both SyN update directions), shared by the
+// CC kernel and the persistent level kernel.
+#include <cfloat>
+#include <cmath>
+
+#pragma once
+
+#include "synx_kernels.cuh"
+
+namespace synx {
+
+// ------------------------------------------------------------------------------------------
+// Neighbourhood cross-correlation: value and both update directions.
+//
+// A block owns a 32 x 8 tile of output columns and marches along z over a chunk of ZC
+// slices.  Each thread keeps FP64 running z-window sums of F, M, F^2, M^2, FM for up to CPT
+// halo columns; the raw (F, M) values of the last 2R+1 slices sit in a shared-memory ring so
+// the leaving slice is subtracted without a second global read.  Per slice the column sums
+// are box-summed along x and then y in shared memory (FP64), giving the five window sums of
+// each output voxel, from which the CC terms and derivatives follow.  The in-bounds count is
+// separable (cx*cy*cz) and computed analytically.
+// ------------------------------------------------------------------------------------------
+struct CCParams {
+  float h[3];      // spacing
+  float dir[9];    // direction cosines
+  int identity_dir;
+  double eps;
+  int ZC;          // z-chunk per block
+};
+
+__device__ __forceinline__ int pmod(int a, int m) {
+  int r = a % m;
+  return r < 0 ? r + m : r;
+}
+
+__device__ __forceinline__ float grad1(float vm, float v0, float vp, int pos, int n, float h) {
+  if (n < 2 || pos == n - 1) return 0.0f;
+  if (pos == 0) return 0.5f * (vp - v0) / h;
+  return (vp - vm) / (2.0f * h);
+}
+
+template <int R, int DIM>
+struct CCShape {
+  static constexpr int TX = 32, TY = 8;
+  static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HC = HX * HY;
+  static constexpr int RZ = DIM == 3 ? R : 0;
+  static constexpr int RD = 2 * RZ + 1;
+  static constexpr int CPT = (HC + 255) / 256;
+  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)5 * HC * sizeof(double) +
+                                 (size_t)5 * HY * TX * sizeof(double);
+};
+
+// One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
+// Returns the tile's sum of local cc (valid in thread 0).  All threads of the block must call
+// it; `smem_raw` holds CCShape<R, DIM>::smem bytes and `red` 32 doubles.
+template <int R, int DIM>
+__device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const float* __restrict__ Mt, const Dims& d,
+                                          const CCParams& P, float* __restrict__ gF, float* __restrict__ gM,
+                                          float* __restrict__ cc_out, int bx, int by, int bz,
+                                          unsigned char* smem_raw, double* red) {
+  using S = CCShape<R, DIM>;
+  constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
+  float2* ring = reinterpret_cast<float2*>(smem_raw);
+  double* cs = reinterpret_cast<double*>(ring + RD * HC);
+  double* xs = cs + 5 * HC;
+
+  const int tid = threadIdx.x;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const long long nxy = (long long)nx * ny, N = d.N;
+  const int x0 = bx * TX, y0 = by * S::TY;
+  const int z0 = bz * P.ZC;
+  const int z1 = min(z0 + P.ZC, nz);
+
+  // owned halo columns
+  int gofs[CPT];
+  bool gval[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    int col = tid + c * 256;
+    int hx = col % HX, hy = col / HX;
+    int gx = x0 - R + hx, gy = y0 - R + hy;
+    gval[c] = col < HC && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+    gofs[c] = gval[c] ? gy * nx + gx : 0;
+  }
+  double acc[CPT][5];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c)
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc[c][q] = 0.0;
+
+  // warm-up: slices z0-RZ .. z0+RZ-1
+  for (int zs = z0 - RZ; zs < z0 + RZ; ++zs) {
+    const bool zin = zs >= 0 && zs < nz;
+    const int slot = pmod(zs, RD);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      int col = tid + c * 256;
+      if (col < HC) {
+        float2 v = make_float2(0.0f, 0.0f);
+        if (zin && gval[c]) {
+          long long o = (long long)zs * nxy + gofs[c];
+          v.x = __ldg(Ft + o);
+          v.y = __ldg(Mt + o);
+          double f = v.x, m = v.y;
+          acc[c][0] += f;
+          acc[c][1] += m;
+          acc[c][2] += f * f;
+          acc[c][3] += m * m;
+          acc[c][4] += f * m;
+        }
+        ring[slot * HC + col] = v;
+      }
+    }
+  }
+
+  double cc_acc = 0.0;
+  const int tx = tid & 31, ty = tid >> 5;
+  const int ox = x0 + tx, oy = y0 + ty;
+  const bool out_ok = ox < nx && oy < ny;
+  const double cxn = (double)(min(ox + R, nx - 1) - max(ox - R, 0) + 1);
+  const double cyn = (double)(min(oy + R, ny - 1) - max(oy - R, 0) + 1);
+
+  for (int zc = z0; zc < z1; ++zc) {
+    // slide the z window: subtract slice zc-RZ-1 (if it was added), add slice zc+RZ
+    const int ze = zc + RZ, zl = zc - RZ - 1;
+    const int slot = pmod(ze, RD);
+    const bool sub = zc > z0 && zl >= 0;
+    const bool zin = ze < nz;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      int col = tid + c * 256;
+      if (col < HC) {
+        if (sub && gval[c]) {
+          float2 o = ring[slot * HC + col];
+          double f = o.x, m = o.y;
+          acc[c][0] -= f;
+          acc[c][1] -= m;
+          acc[c][2] -= f * f;
+          acc[c][3] -= m * m;
+          acc[c][4] -= f * m;
+        }
+        float2 v = make_float2(0.0f, 0.0f);
+        if (zin && gval[c]) {
+          long long o = (long long)ze * nxy + gofs[c];
+          v.x = __ldg(Ft + o);
+          v.y = __ldg(Mt + o);
+          double f = v.x, m = v.y;
+          acc[c][0] += f;
+          acc[c][1] += m;
+          acc[c][2] += f * f;
+          acc[c][3] += m * m;
+          acc[c][4] += f * m;
+        }
+        ring[slot * HC + col] = v;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) cs[q * HC + col] = acc[c][q];
+      }
+    }
+    __syncthreads();
+    // x box sums: HY rows x TX outputs
+    for (int p = tid; p < HY * TX; p += 256) {
+      const int hy = p / TX, px = p % TX;
+      const double* src = cs + hy * HX + px;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j <= 2 * R; ++j) s += src[q * HC + j];
+        xs[q * HY * TX + p] = s;
+      }
+    }
+    __syncthreads();
+    if (out_ok) {
+      double Sq[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j <= 2 * R; ++j) s += xs[q * HY * TX + (ty + j) * TX + tx];
+        Sq[q] = s;
+      }
+      const double czn = (double)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
+      const double n = cxn * cyn * czn;
+      const double inv_n = __drcp_rn(n);
+      const double mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
+      const double sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
+      const double sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
+      const double sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
+      const int cidx = (ty + R) * HX + (tx + R);
+      const float2* rc = ring + pmod(zc, RD) * HC;
+      const float2 v0 = rc[cidx];
+      const double fh = (double)v0.x - mF, mh = (double)v0.y - mM;
+      double cc = 1.0, aF = 0.0, aM = 0.0;
+      if (sFF > P.eps && sMM > P.eps) {
+        const double prod = sFF * sMM;
+        const double ip = __drcp_rn(prod);
+        cc = sFM * sFM * ip;
+        const double coef = 2.0 * sFM * ip;
+        aF = coef * (fh - sFM * sFF * ip * mh);
+        aM = coef * (mh - sFM * sMM * ip * fh);
+      }
+      cc_acc += cc;
+      // central differences of both warped images (index axes)
+      float gMi[3], gFi[3];
+      {
+        const float2 xm = rc[cidx - 1], xp = rc[cidx + 1];
+        gMi[0] = grad1(xm.y, v0.y, xp.y, ox, nx, P.h[0]);
+        gFi[0] = grad1(xm.x, v0.x, xp.x, ox, nx, P.h[0]);
+        const float2 ym = rc[cidx - HX], yp = rc[cidx + HX];
+        gMi[1] = grad1(ym.y, v0.y, yp.y, oy, ny, P.h[1]);
+        gFi[1] = grad1(ym.x, v0.x, yp.x, oy, ny, P.h[1]);
+        gMi[2] = gFi[2] = 0.0f;
+        if (DIM == 3) {
+          const float2 zm = ring[pmod(zc - 1, RD) * HC + cidx], zp = ring[pmod(zc + 1, RD) * HC + cidx];
+          gMi[2] = grad1(zm.y, v0.y, zp.y, zc, nz, P.h[2]);
+          gFi[2] = grad1(zm.x, v0.x, zp.x, zc, nz, P.h[2]);
+        }
+      }
+      const long long oi = (long long)zc * nxy + (long long)oy * nx + ox;
+#pragma unroll
+      for (int dd = 0; dd < DIM; ++dd) {
+        float pm, pf;
+        if (P.identity_dir) {
+          pm = gMi[dd];
+          pf = gFi[dd];
+        } else {
+          pm = 0.0f;
+          pf = 0.0f;
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) {
+            pm += P.dir[dd * 3 + a] * gMi[a];
+            pf += P.dir[dd * 3 + a] * gFi[a];
+          }
+        }
+        gF[dd * N + oi] = (float)(aF * (double)pm);
+        gM[dd * N + oi] = (float)(aM * (double)pf);
+      }
+      if (cc_out != nullptr) cc_out[oi] = (float)cc;
+    }
+    __syncthreads();
+  }
+  return block_sum_d(cc_acc, red);
+}
+
+}  // namespace synx

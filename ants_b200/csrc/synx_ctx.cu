@@ -17,6 +17,7 @@
 
 #include "../../include/synx.h"
 #include "synx_kernels.cuh"
+#include "synx_level.cuh"
 
 using namespace synx;
 
@@ -188,6 +189,7 @@ struct synx_ctx {
   int R_upd[3] = {0, 0, 0}, R_tot[3] = {0, 0, 0};
   IterCtl* ctl = nullptr;
   LogDev logdev{};
+  int coop_max = 0;  // largest cooperative grid of the level kernel (0: not queried)
   unsigned* hist = nullptr;  // 256 bins + 2 min/max
   // host mirrors
   std::vector<float> h_coeff_upd, h_coeff_tot;
@@ -265,6 +267,7 @@ int allocate(synx_ctx* c) {
     ccb = std::max(ccb, cc_blocks(g, c->P.cc_radius));
     invb = std::max(invb, inv_blocks(g));
   }
+  invb = std::max(invb, 2048);  // also holds one slot per block of the persistent level kernel
   // step entry points on arbitrary grids reuse nothing from here
   const int coeff_cap = 1024;
   int max_iters = 1;
@@ -549,6 +552,95 @@ void enqueue_iteration(synx_ctx* c, bool profile) {
   launch_converge(c->ctl, c->logdev, c->P.convergence_threshold, c->P.convergence_window, s);
 }
 
+// The persistent level kernel serves small levels (launch latency dominates there) when the
+// stage uses the common options it implements; larger levels, the event-profiled mode and the
+// rarer options (total-field smoothing, no update smoothing, wide kernels) take the per-kernel
+// path.
+constexpr long long kPersistentMaxVoxels = 2500000;
+
+bool use_persistent(synx_ctx* c, const GridInfo& g, bool profile, int* blocks) {
+  if (profile || (c->P.flags & SYNX_F_NO_PERSISTENT)) return false;
+  if (g.d.N > kPersistentMaxVoxels || c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
+  int rs = 1;
+  for (int a = 0; a < c->D; ++a) rs = std::max(rs, c->R_upd[a]);
+  if (rs > kLevelMaxSmoothRadius) return false;
+  if (c->coop_max <= 0) c->coop_max = level_max_blocks(c->D, c->P.cc_radius, kLevelMaxSmoothRadius, c->device);
+  if (c->coop_max <= 0) return false;
+  long long want = (g.d.N + 2047) / 2048;
+  want = std::max<long long>(want, 16);
+  *blocks = (int)std::min<long long>(want, std::min(c->coop_max, c->inv_cap));
+  return *blocks > 0;
+}
+
+LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
+  LevelArgs A;
+  memset(&A, 0, sizeof(A));
+  const int D = c->D;
+  const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
+  const int target_units = 2 * 296;  // about two tiles per block of a full cooperative grid
+  auto zb_for = [&](int halves) {
+    int per = std::max(1, target_units / (gx * gy * halves));
+    return std::max(1, (g.d.nz + per - 1) / per);
+  };
+  const int zw = zb_for(1), zc2 = zb_for(2);
+  A.warp = WarpArgs{c->Fs, c->Ms, c->psiF, c->psiM, c->Ft, c->Mt, c->gF.d, c->gM.d, g.d,
+                    make_affine(g, c->gF), make_affine(g, c->gM), zw};
+  A.cc = make_cc_params(g, c->P.cc_radius);
+  A.cc_gx = gx;
+  A.cc_gy = gy;
+  A.cc_gz = (g.d.nz + A.cc.ZC - 1) / A.cc.ZC;
+  A.gF = c->gFu;
+  A.gM = c->gMu;
+  const double var = c->P.update_variance;
+  const float w1 = var < 0.5 ? (float)(1.0 - var / 0.5) : 1.0f;
+  const float* kh[3] = {c->h_coeff_upd.data(), c->h_coeff_upd.data() + c->coeff_cap,
+                        c->h_coeff_upd.data() + 2 * c->coeff_cap};
+  const float* in[2] = {c->gFu, c->gMu};
+  float* t2[2] = {c->t2F, c->t2M};
+  float* t1[2] = {c->t1F, c->t1M};
+  int RR = 1;
+  A.sxy = make_smooth_args(in, D == 3 ? t2 : t1, in, 2, g, kh, c->R_upd, true, w1, 1.0f - w1, true, &RR);
+  A.sz = A.sxy;
+  A.sz.in = Ptr2c{{c->t2F, c->t2M}};
+  A.sz.out = Ptr2{{c->t1F, c->t1M}};
+  A.sz.ZC = smooth_z_chunk(g.d, 2, RR);
+  A.sz_gz = (g.d.nz + A.sz.ZC - 1) / A.sz.ZC;
+  A.r_smooth = RR;
+  A.comp.d = Ptr2c{{c->t1F, c->t1M}};
+  A.comp.w = Ptr2c{{c->phiF, c->phiM}};
+  A.comp.o = Ptr2{{c->phiF, c->phiM}};
+  A.comp.g = g.d;
+  A.comp.m = make_affine(g, g);
+  A.comp.eta = c->P.learning_rate;
+  A.comp.zb = zc2;
+  const float* phis[2] = {c->phiF, c->phiM};
+  float* psis[2] = {c->psiF, c->psiM};
+  const float* psic[2] = {c->psiF, c->psiM};
+  float* phim[2] = {c->phiF, c->phiM};
+  A.invA = make_inv_args(phis, psis, 2, g, zc2);
+  A.invB = make_inv_args(psic, phim, 2, g, zc2);
+  A.g = g.d;
+  A.ctl = c->ctl;
+  A.log = c->logdev;
+  A.cc_partials = c->cc_partials;
+  A.inv_psum = c->inv_psum;
+  A.inv_pmax = c->inv_pmax;
+  A.pcap = c->inv_cap;
+  A.iters = iters;
+  A.el_gx = gx;
+  A.el_gy = gy;
+  A.warp_gz = (g.d.nz + zw - 1) / zw;
+  A.comp_gz = (g.d.nz + zc2 - 1) / zc2;
+  A.inv_gz = A.comp_gz;
+  A.inv_max_iter = c->P.inv_max_iter;
+  A.inv_mean_tol = c->P.inv_mean_tol;
+  A.inv_max_tol = c->P.inv_max_tol;
+  A.conv_threshold = c->P.convergence_threshold;
+  A.conv_window = c->P.convergence_window;
+  A.diag = affine_diag_host(A.warp.mF) && affine_diag_host(A.warp.mM) && affine_diag_host(A.comp.m);
+  return A;
+}
+
 int run_level_impl(synx_ctx* c, int level) {
   if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_run_level: images not set");
   if (level != c->cur_level + 1 || level >= c->P.n_levels)
@@ -584,7 +676,13 @@ int run_level_impl(synx_ctx* c, int level) {
   c->ev_pairs_inv.clear();
   c->ev_pairs_cc.clear();
   CUDA_TRY(c, cudaEventRecord(c->lev_ev[1], c->stream));
-  if (graphs && iters > 0) {
+  int coop_blocks = 0;
+  const bool persistent = iters > 0 && use_persistent(c, gl, profile, &coop_blocks);
+  if (persistent) {
+    // every iteration of this level in one cooperative launch
+    LevelArgs A = make_level_args(c, gl, iters);
+    CUDA_TRY(c, launch_level(A, D, c->P.cc_radius, coop_blocks, c->stream));
+  } else if (graphs && iters > 0) {
     // one iteration is captured once per level and context (all its launch arguments are fixed
     // for a given level: the buffers are reset to the same assignment by synx_set_images) and
     // replayed `iters` times; the device-side stop flag ends a converged level early
@@ -621,6 +719,8 @@ int run_level_impl(synx_ctx* c, int level) {
     CUDA_TRY(c, cudaMemcpyAsync(li.data(), c->logdev.inv_iters, 4 * iters, cudaMemcpyDeviceToHost, c->stream));
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (hctl.bar_err)
+    return set_err(c, SYNX_E_CUDA, "level " + std::to_string(level) + ": a grid barrier of the level kernel timed out");
   const int done = std::min(hctl.iter, iters);
   long long sub_iters = 0;
   for (int k = 0; k < done; ++k) {

@@ -14,7 +14,8 @@
 #include <cstdio>
 #include <cstring>
 
-#include "synx_kernels.cuh"
+#include "synx_level.cuh"
+#include "synx_phases.cuh"
 
 namespace synx {
 
@@ -150,27 +151,7 @@ static bool affine_diag(const Affine& m) {
     if (m.B[k] != 0.0f || m.A[k] != 0.0f) return false;
   return true;
 }
-
-// DIAG: the grids share axis directions (no rotation between them), the common case; the
-// map is then one FMA pair per axis.
-template <int DIM, bool DIAG = false>
-__device__ __forceinline__ void map_point(const Affine& m, float fx, float fy, float fz, float ux, float uy, float uz,
-                                          float& cx, float& cy, float& cz) {
-  if (DIAG) {
-    cx = fmaf(m.A[0], ux, fmaf(m.B[0], fx, m.t[0]));
-    cy = fmaf(m.A[4], uy, fmaf(m.B[4], fy, m.t[1]));
-    cz = DIM == 3 ? fmaf(m.A[8], uz, fmaf(m.B[8], fz, m.t[2])) : 0.0f;
-    return;
-  }
-  cx = m.t[0] + m.B[0] * fx + m.B[1] * fy + m.A[0] * ux + m.A[1] * uy;
-  cy = m.t[1] + m.B[3] * fx + m.B[4] * fy + m.A[3] * ux + m.A[4] * uy;
-  cz = 0.0f;
-  if (DIM == 3) {
-    cx += m.B[2] * fz + m.A[2] * uz;
-    cy += m.B[5] * fz + m.A[5] * uz;
-    cz = m.t[2] + m.B[6] * fx + m.B[7] * fy + m.B[8] * fz + m.A[6] * ux + m.A[7] * uy + m.A[8] * uz;
-  }
-}
+bool affine_diag_host(const Affine& m) { return affine_diag(m); }
 
 // ------------------------------------------------------------------------------------------
 // Level control reset
@@ -181,6 +162,8 @@ __global__ void k_zero_ctl_level(IterCtl* ctl) {
   ctl->total_abs = 0.0;
   ctl->maxnorm[0] = ctl->maxnorm[1] = 0u;
   ctl->cc_counter = 0u;
+  ctl->bar_count = 0u;
+  ctl->bar_err = 0;
   for (int p = 0; p < 2; ++p)
     for (int h = 0; h < 2; ++h) {
       ctl->inv[p][h].counter = 0u;
@@ -193,76 +176,33 @@ void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s) {
   k_zero_ctl_level<<<1, 1, 0, s>>>(ctl);
 }
 
-// ------------------------------------------------------------------------------------------
-// Warp of both images through their inverse half-fields onto the level grid.
-// ------------------------------------------------------------------------------------------
-template <int DIM, bool DIAG>
-__device__ __forceinline__ float sample(const float* __restrict__ img, const Dims& di, const Affine& m, float fx,
-                                        float fy, float fz, float ux, float uy, float uz) {
-  float cx, cy, cz;
-  map_point<DIM, DIAG>(m, fx, fy, fz, ux, uy, uz, cx, cy, cz);
-  if (!inside_buffer<DIM>(di, cx, cy, cz)) return 0.0f;
-  return lerp_at<DIM>(img, make_cell<DIM>(di, cx, cy, cz));
-}
 
+// ------------------------------------------------------------------------------------------
+// Warps (one tile per block).
+// ------------------------------------------------------------------------------------------
 template <int DIM, bool DIAG>
-__global__ void __launch_bounds__(256)
-    k_warp_pair(const float* __restrict__ F, Dims dF, Affine mF, const float* __restrict__ psiF,
-                const float* __restrict__ M, Dims dM, Affine mM, const float* __restrict__ psiM, Dims dv, int zb,
-                float* __restrict__ Ft, float* __restrict__ Mt, IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_warp_pair(const WarpArgs a, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && ctl != nullptr) {
-    ctl->maxnorm[0] = 0u;
+    ctl->maxnorm[0] = 0u;  // the update scaling of this iteration starts from zero
     ctl->maxnorm[1] = 0u;
   }
-  const Coord3 c = coord3(dv, zb, 1);
-  if (!c.ok) return;
-  const int N = (int)dv.N, nxy = dv.nx * dv.ny;
-  const float fx = (float)c.x, fy = (float)c.y;
-  const int i0 = c.z0 * nxy + c.y * dv.nx + c.x;
-  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
-  if (c.z0 < c.z1) {
-    a0 = psiF[i0];
-    a1 = psiF[N + i0];
-    a2 = DIM == 3 ? psiF[2 * N + i0] : 0.0f;
-    b0 = psiM[i0];
-    b1 = psiM[N + i0];
-    b2 = DIM == 3 ? psiM[2 * N + i0] : 0.0f;
-  }
-  for (int z = c.z0; z < c.z1; ++z) {
-    const int i = z * nxy + c.y * dv.nx + c.x;
-    const float fz = (float)z;
-    const float u0 = a0, u1 = a1, u2 = a2, v0 = b0, v1 = b1, v2 = b2;
-    if (z + 1 < c.z1) {  // next slice's displacements, loaded ahead of this slice's gathers
-      const int j = i + nxy;
-      a0 = psiF[j];
-      a1 = psiF[N + j];
-      a2 = DIM == 3 ? psiF[2 * N + j] : 0.0f;
-      b0 = psiM[j];
-      b1 = psiM[N + j];
-      b2 = DIM == 3 ? psiM[2 * N + j] : 0.0f;
-    }
-    Ft[i] = sample<DIM, DIAG>(F, dF, mF, fx, fy, fz, u0, u1, u2);
-    Mt[i] = sample<DIM, DIAG>(M, dM, mM, fx, fy, fz, v0, v1, v2);
-  }
+  warp_pair_tile<DIM, DIAG>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, const float* M, const GridInfo& gM,
                       const float* psiM, const GridInfo& gv, float* Ft, float* Mt, IterCtl* ctl, cudaStream_t s) {
   count_launch();
-  Affine mF = make_affine(gv, gF), mM = make_affine(gv, gM);
+  WarpArgs a{F, M, psiF, psiM, Ft, Mt, gF.d, gM.d, gv.d, make_affine(gv, gF), make_affine(gv, gM), 0};
   const Map3 m = map3(gv.d);
-  const bool dg = affine_diag(mF) && affine_diag(mM);
+  a.zb = m.zb;
+  const bool dg = affine_diag(a.mF) && affine_diag(a.mM);
   if (gv.d.dim == 3) {
-    if (dg)
-      k_warp_pair<3, true><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
-    else
-      k_warp_pair<3, false><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+    if (dg) k_warp_pair<3, true><<<m.grid, 256, 0, s>>>(a, ctl);
+    else k_warp_pair<3, false><<<m.grid, 256, 0, s>>>(a, ctl);
   } else {
-    if (dg)
-      k_warp_pair<2, true><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
-    else
-      k_warp_pair<2, false><<<m.grid, 256, 0, s>>>(F, gF.d, mF, psiF, M, gM.d, mM, psiM, gv.d, m.zb, Ft, Mt, ctl);
+    if (dg) k_warp_pair<2, true><<<m.grid, 256, 0, s>>>(a, ctl);
+    else k_warp_pair<2, false><<<m.grid, 256, 0, s>>>(a, ctl);
   }
 }
 
@@ -275,7 +215,8 @@ __global__ void __launch_bounds__(256) k_warp_image(const float* __restrict__ im
   const int N = (int)dv.N, nxy = dv.nx * dv.ny;
   for (int z = c.z0; z < c.z1; ++z) {
     const int i = z * nxy + c.y * dv.nx + c.x;
-    out[i] = sample<DIM, false>(img, di, m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f);
+    out[i] = sample<DIM, false>(img, di, m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i],
+                                DIM == 3 ? u[2 * N + i] : 0.0f);
   }
 }
 
@@ -291,197 +232,32 @@ void launch_warp_image(const float* img, const GridInfo& gi, const float* u, con
 }
 
 // ------------------------------------------------------------------------------------------
-// Gaussian smoothing of displacement fields, all axes in one pass.
-//
-// A block owns a 32 x 8 tile of output columns of one field and marches along z.  For each
-// input slice it stages the (32+2Rx) x (8+2Ry) halo tile of every component in shared
-// memory (replicate-edge indices), convolves along x, then y (each thread its own column),
-// and keeps the xy-smoothed slices of the last 2Rz+1 z positions in a per-thread shared
-// ring; the z convolution of that ring gives the output.  The pass order (x, y, z) and the
-// float rounding after each axis follow the separable filter.  The epilogue applies SyN's
-// boundary zeroing and blend, and reduces max ||u / spacing|| for the update scaling.
+// Gaussian smoothing of displacement fields: an xy kernel (one block per tile, slice and field)
+// and, in 3-D, a z kernel (one thread per column chunk).  The SyN epilogue (boundary zeroing,
+// blend for small variances) and the max ||u/h|| reduction run in the last pass.
 // ------------------------------------------------------------------------------------------
-struct Ptr2c {
-  const float* p[2];
-};
-struct Ptr2 {
-  float* p[2];
-};
-
-constexpr int kSmoothRMax = 12;
-
-struct Smooth3Args {
-  Ptr2c in, orig;
-  Ptr2 out;
-  float k[3][2 * kSmoothRMax + 1];  // per-axis kernels, zero-padded and centred to radius R
-  int ZC, halves, epilogue, do_max;
-  float w1, w2;
-  float ih[3];
-};
-
-__host__ __device__ inline size_t smooth3_smem_floats(int dim, int R) {
-  const int HXP = (32 + 2 * R + 3) & ~3, HY = 8 + 2 * R;
-  return (size_t)dim * HY * HXP + (size_t)dim * HY * 32;
-}
-
-// xy part: one block per (32 x 8 tile, slice, field).  The halo tile of every component is
-// staged in shared memory with replicate-edge indices, convolved along x (each work item makes
-// four consecutive outputs from float4 loads) and then along y.  In 2-D this is the whole
-// filter and the SyN epilogue runs here; in 3-D the xy-smoothed slice goes to `out` for the z
-// kernel.
 template <int DIM, int R>
 __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
-  constexpr int K = 2 * R + 1;
-  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = 8 + 2 * R;
-  constexpr int NQ = (2 * R + 3) / 4 + 1;  // float4 loads covering 4 + 2R taps
   extern __shared__ __align__(16) float sm3[];
   __shared__ float red[32];
-  float* tile = sm3;                    // [DIM][HY][HXP]
-  float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
-  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
-  const int h = blockIdx.z / nz;
-  const int z = blockIdx.z - h * nz;
-  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
-  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
-  const float* plane = src + z * nxy;
-  for (int row = ty; row < DIM * HY; row += 8) {
-    const int c = row / HY, hy = row - c * HY;
-    const int gy = min(max(y0 - R + hy, 0), ny - 1);
-    const float* line = plane + c * N + gy * nx;
-    float* trow = tile + row * HXP;
-#pragma unroll
-    for (int hx = tx; hx < HX; hx += 32) trow[hx] = __ldg(line + min(max(x0 - R + hx, 0), nx - 1));
-  }
-  __syncthreads();
-  for (int it = tid; it < DIM * HY * 8; it += 256) {
-    const int row = it >> 3, q = it & 7;
-    const float4* t4 = reinterpret_cast<const float4*>(tile + row * HXP) + q;
-    float w[4 * NQ];
-#pragma unroll
-    for (int m = 0; m < NQ; ++m) {
-      const float4 v = t4[m];
-      w[4 * m] = v.x;
-      w[4 * m + 1] = v.y;
-      w[4 * m + 2] = v.z;
-      w[4 * m + 3] = v.w;
-    }
-    float o[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      float acc = 0.0f;
-#pragma unroll
-      for (int j = 0; j < K; ++j) acc = fmaf(a.k[0][j], w[i + j], acc);
-      o[i] = acc;
-    }
-    reinterpret_cast<float4*>(xsum + row * 32)[q] = make_float4(o[0], o[1], o[2], o[3]);
-  }
-  __syncthreads();
-  const int ox = x0 + tx, oy = y0 + ty;
-  const bool ok = ox < nx && oy < ny;
-  float y[DIM];
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    const float* col = xsum + (c * HY + ty) * 32 + tx;
-    float acc = 0.0f;
-#pragma unroll
-    for (int j = 0; j < K; ++j) acc = fmaf(a.k[1][j], col[j * 32], acc);
-    y[c] = acc;
-  }
-  if (DIM == 3) {
-    if (ok) {
-      const int i = z * nxy + oy * nx + ox;
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) dst[c * N + i] = y[c];
-    }
-    return;
-  }
-  // 2-D: SyN epilogue and max norm
-  float mx = 0.0f;
-  if (ok) {
-    const int i = oy * nx + ox;
-    const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
-    const bool edge = a.epilogue && (ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1);
-    float nrm2 = 0.0f;
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      float r = y[c];
-      if (a.epilogue) {
-        if (edge) r = 0.0f;
-        else if (a.w2 != 0.0f) r = r * a.w1 + org[c * N + i] * a.w2;
-      }
-      const float q = r * a.ih[c];
-      nrm2 += q * q;
-      dst[c * N + i] = r;
-    }
-    mx = sqrtf(nrm2);
-  }
-  if (a.do_max) {
+  const int h = blockIdx.z / d.nz;
+  const int z = blockIdx.z - h * d.nz;
+  const float mx = smooth_xy_tile<DIM, R>(a, d, blockIdx.x, blockIdx.y, z, h, sm3);
+  if (DIM == 2 && a.do_max) {
     const float bm = block_max_f(mx, red);
-    if (tid == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
+    if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
   }
 }
 
-// z part (3-D): each thread owns one (x, y) column of one field over a chunk of slices and
-// keeps the last 2R+1 xy-smoothed values per component in registers; the z loop is unrolled
-// by 2R+1 so every ring index is a compile-time constant.  No shared memory, no barriers in
-// the loop.  Applies the SyN epilogue and reduces the max norm.
 template <int R>
 __global__ void __launch_bounds__(256) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
-  constexpr int K = 2 * R + 1, RD = K;
   __shared__ float red[32];
-  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
   const int nzc = gridDim.z / a.halves;
   const int h = blockIdx.z / nzc;
   const int zc = blockIdx.z - h * nzc;
-  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
-  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
-  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
-  const int ox = blockIdx.x * 32 + (threadIdx.x & 31), oy = blockIdx.y * 8 + (threadIdx.x >> 5);
-  const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
-  float mx = 0.0f;
-  if (ox < nx && oy < ny) {
-    const float* col = src + oy * nx + ox;
-    float ring[3][RD];
-#pragma unroll
-    for (int u = 0; u < 2 * R; ++u) {
-      const int zs = min(max(z0 - R + u, 0), nz - 1);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) ring[c][u] = __ldg(col + c * N + zs * nxy);
-    }
-    const bool xyedge = ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1;
-    for (int zb = z0; zb < z1; zb += RD) {
-#pragma unroll
-      for (int u = 0; u < RD; ++u) {
-        const int z = zb + u;
-        if (z < z1) {
-          const int zs = min(z + R, nz - 1);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) ring[c][(u + 2 * R) % RD] = __ldg(col + c * N + zs * nxy);
-          const int i = z * nxy + oy * nx + ox;
-          const bool edge = a.epilogue && (xyedge || z == 0 || z == nz - 1);
-          float nrm2 = 0.0f;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int j = 0; j < K; ++j) acc = fmaf(a.k[2][j], ring[c][(u + j) % RD], acc);
-            if (a.epilogue) {
-              if (edge) acc = 0.0f;
-              else if (a.w2 != 0.0f) acc = acc * a.w1 + org[c * N + i] * a.w2;
-            }
-            const float q = acc * a.ih[c];
-            nrm2 += q * q;
-            dst[c * N + i] = acc;
-          }
-          mx = fmaxf(mx, sqrtf(nrm2));
-        }
-      }
-    }
-  }
+  const float mx = smooth_z_column<R>(a, d, blockIdx.x, blockIdx.y, zc, h);
   if (a.do_max) {
     const float bm = block_max_f(mx, red);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
@@ -523,13 +299,15 @@ cudaError_t smooth3_prepare() {
   return e;
 }
 
-void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
-                         int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
-                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s) {
+Smooth3Args make_smooth_args(const float* const* in, float* const* out, const float* const* orig, int halves,
+                             const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
+                             float w2, bool maxnorm, int* radius) {
   const int dim = g.d.dim;
   const int RR = smooth3_radius(dim, R);
   Smooth3Args a;
   memset(&a, 0, sizeof(a));
+  a.in = Ptr2c{{in[0], halves > 1 ? in[1] : in[0]}};
+  a.out = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
   a.orig = Ptr2c{{orig ? orig[0] : nullptr, orig ? (halves > 1 ? orig[1] : orig[0]) : nullptr}};
   for (int ax = 0; ax < 3; ++ax) {
     a.ih[ax] = (float)(1.0 / g.sp[ax]);
@@ -544,11 +322,25 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   a.do_max = maxnorm ? 1 : 0;
   a.w1 = w1;
   a.w2 = w2;
+  *radius = RR;
+  return a;
+}
+
+int smooth_z_chunk(const Dims& d, int halves, int RR) {
+  const int gx = (d.nx + 31) / 32, gy = (d.ny + 7) / 8;
+  const int target = 148 * 8;
+  const int chunks = std::max(1, (target + gx * gy * halves - 1) / (gx * gy * halves));
+  int zc = (d.nz + chunks - 1) / chunks;
+  return std::min(std::max(zc, 2 * RR + 1), d.nz);
+}
+
+void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
+                         int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
+                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s) {
+  const int dim = g.d.dim;
+  int RR = 1;
+  Smooth3Args a = make_smooth_args(in, dim == 3 ? tmp : out, orig, halves, g, khost, R, epilogue, w1, w2, maxnorm, &RR);
   const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
-  // xy pass: in -> (3-D: tmp, 2-D: out)
-  a.in = Ptr2c{{in[0], halves > 1 ? in[1] : in[0]}};
-  float* const* xyout = dim == 3 ? tmp : out;
-  a.out = Ptr2{{xyout[0], halves > 1 ? xyout[1] : xyout[0]}};
   const dim3 gxy(gx, gy, g.d.nz * halves);
   const size_t smem = smooth3_smem_floats(dim, RR) * 4;
   count_launch();
@@ -580,12 +372,8 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   // z pass: tmp -> out with the epilogue
   a.in = Ptr2c{{tmp[0], halves > 1 ? tmp[1] : tmp[0]}};
   a.out = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
-  const int target = 148 * 8;
-  const int chunks = std::max(1, (target + gx * gy * halves - 1) / (gx * gy * halves));
-  int zc = (g.d.nz + chunks - 1) / chunks;
-  zc = std::min(std::max(zc, 2 * RR + 1), g.d.nz);
-  a.ZC = zc;
-  const dim3 gz(gx, gy, ((g.d.nz + zc - 1) / zc) * halves);
+  a.ZC = smooth_z_chunk(g.d, halves, RR);
+  const dim3 gz(gx, gy, ((g.d.nz + a.ZC - 1) / a.ZC) * halves);
   count_launch();
 #define SYNX_SZ(RV)                                    \
   case RV:                                             \
@@ -609,6 +397,7 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   }
 #undef SYNX_SZ
 }
+
 
 // Single-axis fallback for kernels too wide for the fused pass.
 template <int DIM>
@@ -678,76 +467,37 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
                                             maxnorm ? 1 : 0, ih[0], ih[1], ih[2], ctl);
 }
 
+
 // ------------------------------------------------------------------------------------------
-// Composition out = w + s * d(x + w), s = eta / max||d/spacing|| (SyN's update scaling fused).
-// Reads w only at its own voxel, so it runs in place (out == w).
+// Composition (one tile per block, both halves by blockIdx.z).
 // ------------------------------------------------------------------------------------------
 template <int DIM, bool DIAG>
-__global__ void __launch_bounds__(256) k_compose(Ptr2c dd, Ptr2c ww, Ptr2 oo, Dims d, int zb, int halves, Affine m,
-                                                 double eta, IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_compose(const ComposeArgs a, int halves, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
-  const Coord3 c3 = coord3(d, zb, halves);
-  if (!c3.ok) return;
-  const int h = c3.h;
-  const float* __restrict__ D = (h ? dd.p[1] : dd.p[0]);
-  const float* W = (h ? ww.p[1] : ww.p[0]);
-  float* O = (h ? oo.p[1] : oo.p[0]);
-  float scale = 1.0f;
-  if (eta > 0.0) {
-    const float mx = __uint_as_float(ctl->maxnorm[h]);
-    scale = mx > 0.0f ? (float)(eta / (double)mx) : (float)eta;
-  }
-  const int N = (int)d.N, nxy = d.nx * d.ny;
-  const float fx = (float)c3.x, fy = (float)c3.y;
-  const int i0 = c3.z0 * nxy + c3.y * d.nx + c3.x;
-  float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
-  if (c3.z0 < c3.z1) {
-    n0 = W[i0];
-    n1 = W[N + i0];
-    n2 = DIM == 3 ? W[2 * N + i0] : 0.0f;
-  }
-  for (int z = c3.z0; z < c3.z1; ++z) {
-    const int i = z * nxy + c3.y * d.nx + c3.x;
-    const float w0 = n0, w1 = n1, w2 = n2;
-    if (z + 1 < c3.z1) {  // next slice's warp vector, loaded ahead of this slice's gathers
-      n0 = W[i + nxy];
-      n1 = W[N + i + nxy];
-      n2 = DIM == 3 ? W[2 * N + i + nxy] : 0.0f;
-    }
-    float cx, cy, cz;
-    map_point<DIM, DIAG>(m, fx, fy, (float)z, w0, w1, w2, cx, cy, cz);
-    if (inside_buffer<DIM>(d, cx, cy, cz)) {
-      const Cell c = make_cell<DIM>(d, cx, cy, cz);
-      O[i] = fmaf(scale, lerp_at<DIM>(D, c), w0);
-      O[N + i] = fmaf(scale, lerp_at<DIM>(D + N, c), w1);
-      if (DIM == 3) O[2 * N + i] = fmaf(scale, lerp_at<DIM>(D + 2 * N, c), w2);
-    } else {
-      O[i] = w0;
-      O[N + i] = w1;
-      if (DIM == 3) O[2 * N + i] = w2;
-    }
-  }
+  const int gz = gridDim.z / halves;
+  const int h = blockIdx.z / gz;
+  compose_tile<DIM, DIAG>(a, ctl, h, blockIdx.x, blockIdx.y, blockIdx.z - h * gz);
 }
 
 void launch_compose(const float* const* d, const float* const* w, float* const* out, int halves, const GridInfo& g,
                     float eta, IterCtl* ctl, cudaStream_t s) {
   count_launch();
-  Ptr2c pd{{d[0], halves > 1 ? d[1] : d[0]}};
-  Ptr2c pw{{w[0], halves > 1 ? w[1] : w[0]}};
-  Ptr2 po{{out[0], halves > 1 ? out[1] : out[0]}};
-  Affine a = make_affine(g, g);
+  ComposeArgs a;
+  a.d = Ptr2c{{d[0], halves > 1 ? d[1] : d[0]}};
+  a.w = Ptr2c{{w[0], halves > 1 ? w[1] : w[0]}};
+  a.o = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
+  a.g = g.d;
+  a.m = make_affine(g, g);
+  a.eta = (double)eta;
   const Map3 m = map3(g.d, halves);
-  const bool dg = affine_diag(a);
+  a.zb = m.zb;
+  const bool dg = affine_diag(a.m);
   if (g.d.dim == 3) {
-    if (dg)
-      k_compose<3, true><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
-    else
-      k_compose<3, false><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+    if (dg) k_compose<3, true><<<m.grid, 256, 0, s>>>(a, halves, ctl);
+    else k_compose<3, false><<<m.grid, 256, 0, s>>>(a, halves, ctl);
   } else {
-    if (dg)
-      k_compose<2, true><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
-    else
-      k_compose<2, false><<<m.grid, 256, 0, s>>>(pd, pw, po, g.d, m.zb, halves, a, (double)eta, ctl);
+    if (dg) k_compose<2, true><<<m.grid, 256, 0, s>>>(a, halves, ctl);
+    else k_compose<2, false><<<m.grid, 256, 0, s>>>(a, halves, ctl);
   }
 }
 
@@ -758,62 +508,31 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
 // (InvCtl.exec), so all max_iter+1 launches are enqueued up front and the ones past
 // convergence return at once.
 // ------------------------------------------------------------------------------------------
-struct InvParams {
-  float A[9];
-  float ih[3];
-  int k, max_iter, phase, stop_aware, zb, halves;
+struct InvLaunch {
+  int k, max_iter, phase, stop_aware, halves;
   double mean_tol, max_tol;
 };
 
 template <int DIM, bool DIAG>
-__device__ __forceinline__ void residual(const float* __restrict__ phi, const Dims& d, const float* A, float fx,
-                                         float fy, float fz, const float p[3], float e[3]) {
-  float cx, cy, cz;
-  if (DIAG) {
-    cx = fmaf(A[0], p[0], fx);
-    cy = fmaf(A[4], p[1], fy);
-    cz = DIM == 3 ? fmaf(A[8], p[2], fz) : 0.0f;
-  } else {
-  cx = fx + A[0] * p[0] + A[1] * p[1];
-  cy = fy + A[3] * p[0] + A[4] * p[1];
-  cz = 0.0f;
-  if (DIM == 3) {
-    cx += A[2] * p[2];
-    cy += A[5] * p[2];
-    cz = fz + A[6] * p[0] + A[7] * p[1] + A[8] * p[2];
-  }
-  }
-  e[0] = p[0];
-  e[1] = p[1];
-  e[2] = DIM == 3 ? p[2] : 0.0f;
-  if (inside_buffer<DIM>(d, cx, cy, cz)) {
-    const Cell c = make_cell<DIM>(d, cx, cy, cz);
-    const int N = (int)d.N;
-    e[0] += lerp_at<DIM>(phi, c);
-    e[1] += lerp_at<DIM>(phi + N, c);
-    if (DIM == 3) e[2] += lerp_at<DIM>(phi + 2 * N, c);
-  }
-}
-
-template <int DIM, bool DIAG>
-__global__ void __launch_bounds__(256, 4) k_invert_step(Ptr2c phis, Ptr2 psis, Dims d, InvParams P, IterCtl* ctl,
-                                                     double* __restrict__ psum, float* __restrict__ pmax, int pcap) {
-  if (P.stop_aware && ctl->stop) return;
+__global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaunch L, IterCtl* ctl,
+                                                        double* __restrict__ psum, float* __restrict__ pmax,
+                                                        int pcap) {
+  if (L.stop_aware && ctl->stop) return;
   __shared__ double redd[32];
   __shared__ float redf[32];
   __shared__ int am_last;
-  const Coord3 c3 = coord3(d, P.zb, P.halves);
-  const int h = c3.h;
-  InvCtl& C = ctl->inv[P.phase][h];
-  const float* __restrict__ phi = (h ? phis.p[1] : phis.p[0]);
-  float* __restrict__ psi = (h ? psis.p[1] : psis.p[0]);
-  const int k = P.k;
+  const int gz = gridDim.z / L.halves;
+  const int h = blockIdx.z / gz;
+  const int bz = blockIdx.z - h * gz;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * bz);
+  InvCtl& C = ctl->inv[L.phase][h];
+  const int k = L.k;
   bool apply = false, stats = true;
   float eps = 0.0f, lim = 0.0f;
   if (k > 0) {
     const int s = k & 1;
     if (!C.exec[s]) {
-      if (c3.bid == 0 && threadIdx.x == 0) C.exec[s ^ 1] = 0;
+      if (bid == 0 && threadIdx.x == 0) C.exec[s ^ 1] = 0;
       return;
     }
     apply = true;
@@ -821,76 +540,22 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(Ptr2c phis, Ptr2 psis, D
     const float mx = C.maxv[s];
     const double mean = C.mean[s];
     lim = eps * mx;
-    stats = (k + 1 <= P.max_iter) && ((double)mx > P.max_tol) && (mean > P.mean_tol);
-    if (!stats && c3.bid == 0 && threadIdx.x == 0) {
+    stats = (k + 1 <= L.max_iter) && ((double)mx > L.max_tol) && (mean > L.mean_tol);
+    if (!stats && bid == 0 && threadIdx.x == 0) {
       C.exec[s ^ 1] = 0;
       C.iters = k;
     }
   }
-  if (!stats && !c3.ok) return;
-  const int N = (int)d.N, nxy = d.nx * d.ny;
   double acc = 0.0;
   float mxl = 0.0f;
-  if (c3.ok) {
-    const float fx = (float)c3.x, fy = (float)c3.y;
-    const bool xyedge = c3.x == 0 || c3.x == d.nx - 1 || c3.y == 0 || c3.y == d.ny - 1;
-    // the iterate of the next slice is loaded before this slice's gathers (one dependent
-    // memory round trip per slice instead of two)
-    const int i0 = c3.z0 * nxy + c3.y * d.nx + c3.x;
-    float pn[3] = {0.0f, 0.0f, 0.0f};
-    if (c3.z0 < c3.z1) {
-      pn[0] = psi[i0];
-      pn[1] = psi[N + i0];
-      pn[2] = DIM == 3 ? psi[2 * N + i0] : 0.0f;
-    }
-    for (int z = c3.z0; z < c3.z1; ++z) {
-      const int i = z * nxy + c3.y * d.nx + c3.x;
-      const float fz = (float)z;
-      float p[3] = {pn[0], pn[1], pn[2]};
-      if (z + 1 < c3.z1) {
-        pn[0] = psi[i + nxy];
-        pn[1] = psi[N + i + nxy];
-        pn[2] = DIM == 3 ? psi[2 * N + i + nxy] : 0.0f;
-      }
-      float e[3];
-      if (apply) {
-        residual<DIM, DIAG>(phi, d, P.A, fx, fy, fz, p, e);
-        float s2 = 0.0f;
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          const float v = e[c] * P.ih[c];
-          s2 += v * v;
-        }
-        const float nrm = sqrtf(s2);
-        const float f = nrm > lim ? lim / nrm : 1.0f;
-        const bool edge = xyedge || (DIM == 3 && (z == 0 || z == d.nz - 1));
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) p[c] = edge ? 0.0f : p[c] + ((-e[c]) * f) * eps;
-        psi[i] = p[0];
-        psi[N + i] = p[1];
-        if (DIM == 3) psi[2 * N + i] = p[2];
-      }
-      if (stats) {
-        residual<DIM, DIAG>(phi, d, P.A, fx, fy, fz, p, e);
-        float s2 = 0.0f;
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) {
-          const float v = e[c] * P.ih[c];
-          s2 += v * v;
-        }
-        const float nrm = sqrtf(s2);
-        acc += (double)nrm;
-        mxl = fmaxf(mxl, nrm);
-      }
-    }
-  }
+  invert_tile<DIM, DIAG>(a, h, blockIdx.x, blockIdx.y, bz, apply, stats, eps, lim, acc, mxl);
   if (!stats) return;
   const double bs = block_sum_d(acc, redd);
   const float bm = block_max_f(mxl, redf);
-  const int nb = gridDim.x * gridDim.y * (gridDim.z / P.halves);
+  const int nb = gridDim.x * gridDim.y * gz;
   if (threadIdx.x == 0) {
-    psum[h * pcap + c3.bid] = bs;
-    pmax[h * pcap + c3.bid] = bm;
+    psum[h * pcap + bid] = bs;
+    pmax[h * pcap + bid] = bm;
     __threadfence();
     const unsigned t = atomicAdd(&C.counter, 1u);
     am_last = (t == (unsigned)nb - 1);
@@ -908,7 +573,7 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(Ptr2c phis, Ptr2 psis, D
     m = block_max_f(m, redf);
     if (threadIdx.x == 0) {
       const int s1 = (k + 1) & 1;
-      C.mean[s1] = s / (double)N;
+      C.mean[s1] = s / (double)a.g.N;
       C.maxv[s1] = m;
       C.exec[s1] = 1;
       C.iters = k;
@@ -920,40 +585,37 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(Ptr2c phis, Ptr2 psis, D
 constexpr int kInvTarget = 148 * 24;  // blocks: short per-thread z walks, small last-wave tail
 int inv_blocks(const GridInfo& g) { return map3(g.d, 2, kInvTarget).nblocks; }
 
+InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb) {
+  InvArgs a;
+  a.phi = Ptr2c{{phi[0], halves > 1 ? phi[1] : phi[0]}};
+  a.psi = Ptr2{{psi[0], halves > 1 ? psi[1] : psi[0]}};
+  a.g = g.d;
+  const Affine m = make_affine(g, g);
+  for (int j = 0; j < 9; ++j) a.A[j] = m.A[j];
+  for (int j = 0; j < 3; ++j) a.ih[j] = (float)(1.0 / g.sp[j]);
+  a.zb = zb;
+  return a;
+}
+
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
                         bool stop_aware) {
   count_launch();
-  Ptr2c pp{{phi[0], halves > 1 ? phi[1] : phi[0]}};
-  Ptr2 ps{{psi[0], halves > 1 ? psi[1] : psi[0]}};
-  InvParams P;
-  Affine a = make_affine(g, g);
-  for (int j = 0; j < 9; ++j) P.A[j] = a.A[j];
-  for (int j = 0; j < 3; ++j) P.ih[j] = (float)(1.0 / g.sp[j]);
-  // the block decomposition is the same for one or two halves, so the partial buffers sized
-  // by inv_blocks() fit either
+  // the block decomposition is the same for one or two halves, so the partial buffers sized by
+  // inv_blocks() fit either
   const Map3 m2 = map3(g.d, 2, kInvTarget);
   Map3 m = m2;
   m.grid.z = (m2.grid.z / 2) * halves;
-  P.k = k;
-  P.max_iter = max_iter;
-  P.phase = phase;
-  P.stop_aware = stop_aware ? 1 : 0;
-  P.zb = m.zb;
-  P.halves = halves;
-  P.mean_tol = mean_tol;
-  P.max_tol = max_tol;
-  const bool dg = affine_diag(a);
+  const InvArgs a = make_inv_args(phi, psi, halves, g, m.zb);
+  InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, mean_tol, max_tol};
+  Affine am = make_affine(g, g);
+  const bool dg = affine_diag(am);
   if (g.d.dim == 3) {
-    if (dg)
-      k_invert_step<3, true><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
-    else
-      k_invert_step<3, false><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+    if (dg) k_invert_step<3, true><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    else k_invert_step<3, false><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   } else {
-    if (dg)
-      k_invert_step<2, true><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
-    else
-      k_invert_step<2, false><<<m.grid, 256, 0, s>>>(pp, ps, g.d, P, ctl, pb.sum, pb.maxv, pb.capacity);
+    if (dg) k_invert_step<2, true><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    else k_invert_step<2, false><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   }
 }
 
@@ -962,40 +624,14 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
 // ------------------------------------------------------------------------------------------
 __global__ void k_converge(IterCtl* ctl, LogDev log, double threshold, int window) {
   if (ctl->stop) return;
-  const int k = ctl->iter;
-  const double v = ctl->metric;
-  ctl->total_abs += fabs(v);
-  const int W = window < 2 ? 2 : (window > kMaxWindow ? kMaxWindow : window);
-  ctl->energies[k % W] = v;
-  const int k1 = k + 1;
-  double conv = DBL_MAX;
-  if (k1 >= W) {
-    double num0 = 0, den0 = 0, num1 = 0, den1 = 0;
-    for (int j = 0; j < W; ++j) {
-      const double u = (double)j / (double)(W - 1);
-      const double z = ctl->energies[(k1 - W + j) % W] / ctl->total_abs;
-      const double w0 = 1.0 - u, w1 = u, ws = w0 * w0 + w1 * w1;
-      num0 += w0 * w0 * (w0 * z / ws);
-      den0 += w0 * w0;
-      num1 += w1 * w1 * (w1 * z / ws);
-      den1 += w1 * w1;
-    }
-    const double c0 = den0 > 0 ? num0 / den0 : 0.0, c1 = den1 > 0 ? num1 / den1 : 0.0;
-    conv = -(c1 - c0);
-  }
-  if (k < log.cap) {
-    log.metric[k] = v;
-    log.conv[k] = conv;
-    log.inv_iters[k] = ctl->inv[0][0].iters + ctl->inv[0][1].iters + ctl->inv[1][0].iters + ctl->inv[1][1].iters;
-  }
-  ctl->iter = k1;
-  if (conv < threshold) ctl->stop = 1;
+  converge_step(ctl, log, threshold, window);
 }
 
 void launch_converge(IterCtl* ctl, LogDev log, double threshold, int window, cudaStream_t s) {
   count_launch();
   k_converge<<<1, 1, 0, s>>>(ctl, log, threshold, window);
 }
+
 
 // ------------------------------------------------------------------------------------------
 // Field resampling between level grids (linear, 0 outside), up to 4 fields per launch.

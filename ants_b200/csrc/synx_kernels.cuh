@@ -33,6 +33,10 @@ struct IterCtl {
   double total_abs;           // running sum of |metric| over the level
   double energies[kMaxWindow];
   InvCtl inv[2][2];           // [phase A (psi), phase B (phi)][half]
+  unsigned bar_count;         // grid barrier of the persistent level kernel: arrivals,
+  unsigned bar_gen;           // generation,
+  int bar_err;                // and 1 if a wait gave up (the kernel then returns)
+  int pad1;
 };
 
 struct LogDev {

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libsynx.so")
 SYNX_MAX_LEVELS = 8
 SYNX_F_PROFILE_EVENTS = 0x1
 SYNX_F_USE_GRAPHS = 0x2
+SYNX_F_NO_PERSISTENT = 0x4
 
 ERRORS = {-1: "invalid argument", -2: "bad state", -3: "CUDA error", -4: "out of device memory", -5: "unsupported"}
 

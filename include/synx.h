@@ -84,6 +84,7 @@ typedef struct synx_params {
 
 #define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
 #define SYNX_F_USE_GRAPHS 0x2     /* capture each iteration as a CUDA graph and replay it */
+#define SYNX_F_NO_PERSISTENT 0x4 /* run small levels as separate kernels too (no persistent level kernel) */
 
 /* Fill *p with antsRegistration's defaults for a SyN stage of dimension dim
  * (SyN[0.1,3,0], CC radius 4, one level, 1 iteration, shrink 1, sigma 0 vox). */

@@ -14,7 +14,7 @@ import pytest
 
 import oracle as O
 from ants_b200 import phantoms
-from ants_b200.synx import SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage
+from ants_b200.synx import SYNX_F_NO_PERSISTENT, SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage
 
 pytestmark = pytest.mark.gpu
 
@@ -59,12 +59,18 @@ SCHEDULES = [
 ]
 
 
+# "persistent": levels that fit run as one cooperative kernel per level (the default);
+# "kernels": the same levels as one launch per phase (SYNX_F_NO_PERSISTENT)
+PATHS = {"persistent": SYNX_F_USE_GRAPHS, "kernels": SYNX_F_USE_GRAPHS | SYNX_F_NO_PERSISTENT}
+
+
+@pytest.mark.parametrize("path", sorted(PATHS))
 @pytest.mark.parametrize("dim,size,radius,iters,shrink,sigmas", SCHEDULES)
-def test_multilevel_matches_oracle(cuda, dim, size, radius, iters, shrink, sigmas):
+def test_multilevel_matches_oracle(cuda, dim, size, radius, iters, shrink, sigmas, path):
     f, m = make_pair(dim, size, seed=7)
     g = Geom(size)
     P = SyNParams(dim=dim, cc_radius=radius, iterations=iters, shrink_factors=shrink, smoothing_sigmas=sigmas,
-                  convergence_threshold=1e-12)
+                  convergence_threshold=1e-12, flags=PATHS[path])
     with SyNStage(P) as st:
         st.set_images(f, g, m, g)
         st.run()
@@ -115,6 +121,29 @@ def test_graph_replay_is_bit_identical_and_deterministic(cuda):
         np.testing.assert_array_equal(o[0][0], outs[0][0][0])
         np.testing.assert_array_equal(o[0][1], outs[0][0][1])
         assert o[1] == outs[0][1]
+
+
+@pytest.mark.parametrize("dim,size,radius", [(2, (80, 66), 1), (2, (50, 61), 7), (3, (26, 23, 29), 5)])
+def test_persistent_level_radii_and_repeatability(cuda, dim, size, radius):
+    # odd sizes and the extreme CC radii through the persistent level kernel; two runs give the
+    # same bits (its reductions are ordered), and both agree with the per-phase launches
+    f, m = make_pair(dim, size, seed=11)
+    g = Geom(size)
+    outs = []
+    for flags in (PATHS["persistent"], PATHS["persistent"], PATHS["kernels"]):
+        P = SyNParams(dim=dim, cc_radius=radius, iterations=(8, 5), shrink_factors=(2, 1),
+                      smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12, flags=flags)
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.run()
+            outs.append((st.fields(), [r.metric for r in st.log()], st.output_geom()))
+    np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
+    np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
+    assert outs[0][1] == outs[1][1]
+    np.testing.assert_allclose(outs[0][1], outs[2][1], atol=2e-3)
+    sp = outs[0][2].spacing
+    for a, b in zip(outs[0][0], outs[2][0]):
+        assert rms_vox(planes(a), planes(b), sp) <= 0.05
 
 
 def test_convergence_stops_level_early(cuda):
