@@ -560,14 +560,17 @@ constexpr long long kPersistentMaxVoxels = 2500000;
 
 bool use_persistent(synx_ctx* c, const GridInfo& g, bool profile, int* blocks) {
   if (profile || (c->P.flags & SYNX_F_NO_PERSISTENT)) return false;
-  if (g.d.N > kPersistentMaxVoxels || c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
+  const long long max_vox = c->P.persistent_max_voxels > 0 ? c->P.persistent_max_voxels : kPersistentMaxVoxels;
+  if (g.d.N > max_vox || c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
   int rs = 1;
   for (int a = 0; a < c->D; ++a) rs = std::max(rs, c->R_upd[a]);
   if (rs > kLevelMaxSmoothRadius) return false;
   if (c->coop_max <= 0) c->coop_max = level_max_blocks(c->D, c->P.cc_radius, kLevelMaxSmoothRadius, c->device);
   if (c->coop_max <= 0) return false;
-  long long want = (g.d.N + 2047) / 2048;
-  want = std::max<long long>(want, 16);
+  // every co-resident block: the phases are latency-bound at these sizes, so more warps in
+  // flight shorten each phase by more than the wider barrier costs (measured at 13k-900k voxels)
+  long long want = c->coop_max;
+  if (c->P.persistent_blocks > 0) want = c->P.persistent_blocks;
   *blocks = (int)std::min<long long>(want, std::min(c->coop_max, c->inv_cap));
   return *blocks > 0;
 }

@@ -59,7 +59,9 @@ class SynxParams(C.Structure):
         ("flags", C.c_int32),
         ("inv_mean_tol", C.c_double),
         ("inv_max_tol", C.c_double),
-        ("reserved", C.c_int32 * 8),
+        ("persistent_blocks", C.c_int32),
+        ("persistent_max_voxels", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -214,6 +216,8 @@ class SyNParams:
     inv_mean_tol: float = 0.001
     inv_max_tol: float = 0.1
     flags: int = 0
+    persistent_blocks: int = 0  # launch shape of the persistent level kernel (0: automatic)
+    persistent_max_voxels: int = 0  # largest level it runs (0: automatic)
 
     def to_c(self) -> SynxParams:
         n = len(self.iterations)
@@ -242,6 +246,8 @@ class SyNParams:
         p.inv_mean_tol = self.inv_mean_tol
         p.inv_max_tol = self.inv_max_tol
         p.flags = self.flags
+        p.persistent_blocks = self.persistent_blocks
+        p.persistent_max_voxels = self.persistent_max_voxels
         return p
 
 

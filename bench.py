@@ -12,9 +12,12 @@ A voxel-iteration is one voxel of a level grid processed by one full SyN iterati
               flushed (256 MB write) between steps.
   e2e      -- the same stage through the C ABI with pinned host buffers: host->device images and
               device->host forward and inverse fields inside the timed region.
-  roofline -- the fixed-point inverse (the largest kernel class) timed with CUDA events around its
-              launches in a second, event-instrumented pass over the same K steps; algorithmic bytes
-              = executed sub-iterations x voxels x 36 B.
+  roofline -- the persistent level kernel (k_level: one cooperative launch runs every iteration of
+              a pyramid level; the largest kernel of the step) on its largest launch, the 91x109x91
+              level, timed with CUDA events on the stage's stream inside the timed region.
+              Algorithmic bytes = voxels x (iterations x 176 B + inverse half-field sub-iterations
+              x 36 B), the compulsory traffic of each step (BYTES_PER_ITER_VOXEL below);
+              `achieved_whole_step` applies the same model to all levels over the step time.
   --impl reference -- the CPU path (the oracle restatement of the reference arithmetic, all host
               threads) on a bounded sample of the same workload: one full-resolution iteration per step.
 
@@ -44,10 +47,20 @@ STAGE = dict(cc_radius=4, iterations=(100, 70, 50, 20), shrink_factors=(8, 4, 2,
              convergence_window=10)
 WORKLOAD = ("3-D SyN[0.1,3,0] + CC[r=4], 182x218x182 at 1 mm, shrink 8x4x2x1, sigmas 3x2x1x0 vox, "
             "iterations 100x70x50x20, convergence [1e-12,10]")
+# Compulsory (algorithmic) bytes of one 3-D SyN iteration per voxel, f32 fields of 12 B, every
+# operand counted once per step:
+#   warp both images + CC + derivatives: read 2 inverse half-fields, 2 image samples,
+#     write 2 derivative fields                                                   4c + 8 =  56
+#   smooth both update fields + max norm: read 2, write 2                          4c     =  48
+#   scale + compose both halves: read 2 updates, read + write 2 half-fields        6c     =  72
+# plus 3c = 36 B per voxel for each fixed-point inverse sub-iteration of one half-field
+# (read psi, gather phi, write psi).
+BYTES_PER_ITER_VOXEL = 176
 BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi
-# DRAM bytes per full-resolution k_invert_step launch (apply + statistics, both halves) from the
-# ncu capture summarised in profiles/k_invert_step_182x218x182.md
-INV_TRAFFIC_BYTES = None
+ROOF_LEVEL = 2  # the 91x109x91 level: the largest k_level launch
+# DRAM bytes (read + write) of that k_level launch, from the ncu capture summarised in
+# profiles/k_level_91x109x91.md (5.230 GB read + 6.070 GB written)
+LEVEL_TRAFFIC_BYTES = 11.300e9
 
 
 def dist_env():
@@ -218,6 +231,7 @@ def main(argv=None) -> int:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = S.launch_count()
+    stage.reset_profile()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     vox_iters = 0
     its = {}
@@ -237,21 +251,7 @@ def main(argv=None) -> int:
     t_total, vox_all = replicas.aggregate(sum(step_ms) / 1000.0, vox_iters, dev)
     value = vox_all / t_total
 
-    # ---- event-instrumented pass over the same workload: time of the fixed-point inverse ----
-    pstage = S.SyNStage(S.SyNParams(dim=3, flags=S.SYNX_F_PROFILE_EVENTS, **STAGE), device=local,
-                        stream=stream.cuda_stream)
-    step_device(pstage)
-    pstage.reset_profile()
-    pev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    pev[0].record(stream)
-    for k in range(args.steps):
-        step_device(pstage)
-    pev[1].record(stream)
-    torch.cuda.synchronize()
-    prof = pstage.profile()
-    prof_levels = pstage.level_profile()
-    prof_total_ms = pev[0].elapsed_time(pev[1])
-    pstage.close()
+    prof_levels = stage.level_profile()
 
     # ---- end to end through the C ABI with pinned host buffers ----
     Fh = torch.from_numpy(fixed).pin_memory().numpy()
@@ -279,22 +279,25 @@ def main(argv=None) -> int:
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
-        roof = None
-        if prof["inverse_ms"] > 0:
-            bytes_alg = prof["inverse_voxels"] * BYTES_PER_INV_VOXEL
-            achieved = bytes_alg / (prof["inverse_ms"] / 1000.0) / 1e9
-            full = prof_levels[-1]
-            full_ach = (full["inverse_subiterations"] * full["voxels"] * BYTES_PER_INV_VOXEL /
-                        (full["inverse_ms"] / 1000.0) / 1e9) if full["inverse_ms"] > 0 else None
-            roof = {"kernel": "k_invert_step (fixed-point inverse sub-iteration, all levels)", "bound": "hbm",
-                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_source": peak_kind, "traffic": INV_TRAFFIC_BYTES,
-                    "algorithmic_bytes_per_half_field_voxel": BYTES_PER_INV_VOXEL,
-                    "achieved_full_resolution_level": full_ach,
-                    "frac_full_resolution_level": (full_ach / peak) if full_ach else None,
-                    "share_of_instrumented_step": prof["inverse_ms"] / prof_total_ms,
-                    "cc_share_of_instrumented_step": prof["cc_ms"] / prof_total_ms,
-                    "level_ms_per_step": [round(l["iterate_ms"] / args.steps, 3) for l in prof_levels]}
+        lv = prof_levels[ROOF_LEVEL]
+        alg = lv["voxels"] * (lv["iterations"] * BYTES_PER_ITER_VOXEL + lv["inverse_subiterations"] * BYTES_PER_INV_VOXEL)
+        achieved = alg / (lv["iterate_ms"] / 1000.0) / 1e9
+
+        def level_gbs(l):
+            b = l["voxels"] * (l["iterations"] * BYTES_PER_ITER_VOXEL + l["inverse_subiterations"] * BYTES_PER_INV_VOXEL)
+            return round(b / (l["iterate_ms"] / 1000.0) / 1e9, 1) if l["iterate_ms"] > 0 else None
+
+        roof = {"kernel": "k_level (persistent level kernel), 91x109x91 level", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": LEVEL_TRAFFIC_BYTES,
+                "algorithmic_bytes_per_launch": alg / args.steps, "launch_ms": lv["iterate_ms"] / args.steps,
+                "bytes_per_voxel_iteration": BYTES_PER_ITER_VOXEL, "bytes_per_inverse_subiteration_voxel": BYTES_PER_INV_VOXEL,
+                "achieved_gbs_per_level": [level_gbs(l) for l in prof_levels],
+                "level_ms_per_step": [round(l["iterate_ms"] / args.steps, 3) for l in prof_levels],
+                "level_voxels": [l["voxels"] for l in prof_levels],
+                "achieved_whole_step": sum(
+                    l["voxels"] * (l["iterations"] * BYTES_PER_ITER_VOXEL + l["inverse_subiterations"] * BYTES_PER_INV_VOXEL)
+                    for l in prof_levels) / t_total / 1e9}
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
             threads = os.cpu_count() or 1

@@ -79,7 +79,9 @@ typedef struct synx_params {
   int32_t flags;             /* SYNX_F_* */
   double inv_mean_tol;
   double inv_max_tol;
-  int32_t reserved[8];
+  int32_t persistent_blocks;     /* grid of the persistent level kernel; 0: automatic */
+  int32_t persistent_max_voxels; /* largest level run by it; 0: automatic (2,500,000) */
+  int32_t reserved[6];
 } synx_params;
 
 #define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
