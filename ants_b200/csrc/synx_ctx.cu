@@ -198,6 +198,10 @@ struct synx_ctx {
   GridInfo cur_grid{};
   std::vector<int32_t> log_level, log_iter, log_inv;
   std::vector<double> log_metric, log_conv;
+  // read-back staging of the running level
+  IterCtl h_ctl{};
+  std::vector<double> h_lm, h_lc;
+  std::vector<int> h_li;
   // canonical buffer assignment (level changes swap field and work buffers)
   float* canon[8] = {};
   // graphs: one executable per level, valid while the arena and grids are unchanged
@@ -259,6 +263,8 @@ int build_levels(synx_ctx* c) {
   return SYNX_OK;
 }
 
+long long level_inv_units(const GridInfo& g);
+
 int allocate(synx_ctx* c) {
   const int D = c->D;
   const long long Nmax = c->Nmax, NI = std::max(c->NF, c->NM);
@@ -267,7 +273,8 @@ int allocate(synx_ctx* c) {
     ccb = std::max(ccb, cc_blocks(g, c->P.cc_radius));
     invb = std::max(invb, inv_blocks(g));
   }
-  invb = std::max(invb, 2048);  // also holds one slot per block of the persistent level kernel
+  invb = std::max(invb, 2048);
+  for (auto& g : c->lv) invb = (int)std::max<long long>(invb, level_inv_units(g));  // level kernel: one slot per tile
   // step entry points on arbitrary grids reuse nothing from here
   const int coeff_cap = 1024;
   int max_iters = 1;
@@ -558,20 +565,33 @@ void enqueue_iteration(synx_ctx* c, bool profile) {
 // path.
 constexpr long long kPersistentMaxVoxels = 2500000;
 
-bool use_persistent(synx_ctx* c, const GridInfo& g, bool profile, int* blocks) {
+// Inversion tiles per half-field of the level kernel on grid g (one residual partial slot each).
+long long level_inv_units(const GridInfo& g) {
+  const int zb = level_zb(g.d, 2);
+  return (long long)((g.d.nx + 31) / 32) * ((g.d.ny + 7) / 8) * ((g.d.nz + zb - 1) / zb);
+}
+
+// Whether a level runs in the level kernel (alone or in a batch): the options it implements, and
+// a level small enough that launch latency, not bandwidth, dominates the per-kernel path.
+bool persistent_eligible(synx_ctx* c, const GridInfo& g, bool profile) {
   if (profile || (c->P.flags & SYNX_F_NO_PERSISTENT)) return false;
   const long long max_vox = c->P.persistent_max_voxels > 0 ? c->P.persistent_max_voxels : kPersistentMaxVoxels;
   if (g.d.N > max_vox || c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
   int rs = 1;
   for (int a = 0; a < c->D; ++a) rs = std::max(rs, c->R_upd[a]);
   if (rs > kLevelMaxSmoothRadius) return false;
+  if (c->P.cc_radius < 1 || c->P.cc_radius > 7) return false;
+  return level_inv_units(g) <= c->inv_cap;
+}
+
+bool use_persistent(synx_ctx* c, const GridInfo& g, bool profile, int* blocks) {
+  if (!persistent_eligible(c, g, profile)) return false;
   if (c->coop_max <= 0) c->coop_max = level_max_blocks(c->D, c->P.cc_radius, kLevelMaxSmoothRadius, c->device);
   if (c->coop_max <= 0) return false;
   // every co-resident block: the phases are latency-bound at these sizes, so more warps in
   // flight shorten each phase by more than the wider barrier costs (measured at 13k-900k voxels)
-  long long want = c->coop_max;
-  if (c->P.persistent_blocks > 0) want = c->P.persistent_blocks;
-  *blocks = (int)std::min<long long>(want, std::min(c->coop_max, c->inv_cap));
+  *blocks = c->coop_max;
+  if (c->P.persistent_blocks > 0) *blocks = std::min(c->P.persistent_blocks, c->coop_max);
   return *blocks > 0;
 }
 
@@ -580,12 +600,7 @@ LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
   memset(&A, 0, sizeof(A));
   const int D = c->D;
   const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
-  const int target_units = 2 * 296;  // about two tiles per block of a full cooperative grid
-  auto zb_for = [&](int halves) {
-    int per = std::max(1, target_units / (gx * gy * halves));
-    return std::max(1, (g.d.nz + per - 1) / per);
-  };
-  const int zw = zb_for(1), zc2 = zb_for(2);
+  const int zw = level_zb(g.d, 1), zc2 = level_zb(g.d, 2);
   A.warp = WarpArgs{c->Fs, c->Ms, c->psiF, c->psiM, c->Ft, c->Mt, c->gF.d, c->gM.d, g.d,
                     make_affine(g, c->gF), make_affine(g, c->gM), zw};
   A.cc = make_cc_params(g, c->P.cc_radius);
@@ -644,7 +659,9 @@ LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
   return A;
 }
 
-int run_level_impl(synx_ctx* c, int level) {
+// Level set-up, enqueued on c->stream: pyramid smoothing of both images, resampling (or zeroing)
+// of the four half-fields, reset of the control block.
+int level_begin(synx_ctx* c, int level) {
   if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_run_level: images not set");
   if (level != c->cur_level + 1 || level >= c->P.n_levels)
     return set_err(c, SYNX_E_STATE, "synx_run_level: levels must run in order 0.." + std::to_string(c->P.n_levels - 1));
@@ -672,13 +689,21 @@ int run_level_impl(synx_ctx* c, int level) {
   c->cur_level = level;
   launch_zero_ctl_level(c->ctl, c->stream);
   CUDA_TRY(c, cudaGetLastError());
-  const int iters = c->P.iterations[level];
-  const bool profile = (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0;
-  const bool graphs = (c->P.flags & SYNX_F_USE_GRAPHS) != 0 && !profile;
   c->ev_used = 0;
   c->ev_pairs_inv.clear();
   c->ev_pairs_cc.clear();
   CUDA_TRY(c, cudaEventRecord(c->lev_ev[1], c->stream));
+  return SYNX_OK;
+}
+
+// The level's iterations, enqueued on c->stream: the level kernel, graph replay of one iteration,
+// or plain launches.
+int level_iterate(synx_ctx* c, int level) {
+  const GridInfo& gl = c->lv[level];
+  const int D = c->D;
+  const int iters = c->P.iterations[level];
+  const bool profile = (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0;
+  const bool graphs = (c->P.flags & SYNX_F_USE_GRAPHS) != 0 && !profile;
   int coop_blocks = 0;
   const bool persistent = iters > 0 && use_persistent(c, gl, profile, &coop_blocks);
   if (persistent) {
@@ -709,19 +734,36 @@ int run_level_impl(synx_ctx* c, int level) {
   } else {
     for (int k = 0; k < iters; ++k) enqueue_iteration(c, profile);
   }
+  return SYNX_OK;
+}
+
+// Enqueue the read-back of the level's control block and log (host staging in the context).
+int level_readback(synx_ctx* c, int level) {
+  const int iters = c->P.iterations[level];
   CUDA_TRY(c, cudaEventRecord(c->lev_ev[2], c->stream));
   CUDA_TRY(c, cudaGetLastError());
   // collect the level's log
-  IterCtl hctl;
-  CUDA_TRY(c, cudaMemcpyAsync(&hctl, c->ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, c->stream));
-  std::vector<double> lm(std::max(iters, 1)), lc(std::max(iters, 1));
-  std::vector<int> li(std::max(iters, 1));
+  CUDA_TRY(c, cudaMemcpyAsync(&c->h_ctl, c->ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, c->stream));
+  c->h_lm.assign(std::max(iters, 1), 0.0);
+  c->h_lc.assign(std::max(iters, 1), 0.0);
+  c->h_li.assign(std::max(iters, 1), 0);
   if (iters > 0) {
-    CUDA_TRY(c, cudaMemcpyAsync(lm.data(), c->logdev.metric, 8 * iters, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(lc.data(), c->logdev.conv, 8 * iters, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(li.data(), c->logdev.inv_iters, 4 * iters, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_lm.data(), c->logdev.metric, 8 * iters, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_lc.data(), c->logdev.conv, 8 * iters, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_li.data(), c->logdev.inv_iters, 4 * iters, cudaMemcpyDeviceToHost, c->stream));
   }
-  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return SYNX_OK;
+}
+
+// After the stream has drained: append the level's log and profile.
+int level_finish(synx_ctx* c, int level) {
+  const GridInfo& gl = c->lv[level];
+  const int iters = c->P.iterations[level];
+  const bool profile = (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0;
+  const IterCtl& hctl = c->h_ctl;
+  const std::vector<double>& lm = c->h_lm;
+  const std::vector<double>& lc = c->h_lc;
+  const std::vector<int>& li = c->h_li;
   if (hctl.bar_err)
     return set_err(c, SYNX_E_CUDA, "level " + std::to_string(level) + ": a grid barrier of the level kernel timed out");
   const int done = std::min(hctl.iter, iters);
@@ -767,7 +809,192 @@ int run_level_impl(synx_ctx* c, int level) {
   return SYNX_OK;
 }
 
+int run_level_impl(synx_ctx* c, int level) {
+  int rc = level_begin(c, level);
+  if (!rc) rc = level_iterate(c, level);
+  if (!rc) rc = level_readback(c, level);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return level_finish(c, level);
+}
+
 bool valid_ctx(const synx_ctx* c) { return c != nullptr; }
+
+// Blocks of a batched level launch for pairs with work w[i]: at least one each, the rest in
+// proportion to the work (largest remainders first).  Depends on nothing but w and G.
+std::vector<int> split_blocks(const std::vector<double>& w, int G) {
+  const int n = (int)w.size();
+  std::vector<int> g(n, 1);
+  double W = 0.0;
+  for (double x : w) W += x;
+  int left = G - n;
+  if (left <= 0 || W <= 0.0) return g;
+  std::vector<std::pair<double, int>> frac;
+  int used = 0;
+  for (int i = 0; i < n; ++i) {
+    const double share = left * (w[i] / W);
+    const int whole = (int)share;
+    g[i] += whole;
+    used += whole;
+    frac.push_back({share - whole, i});
+  }
+  std::sort(frac.begin(), frac.end(), [](const auto& a, const auto& b) {
+    return a.first != b.first ? a.first > b.first : a.second < b.second;
+  });
+  for (int k = 0; k < left - used && k < n; ++k) g[frac[k].second] += 1;
+  return g;
+}
+
+}  // namespace
+
+struct synx_batch {
+  int device = 0;
+  std::string err;
+  LevelArgs* d_args = nullptr;  // device staging of the per-pair level arguments
+  int* d_first = nullptr;
+  int cap = 0;
+  std::vector<LevelArgs> h_args;
+  std::vector<int> h_first;
+  cudaEvent_t ev = nullptr;
+};
+
+namespace {
+
+int batch_err(synx_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  g_last_error = msg;
+  return code;
+}
+
+int batch_reserve(synx_batch* b, int n) {
+  if (n <= b->cap) return SYNX_OK;
+  if (b->d_args) cudaFree(b->d_args);
+  if (b->d_first) cudaFree(b->d_first);
+  b->d_args = nullptr;
+  b->d_first = nullptr;
+  b->cap = 0;
+  const int cap = std::max(n, 64);
+  if (cudaMalloc((void**)&b->d_args, sizeof(LevelArgs) * (size_t)cap) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_first, sizeof(int) * (size_t)(cap + 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return batch_err(b, SYNX_E_NOMEM, "synx_batch: staging allocation failed");
+  }
+  b->cap = cap;
+  return SYNX_OK;
+}
+
+// Restores each context's own stream when the batch step ends.
+struct StreamSwap {
+  std::vector<std::pair<synx_ctx*, cudaStream_t>> saved;
+  ~StreamSwap() {
+    for (auto& p : saved) p.first->stream = p.second;
+  }
+};
+
+// One batch step: every context with a level left runs its next level.  Levels that the level
+// kernel serves share cooperative launches (one per dimension and CC radius); the others run
+// their own per-kernel path on the same stream.  One host synchronisation for the whole step.
+int batch_step(synx_batch* b, synx_ctx* const* cs, int n, cudaStream_t s, int* advanced) {
+  if (advanced) *advanced = 0;
+  if (!b || (n > 0 && !cs) || n < 0) return batch_err(b, SYNX_E_ARG, "synx_batch_step: bad arguments");
+  std::vector<synx_ctx*> act;
+  for (int i = 0; i < n; ++i) {
+    synx_ctx* c = cs[i];
+    if (!c) return batch_err(b, SYNX_E_ARG, "synx_batch_step: null context");
+    if (c->device != b->device) return batch_err(b, SYNX_E_ARG, "synx_batch_step: context on another device");
+    if (!c->images_set) return batch_err(b, SYNX_E_STATE, "synx_batch_step: images not set");
+    if (std::find(act.begin(), act.end(), c) != act.end())
+      return batch_err(b, SYNX_E_ARG, "synx_batch_step: a context appears twice");
+    if (c->cur_level + 1 < c->P.n_levels) act.push_back(c);
+  }
+  if (act.empty()) return SYNX_OK;
+  if (cudaSetDevice(b->device) != cudaSuccess) return batch_err(b, SYNX_E_CUDA, "synx_batch_step: cudaSetDevice");
+  StreamSwap swap;
+  for (synx_ctx* c : act) {
+    if (c->stream != s) {
+      // work already queued on the context's own stream comes first
+      if (cudaEventRecord(b->ev, c->stream) != cudaSuccess || cudaStreamWaitEvent(s, b->ev, 0) != cudaSuccess)
+        return batch_err(b, SYNX_E_CUDA, "synx_batch_step: stream ordering failed");
+    }
+    swap.saved.push_back({c, c->stream});
+    c->stream = s;
+  }
+  auto fail = [&](synx_ctx* c, int rc) { return batch_err(b, rc, c->err); };
+  for (synx_ctx* c : act) {
+    const int rc = level_begin(c, c->cur_level + 1);
+    if (rc) return fail(c, rc);
+  }
+  // group the levels the level kernel serves by (dimension, CC radius)
+  std::vector<synx_ctx*> rest;
+  std::vector<std::vector<synx_ctx*>> groups;
+  for (synx_ctx* c : act) {
+    const int l = c->cur_level;
+    const bool profile = (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0;
+    if (c->P.iterations[l] > 0 && persistent_eligible(c, c->lv[l], profile)) {
+      bool placed = false;
+      for (auto& g : groups)
+        if (g[0]->D == c->D && g[0]->P.cc_radius == c->P.cc_radius) {
+          g.push_back(c);
+          placed = true;
+          break;
+        }
+      if (!placed) groups.push_back({c});
+    } else {
+      rest.push_back(c);
+    }
+  }
+  for (auto& grp : groups) {
+    const int D = grp[0]->D, rcc = grp[0]->P.cc_radius;
+    const int Gmax = level_batch_max_blocks(D, rcc, b->device);
+    if (Gmax <= 0) {
+      for (synx_ctx* c : grp) rest.push_back(c);
+      continue;
+    }
+    for (size_t at = 0; at < grp.size(); at += (size_t)Gmax) {
+      const int m = (int)std::min(grp.size() - at, (size_t)Gmax);
+      int rc = batch_reserve(b, m);
+      if (rc) return rc;
+      b->h_args.resize(m);
+      b->h_first.assign(m + 1, 0);
+      std::vector<double> w(m);
+      for (int i = 0; i < m; ++i) {
+        synx_ctx* c = grp[at + i];
+        const int l = c->cur_level;
+        b->h_args[i] = make_level_args(c, c->lv[l], c->P.iterations[l]);
+        w[i] = (double)c->lv[l].d.N * c->P.iterations[l];
+      }
+      const std::vector<int> gsz = split_blocks(w, Gmax);
+      for (int i = 0; i < m; ++i) b->h_first[i + 1] = b->h_first[i] + gsz[i];
+      if (cudaMemcpyAsync(b->d_args, b->h_args.data(), sizeof(LevelArgs) * m, cudaMemcpyHostToDevice, s) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(b->d_first, b->h_first.data(), sizeof(int) * (m + 1), cudaMemcpyHostToDevice, s) !=
+              cudaSuccess)
+        return batch_err(b, SYNX_E_CUDA, "synx_batch_step: argument upload failed");
+      BatchLevelArgs B{b->d_args, b->d_first, m};
+      const cudaError_t e = launch_level_batch(B, D, rcc, b->h_first[m], s);
+      if (e != cudaSuccess)
+        return batch_err(b, SYNX_E_CUDA, std::string("synx_batch_step: batched level launch: ") + cudaGetErrorString(e));
+    }
+  }
+  for (synx_ctx* c : rest) {
+    const int rc = level_iterate(c, c->cur_level);
+    if (rc) return fail(c, rc);
+  }
+  for (synx_ctx* c : act) {
+    const int rc = level_readback(c, c->cur_level);
+    if (rc) return fail(c, rc);
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    const std::string m = cudaGetErrorString(cudaGetLastError());
+    return batch_err(b, SYNX_E_CUDA, "synx_batch_step: " + m);
+  }
+  for (synx_ctx* c : act) {
+    const int rc = level_finish(c, c->cur_level);
+    if (rc) return fail(c, rc);
+  }
+  if (advanced) *advanced = (int)act.size();
+  return SYNX_OK;
+}
 
 }  // namespace
 
@@ -921,6 +1148,51 @@ int synx_set_images_device(synx_ctx* c, const float* F, const synx_geom* gf, con
 int synx_run_level(synx_ctx* c, int level) {
   if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
   return run_level_impl(c, level);
+}
+
+int synx_batch_create(int device, synx_batch** out) {
+  if (!out) return set_err(nullptr, SYNX_E_ARG, "synx_batch_create: null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_err(nullptr, SYNX_E_CUDA, "synx_batch_create: no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return set_err(nullptr, SYNX_E_ARG, "synx_batch_create: bad device index");
+  if (cudaSetDevice(device) != cudaSuccess) return set_err(nullptr, SYNX_E_CUDA, "synx_batch_create: cudaSetDevice");
+  synx_batch* b = new synx_batch();
+  b->device = device;
+  if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+    delete b;
+    return set_err(nullptr, SYNX_E_CUDA, "synx_batch_create: event creation failed");
+  }
+  *out = b;
+  return SYNX_OK;
+}
+
+int synx_batch_destroy(synx_batch* b) {
+  if (!b) return SYNX_OK;
+  cudaSetDevice(b->device);
+  if (b->d_args) cudaFree(b->d_args);
+  if (b->d_first) cudaFree(b->d_first);
+  if (b->ev) cudaEventDestroy(b->ev);
+  delete b;
+  return SYNX_OK;
+}
+
+const char* synx_batch_last_error(const synx_batch* b) { return b ? b->err.c_str() : g_last_error.c_str(); }
+
+int synx_batch_step(synx_batch* b, synx_ctx* const* ctxs, int n, void* cuda_stream, int* advanced) {
+  return batch_step(b, ctxs, n, (cudaStream_t)cuda_stream, advanced);
+}
+
+int synx_batch_run(synx_batch* b, synx_ctx* const* ctxs, int n, void* cuda_stream) {
+  for (;;) {
+    int adv = 0;
+    const int rc = batch_step(b, ctxs, n, (cudaStream_t)cuda_stream, &adv);
+    if (rc) return rc;
+    if (adv == 0) return SYNX_OK;
+  }
 }
 
 int synx_run(synx_ctx* c) {

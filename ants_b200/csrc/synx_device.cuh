@@ -130,6 +130,26 @@ __device__ __forceinline__ float block_max_f(float v, float* sh /* >= 32 */) {
   return r;
 }
 
+// Sum of a double and max of a float over the block in one pass; the results are valid in
+// thread 0 (warp 0).
+__device__ __forceinline__ void block_sum_max(double& s, float& m, double* shd, float* shf) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  s = warp_sum_d(s);
+  m = warp_max_f(m);
+  __syncthreads();
+  if (lane == 0) {
+    shd[w] = s;
+    shf[w] = m;
+  }
+  __syncthreads();
+  if (w == 0) {
+    s = lane < nw ? shd[lane] : 0.0;
+    m = lane < nw ? shf[lane] : 0.0f;
+    s = warp_sum_d(s);
+    m = warp_max_f(m);
+  }
+}
+
 // Non-negative floats order like their bit patterns: atomicMax on the bits is a float max.
 __device__ __forceinline__ void atomic_max_nonneg(unsigned int* addr, float v) {
   atomicMax(addr, __float_as_uint(fmaxf(v, 0.0f)));

@@ -6,25 +6,25 @@
 
 namespace synx {
 
-void* level_kernel_r1(int dim);
-void* level_kernel_r2(int dim);
-void* level_kernel_r3(int dim);
-void* level_kernel_r4(int dim);
-void* level_kernel_r5(int dim);
-void* level_kernel_r6(int dim);
-void* level_kernel_r7(int dim);
+void* level_kernel_r1(int dim, bool batch);
+void* level_kernel_r2(int dim, bool batch);
+void* level_kernel_r3(int dim, bool batch);
+void* level_kernel_r4(int dim, bool batch);
+void* level_kernel_r5(int dim, bool batch);
+void* level_kernel_r6(int dim, bool batch);
+void* level_kernel_r7(int dim, bool batch);
 
 namespace {
 
-void* pick_kernel(int dim, int rcc) {
+void* pick_kernel(int dim, int rcc, bool batch) {
   switch (rcc) {
-    case 1: return level_kernel_r1(dim);
-    case 2: return level_kernel_r2(dim);
-    case 3: return level_kernel_r3(dim);
-    case 4: return level_kernel_r4(dim);
-    case 5: return level_kernel_r5(dim);
-    case 6: return level_kernel_r6(dim);
-    case 7: return level_kernel_r7(dim);
+    case 1: return level_kernel_r1(dim, batch);
+    case 2: return level_kernel_r2(dim, batch);
+    case 3: return level_kernel_r3(dim, batch);
+    case 4: return level_kernel_r4(dim, batch);
+    case 5: return level_kernel_r5(dim, batch);
+    case 6: return level_kernel_r6(dim, batch);
+    case 7: return level_kernel_r7(dim, batch);
     default: return nullptr;
   }
 }
@@ -37,10 +37,8 @@ size_t level_smem_bytes(int dim, int cc_radius, int r_smooth) {
   return std::max(a, b);
 }
 
-int level_max_blocks(int dim, int cc_radius, int r_smooth, int device) {
-  void* k = pick_kernel(dim, cc_radius);
+static int max_blocks_of(void* k, size_t smem, int device) {
   if (!k) return 0;
-  const size_t smem = level_smem_bytes(dim, cc_radius, r_smooth);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
@@ -56,13 +54,40 @@ int level_max_blocks(int dim, int cc_radius, int r_smooth, int device) {
   return per_sm * sms;
 }
 
+int level_max_blocks(int dim, int cc_radius, int r_smooth, int device) {
+  return max_blocks_of(pick_kernel(dim, cc_radius, false), level_smem_bytes(dim, cc_radius, r_smooth), device);
+}
+
 cudaError_t launch_level(const LevelArgs& A, int dim, int cc_radius, int blocks, cudaStream_t s) {
-  void* k = pick_kernel(dim, cc_radius);
+  void* k = pick_kernel(dim, cc_radius, false);
   if (!k) return cudaErrorInvalidValue;
   add_launch_count(1);
   const size_t smem = level_smem_bytes(dim, cc_radius, A.r_smooth);
   void* args[] = {(void*)&A};
   return cudaLaunchCooperativeKernel(k, dim3(blocks), dim3(256), args, smem, s);
+}
+
+int level_batch_max_blocks(int dim, int cc_radius, int device) {
+  return max_blocks_of(pick_kernel(dim, cc_radius, true), level_smem_bytes(dim, cc_radius, kLevelMaxSmoothRadius),
+                       device);
+}
+
+cudaError_t launch_level_batch(const BatchLevelArgs& B, int dim, int cc_radius, int blocks, cudaStream_t s) {
+  void* k = pick_kernel(dim, cc_radius, true);
+  if (!k || B.npairs < 1 || blocks < B.npairs) return cudaErrorInvalidValue;
+  add_launch_count(1);
+  const size_t smem = level_smem_bytes(dim, cc_radius, kLevelMaxSmoothRadius);
+  void* args[] = {(void*)&B};
+  return cudaLaunchCooperativeKernel(k, dim3(blocks), dim3(256), args, smem, s);
+}
+
+int level_zb(const Dims& d, int halves) {
+  // about two tiles per block of a full cooperative grid (296 blocks on 148 SMs); a constant, so
+  // the decomposition is the same whatever grid or group runs the level
+  const int target_units = 2 * 296;
+  const int gx = (d.nx + 31) / 32, gy = (d.ny + 7) / 8;
+  const int per = std::max(1, target_units / (gx * gy * halves));
+  return std::max(1, (d.nz + per - 1) / per);
 }
 
 }  // namespace synx

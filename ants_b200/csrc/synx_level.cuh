@@ -22,7 +22,7 @@ struct LevelArgs {
   double* cc_partials;
   double* inv_psum;
   float* inv_pmax;
-  int pcap;             // partial slots per half (>= grid size)
+  int pcap;             // partial slots per half (>= inversion tiles per half)
   int iters;            // iterations of the level
   int r_smooth;         // update-field smoothing radius (1..8)
   int cc_gx, cc_gy, cc_gz;
@@ -35,12 +35,26 @@ struct LevelArgs {
   int diag;             // index maps without rotation
 };
 
+// Several pairs in one launch of the level kernel (same dimension and CC radius).
+struct BatchLevelArgs {
+  const LevelArgs* pairs;  // device array of npairs
+  const int* first_block;  // device array of npairs + 1: pair p owns [first_block[p], first_block[p+1])
+  int npairs;
+};
+
 constexpr int kLevelMaxSmoothRadius = 8;
 
 size_t level_smem_bytes(int dim, int cc_radius, int r_smooth);
 // Largest cooperative grid for the level kernel on `device` (0 if unsupported).
 int level_max_blocks(int dim, int cc_radius, int r_smooth, int device);
 cudaError_t launch_level(const LevelArgs& A, int dim, int cc_radius, int blocks, cudaStream_t s);
+// Largest cooperative grid of the batched level kernel, and its launch (blocks = first_block[npairs]).
+int level_batch_max_blocks(int dim, int cc_radius, int device);
+cudaError_t launch_level_batch(const BatchLevelArgs& B, int dim, int cc_radius, int blocks, cudaStream_t s);
+
+// Tile depth (z slices) of the level kernel's per-voxel phases for `halves` field halves; depends
+// on the level grid only.
+int level_zb(const Dims& d, int halves);
 
 // Helpers shared with the standalone launchers (synx_kernels.cu, synx_cc.cu).
 bool affine_diag_host(const Affine& m);

@@ -9,7 +9,12 @@
 // deterministic: block partials in fixed slots, reduced in a fixed order by every block that
 // needs the result.  The grid barrier spins on a generation counter with an iteration limit;
 // if a wait gives up, the kernel records the error (IterCtl::bar_err) and every block returns.
-#include <cooperative_groups.h>
+//
+// The batched form (k_level_batch) runs several pairs in one launch: each pair owns a contiguous
+// group of blocks, its own control block and barrier, and advances through its own level
+// independently of the others.  Every tile decomposition and every reduction order depends on
+// the pair's level grid only, never on how many blocks its group has, so a pair gives the same
+// bits alone and in any batch.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -30,16 +35,22 @@ constexpr long long kBarrierSpinLimit = 1ll << 24;  // ~ a second of polling bef
 __device__ __forceinline__ unsigned ld_volatile_u(const unsigned* p) { return *(volatile const unsigned*)p; }
 __device__ __forceinline__ int ld_volatile_i(const int* p) { return *(volatile const int*)p; }
 
-// Grid-wide barrier for a cooperative launch (all blocks co-resident).  Returns false once any
-// block's wait has timed out.
-__device__ bool grid_barrier(IterCtl* ctl) {
+// The blocks that work on one pair: block b of G (a whole cooperative grid, or one pair's group
+// in the batched kernel).
+struct Grp {
+  int b, G;
+};
+
+// Barrier over the G blocks of a group (all co-resident: cooperative launch).  Returns false
+// once any block's wait has timed out.
+__device__ bool grid_barrier(IterCtl* ctl, int G) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned gen = ld_volatile_u(&ctl->bar_gen);
     __threadfence();
     const unsigned arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
-    if (arrived == gridDim.x) {
+    if (arrived == (unsigned)G) {
       ctl->bar_count = 0u;
       __threadfence();
       atomicAdd(&ctl->bar_gen, 1u);
@@ -105,22 +116,20 @@ __device__ float smooth_z_dispatch(const LevelArgs& A, int bx, int by, int zc, i
   }
 }
 
-// Deterministic reduction of per-block partials (sum and max per half) by one block: every
+// Deterministic reduction of the per-tile partials (n per half; sum and max per half): every
 // block that runs it gets bit-identical results.
-__device__ void reduce_partials(const LevelArgs& A, double out_sum[2], float out_max[2], double* redd,
+__device__ void reduce_partials(const LevelArgs& A, int n, double out_sum[2], float out_max[2], double* redd,
                                 float* redf) {
   __shared__ double s_sum[2];
   __shared__ float s_max[2];
-  const int G = gridDim.x;
   for (int h = 0; h < 2; ++h) {
     double s = 0.0;
     float m = 0.0f;
-    for (int b = threadIdx.x; b < G; b += blockDim.x) {
+    for (int b = threadIdx.x; b < n; b += blockDim.x) {
       s += __ldcg(A.inv_psum + h * A.pcap + b);
       m = fmaxf(m, __ldcg(A.inv_pmax + h * A.pcap + b));
     }
-    s = block_sum_d(s, redd);
-    m = block_max_f(m, redf);
+    block_sum_max(s, m, redd, redf);
     if (threadIdx.x == 0) {
       s_sum[h] = s;
       s_max[h] = m;
@@ -133,32 +142,32 @@ __device__ void reduce_partials(const LevelArgs& A, double out_sum[2], float out
   out_max[1] = s_max[1];
 }
 
+// One fixed-point inversion of both halves (psi <- inv(phi), warm-started from psi).  Each tile
+// writes its own residual partials, so the statistics do not depend on the group size.
 template <int DIM, bool DIAG>
-__device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, double* redd, float* redf) {
+__device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, const Grp& gp, double* redd,
+                              float* redf) {
   IterCtl* ctl = A.ctl;
   const Units U{A.el_gx, A.el_gy, A.inv_gz, 2};
-  const int nu = U.count();
+  const int nu = U.count(), nh = nu / 2;
   const double N = (double)A.g.N;
   // statistics of the starting iterate
-  double acc[2] = {0.0, 0.0};
-  float mx[2] = {0.0f, 0.0f};
-  for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+  for (int u = gp.b; u < nu; u += gp.G) {
     int bx, by, bz, h;
     U.at(u, bx, by, bz, h);
-    invert_tile<DIM, DIAG>(I, h, bx, by, bz, false, true, 0.0f, 0.0f, acc[h], mx[h]);
-  }
-  for (int h = 0; h < 2; ++h) {
-    const double bs = block_sum_d(acc[h], redd);
-    const float bm = block_max_f(mx[h], redf);
+    double acc = 0.0;
+    float mx = 0.0f;
+    invert_tile<DIM, DIAG>(I, h, bx, by, bz, false, true, 0.0f, 0.0f, acc, mx);
+    block_sum_max(acc, mx, redd, redf);
     if (threadIdx.x == 0) {
-      A.inv_psum[h * A.pcap + blockIdx.x] = bs;
-      A.inv_pmax[h * A.pcap + blockIdx.x] = bm;
+      A.inv_psum[h * A.pcap + (u - h * nh)] = acc;
+      A.inv_pmax[h * A.pcap + (u - h * nh)] = mx;
     }
   }
-  if (!grid_barrier(ctl)) return false;
+  if (!grid_barrier(ctl, gp.G)) return false;
   double sum[2];
   float mxv[2];
-  reduce_partials(A, sum, mxv, redd, redf);
+  reduce_partials(A, nh, sum, mxv, redd, redf);
   bool exec[2] = {true, true};
   int iters[2] = {0, 0};
   for (int k = 1; k <= A.inv_max_iter; ++k) {
@@ -170,32 +179,29 @@ __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, d
       st[h] = exec[h] && (k + 1 <= A.inv_max_iter) && ((double)mxv[h] > A.inv_max_tol) &&
               (sum[h] / N > A.inv_mean_tol);
       lim[h] = eps * mxv[h];
-      acc[h] = 0.0;
-      mx[h] = 0.0f;
       if (exec[h]) iters[h] = k;
     }
-    for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+    for (int u = gp.b; u < nu; u += gp.G) {
       int bx, by, bz, h;
       U.at(u, bx, by, bz, h);
-      if (exec[h]) invert_tile<DIM, DIAG>(I, h, bx, by, bz, true, st[h], eps, lim[h], acc[h], mx[h]);
-    }
-    const bool any = st[0] || st[1];
-    if (any) {
-      for (int h = 0; h < 2; ++h) {
-        const double bs = block_sum_d(acc[h], redd);
-        const float bm = block_max_f(mx[h], redf);
+      if (!exec[h]) continue;  // uniform over the block
+      double acc = 0.0;
+      float mx = 0.0f;
+      invert_tile<DIM, DIAG>(I, h, bx, by, bz, true, st[h], eps, lim[h], acc, mx);
+      if (st[h]) {
+        block_sum_max(acc, mx, redd, redf);
         if (threadIdx.x == 0) {
-          A.inv_psum[h * A.pcap + blockIdx.x] = bs;
-          A.inv_pmax[h * A.pcap + blockIdx.x] = bm;
+          A.inv_psum[h * A.pcap + (u - h * nh)] = acc;
+          A.inv_pmax[h * A.pcap + (u - h * nh)] = mx;
         }
       }
     }
-    if (!grid_barrier(ctl)) return false;
-    if (any) reduce_partials(A, sum, mxv, redd, redf);
+    if (!grid_barrier(ctl, gp.G)) return false;
+    if (st[0] || st[1]) reduce_partials(A, nh, sum, mxv, redd, redf);
     exec[0] = st[0];
     exec[1] = st[1];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (gp.b == 0 && threadIdx.x == 0) {
     ctl->inv[phase][0].iters = iters[0];
     ctl->inv[phase][1].iters = iters[1];
   }
@@ -203,9 +209,9 @@ __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, d
 }
 
 template <int DIM, int RCC, bool DIAG>
-__device__ void level_body(const LevelArgs& A, unsigned char* smem, double* redd, float* redf) {
+__device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* smem, double* redd, float* redf) {
   IterCtl* ctl = A.ctl;
-  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  const int G = gp.G, b = gp.b, tid = threadIdx.x;
   const Units UW{A.el_gx, A.el_gy, A.warp_gz, 1};
   const Units UC{A.el_gx, A.el_gy, A.comp_gz, 2};
   const Units UXY{A.el_gx, A.el_gy, A.g.nz, 2};
@@ -219,14 +225,14 @@ __device__ void level_body(const LevelArgs& A, unsigned char* smem, double* redd
       UW.at(u, bx, by, bz, h);
       warp_pair_tile<DIM, DIAG>(A.warp, bx, by, bz);
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl, G)) return;
     // 2. CC tiles (same tiles and partial slots as the standalone kernel)
     for (int t = b; t < ncc; t += G) {
       const int bx = t % A.cc_gx, by = (t / A.cc_gx) % A.cc_gy, bz = t / (A.cc_gx * A.cc_gy);
       const double s = cc_tile<RCC, DIM>(A.warp.Ft, A.warp.Mt, A.g, A.cc, A.gF, A.gM, nullptr, bx, by, bz, smem, redd);
       if (tid == 0) A.cc_partials[t] = s;
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl, G)) return;
     // 3. update smoothing (xy, then z in 3-D) with the max ||u/h|| per half
     float mxs[2] = {0.0f, 0.0f};
     for (int u = b; u < UXY.count(); u += G) {
@@ -236,7 +242,7 @@ __device__ void level_body(const LevelArgs& A, unsigned char* smem, double* redd
       if (DIM == 2) mxs[h] = fmaxf(mxs[h], m);
     }
     if (DIM == 3) {
-      if (!grid_barrier(ctl)) return;
+      if (!grid_barrier(ctl, G)) return;
       for (int u = b; u < UZ.count(); u += G) {
         int bx, by, zc, h;
         UZ.at(u, bx, by, zc, h);
@@ -247,17 +253,17 @@ __device__ void level_body(const LevelArgs& A, unsigned char* smem, double* redd
       const float bm = block_max_f(mxs[h], redf);
       if (tid == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl, G)) return;
     // 4. scale + compose into the forward half-fields, in place
     for (int u = b; u < UC.count(); u += G) {
       int bx, by, bz, h;
       UC.at(u, bx, by, bz, h);
       compose_tile<DIM, DIAG>(A.comp, ctl, h, bx, by, bz);
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl, G)) return;
     // 5, 6. psi <- inv(phi) warm from psi, then phi <- inv(psi) warm from phi
-    if (!inverse_phase<DIM, DIAG>(A, A.invA, 0, redd, redf)) return;
-    if (!inverse_phase<DIM, DIAG>(A, A.invB, 1, redd, redf)) return;
+    if (!inverse_phase<DIM, DIAG>(A, A.invA, 0, gp, redd, redf)) return;
+    if (!inverse_phase<DIM, DIAG>(A, A.invB, 1, gp, redd, redf)) return;
     // 7. metric (reduced like the standalone CC kernel) and the convergence monitor
     if (b == 0) {
       double s = 0.0;
@@ -270,7 +276,7 @@ __device__ void level_body(const LevelArgs& A, unsigned char* smem, double* redd
         ctl->maxnorm[0] = ctl->maxnorm[1] = 0u;
       }
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl, G)) return;
   }
 }
 
@@ -279,8 +285,37 @@ __global__ void __launch_bounds__(256, 2) k_level(const __grid_constant__ LevelA
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double redd[32];
   __shared__ float redf[32];
-  if (A.diag) level_body<DIM, RCC, true>(A, smem, redd, redf);
-  else level_body<DIM, RCC, false>(A, smem, redd, redf);
+  const Grp gp{(int)blockIdx.x, (int)gridDim.x};
+  if (A.diag) level_body<DIM, RCC, true>(A, gp, smem, redd, redf);
+  else level_body<DIM, RCC, false>(A, gp, smem, redd, redf);
+}
+
+// Several pairs in one cooperative launch: pair p owns blocks [first_block[p], first_block[p+1]).
+template <int DIM, int RCC>
+__global__ void __launch_bounds__(256, 2) k_level_batch(const __grid_constant__ BatchLevelArgs B) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double redd[32];
+  __shared__ float redf[32];
+  __shared__ __align__(16) unsigned long long a_raw[sizeof(LevelArgs) / 8];
+  __shared__ int s_pair;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = B.npairs - 1;  // the last pair whose first block is <= blockIdx.x
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (B.first_block[mid] <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    s_pair = lo;
+  }
+  __syncthreads();
+  const int p = s_pair;
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(B.pairs + p);
+  for (int i = threadIdx.x; i < (int)(sizeof(LevelArgs) / 8); i += blockDim.x) a_raw[i] = src[i];
+  __syncthreads();
+  const LevelArgs& A = *reinterpret_cast<const LevelArgs*>(a_raw);
+  const Grp gp{(int)blockIdx.x - B.first_block[p], B.first_block[p + 1] - B.first_block[p]};
+  if (A.diag) level_body<DIM, RCC, true>(A, gp, smem, redd, redf);
+  else level_body<DIM, RCC, false>(A, gp, smem, redd, redf);
 }
 
 }  // namespace

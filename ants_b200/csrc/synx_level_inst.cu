@@ -11,7 +11,8 @@
 
 namespace synx {
 
-void* SYNX_CAT(level_kernel_r, SYNX_RCC)(int dim) {
+void* SYNX_CAT(level_kernel_r, SYNX_RCC)(int dim, bool batch) {
+  if (batch) return dim == 3 ? (void*)k_level_batch<3, SYNX_RCC> : (void*)k_level_batch<2, SYNX_RCC>;
   return dim == 3 ? (void*)k_level<3, SYNX_RCC> : (void*)k_level<2, SYNX_RCC>;
 }
 

@@ -165,6 +165,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_invert_field": (I, [V, V, P(SynxGeom), I, D, D, P(I), V]),
         "synx_resample_field": (I, [V, P(SynxGeom), V, P(SynxGeom), V]),
         "synx_shrink_geom": (I, [P(SynxGeom), I, P(SynxGeom)]),
+        "synx_batch_create": (I, [I, P(V)]),
+        "synx_batch_destroy": (I, [V]),
+        "synx_batch_last_error": (C.c_char_p, [V]),
+        "synx_batch_step": (I, [V, P(V), I, V, P(I)]),
+        "synx_batch_run": (I, [V, P(V), I, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -258,6 +263,58 @@ class LogRecord:
     metric: float
     convergence: float
     inverse_iterations: int
+
+
+class Batch:
+    """Advances many SyN stages together (synx_batch_*): each step runs every stage's next level,
+    the small levels of all stages sharing cooperative launches.  A stage's results do not depend
+    on what else is in the batch."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.synx_batch_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.synx_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, rc):
+        if rc != 0:
+            msg = self.lib.synx_batch_last_error(self.h).decode(errors="replace")
+            raise SynxError(f"synx error {rc} ({ERRORS.get(rc, '?')}): {msg}")
+
+    @staticmethod
+    def _handles(stages):
+        arr = (C.c_void_p * max(len(stages), 1))()
+        for i, st in enumerate(stages):
+            arr[i] = st.h
+        return arr
+
+    def step(self, stages, stream: int | None = None) -> int:
+        """Run the next level of every stage that has one; returns how many ran a level."""
+        adv = C.c_int(0)
+        self._ck(self.lib.synx_batch_step(self.h, self._handles(stages), len(stages), C.c_void_p(stream or 0),
+                                          C.byref(adv)))
+        return adv.value
+
+    def run(self, stages, stream: int | None = None) -> None:
+        """Run every remaining level of every stage."""
+        self._ck(self.lib.synx_batch_run(self.h, self._handles(stages), len(stages), C.c_void_p(stream or 0)))
 
 
 class SyNStage:

@@ -111,6 +111,23 @@ int synx_set_images_device(synx_ctx* ctx, const float* fixed_dev, const synx_geo
 int synx_run(synx_ctx* ctx);
 int synx_run_level(synx_ctx* ctx, int level);
 
+/* Batched pairs.  No reference counterpart: antsRegistration registers one pair per process
+ * (antsRegistration.cxx:554-777); these entry points advance many contexts together.
+ * A batch holds only device staging for the launch arguments.  synx_batch_step advances every
+ * listed context that has a level left by its next level (synx_run_level semantics per
+ * context, same results bit for bit whatever else is in the batch); levels that the persistent
+ * level kernel serves share one cooperative launch per (dimension, CC radius); *advanced gets
+ * the number of contexts that ran a level.  All work goes on cuda_stream (ordered after work
+ * already queued on each context's own stream); the call returns after the step has finished.
+ * synx_batch_run repeats steps until every context has run all its levels.  Contexts must be on
+ * the batch's device and must not be used elsewhere during the call. */
+typedef struct synx_batch synx_batch;
+int synx_batch_create(int device, synx_batch** out);
+int synx_batch_destroy(synx_batch* batch);
+const char* synx_batch_last_error(const synx_batch* batch);
+int synx_batch_step(synx_batch* batch, synx_ctx* const* ctxs, int n, void* cuda_stream, int* advanced);
+int synx_batch_run(synx_batch* batch, synx_ctx* const* ctxs, int n, void* cuda_stream);
+
 /* Geometry of the grid the output fields live on (the last level run). */
 int synx_get_output_geom(const synx_ctx* ctx, synx_geom* out);
 /* Final forward (prefix0Warp) and inverse (prefix0InverseWarp) fields, interleaved, host. */

@@ -79,3 +79,5 @@ def test_step_calls_reject_null_pointers():
     v = C.c_double()
     assert lib.synx_cc_metric(None, None, C.byref(g), 2, None, None, C.byref(v), None) == -1
     assert lib.synx_invert_field(None, None, C.byref(g), 20, 0.001, 0.1, None, None) == -1
+    assert lib.synx_batch_step(None, None, 0, None, None) == -1
+    assert lib.synx_batch_run(None, None, 0, None) == -1
