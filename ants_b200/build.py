@@ -20,13 +20,13 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-Xcompiler", "-pthread",
               "--expt-relaxed-constexpr"]
 
 LIB = os.path.join(HERE, "libsynx.so")
 CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
 
-LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu"]
+LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu", "synx_server.cpp"]
 LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh", "synx_phases.cuh", "synx_cc_tile.cuh", "synx_level.cuh",
                "synx_level_body.cuh"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
@@ -61,7 +61,7 @@ LEVEL_RADII = range(1, 8)  # the persistent level kernel is instantiated once pe
 
 def _objects() -> list[tuple[str, str, list[str]]]:
     """(source, object, extra flags) for every compile unit of libsynx.so."""
-    units = [(os.path.join(CSRC, s), os.path.join(BUILD_DIR, s.replace(".cu", ".o")), []) for s in LIB_SOURCES]
+    units = [(os.path.join(CSRC, s), os.path.join(BUILD_DIR, os.path.splitext(s)[0] + ".o"), []) for s in LIB_SOURCES]
     inst = os.path.join(CSRC, "synx_level_inst.cu")
     units += [(inst, os.path.join(BUILD_DIR, f"synx_level_r{r}.o"), [f"-DSYNX_RCC={r}"]) for r in LEVEL_RADII]
     return units
@@ -84,7 +84,7 @@ def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
             list(ex.map(_run, jobs))
     objs = [o for _, o, _ in _objects()]
     if force or jobs or _stale(LIB, objs):
-        _run([_nvcc(), *ARCH, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *objs, "-lcudart"])
+        _run([_nvcc(), *ARCH, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *objs, "-lcudart", "-Xcompiler", "-pthread"])
     return LIB
 
 

@@ -265,7 +265,15 @@ int build_levels(synx_ctx* c) {
 
 long long level_inv_units(const GridInfo& g);
 
-int allocate(synx_ctx* c) {
+// Byte offsets of everything a context keeps on the device, for its images and schedule.
+struct ArenaPlan {
+  size_t F0, M0, Fs, Ms, Tmp, Field[4], Ft, Mt, Work[6], CC, IS, IM, Cu, Ct, Ci, Ctl, Lm, Lc, Li, H;
+  size_t total;
+  int ccb, invb, coeff_cap, max_iters;
+};
+
+ArenaPlan arena_plan(const synx_ctx* c) {
+  ArenaPlan a{};
   const int D = c->D;
   const long long Nmax = c->Nmax, NI = std::max(c->NF, c->NM);
   int ccb = 0, invb = 0;
@@ -285,17 +293,31 @@ int allocate(synx_ctx* c) {
     sz += align_up(bytes);
     return o;
   };
-  size_t oF0 = add(4 * c->NF), oM0 = add(4 * c->NM), oFs = add(4 * c->NF), oMs = add(4 * c->NM), oTmp = add(4 * NI);
-  size_t oField[4];
-  for (int k = 0; k < 4; ++k) oField[k] = add(4 * (size_t)D * Nmax);
-  size_t oFt = add(4 * Nmax), oMt = add(4 * Nmax);
-  size_t oWork[6];
-  for (int k = 0; k < 6; ++k) oWork[k] = add(4 * (size_t)D * Nmax);
-  size_t oCC = add(8 * (size_t)ccb), oIS = add(8 * 2 * (size_t)invb), oIM = add(4 * 2 * (size_t)invb);
-  size_t oCu = add(4 * 3 * coeff_cap), oCt = add(4 * 3 * coeff_cap), oCi = add(8 * 3 * coeff_cap);
-  size_t oCtl = add(sizeof(IterCtl));
-  size_t oLm = add(8 * (size_t)max_iters), oLc = add(8 * (size_t)max_iters), oLi = add(4 * (size_t)max_iters);
-  size_t oH = add(4 * 258);
+  a.F0 = add(4 * c->NF), a.M0 = add(4 * c->NM), a.Fs = add(4 * c->NF), a.Ms = add(4 * c->NM), a.Tmp = add(4 * NI);
+  for (int k = 0; k < 4; ++k) a.Field[k] = add(4 * (size_t)D * Nmax);
+  a.Ft = add(4 * Nmax), a.Mt = add(4 * Nmax);
+  for (int k = 0; k < 6; ++k) a.Work[k] = add(4 * (size_t)D * Nmax);
+  a.CC = add(8 * (size_t)ccb), a.IS = add(8 * 2 * (size_t)invb), a.IM = add(4 * 2 * (size_t)invb);
+  a.Cu = add(4 * 3 * coeff_cap), a.Ct = add(4 * 3 * coeff_cap), a.Ci = add(8 * 3 * coeff_cap);
+  a.Ctl = add(sizeof(IterCtl));
+  a.Lm = add(8 * (size_t)max_iters), a.Lc = add(8 * (size_t)max_iters), a.Li = add(4 * (size_t)max_iters);
+  a.H = add(4 * 258);
+  a.total = sz;
+  a.ccb = ccb;
+  a.invb = invb;
+  a.coeff_cap = coeff_cap;
+  a.max_iters = max_iters;
+  return a;
+}
+
+int allocate(synx_ctx* c) {
+  const ArenaPlan pl = arena_plan(c);
+  const size_t sz = pl.total;
+  const int ccb = pl.ccb, invb = pl.invb, coeff_cap = pl.coeff_cap, max_iters = pl.max_iters;
+  const size_t oF0 = pl.F0, oM0 = pl.M0, oFs = pl.Fs, oMs = pl.Ms, oTmp = pl.Tmp, oFt = pl.Ft, oMt = pl.Mt;
+  const size_t *oField = pl.Field, *oWork = pl.Work;
+  const size_t oCC = pl.CC, oIS = pl.IS, oIM = pl.IM, oCu = pl.Cu, oCt = pl.Ct, oCi = pl.Ci, oCtl = pl.Ctl;
+  const size_t oLm = pl.Lm, oLc = pl.Lc, oLi = pl.Li, oH = pl.H;
   if (c->arena && c->arena_bytes >= sz) {
     // reuse
   } else {
@@ -1148,6 +1170,29 @@ int synx_set_images_device(synx_ctx* c, const float* F, const synx_geom* gf, con
 int synx_run_level(synx_ctx* c, int level) {
   if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
   return run_level_impl(c, level);
+}
+
+int synx_footprint(const synx_params* p, const synx_geom* fixed_geom, const synx_geom* moving_geom, int64_t* bytes) {
+  if (!p || !fixed_geom || !moving_geom || !bytes) return set_err(nullptr, SYNX_E_ARG, "synx_footprint: null argument");
+  if (p->dim != 2 && p->dim != 3) return set_err(nullptr, SYNX_E_ARG, "synx_footprint: dim must be 2 or 3");
+  if (p->n_levels < 1 || p->n_levels > SYNX_MAX_LEVELS)
+    return set_err(nullptr, SYNX_E_ARG, "synx_footprint: n_levels must be in 1..8");
+  for (int l = 0; l < p->n_levels; ++l)
+    if (p->shrink_factors[l] < 1) return set_err(nullptr, SYNX_E_ARG, "synx_footprint: shrink factors must be >= 1");
+  if (!check_geom(fixed_geom, p->dim) || !check_geom(moving_geom, p->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_footprint: invalid geometry");
+  synx_ctx c;
+  c.P = *p;
+  c.D = p->dim;
+  c.geF = *fixed_geom;
+  c.geM = *moving_geom;
+  geom_to_grid(c.geF, c.gF);
+  geom_to_grid(c.geM, c.gM);
+  c.NF = c.gF.d.N;
+  c.NM = c.gM.d.N;
+  build_levels(&c);
+  *bytes = (int64_t)arena_plan(&c).total;
+  return SYNX_OK;
 }
 
 int synx_batch_create(int device, synx_batch** out) {

@@ -65,6 +65,23 @@ class SynxParams(C.Structure):
     ]
 
 
+class SynxServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_active", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("reserved", C.c_int32 * 8)]
+
+
+class SynxRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("levels_done", C.c_int32), ("device_bytes", C.c_int64),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double), ("error", C.c_char * 256)]
+
+
+class SynxServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64),
+                ("resident", C.c_int64), ("bytes_resident", C.c_int64), ("bytes_peak", C.c_int64),
+                ("budget", C.c_int64), ("bytes_pooled", C.c_int64), ("steps", C.c_int64), ("step_seconds", C.c_double),
+                ("resident_byte_seconds", C.c_double), ("elapsed", C.c_double)]
+
+
 # ---- geometry --------------------------------------------------------------------------------
 @dataclass
 class Geom:
@@ -170,6 +187,13 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_batch_last_error": (C.c_char_p, [V]),
         "synx_batch_step": (I, [V, P(V), I, V, P(I)]),
         "synx_batch_run": (I, [V, P(V), I, V]),
+        "synx_footprint": (I, [P(SynxParams), P(SynxGeom), P(SynxGeom), P(C.c_int64)]),
+        "synx_server_create": (I, [P(SynxServerConfig), P(V)]),
+        "synx_server_destroy": (I, [V]),
+        "synx_server_last_error": (C.c_char_p, [V]),
+        "synx_server_submit": (I, [V, P(SynxParams), V, P(SynxGeom), V, P(SynxGeom), V, V, P(C.c_int64)]),
+        "synx_server_wait": (I, [V, C.c_int64, D, P(SynxRequestInfo)]),
+        "synx_server_get_stats": (I, [V, P(SynxServerStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -263,6 +287,97 @@ class LogRecord:
     metric: float
     convergence: float
     inverse_iterations: int
+
+
+def footprint(params: "SyNParams", fixed_geom: "Geom", moving_geom: "Geom") -> int:
+    """Device bytes a stage holds for these grids (synx_footprint)."""
+    lib = load_library()
+    cp, gf, gm = params.to_c(), fixed_geom.to_c(), moving_geom.to_c()
+    b = C.c_int64(0)
+    _check(lib.synx_footprint(C.byref(cp), C.byref(gf), C.byref(gm), C.byref(b)))
+    return b.value
+
+
+class Server:
+    """The serving loop (synx_server_*): submit registration requests from any thread; a server
+    thread admits them by device footprint and advances all resident ones together, one pyramid
+    level per step.  Results go to host arrays this object allocates per request."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_active: int = 0):
+        self.lib = load_library()
+        cfg = SynxServerConfig(device, max_active, hbm_budget_bytes)
+        h = C.c_void_p()
+        rc = self.lib.synx_server_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise SynxError(f"synx error {rc}: {self.lib.synx_server_last_error(None).decode(errors='replace')}")
+        self.h = h
+        self._live = {}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.synx_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _err(self, rc):
+        raise SynxError(f"synx error {rc} ({ERRORS.get(rc, '?')}): "
+                        f"{self.lib.synx_server_last_error(self.h).decode(errors='replace')}")
+
+    def submit(self, params: "SyNParams", fixed: np.ndarray, fixed_geom: "Geom", moving: np.ndarray,
+               moving_geom: "Geom", out: tuple | None = None) -> int:
+        """Queue a request; `out` = (forward, inverse) float32 host arrays of shape
+        fixed_geom.shape + (dim,) to receive the fields (allocated here when omitted; pass pinned
+        arrays for faster copies)."""
+        f = np.ascontiguousarray(fixed, dtype=np.float32)
+        m = np.ascontiguousarray(moving, dtype=np.float32)
+        shp = tuple(fixed_geom.shape) + (params.dim,)
+        if out is None:
+            fwd = np.empty(shp, np.float32)
+            inv = np.empty(shp, np.float32)
+        else:
+            fwd, inv = out
+            if fwd.shape != shp or inv.shape != shp or fwd.dtype != np.float32 or inv.dtype != np.float32 or \
+                    not (fwd.flags["C_CONTIGUOUS"] and inv.flags["C_CONTIGUOUS"]):
+                raise ValueError(f"output arrays must be C-contiguous float32 of shape {shp}")
+        cp, gf, gm = params.to_c(), fixed_geom.to_c(), moving_geom.to_c()
+        rid = C.c_int64(0)
+        rc = self.lib.synx_server_submit(self.h, C.byref(cp), _ptr(f), C.byref(gf), _ptr(m), C.byref(gm), _ptr(fwd),
+                                         _ptr(inv), C.byref(rid))
+        if rc != 0:
+            self._err(rc)
+        self._live[rid.value] = (f, m, fwd, inv)
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0):
+        """Blocks until request `rid` is done; returns (forward, inverse, info dict)."""
+        info = SynxRequestInfo()
+        rc = self.lib.synx_server_wait(self.h, rid, float(timeout), C.byref(info))
+        if rc != 0:
+            if rc != -2:  # a timeout leaves the request running; anything else ended it
+                self._live.pop(rid, None)
+            self._err(rc)
+        _, _, fwd, inv = self._live.pop(rid)
+        d = {k: getattr(info, k) for k in ("status", "levels_done", "device_bytes", "t_submit", "t_admit", "t_done")}
+        return fwd, inv, d
+
+    def stats(self) -> dict:
+        st = SynxServerStats()
+        rc = self.lib.synx_server_get_stats(self.h, C.byref(st))
+        if rc != 0:
+            self._err(rc)
+        return {k: getattr(st, k) for k, _ in SynxServerStats._fields_}
 
 
 class Batch:

@@ -297,6 +297,130 @@ def run_batched(args) -> int:
 
 
 # ---------------------------------------------------------------------------------------------
+# Serving mix: (dimension, size, weight); 3-level schedule, CC r=2 (2-D) / r=4 (3-D)
+SERVE_MIX = [(2, (256, 256), 0.3), (2, (512, 512), 0.1), (3, (128, 128, 128), 0.3), (3, (182, 218, 182), 0.2),
+             (3, (256, 256, 256), 0.1)]
+SERVE_STAGE = dict(iterations=(40, 20, 10), shrink_factors=(4, 2, 1), smoothing_sigmas=(2.0, 1.0, 0.0),
+                   learning_rate=0.1, update_variance=3.0, total_variance=0.0, convergence_threshold=1e-12,
+                   convergence_window=10)
+SERVE_POOL = 2  # distinct seeded pairs per size class (requests reuse them)
+
+
+def _serve_pair(job):
+    from ants_b200 import phantoms
+    cls, k = job
+    dim, size, _ = SERVE_MIX[cls]
+    seed = 0x5EED0000 + 2000 + 10 * cls + k
+    return phantoms.pair_2d(size, seed=seed) if dim == 2 else phantoms.pair_3d(size, seed=seed)
+
+
+def run_serving(args) -> int:
+    """Poisson arrivals of registration requests (the 2-D/3-D mix above) into the serving loop
+    (synx_server_*): continuous batching, admission by device footprint, every resident request
+    advanced one level per step.  Latency = completion - submission on the server's clock; one
+    rate after another on the same server."""
+    import multiprocessing as mp
+    import threading
+    from concurrent.futures import ProcessPoolExecutor
+
+    ws, rank, local = dist_env()
+    jobs = [(c, k) for c in range(len(SERVE_MIX)) for k in range(SERVE_POOL)]
+    with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+        pool = dict(zip(jobs, ex.map(_serve_pair, jobs)))
+    import torch
+    from ants_b200 import synx as S
+
+    # pinned host memory for request inputs and results (as a serving front end would hold them)
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    pool = {k: (pinned(f), pinned(m)) for k, (f, m) in pool.items()}
+    outs = {}
+    for c, (d, size, _) in enumerate(SERVE_MIX):
+        shp = tuple(reversed(size)) + (d,)
+        outs[c] = [(torch.empty(shp, pin_memory=True).numpy(), torch.empty(shp, pin_memory=True).numpy())
+                   for _ in range(4)]
+    out_next = {c: 0 for c in outs}
+
+    rates = [float(x) for x in args.rates.split(",") if x]
+    rng = np.random.default_rng(0x5EED0000 + 3000 + rank)
+    weights = np.array([w for _, _, w in SERVE_MIX])
+    params = {d: S.SyNParams(dim=d, cc_radius=2 if d == 2 else 4, **SERVE_STAGE) for d in (2, 3)}
+    geoms = [S.Geom(size) for _, size, _ in SERVE_MIX]
+    srv = S.Server(local)
+
+    def request(cls, k):
+        f, m = pool[(cls, k)]
+        o = outs[cls][out_next[cls] % len(outs[cls])]  # results are not inspected; buffers rotate
+        out_next[cls] += 1
+        return srv.submit(params[SERVE_MIX[cls][0]], f, geoms[cls], m, geoms[cls], out=o)
+
+    # service time of each class alone (also warms every code path)
+    alone_ms = []
+    for cls in range(len(SERVE_MIX)):
+        for _ in range(2):
+            _, _, info = srv.wait(request(cls, 0), timeout=600)
+        alone_ms.append(round(1000.0 * (info["t_done"] - info["t_submit"]), 2))
+    launches0 = S.launch_count()
+    per_rate = []
+    with ClockSampler(local) as clk:
+        for lam in rates:
+            n = int(min(60, max(8, round(lam * args.window))))
+            classes = rng.choice(len(SERVE_MIX), size=n, p=weights)
+            gaps = rng.exponential(1.0 / lam, size=n)
+            st0 = srv.stats()
+            ids, results = [], {}
+
+            def collect():
+                for i in range(n):
+                    while len(ids) <= i:
+                        time.sleep(0.0005)
+                    results[i] = srv.wait(ids[i], timeout=900)[2]
+
+            th = threading.Thread(target=collect)
+            th.start()
+            t_next = time.perf_counter()
+            for i in range(n):
+                t_next += gaps[i]
+                d = t_next - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids.append(request(int(classes[i]), i % SERVE_POOL))
+            th.join()
+            st1 = srv.stats()
+            lat = np.array([1000.0 * (results[i]["t_done"] - results[i]["t_submit"]) for i in range(n)])
+            wait_q = np.array([1000.0 * (results[i]["t_admit"] - results[i]["t_submit"]) for i in range(n)])
+            span = max(r["t_done"] for r in results.values()) - min(r["t_submit"] for r in results.values())
+            occ = (st1["resident_byte_seconds"] - st0["resident_byte_seconds"]) / max(st1["elapsed"] - st0["elapsed"], 1e-9)
+            per_rate.append({"rate_per_s": lam, "requests": n, "p50_ms": float(np.percentile(lat, 50)),
+                             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                             "p99_admission_wait_ms": float(np.percentile(wait_q, 99)),
+                             "pairs_per_hour": n / span * 3600.0,
+                             "hbm_mean_resident_gb": occ / 1e9, "hbm_peak_resident_gb": st1["bytes_peak"] / 1e9,
+                             "steps": st1["steps"] - st0["steps"],
+                             "mix_counts": [int((classes == c).sum()) for c in range(len(SERVE_MIX))]})
+    launches = S.launch_count() - launches0
+    stats = srv.stats()
+    srv.close()
+    if rank == 0:
+        top = per_rate[-1]
+        line = {"metric": "serving p50/p99 latency (Poisson arrivals, 2-D/3-D mix)", "value": top["p99_ms"],
+                "unit": "ms (p99 at the highest rate)", "n_gpus": ws, "steps": len(rates), "warmup": len(SERVE_MIX) * 2,
+                "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded phantom pairs (2 per size class, reused by requests)",
+                "config": {"workload": "mix 2-D 256^2 (0.3) / 512^2 (0.1), 3-D 128^3 (0.3) / 182x218x182 (0.2) / "
+                                       "256^3 (0.1); CC r=2 (2-D) / r=4 (3-D); SyN[0.1,3,0], f 4x2x1, s 2x1x0 vox, "
+                                       "c 40x20x10 [1e-12,10]",
+                           "hbm_budget_gb": stats["budget"] / 1e9, "alone_service_ms_per_class": alone_ms,
+                           "per_rate": per_rate},
+                "clocks": clk.summary(), "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,12 +428,17 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="synx", choices=["synx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="single", choices=["single", "batched"],
+    ap.add_argument("--config", default="single", choices=["single", "batched", "serving"],
                     help="single: the 182x218x182 pair (default); batched: 32 pairs of uneven sizes, "
-                         "batched vs sequential pairs/hour")
+                         "batched vs sequential pairs/hour; serving: Poisson arrivals of a 2-D/3-D mix, "
+                         "p50/p99 latency")
+    ap.add_argument("--rates", default="0.5,2,5,10,20", help="serving: arrival rates (requests/s)")
+    ap.add_argument("--window", type=float, default=12.0, help="serving: seconds of arrivals per rate")
     args = ap.parse_args(argv)
     if args.config == "batched":
         return run_batched(args)
+    if args.config == "serving":
+        return run_serving(args)
 
     ws, rank, local = dist_env()
     from ants_b200 import phantoms, replicas

@@ -128,6 +128,59 @@ const char* synx_batch_last_error(const synx_batch* batch);
 int synx_batch_step(synx_batch* batch, synx_ctx* const* ctxs, int n, void* cuda_stream, int* advanced);
 int synx_batch_run(synx_batch* batch, synx_ctx* const* ctxs, int n, void* cuda_stream);
 
+/* Device bytes a context holds for this stage and these image grids (what synx_set_images
+ * allocates); no device work. */
+int synx_footprint(const synx_params* params, const synx_geom* fixed_geom, const synx_geom* moving_geom,
+                   int64_t* bytes);
+
+/* Serving loop.  No reference counterpart (the reference runs one registration per process).
+ * A server thread owns one stream and a batch; requests queue on submission and are admitted in
+ * arrival order whenever their footprint (synx_footprint) fits the device-memory budget and the
+ * active limit (a request that does not fit yet does not block smaller ones behind it).  Every
+ * admitted request keeps its images, pyramid and fields resident; each loop step advances every
+ * resident request by one level in one synx_batch_step, so requests that arrive while others
+ * run join at the next step.  A finished request's context is kept in a pool with its device
+ * arena and reused by a later request with the same stage parameters whose footprint it covers
+ * (no device allocation on that path); pooled contexts are freed when admission needs the memory.
+ * A request's result is bit-identical to running it alone.  The caller's input buffers must
+ * stay valid until the request is admitted (status >= 1), output buffers until it is done. */
+typedef struct synx_server synx_server;
+typedef struct synx_server_config {
+  int32_t device;
+  int32_t max_active;        /* most resident requests (0: no limit) */
+  int64_t hbm_budget_bytes;  /* device bytes resident requests may hold (0: 90% of free memory) */
+  int32_t reserved[8];
+} synx_server_config;
+typedef struct synx_request_info {
+  int32_t status;            /* 0 queued, 1 resident, 2 done, negative: SYNX_E_* failure */
+  int32_t levels_done;
+  int64_t device_bytes;      /* its footprint */
+  double t_submit, t_admit, t_done;  /* seconds since the server started (steady clock) */
+  char error[256];
+} synx_request_info;
+typedef struct synx_server_stats {
+  int64_t submitted, completed, failed, queued, resident;
+  int64_t bytes_resident;    /* arenas of resident requests */
+  int64_t bytes_peak;        /* peak of resident + pooled */
+  int64_t budget;
+  int64_t bytes_pooled;      /* arenas of finished contexts kept for reuse */
+  int64_t steps;
+  double step_seconds;       /* host time spent inside batch steps */
+  double resident_byte_seconds;  /* integral of bytes_resident over time (mean occupancy = / elapsed) */
+  double elapsed;
+} synx_server_stats;
+int synx_server_create(const synx_server_config* cfg, synx_server** out);
+/* Stops the loop after the resident requests finish; queued requests fail with SYNX_E_STATE. */
+int synx_server_destroy(synx_server* server);
+const char* synx_server_last_error(const synx_server* server);
+int synx_server_submit(synx_server* server, const synx_params* params, const float* fixed_host,
+                       const synx_geom* fixed_geom, const float* moving_host, const synx_geom* moving_geom,
+                       float* forward_host, float* inverse_host, int64_t* request_id);
+/* Waits up to timeout_s (< 0: no limit) for the request to finish; fills *info (may be NULL).
+ * Returns 0 when it is done, SYNX_E_STATE on timeout, or its failure code. */
+int synx_server_wait(synx_server* server, int64_t request_id, double timeout_s, synx_request_info* info);
+int synx_server_get_stats(synx_server* server, synx_server_stats* stats);
+
 /* Geometry of the grid the output fields live on (the last level run). */
 int synx_get_output_geom(const synx_ctx* ctx, synx_geom* out);
 /* Final forward (prefix0Warp) and inverse (prefix0InverseWarp) fields, interleaved, host. */

@@ -81,3 +81,16 @@ def test_step_calls_reject_null_pointers():
     assert lib.synx_invert_field(None, None, C.byref(g), 20, 0.001, 0.1, None, None) == -1
     assert lib.synx_batch_step(None, None, 0, None, None) == -1
     assert lib.synx_batch_run(None, None, 0, None) == -1
+
+
+def test_footprint_without_a_gpu():
+    # the device bytes a stage would hold are computed on the host
+    from ants_b200.synx import Geom, SyNParams, footprint
+    P = SyNParams(dim=3, cc_radius=4, iterations=(100, 70, 50, 20), shrink_factors=(8, 4, 2, 1),
+                  smoothing_sigmas=(3.0, 2.0, 1.0, 0.0))
+    big = footprint(P, Geom((182, 218, 182)), Geom((182, 218, 182)))
+    small = footprint(P, Geom((91, 109, 91)), Geom((91, 109, 91)))
+    n = 182 * 218 * 182
+    # 4 half-fields + 6 work fields of 3 components, 2 warped images, 5 image buffers: 37 floats/voxel
+    assert 37 * 4 * n <= big < 37 * 4 * n * 1.05
+    assert small < big / 7
