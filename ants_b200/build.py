@@ -25,12 +25,14 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 
 LIB = os.path.join(HERE, "libsynx.so")
 CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
+APPLY_CLI = os.path.join(HERE, "antsApplyTransforms_b200")
 
 LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu", "synx_server.cpp"]
 LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh", "synx_phases.cuh", "synx_cc_tile.cuh", "synx_level.cuh",
                "synx_level_body.cuh"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
-CLI_HEADERS = ["nifti_io.h", "ants_registration.h"]
+APPLY_SOURCES = ["ants_apply_transforms.cpp", "nifti_io.cpp"]
+CLI_HEADERS = ["nifti_io.h", "ants_registration.h", "ants_apply_transforms.h", "cli_common.h"]
 
 
 def _nvcc() -> str:
@@ -88,18 +90,24 @@ def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
     return LIB
 
 
-def build_cli(force: bool = False) -> str | None:
-    srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES]
+def _build_exe(target: str, sources: list[str], force: bool) -> str | None:
+    srcs = [os.path.join(CSRC, s) for s in sources]
     if not all(os.path.exists(s) for s in srcs):
         return None
     deps = srcs + [os.path.join(CSRC, h) for h in CLI_HEADERS] + [LIB]
-    if not force and not _stale(CLI, deps):
-        return CLI
-    cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", "/usr/local/cuda/include", "-o", CLI,
+    if not force and not _stale(target, deps):
+        return target
+    cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", "/usr/local/cuda/include", "-o", target,
            *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN", "-L", "/usr/local/cuda/lib64", "-lcudart",
            "-Wl,-rpath,/usr/local/cuda/lib64", "-lz"]
     _run(cmd)
-    return CLI
+    return target
+
+
+def build_cli(force: bool = False) -> str | None:
+    """antsRegistrationSyN_b200 and antsApplyTransforms_b200."""
+    _build_exe(APPLY_CLI, APPLY_SOURCES, force)
+    return _build_exe(CLI, CLI_SOURCES, force)
 
 
 def build_all(force: bool = False) -> None:

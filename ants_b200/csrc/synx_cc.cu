@@ -9,7 +9,7 @@ namespace synx {
 
 // Standalone CC kernel: one tile per block, deterministic metric reduction (block partials,
 // the last block sums them in order).
-template <int R, int DIM>
+template <int R, int DIM, typename T>
 __global__ void __launch_bounds__(256)
     k_cc(const float* __restrict__ Ft, const float* __restrict__ Mt, Dims d, CCParams P, float* __restrict__ gF,
          float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out) {
@@ -18,7 +18,7 @@ __global__ void __launch_bounds__(256)
   __shared__ double red[32];
   __shared__ int am_last;
   const int tid = threadIdx.x;
-  const double bs = cc_tile<R, DIM>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw, red);
+  const double bs = cc_tile<R, DIM, T>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw, red);
   const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
   const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (tid == 0) {
@@ -43,9 +43,12 @@ __global__ void __launch_bounds__(256)
 
 template <int R, int DIM>
 static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, float* gF, float* gM, double* partials,
-                        IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P) {
-  using S = CCShape<R, DIM>;
-  k_cc<R, DIM><<<grid, 256, S::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
+                        IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P, bool fp32) {
+  if (fp32)
+    k_cc<R, DIM, float><<<grid, 256, CCShape<R, DIM, float>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
+  else
+    k_cc<R, DIM, double><<<grid, 256, CCShape<R, DIM, double>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl,
+                                                                          cc_out);
 }
 
 static int cc_zchunk(const GridInfo& g, int radius) {
@@ -67,14 +70,19 @@ int cc_blocks(const GridInfo& g, int radius) {
 }
 
 size_t cc_smem_bytes(int dim, int radius) {
+  // CCShape<R, DIM, double>::smem for a run-time radius
   const size_t TX = 32, TY = 8, HX = TX + 2 * radius, HY = TY + 2 * radius, HC = HX * HY;
   const size_t RD = dim == 3 ? 2 * radius + 1 : 1;
-  return RD * HC * 8 + 5 * HC * 8 + 5 * HY * TX * 8;
+  return RD * HC * 8 + 5 * HY * (HX | 1) * 8 + 5 * HY * (TX + 1) * 8;
 }
 
 template <int R, int DIM>
 static cudaError_t cc_prepare_t() {
-  return cudaFuncSetAttribute(k_cc<R, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CCShape<R, DIM>::smem);
+  cudaError_t e = cudaFuncSetAttribute(k_cc<R, DIM, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)CCShape<R, DIM, double>::smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_cc<R, DIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)CCShape<R, DIM, float>::smem);
 }
 
 cudaError_t cc_prepare(int dim, int radius) {
@@ -114,16 +122,16 @@ CCParams make_cc_params(const GridInfo& g, int radius) {
 }
 
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out) {
+               IterCtl* ctl, cudaStream_t s, float* cc_out, bool fp32_sums) {
   add_launch_count(1);
   const CCParams P = make_cc_params(g, radius);
   dim3 grid((g.d.nx + 31) / 32, (g.d.ny + 7) / 8, (g.d.nz + P.ZC - 1) / P.ZC);
 #define SYNX_CC_CASE(RR)                                                                         \
   case RR:                                                                                       \
     if (g.d.dim == 3)                                                                            \
-      cc_launch_t<RR, 3>(Ft, Mt, g, gF, gM, partials, ctl, s, cc_out, grid, P);                  \
+      cc_launch_t<RR, 3>(Ft, Mt, g, gF, gM, partials, ctl, s, cc_out, grid, P, fp32_sums);       \
     else                                                                                         \
-      cc_launch_t<RR, 2>(Ft, Mt, g, gF, gM, partials, ctl, s, cc_out, grid, P);                  \
+      cc_launch_t<RR, 2>(Ft, Mt, g, gF, gM, partials, ctl, s, cc_out, grid, P, fp32_sums);       \
     break;
   switch (radius) {
     SYNX_CC_CASE(1)

@@ -16,9 +16,17 @@ namespace synx {
 // slices.  Each thread keeps FP64 running z-window sums of F, M, F^2, M^2, FM for up to CPT
 // halo columns; the raw (F, M) values of the last 2R+1 slices sit in a shared-memory ring so
 // the leaving slice is subtracted without a second global read.  Per slice the column sums
-// are box-summed along x and then y in shared memory (FP64), giving the five window sums of
-// each output voxel, from which the CC terms and derivatives follow.  The in-bounds count is
-// separable (cx*cy*cz) and computed analytically.
+// are box-summed along x and then y in shared memory (FP64) with sliding windows: along x one
+// thread per (quantity, halo row, half of the 32 outputs), along y one thread per (quantity,
+// output column) walking the 8 output rows; the rows of both staging arrays have an odd pitch,
+// so the threads of a half-warp, which differ in row, hit distinct banks.  This gives the five
+// window sums of each output voxel, from which the CC terms and derivatives follow.  The
+// in-bounds count is separable (cx*cy*cz) and computed analytically.
+//
+// T is the type of the window sums and of the variance terms formed from them: double (the
+// default; the sums of F^2 and M^2 cancel badly in float when the window is nearly flat) or
+// float (the precision study's variant).  The tile's sum of cc is accumulated in double either
+// way.
 // ------------------------------------------------------------------------------------------
 struct CCParams {
   float h[3];      // spacing
@@ -39,30 +47,45 @@ __device__ __forceinline__ float grad1(float vm, float v0, float vp, int pos, in
   return (vp - vm) / (2.0f * h);
 }
 
-template <int R, int DIM>
+template <int R, int DIM, typename T = double>
 struct CCShape {
   static constexpr int TX = 32, TY = 8;
   static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HC = HX * HY;
   static constexpr int RZ = DIM == 3 ? R : 0;
   static constexpr int RD = 2 * RZ + 1;
   static constexpr int CPT = (HC + 255) / 256;
-  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)5 * HC * sizeof(double) +
-                                 (size_t)5 * HY * TX * sizeof(double);
+  static constexpr int CSP = HX | 1;   // row pitch of the column sums (odd)
+  static constexpr int XSP = TX + 1;   // row pitch of the x box sums (odd)
+  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)5 * HY * CSP * sizeof(T) +
+                                 (size_t)5 * HY * XSP * sizeof(T);
 };
 
 // One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
 // Returns the tile's sum of local cc (valid in thread 0).  All threads of the block must call
 // it; `smem_raw` holds CCShape<R, DIM>::smem bytes and `red` 32 doubles.
-template <int R, int DIM>
+template <typename T>
+__device__ __forceinline__ T rcp_rn(T x);
+template <>
+__device__ __forceinline__ double rcp_rn<double>(double x) {
+  return __drcp_rn(x);
+}
+template <>
+__device__ __forceinline__ float rcp_rn<float>(float x) {
+  return __frcp_rn(x);
+}
+
+template <int R, int DIM, typename T = double>
 __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const float* __restrict__ Mt, const Dims& d,
                                           const CCParams& P, float* __restrict__ gF, float* __restrict__ gM,
                                           float* __restrict__ cc_out, int bx, int by, int bz,
                                           unsigned char* smem_raw, double* red) {
-  using S = CCShape<R, DIM>;
+  using S = CCShape<R, DIM, T>;
   constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
+  constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY;
   float2* ring = reinterpret_cast<float2*>(smem_raw);
-  double* cs = reinterpret_cast<double*>(ring + RD * HC);
-  double* xs = cs + 5 * HC;
+  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [5][HY][CSP]; reused as ys [5][TY][TX] after the x pass
+  T* xs = cs + 5 * HY * CSP;                      // [5][HY][XSP]
+  T* ys = cs;
 
   const int tid = threadIdx.x;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
@@ -72,7 +95,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   const int z1 = min(z0 + P.ZC, nz);
 
   // owned halo columns
-  int gofs[CPT];
+  int gofs[CPT], sofs[CPT];
   bool gval[CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) {
@@ -81,12 +104,16 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     int gx = x0 - R + hx, gy = y0 - R + hy;
     gval[c] = col < HC && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
     gofs[c] = gval[c] ? gy * nx + gx : 0;
+    sofs[c] = hy * CSP + hx;
   }
-  double acc[CPT][5];
+  // sliding-window tasks: x pass (quantity, half, halo row), y pass (quantity, output column)
+  const int xrow = tid % HY, xhalf = (tid / HY) & 1, xq = tid / (2 * HY);
+  const int ycol = tid & 31, yq = tid >> 5;
+  T acc[CPT][5];
 #pragma unroll
   for (int c = 0; c < CPT; ++c)
 #pragma unroll
-    for (int q = 0; q < 5; ++q) acc[c][q] = 0.0;
+    for (int q = 0; q < 5; ++q) acc[c][q] = T(0);
 
   // warm-up: slices z0-RZ .. z0+RZ-1
   for (int zs = z0 - RZ; zs < z0 + RZ; ++zs) {
@@ -101,7 +128,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
           long long o = (long long)zs * nxy + gofs[c];
           v.x = __ldg(Ft + o);
           v.y = __ldg(Mt + o);
-          double f = v.x, m = v.y;
+          const T f = v.x, m = v.y;
           acc[c][0] += f;
           acc[c][1] += m;
           acc[c][2] += f * f;
@@ -117,8 +144,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   const int tx = tid & 31, ty = tid >> 5;
   const int ox = x0 + tx, oy = y0 + ty;
   const bool out_ok = ox < nx && oy < ny;
-  const double cxn = (double)(min(ox + R, nx - 1) - max(ox - R, 0) + 1);
-  const double cyn = (double)(min(oy + R, ny - 1) - max(oy - R, 0) + 1);
+  const T cxn = (T)(min(ox + R, nx - 1) - max(ox - R, 0) + 1);
+  const T cyn = (T)(min(oy + R, ny - 1) - max(oy - R, 0) + 1);
 
   for (int zc = z0; zc < z1; ++zc) {
     // slide the z window: subtract slice zc-RZ-1 (if it was added), add slice zc+RZ
@@ -132,7 +159,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       if (col < HC) {
         if (sub && gval[c]) {
           float2 o = ring[slot * HC + col];
-          double f = o.x, m = o.y;
+          const T f = o.x, m = o.y;
           acc[c][0] -= f;
           acc[c][1] -= m;
           acc[c][2] -= f * f;
@@ -144,7 +171,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
           long long o = (long long)ze * nxy + gofs[c];
           v.x = __ldg(Ft + o);
           v.y = __ldg(Mt + o);
-          double f = v.x, m = v.y;
+          const T f = v.x, m = v.y;
           acc[c][0] += f;
           acc[c][1] += m;
           acc[c][2] += f * f;
@@ -153,53 +180,67 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         }
         ring[slot * HC + col] = v;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) cs[q * HC + col] = acc[c][q];
+        for (int q = 0; q < 5; ++q) cs[q * HY * CSP + sofs[c]] = acc[c][q];
       }
     }
     __syncthreads();
-    // x box sums: HY rows x TX outputs
-    for (int p = tid; p < HY * TX; p += 256) {
-      const int hy = p / TX, px = p % TX;
-      const double* src = cs + hy * HX + px;
+    // x box sums, sliding along the row: outputs 16 h .. 16 h + 15 of one halo row
+    if (xq < 5) {
+      const T* src = cs + xq * HY * CSP + xrow * CSP + 16 * xhalf;
+      T* dst = xs + xq * HY * XSP + xrow * XSP + 16 * xhalf;
+      T s = T(0);
 #pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        double s = 0.0;
+      for (int j = 0; j <= 2 * R; ++j) s += src[j];
+      dst[0] = s;
 #pragma unroll
-        for (int j = 0; j <= 2 * R; ++j) s += src[q * HC + j];
-        xs[q * HY * TX + p] = s;
+      for (int x = 1; x < 16; ++x) {
+        s += src[x + 2 * R];
+        s -= src[x - 1];
+        dst[x] = s;
+      }
+    }
+    __syncthreads();
+    // y box sums, sliding down one output column over the TY output rows
+    if (yq < 5) {
+      const T* src = xs + yq * HY * XSP + ycol;
+      T* dst = ys + yq * TY * TX + ycol;
+      T s = T(0);
+#pragma unroll
+      for (int j = 0; j <= 2 * R; ++j) s += src[j * XSP];
+      dst[0] = s;
+#pragma unroll
+      for (int y = 1; y < TY; ++y) {
+        s += src[(y + 2 * R) * XSP];
+        s -= src[(y - 1) * XSP];
+        dst[y * TX] = s;
       }
     }
     __syncthreads();
     if (out_ok) {
-      double Sq[5];
+      T Sq[5];
 #pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j <= 2 * R; ++j) s += xs[q * HY * TX + (ty + j) * TX + tx];
-        Sq[q] = s;
-      }
-      const double czn = (double)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
-      const double n = cxn * cyn * czn;
-      const double inv_n = __drcp_rn(n);
-      const double mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
-      const double sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
-      const double sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
-      const double sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
+      for (int q = 0; q < 5; ++q) Sq[q] = ys[q * TY * TX + ty * TX + tx];
+      const T czn = (T)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
+      const T n = cxn * cyn * czn;
+      const T inv_n = rcp_rn(n);
+      const T mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
+      const T sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
+      const T sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
+      const T sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
       const int cidx = (ty + R) * HX + (tx + R);
       const float2* rc = ring + pmod(zc, RD) * HC;
       const float2 v0 = rc[cidx];
-      const double fh = (double)v0.x - mF, mh = (double)v0.y - mM;
-      double cc = 1.0, aF = 0.0, aM = 0.0;
-      if (sFF > P.eps && sMM > P.eps) {
-        const double prod = sFF * sMM;
-        const double ip = __drcp_rn(prod);
+      const T fh = (T)v0.x - mF, mh = (T)v0.y - mM;
+      T cc = T(1), aF = T(0), aM = T(0);
+      if (sFF > (T)P.eps && sMM > (T)P.eps) {
+        const T prod = sFF * sMM;
+        const T ip = rcp_rn(prod);
         cc = sFM * sFM * ip;
-        const double coef = 2.0 * sFM * ip;
+        const T coef = T(2) * sFM * ip;
         aF = coef * (fh - sFM * sFF * ip * mh);
         aM = coef * (mh - sFM * sMM * ip * fh);
       }
-      cc_acc += cc;
+      cc_acc += (double)cc;
       // central differences of both warped images (index axes)
       float gMi[3], gFi[3];
       {
@@ -232,8 +273,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
             pf += P.dir[dd * 3 + a] * gFi[a];
           }
         }
-        gF[dd * N + oi] = (float)(aF * (double)pm);
-        gM[dd * N + oi] = (float)(aM * (double)pf);
+        gF[dd * N + oi] = (float)(aF * (T)pm);
+        gM[dd * N + oi] = (float)(aM * (T)pf);
       }
       if (cc_out != nullptr) cc_out[oi] = (float)cc;
     }

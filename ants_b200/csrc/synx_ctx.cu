@@ -526,7 +526,8 @@ void enqueue_iteration(synx_ctx* c, bool profile) {
   };
   launch_warp_pair(c->Fs, c->gF, c->psiF, c->Ms, c->gM, c->psiM, g, c->Ft, c->Mt, c->ctl, s);
   int e0 = profile ? ev() : -1;
-  launch_cc(c->Ft, c->Mt, g, c->P.cc_radius, c->gFu, c->gMu, c->cc_partials, c->ctl, s);
+  launch_cc(c->Ft, c->Mt, g, c->P.cc_radius, c->gFu, c->gMu, c->cc_partials, c->ctl, s, nullptr,
+            (c->P.flags & SYNX_F_CC_FP32_SUMS) != 0);
   if (profile) c->ev_pairs_cc.push_back({e0, ev()});
   // update-field smoothing, SyN epilogue (boundary zero, blend) and max ||u/spacing||
   const float* upd[2] = {c->t1F, c->t1M};
@@ -561,22 +562,35 @@ void enqueue_iteration(synx_ctx* c, bool profile) {
     float* o[2] = {c->phiF, c->phiM};
     launch_compose(upd, w, o, 2, g, (float)c->P.learning_rate, c->ctl, s);
   }
+  // precision study: half-fields stored in half precision (rounded after every step that writes them)
+  const bool fp16 = (c->P.flags & SYNX_F_FIELDS_FP16) != 0;
+  auto round_pair = [&](float* a, float* b) {
+    float* f[2] = {a, b};
+    launch_round_half(f, 2, (long long)c->D * g.d.N, s);
+  };
+  if (fp16) round_pair(c->phiF, c->phiM);
   // fixed-point inverses: psi <- inv(phi) warm from psi, then phi <- inv(psi) warm from phi
   PartialBufs pb{c->inv_psum, c->inv_pmax, c->inv_cap};
   const int mi = c->P.inv_max_iter;
   int e1 = profile ? ev() : -1;
+  // the CC derivative buffers are free until the next iteration: they carry the inverse residual
+  float* ecache[2] = {c->gFu, c->gMu};
   {
     const float* phi[2] = {c->phiF, c->phiM};
     float* psi[2] = {c->psiF, c->psiM};
     for (int k = 0; k <= mi; ++k)
-      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 0, pb, s);
+      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 0, pb, s, true,
+                         ecache);
   }
+  if (fp16) round_pair(c->psiF, c->psiM);
   {
     const float* phi[2] = {c->psiF, c->psiM};
     float* psi[2] = {c->phiF, c->phiM};
     for (int k = 0; k <= mi; ++k)
-      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 1, pb, s);
+      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 1, pb, s, true,
+                         ecache);
   }
+  if (fp16) round_pair(c->phiF, c->phiM);
   if (profile) c->ev_pairs_inv.push_back({e1, ev()});
   launch_converge(c->ctl, c->logdev, c->P.convergence_threshold, c->P.convergence_window, s);
 }
@@ -596,7 +610,7 @@ long long level_inv_units(const GridInfo& g) {
 // Whether a level runs in the level kernel (alone or in a batch): the options it implements, and
 // a level small enough that launch latency, not bandwidth, dominates the per-kernel path.
 bool persistent_eligible(synx_ctx* c, const GridInfo& g, bool profile) {
-  if (profile || (c->P.flags & SYNX_F_NO_PERSISTENT)) return false;
+  if (profile || (c->P.flags & (SYNX_F_NO_PERSISTENT | SYNX_F_CC_FP32_SUMS | SYNX_F_FIELDS_FP16))) return false;
   const long long max_vox = c->P.persistent_max_voxels > 0 ? c->P.persistent_max_voxels : kPersistentMaxVoxels;
   if (g.d.N > max_vox || c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
   int rs = 1;
@@ -657,8 +671,11 @@ LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
   float* psis[2] = {c->psiF, c->psiM};
   const float* psic[2] = {c->psiF, c->psiM};
   float* phim[2] = {c->phiF, c->phiM};
-  A.invA = make_inv_args(phis, psis, 2, g, zc2);
-  A.invB = make_inv_args(psic, phim, 2, g, zc2);
+  // the CC derivative buffers are free from the composition to the next iteration's CC phase:
+  // they carry the inverse residual between sub-iterations
+  float* ecache[2] = {c->gFu, c->gMu};
+  A.invA = make_inv_args(phis, psis, 2, g, zc2, ecache);
+  A.invB = make_inv_args(psic, phim, 2, g, zc2, ecache);
   A.g = g.d;
   A.ctl = c->ctl;
   A.log = c->logdev;
@@ -706,6 +723,10 @@ int level_begin(synx_ctx* c, int level) {
     std::swap(c->psiF, c->gMu);
     std::swap(c->phiM, c->t1F);
     std::swap(c->psiM, c->t1M);
+    if (c->P.flags & SYNX_F_FIELDS_FP16) {
+      float* hf[4] = {c->phiF, c->psiF, c->phiM, c->psiM};
+      launch_round_half(hf, 4, (long long)D * gl.d.N, c->stream);
+    }
   }
   c->cur_grid = gl;
   c->cur_level = level;
@@ -1508,7 +1529,12 @@ int synx_warp_image(const float* img, const synx_geom* gi, const float* u, const
 
 int synx_cc_metric(const float* F, const float* M, const synx_geom* gg, int radius, float* gF, float* gM,
                    double* value, void* stream) {
-  if (!F || !M || !gF || !gM || !gg || !check_geom(gg, gg->dim))
+  return synx_cc_metric_ex(F, M, gg, radius, 0, gF, gM, value, stream);
+}
+
+int synx_cc_metric_ex(const float* F, const float* M, const synx_geom* gg, int radius, int flags, float* gF, float* gM,
+                      double* value, void* stream) {
+  if (!F || !M || !gF || !gM || !gg || !check_geom(gg, gg->dim) || (flags & ~SYNX_F_CC_FP32_SUMS))
     return set_err(nullptr, SYNX_E_ARG, "synx_cc_metric: bad arguments");
   if (!cc_radius_supported(gg->dim, radius)) return set_err(nullptr, SYNX_E_UNSUPPORTED, "synx_cc_metric: radius");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1518,7 +1544,7 @@ int synx_cc_metric(const float* F, const float* M, const synx_geom* gg, int radi
   TempCtl t;
   STEP_TRY(t.alloc(cc_blocks(g, radius)));
   STEP_TRY(cudaMemsetAsync(t.ctl, 0, sizeof(IterCtl), s));
-  launch_cc(F, M, g, radius, gF, gM, t.part, t.ctl, s);
+  launch_cc(F, M, g, radius, gF, gM, t.part, t.ctl, s, nullptr, (flags & SYNX_F_CC_FP32_SUMS) != 0);
   IterCtl h;
   STEP_TRY(cudaMemcpyAsync(&h, t.ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, s));
   STEP_TRY(cudaStreamSynchronize(s));

@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <cstring>
 
+#include <cuda_fp16.h>
+
 #include "synx_level.cuh"
 #include "synx_phases.cuh"
 
@@ -585,10 +587,12 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaun
 constexpr int kInvTarget = 148 * 24;  // blocks: short per-thread z walks, small last-wave tail
 int inv_blocks(const GridInfo& g) { return map3(g.d, 2, kInvTarget).nblocks; }
 
-InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb) {
+InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb,
+                      float* const* ecache) {
   InvArgs a;
   a.phi = Ptr2c{{phi[0], halves > 1 ? phi[1] : phi[0]}};
   a.psi = Ptr2{{psi[0], halves > 1 ? psi[1] : psi[0]}};
+  a.ecache = ecache ? Ptr2{{ecache[0], halves > 1 ? ecache[1] : ecache[0]}} : Ptr2{{nullptr, nullptr}};
   a.g = g.d;
   const Affine m = make_affine(g, g);
   for (int j = 0; j < 9; ++j) a.A[j] = m.A[j];
@@ -599,14 +603,14 @@ InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, co
 
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
-                        bool stop_aware) {
+                        bool stop_aware, float* const* ecache) {
   count_launch();
   // the block decomposition is the same for one or two halves, so the partial buffers sized by
   // inv_blocks() fit either
   const Map3 m2 = map3(g.d, 2, kInvTarget);
   Map3 m = m2;
   m.grid.z = (m2.grid.z / 2) * halves;
-  const InvArgs a = make_inv_args(phi, psi, halves, g, m.zb);
+  const InvArgs a = make_inv_args(phi, psi, halves, g, m.zb, ecache);
   InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, mean_tol, max_tol};
   Affine am = make_affine(g, g);
   const bool dg = affine_diag(am);
@@ -659,6 +663,20 @@ __global__ void __launch_bounds__(256) k_resample(Ptr4c in, Dims di, Ptr4 out, D
 #pragma unroll
       for (int k = 0; k < DIM; ++k) out.p[f][k * No + i] = ok ? lerp_at<DIM>(in.p[f] + k * Ni, c) : 0.0f;
   }
+}
+
+__global__ void __launch_bounds__(256) k_round_half(Ptr4 f, int nf, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    for (int k = 0; k < nf; ++k) f.p[k][i] = __half2float(__float2half_rn(f.p[k][i]));
+}
+
+void launch_round_half(float* const* f, int nf, long long n, cudaStream_t s) {
+  count_launch();
+  Ptr4 p{};
+  for (int k = 0; k < nf && k < 4; ++k) p.p[k] = f[k];
+  const long long blocks = std::min<long long>((n + 255) / 256, 148 * 16);
+  k_round_half<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(p, std::min(nf, 4), n);
 }
 
 void launch_resample_fields(const float* const* in, const GridInfo& gi, float* const* out, const GridInfo& go,

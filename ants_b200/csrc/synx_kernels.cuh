@@ -76,8 +76,12 @@ size_t cc_smem_bytes(int dim, int radius);
 bool cc_radius_supported(int dim, int radius);
 // Raise the dynamic shared-memory limit of the CC kernel (once per device, outside capture).
 cudaError_t cc_prepare(int dim, int radius);
+// fp32_sums: window sums and variance terms in float (the precision study's variant).
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr);
+               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr, bool fp32_sums = false);
+// Round nf fields of n floats each to the nearest half-precision value, in place (the
+// precision study's FP16 field storage).
+void launch_round_half(float* const* f, int nf, long long n, cudaStream_t s);
 
 // Gaussian smoothing of `halves` fields along every axis: an xy-tile kernel and, in 3-D, a
 // z-column kernel (host kernels khost[a] of radius R[a] per axis, passed by value in the
@@ -104,9 +108,11 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
 
 // One launch of the fused fixed-point inverse (k = 0 .. max_iter) for `halves` pairs.
 int inv_blocks(const GridInfo& g);
+// ecache: per-half residual buffers (D x N floats each) that carry the residual from a launch's
+// statistics pass to the next launch's update; null recomputes it there.
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
-                        bool stop_aware = true);
+                        bool stop_aware = true, float* const* ecache = nullptr);
 
 void launch_converge(IterCtl* ctl, LogDev log, double threshold, int window, cudaStream_t s);
 

@@ -63,6 +63,7 @@ Smooth3Args make_smooth_args(const float* const* in, float* const* out, const fl
                              const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
                              float w2, bool maxnorm, int* radius);
 int smooth_z_chunk(const Dims& d, int halves, int RR);
-InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb);
+InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb,
+                      float* const* ecache = nullptr);
 
 }  // namespace synx

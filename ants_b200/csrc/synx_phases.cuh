@@ -159,6 +159,8 @@ __device__ __forceinline__ void compose_tile(const ComposeArgs& a, const IterCtl
 struct InvArgs {
   Ptr2c phi;   // field being inverted (read-only, gathered)
   Ptr2 psi;    // iterate (updated in place at its own voxels)
+  Ptr2 ecache; // residual of the current iterate per voxel (written by the statistics pass, read by
+               // the next update), or null: the update then recomputes it
   Dims g;
   float A[9];
   float ih[3];
@@ -196,7 +198,9 @@ __device__ __forceinline__ void inv_residual(const float* __restrict__ phi, cons
 }
 
 // apply: psi += eps * clamp(-E, lim) (boundary voxels pinned to 0); stats: accumulate ||E/h|| of
-// the (updated) iterate into acc (sum) and mx (max).
+// the (updated) iterate into acc (sum) and mx (max).  With a residual cache, the statistics pass
+// stores E and the next update reads it back instead of gathering phi again: the same values,
+// since E depends only on the iterate and phi, which have not changed in between.
 template <int DIM, bool DIAG>
 __device__ __forceinline__ void invert_tile(const InvArgs& a, int h, int bx, int by, int bz, bool apply, bool stats,
                                             float eps, float lim, double& acc, float& mx) {
@@ -205,6 +209,7 @@ __device__ __forceinline__ void invert_tile(const InvArgs& a, int h, int bx, int
   if (x >= d.nx || y >= d.ny) return;
   const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
   float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
+  float* __restrict__ ec = h ? a.ecache.p[1] : a.ecache.p[0];
   const int z0 = bz * a.zb, z1 = min(z0 + a.zb, d.nz);
   const int N = (int)d.N, nxy = d.nx * d.ny;
   const float fx = (float)x, fy = (float)y;
@@ -229,7 +234,13 @@ __device__ __forceinline__ void invert_tile(const InvArgs& a, int h, int bx, int
     }
     float e[3];
     if (apply) {
-      inv_residual<DIM, DIAG>(phi, d, a.A, fx, fy, fz, p, e);
+      if (ec != nullptr) {
+        e[0] = ec[i];
+        e[1] = ec[N + i];
+        e[2] = DIM == 3 ? ec[2 * N + i] : 0.0f;
+      } else {
+        inv_residual<DIM, DIAG>(phi, d, a.A, fx, fy, fz, p, e);
+      }
       float s2 = 0.0f;
 #pragma unroll
       for (int c = 0; c < DIM; ++c) {
@@ -247,6 +258,11 @@ __device__ __forceinline__ void invert_tile(const InvArgs& a, int h, int bx, int
     }
     if (stats) {
       inv_residual<DIM, DIAG>(phi, d, a.A, fx, fy, fz, p, e);
+      if (ec != nullptr) {
+        ec[i] = e[0];
+        ec[N + i] = e[1];
+        if (DIM == 3) ec[2 * N + i] = e[2];
+      }
       float s2 = 0.0f;
 #pragma unroll
       for (int c = 0; c < DIM; ++c) {

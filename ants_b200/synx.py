@@ -23,6 +23,8 @@ SYNX_MAX_LEVELS = 8
 SYNX_F_PROFILE_EVENTS = 0x1
 SYNX_F_USE_GRAPHS = 0x2
 SYNX_F_NO_PERSISTENT = 0x4
+SYNX_F_CC_FP32_SUMS = 0x8
+SYNX_F_FIELDS_FP16 = 0x10
 
 ERRORS = {-1: "invalid argument", -2: "bad state", -3: "CUDA error", -4: "out of device memory", -5: "unsupported"}
 
@@ -176,6 +178,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_warp_image": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
         "synx_cc_metric": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
         "synx_cc_metric_noalloc": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
+        "synx_cc_metric_ex": (I, [V, V, P(SynxGeom), I, I, V, V, P(D), V]),
         "synx_noalloc_last_error": (C.c_char_p, []),
         "synx_smooth_field": (I, [V, V, P(SynxGeom), D, P(D), V]),
         "synx_compose": (I, [V, V, P(SynxGeom), F, V, V]),
@@ -593,11 +596,13 @@ def warp_image(img, img_geom: Geom, u, grid: Geom, out, stream=None) -> None:
     _check(load_library().synx_warp_image(_ptr(img), C.byref(a), _ptr(u), C.byref(b), _ptr(out), _stream(stream)))
 
 
-def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
+def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None, fp32_sums: bool = False) -> float:
+    """CC value and both update directions; fp32_sums selects float window sums (precision study)."""
     gc = g.to_c()
     v = C.c_double()
-    _check(load_library().synx_cc_metric(_ptr(F), _ptr(M), C.byref(gc), radius, _ptr(gF), _ptr(gM), C.byref(v),
-                                         _stream(stream)))
+    flags = SYNX_F_CC_FP32_SUMS if fp32_sums else 0
+    _check(load_library().synx_cc_metric_ex(_ptr(F), _ptr(M), C.byref(gc), radius, flags, _ptr(gF), _ptr(gM),
+                                            C.byref(v), _stream(stream)))
     return v.value
 
 

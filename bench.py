@@ -421,6 +421,159 @@ def run_serving(args) -> int:
 
 
 # ---------------------------------------------------------------------------------------------
+PREC_SIZE = (256, 256, 256)
+PREC_SPACING = (0.7, 0.7, 0.7)
+PREC_STAGE = dict(cc_radius=5, iterations=(70, 50, 20), shrink_factors=(4, 2, 1), smoothing_sigmas=(2.0, 1.0, 0.0),
+                  learning_rate=0.1, update_variance=3.0, total_variance=0.0, convergence_threshold=1e-12,
+                  convergence_window=10)
+
+
+def _twelve_bit(a):
+    a = a.astype(np.float64)
+    return ((a - a.min()) / (a.max() - a.min()) * 4095.0).astype(np.float32)
+
+
+def run_precision(args) -> int:
+    """Precision study on a 256^3 pair at 0.7 mm with intensities in [0, 4095] (CC r=5):
+    step level, the CC value and derivative fields with window sums in double (default) and in
+    float, on the raw 12-bit intensities and after antsRegistration's [0,1] rescaling; the other
+    steps (warp, update smoothing, compose, inverse) in float against the double oracle; end to
+    end, the final fields of each variant (double or float CC sums, float or half-precision field
+    storage) against the double-precision oracle registration, with each variant's throughput."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ants_b200 import phantoms
+
+    f, m = phantoms.pair_3d(PREC_SIZE, seed=0x5EED0000 + 4000)
+    f, m = _twelve_bit(f), _twelve_bit(m)
+    import torch
+    from ants_b200 import synx as S
+
+    O.set_threads(os.cpu_count() or 1)
+    g = S.Geom(PREC_SIZE, spacing=PREC_SPACING)
+    dev = torch.device("cuda", 0)
+    out = {"workload": "256^3 at 0.7 mm, layered-ellipsoid phantom pair scaled to [0,4095], CC r=5, SyN[0.1,3,0], "
+                       "f 4x2x1, s 2x1x0 vox, c 70x50x20 [1e-12,10]", "host_threads": os.cpu_count()}
+
+    def rel_rms(a, b):
+        return float(np.sqrt(((a - b) ** 2).mean() / max((b ** 2).mean(), 1e-300)))
+
+    def event_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    # ---- step level: CC ----
+    cc_rows = []
+    fp, mp = O.preprocess(f, dtype=np.float64).astype(np.float32), O.preprocess(m, dtype=np.float64).astype(np.float32)
+    for label, (a, b) in (("raw 12-bit", (f, m)), ("rescaled to [0,1]", (fp, mp))):
+        t0 = time.perf_counter()
+        v64, gF64, gM64, _ = O.cc_metric(a, b, g, 5, dtype=np.float64)
+        t_or = time.perf_counter() - t0
+        A, B = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        gF = torch.empty((3,) + g.shape, device=dev)
+        gM = torch.empty_like(gF)
+        for fp32 in (False, True):
+            v = S.cc_metric(A, B, g, 5, gF, gM, fp32_sums=fp32)
+            hF, hM = gF.cpu().numpy(), gM.cpu().numpy()
+            ms = event_ms(lambda: S.cc_metric(A, B, g, 5, gF, gM, fp32_sums=fp32))
+            cc_rows.append({"data": label, "window_sums": "float" if fp32 else "double",
+                            "metric_abs_err": abs(v - v64), "metric": v, "metric_fp64_oracle": v64,
+                            "grad_rel_rms_err": max(rel_rms(hF, gF64), rel_rms(hM, gM64)),
+                            "grad_max_abs_err": float(max(np.abs(hF - gF64).max(), np.abs(hM - gM64).max())),
+                            "ms_per_call": ms, "oracle_fp64_s": t_or})
+    out["cc_step"] = cc_rows
+
+    # ---- step level: the float steps against the double oracle ----
+    rng = np.random.default_rng(0x5EED0000 + 4001)
+    u = np.moveaxis(phantoms.smooth_field(g.shape, 8.0, 4.0, rng), -1, 0).astype(np.float32).copy()
+    w = np.moveaxis(phantoms.smooth_field(g.shape, 10.0, 5.0, rng), -1, 0).astype(np.float32).copy()
+    U, W = torch.from_numpy(u).to(dev), torch.from_numpy(w).to(dev)
+    steps = {}
+    Fp = torch.from_numpy(fp).to(dev)
+    o1 = torch.empty(g.shape, device=dev)
+    S.warp_image(Fp, g, U, g, o1)
+    ref = O.warp_image(fp, g, u, g, dtype=np.float64)
+    h = o1.cpu().numpy()
+    steps["warp"] = {"max_abs_err": float(np.abs(h - ref).max()), "rel_rms_err": rel_rms(h, ref)}
+    o3 = torch.empty_like(U)
+    S.smooth_field(U, o3, g, 3.0)
+    ref = O.smooth_field(u, g, 3.0, dtype=np.float64)
+    h = o3.cpu().numpy()
+    steps["update_smoothing"] = {"max_abs_err": float(np.abs(h - ref).max()), "rel_rms_err": rel_rms(h, ref)}
+    S.compose(U, W, g, o3)
+    ref = O.compose(u, w, g, dtype=np.float64)
+    h = o3.cpu().numpy()
+    steps["compose"] = {"max_abs_err": float(np.abs(h - ref).max()), "rel_rms_err": rel_rms(h, ref)}
+    psi = torch.zeros_like(W)
+    it = S.invert_field(W, psi, g)
+    ref, it_ref, _, _ = O.invert(w, np.zeros_like(w), g, dtype=np.float64)
+    h = psi.cpu().numpy()
+    steps["inverse"] = {"max_abs_err": float(np.abs(h - ref).max()), "rel_rms_err": rel_rms(h, ref),
+                        "iterations": it, "iterations_fp64": it_ref}
+    out["float_steps_vs_fp64_oracle"] = steps
+
+    # ---- end to end ----
+    sizes = [S.shrink_geom(g, k).count for k in PREC_STAGE["shrink_factors"]]
+    Fd, Md = torch.from_numpy(f).to(dev), torch.from_numpy(m).to(dev)
+
+    def e2e(preprocess, flags):
+        P = S.SyNParams(dim=3, preprocess=preprocess, flags=flags, **PREC_STAGE)
+        st = S.SyNStage(P)
+        st.set_images(Fd, g, Md, g)
+        st.run()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        st.set_images(Fd, g, Md, g)
+        st.run()
+        b.record()
+        b.synchronize()
+        fw, iv = st.fields()
+        vi = sum(sizes[r.level] for r in st.log())
+        res = (np.moveaxis(fw, -1, 0).copy(), np.moveaxis(iv, -1, 0).copy(), vi / (a.elapsed_time(b) / 1e3),
+               [r.metric for r in st.log()][-1])
+        st.close()
+        return res
+
+    def rms_vox(a, b):
+        sp = np.asarray(PREC_SPACING).reshape(3, 1, 1, 1)
+        return float(np.sqrt((((a - b) / sp) ** 2).sum(0).mean()))
+
+    variants = [("double CC sums, float fields (default)", S.SYNX_F_USE_GRAPHS),
+                ("float CC sums", S.SYNX_F_USE_GRAPHS | S.SYNX_F_CC_FP32_SUMS),
+                ("half-precision field storage", S.SYNX_F_USE_GRAPHS | S.SYNX_F_FIELDS_FP16),
+                ("float CC sums + half-precision fields",
+                 S.SYNX_F_USE_GRAPHS | S.SYNX_F_CC_FP32_SUMS | S.SYNX_F_FIELDS_FP16)]
+    rows = []
+    for preprocess, vlist in ((True, variants), (False, variants[:2])):
+        P = S.SyNParams(dim=3, preprocess=preprocess, **PREC_STAGE)
+        t0 = time.perf_counter()
+        rf, ri, _, rlog = O.syn_register(f, g, m, g, P, dtype=np.float64)
+        t_or = time.perf_counter() - t0
+        for name, flags in vlist:
+            fw, iv, vis, last = e2e(preprocess, flags)
+            rows.append({"intensities": "rescaled to [0,1] (antsRegistration)" if preprocess else "raw 12-bit",
+                         "variant": name, "forward_rms_vox_vs_fp64": rms_vox(fw, rf),
+                         "inverse_rms_vox_vs_fp64": rms_vox(iv, ri), "final_metric": last,
+                         "final_metric_fp64": rlog[-1]["metric"], "voxel_iter_per_s": vis,
+                         "oracle_fp64_s": t_or})
+    out["end_to_end"] = rows
+    line = {"metric": "precision study (error vs FP64 oracle, per variant)", "value": rows[0]["forward_rms_vox_vs_fp64"],
+            "unit": "voxel RMS (default variant, forward field)", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "higher_is_better": False, "dtype": "f32", "data": "synthetic: seeded phantom pair",
+            "config": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -428,7 +581,7 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="synx", choices=["synx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="single", choices=["single", "batched", "serving"],
+    ap.add_argument("--config", default="single", choices=["single", "batched", "serving", "precision"],
                     help="single: the 182x218x182 pair (default); batched: 32 pairs of uneven sizes, "
                          "batched vs sequential pairs/hour; serving: Poisson arrivals of a 2-D/3-D mix, "
                          "p50/p99 latency")
@@ -439,6 +592,8 @@ def main(argv=None) -> int:
         return run_batched(args)
     if args.config == "serving":
         return run_serving(args)
+    if args.config == "precision":
+        return run_precision(args)
 
     ws, rank, local = dist_env()
     from ants_b200 import phantoms, replicas

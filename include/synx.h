@@ -87,6 +87,9 @@ typedef struct synx_params {
 #define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
 #define SYNX_F_USE_GRAPHS 0x2     /* capture each iteration as a CUDA graph and replay it */
 #define SYNX_F_NO_PERSISTENT 0x4 /* run small levels as separate kernels too (no persistent level kernel) */
+/* Precision-study variants (not antsRegistration behaviour; both run the per-kernel path): */
+#define SYNX_F_CC_FP32_SUMS 0x8  /* CC window sums and variance terms in float instead of double */
+#define SYNX_F_FIELDS_FP16 0x10  /* half-fields rounded to half precision wherever they are stored */
 
 /* Fill *p with antsRegistration's defaults for a SyN stage of dimension dim
  * (SyN[0.1,3,0], CC radius 4, one level, 1 iteration, shrink 1, sigma 0 vox). */
@@ -246,6 +249,9 @@ int synx_warp_image(const float* img_dev, const synx_geom* img_geom, const float
  * ImageRegistration/itkCrossCorrelationRegistrationFunction.cxx:179-504). */
 int synx_cc_metric(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
                    float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
+/* Same with flags: SYNX_F_CC_FP32_SUMS selects float window sums (precision study). */
+int synx_cc_metric_ex(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius, int flags,
+                      float* grad_fixed_dev, float* grad_moving_dev, double* value, void* cuda_stream);
 
 /* Same computation as synx_cc_metric, for callers that cannot allocate device memory (a
  * pipeline being captured into a CUDA graph, a host whose device memory is owned by another
