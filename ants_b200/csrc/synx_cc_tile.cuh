@@ -147,12 +147,24 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   const T cxn = (T)(min(ox + R, nx - 1) - max(ox - R, 0) + 1);
   const T cyn = (T)(min(oy + R, ny - 1) - max(oy - R, 0) + 1);
 
+  // the (F, M) values of the slice entering the z window are loaded one slice ahead, so the
+  // loads overlap the previous slice's box sums and CC terms
+  float2 nv[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    nv[c] = make_float2(0.0f, 0.0f);
+    if (z0 < z1 && z0 + RZ < nz && gval[c]) {
+      const long long o = (long long)(z0 + RZ) * nxy + gofs[c];
+      nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
+    }
+  }
   for (int zc = z0; zc < z1; ++zc) {
     // slide the z window: subtract slice zc-RZ-1 (if it was added), add slice zc+RZ
     const int ze = zc + RZ, zl = zc - RZ - 1;
     const int slot = pmod(ze, RD);
     const bool sub = zc > z0 && zl >= 0;
     const bool zin = ze < nz;
+    const bool znext = zc + 1 < z1 && ze + 1 < nz;
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
       int col = tid + c * 256;
@@ -166,11 +178,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
           acc[c][3] -= m * m;
           acc[c][4] -= f * m;
         }
-        float2 v = make_float2(0.0f, 0.0f);
+        const float2 v = nv[c];  // zero outside the volume
         if (zin && gval[c]) {
-          long long o = (long long)ze * nxy + gofs[c];
-          v.x = __ldg(Ft + o);
-          v.y = __ldg(Mt + o);
           const T f = v.x, m = v.y;
           acc[c][0] += f;
           acc[c][1] += m;
@@ -181,6 +190,11 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         ring[slot * HC + col] = v;
 #pragma unroll
         for (int q = 0; q < 5; ++q) cs[q * HY * CSP + sofs[c]] = acc[c][q];
+        nv[c] = make_float2(0.0f, 0.0f);
+        if (znext && gval[c]) {
+          const long long o = (long long)(ze + 1) * nxy + gofs[c];
+          nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
+        }
       }
     }
     __syncthreads();

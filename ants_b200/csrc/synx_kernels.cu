@@ -238,6 +238,9 @@ void launch_warp_image(const float* img, const GridInfo& gi, const float* u, con
 // and, in 3-D, a z kernel (one thread per column chunk).  The SyN epilogue (boundary zeroing,
 // blend for small variances) and the max ||u/h|| reduction run in the last pass.
 // ------------------------------------------------------------------------------------------
+// rows of the standalone xy smoothing tile (32 x 32: 2R halo rows per 32 output rows)
+constexpr int kSmoothTileY = 32;
+
 template <int DIM, int R>
 __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, 
   __shared__ float red[32];
   const int h = blockIdx.z / d.nz;
   const int z = blockIdx.z - h * d.nz;
-  const float mx = smooth_xy_tile<DIM, R>(a, d, blockIdx.x, blockIdx.y, z, h, sm3);
+  const float mx = smooth_xy_tile<DIM, R, kSmoothTileY>(a, d, blockIdx.x, blockIdx.y, z, h, sm3);
   if (DIM == 2 && a.do_max) {
     const float bm = block_max_f(mx, red);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
@@ -277,10 +280,10 @@ bool smooth3_supported(int dim, const int R[3]) { return smooth3_radius(dim, R) 
 template <int R>
 static cudaError_t smooth3_attr_both() {
   cudaError_t e = cudaFuncSetAttribute(k_smooth_xy<3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(smooth3_smem_floats(3, R) * 4));
+                                       (int)(smooth3_smem_floats(3, R, kSmoothTileY) * 4));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_smooth_xy<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(smooth3_smem_floats(2, R) * 4));
+                             (int)(smooth3_smem_floats(2, R, kSmoothTileY) * 4));
   return e;
 }
 
@@ -342,9 +345,10 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   const int dim = g.d.dim;
   int RR = 1;
   Smooth3Args a = make_smooth_args(in, dim == 3 ? tmp : out, orig, halves, g, khost, R, epilogue, w1, w2, maxnorm, &RR);
+  // xy tiles are 32 x kSmoothTileY; the z pass below keeps 32 x 8 columns
   const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
-  const dim3 gxy(gx, gy, g.d.nz * halves);
-  const size_t smem = smooth3_smem_floats(dim, RR) * 4;
+  const dim3 gxy(gx, (g.d.ny + kSmoothTileY - 1) / kSmoothTileY, g.d.nz * halves);
+  const size_t smem = smooth3_smem_floats(dim, RR, kSmoothTileY) * 4;
   count_launch();
 #define SYNX_SXY(RV)                                             \
   case RV:                                                       \
@@ -512,6 +516,7 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
 // ------------------------------------------------------------------------------------------
 struct InvLaunch {
   int k, max_iter, phase, stop_aware, halves;
+  int tx, ty, tz;  // 32 x 8 x zb tiles of one half
   double mean_tol, max_tol;
 };
 
@@ -523,10 +528,11 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaun
   __shared__ double redd[32];
   __shared__ float redf[32];
   __shared__ int am_last;
-  const int gz = gridDim.z / L.halves;
-  const int h = blockIdx.z / gz;
-  const int bz = blockIdx.z - h * gz;
-  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * bz);
+  // gridDim.x / halves blocks per half walk that half's tiles: one wave of blocks, so the
+  // launches that find their half converged cost one short launch
+  const int nb = gridDim.x / L.halves;
+  const int h = blockIdx.x / nb;
+  const int bid = blockIdx.x - h * nb;
   InvCtl& C = ctl->inv[L.phase][h];
   const int k = L.k;
   bool apply = false, stats = true;
@@ -550,11 +556,14 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaun
   }
   double acc = 0.0;
   float mxl = 0.0f;
-  invert_tile<DIM, DIAG>(a, h, blockIdx.x, blockIdx.y, bz, apply, stats, eps, lim, acc, mxl);
+  const int ntiles = L.tx * L.ty * L.tz;
+  for (int t = bid; t < ntiles; t += nb) {
+    const int bx = t % L.tx, r = t / L.tx;
+    invert_tile<DIM, DIAG>(a, h, bx, r % L.ty, r / L.ty, apply, stats, eps, lim, acc, mxl);
+  }
   if (!stats) return;
   const double bs = block_sum_d(acc, redd);
   const float bm = block_max_f(mxl, redf);
-  const int nb = gridDim.x * gridDim.y * gz;
   if (threadIdx.x == 0) {
     psum[h * pcap + bid] = bs;
     pmax[h * pcap + bid] = bm;
@@ -584,8 +593,9 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaun
   }
 }
 
-constexpr int kInvTarget = 148 * 24;  // blocks: short per-thread z walks, small last-wave tail
-int inv_blocks(const GridInfo& g) { return map3(g.d, 2, kInvTarget).nblocks; }
+constexpr int kInvTarget = 148 * 24;    // tiles: short per-thread z walks
+constexpr int kInvBlocksPerHalf = 296;  // 148 SMs x 4 resident blocks shared by two halves
+int inv_blocks(const GridInfo& g) { return std::max(map3(g.d, 2, kInvTarget).nblocks, kInvBlocksPerHalf); }
 
 InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb,
                       float* const* ecache) {
@@ -605,21 +615,23 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
                         bool stop_aware, float* const* ecache) {
   count_launch();
-  // the block decomposition is the same for one or two halves, so the partial buffers sized by
-  // inv_blocks() fit either
+  // tiles of one half (the same decomposition for one or two halves); blocks per half: one
+  // wave, at most the partial slots inv_blocks() sized
   const Map3 m2 = map3(g.d, 2, kInvTarget);
-  Map3 m = m2;
-  m.grid.z = (m2.grid.z / 2) * halves;
-  const InvArgs a = make_inv_args(phi, psi, halves, g, m.zb, ecache);
-  InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, mean_tol, max_tol};
+  const int tz = (int)m2.grid.z / 2;
+  const int ntiles = (int)m2.grid.x * (int)m2.grid.y * tz;
+  const int nb = std::max(1, std::min({ntiles, kInvBlocksPerHalf, pb.capacity}));
+  const InvArgs a = make_inv_args(phi, psi, halves, g, m2.zb, ecache);
+  InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, (int)m2.grid.x, (int)m2.grid.y, tz, mean_tol, max_tol};
   Affine am = make_affine(g, g);
   const bool dg = affine_diag(am);
+  const dim3 grid((unsigned)(nb * halves));
   if (g.d.dim == 3) {
-    if (dg) k_invert_step<3, true><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
-    else k_invert_step<3, false><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    if (dg) k_invert_step<3, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    else k_invert_step<3, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   } else {
-    if (dg) k_invert_step<2, true><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
-    else k_invert_step<2, false><<<m.grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    if (dg) k_invert_step<2, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    else k_invert_step<2, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   }
 }
 

@@ -288,21 +288,24 @@ struct Smooth3Args {
   float ih[3];
 };
 
-__host__ __device__ inline size_t smooth3_smem_floats(int dim, int R) {
-  const int HXP = (32 + 2 * R + 3) & ~3, HY = 8 + 2 * R;
+__host__ __device__ inline size_t smooth3_smem_floats(int dim, int R, int TY = 8) {
+  const int HXP = (32 + 2 * R + 3) & ~3, HY = TY + 2 * R;
   return (size_t)dim * HY * HXP + (size_t)dim * HY * 32;
 }
 
-// xy part for one (32 x 8 tile, slice z, field h): halo tile of every component staged in shared
+// xy part for one (32 x TY tile, slice z, field h): halo tile of every component staged in shared
 // memory with replicate-edge indices, convolved along x (each work item makes four consecutive
-// outputs from float4 loads) and then along y.  In 3-D the xy-smoothed values go to `out` for the
-// z part; in 2-D this is the whole filter and the SyN epilogue runs here (max norm returned).
-// All threads of the block must call it; `sm` holds smooth3_smem_floats(DIM, R) floats.
-template <int DIM, int R>
+// outputs from float4 loads) and then along y (each thread makes TY/8 consecutive rows of one
+// column from registers).  Taller tiles convolve fewer halo rows along x per output (TY + 2R
+// rows for TY outputs).  In 3-D the xy-smoothed values go to `out` for the z part; in 2-D this
+// is the whole filter and the SyN epilogue runs here (max norm returned).  All threads of the
+// block must call it; `sm` holds smooth3_smem_floats(DIM, R, TY) floats.
+template <int DIM, int R, int TY = 8>
 __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
                                                 float* sm) {
-  constexpr int K = 2 * R + 1;
-  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = 8 + 2 * R;
+  static_assert(TY % 8 == 0, "8 warps share the tile rows");
+  constexpr int K = 2 * R + 1, RPT = TY / 8;
+  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
   constexpr int NQ = (2 * R + 3) / 4 + 1;  // float4 loads covering 4 + 2R taps
   float* tile = sm;                    // [DIM][HY][HXP]
   float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
@@ -310,7 +313,7 @@ __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims
   const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
   float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  const int x0 = bx * 32, y0 = by * 8;
+  const int x0 = bx * 32, y0 = by * TY;
   const float* plane = src + z * nxy;
   for (int row = ty; row < DIM * HY; row += 8) {
     const int c = row / HY, hy = row - c * HY;
@@ -344,41 +347,52 @@ __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims
     reinterpret_cast<float4*>(xsum + row * 32)[q] = make_float4(o[0], o[1], o[2], o[3]);
   }
   __syncthreads();
-  const int ox = x0 + tx, oy = y0 + ty;
-  const bool ok = ox < nx && oy < ny;
-  float y[DIM];
+  const int ox = x0 + tx, ty0 = ty * RPT;
+  float y[DIM][RPT];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
-    const float* col = xsum + (c * HY + ty) * 32 + tx;
-    float acc = 0.0f;
+    const float* col = xsum + (c * HY + ty0) * 32 + tx;
+    float w[RPT + 2 * R];
 #pragma unroll
-    for (int j = 0; j < K; ++j) acc = fmaf(a.k[1][j], col[j * 32], acc);
-    y[c] = acc;
+    for (int j = 0; j < RPT + 2 * R; ++j) w[j] = col[j * 32];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc = fmaf(a.k[1][j], w[r + j], acc);
+      y[c][r] = acc;
+    }
   }
   __syncthreads();  // the tile and xsum may be reused by the caller's next tile
   float mx = 0.0f;
-  if (!ok) return mx;
-  const int i = z * nxy + oy * nx + ox;
-  if (DIM == 3) {
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) dst[c * N + i] = y[c];
-    return mx;
-  }
+  if (ox >= nx) return mx;
   const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
-  const bool edge = a.epilogue && (ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1);
-  float nrm2 = 0.0f;
 #pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    float r = y[c];
-    if (a.epilogue) {
-      if (edge) r = 0.0f;
-      else if (a.w2 != 0.0f) r = r * a.w1 + org[c * N + i] * a.w2;
+  for (int r = 0; r < RPT; ++r) {
+    const int oy = y0 + ty0 + r;
+    if (oy >= ny) break;
+    const int i = z * nxy + oy * nx + ox;
+    if (DIM == 3) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) dst[c * N + i] = y[c][r];
+      continue;
     }
-    const float q = r * a.ih[c];
-    nrm2 += q * q;
-    dst[c * N + i] = r;
+    const bool edge = a.epilogue && (ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1);
+    float nrm2 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      float v = y[c][r];
+      if (a.epilogue) {
+        if (edge) v = 0.0f;
+        else if (a.w2 != 0.0f) v = v * a.w1 + org[c * N + i] * a.w2;
+      }
+      const float q = v * a.ih[c];
+      nrm2 += q * q;
+      dst[c * N + i] = v;
+    }
+    mx = fmaxf(mx, sqrtf(nrm2));
   }
-  return sqrtf(nrm2);
+  return mx;
 }
 
 // z part (3-D) for one (x, y) column of field h over slices [zc*ZC, zc*ZC + ZC): the last 2R+1
