@@ -33,7 +33,7 @@ void* pick_kernel(int dim, int rcc, bool batch) {
 
 size_t level_smem_bytes(int dim, int cc_radius, int r_smooth) {
   const size_t a = cc_smem_bytes(dim, cc_radius);
-  const size_t b = smooth3_smem_floats(dim, std::max(r_smooth, kLevelMaxSmoothRadius)) * 4;
+  const size_t b = smooth3_smem_floats(dim, std::max(r_smooth, kLevelMaxSmoothRadius), kLevelSmoothTY) * 4;
   return std::max(a, b);
 }
 

@@ -43,6 +43,7 @@ struct BatchLevelArgs {
 };
 
 constexpr int kLevelMaxSmoothRadius = 8;
+constexpr int kLevelSmoothTY = 32;  // rows of the xy smoothing tiles in the level kernel
 
 size_t level_smem_bytes(int dim, int cc_radius, int r_smooth);
 // Largest cooperative grid for the level kernel on `device` (0 if unsupported).

@@ -86,7 +86,7 @@ struct Units {
 
 template <int DIM, int R>
 __device__ __forceinline__ float smooth_xy_r(const LevelArgs& A, int bx, int by, int z, int h, float* sm) {
-  return smooth_xy_tile<DIM, R>(A.sxy, A.g, bx, by, z, h, sm);
+  return smooth_xy_tile<DIM, R, kLevelSmoothTY>(A.sxy, A.g, bx, by, z, h, sm);
 }
 
 template <int DIM>
@@ -214,7 +214,7 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
   const int G = gp.G, b = gp.b, tid = threadIdx.x;
   const Units UW{A.el_gx, A.el_gy, A.warp_gz, 1};
   const Units UC{A.el_gx, A.el_gy, A.comp_gz, 2};
-  const Units UXY{A.el_gx, A.el_gy, A.g.nz, 2};
+  const Units UXY{A.el_gx, (A.g.ny + kLevelSmoothTY - 1) / kLevelSmoothTY, A.g.nz, 2};
   const Units UZ{A.el_gx, A.el_gy, A.sz_gz, 2};
   const int ncc = A.cc_gx * A.cc_gy * A.cc_gz;
   for (int it = 0; it < A.iters; ++it) {
