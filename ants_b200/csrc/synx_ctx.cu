@@ -162,6 +162,8 @@ struct synx_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaStream_t aux = nullptr;        // captures the inverse loop bodies of the level graphs
+  bool loop_graphs_failed = false;   // the driver refused conditional nodes: graphs use plain launches
   std::string err;
   bool images_set = false;
   synx_geom geF{}, geM{};
@@ -511,7 +513,11 @@ void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const
 }
 
 // One SyN iteration on the current level (all launches asynchronous, stop-aware).
-void enqueue_iteration(synx_ctx* c, bool profile) {
+// Enqueues one SyN iteration on c->stream.  loops (only while the stream is being captured into a
+// graph): each fixed-point inverse becomes its k = 0 launch followed by a conditional WHILE node
+// whose body is one sub-iteration launch plus the loop-control kernel, instead of all
+// max_iter + 1 launches of which the converged tail does nothing.
+cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
   const GridInfo& g = c->cur_grid;
   cudaStream_t s = c->stream;
   auto ev = [&](void) -> int {
@@ -575,24 +581,57 @@ void enqueue_iteration(synx_ctx* c, bool profile) {
   int e1 = profile ? ev() : -1;
   // the CC derivative buffers are free until the next iteration: they carry the inverse residual
   float* ecache[2] = {c->gFu, c->gMu};
+  auto inversion = [&](int phase, const float* const* phi, float* const* psi) -> cudaError_t {
+    const double mt = c->P.inv_mean_tol, xt = c->P.inv_max_tol;
+    if (!loops) {
+      for (int k = 0; k <= mi; ++k) launch_invert_step(phi, psi, 2, g, k, mi, mt, xt, c->ctl, phase, pb, s, true, ecache);
+      return cudaSuccess;
+    }
+    launch_invert_step(phi, psi, 2, g, 0, mi, mt, xt, c->ctl, phase, pb, s, true, ecache);
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd);
+    if (e != cudaSuccess) return e;
+    if (st != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+    cudaGraphConditionalHandle h = 0;
+    if ((e = cudaGraphConditionalHandleCreate(&h, cg, 0, 0)) != cudaSuccess) return e;
+    launch_inv_loop_control(c->ctl, phase, h, mi, true, s);
+    if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd)) != cudaSuccess) return e;
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if ((e = cudaGraphAddNode(&node, cg, deps, nd, &np)) != cudaSuccess) return e;
+    if ((e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+      return e;
+    if ((e = cudaStreamBeginCaptureToGraph(c->aux, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return e;
+    launch_invert_step(phi, psi, 2, g, -1, mi, mt, xt, c->ctl, phase, pb, c->aux, true, ecache);
+    launch_inv_loop_control(c->ctl, phase, h, mi, false, c->aux);
+    cudaGraph_t body = nullptr;
+    return cudaStreamEndCapture(c->aux, &body);
+  };
   {
     const float* phi[2] = {c->phiF, c->phiM};
     float* psi[2] = {c->psiF, c->psiM};
-    for (int k = 0; k <= mi; ++k)
-      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 0, pb, s, true,
-                         ecache);
+    const cudaError_t e = inversion(0, phi, psi);
+    if (e != cudaSuccess) return e;
   }
   if (fp16) round_pair(c->psiF, c->psiM);
   {
     const float* phi[2] = {c->psiF, c->psiM};
     float* psi[2] = {c->phiF, c->phiM};
-    for (int k = 0; k <= mi; ++k)
-      launch_invert_step(phi, psi, 2, g, k, mi, c->P.inv_mean_tol, c->P.inv_max_tol, c->ctl, 1, pb, s, true,
-                         ecache);
+    const cudaError_t e = inversion(1, phi, psi);
+    if (e != cudaSuccess) return e;
   }
   if (fp16) round_pair(c->phiF, c->phiM);
   if (profile) c->ev_pairs_inv.push_back({e1, ev()});
   launch_converge(c->ctl, c->logdev, c->P.convergence_threshold, c->P.convergence_window, s);
+  return cudaSuccess;
 }
 
 // The persistent level kernel serves small levels (launch latency dominates there) when the
@@ -758,24 +797,44 @@ int level_iterate(synx_ctx* c, int level) {
     // for a given level: the buffers are reset to the same assignment by synx_set_images) and
     // replayed `iters` times; the device-side stop flag ends a converged level early
     if (!c->gexec_lv[level]) {
-      cudaGraph_t graph;
-      const long long before = launch_count();
-      CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      enqueue_iteration(c, false);
-      CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
-      c->graph_nodes[level] = launch_count() - before;
-      add_launch_count(-c->graph_nodes[level]);  // capture launches nothing
-      cudaError_t e = cudaGraphInstantiate(&c->gexec_lv[level], graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) {
+      if (!c->aux && !c->loop_graphs_failed &&
+          cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        c->aux = nullptr;
+        c->loop_graphs_failed = true;
+      }
+      // with the inverse loops as conditional nodes first; if the driver refuses them, again
+      // with plain launches
+      for (bool loops : {!c->loop_graphs_failed, false}) {
+        const long long before = launch_count();
+        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t eq = enqueue_iteration(c, false, loops);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+        c->graph_nodes[level] = launch_count() - before;
+        add_launch_count(-c->graph_nodes[level]);  // capture launches nothing
+        cudaError_t e = eq != cudaSuccess ? eq : ee;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&c->gexec_lv[level], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e == cudaSuccess) break;
         c->gexec_lv[level] = nullptr;
-        return set_err(c, SYNX_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        if (loops && c->aux) {
+          cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+          if (cudaStreamIsCapturing(c->aux, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t dead = nullptr;
+            cudaStreamEndCapture(c->aux, &dead);
+            if (dead) cudaGraphDestroy(dead);
+          }
+        }
+        cudaGetLastError();
+        if (!loops) return set_err(c, SYNX_E_CUDA, std::string("level graph: ") + cudaGetErrorString(e));
+        c->loop_graphs_failed = true;
       }
     }
     for (int k = 0; k < iters; ++k) CUDA_TRY(c, cudaGraphLaunch(c->gexec_lv[level], c->stream));
     add_launch_count(c->graph_nodes[level] * (long long)iters);
   } else {
-    for (int k = 0; k < iters; ++k) enqueue_iteration(c, profile);
+    for (int k = 0; k < iters; ++k) CUDA_TRY(c, enqueue_iteration(c, profile));
   }
   return SYNX_OK;
 }
@@ -1140,6 +1199,7 @@ int synx_destroy(synx_ctx* ctx) {
   for (auto e : ctx->lev_ev)
     if (e) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
   delete ctx;
   return SYNX_OK;
 }

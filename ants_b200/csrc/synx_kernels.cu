@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaun
   const int h = blockIdx.x / nb;
   const int bid = blockIdx.x - h * nb;
   InvCtl& C = ctl->inv[L.phase][h];
-  const int k = L.k;
+  const int k = L.k >= 0 ? L.k : *(volatile const int*)&ctl->inv[L.phase][0].kdev;
   bool apply = false, stats = true;
   float eps = 0.0f, lim = 0.0f;
   if (k > 0) {
@@ -633,6 +633,28 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
     if (dg) k_invert_step<2, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
     else k_invert_step<2, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   }
+}
+
+__global__ void k_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter,
+                                   int init) {
+  InvCtl* C = ctl->inv[phase];
+  unsigned go = 0;
+  if (init) {
+    C[0].kdev = 1;
+    go = ctl->stop ? 0u : 1u;
+  } else {
+    const int next = C[0].kdev + 1;
+    const int s = next & 1;
+    go = (!ctl->stop && next <= max_iter && (C[0].exec[s] || C[1].exec[s])) ? 1u : 0u;
+    C[0].kdev = next;
+  }
+  cudaGraphSetConditional(handle, go);
+}
+
+void launch_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, bool init,
+                             cudaStream_t s) {
+  count_launch();
+  k_inv_loop_control<<<1, 1, 0, s>>>(ctl, phase, handle, max_iter, init ? 1 : 0);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -16,7 +16,8 @@ struct InvCtl {
   double mean[2];
   int iters;
   unsigned counter;
-  int pad[2];
+  int kdev;  // sub-iteration index for launches that read it from the device (graph loop bodies)
+  int pad;
 };
 
 constexpr int kMaxWindow = 64;
@@ -109,10 +110,18 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
 // One launch of the fused fixed-point inverse (k = 0 .. max_iter) for `halves` pairs.
 int inv_blocks(const GridInfo& g);
 // ecache: per-half residual buffers (D x N floats each) that carry the residual from a launch's
-// statistics pass to the next launch's update; null recomputes it there.
+// statistics pass to the next launch's update; null recomputes it there.  k < 0: the launch is a
+// CUDA-graph loop body and reads its sub-iteration index from the control block (kdev).
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
                         bool stop_aware = true, float* const* ecache = nullptr);
+// Loop control of a fixed-point inverse captured as a conditional WHILE graph node: init (after
+// the k = 0 statistics launch) sets kdev = 1 and the loop condition to "level still running";
+// the step form (the loop body's second kernel) advances kdev and sets the condition to "some
+// half still iterating and kdev <= max_iter".  It always sets the condition, so the loop ends
+// within max_iter bodies.
+void launch_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, bool init,
+                             cudaStream_t s);
 
 void launch_converge(IterCtl* ctl, LogDev log, double threshold, int window, cudaStream_t s);
 

@@ -581,6 +581,9 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="synx", choices=["synx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-launches", action="store_true",
+                    help="launch every kernel directly instead of replaying per-level CUDA graphs (the same "
+                         "work; profilers see each kernel, which they do not inside graphs with conditional nodes)")
     ap.add_argument("--config", default="single", choices=["single", "batched", "serving", "precision"],
                     help="single: the 182x218x182 pair (default); batched: 32 pairs of uneven sizes, "
                          "batched vs sequential pairs/hour; serving: Poisson arrivals of a 2-D/3-D mix, "
@@ -623,8 +626,8 @@ def main(argv=None) -> int:
 
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    stage = S.SyNStage(S.SyNParams(dim=3, flags=S.SYNX_F_USE_GRAPHS, **STAGE), device=local,
-                       stream=stream.cuda_stream)
+    stage = S.SyNStage(S.SyNParams(dim=3, flags=0 if args.plain_launches else S.SYNX_F_USE_GRAPHS, **STAGE),
+                       device=local, stream=stream.cuda_stream)
     Fd = torch.from_numpy(fixed).to(dev)
     Md = torch.from_numpy(moving).to(dev)
     fwd_d = torch.empty((3,) + g.shape, device=dev)
@@ -725,7 +728,7 @@ def main(argv=None) -> int:
             "data": "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field",
             "config": {"workload": WORKLOAD, "iterations_run_per_level": [its.get(l, 0) for l in range(4)],
                        "voxel_iterations_per_step": vox_iters // args.steps, "l2": "flushed between steps (256 MB)",
-                       "parallelism": f"replicas x{ws}", "cuda_graphs": True},
+                       "parallelism": f"replicas x{ws}", "cuda_graphs": not args.plain_launches},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(Fh.nbytes + Mh.nbytes),
                     "d2h_bytes_per_step": int(fwd_h.nbytes + inv_h.nbytes),
                     "ms_per_step": 1000.0 * t_e2e / args.steps},

@@ -106,21 +106,27 @@ def test_total_field_smoothing_and_blend(cuda, dim, size, uvar, tvar):
     assert rms_vox(inv, ri, go.spacing) <= 0.05
 
 
-def test_graph_replay_is_bit_identical_and_deterministic(cuda):
+@pytest.mark.parametrize("persistent", [True, False])
+def test_graph_replay_is_bit_identical_and_deterministic(cuda, persistent):
+    # graph replay (with the fixed-point inverse loops as conditional graph nodes on the
+    # per-kernel path) gives the same bits as plain launches, run after run
     f, m = make_pair(3, (36, 34, 32), seed=3)
     g = Geom((36, 34, 32))
+    base = 0 if persistent else SYNX_F_NO_PERSISTENT
     outs = []
-    for flags in (0, SYNX_F_USE_GRAPHS, SYNX_F_USE_GRAPHS):
+    for flags in (base, base | SYNX_F_USE_GRAPHS, base | SYNX_F_USE_GRAPHS):
         P = SyNParams(dim=3, cc_radius=3, iterations=(6, 4), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0),
                       flags=flags)
         with SyNStage(P) as st:
             st.set_images(f, g, m, g)
             st.run()
-            outs.append((st.fields(), [r.metric for r in st.log()]))
+            outs.append((st.fields(), [(r.metric, r.inverse_iterations) for r in st.log()]))
     for o in outs[1:]:
         np.testing.assert_array_equal(o[0][0], outs[0][0][0])
         np.testing.assert_array_equal(o[0][1], outs[0][0][1])
         assert o[1] == outs[0][1]
+    # the cold-started first inversions take several sub-iterations: the loops really iterate
+    assert max(k for _, k in outs[0][1]) > 4
 
 
 @pytest.mark.parametrize("dim,size,radius", [(2, (80, 66), 1), (2, (50, 61), 7), (3, (26, 23, 29), 5)])
@@ -146,12 +152,13 @@ def test_persistent_level_radii_and_repeatability(cuda, dim, size, radius):
         assert rms_vox(planes(a), planes(b), sp) <= 0.05
 
 
-def test_convergence_stops_level_early(cuda):
+@pytest.mark.parametrize("path", sorted(PATHS))
+def test_convergence_stops_level_early(cuda, path):
     # a pair that is already aligned stops as soon as the window fills (slope >= 0)
     f, _ = make_pair(2, (64, 64), seed=5)
     g = Geom((64, 64))
     P = SyNParams(dim=2, cc_radius=2, iterations=(40,), shrink_factors=(1,), smoothing_sigmas=(0.0,),
-                  convergence_threshold=1e-6, convergence_window=10)
+                  convergence_threshold=1e-6, convergence_window=10, flags=PATHS[path])
     with SyNStage(P) as st:
         st.set_images(f, g, f, g)
         st.run()
