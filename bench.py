@@ -59,8 +59,8 @@ BYTES_PER_ITER_VOXEL = 176
 BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi
 ROOF_LEVEL = 2  # the 91x109x91 level: the largest k_level launch
 # DRAM bytes (read + write) of that k_level launch, from the ncu capture summarised in
-# profiles/k_level_91x109x91.md (5.518 GB read + 7.263 GB written)
-LEVEL_TRAFFIC_BYTES = 12.781e9
+# profiles/k_level_91x109x91.md (5.521 GB read + 7.273 GB written)
+LEVEL_TRAFFIC_BYTES = 12.794e9
 
 
 def dist_env():
