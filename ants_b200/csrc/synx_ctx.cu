@@ -958,7 +958,14 @@ struct synx_batch {
   std::vector<LevelArgs> h_args;
   std::vector<int> h_first;
   cudaEvent_t ev = nullptr;
+  // lanes: the levels that run their own kernels (too large for the level kernel) run on these
+  // streams concurrently, pair by pair round robin, so one pair's launch gaps and kernel tails
+  // overlap another pair's work
+  std::vector<cudaStream_t> lanes;
+  std::vector<cudaEvent_t> lane_ev;
 };
+
+constexpr int kBatchLanes = 4;
 
 namespace {
 
@@ -1078,9 +1085,27 @@ int batch_step(synx_batch* b, synx_ctx* const* cs, int n, cudaStream_t s, int* a
         return batch_err(b, SYNX_E_CUDA, std::string("synx_batch_step: batched level launch: ") + cudaGetErrorString(e));
     }
   }
-  for (synx_ctx* c : rest) {
-    const int rc = level_iterate(c, c->cur_level);
-    if (rc) return fail(c, rc);
+  if (!rest.empty()) {
+    // fork: every lane waits for the set-up enqueued on s, runs its pairs' levels, and s joins
+    const int L = (int)std::min(b->lanes.size(), rest.size());
+    if (L > 1) {
+      if (cudaEventRecord(b->ev, s) != cudaSuccess) return batch_err(b, SYNX_E_CUDA, "synx_batch_step: fork");
+      for (int l = 0; l < L; ++l)
+        if (cudaStreamWaitEvent(b->lanes[l], b->ev, 0) != cudaSuccess)
+          return batch_err(b, SYNX_E_CUDA, "synx_batch_step: fork");
+    }
+    for (size_t i = 0; i < rest.size(); ++i) {
+      synx_ctx* c = rest[i];
+      if (L > 1) c->stream = b->lanes[i % L];
+      const int rc = level_iterate(c, c->cur_level);
+      c->stream = s;
+      if (rc) return fail(c, rc);
+    }
+    if (L > 1)
+      for (int l = 0; l < L; ++l)
+        if (cudaEventRecord(b->lane_ev[l], b->lanes[l]) != cudaSuccess ||
+            cudaStreamWaitEvent(s, b->lane_ev[l], 0) != cudaSuccess)
+          return batch_err(b, SYNX_E_CUDA, "synx_batch_step: join");
   }
   for (synx_ctx* c : act) {
     const int rc = level_readback(c, c->cur_level);
@@ -1288,7 +1313,18 @@ int synx_batch_create(int device, synx_batch** out) {
   if (cudaSetDevice(device) != cudaSuccess) return set_err(nullptr, SYNX_E_CUDA, "synx_batch_create: cudaSetDevice");
   synx_batch* b = new synx_batch();
   b->device = device;
-  if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+  bool lanes_ok = true;
+  for (int l = 0; l < kBatchLanes && lanes_ok; ++l) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    lanes_ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+    if (st) b->lanes.push_back(st);
+    if (ev) b->lane_ev.push_back(ev);
+  }
+  if (!lanes_ok || cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+    for (auto st : b->lanes) cudaStreamDestroy(st);
+    for (auto ev : b->lane_ev) cudaEventDestroy(ev);
     delete b;
     return set_err(nullptr, SYNX_E_CUDA, "synx_batch_create: event creation failed");
   }
@@ -1302,6 +1338,11 @@ int synx_batch_destroy(synx_batch* b) {
   if (b->d_args) cudaFree(b->d_args);
   if (b->d_first) cudaFree(b->d_first);
   if (b->ev) cudaEventDestroy(b->ev);
+  for (auto st : b->lanes) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (auto ev : b->lane_ev) cudaEventDestroy(ev);
   delete b;
   return SYNX_OK;
 }

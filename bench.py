@@ -221,7 +221,8 @@ def run_batched(args) -> int:
     dev_pairs = [(torch.from_numpy(np.ascontiguousarray(f)).to(dev), torch.from_numpy(np.ascontiguousarray(m)).to(dev))
                  for f, m in pairs]
     outs = [(torch.empty((3,) + g.shape, device=dev), torch.empty((3,) + g.shape, device=dev)) for g in geoms]
-    P = S.SyNParams(dim=3, **BATCH_STAGE)
+    # both arms replay their per-kernel levels from CUDA graphs (the faster single-pair setting)
+    P = S.SyNParams(dim=3, flags=S.SYNX_F_USE_GRAPHS, **BATCH_STAGE)
     seq = [S.SyNStage(P, device=local, stream=stream.cuda_stream) for _ in range(BATCH_PAIRS)]
     bat = [S.SyNStage(P, device=local, stream=stream.cuda_stream) for _ in range(BATCH_PAIRS)]
     batch = S.Batch(local)
