@@ -256,7 +256,9 @@ __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, 
 }
 
 template <int R>
-__global__ void __launch_bounds__(256) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
+// up to R = 6: at least 3 blocks per SM (a few ring registers spill at R = 5, 6; the extra warps
+// hide more load latency than the spills cost); wider rings keep every register they need
+__global__ void __launch_bounds__(256, (R <= 6 ? 3 : 1)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
   __shared__ float red[32];
   const int nzc = gridDim.z / a.halves;
