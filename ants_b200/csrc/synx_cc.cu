@@ -1,4 +1,5 @@
 // Neighbourhood cross-correlation kernel (value and both SyN update directions), sm_100a.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 
@@ -51,16 +52,28 @@ static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, flo
                                                                           cc_out);
 }
 
+// z-chunk of one CC block.  Each block first fills its z window (2R slices, column updates only,
+// about a third of a full slice's work each), then marches its chunk; 2 blocks are resident per
+// SM.  The chunk count minimises waves x (chunk + warm-up cost), so the last wave is not mostly
+// empty (e.g. 182 slices over 6 x 28 tiles: 7 chunks, 1176 blocks = 3.97 waves of 296).
 static int cc_zchunk(const GridInfo& g, int radius) {
   if (g.d.dim == 2) return 1;
-  const int bx = (g.d.nx + 31) / 32, by = (g.d.ny + 7) / 8;
-  const int target = 148 * 6;
-  int chunks = (target + bx * by - 1) / (bx * by);
-  int zc = (g.d.nz + chunks - 1) / chunks;
-  zc = zc < 4 * radius ? 4 * radius : zc;
-  if (zc > g.d.nz) zc = g.d.nz;
-  if (zc < 1) zc = 1;
-  return zc;
+  const int bxy = ((g.d.nx + 31) / 32) * ((g.d.ny + 7) / 8);
+  const int nz = g.d.nz, slots = 2 * 148;
+  const int max_chunks = std::max(1, nz / std::max(2 * radius, 1));
+  int best_zc = nz;
+  double best = 1e30;
+  for (int c = 1; c <= max_chunks; ++c) {
+    const int zc = (nz + c - 1) / c;
+    const int blocks = bxy * ((nz + zc - 1) / zc);
+    const double waves = (double)((blocks + slots - 1) / slots);
+    const double cost = waves * (zc + 0.35 * 2 * radius);
+    if (cost < best - 1e-9) {
+      best = cost;
+      best_zc = zc;
+    }
+  }
+  return best_zc;
 }
 
 int cc_blocks(const GridInfo& g, int radius) {
