@@ -660,7 +660,7 @@ void launch_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle
 }
 
 // ------------------------------------------------------------------------------------------
-// Convergence monitor and per-iteration log (one thread).
+// Convergence monitor and per-iteration log (one warp).
 // ------------------------------------------------------------------------------------------
 __global__ void k_converge(IterCtl* ctl, LogDev log, double threshold, int window) {
   if (ctl->stop) return;
@@ -669,7 +669,7 @@ __global__ void k_converge(IterCtl* ctl, LogDev log, double threshold, int windo
 
 void launch_converge(IterCtl* ctl, LogDev log, double threshold, int window, cudaStream_t s) {
   count_launch();
-  k_converge<<<1, 1, 0, s>>>(ctl, log, threshold, window);
+  k_converge<<<1, 32, 0, s>>>(ctl, log, threshold, window);
 }
 
 

@@ -272,8 +272,11 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
       if (tid == 0) {
         ctl->cc_sum = s;
         ctl->metric = -s / (double)A.g.N;
-        converge_step(ctl, A.log, A.conv_threshold, A.conv_window);
         ctl->maxnorm[0] = ctl->maxnorm[1] = 0u;
+      }
+      if (tid < 32) {
+        __syncwarp();
+        converge_step(ctl, A.log, A.conv_threshold, A.conv_window);
       }
     }
     if (!grid_barrier(ctl, G)) return;

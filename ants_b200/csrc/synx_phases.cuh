@@ -449,29 +449,45 @@ __device__ __forceinline__ float smooth_z_column(const Smooth3Args& a, const Dim
   return mx;
 }
 
-// ---- convergence monitor and per-iteration log (one thread) ----------------------------------------
+// ---- convergence monitor and per-iteration log (one warp) ------------------------------------------
 // The last `window` energies, each divided by the running sum of |energy| of the level, are
 // fitted with a single-span linear B-spline on [0,1] by one level of multilevel B-spline
 // approximation; the convergence value is minus the fitted slope.
+// Called by all 32 lanes of one warp: lane j takes window entries j, j + 32, ... (the newest value
+// comes from ctl->metric, the older ones from the ring), the four sums are reduced across the
+// warp in a fixed order, and lane 0 updates the ring, the log and the stop flag.
 __device__ __forceinline__ void converge_step(IterCtl* ctl, const LogDev& log, double threshold, int window) {
+  const int lane = threadIdx.x & 31;
   const int k = ctl->iter;
   const double v = ctl->metric;
-  ctl->total_abs += fabs(v);
+  const double tabs = ctl->total_abs + fabs(v);
   const int W = window < 2 ? 2 : (window > kMaxWindow ? kMaxWindow : window);
-  ctl->energies[k % W] = v;
   const int k1 = k + 1;
-  double conv = DBL_MAX;
-  if (k1 >= W) {
-    double num0 = 0, den0 = 0, num1 = 0, den1 = 0;
-    for (int j = 0; j < W; ++j) {
+  const bool full = k1 >= W;
+  double num0 = 0, den0 = 0, num1 = 0, den1 = 0;
+  if (full) {
+    for (int j = lane; j < W; j += 32) {
+      const int slot = (k1 - W + j) % W;
+      const double e = slot == k % W ? v : ctl->energies[slot];
       const double u = (double)j / (double)(W - 1);
-      const double z = ctl->energies[(k1 - W + j) % W] / ctl->total_abs;
+      const double z = e / tabs;
       const double w0 = 1.0 - u, w1 = u, ws = w0 * w0 + w1 * w1;
       num0 += w0 * w0 * (w0 * z / ws);
       den0 += w0 * w0;
       num1 += w1 * w1 * (w1 * z / ws);
       den1 += w1 * w1;
     }
+    num0 = warp_sum_d(num0);
+    den0 = warp_sum_d(den0);
+    num1 = warp_sum_d(num1);
+    den1 = warp_sum_d(den1);
+  }
+  __syncwarp();
+  if (lane != 0) return;
+  ctl->total_abs = tabs;
+  ctl->energies[k % W] = v;
+  double conv = DBL_MAX;
+  if (full) {
     const double c0 = den0 > 0 ? num0 / den0 : 0.0, c1 = den1 > 0 ? num1 / den1 : 0.0;
     conv = -(c1 - c0);
   }
