@@ -12,11 +12,12 @@ A voxel-iteration is one voxel of a level grid processed by one full SyN iterati
               flushed (256 MB write) between steps.
   e2e      -- the same stage through the C ABI with pinned host buffers: host->device images and
               device->host forward and inverse fields inside the timed region.
-  roofline -- the persistent level kernel (k_level: one cooperative launch runs every iteration of
-              a pyramid level; the largest kernel of the step) on its largest launch, the 91x109x91
-              level, timed with CUDA events on the stage's stream inside the timed region.
-              Algorithmic bytes = voxels x (iterations x 176 B + inverse half-field sub-iterations
-              x 36 B), the compulsory traffic of each step (BYTES_PER_ITER_VOXEL below);
+  roofline -- the dominant unit of the step: one full-resolution SyN iteration, replayed as one CUDA
+              graph (warp, CC, xy and z smoothing, compose, and the two fixed-point inverses as
+              conditional loops: 56 % of the step), timed with CUDA events on the stage's stream
+              around the level inside the timed region and divided by its iterations.
+              Algorithmic bytes = voxels x (176 B + inverse half-field sub-iterations x 36 B) per
+              iteration, the compulsory traffic of each step (BYTES_PER_ITER_VOXEL below);
               `achieved_whole_step` applies the same model to all levels over the step time.
   --impl reference -- the CPU path (the oracle restatement of the reference arithmetic, all host
               threads) on a bounded sample of the same workload: one full-resolution iteration per step.
@@ -57,10 +58,10 @@ WORKLOAD = ("3-D SyN[0.1,3,0] + CC[r=4], 182x218x182 at 1 mm, shrink 8x4x2x1, si
 # (read psi, gather phi, write psi).
 BYTES_PER_ITER_VOXEL = 176
 BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi
-ROOF_LEVEL = 2  # the 91x109x91 level: the largest k_level launch
-# DRAM bytes (read + write) of that k_level launch, from the ncu capture summarised in
-# profiles/k_level_91x109x91.md (5.521 GB read + 7.273 GB written)
-LEVEL_TRAFFIC_BYTES = 12.794e9
+ROOF_LEVEL = 3  # the 182x218x182 level: one iteration graph per replay
+# DRAM bytes (read + write) of one replay of that iteration graph, from the ncu capture summarised
+# in profiles/iteration_graph_182x218x182.md
+ITER_GRAPH_TRAFFIC_BYTES = None
 
 
 def dist_env():
@@ -700,15 +701,17 @@ def main(argv=None) -> int:
         lv = prof_levels[ROOF_LEVEL]
         alg = lv["voxels"] * (lv["iterations"] * BYTES_PER_ITER_VOXEL + lv["inverse_subiterations"] * BYTES_PER_INV_VOXEL)
         achieved = alg / (lv["iterate_ms"] / 1000.0) / 1e9
+        n_iter = max(lv["iterations"], 1)
 
         def level_gbs(l):
             b = l["voxels"] * (l["iterations"] * BYTES_PER_ITER_VOXEL + l["inverse_subiterations"] * BYTES_PER_INV_VOXEL)
             return round(b / (l["iterate_ms"] / 1000.0) / 1e9, 1) if l["iterate_ms"] > 0 else None
 
-        roof = {"kernel": "k_level (persistent level kernel), 91x109x91 level", "bound": "hbm",
+        roof = {"kernel": "full-resolution SyN iteration graph (182x218x182: warp, CC, smoothing, compose, "
+                          "fixed-point inverse loops)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": LEVEL_TRAFFIC_BYTES,
-                "algorithmic_bytes_per_launch": alg / args.steps, "launch_ms": lv["iterate_ms"] / args.steps,
+                "traffic": ITER_GRAPH_TRAFFIC_BYTES,
+                "algorithmic_bytes_per_launch": alg / n_iter, "launch_ms": lv["iterate_ms"] / n_iter,
                 "bytes_per_voxel_iteration": BYTES_PER_ITER_VOXEL, "bytes_per_inverse_subiteration_voxel": BYTES_PER_INV_VOXEL,
                 "achieved_gbs_per_level": [level_gbs(l) for l in prof_levels],
                 "level_ms_per_step": [round(l["iterate_ms"] / args.steps, 3) for l in prof_levels],

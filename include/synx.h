@@ -80,7 +80,7 @@ typedef struct synx_params {
   double inv_mean_tol;
   double inv_max_tol;
   int32_t persistent_blocks;     /* grid of the persistent level kernel; 0: automatic */
-  int32_t persistent_max_voxels; /* largest level run by it; 0: automatic (2,500,000) */
+  int32_t persistent_max_voxels; /* largest level run by it; 0: automatic (400,000) */
   int32_t reserved[6];
 } synx_params;
 
