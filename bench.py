@@ -61,7 +61,7 @@ BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel:
 ROOF_LEVEL = 3  # the 182x218x182 level: one iteration graph per replay
 # DRAM bytes (read + write) of one replay of that iteration graph, from the ncu capture summarised
 # in profiles/iteration_graph_182x218x182.md
-ITER_GRAPH_TRAFFIC_BYTES = None
+ITER_GRAPH_TRAFFIC_BYTES = 3.824e9  # 2.401 GB read + 1.423 GB written
 
 
 def dist_env():
