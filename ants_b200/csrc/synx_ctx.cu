@@ -736,6 +736,11 @@ LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
   A.conv_threshold = c->P.convergence_threshold;
   A.conv_window = c->P.convergence_window;
   A.diag = affine_diag_host(A.warp.mF) && affine_diag_host(A.warp.mM) && affine_diag_host(A.comp.m);
+  // failure-detection test: every barrier waits for one block that was never launched, with a short
+  // poll limit, so the first wait runs out, sets the error flag and the kernel ends
+  const bool inject = c->P.test_inject == SYNX_INJECT_BARRIER_TIMEOUT;
+  A.bar_extra = inject ? 1 : 0;
+  A.bar_spins = inject ? (1ll << 14) : (1ll << 24);
   return A;
 }
 
@@ -1181,6 +1186,8 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     return set_err(nullptr, SYNX_E_ARG, "synx_create: inverse iteration cap must be in 1..1000");
   if (p.update_variance < 0 || p.total_variance < 0)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: negative smoothing variance");
+  if (p.test_inject != 0 && p.test_inject != SYNX_INJECT_BARRIER_TIMEOUT)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: unknown test_inject value");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();

@@ -33,6 +33,8 @@ struct LevelArgs {
   double conv_threshold;
   int conv_window;
   int diag;             // index maps without rotation
+  int bar_extra;        // blocks a barrier waits for beyond the group (0; 1 in the failure-detection test)
+  long long bar_spins;  // polls of a barrier wait before it gives up and sets IterCtl::bar_err
 };
 
 // Several pairs in one launch of the level kernel (same dimension and CC radius).

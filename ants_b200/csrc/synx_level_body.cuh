@@ -30,7 +30,8 @@ namespace synx {
 
 namespace {
 
-constexpr long long kBarrierSpinLimit = 1ll << 24;  // ~ a second of polling before giving up
+// The barrier's spin limit comes from LevelArgs::bar_spins (about 2^24 polls, a second or more,
+// unless a failure-detection test shortens it).
 
 __device__ __forceinline__ unsigned ld_volatile_u(const unsigned* p) { return *(volatile const unsigned*)p; }
 __device__ __forceinline__ int ld_volatile_i(const int* p) { return *(volatile const int*)p; }
@@ -43,7 +44,7 @@ struct Grp {
 
 // Barrier over the G blocks of a group (all co-resident: cooperative launch).  Returns false
 // once any block's wait has timed out.
-__device__ bool grid_barrier(IterCtl* ctl, int G) {
+__device__ bool grid_barrier(IterCtl* ctl, int G, long long spin_limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -57,7 +58,7 @@ __device__ bool grid_barrier(IterCtl* ctl, int G) {
     } else {
       long long spins = 0;
       while (ld_volatile_u(&ctl->bar_gen) == gen) {
-        if (ld_volatile_i(&ctl->bar_err) || ++spins > kBarrierSpinLimit) {
+        if (ld_volatile_i(&ctl->bar_err) || ++spins > spin_limit) {
           atomicExch(&ctl->bar_err, 1);
           break;
         }
@@ -164,7 +165,7 @@ __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, c
       A.inv_pmax[h * A.pcap + (u - h * nh)] = mx;
     }
   }
-  if (!grid_barrier(ctl, gp.G)) return false;
+  if (!grid_barrier(ctl, gp.G + A.bar_extra, A.bar_spins)) return false;
   double sum[2];
   float mxv[2];
   reduce_partials(A, nh, sum, mxv, redd, redf);
@@ -196,7 +197,7 @@ __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, c
         }
       }
     }
-    if (!grid_barrier(ctl, gp.G)) return false;
+    if (!grid_barrier(ctl, gp.G + A.bar_extra, A.bar_spins)) return false;
     if (st[0] || st[1]) reduce_partials(A, nh, sum, mxv, redd, redf);
     exec[0] = st[0];
     exec[1] = st[1];
@@ -225,14 +226,14 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
       UW.at(u, bx, by, bz, h);
       warp_pair_tile<DIM, DIAG>(A.warp, bx, by, bz);
     }
-    if (!grid_barrier(ctl, G)) return;
+    if (!grid_barrier(ctl, G + A.bar_extra, A.bar_spins)) return;
     // 2. CC tiles (same tiles and partial slots as the standalone kernel)
     for (int t = b; t < ncc; t += G) {
       const int bx = t % A.cc_gx, by = (t / A.cc_gx) % A.cc_gy, bz = t / (A.cc_gx * A.cc_gy);
       const double s = cc_tile<RCC, DIM>(A.warp.Ft, A.warp.Mt, A.g, A.cc, A.gF, A.gM, nullptr, bx, by, bz, smem, redd);
       if (tid == 0) A.cc_partials[t] = s;
     }
-    if (!grid_barrier(ctl, G)) return;
+    if (!grid_barrier(ctl, G + A.bar_extra, A.bar_spins)) return;
     // 3. update smoothing (xy, then z in 3-D) with the max ||u/h|| per half
     float mxs[2] = {0.0f, 0.0f};
     for (int u = b; u < UXY.count(); u += G) {
@@ -242,7 +243,7 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
       if (DIM == 2) mxs[h] = fmaxf(mxs[h], m);
     }
     if (DIM == 3) {
-      if (!grid_barrier(ctl, G)) return;
+      if (!grid_barrier(ctl, G + A.bar_extra, A.bar_spins)) return;
       for (int u = b; u < UZ.count(); u += G) {
         int bx, by, zc, h;
         UZ.at(u, bx, by, zc, h);
@@ -253,14 +254,14 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
       const float bm = block_max_f(mxs[h], redf);
       if (tid == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
     }
-    if (!grid_barrier(ctl, G)) return;
+    if (!grid_barrier(ctl, G + A.bar_extra, A.bar_spins)) return;
     // 4. scale + compose into the forward half-fields, in place
     for (int u = b; u < UC.count(); u += G) {
       int bx, by, bz, h;
       UC.at(u, bx, by, bz, h);
       compose_tile<DIM, DIAG>(A.comp, ctl, h, bx, by, bz);
     }
-    if (!grid_barrier(ctl, G)) return;
+    if (!grid_barrier(ctl, G + A.bar_extra, A.bar_spins)) return;
     // 5, 6. psi <- inv(phi) warm from psi, then phi <- inv(psi) warm from phi
     if (!inverse_phase<DIM, DIAG>(A, A.invA, 0, gp, redd, redf)) return;
     if (!inverse_phase<DIM, DIAG>(A, A.invB, 1, gp, redd, redf)) return;
@@ -279,7 +280,7 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
         converge_step(ctl, A.log, A.conv_threshold, A.conv_window);
       }
     }
-    if (!grid_barrier(ctl, G)) return;
+    if (!grid_barrier(ctl, G + A.bar_extra, A.bar_spins)) return;
   }
 }
 

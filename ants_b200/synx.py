@@ -25,6 +25,7 @@ SYNX_F_USE_GRAPHS = 0x2
 SYNX_F_NO_PERSISTENT = 0x4
 SYNX_F_CC_FP32_SUMS = 0x8
 SYNX_F_FIELDS_FP16 = 0x10
+SYNX_INJECT_BARRIER_TIMEOUT = 1
 
 ERRORS = {-1: "invalid argument", -2: "bad state", -3: "CUDA error", -4: "out of device memory", -5: "unsupported"}
 
@@ -63,7 +64,8 @@ class SynxParams(C.Structure):
         ("inv_max_tol", C.c_double),
         ("persistent_blocks", C.c_int32),
         ("persistent_max_voxels", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("test_inject", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -250,6 +252,7 @@ class SyNParams:
     flags: int = 0
     persistent_blocks: int = 0  # launch shape of the persistent level kernel (0: automatic)
     persistent_max_voxels: int = 0  # largest level it runs (0: automatic)
+    test_inject: int = 0  # SYNX_INJECT_* (failure-detection tests)
 
     def to_c(self) -> SynxParams:
         n = len(self.iterations)
@@ -280,6 +283,7 @@ class SyNParams:
         p.flags = self.flags
         p.persistent_blocks = self.persistent_blocks
         p.persistent_max_voxels = self.persistent_max_voxels
+        p.test_inject = self.test_inject
         return p
 
 

@@ -81,7 +81,8 @@ typedef struct synx_params {
   double inv_max_tol;
   int32_t persistent_blocks;     /* grid of the persistent level kernel; 0: automatic */
   int32_t persistent_max_voxels; /* largest level run by it; 0: automatic (400,000) */
-  int32_t reserved[6];
+  int32_t test_inject;           /* 0; SYNX_INJECT_* makes a failure happen for tests */
+  int32_t reserved[5];
 } synx_params;
 
 #define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
@@ -90,6 +91,12 @@ typedef struct synx_params {
 /* Precision-study variants (not antsRegistration behaviour; both run the per-kernel path): */
 #define SYNX_F_CC_FP32_SUMS 0x8  /* CC window sums and variance terms in float instead of double */
 #define SYNX_F_FIELDS_FP16 0x10  /* half-fields rounded to half precision wherever they are stored */
+
+/* Failure injection for tests (host-side; nothing faults): the level kernel's grid barrier waits for
+ * one block more than it launched, with a short poll limit, so the wait runs out, the kernel ends
+ * and synx_run / synx_run_level return SYNX_E_CUDA with a barrier-timeout message.  The context
+ * and the GPU stay usable. */
+#define SYNX_INJECT_BARRIER_TIMEOUT 1
 
 /* Fill *p with antsRegistration's defaults for a SyN stage of dimension dim
  * (SyN[0.1,3,0], CC radius 4, one level, 1 iteration, shrink 1, sigma 0 vox). */
