@@ -60,7 +60,7 @@ static int cc_zchunk(const GridInfo& g, int radius) {
   if (g.d.dim == 2) return 1;
   const int bxy = ((g.d.nx + 31) / 32) * ((g.d.ny + 7) / 8);
   const int nz = g.d.nz, slots = 2 * 148;
-  const int max_chunks = std::max(1, nz / std::max(2 * radius, 1));
+  const int max_chunks = std::max(1, nz / std::max(radius, 1));  // chunks of at least R slices
   int best_zc = nz;
   double best = 1e30;
   for (int c = 1; c <= max_chunks; ++c) {
