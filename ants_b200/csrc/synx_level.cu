@@ -82,12 +82,23 @@ cudaError_t launch_level_batch(const BatchLevelArgs& B, int dim, int cc_radius, 
 }
 
 int level_zb(const Dims& d, int halves) {
-  // about two tiles per block of a full cooperative grid (296 blocks on 148 SMs); a constant, so
-  // the decomposition is the same whatever grid or group runs the level
-  const int target_units = 2 * 296;
-  const int gx = (d.nx + 31) / 32, gy = (d.ny + 7) / 8;
-  const int per = std::max(1, target_units / (gx * gy * halves));
-  return std::max(1, (d.nz + per - 1) / per);
+  // z depth of the 32 x 8 tiles of a per-voxel phase: minimises the rounds of tiles over a full
+  // cooperative grid (296 blocks on 148 SMs) times the work of one tile (its slices plus about
+  // half a slice of set-up).  A constant grid size, so the decomposition is the same whatever grid
+  // or group runs the level.
+  const int G = 296;
+  const int gxy = ((d.nx + 31) / 32) * ((d.ny + 7) / 8) * halves;
+  int best_zb = d.nz;
+  double best = -1.0;
+  for (int zb = 1; zb <= d.nz; ++zb) {
+    const long long units = (long long)gxy * ((d.nz + zb - 1) / zb);
+    const double cost = (double)((units + G - 1) / G) * (zb + 0.5);
+    if (best < 0 || cost < best) {
+      best = cost;
+      best_zb = zb;
+    }
+  }
+  return best_zb;
 }
 
 }  // namespace synx
