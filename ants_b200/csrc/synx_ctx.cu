@@ -698,7 +698,7 @@ LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
   A.sz = A.sxy;
   A.sz.in = Ptr2c{{c->t2F, c->t2M}};
   A.sz.out = Ptr2{{c->t1F, c->t1M}};
-  A.sz.ZC = smooth_z_chunk(g.d, 2, RR);
+  A.sz.ZC = smooth_z_chunk(g.d, 2, RR, 296);
   A.sz_gz = (g.d.nz + A.sz.ZC - 1) / A.sz.ZC;
   A.r_smooth = RR;
   A.comp.d = Ptr2c{{c->t1F, c->t1M}};

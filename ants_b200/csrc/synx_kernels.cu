@@ -256,15 +256,16 @@ __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, 
 }
 
 template <int R>
-// up to R = 6: at least 3 blocks per SM (a few ring registers spill at R = 5, 6; the extra warps
-// hide more load latency than the spills cost); wider rings keep every register they need
-__global__ void __launch_bounds__(256, (R <= 6 ? 3 : 1)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
+// the ring lives in shared memory ((2R+1) x 3 x 256 floats, smooth_z_smem_bytes), so few registers
+// are needed: 5 resident blocks per SM up to R = 6 (40 KB of ring each), 3 up to R = 12
+__global__ void __launch_bounds__(256, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
   if (ctl != nullptr && ctl->stop) return;
+  extern __shared__ float zring[];
   __shared__ float red[32];
   const int nzc = gridDim.z / a.halves;
   const int h = blockIdx.z / nzc;
   const int zc = blockIdx.z - h * nzc;
-  const float mx = smooth_z_column<R>(a, d, blockIdx.x, blockIdx.y, zc, h);
+  const float mx = smooth_z_column_smem<R>(a, d, blockIdx.x, blockIdx.y, zc, h, zring);
   if (a.do_max) {
     const float bm = block_max_f(mx, red);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
@@ -279,6 +280,8 @@ static int smooth3_radius(int dim, const int R[3]) {
 
 bool smooth3_supported(int dim, const int R[3]) { return smooth3_radius(dim, R) <= kSmoothRMax; }
 
+static size_t smooth_z_smem_bytes(int R) { return (size_t)(2 * R + 1) * 3 * 256 * sizeof(float); }
+
 template <int R>
 static cudaError_t smooth3_attr_both() {
   cudaError_t e = cudaFuncSetAttribute(k_smooth_xy<3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -286,6 +289,8 @@ static cudaError_t smooth3_attr_both() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_smooth_xy<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(smooth3_smem_floats(2, R, kSmoothTileY) * 4));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_smooth_z<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_z_smem_bytes(R));
   return e;
 }
 
@@ -333,12 +338,22 @@ Smooth3Args make_smooth_args(const float* const* in, float* const* out, const fl
   return a;
 }
 
-int smooth_z_chunk(const Dims& d, int halves, int RR) {
-  const int gx = (d.nx + 31) / 32, gy = (d.ny + 7) / 8;
-  const int target = 148 * 8;
-  const int chunks = std::max(1, (target + gx * gy * halves - 1) / (gx * gy * halves));
-  int zc = (d.nz + chunks - 1) / chunks;
-  return std::min(std::max(zc, 2 * RR + 1), d.nz);
+int smooth_z_chunk(const Dims& d, int halves, int RR, int slots) {
+  // z chunk of one column walk of the level kernel's z phase: minimises the waves of walks over
+  // `slots` blocks times the work of a walk (its slices plus the ring fill, 2R loads, about R
+  // slices)
+  const int cols = ((d.nx + 31) / 32) * ((d.ny + 7) / 8) * halves;
+  int best_zc = d.nz;
+  double best = -1.0;
+  for (int zc = 1; zc <= d.nz; ++zc) {
+    const long long blocks = (long long)cols * ((d.nz + zc - 1) / zc);
+    const double cost = (double)((blocks + slots - 1) / slots) * (zc + RR);
+    if (best < 0 || cost < best) {
+      best = cost;
+      best_zc = zc;
+    }
+  }
+  return best_zc;
 }
 
 void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
@@ -380,12 +395,17 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   // z pass: tmp -> out with the epilogue
   a.in = Ptr2c{{tmp[0], halves > 1 ? tmp[1] : tmp[0]}};
   a.out = Ptr2{{out[0], halves > 1 ? out[1] : out[0]}};
-  a.ZC = smooth_z_chunk(g.d, halves, RR);
+  {
+    // about 8 column walks per SM of at least 2R + 1 slices (longer walks measured slower here)
+    const int cols = gx * gy * halves;
+    const int chunks = std::max(1, (148 * 8 + cols - 1) / cols);
+    a.ZC = std::min(std::max((g.d.nz + chunks - 1) / chunks, 2 * RR + 1), g.d.nz);
+  }
   const dim3 gz(gx, gy, ((g.d.nz + a.ZC - 1) / a.ZC) * halves);
   count_launch();
 #define SYNX_SZ(RV)                                    \
   case RV:                                             \
-    k_smooth_z<RV><<<gz, 256, 0, s>>>(a, g.d, ctl);    \
+    k_smooth_z<RV><<<gz, 256, smooth_z_smem_bytes(RV), s>>>(a, g.d, ctl);    \
     break;
   switch (RR) {
     SYNX_SZ(1)

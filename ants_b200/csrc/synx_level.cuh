@@ -65,7 +65,7 @@ CCParams make_cc_params(const GridInfo& g, int radius);
 Smooth3Args make_smooth_args(const float* const* in, float* const* out, const float* const* orig, int halves,
                              const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
                              float w2, bool maxnorm, int* radius);
-int smooth_z_chunk(const Dims& d, int halves, int RR);
+int smooth_z_chunk(const Dims& d, int halves, int RR, int slots);
 InvArgs make_inv_args(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int zb,
                       float* const* ecache = nullptr);
 

@@ -449,6 +449,63 @@ __device__ __forceinline__ float smooth_z_column(const Smooth3Args& a, const Dim
   return mx;
 }
 
+// The same z part with the ring in shared memory (`ring` holds (2R+1) x 3 x blockDim floats, slot-
+// major, thread-minor: each thread touches only its own column, so no barrier is needed and the
+// accesses are conflict-free).  Far fewer registers than the register ring, so more blocks fit on
+// an SM; the arithmetic and its order are the same, so the results have the same bits.
+template <int R>
+__device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, const Dims& d, int bx, int by, int zc,
+                                                      int h, float* ring) {
+  constexpr int K = 2 * R + 1, RD = K;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
+  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
+  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+  const int ox = bx * 32 + (threadIdx.x & 31), oy = by * 8 + (threadIdx.x >> 5);
+  const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
+  float mx = 0.0f;
+  if (ox >= nx || oy >= ny) return mx;
+  const int T = blockDim.x, t = threadIdx.x;
+  auto slot = [&](int s, int c) -> float& { return ring[(s * 3 + c) * T + t]; };
+  const float* col = src + oy * nx + ox;
+#pragma unroll
+  for (int u = 0; u < 2 * R; ++u) {
+    const int zs = min(max(z0 - R + u, 0), nz - 1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) slot(u, c) = __ldg(col + c * N + zs * nxy);
+  }
+  const bool xyedge = ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1;
+  for (int zb = z0; zb < z1; zb += RD) {
+#pragma unroll
+    for (int u = 0; u < RD; ++u) {
+      const int z = zb + u;
+      if (z < z1) {
+        const int zs = min(z + R, nz - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) slot((u + 2 * R) % RD, c) = __ldg(col + c * N + zs * nxy);
+        const int i = z * nxy + oy * nx + ox;
+        const bool edge = a.epilogue && (xyedge || z == 0 || z == nz - 1);
+        float nrm2 = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float acc = 0.0f;
+#pragma unroll
+          for (int j = 0; j < K; ++j) acc = fmaf(a.k[2][j], slot((u + j) % RD, c), acc);
+          if (a.epilogue) {
+            if (edge) acc = 0.0f;
+            else if (a.w2 != 0.0f) acc = acc * a.w1 + org[c * N + i] * a.w2;
+          }
+          const float q = acc * a.ih[c];
+          nrm2 += q * q;
+          dst[c * N + i] = acc;
+        }
+        mx = fmaxf(mx, sqrtf(nrm2));
+      }
+    }
+  }
+  return mx;
+}
+
 // ---- convergence monitor and per-iteration log (one warp) ------------------------------------------
 // The last `window` energies, each divided by the running sum of |energy| of the level, are
 // fitted with a single-span linear B-spline on [0,1] by one level of multilevel B-spline
