@@ -180,7 +180,8 @@ typedef struct synx_server_stats {
   double elapsed;
 } synx_server_stats;
 int synx_server_create(const synx_server_config* cfg, synx_server** out);
-/* Stops the loop after the resident requests finish; queued requests fail with SYNX_E_STATE. */
+/* Stops the loop after the resident requests finish; queued requests fail with SYNX_E_STATE.  No
+ * other call on this server (submit, wait, stats) may run concurrently with it or follow it. */
 int synx_server_destroy(synx_server* server);
 const char* synx_server_last_error(const synx_server* server);
 int synx_server_submit(synx_server* server, const synx_params* params, const float* fixed_host,
