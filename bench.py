@@ -61,7 +61,7 @@ BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel:
 ROOF_LEVEL = 3  # the 182x218x182 level: one iteration graph per replay
 # DRAM bytes (read + write) of one replay of that iteration graph, from the ncu capture summarised
 # in profiles/iteration_graph_182x218x182.md
-ITER_GRAPH_TRAFFIC_BYTES = 3.824e9  # 2.401 GB read + 1.423 GB written
+ITER_GRAPH_TRAFFIC_BYTES = 3.820e9  # 2.419 GB read + 1.401 GB written (mean of two replays)
 
 
 def dist_env():
@@ -69,18 +69,65 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region.
+
+    NVML is read every 20 ms from a host thread (read-only queries: current and maximum SM clock,
+    active clock-event reasons), on the device matched by UUID, then PCI bus id.  Without NVML the
+    sampler falls back to an `nvidia-smi -lms 200` process."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.02
+    # NVML clock-event reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.out = None
+        self.nvml = None
+        self.handle = None
+        self.thread = None
+        self.stop = None
+        self.rows = []  # (sm MHz, max sm MHz, reason bits)
+
+    def _nvml_handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        self.nvml = N
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            try:
+                return N.nvmlDeviceGetHandleByUUID("GPU-" + str(p.uuid))
+            except Exception:
+                bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+                return N.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return N.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        N, h = self.nvml, self.handle
+        while not self.stop.is_set():
+            try:
+                self.rows.append((float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)),
+                                  float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)),
+                                  int(N.nvmlDeviceGetCurrentClocksEventReasons(h))))
+            except Exception:
+                pass
+            self.stop.wait(self.PERIOD_S)
 
     def __enter__(self):
+        try:
+            import threading
+            self.handle = self._nvml_handle()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._sample, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.handle = None
         try:
             self.out = open(os.path.join("/tmp", f"synx_clocks_{os.getpid()}.csv"), "w+")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -91,6 +138,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -99,6 +149,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
+        if self.thread is not None:
+            sm = [r[0] for r in self.rows]
+            reasons = sorted(n for n, bit in self.REASON_BITS.items() if any(r[2] & bit for r in self.rows))
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(r[1] for r in self.rows) if self.rows else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 20 ms"}
         if self.out is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.out.seek(0)
@@ -115,7 +171,7 @@ class ClockSampler:
             except (ValueError, IndexError):
                 continue
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peak_hbm():
@@ -136,9 +192,11 @@ def voxel_iterations(log, sizes) -> int:
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_sample(fixed, moving, g, threads: int):
-    """One full-resolution SyN iteration of the CPU path (oracle restatement, `threads` host
-    threads) from zero fields on the preprocessed, unsmoothed images (sigma = 0 at level 4)."""
+def cpu_sample(fixed, moving, g, threads: int, min_seconds: float = 0.0, max_iterations: int = 1):
+    """Full-resolution SyN iterations of the CPU path (oracle restatement, `threads` host threads)
+    from zero fields on the preprocessed, unsmoothed images (sigma = 0 at level 4): at least one,
+    repeated until `min_seconds` have passed or `max_iterations` have run.  Returns
+    (voxel-iterations per second, seconds, iterations)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from ants_b200.synx import SyNParams
@@ -146,10 +204,14 @@ def cpu_sample(fixed, moving, g, threads: int):
     P = SyNParams(dim=3, **STAGE)
     Fp, Mp = O.preprocess(fixed), O.preprocess(moving)
     z = np.zeros((3,) + g.shape, np.float32)
-    t0 = time.perf_counter()
-    O.syn_iteration(Fp, g, Mp, g, P, g, z, z, z, z)
-    dt = time.perf_counter() - t0
-    return g.count / dt, dt
+    n, t0 = 0, time.perf_counter()
+    while True:
+        O.syn_iteration(Fp, g, Mp, g, P, g, z, z, z, z)
+        n += 1
+        dt = time.perf_counter() - t0
+        if dt >= min_seconds or n >= max_iterations:
+            break
+    return g.count * n / dt, dt, n
 
 
 def run_reference(args, fixed, moving, g):
@@ -158,7 +220,7 @@ def run_reference(args, fixed, moving, g):
         cpu_sample(fixed, moving, g, threads)
     times = []
     for _ in range(args.steps):
-        _, dt = cpu_sample(fixed, moving, g, threads)
+        _, dt, _ = cpu_sample(fixed, moving, g, threads)
         times.append(dt)
     total = sum(times)
     value = g.count * args.steps / total
@@ -722,9 +784,10 @@ def main(argv=None) -> int:
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
             threads = os.cpu_count() or 1
-            v_cpu, dt = cpu_sample(fixed, moving, g, threads)
+            v_cpu, dt, n_cpu = cpu_sample(fixed, moving, g, threads, min_seconds=10.0, max_iterations=20)
             cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"one full-resolution SyN-CC iteration from zero fields ({dt:.1f} s)"}
+                   "sample": f"{n_cpu} full-resolution (182x218x182) SyN-CC iterations from zero fields "
+                             f"({dt:.1f} s of CPU work)"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_total / args.steps, "higher_is_better": True,
