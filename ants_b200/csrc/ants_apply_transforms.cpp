@@ -4,10 +4,14 @@
 // fields antsRegistration wrote (prefix0Warp.nii.gz / prefix0InverseWarp.nii.gz).  Options follow
 // Examples/antsApplyTransforms.cxx:1063-1240:
 //   -d/--dimensionality 2|3      -i/--input image     -r/--reference-image image
-//   -t/--transform field  (repeatable).  As in the reference's transform stack (:1183-1196), a
+//   -t/--transform file  (repeatable).  As in the reference's transform stack (:1183-1196), a
 //       reference point is moved first by the LAST transform given, then by the one before it.
-//       [field,0] is accepted; [field,1] is rejected (a displacement field has no closed-form
-//       inverse: pass the InverseWarp field instead).  Affine (.mat) files are not supported.
+//       A displacement field image: [field,0] is accepted; [field,1] is rejected (a displacement
+//       field has no closed-form inverse: pass the InverseWarp field instead).
+//       A linear transform file (.mat / .txt, e.g. prefix0GenericAffine.mat; the types
+//       synx_read_linear_transform reads): [file,1] applies its inverse.  A file holding several
+//       transforms enters the stack in file order (reversed and each inverted for [file,1]).
+//       HDF5 composite files (.h5) are not supported.
 //   -n/--interpolation Linear (the default; other interpolators are rejected)
 //   -f/--default-value v (0): value where the point maps outside the input image
 //   -o/--output warped | [collapsed,1] | DisplacementField[collapsed]  (the collapsed form writes
@@ -15,12 +19,17 @@
 //   --float 0|1 (computation is float32 either way)   -v/--verbose 0|1   --gpu N (not a reference option)
 //
 // GPU path: every field is brought onto the reference grid (synx_resample_field when its grid
-// differs), the stack is composed in place, w <- w + u_i(x + w) from the last transform to the
-// first (synx_compose), and the input is sampled once at x + w (synx_warp_image).
+// differs; a linear transform is written there as its displacement T(p) - p by
+// synx_linear_field), the stack is composed in place, w <- w + u_i(x + w) from the last transform
+// to the first (synx_compose), and the input is sampled once at x + w (synx_warp_image).  A
+// displacement on the reference grid is zero outside it, so a transform that is not applied first
+// acts as the identity where the transforms before it move a point off the reference grid (a
+// linear transform applied first, the usual `-t warp -t affine` order, is exact everywhere).
 #include "ants_apply_transforms.h"
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
@@ -60,6 +69,18 @@ void step_ok(int rc, const char* what) {
   if (rc != 0) throw std::runtime_error(std::string(what) + ": " + synx_last_error(nullptr));
 }
 
+bool ends_with(const std::string& s, const std::string& suffix) {
+  return s.size() >= suffix.size() && s.compare(s.size() - suffix.size(), suffix.size(), suffix) == 0;
+}
+
+// One transform of the stack: a displacement field image, or a linear transform of a .mat/.txt file.
+struct StackEntry {
+  std::string file;
+  bool is_linear = false;
+  bool invert = false;
+  synx_linear linear{};
+};
+
 int run(const std::vector<std::string>& args, std::ostream& out) {
   std::map<std::string, std::vector<std::string>> opt;
   const std::map<std::string, std::string> alias = {
@@ -73,7 +94,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     else if (alias.count(k)) name = alias.at(k);
     else throw std::runtime_error("unexpected argument '" + k + "'");
     if (name == "help") {
-      out << "antsApplyTransforms_b200: antsApplyTransforms for displacement fields on a B200\n";
+      out << "antsApplyTransforms_b200: antsApplyTransforms for displacement-field and linear transform stacks on a B200\n";
       return EXIT_SUCCESS;
     }
     if (i + 1 >= args.size()) throw std::runtime_error("option --" + name + " needs a value");
@@ -115,24 +136,44 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   }
   if (!collapse && !opt.count("input")) throw std::runtime_error("an input image (-i) is required");
 
-  // transforms: file names in command-line order
-  std::vector<std::string> fields;
+  // transforms in command-line order
+  std::vector<StackEntry> stack;
   for (const std::string& v : opt["transform"]) {
     OptionCall t = parse_call(v);
     std::string file = t.name;
+    bool invert = false;
     if (file.empty()) {
       if (t.params.empty()) throw std::runtime_error("empty transform '" + v + "'");
       file = t.params[0];
-      if (t.params.size() > 1 && (t.params[1] == "1" || lower(t.params[1]) == "true"))
-        throw std::runtime_error("the inverse of displacement field '" + file +
-                                 "' is not available: use the inverse warp file antsRegistration wrote");
+      invert = t.params.size() > 1 && (t.params[1] == "1" || lower(t.params[1]) == "true");
     }
     if (lower(file) == "identity") continue;
     const std::string lf = lower(file);
-    if (lf.size() >= 4 && (lf.compare(lf.size() - 4, 4, ".mat") == 0 || lf.compare(lf.size() - 4, 4, ".txt") == 0 ||
-                           (lf.size() >= 3 && lf.compare(lf.size() - 3, 3, ".h5") == 0)))
-      throw std::runtime_error("transform '" + file + "' is not a displacement field image (only fields are supported)");
-    fields.push_back(file);
+    if (ends_with(lf, ".h5") || ends_with(lf, ".hdf5") || ends_with(lf, ".xfm"))
+      throw std::runtime_error("transform '" + file + "': HDF5/composite transform files are not supported");
+    if (ends_with(lf, ".mat") || ends_with(lf, ".txt")) {
+      const int n = synx_read_linear_transform(file.c_str(), dim, 0, nullptr);
+      if (n < 0) throw std::runtime_error(synx_last_error(nullptr));
+      std::vector<StackEntry> part;
+      for (int i = 0; i < n; ++i) {
+        StackEntry e;
+        e.file = file;
+        e.is_linear = true;
+        e.invert = invert;
+        step_ok(synx_read_linear_transform(file.c_str(), dim, i, &e.linear) < 0 ? -1 : 0,
+                "synx_read_linear_transform");
+        part.push_back(e);
+      }
+      if (invert) std::reverse(part.begin(), part.end());
+      stack.insert(stack.end(), part.begin(), part.end());
+      continue;
+    }
+    if (invert)
+      throw std::runtime_error("the inverse of displacement field '" + file +
+                               "' is not available: use the inverse warp file antsRegistration wrote");
+    StackEntry e;
+    e.file = file;
+    stack.push_back(e);
   }
 
   const nifti::Image ref = nifti::read(one("reference-image", ""));
@@ -143,26 +184,36 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   // compose the stack on the reference grid: w = u_n, then w <- w + u_i(x + w), i = n-1 .. 1
   DeviceBuffer w((size_t)N * dim), tmp((size_t)N * dim);
   CLI_CK(cudaMemset(w.p, 0, 4 * (size_t)N * dim));
-  for (int k = (int)fields.size() - 1; k >= 0; --k) {
-    const nifti::Image f = nifti::read(fields[k]);
-    if (f.components != dim || f.dim != dim)
-      throw std::runtime_error("'" + fields[k] + "' is not a " + std::to_string(dim) + "-D displacement field");
-    const synx_geom gf = to_geom(f, dim);
-    const long long Nf = f.voxels();
-    // this field on the reference grid, in tmp
-    if (same_grid(gf, gr)) {
-      CLI_CK(cudaMemcpy(tmp.p, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+  for (int k = (int)stack.size() - 1; k >= 0; --k) {
+    const StackEntry& e = stack[k];
+    std::string note;
+    // this transform's displacement on the reference grid, in tmp
+    if (e.is_linear) {
+      std::vector<float> u((size_t)N * dim);
+      step_ok(synx_linear_field(&e.linear, e.invert ? 1 : 0, &gr, u.data()), "synx_linear_field");
+      CLI_CK(cudaMemcpy(tmp.p, u.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+      note = e.invert ? " (linear, inverse)" : " (linear)";
     } else {
-      DeviceBuffer src((size_t)Nf * dim);
-      CLI_CK(cudaMemcpy(src.p, f.data.data(), 4 * (size_t)Nf * dim, cudaMemcpyHostToDevice));
-      step_ok(synx_resample_field(src.p, &gf, tmp.p, &gr, nullptr), "synx_resample_field");
+      const nifti::Image f = nifti::read(e.file);
+      if (f.components != dim || f.dim != dim)
+        throw std::runtime_error("'" + e.file + "' is not a " + std::to_string(dim) + "-D displacement field");
+      const synx_geom gf = to_geom(f, dim);
+      const long long Nf = f.voxels();
+      if (same_grid(gf, gr)) {
+        CLI_CK(cudaMemcpy(tmp.p, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+      } else {
+        DeviceBuffer src((size_t)Nf * dim);
+        CLI_CK(cudaMemcpy(src.p, f.data.data(), 4 * (size_t)Nf * dim, cudaMemcpyHostToDevice));
+        step_ok(synx_resample_field(src.p, &gf, tmp.p, &gr, nullptr), "synx_resample_field");
+        note = " (resampled)";
+      }
     }
-    if (k == (int)fields.size() - 1) {
+    if (k == (int)stack.size() - 1) {
       std::swap(w.p, tmp.p);
     } else {
       step_ok(synx_compose(tmp.p, w.p, &gr, 1.0f, w.p, nullptr), "synx_compose");
     }
-    if (verbose) out << "  transform " << k << ": " << fields[k] << (same_grid(gf, gr) ? "" : " (resampled)") << "\n";
+    if (verbose) out << "  transform " << k << ": " << e.file << note << "\n";
   }
 
   if (collapse) {
@@ -200,7 +251,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   if (defval != 0.0f)
     for (float& x : res.data) x += defval;
   nifti::write(out_path, res);
-  if (verbose) out << "wrote " << out_path << " (" << fields.size() << " displacement fields)\n";
+  if (verbose) out << "wrote " << out_path << " (" << stack.size() << " transforms)\n";
   return EXIT_SUCCESS;
 }
 

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/synx.h"
+#include "synx_host.h"
 #include "synx_kernels.cuh"
 #include "synx_level.cuh"
 
@@ -1131,6 +1132,11 @@ int batch_step(synx_batch* b, synx_ctx* const* cs, int n, cudaStream_t s, int* a
 }
 
 }  // namespace
+
+int synx::set_global_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
 
 extern "C" {
 

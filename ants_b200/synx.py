@@ -41,6 +41,17 @@ class SynxGeom(C.Structure):
     ]
 
 
+class SynxLinear(C.Structure):
+    """synx_linear: T(p) = A (p - c) + t + c on physical (LPS) points."""
+    _fields_ = [
+        ("dim", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("matrix", C.c_double * 9),
+        ("translation", C.c_double * 3),
+        ("center", C.c_double * 3),
+    ]
+
+
 class SynxParams(C.Structure):
     _fields_ = [
         ("dim", C.c_int32),
@@ -199,6 +210,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_server_submit": (I, [V, P(SynxParams), V, P(SynxGeom), V, P(SynxGeom), V, V, P(C.c_int64)]),
         "synx_server_wait": (I, [V, C.c_int64, D, P(SynxRequestInfo)]),
         "synx_server_get_stats": (I, [V, P(SynxServerStats)]),
+        "synx_read_linear_transform": (I, [C.c_char_p, I, I, P(SynxLinear)]),
+        "synx_linear_field": (I, [P(SynxLinear), I, P(SynxGeom), V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -647,3 +660,55 @@ def invert_field(phi, psi, g: Geom, max_iter=20, mean_tol=0.001, max_tol=0.1, st
 def resample_field(u, gi: Geom, out, go: Geom, stream=None) -> None:
     a, b = gi.to_c(), go.to_c()
     _check(load_library().synx_resample_field(_ptr(u), C.byref(a), _ptr(out), C.byref(b), _stream(stream)))
+
+
+@dataclass
+class LinearTransform:
+    """A linear transform of an ITK transform file: T(p) = matrix (p - center) + translation + center."""
+
+    matrix: np.ndarray  # (dim, dim)
+    translation: np.ndarray  # (dim,)
+    center: np.ndarray  # (dim,)
+
+    @property
+    def dim(self) -> int:
+        return self.matrix.shape[0]
+
+    def to_c(self) -> SynxLinear:
+        t = SynxLinear()
+        d = self.dim
+        t.dim = d
+        m = np.eye(3)
+        m[:d, :d] = self.matrix
+        for k in range(9):
+            t.matrix[k] = float(m.flat[k])
+        for k in range(d):
+            t.translation[k] = float(self.translation[k])
+            t.center[k] = float(self.center[k])
+        return t
+
+
+def count_linear_transforms(path, dim: int) -> int:
+    """Number of linear transforms in an ITK transform file (.mat or .txt)."""
+    rc = load_library().synx_read_linear_transform(os.fsencode(str(path)), dim, 0, None)
+    if rc < 0:
+        _check(rc)
+    return rc
+
+
+def read_linear_transform(path, dim: int, index: int = 0) -> LinearTransform:
+    """Transform `index` of an ITK transform file (.mat MATLAB v4 or .txt Insight text)."""
+    t = SynxLinear()
+    rc = load_library().synx_read_linear_transform(os.fsencode(str(path)), dim, index, C.byref(t))
+    if rc < 0:
+        _check(rc)
+    m = np.array(list(t.matrix), dtype=np.float64).reshape(3, 3)[:dim, :dim]
+    return LinearTransform(m, np.array(list(t.translation)[:dim]), np.array(list(t.center)[:dim]))
+
+
+def linear_field(t: LinearTransform, g: Geom, invert: bool = False) -> np.ndarray:
+    """Displacement T(p) - p (or T^-1(p) - p) at every voxel of `g`, interleaved: shape g.shape + (dim,)."""
+    out = np.empty(g.shape + (g.dim,), dtype=np.float32)
+    tc, gc = t.to_c(), g.to_c()
+    _check(load_library().synx_linear_field(C.byref(tc), int(bool(invert)), C.byref(gc), _ptr(out)))
+    return out

@@ -301,6 +301,37 @@ int synx_resample_field(const float* in_dev, const synx_geom* in_geom, float* ou
  * ShrinkImageFilter output information hxx:16-39). */
 int synx_shrink_geom(const synx_geom* in, int factor, synx_geom* out);
 
+/* ---- Linear transforms (host only, no CUDA call) --------------------------------------------
+ * The linear transforms antsRegistration writes next to its warps (prefix0GenericAffine.mat, or
+ * Rigid/Similarity/Translation/Affine .mat files without collapsing) and antsApplyTransforms reads
+ * in its transform stack: Utilities/itkantsReadWriteTransform.h:19-120 hands .mat/.txt files to
+ * ITK's transform file reader.  Every supported type is stored as the matrix-offset form ITK's
+ * MatrixOffsetTransformBase applies to physical (LPS) points:  T(p) = A (p - c) + t + c.        */
+typedef struct synx_linear {
+  int32_t dim;            /* 2 or 3 */
+  int32_t reserved0;
+  double matrix[9];       /* A, row-major 3x3; a 2-D transform fills the leading 2x2 block */
+  double translation[3];  /* t */
+  double center[3];       /* c, the transform's fixed parameters */
+} synx_linear;
+
+/* Reads linear transform `index` (0-based, file order) of an ITK transform file: the MATLAB v4
+ * binary form (.mat; a parameter variable named after the transform type, then "fixed") or the
+ * Insight text form (.txt: "Transform:", "Parameters:", "FixedParameters:" lines).  Types, double
+ * or float, `dim` x `dim`: AffineTransform, MatrixOffsetTransformBase, TranslationTransform,
+ * IdentityTransform, Euler2DTransform, Rigid2DTransform, Similarity2DTransform, Euler3DTransform,
+ * VersorRigid3DTransform, Similarity3DTransform; a CompositeTransform entry is skipped (its
+ * components follow it, in the order a composite adds them).  `out` may be NULL to count.
+ * Returns the number of linear transforms in the file (>= 1), or SYNX_E_ARG (missing, malformed
+ * or empty file, dimension mismatch, index out of range) / SYNX_E_UNSUPPORTED (another transform
+ * type); synx_last_error(NULL) names the reason. */
+int synx_read_linear_transform(const char* path, int dim, int index, synx_linear* out);
+
+/* Displacement field of a linear transform on `grid`, in host memory, interleaved components
+ * (the Warp.nii.gz layout): u(p) = T(p) - p at every voxel centre p, or T^-1(p) - p with
+ * invert = 1 (SYNX_E_ARG when A is singular).  Double arithmetic, float output. */
+int synx_linear_field(const synx_linear* transform, int invert, const synx_geom* grid, float* field_host);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,217 @@
+"""Linear transforms of ITK transform files (synx_read_linear_transform) and their displacement
+fields (synx_linear_field): host-only entry points of the C ABI, checked on the CPU against
+numpy and scipy's rotation conventions.  The files are written here in the two forms ITK's
+transform IO uses: MATLAB v4 binary (.mat) and Insight text (.txt, the layout of
+Scripts/ANTSAverage3DAffine.sh:94-98)."""
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+from scipy.spatial.transform import Rotation
+
+from ants_b200 import synx
+from ants_b200.synx import Geom, LinearTransform, SynxError
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+APPLY = os.path.join(ROOT, "ants_b200", "antsApplyTransforms_b200")
+
+
+def write_mat(path, variables, big=False, single=False, rowwise=False):
+    """MATLAB v4: per variable a header (type, rows, cols, imagf, namelen), the name with its NUL,
+    then the values.  type = 1000 M + 100 O + 10 P (M byte order, O storage order, P precision)."""
+    e = ">" if big else "<"
+    with open(path, "wb") as fh:
+        for name, vals in variables:
+            vals = np.asarray(vals, dtype=np.float64).ravel()
+            typ = (1000 if big else 0) + (100 if rowwise else 0) + (10 if single else 0)
+            nm = name.encode() + b"\0"
+            fh.write(struct.pack(e + "5i", typ, len(vals), 1, 0, len(nm)))
+            fh.write(nm)
+            fh.write(vals.astype(e + ("f4" if single else "f8")).tobytes())
+
+
+def write_txt(path, transforms):
+    lines = ["#Insight Transform File V1.0 "]
+    for i, (name, params, fixed) in enumerate(transforms):
+        lines += [f"# Transform {i} ", f"Transform: {name}  ",
+                  "Parameters:  " + " ".join(repr(float(v)) for v in params) + "  ",
+                  "FixedParameters: " + " ".join(repr(float(v)) for v in fixed) + " "]
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+
+
+def physical_points(g: Geom) -> np.ndarray:
+    """p = origin + D diag(spacing) index at every voxel, shape g.shape + (dim,)."""
+    axes = np.meshgrid(*[np.arange(n) for n in reversed(g.size)], indexing="ij")
+    idx = np.stack(list(reversed(axes)), -1).astype(np.float64)  # (..., dim) in x, y, z order
+    return np.asarray(g.origin) + (idx * np.asarray(g.spacing)) @ g.direction.T
+
+
+def apply(t: LinearTransform, p: np.ndarray, inverse=False) -> np.ndarray:
+    if inverse:
+        return (p - t.translation - t.center) @ np.linalg.inv(t.matrix).T + t.center
+    return (p - t.center) @ t.matrix.T + t.translation + t.center
+
+
+AFFINE3 = np.array([1.05, 0.08, -0.03, -0.06, 0.97, 0.04, 0.02, -0.05, 1.02])
+TRANS3 = np.array([2.5, -1.25, 3.0])
+CENTER3 = np.array([10.0, -4.0, 7.5])
+
+
+@pytest.mark.parametrize("big,single,rowwise", [(False, False, False), (True, False, False), (False, True, False),
+                                                (False, False, True)])
+def test_read_affine_mat(tmp_path, big, single, rowwise):
+    p = tmp_path / "a.mat"
+    name = "AffineTransform_float_3_3" if single else "AffineTransform_double_3_3"
+    write_mat(p, [(name, np.r_[AFFINE3, TRANS3]), ("fixed", CENTER3)], big=big, single=single, rowwise=rowwise)
+    assert synx.count_linear_transforms(p, 3) == 1
+    t = synx.read_linear_transform(p, 3)
+    tol = 1e-7 if single else 0.0
+    np.testing.assert_allclose(t.matrix, AFFINE3.reshape(3, 3), atol=tol)
+    np.testing.assert_allclose(t.translation, TRANS3, atol=tol)
+    np.testing.assert_allclose(t.center, CENTER3, atol=tol)
+
+
+def test_read_text_form_of_the_reference_script(tmp_path):
+    p = tmp_path / "avg.txt"
+    write_txt(p, [("MatrixOffsetTransformBase_double_3_3", np.r_[AFFINE3, TRANS3], CENTER3)])
+    t = synx.read_linear_transform(p, 3)
+    np.testing.assert_array_equal(t.matrix, AFFINE3.reshape(3, 3))
+    np.testing.assert_array_equal(t.translation, TRANS3)
+    np.testing.assert_array_equal(t.center, CENTER3)
+
+
+def test_rotation_types_follow_itk_conventions(tmp_path):
+    ax, ay, az = 0.3, -0.2, 0.45
+    c = [1.0, 2.0, 3.0]
+    cases = [
+        # Euler3DTransform: A = Rz Rx Ry (rotate about y, then x, then z, fixed axes)
+        ("Euler3DTransform_double_3_3", [ax, ay, az, 1, 2, 3], c, Rotation.from_euler("yxz", [ay, ax, az]).as_matrix()),
+        # with the fourth fixed parameter set: A = Rz Ry Rx
+        ("Euler3DTransform_double_3_3", [ax, ay, az, 1, 2, 3], c + [1.0],
+         Rotation.from_euler("xyz", [ax, ay, az]).as_matrix()),
+        ("VersorRigid3DTransform_double_3_3", [0.1, -0.2, 0.15, 1, 2, 3], c,
+         Rotation.from_quat([0.1, -0.2, 0.15, np.sqrt(1 - 0.1**2 - 0.2**2 - 0.15**2)]).as_matrix()),
+        ("Similarity3DTransform_double_3_3", [0.1, -0.2, 0.15, 1, 2, 3, 1.3], c,
+         1.3 * Rotation.from_quat([0.1, -0.2, 0.15, np.sqrt(1 - 0.1**2 - 0.2**2 - 0.15**2)]).as_matrix()),
+        ("TranslationTransform_double_3_3", [1, 2, 3], [], np.eye(3)),
+    ]
+    for i, (name, params, fixed, A) in enumerate(cases):
+        p = tmp_path / f"r{i}.txt"
+        write_txt(p, [(name, params, fixed)])
+        t = synx.read_linear_transform(p, 3)
+        np.testing.assert_allclose(t.matrix, A, atol=1e-12, err_msg=name)
+        np.testing.assert_allclose(t.translation, [1, 2, 3], err_msg=name)
+        np.testing.assert_allclose(t.center, fixed[:3] if fixed else [0, 0, 0], err_msg=name)
+    th = 0.4
+    R = np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+    for name, params, A in [("Euler2DTransform_double_2_2", [th, 5, -6], R),
+                            ("Rigid2DTransform_double_2_2", [th, 5, -6], R),
+                            ("Similarity2DTransform_double_2_2", [0.8, th, 5, -6], 0.8 * R)]:
+        p = tmp_path / f"{name}.mat"
+        write_mat(p, [(name, params), ("fixed", [3.0, 4.0])])
+        t = synx.read_linear_transform(p, 2)
+        np.testing.assert_allclose(t.matrix, A, atol=1e-12, err_msg=name)
+        np.testing.assert_allclose(t.translation, [5, -6])
+        np.testing.assert_allclose(t.center, [3, 4])
+    write_txt(tmp_path / "id.txt", [("IdentityTransform_double_3_3", [], [])])
+    t = synx.read_linear_transform(tmp_path / "id.txt", 3)
+    np.testing.assert_array_equal(t.matrix, np.eye(3))
+    np.testing.assert_array_equal(t.translation, 0)
+
+
+def test_composite_file_lists_components_in_order(tmp_path):
+    p = tmp_path / "comp.txt"
+    write_txt(p, [("CompositeTransform_double_3_3", [], []),
+                  ("TranslationTransform_double_3_3", [1, 0, 0], []),
+                  ("AffineTransform_double_3_3", np.r_[AFFINE3, TRANS3], CENTER3)])
+    assert synx.count_linear_transforms(p, 3) == 2
+    np.testing.assert_array_equal(synx.read_linear_transform(p, 3, 0).translation, [1, 0, 0])
+    np.testing.assert_array_equal(synx.read_linear_transform(p, 3, 1).matrix, AFFINE3.reshape(3, 3))
+
+
+@pytest.mark.parametrize("content,needle,code", [
+    ("txt:BSplineTransform_double_3_3", "not supported", -5),
+    ("txt:AffineTransform_double_2_2", "not a 3-D transform", -1),
+    ("txt:AffineTransform_double_3_3:short", "expected 12", -1),
+    ("mat:garbage", "not a MATLAB v4 file", -1),
+    ("mat:truncated", "truncated", -1),
+    ("txt:noheader", "not an Insight transform text file", -1),
+    ("missing", "cannot open transform file", -1),
+    ("index", "out of range", -1),
+])
+def test_read_errors(tmp_path, content, needle, code):
+    kind = content.split(":")
+    if kind[0] == "txt" and kind[1] == "noheader":
+        p = tmp_path / "x.txt"
+        p.write_text("Transform: AffineTransform_double_3_3\nParameters: 1 0 0 0 1 0 0 0 1 0 0 0\n")
+    elif kind[0] == "txt":
+        p = tmp_path / "x.txt"
+        n = 6 if len(kind) > 2 else 12
+        write_txt(p, [(kind[1], list(range(n)), [0, 0, 0])])
+    elif content == "mat:garbage":
+        p = tmp_path / "x.mat"
+        p.write_bytes(b"\x7f\x7f\x7f\x7f" * 10)
+    elif content == "mat:truncated":
+        p = tmp_path / "x.mat"
+        write_mat(p, [("AffineTransform_double_3_3", np.r_[AFFINE3, TRANS3])])
+        p.write_bytes(p.read_bytes()[:-9])
+    elif content == "missing":
+        p = tmp_path / "none.mat"
+    else:
+        p = tmp_path / "x.mat"
+        write_mat(p, [("AffineTransform_double_3_3", np.r_[AFFINE3, TRANS3]), ("fixed", CENTER3)])
+        with pytest.raises(SynxError, match=needle):
+            synx.read_linear_transform(p, 3, 1)
+        return
+    lib = synx.load_library()
+    rc = lib.synx_read_linear_transform(os.fsencode(str(p)), 3, 0, None)
+    assert rc == code
+    assert needle in lib.synx_last_error(None).decode()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_linear_field_matches_numpy(dim):
+    if dim == 3:
+        t = LinearTransform(AFFINE3.reshape(3, 3), TRANS3, CENTER3)
+        direction = Rotation.from_euler("xyz", [0.2, -0.1, 0.3]).as_matrix()
+        g = Geom((17, 13, 11), (1.2, 0.9, 1.5), (-5.0, 3.0, 2.0), direction)
+    else:
+        t = LinearTransform(np.array([[0.95, 0.1], [-0.07, 1.04]]), np.array([1.5, -2.0]), np.array([4.0, 6.0]))
+        th = 0.3
+        g = Geom((23, 19), (1.1, 0.8), (2.0, -1.0), np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]]))
+    P = physical_points(g)
+    for inverse in (False, True):
+        u = synx.linear_field(t, g, invert=inverse)
+        assert u.shape == g.shape + (dim,)
+        np.testing.assert_allclose(u, apply(t, P, inverse) - P, atol=2e-5)
+    # forward then inverse is the identity
+    np.testing.assert_allclose(apply(t, apply(t, P), inverse=True), P, atol=1e-9)
+
+
+def test_linear_field_rejects_singular_inverse_and_bad_grids():
+    t = LinearTransform(np.array([[1.0, 2.0, 0.0], [2.0, 4.0, 0.0], [0.0, 0.0, 1.0]]), np.zeros(3), np.zeros(3))
+    g = Geom((4, 4, 4))
+    synx.linear_field(t, g)  # the forward map needs no inverse
+    with pytest.raises(SynxError, match="singular"):
+        synx.linear_field(t, g, invert=True)
+    with pytest.raises(SynxError, match="dimensions differ"):
+        synx.linear_field(t, Geom((4, 4)))
+
+
+@pytest.fixture(scope="module")
+def apply_exe():
+    from ants_b200 import build
+    build.build_all()
+    assert os.path.exists(APPLY)
+    return APPLY
+
+
+@pytest.mark.parametrize("tname,needle", [("affine.h5", "not supported"), ("missing.mat", "cannot open transform file")])
+def test_cli_rejects_unreadable_transforms(apply_exe, tmp_path, tname, needle):
+    r = subprocess.run([apply_exe, "-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz", "-t",
+                        str(tmp_path / tname)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    assert needle in r.stderr
