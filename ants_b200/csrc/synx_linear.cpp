@@ -393,13 +393,16 @@ int synx_linear_field(const synx_linear* t, int invert, const synx_geom* g, floa
     u0[r] = b[r];
     for (int m = 0; m < D; ++m) u0[r] += (M[r * 3 + m] - (r == m ? 1.0 : 0.0)) * g->origin[m];
   }
+  // component planes: component r of voxel i at field[r * N + i]
   const int64_t nx = g->size[0], ny = g->size[1], nz = D == 3 ? g->size[2] : 1;
-  size_t o = 0;
+  const size_t N = (size_t)(nx * ny * nz);
+  size_t i = 0;
   for (int64_t z = 0; z < nz; ++z)
     for (int64_t y = 0; y < ny; ++y)
-      for (int64_t x = 0; x < nx; ++x) {
+      for (int64_t x = 0; x < nx; ++x, ++i) {
         const double i0 = (double)x, i1 = (double)y, i2 = (double)z;
-        for (int r = 0; r < D; ++r) field[o++] = (float)(u0[r] + E[r * 3] * i0 + E[r * 3 + 1] * i1 + E[r * 3 + 2] * i2);
+        for (int r = 0; r < D; ++r)
+          field[(size_t)r * N + i] = (float)(u0[r] + E[r * 3] * i0 + E[r * 3 + 1] * i1 + E[r * 3 + 2] * i2);
       }
   return SYNX_OK;
 }

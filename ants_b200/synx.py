@@ -707,8 +707,9 @@ def read_linear_transform(path, dim: int, index: int = 0) -> LinearTransform:
 
 
 def linear_field(t: LinearTransform, g: Geom, invert: bool = False) -> np.ndarray:
-    """Displacement T(p) - p (or T^-1(p) - p) at every voxel of `g`, interleaved: shape g.shape + (dim,)."""
-    out = np.empty(g.shape + (g.dim,), dtype=np.float32)
+    """Displacement T(p) - p (or T^-1(p) - p) at every voxel of `g`, as component planes (the
+    layout of the step functions): shape (dim,) + g.shape."""
+    out = np.empty((g.dim,) + g.shape, dtype=np.float32)
     tc, gc = t.to_c(), g.to_c()
     _check(load_library().synx_linear_field(C.byref(tc), int(bool(invert)), C.byref(gc), _ptr(out)))
     return out

@@ -16,9 +16,11 @@
  *   - Return value 0 = success, negative = error class (SYNX_E_*); synx_last_error() gives
  *     the message of the last failing call on that context (or the thread's last global
  *     error when ctx is NULL).
- *   - Images are float32, x fastest.  Displacement fields are physical-space vectors (mm)
- *     and are exchanged in ITK's interleaved layout (x,y[,z] per voxel, voxel order x
- *     fastest), which is also the layout of the vector NIfTI written as prefix0Warp.nii.gz.
+ *   - Images are float32, x fastest.  Displacement fields are physical-space vectors (mm).
+ *     The stage's field exchange (synx_get_fields, synx_get/set_half_fields) uses ITK's
+ *     interleaved in-memory layout (x,y[,z] per voxel, voxel order x fastest); the step entry
+ *     points and synx_linear_field use component planes (component c of voxel i at f[c*N+i]),
+ *     the order in which a vector NIfTI such as prefix0Warp.nii.gz stores its components.
  *   - "host" pointers are ordinary CPU memory; "dev" pointers are CUDA device memory on the
  *     context's device.  Every call is ordered on the context's CUDA stream.
  *   - A context is used by one host thread at a time; several contexts may run concurrently.
@@ -327,9 +329,11 @@ typedef struct synx_linear {
  * type); synx_last_error(NULL) names the reason. */
 int synx_read_linear_transform(const char* path, int dim, int index, synx_linear* out);
 
-/* Displacement field of a linear transform on `grid`, in host memory, interleaved components
- * (the Warp.nii.gz layout): u(p) = T(p) - p at every voxel centre p, or T^-1(p) - p with
- * invert = 1 (SYNX_E_ARG when A is singular).  Double arithmetic, float output. */
+/* Displacement field of a linear transform on `grid`, in host memory, as component planes
+ * (component c of voxel i at field[c*N + i], the layout of the step entry points, ready to copy
+ * to the device for synx_compose / synx_warp_image): u(p) = T(p) - p at every voxel centre p,
+ * or T^-1(p) - p with invert = 1 (SYNX_E_ARG when A is singular).  Double arithmetic, float
+ * output. */
 int synx_linear_field(const synx_linear* transform, int invert, const synx_geom* grid, float* field_host);
 
 #ifdef __cplusplus

@@ -113,10 +113,10 @@ def linear_stack_case(dim, tmp_path):
         for var, vals in ((name, np.r_[t.matrix.ravel(), t.translation]), ("fixed", t.center)):
             nm = var.encode() + b"\0"
             fh.write(np.array([0, len(vals), 1, 0, len(nm)], "<i4").tobytes() + nm + np.asarray(vals, "<f8").tobytes())
-    u_fwd = synx.linear_field(t, g)
+    u_fwd = synx.linear_field(t, g)  # component planes, as the step functions take them
     u_inv = synx.linear_field(t, g, invert=True)
-    w = O.compose(planes(a), planes(u_fwd), g)  # the affine first, then a
-    return g, gi, img, a, w, planes(u_inv)
+    w = O.compose(planes(a), u_fwd, g)  # the affine first, then a
+    return g, gi, img, a, w, u_inv
 
 
 @pytest.mark.gpu

@@ -185,10 +185,36 @@ def test_linear_field_matches_numpy(dim):
     P = physical_points(g)
     for inverse in (False, True):
         u = synx.linear_field(t, g, invert=inverse)
-        assert u.shape == g.shape + (dim,)
-        np.testing.assert_allclose(u, apply(t, P, inverse) - P, atol=2e-5)
+        assert u.shape == (dim,) + g.shape  # component planes
+        np.testing.assert_allclose(u, np.moveaxis(apply(t, P, inverse) - P, -1, 0), atol=2e-5)
     # forward then inverse is the identity
     np.testing.assert_allclose(apply(t, apply(t, P), inverse=True), P, atol=1e-9)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_linear_field_drives_the_step_functions(dim):
+    """The field's layout is the one the step functions take: warping an image that is linear in
+    physical space through it (the oracle's warp, whose layout the GPU parity tests pin) gives
+    that linear function at T(p) wherever T(p) stays inside the image."""
+    import oracle as O
+    if dim == 3:
+        t = LinearTransform(AFFINE3.reshape(3, 3), TRANS3, CENTER3)
+        g = Geom((20, 18, 16), (1.0, 1.2, 0.9), (4.0, -6.0, 2.0))
+        gi = Geom((40, 40, 36), (1.0, 1.0, 1.0), (-6.0, -16.0, -8.0))
+    else:
+        t = LinearTransform(np.array([[0.95, 0.1], [-0.07, 1.04]]), np.array([1.5, -2.0]), np.array([4.0, 6.0]))
+        g = Geom((24, 20), (1.1, 0.8), (2.0, -1.0))
+        gi = Geom((44, 40), (1.0, 1.0), (-8.0, -11.0))
+    coef = np.array([0.7, -0.4, 0.25])[:dim]
+    img = (physical_points(gi) @ coef + 3.0).astype(np.float32)
+    got = O.warp_image(img, gi, synx.linear_field(t, g), g)
+    Tp = apply(t, physical_points(g))
+    want = Tp @ coef + 3.0
+    lo = np.asarray(gi.origin)
+    hi = lo + (np.asarray(gi.size) - 1) * np.asarray(gi.spacing)
+    inside = np.all((Tp > lo + 1e-3) & (Tp < hi - 1e-3), axis=-1)
+    assert inside.mean() > 0.9
+    np.testing.assert_allclose(got[inside], want[inside], atol=2e-4)
 
 
 def test_linear_field_rejects_singular_inverse_and_bad_grids():
