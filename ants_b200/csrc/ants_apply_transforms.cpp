@@ -1,16 +1,23 @@
-// antsApplyTransforms-compatible command line for displacement-field transforms, on the synx C ABI.
+// antsApplyTransforms-compatible command line for displacement-field and linear transforms, on the
+// synx C ABI.
 //
 // The step right after the SyN stage: resample an image into the reference space through the
-// fields antsRegistration wrote (prefix0Warp.nii.gz / prefix0InverseWarp.nii.gz).  Options follow
+// fields antsRegistration wrote (prefix0Warp.nii.gz / prefix0InverseWarp.nii.gz) and the linear
+// transforms before them (prefix0GenericAffine.mat).  Options follow
 // Examples/antsApplyTransforms.cxx:1063-1240:
 //   -d/--dimensionality 2|3      -i/--input image     -r/--reference-image image
-//   -t/--transform file  (repeatable).  As in the reference's transform stack (:1183-1196), a
-//       reference point is moved first by the LAST transform given, then by the one before it.
+//   -t/--transform file  (repeatable).  Order: a reference point is moved by the FIRST transform
+//       given, then by the second, and so on; the input is sampled where the last one puts it.
+//       This is the reference's order: its parser stores repeated options newest first
+//       (Utilities/antsCommandLineOption.cxx:42,64 push_front), the transform loop adds them to
+//       an ITK composite in that stored order (Examples/itkantsRegistrationHelper.h:1284-1459),
+//       and a composite applies the transform added last first.  So `-t 1Warp -t 0GenericAffine.mat`
+//       maps p to A(p + u(p)), as the registration's own composite does.
 //       A displacement field image: [field,0] is accepted; [field,1] is rejected (a displacement
 //       field has no closed-form inverse: pass the InverseWarp field instead).
-//       A linear transform file (.mat / .txt, e.g. prefix0GenericAffine.mat; the types
-//       synx_read_linear_transform reads): [file,1] applies its inverse.  A file holding several
-//       transforms enters the stack in file order (reversed and each inverted for [file,1]).
+//       A linear transform file (.mat / .txt; the types synx_read_linear_transform reads): [file,1]
+//       applies its inverse.  The transforms of one file act as the composite the file holds: the
+//       last one first, or for [file,1] the inverse of the first one first (:1440-1451).
 //       HDF5 composite files (.h5) are not supported.
 //   -n/--interpolation Linear (the default; other interpolators are rejected)
 //   -f/--default-value v (0): value where the point maps outside the input image
@@ -18,18 +25,28 @@
 //       the single displacement field equivalent to the stack, on the reference grid, :1115-1131)
 //   --float 0|1 (computation is float32 either way)   -v/--verbose 0|1   --gpu N (not a reference option)
 //
-// GPU path: every field is brought onto the reference grid (synx_resample_field when its grid
-// differs; a linear transform is written there as its displacement T(p) - p by
-// synx_linear_field), the stack is composed in place, w <- w + u_i(x + w) from the last transform
-// to the first (synx_compose), and the input is sampled once at x + w (synx_warp_image).  A
-// displacement on the reference grid is zero outside it, so a transform that is not applied first
-// acts as the identity where the transforms before it move a point off the reference grid (a
-// linear transform applied first, the usual `-t warp -t affine` order, is exact everywhere).
+// GPU path.  The chain of transforms, in application order, is split into a leading run of
+// linear transforms L_pre, a middle part from the first field to the last field, and a trailing
+// run of linear transforms L_post (a chain without fields is all L_pre).  The linear ends are
+// folded into grid geometry, which the device functions take as general index <-> physical maps:
+//   * the evaluation grid G has the reference grid's voxels at L_pre(p) (direction M*D, origin
+//     M*o + b for L_pre(p) = M p + b);
+//   * the input image is given the geometry under which sampling at q reads it at L_post(q).
+// The middle part is composed on G: the first field is copied onto G (synx_resample_field when
+// its own grid differs), every later transform's displacement is brought onto G (resampled, or
+// synx_linear_field for a linear transform) and composed, w <- w + u(x + w) (synx_compose).
+// The input is sampled once at L_post(x_G + w) (synx_warp_image).  Exact (one interpolation per
+// field, as ITK's composite) when the middle part is a single field, or fields that share G:
+// e.g. `-t 1Warp -t 0GenericAffine.mat` on the fixed grid and `-t [0GenericAffine.mat,1]
+// -t 1InverseWarp` on the moving grid.  A later middle transform is read through its copy on G:
+// a second interpolation for a field on another grid, and no displacement where the point has
+// left G.  The collapsed field, L_post(x_G + w) - p, is assembled on the host while it is written.
 #include "ants_apply_transforms.h"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
@@ -73,12 +90,90 @@ bool ends_with(const std::string& s, const std::string& suffix) {
   return s.size() >= suffix.size() && s.compare(s.size() - suffix.size(), suffix.size(), suffix) == 0;
 }
 
-// One transform of the stack: a displacement field image, or a linear transform of a .mat/.txt file.
-struct StackEntry {
+// An affine map p -> M p + b (3x3 row-major; a 2-D map keeps the third row and column identity).
+struct Map {
+  double M[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  double b[3] = {0, 0, 0};
+};
+
+Map mul(const Map& second, const Map& first) {  // second(first(p))
+  Map r;
+  for (int i = 0; i < 3; ++i) {
+    r.b[i] = second.b[i];
+    for (int k = 0; k < 3; ++k) {
+      double s = 0.0;
+      for (int m = 0; m < 3; ++m) s += second.M[i * 3 + m] * first.M[m * 3 + k];
+      r.M[i * 3 + k] = s;
+      r.b[i] += second.M[i * 3 + k] * first.b[k];
+    }
+  }
+  return r;
+}
+
+bool inverse(const Map& a, Map& r) {
+  const double* m = a.M;
+  const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                     m[2] * (m[3] * m[7] - m[4] * m[6]);
+  double scale = 0.0;
+  for (int k = 0; k < 9; ++k) scale = std::max(scale, std::fabs(m[k]));
+  if (!(std::fabs(det) > 1e-12 * scale * scale * scale)) return false;
+  const double id = 1.0 / det;
+  r.M[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+  r.M[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+  r.M[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+  r.M[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+  r.M[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+  r.M[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+  r.M[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+  r.M[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+  r.M[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+  for (int i = 0; i < 3; ++i) {
+    r.b[i] = 0.0;
+    for (int k = 0; k < 3; ++k) r.b[i] -= r.M[i * 3 + k] * a.b[k];
+  }
+  return true;
+}
+
+// T(p) = A (p - c) + t + c, or its inverse.
+Map map_of(const synx_linear& t, bool invert) {
+  Map m;
+  for (int k = 0; k < 9; ++k) m.M[k] = t.matrix[k];
+  if (t.dim == 2) {
+    m.M[2] = m.M[5] = m.M[6] = m.M[7] = 0.0;
+    m.M[8] = 1.0;
+  }
+  for (int i = 0; i < 3; ++i) {
+    m.b[i] = i < t.dim ? t.translation[i] + t.center[i] : 0.0;
+    for (int k = 0; k < t.dim; ++k) m.b[i] -= m.M[i * 3 + k] * t.center[k];
+  }
+  if (!invert) return m;
+  Map r;
+  if (!inverse(m, r)) throw std::runtime_error("a linear transform of the stack has a singular matrix, no inverse");
+  return r;
+}
+
+// The grid whose voxel i sits at L(p_i), p_i the voxel of g: direction M D, origin M o + b.
+synx_geom push_forward(const synx_geom& g, const Map& L) {
+  synx_geom r = g;
+  for (int i = 0; i < 3; ++i) {
+    r.origin[i] = L.b[i];
+    for (int k = 0; k < 3; ++k) {
+      r.origin[i] += L.M[i * 3 + k] * g.origin[k];
+      double s = 0.0;
+      for (int m = 0; m < 3; ++m) s += L.M[i * 3 + m] * g.direction[m * 3 + k];
+      r.direction[i * 3 + k] = s;
+    }
+  }
+  return r;
+}
+
+// One transform of the chain, in application order.
+struct ChainItem {
   std::string file;
   bool is_linear = false;
-  bool invert = false;
+  Map map;  // linear transforms
   synx_linear linear{};
+  bool invert = false;
 };
 
 int run(const std::vector<std::string>& args, std::ostream& out) {
@@ -136,8 +231,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   }
   if (!collapse && !opt.count("input")) throw std::runtime_error("an input image (-i) is required");
 
-  // transforms in command-line order
-  std::vector<StackEntry> stack;
+  // the chain in application order: command-line order, each file's transforms as its composite
+  std::vector<ChainItem> chain;
   for (const std::string& v : opt["transform"]) {
     OptionCall t = parse_call(v);
     std::string file = t.name;
@@ -154,66 +249,85 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     if (ends_with(lf, ".mat") || ends_with(lf, ".txt")) {
       const int n = synx_read_linear_transform(file.c_str(), dim, 0, nullptr);
       if (n < 0) throw std::runtime_error(synx_last_error(nullptr));
-      std::vector<StackEntry> part;
+      std::vector<ChainItem> part;
       for (int i = 0; i < n; ++i) {
-        StackEntry e;
-        e.file = file;
-        e.is_linear = true;
-        e.invert = invert;
-        step_ok(synx_read_linear_transform(file.c_str(), dim, i, &e.linear) < 0 ? -1 : 0,
+        ChainItem c;
+        c.file = file;
+        c.is_linear = true;
+        c.invert = invert;
+        step_ok(synx_read_linear_transform(file.c_str(), dim, i, &c.linear) < 0 ? -1 : 0,
                 "synx_read_linear_transform");
-        part.push_back(e);
+        c.map = map_of(c.linear, invert);
+        part.push_back(c);
       }
-      if (invert) std::reverse(part.begin(), part.end());
-      stack.insert(stack.end(), part.begin(), part.end());
+      // a composite applies its last transform first; its inverse applies the first one's inverse first
+      if (!invert) std::reverse(part.begin(), part.end());
+      chain.insert(chain.end(), part.begin(), part.end());
       continue;
     }
     if (invert)
       throw std::runtime_error("the inverse of displacement field '" + file +
                                "' is not available: use the inverse warp file antsRegistration wrote");
-    StackEntry e;
-    e.file = file;
-    stack.push_back(e);
+    ChainItem c;
+    c.file = file;
+    chain.push_back(c);
   }
+
+  // split: leading linear run, middle (first field .. last field), trailing linear run
+  size_t first_field = chain.size(), last_field = chain.size();
+  for (size_t k = 0; k < chain.size(); ++k)
+    if (!chain[k].is_linear) {
+      if (first_field == chain.size()) first_field = k;
+      last_field = k;
+    }
+  Map pre, post;
+  const size_t lead_end = first_field;  // [0, lead_end) folds into the evaluation grid
+  const size_t tail_begin = first_field == chain.size() ? chain.size() : last_field + 1;
+  for (size_t k = 0; k < lead_end; ++k) pre = mul(chain[k].map, pre);
+  for (size_t k = tail_begin; k < chain.size(); ++k) post = mul(chain[k].map, post);
 
   const nifti::Image ref = nifti::read(one("reference-image", ""));
   const synx_geom gr = to_geom(ref, dim);
   const long long N = gr.size[0] * gr.size[1] * gr.size[2];
+  const synx_geom ge = push_forward(gr, pre);  // the evaluation grid
   if (cudaSetDevice(gpu) != cudaSuccess) throw std::runtime_error("cannot use GPU " + std::to_string(gpu));
 
-  // compose the stack on the reference grid: w = u_n, then w <- w + u_i(x + w), i = n-1 .. 1
+  // compose the middle part on the evaluation grid
   DeviceBuffer w((size_t)N * dim), tmp((size_t)N * dim);
   CLI_CK(cudaMemset(w.p, 0, 4 * (size_t)N * dim));
-  for (int k = (int)stack.size() - 1; k >= 0; --k) {
-    const StackEntry& e = stack[k];
+  for (size_t k = 0; k < chain.size(); ++k) {
+    const ChainItem& c = chain[k];
+    if (k < lead_end || k >= tail_begin) {
+      if (verbose)
+        out << "  transform " << k << ": " << c.file << (c.invert ? " (linear, inverse" : " (linear")
+            << (k < lead_end ? ", folded into the evaluation grid)" : ", folded into the input geometry)") << "\n";
+      continue;
+    }
     std::string note;
-    // this transform's displacement on the reference grid, in tmp
-    if (e.is_linear) {
+    // this transform's displacement on the evaluation grid, in tmp (in w for the first field)
+    float* dst = k == first_field ? w.p : tmp.p;
+    if (c.is_linear) {
       std::vector<float> u((size_t)N * dim);
-      step_ok(synx_linear_field(&e.linear, e.invert ? 1 : 0, &gr, u.data()), "synx_linear_field");
-      CLI_CK(cudaMemcpy(tmp.p, u.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
-      note = e.invert ? " (linear, inverse)" : " (linear)";
+      step_ok(synx_linear_field(&c.linear, c.invert ? 1 : 0, &ge, u.data()), "synx_linear_field");
+      CLI_CK(cudaMemcpy(dst, u.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+      note = c.invert ? " (linear, inverse)" : " (linear)";
     } else {
-      const nifti::Image f = nifti::read(e.file);
+      const nifti::Image f = nifti::read(c.file);
       if (f.components != dim || f.dim != dim)
-        throw std::runtime_error("'" + e.file + "' is not a " + std::to_string(dim) + "-D displacement field");
+        throw std::runtime_error("'" + c.file + "' is not a " + std::to_string(dim) + "-D displacement field");
       const synx_geom gf = to_geom(f, dim);
       const long long Nf = f.voxels();
-      if (same_grid(gf, gr)) {
-        CLI_CK(cudaMemcpy(tmp.p, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+      if (same_grid(gf, ge)) {
+        CLI_CK(cudaMemcpy(dst, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
       } else {
         DeviceBuffer src((size_t)Nf * dim);
         CLI_CK(cudaMemcpy(src.p, f.data.data(), 4 * (size_t)Nf * dim, cudaMemcpyHostToDevice));
-        step_ok(synx_resample_field(src.p, &gf, tmp.p, &gr, nullptr), "synx_resample_field");
+        step_ok(synx_resample_field(src.p, &gf, dst, &ge, nullptr), "synx_resample_field");
         note = " (resampled)";
       }
     }
-    if (k == (int)stack.size() - 1) {
-      std::swap(w.p, tmp.p);
-    } else {
-      step_ok(synx_compose(tmp.p, w.p, &gr, 1.0f, w.p, nullptr), "synx_compose");
-    }
-    if (verbose) out << "  transform " << k << ": " << e.file << note << "\n";
+    if (k != first_field) step_ok(synx_compose(tmp.p, w.p, &ge, 1.0f, w.p, nullptr), "synx_compose");
+    if (verbose) out << "  transform " << k << ": " << c.file << note << "\n";
   }
 
   if (collapse) {
@@ -228,6 +342,27 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     for (int k = 0; k < 9; ++k) fo.direction[k] = gr.direction[k];
     fo.data.resize((size_t)N * dim);
     CLI_CK(cudaMemcpy(fo.data.data(), w.p, 4 * (size_t)N * dim, cudaMemcpyDeviceToHost));
+    if (lead_end > 0 || tail_begin < chain.size()) {
+      // displacement of reference voxel p: L_post(L_pre(p) + w) - p, component planes
+      const long long nx = gr.size[0], ny = gr.size[1];
+      for (long long i = 0; i < N; ++i) {
+        const double idx[3] = {(double)(i % nx), (double)((i / nx) % ny), (double)(i / (nx * ny))};
+        double p[3], q[3];
+        for (int r = 0; r < 3; ++r) {
+          p[r] = gr.origin[r];
+          for (int c = 0; c < 3; ++c) p[r] += gr.direction[r * 3 + c] * gr.spacing[c] * idx[c];
+        }
+        for (int r = 0; r < 3; ++r) {
+          q[r] = pre.b[r] + (r < dim ? fo.data[(size_t)r * N + i] : 0.0);
+          for (int c = 0; c < 3; ++c) q[r] += pre.M[r * 3 + c] * p[c];
+        }
+        for (int r = 0; r < dim; ++r) {
+          double s = post.b[r];
+          for (int c = 0; c < 3; ++c) s += post.M[r * 3 + c] * q[c];
+          fo.data[(size_t)r * N + i] = (float)(s - p[r]);
+        }
+      }
+    }
     nifti::write(out_path, fo);
     if (verbose) out << "wrote the collapsed displacement field " << out_path << "\n";
     return EXIT_SUCCESS;
@@ -235,7 +370,13 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
 
   nifti::Image in = nifti::read(one("input", ""));
   if (in.components != 1) throw std::runtime_error("the input must be a scalar image");
-  const synx_geom gi = to_geom(in, dim);
+  synx_geom gi = to_geom(in, dim);
+  if (tail_begin < chain.size()) {
+    // sampling at q reads the input at L_post(q): the input's grid pulled back by L_post
+    Map back;
+    if (!inverse(post, back)) throw std::runtime_error("the trailing linear transforms have a singular matrix");
+    gi = push_forward(gi, back);
+  }
   // a default value v outside the input: sample (I - v) with 0 outside and add v back (inside the
   // buffer the linear weights sum to one, so the result there is the sample of I)
   if (defval != 0.0f)
@@ -243,7 +384,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const long long Ni = in.voxels();
   DeviceBuffer di((size_t)Ni), dout((size_t)N);
   CLI_CK(cudaMemcpy(di.p, in.data.data(), 4 * (size_t)Ni, cudaMemcpyHostToDevice));
-  step_ok(synx_warp_image(di.p, &gi, w.p, &gr, dout.p, nullptr), "synx_warp_image");
+  step_ok(synx_warp_image(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image");
   nifti::Image res = ref;
   res.components = 1;
   res.data.resize((size_t)N);
@@ -251,7 +392,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   if (defval != 0.0f)
     for (float& x : res.data) x += defval;
   nifti::write(out_path, res);
-  if (verbose) out << "wrote " << out_path << " (" << stack.size() << " transforms)\n";
+  if (verbose) out << "wrote " << out_path << " (" << chain.size() << " transforms)\n";
   return EXIT_SUCCESS;
 }
 

@@ -1,12 +1,12 @@
-"""The antsApplyTransforms-compatible front end (ants_b200/antsApplyTransforms_b200): images
-resampled through displacement-field stacks, and the collapsed-field output, against the oracle."""
+"""The antsApplyTransforms-compatible front end (ants_b200/antsApplyTransforms_b200): argument
+checks, the default value outside the input, and agreement with the registration's own warped
+output.  Stacks of several transforms are tested in test_zz_stack_apply.py."""
 import os
 import subprocess
 
 import numpy as np
 import pytest
 
-import oracle as O
 from ants_b200 import nifti, phantoms
 from ants_b200.synx import Geom
 
@@ -27,15 +27,6 @@ def run(exe, args):
     return subprocess.run([exe, *args], capture_output=True, text=True, timeout=600)
 
 
-def field(g, sigma, max_norm, seed):
-    u = phantoms.smooth_field(g.shape, sigma, max_norm, np.random.default_rng(seed))
-    return u.astype(np.float32)  # interleaved: shape + (dim,)
-
-
-def planes(u):
-    return np.ascontiguousarray(np.moveaxis(u, -1, 0))
-
-
 @pytest.mark.parametrize("args,needle", [
     (["-d", "3", "-i", "a.nii.gz", "-o", "x.nii.gz", "-t", "w.nii.gz"], "reference image"),
     (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz", "-t", "[w.nii.gz,1]"], "inverse warp"),
@@ -49,46 +40,6 @@ def test_rejects_bad_input(exe, args, needle):
     r = run(exe, args)
     assert r.returncode == 1
     assert needle in r.stderr
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("dim", [2, 3])
-def test_field_stack_matches_oracle(exe, tmp_path, cuda, dim):
-    g = Geom((60, 52) if dim == 2 else (34, 30, 28), (1.0,) * dim, (2.0,) * dim)
-    gi = Geom((70, 64) if dim == 2 else (40, 36, 30), (0.9,) * dim, (-1.0,) * dim)  # input on its own grid
-    img = np.random.default_rng(dim).uniform(0, 1, gi.shape).astype(np.float32)
-    a, b = field(g, 4.0, 2.5, 10 + dim), field(g, 5.0, 3.0, 20 + dim)
-    nifti.write(tmp_path / "ref.nii.gz", np.zeros(g.shape, np.float32), g)
-    nifti.write(tmp_path / "in.nii.gz", img, gi)
-    nifti.write(tmp_path / "a.nii.gz", a, g, vector=True)
-    nifti.write(tmp_path / "b.nii.gz", b, g, vector=True)
-    base = ["-d", str(dim), "-r", f"{tmp_path}/ref.nii.gz"]
-    # one field
-    r = run(exe, base + ["-i", f"{tmp_path}/in.nii.gz", "-t", f"{tmp_path}/a.nii.gz", "-o", f"{tmp_path}/o1.nii.gz"])
-    assert r.returncode == 0, r.stderr
-    got, go = nifti.read(tmp_path / "o1.nii.gz", dim)
-    assert go.size == g.size
-    # the input grid differs from the reference grid: float vs double index arithmetic moves
-    # interpolation weights by a few ulps (and rim points may fall either side), as in the step tests
-    bad = np.abs(got - O.warp_image(img, gi, planes(a), g)) > 1e-5
-    assert bad.mean() < 1e-3, bad.sum()
-    # -t a -t b: a reference point moves by b first, then by a
-    w = O.compose(planes(a), planes(b), g)
-    r = run(exe, base + ["-i", f"{tmp_path}/in.nii.gz", "-t", f"{tmp_path}/a.nii.gz", "-t", f"[{tmp_path}/b.nii.gz,0]",
-                         "-o", f"{tmp_path}/o2.nii.gz"])
-    assert r.returncode == 0, r.stderr
-    got, _ = nifti.read(tmp_path / "o2.nii.gz", dim)
-    ref = O.warp_image(img, gi, w, g)
-    assert np.abs(got - ref).max() < 1e-4
-    # the collapsed field of the same stack, both output spellings
-    for spelling in (f"[{tmp_path}/c1.nii.gz,1]", f"DisplacementField[{tmp_path}/c2.nii.gz]"):
-        r = run(exe, base + ["-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/b.nii.gz", "-o", spelling])
-        assert r.returncode == 0, r.stderr
-    c1, gc = nifti.read(tmp_path / "c1.nii.gz", dim)
-    c2, _ = nifti.read(tmp_path / "c2.nii.gz", dim)
-    assert gc.size == g.size
-    np.testing.assert_array_equal(c1, c2)
-    assert np.abs(planes(c1) - w).max() < 2e-5
 
 
 @pytest.mark.gpu

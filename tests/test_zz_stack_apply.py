@@ -1,0 +1,226 @@
+"""antsApplyTransforms_b200 transform stacks: order, linear transforms folded into grid geometry,
+and the collapsed field.
+
+The reference applies the FIRST -t to a reference point first (its parser stores repeated options
+newest first, Utilities/antsCommandLineOption.cxx:42,64, and an ITK composite applies the transform
+added last first), so `-t 1Warp -t 0GenericAffine.mat` samples the input at A(p + u(p)).
+
+`chain_displacement` is the reference's composite applied point by point: each field sampled on its
+own grid (the oracle's warp, the interpolation ITK's displacement-field transform uses), each linear
+transform applied analytically.  `emulate_cli` is the command line's scheme restated with the
+oracle's step functions: leading linear transforms folded into the evaluation grid, trailing ones
+into the input image's geometry, the middle composed on the evaluation grid.  CPU tests check the
+scheme against the composite on the stacks where it is exact; GPU tests check the command line
+against the scheme.  This file is collected last, after the allocation-free entry point's, so that
+a run which stops at the first failure has already run every other test.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from ants_b200 import nifti, phantoms
+from ants_b200.synx import Geom
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+APPLY = os.path.join(ROOT, "ants_b200", "antsApplyTransforms_b200")
+
+
+def planes(u):
+    return np.ascontiguousarray(np.moveaxis(u, -1, 0))
+
+
+def points(g: Geom) -> np.ndarray:
+    """Physical point of every voxel as component planes, shape (dim,) + g.shape."""
+    axes = np.meshgrid(*[np.arange(n) for n in reversed(g.size)], indexing="ij")
+    idx = np.stack(list(reversed(axes)), -1).astype(np.float64)
+    return planes(np.asarray(g.origin) + (idx * np.asarray(g.spacing)) @ g.direction.T)
+
+
+class Affine:
+    """p -> M p + b, with the ITK parameters it is written with: A, t, c (M = A, b = t + c - A c)."""
+
+    def __init__(self, A, t, c):
+        self.A, self.t, self.c = np.asarray(A, float), np.asarray(t, float), np.asarray(c, float)
+        self.M, self.b = self.A, self.t + self.c - self.A @ self.c
+
+    def inverse(self):
+        Mi = np.linalg.inv(self.M)
+        r = Affine.__new__(Affine)
+        r.M, r.b = Mi, -Mi @ self.b
+        return r
+
+    def apply(self, P):  # planes
+        return np.tensordot(self.M, P, axes=1) + self.b.reshape((-1,) + (1,) * (P.ndim - 1))
+
+    def write_mat(self, path):  # ITK MATLAB v4 form: parameters (A row-major, t), then "fixed" (c)
+        d = len(self.t)
+        with open(path, "wb") as fh:
+            for var, vals in ((f"AffineTransform_double_{d}_{d}", np.r_[self.A.ravel(), self.t]), ("fixed", self.c)):
+                nm = var.encode() + b"\0"
+                fh.write(np.array([0, len(vals), 1, 0, len(nm)], "<i4").tobytes() + nm +
+                         np.asarray(vals, "<f8").tobytes())
+
+
+def push_forward(g: Geom, L) -> Geom:
+    """The grid whose voxel i sits at L(p_i)."""
+    return Geom(g.size, g.spacing, tuple(L.M @ np.asarray(g.origin) + L.b), L.M @ g.direction)
+
+
+def chain_displacement(chain, gr: Geom) -> np.ndarray:
+    """Displacement of every reference voxel under the chain (application order), planes."""
+    P = points(gr)
+    D = np.zeros_like(P)
+    for kind, obj in chain:
+        if kind == "field":
+            d, gd = obj  # planes on their own grid
+            D = D + np.stack([O.warp_image(np.ascontiguousarray(d[c]), gd, D, gr, dtype=np.float64)
+                              for c in range(gr.dim)])
+        else:
+            D = obj.apply(P + D) - P
+    return D
+
+
+def emulate_cli(chain, gr: Geom, img=None, gi=None):
+    """The command line's scheme with the oracle's step functions.  Returns the collapsed field
+    (planes) and, with an input image, the warped image."""
+    fields = [k for k, (kind, _) in enumerate(chain) if kind == "field"]
+    lead_end = fields[0] if fields else len(chain)
+    tail_begin = fields[-1] + 1 if fields else len(chain)
+    dim = gr.dim
+    pre = Affine(np.eye(dim), np.zeros(dim), np.zeros(dim))
+    post = Affine(np.eye(dim), np.zeros(dim), np.zeros(dim))
+    for k in range(lead_end):
+        L = chain[k][1]
+        pre.M, pre.b = L.M @ pre.M, L.M @ pre.b + L.b
+    for k in range(tail_begin, len(chain)):
+        L = chain[k][1]
+        post.M, post.b = L.M @ post.M, L.M @ post.b + L.b
+    ge = push_forward(gr, pre)
+    w = np.zeros((dim,) + gr.shape, np.float32)
+    for k in range(lead_end, tail_begin):
+        kind, obj = chain[k]
+        if kind == "field":
+            d, gd = obj
+            u = O.resample_field(d, gd, ge)
+        else:
+            u = (obj.apply(points(ge)) - points(ge)).astype(np.float32)
+        w = u if k == lead_end else O.compose(u, w, ge)
+    P = points(gr)
+    collapsed = (post.apply(pre.apply(P) + w) - P).astype(np.float32)
+    warped = None
+    if img is not None:
+        warped = O.warp_image(img, push_forward(gi, post.inverse()), w, ge)
+    return collapsed, warped
+
+
+def field_on(g, sigma, max_norm, seed):
+    return planes(phantoms.smooth_field(g.shape, sigma, max_norm, np.random.default_rng(seed)).astype(np.float32))
+
+
+def affine(dim, k):
+    if dim == 3:
+        A = [[1.03, 0.05, -0.02], [-0.04, 0.98, 0.03], [0.01, -0.03, 1.01]] if k == 0 else \
+            [[0.97, -0.02, 0.04], [0.03, 1.02, -0.01], [-0.02, 0.05, 0.99]]
+        return Affine(A, [1.5, -1.0, 0.75] if k == 0 else [-2.0, 0.5, 1.25], [18.0, 16.0, 15.0])
+    A = [[0.97, 0.06], [-0.05, 1.02]] if k == 0 else [[1.04, -0.03], [0.05, 0.96]]
+    return Affine(A, [1.25, -0.75] if k == 0 else [-0.5, 1.0], [31.0, 27.0])
+
+
+def grids(dim):
+    g = Geom((60, 52) if dim == 2 else (34, 30, 28), (1.0,) * dim, (2.0,) * dim)          # fixed grid
+    gm = Geom((64, 56) if dim == 2 else (36, 32, 30), (0.9,) * dim, (-1.0,) * dim)        # moving grid
+    return g, gm
+
+
+def cases(dim):
+    """(name, chain, reference grid, scheme exact?) with the command-line spelling of each chain."""
+    g, gm = grids(dim)
+    a, b = field_on(g, 4.0, 2.0, 60 + dim), field_on(g, 5.0, 2.5, 70 + dim)
+    inv = field_on(g, 4.0, 2.0, 80 + dim)  # an inverse warp lives on the fixed grid too
+    A, B = affine(dim, 0), affine(dim, 1)
+    return {
+        # two fields on the reference grid: a first, then b
+        "fields": ([("field", (a, g)), ("field", (b, g))], g, ["a", "b"]),
+        # the forward standard stack on the fixed grid: warp first, then the affine
+        "forward": ([("field", (a, g)), ("linear", A)], g, ["a", "A.mat"]),
+        # the inverse standard stack on the moving grid: the affine's inverse first, then the inverse warp
+        "inverse": ([("linear", A.inverse()), ("field", (inv, g))], gm, ["[A.mat,1]", "inv"]),
+        # linear transforms only: A first, then B
+        "linear": ([("linear", A), ("linear", B)], gm, ["A.mat", "B.mat"]),
+        # affine, field, affine: both ends folded
+        "both_ends": ([("linear", B.inverse()), ("field", (a, g)), ("linear", A)], gm, ["[B.mat,1]", "a", "A.mat"]),
+    }, dict(a=a, b=b, inv=inv, A=A, B=B, g=g)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_scheme_is_the_composite_on_exact_stacks(dim):
+    cs, _ = cases(dim)
+    for name, (chain, gr, _) in cs.items():
+        want = chain_displacement(chain, gr)
+        got, _ = emulate_cli(chain, gr)
+        bad = np.abs(got - want) > 1e-4
+        assert bad.mean() < 1e-3, (name, float(np.abs(got - want).max()))
+
+
+def test_order_is_first_given_first_applied():
+    g, _ = grids(2)
+    a, b = field_on(g, 4.0, 2.0, 1), field_on(g, 5.0, 2.5, 2)
+    ab = chain_displacement([("field", (a, g)), ("field", (b, g))], g)
+    np.testing.assert_allclose(ab, O.compose(b, a, g), atol=1e-5)  # a + b(x + a)
+    ba = chain_displacement([("field", (b, g)), ("field", (a, g))], g)
+    assert np.abs(ab - ba).max() > 0.05
+
+
+@pytest.fixture(scope="module")
+def exe():
+    from ants_b200 import build
+    build.build_all()
+    assert os.path.exists(APPLY)
+    return APPLY
+
+
+def run(exe, args):
+    return subprocess.run([exe, *args], capture_output=True, text=True, timeout=600)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_stacks_match_the_scheme(exe, tmp_path, cuda, dim):
+    cs, parts = cases(dim)
+    g, gm = grids(dim)
+    files = {"a": parts["a"], "b": parts["b"], "inv": parts["inv"]}
+    for name, u in files.items():
+        nifti.write(tmp_path / f"{name}.nii.gz", np.ascontiguousarray(np.moveaxis(u, 0, -1)), g, vector=True)
+    parts["A"].write_mat(tmp_path / "A.mat")
+    parts["B"].write_mat(tmp_path / "B.mat")
+    nifti.write(tmp_path / "fixed.nii.gz", np.zeros(g.shape, np.float32), g)
+    nifti.write(tmp_path / "moving.nii.gz", np.zeros(gm.shape, np.float32), gm)
+    gi = Geom((70, 64) if dim == 2 else (40, 36, 32), (0.8,) * dim, (-3.0,) * dim)  # the input's own grid
+    img = np.random.default_rng(90 + dim).uniform(0, 1, gi.shape).astype(np.float32)
+    nifti.write(tmp_path / "in.nii.gz", img, gi)
+
+    def spell(tok):
+        if tok.startswith("["):
+            return f"[{tmp_path}/{tok[1:].split(',')[0]},1]"
+        return f"{tmp_path}/{tok}" + ("" if tok.endswith(".mat") else ".nii.gz")
+
+    for name, (chain, gr, toks) in cs.items():
+        ref = tmp_path / ("fixed.nii.gz" if gr is g else "moving.nii.gz")
+        ts = sum((["-t", spell(t)] for t in toks), [])
+        want_field, want_img = emulate_cli(chain, gr, img, gi)
+        r = run(exe, ["-d", str(dim), "-r", str(ref), "-i", f"{tmp_path}/in.nii.gz", *ts, "-o", f"{tmp_path}/o.nii.gz"])
+        assert r.returncode == 0, (name, r.stderr)
+        got, go = nifti.read(tmp_path / "o.nii.gz", dim)
+        assert go.size == gr.size
+        # float vs double index arithmetic moves interpolation weights by a few ulps and rim points
+        # may fall either side, so a small share of voxels may differ (as in the step tests)
+        bad = np.abs(got - want_img) > 1e-4
+        assert bad.mean() < 2e-3, (name, int(bad.sum()))
+        r = run(exe, ["-d", str(dim), "-r", str(ref), *ts, "-o", f"[{tmp_path}/c.nii.gz,1]"])
+        assert r.returncode == 0, (name, r.stderr)
+        c, _ = nifti.read(tmp_path / "c.nii.gz", dim)
+        bad = np.abs(planes(c) - want_field) > 1e-4
+        assert bad.mean() < 2e-3, (name, int(bad.sum()))
