@@ -90,83 +90,6 @@ bool ends_with(const std::string& s, const std::string& suffix) {
   return s.size() >= suffix.size() && s.compare(s.size() - suffix.size(), suffix.size(), suffix) == 0;
 }
 
-// An affine map p -> M p + b (3x3 row-major; a 2-D map keeps the third row and column identity).
-struct Map {
-  double M[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-  double b[3] = {0, 0, 0};
-};
-
-Map mul(const Map& second, const Map& first) {  // second(first(p))
-  Map r;
-  for (int i = 0; i < 3; ++i) {
-    r.b[i] = second.b[i];
-    for (int k = 0; k < 3; ++k) {
-      double s = 0.0;
-      for (int m = 0; m < 3; ++m) s += second.M[i * 3 + m] * first.M[m * 3 + k];
-      r.M[i * 3 + k] = s;
-      r.b[i] += second.M[i * 3 + k] * first.b[k];
-    }
-  }
-  return r;
-}
-
-bool inverse(const Map& a, Map& r) {
-  const double* m = a.M;
-  const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
-                     m[2] * (m[3] * m[7] - m[4] * m[6]);
-  double scale = 0.0;
-  for (int k = 0; k < 9; ++k) scale = std::max(scale, std::fabs(m[k]));
-  if (!(std::fabs(det) > 1e-12 * scale * scale * scale)) return false;
-  const double id = 1.0 / det;
-  r.M[0] = (m[4] * m[8] - m[5] * m[7]) * id;
-  r.M[1] = (m[2] * m[7] - m[1] * m[8]) * id;
-  r.M[2] = (m[1] * m[5] - m[2] * m[4]) * id;
-  r.M[3] = (m[5] * m[6] - m[3] * m[8]) * id;
-  r.M[4] = (m[0] * m[8] - m[2] * m[6]) * id;
-  r.M[5] = (m[2] * m[3] - m[0] * m[5]) * id;
-  r.M[6] = (m[3] * m[7] - m[4] * m[6]) * id;
-  r.M[7] = (m[1] * m[6] - m[0] * m[7]) * id;
-  r.M[8] = (m[0] * m[4] - m[1] * m[3]) * id;
-  for (int i = 0; i < 3; ++i) {
-    r.b[i] = 0.0;
-    for (int k = 0; k < 3; ++k) r.b[i] -= r.M[i * 3 + k] * a.b[k];
-  }
-  return true;
-}
-
-// T(p) = A (p - c) + t + c, or its inverse.
-Map map_of(const synx_linear& t, bool invert) {
-  Map m;
-  for (int k = 0; k < 9; ++k) m.M[k] = t.matrix[k];
-  if (t.dim == 2) {
-    m.M[2] = m.M[5] = m.M[6] = m.M[7] = 0.0;
-    m.M[8] = 1.0;
-  }
-  for (int i = 0; i < 3; ++i) {
-    m.b[i] = i < t.dim ? t.translation[i] + t.center[i] : 0.0;
-    for (int k = 0; k < t.dim; ++k) m.b[i] -= m.M[i * 3 + k] * t.center[k];
-  }
-  if (!invert) return m;
-  Map r;
-  if (!inverse(m, r)) throw std::runtime_error("a linear transform of the stack has a singular matrix, no inverse");
-  return r;
-}
-
-// The grid whose voxel i sits at L(p_i), p_i the voxel of g: direction M D, origin M o + b.
-synx_geom push_forward(const synx_geom& g, const Map& L) {
-  synx_geom r = g;
-  for (int i = 0; i < 3; ++i) {
-    r.origin[i] = L.b[i];
-    for (int k = 0; k < 3; ++k) {
-      r.origin[i] += L.M[i * 3 + k] * g.origin[k];
-      double s = 0.0;
-      for (int m = 0; m < 3; ++m) s += L.M[i * 3 + m] * g.direction[m * 3 + k];
-      r.direction[i * 3 + k] = s;
-    }
-  }
-  return r;
-}
-
 // One transform of the chain, in application order.
 struct ChainItem {
   std::string file;
@@ -247,22 +170,15 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     if (ends_with(lf, ".h5") || ends_with(lf, ".hdf5") || ends_with(lf, ".xfm"))
       throw std::runtime_error("transform '" + file + "': HDF5/composite transform files are not supported");
     if (ends_with(lf, ".mat") || ends_with(lf, ".txt")) {
-      const int n = synx_read_linear_transform(file.c_str(), dim, 0, nullptr);
-      if (n < 0) throw std::runtime_error(synx_last_error(nullptr));
-      std::vector<ChainItem> part;
-      for (int i = 0; i < n; ++i) {
+      for (const LinearItem& li : read_linear_file(file, dim, invert)) {
         ChainItem c;
         c.file = file;
         c.is_linear = true;
         c.invert = invert;
-        step_ok(synx_read_linear_transform(file.c_str(), dim, i, &c.linear) < 0 ? -1 : 0,
-                "synx_read_linear_transform");
-        c.map = map_of(c.linear, invert);
-        part.push_back(c);
+        c.linear = li.linear;
+        c.map = li.map;
+        chain.push_back(c);
       }
-      // a composite applies its last transform first; its inverse applies the first one's inverse first
-      if (!invert) std::reverse(part.begin(), part.end());
-      chain.insert(chain.end(), part.begin(), part.end());
       continue;
     }
     if (invert)

@@ -11,9 +11,16 @@
 //   -w/--winsorize-image-intensities [lower,upper]   -u/--use-histogram-matching 0
 //   -v/--verbose 0|1   --random-seed N (accepted, no effect: the stage is deterministic)
 //   --gpu N (device index; not a reference option)
+//   -r/--initial-moving-transform file | [file,useInverse] | identity  (repeatable; linear .mat/.txt
+//       files, the first given acting first; image-derived [fixed,moving,mode] is rejected)
+//   -z/--collapse-output-transforms 0|1 (default 1)   -a/--write-composite-transform 0
 // Output: prefix0Warp.nii.gz and prefix0InverseWarp.nii.gz (antsRegistrationTemplateHeader.cxx:74-90
-// names for SyN), plus the warped images when requested.  Other stages, metrics, masks and
-// initial transforms are rejected with EXIT_FAILURE.
+// names for SyN); with initial transforms, prefix0GenericAffine.mat (them, collapsed) and
+// prefix1Warp / prefix1InverseWarp, or without collapsing prefix<n>Warp after the n initial
+// transforms; plus the warped images when requested.  The initial transform is folded into the
+// moving image's geometry (an index <-> physical map the device functions take in general form),
+// which samples the moving image at Init(x + psi_M(x)) exactly.  Other stages, metrics, masks,
+// initial fixed transforms and HDF5 composite output are rejected with EXIT_FAILURE.
 #include "ants_registration.h"
 
 #include <cuda_runtime.h>
@@ -54,7 +61,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       {"-f", "shrink-factors"}, {"-s", "smoothing-sigmas"}, {"-o", "output"}, {"-v", "verbose"},
       {"-w", "winsorize-image-intensities"}, {"-u", "use-histogram-matching"}, {"-x", "masks"},
       {"-r", "initial-moving-transform"}, {"-q", "initial-fixed-transform"}, {"-n", "interpolation"},
-      {"-a", "collapse-output-transforms"}, {"-z", "collapse-output-transforms"}, {"-h", "help"}};
+      {"-a", "write-composite-transform"}, {"-z", "collapse-output-transforms"}, {"-h", "help"}};
   for (size_t i = 0; i < args.size(); ++i) {
     std::string k = args[i];
     std::string name;
@@ -72,10 +79,17 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     auto it = opt.find(n);
     return it == opt.end() ? def : it->second.back();
   };
-  for (const char* bad : {"masks", "initial-moving-transform", "initial-fixed-transform", "restore-state",
-                          "save-state", "write-composite-transform", "restrict-deformation"})
+  for (const char* bad : {"masks", "initial-fixed-transform", "restore-state", "save-state", "restrict-deformation"})
     if (opt.count(bad) && !(std::string(bad) == "masks" && opt[bad].back() == "[NULL,NULL]"))
       throw std::runtime_error(std::string("option --") + bad + " is not supported by this SyN+CC stage");
+  auto flag = [&](const std::string& n, bool def) {
+    if (!opt.count(n)) return def;
+    const std::string v = lower(one(n, ""));
+    return !(v == "0" || v == "false");
+  };
+  if (flag("write-composite-transform", false))
+    throw std::runtime_error("option --write-composite-transform 1 (HDF5 composite output) is not supported");
+  const bool collapse = flag("collapse-output-transforms", true);
   if (opt.count("use-histogram-matching") && (one("use-histogram-matching", "0") == "1" ||
                                               lower(one("use-histogram-matching", "0")) == "true"))
     throw std::runtime_error("--use-histogram-matching 1 is not supported");
@@ -85,6 +99,50 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const int dim = std::atoi(one("dimensionality", "3").c_str());
   if (dim != 2 && dim != 3) throw std::runtime_error("--dimensionality must be 2 or 3");
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
+
+  // initial moving transforms: linear files (or identity), in the order they act on a point (the
+  // first -r given first, as antsApplyTransforms orders -t); the moving image is sampled at
+  // Init(x + psi_M(x)), the composite ITK's SyN builds from the stored initial transforms and the
+  // moving half-field
+  std::vector<LinearItem> init;
+  for (const std::string& v : opt["initial-moving-transform"]) {
+    OptionCall r = parse_call(v);
+    if (r.params.size() > 2)
+      throw std::runtime_error("image-derived initial transforms (" + v +
+                               ") are not supported: pass the transform as a .mat/.txt file");
+    std::string file = r.name.empty() ? (r.params.empty() ? "" : r.params[0]) : r.name;
+    const bool invert = r.name.empty() && r.params.size() > 1 && (r.params[1] == "1" || lower(r.params[1]) == "true");
+    if (lower(file) == "identity") {
+      LinearItem li;
+      std::memset(&li.linear, 0, sizeof(li.linear));
+      li.linear.dim = dim;
+      li.linear.has_center = 1;  // the reference's identity is a MatrixOffsetTransformBase
+      li.linear.matrix[0] = li.linear.matrix[4] = li.linear.matrix[8] = 1.0;
+      init.push_back(li);
+      continue;
+    }
+    const std::string lf = lower(file);
+    const bool is_linear_file = lf.size() > 4 && (lf.compare(lf.size() - 4, 4, ".mat") == 0 ||
+                                                  lf.compare(lf.size() - 4, 4, ".txt") == 0);
+    if (!is_linear_file)
+      throw std::runtime_error("initial moving transform '" + file +
+                               "': only linear transform files (.mat/.txt) are supported");
+    for (const LinearItem& li : read_linear_file(file, dim, invert)) init.push_back(li);
+  }
+  Map init_map;
+  double init_center[3] = {0.0, 0.0, 0.0};
+  bool have_center = false;
+  for (const LinearItem& li : init) {
+    init_map = mul(li.map, init_map);
+    // collapsing keeps the center of the transform that acts first and has one
+    // (itkantsRegistrationHelper.hxx:3787-3798 scans the composite queue from its end)
+    if (!have_center && li.linear.has_center) {
+      for (int k = 0; k < 3; ++k) init_center[k] = li.linear.center[k];
+      have_center = true;
+    }
+  }
+  Map init_inverse;
+  if (!inverse(init_map, init_inverse)) throw std::runtime_error("the initial moving transform is singular");
   const int gpu = std::atoi(one("gpu", "0").c_str());
   if (opt["transform"].size() != 1 || opt["metric"].size() != 1)
     throw std::runtime_error("exactly one stage (one --transform and one --metric) is supported");
@@ -147,9 +205,15 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   nifti::Image moving = nifti::read(m.params[1]);
   if (fixed.components != 1 || moving.components != 1) throw std::runtime_error("scalar images expected");
   synx_geom gf = to_geom(fixed, dim), gm = to_geom(moving, dim);
+  // the initial transform folded into the moving image's geometry: its voxel i is placed at
+  // Init^-1(p_i), so sampling it at q reads the moving image at Init(q)
+  if (!init.empty()) gm = push_forward(gm, init_inverse);
   if (verbose) {
     out << "  Stage 0: SyN[" << p.learning_rate << "," << p.update_variance << "," << p.total_variance
         << "], CC[radius " << p.cc_radius << "], " << L << " levels on GPU " << gpu << std::endl;
+    if (!init.empty())
+      out << "  initial moving transform: " << init.size()
+          << " linear transform(s), folded into the moving image geometry" << std::endl;
   }
   synx_ctx* ctx = nullptr;
   if (synx_create(&p, gpu, nullptr, &ctx) != 0) throw std::runtime_error(std::string("synx_create: ") + synx_last_error(nullptr));
@@ -193,8 +257,21 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   std::vector<float> fwd((size_t)No * dim), inv((size_t)No * dim);
   if (synx_get_fields(ctx, fwd.data(), inv.data()) != 0)
     throw std::runtime_error(std::string("synx_get_fields: ") + synx_last_error(ctx));
-  nifti::write(prefix + "0Warp.nii.gz", field_image(go, fwd));
-  nifti::write(prefix + "0InverseWarp.nii.gz", field_image(go, inv));
+  // file names as antsRegistrationTemplateHeader.h:1436-1458 numbers them: with initial transforms
+  // and collapsing, prefix0GenericAffine.mat holds them and the SyN fields are transform 1; without
+  // collapsing the initial transforms are not rewritten and the SyN fields follow them
+  int warp_index = 0;
+  if (!init.empty()) {
+    warp_index = collapse ? 1 : (int)opt["initial-moving-transform"].size();
+    if (collapse) {
+      const synx_linear total = linear_of(init_map, dim, init_center);
+      if (synx_write_linear_transform((prefix + "0GenericAffine.mat").c_str(), &total) != 0)
+        throw std::runtime_error(std::string("synx_write_linear_transform: ") + synx_last_error(nullptr));
+    }
+  }
+  const std::string wi = std::to_string(warp_index);
+  nifti::write(prefix + wi + "Warp.nii.gz", field_image(go, fwd));
+  nifti::write(prefix + wi + "InverseWarp.nii.gz", field_image(go, inv));
   if (!warped.empty()) nifti::write(warped, like(fixed, warp_on_device(moving, gm, fwd, go)));
   if (!inv_warped.empty()) {
     std::vector<float> inv_on_moving = resample_on_device(inv, go, gm);

@@ -240,6 +240,7 @@ bool to_linear(const RawTransform& r, int dim, synx_linear& L, const std::string
   std::memset(&L, 0, sizeof(L));
   L.dim = dim;
   L.matrix[0] = L.matrix[4] = L.matrix[8] = 1.0;
+  L.has_center = (base == "TranslationTransform" || base == "IdentityTransform") ? 0 : 1;
   const int D = dim;
   const std::vector<double>& p = r.params;
   if (base == "AffineTransform" || base == "MatrixOffsetTransformBase") {
@@ -404,6 +405,62 @@ int synx_linear_field(const synx_linear* t, int invert, const synx_geom* g, floa
         for (int r = 0; r < D; ++r)
           field[(size_t)r * N + i] = (float)(u0[r] + E[r * 3] * i0 + E[r * 3 + 1] * i1 + E[r * 3 + 2] * i2);
       }
+  return SYNX_OK;
+}
+
+int synx_write_linear_transform(const char* path, const synx_linear* t) {
+  const char* fn = "synx_write_linear_transform: ";
+  if (!path || !t) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "null argument");
+  const int D = t->dim;
+  if (D != 2 && D != 3) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "dim must be 2 or 3");
+  const std::string p(path), ext = lower_ext(p);
+  if (ext != ".mat" && ext != ".txt")
+    return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "'" + p + "': write a .mat or .txt file");
+  std::vector<double> params, fixed;
+  for (int i = 0; i < D; ++i)
+    for (int j = 0; j < D; ++j) params.push_back(t->matrix[i * 3 + j]);
+  for (int k = 0; k < D; ++k) params.push_back(t->translation[k]);
+  for (int k = 0; k < D; ++k) fixed.push_back(t->center[k]);
+  const std::string type = "AffineTransform_double_" + std::to_string(D) + "_" + std::to_string(D);
+  std::ofstream f(p, std::ios::binary);
+  if (!f) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "cannot write '" + p + "'");
+  if (ext == ".mat") {
+    auto var = [&](const std::string& name, const std::vector<double>& v) {
+      // type 0: little-endian IEEE, column-wise, double, full numeric matrix; a column vector
+      const int32_t h[5] = {0, (int32_t)v.size(), 1, 0, (int32_t)name.size() + 1};
+      char hb[20];
+      for (int k = 0; k < 5; ++k) {
+        const uint32_t u = (uint32_t)h[k];
+        for (int b = 0; b < 4; ++b) hb[k * 4 + b] = (char)((u >> (8 * b)) & 0xff);
+      }
+      f.write(hb, 20);
+      f.write(name.c_str(), (std::streamsize)name.size() + 1);
+      for (double d : v) {
+        uint64_t u;
+        std::memcpy(&u, &d, 8);
+        char db[8];
+        for (int b = 0; b < 8; ++b) db[b] = (char)((u >> (8 * b)) & 0xff);
+        f.write(db, 8);
+      }
+    };
+    var(type, params);
+    var("fixed", fixed);
+  } else {
+    char buf[64];
+    auto line = [&](const char* key, const std::vector<double>& v) {
+      f << key;
+      for (double d : v) {
+        std::snprintf(buf, sizeof(buf), " %.17g", d);
+        f << buf;
+      }
+      f << "\n";
+    };
+    f << "#Insight Transform File V1.0\n#Transform 0\nTransform: " << type << "\n";
+    line("Parameters:", params);
+    line("FixedParameters:", fixed);
+  }
+  f.close();
+  if (!f) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "cannot write '" + p + "'");
   return SYNX_OK;
 }
 

@@ -45,7 +45,7 @@ class SynxLinear(C.Structure):
     """synx_linear: T(p) = A (p - c) + t + c on physical (LPS) points."""
     _fields_ = [
         ("dim", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("has_center", C.c_int32),
         ("matrix", C.c_double * 9),
         ("translation", C.c_double * 3),
         ("center", C.c_double * 3),
@@ -212,6 +212,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_server_get_stats": (I, [V, P(SynxServerStats)]),
         "synx_read_linear_transform": (I, [C.c_char_p, I, I, P(SynxLinear)]),
         "synx_linear_field": (I, [P(SynxLinear), I, P(SynxGeom), V]),
+        "synx_write_linear_transform": (I, [C.c_char_p, P(SynxLinear)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -678,6 +679,7 @@ class LinearTransform:
         t = SynxLinear()
         d = self.dim
         t.dim = d
+        t.has_center = 1
         m = np.eye(3)
         m[:d, :d] = self.matrix
         for k in range(9):
@@ -704,6 +706,13 @@ def read_linear_transform(path, dim: int, index: int = 0) -> LinearTransform:
         _check(rc)
     m = np.array(list(t.matrix), dtype=np.float64).reshape(3, 3)[:dim, :dim]
     return LinearTransform(m, np.array(list(t.translation)[:dim]), np.array(list(t.center)[:dim]))
+
+
+def write_linear_transform(path, t: LinearTransform) -> None:
+    """Write `t` as an ITK AffineTransform file (.mat MATLAB v4, as antsRegistration writes
+    prefix0GenericAffine.mat, or .txt Insight text)."""
+    tc = t.to_c()
+    _check(load_library().synx_write_linear_transform(os.fsencode(str(path)), C.byref(tc)))
 
 
 def linear_field(t: LinearTransform, g: Geom, invert: bool = False) -> np.ndarray:

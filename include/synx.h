@@ -311,7 +311,8 @@ int synx_shrink_geom(const synx_geom* in, int factor, synx_geom* out);
  * MatrixOffsetTransformBase applies to physical (LPS) points:  T(p) = A (p - c) + t + c.        */
 typedef struct synx_linear {
   int32_t dim;            /* 2 or 3 */
-  int32_t reserved0;
+  int32_t has_center;     /* 1 for the matrix-offset family (it has a center), 0 for Translation and
+                           * Identity transforms (c = 0); collapsing keeps the first center applied */
   double matrix[9];       /* A, row-major 3x3; a 2-D transform fills the leading 2x2 block */
   double translation[3];  /* t */
   double center[3];       /* c, the transform's fixed parameters */
@@ -335,6 +336,12 @@ int synx_read_linear_transform(const char* path, int dim, int index, synx_linear
  * or T^-1(p) - p with invert = 1 (SYNX_E_ARG when A is singular).  Double arithmetic, float
  * output. */
 int synx_linear_field(const synx_linear* transform, int invert, const synx_geom* grid, float* field_host);
+
+/* Writes `transform` as an ITK AffineTransform_double_<dim>_<dim> file: MATLAB v4 (.mat,
+ * little-endian double column vectors "AffineTransform_double_D_D" = A row-major then t, and
+ * "fixed" = c), the form antsRegistration writes prefix0GenericAffine.mat in, or Insight text
+ * (.txt).  SYNX_E_ARG for another extension or a file that cannot be written. */
+int synx_write_linear_transform(const char* path, const synx_linear* transform);
 
 #ifdef __cplusplus
 }

@@ -227,6 +227,41 @@ def test_linear_field_rejects_singular_inverse_and_bad_grids():
         synx.linear_field(t, Geom((4, 4)))
 
 
+@pytest.mark.parametrize("ext", [".mat", ".txt"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_write_round_trip(tmp_path, ext, dim):
+    if dim == 3:
+        t = LinearTransform(AFFINE3.reshape(3, 3), TRANS3, CENTER3)
+    else:
+        t = LinearTransform(np.array([[0.95, 0.1], [-0.07, 1.04]]), np.array([1.5, -2.0]), np.array([4.0, 6.0]))
+    p = tmp_path / f"w{ext}"
+    synx.write_linear_transform(p, t)
+    back = synx.read_linear_transform(p, dim)
+    np.testing.assert_array_equal(back.matrix, t.matrix)
+    np.testing.assert_array_equal(back.translation, t.translation)
+    np.testing.assert_array_equal(back.center, t.center)
+    if ext == ".mat":  # the bytes ITK's MATLAB writer lays down: this file's own writer agrees
+        q = tmp_path / "ref.mat"
+        write_mat(q, [(f"AffineTransform_double_{dim}_{dim}", np.r_[t.matrix.ravel(), t.translation]),
+                      ("fixed", t.center)])
+        assert p.read_bytes() == q.read_bytes()
+    else:
+        assert p.read_text().startswith("#Insight Transform File V1.0")
+
+
+def test_has_center_flags(tmp_path):
+    lib = synx.load_library()
+    for name, params, fixed, want in [("AffineTransform_double_3_3", np.r_[AFFINE3, TRANS3], CENTER3, 1),
+                                      ("Euler3DTransform_double_3_3", [0.1, 0.2, 0.3, 1, 2, 3], [0, 0, 0], 1),
+                                      ("TranslationTransform_double_3_3", [1, 2, 3], [], 0),
+                                      ("IdentityTransform_double_3_3", [], [], 0)]:
+        p = tmp_path / f"{name}.txt"
+        write_txt(p, [(name, params, fixed)])
+        t = synx.SynxLinear()
+        assert lib.synx_read_linear_transform(os.fsencode(str(p)), 3, 0, t) == 1
+        assert t.has_center == want, name
+
+
 @pytest.fixture(scope="module")
 def apply_exe():
     from ants_b200 import build

@@ -224,3 +224,51 @@ def test_stacks_match_the_scheme(exe, tmp_path, cuda, dim):
         c, _ = nifti.read(tmp_path / "c.nii.gz", dim)
         bad = np.abs(planes(c) - want_field) > 1e-4
         assert bad.mean() < 2e-3, (name, int(bad.sum()))
+
+
+@pytest.mark.gpu
+def test_registration_with_an_initial_moving_transform(exe, tmp_path, cuda):
+    """antsRegistration -r init.mat: the moving image is sampled at Init(x + psi_M(x)); the outputs are
+    numbered as the reference numbers them (0GenericAffine.mat, 1Warp, 1InverseWarp), and the warped
+    images agree with antsApplyTransforms through the standard stacks."""
+    from ants_b200 import synx
+    from ants_b200.synx import SyNParams
+    reg = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
+    size = (64, 60)
+    f, m = phantoms.pair_2d(size, seed=33)
+    g = Geom(size)
+    A = Affine([[1.02, 0.03], [-0.02, 0.99]], [0.8, -0.6], [32.0, 30.0])
+    A.write_mat(tmp_path / "init.mat")
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    p = str(tmp_path / "r_")
+    r = run(reg, ["-d", "2", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]", "-t", "SyN[0.2,3,0]",
+                  "-c", "[8x4,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-r", f"{tmp_path}/init.mat",
+                  "-o", f"[{p},{p}warped.nii.gz,{p}inverse_warped.nii.gz]"])
+    assert r.returncode == 0, r.stderr
+    assert os.path.exists(p + "1Warp.nii.gz") and os.path.exists(p + "1InverseWarp.nii.gz")
+    assert not os.path.exists(p + "0Warp.nii.gz")
+    back = synx.read_linear_transform(p + "0GenericAffine.mat", 2)
+    np.testing.assert_allclose(back.matrix, A.A, atol=1e-12)
+    np.testing.assert_allclose(back.center, A.c, atol=1e-12)
+    np.testing.assert_allclose(back.translation, A.t, atol=1e-9)
+    # the stage against the oracle with the initial transform folded into the moving geometry
+    P = SyNParams(dim=2, learning_rate=0.2, cc_radius=2, iterations=(8, 4), shrink_factors=(2, 1),
+                  smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12)
+    rf, ri, _, _ = O.syn_register(f, g, m, push_forward(g, A.inverse()), P)
+    fwd, _ = nifti.read(p + "1Warp.nii.gz", 2)
+    inv, _ = nifti.read(p + "1InverseWarp.nii.gz", 2)
+    for got, want in ((planes(fwd), rf), (planes(inv), ri)):
+        assert float(np.sqrt(((got - want) ** 2).sum(0).mean())) <= 0.05
+    assert float(np.sqrt((planes(fwd) ** 2).sum(0).mean())) > 0.02  # the stage did move
+    # the warped outputs through antsApplyTransforms' standard stacks
+    for ref_img, inp, ts, out in (("f", "m", [f"{p}1Warp.nii.gz", f"{p}0GenericAffine.mat"], "warped"),
+                                  ("m", "f", [f"[{p}0GenericAffine.mat,1]", f"{p}1InverseWarp.nii.gz"],
+                                   "inverse_warped")):
+        r = run(exe, ["-d", "2", "-i", f"{tmp_path}/{inp}.nii.gz", "-r", f"{tmp_path}/{ref_img}.nii.gz",
+                      "-t", ts[0], "-t", ts[1], "-o", f"{tmp_path}/aat_{out}.nii.gz"])
+        assert r.returncode == 0, r.stderr
+        a, _ = nifti.read(tmp_path / f"aat_{out}.nii.gz", 2)
+        b, _ = nifti.read(f"{p}{out}.nii.gz", 2)
+        bad = np.abs(a - b) > 1e-5
+        assert bad.mean() < 1e-3, (out, int(bad.sum()))
