@@ -11,15 +11,17 @@
 //   -w/--winsorize-image-intensities [lower,upper]   -u/--use-histogram-matching 0
 //   -v/--verbose 0|1   --random-seed N (accepted, no effect: the stage is deterministic)
 //   --gpu N (device index; not a reference option)
-//   -r/--initial-moving-transform file | [file,useInverse] | identity  (repeatable; linear .mat/.txt
-//       files, the first given acting first; image-derived [fixed,moving,mode] is rejected)
+//   -r/--initial-moving-transform file | [file,useInverse] | identity | [fixed,moving,feature]
+//       (repeatable, the first given acting first; linear .mat/.txt files, or the translation derived
+//       from two images: feature 0 geometric centers, 1 centers of mass, 2 origins)
 //   -z/--collapse-output-transforms 0|1 (default 1)   -a/--write-composite-transform 0
 // Output: prefix0Warp.nii.gz and prefix0InverseWarp.nii.gz (antsRegistrationTemplateHeader.cxx:74-90
 // names for SyN); with initial transforms, prefix0GenericAffine.mat (them, collapsed) and
 // prefix1Warp / prefix1InverseWarp, or without collapsing prefix<n>Warp after the n initial
 // transforms; plus the warped images when requested.  The initial transform is folded into the
 // moving image's geometry (an index <-> physical map the device functions take in general form),
-// which samples the moving image at Init(x + psi_M(x)) exactly.  Other stages, metrics, masks,
+// which samples the moving image at Init(x + psi_M(x)) exactly.  With -z 0, derived translations are
+// written as prefix<n>DerivedInitialMovingTranslation.mat.  Other stages, metrics, masks,
 // initial fixed transforms and HDF5 composite output are rejected with EXIT_FAILURE.
 #include "ants_registration.h"
 
@@ -36,6 +38,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cli_common.h"
@@ -105,11 +108,27 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   // Init(x + psi_M(x)), the composite ITK's SyN builds from the stored initial transforms and the
   // moving half-field
   std::vector<LinearItem> init;
-  for (const std::string& v : opt["initial-moving-transform"]) {
+  std::vector<std::pair<int, synx_linear>> derived;  // (stored option index, transform) of [fixed,moving,feature]
+  const int n_init = (int)opt["initial-moving-transform"].size();
+  for (int j = 0; j < n_init; ++j) {
+    const std::string& v = opt["initial-moving-transform"][j];
     OptionCall r = parse_call(v);
-    if (r.params.size() > 2)
-      throw std::runtime_error("image-derived initial transforms (" + v +
-                               ") are not supported: pass the transform as a .mat/.txt file");
+    if (r.params.size() > 2) {
+      // [fixed,moving,feature]: a translation derived from the two images (host arithmetic)
+      const int feature = std::atoi(r.params[2].c_str());
+      const nifti::Image a = nifti::read(r.params[0]);
+      const nifti::Image b = nifti::read(r.params[1]);
+      if (a.components != 1 || b.components != 1) throw std::runtime_error("scalar images expected in " + v);
+      const synx_geom ga = to_geom(a, dim), gb = to_geom(b, dim);
+      LinearItem li;
+      if (synx_initial_translation(a.data.data(), &ga, b.data.data(), &gb, feature, &li.linear) != 0)
+        throw std::runtime_error(std::string("synx_initial_translation: ") + synx_last_error(nullptr));
+      li.map = map_of(li.linear, false);
+      init.push_back(li);
+      // the reference stores repeated options newest first and names the file by that index
+      derived.emplace_back(n_init - 1 - j, li.linear);
+      continue;
+    }
     std::string file = r.name.empty() ? (r.params.empty() ? "" : r.params[0]) : r.name;
     const bool invert = r.name.empty() && r.params.size() > 1 && (r.params[1] == "1" || lower(r.params[1]) == "true");
     if (lower(file) == "identity") {
@@ -262,11 +281,18 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   // collapsing the initial transforms are not rewritten and the SyN fields follow them
   int warp_index = 0;
   if (!init.empty()) {
-    warp_index = collapse ? 1 : (int)opt["initial-moving-transform"].size();
+    warp_index = collapse ? 1 : n_init;
     if (collapse) {
       const synx_linear total = linear_of(init_map, dim, init_center);
       if (synx_write_linear_transform((prefix + "0GenericAffine.mat").c_str(), &total) != 0)
         throw std::runtime_error(std::string("synx_write_linear_transform: ") + synx_last_error(nullptr));
+    } else {
+      // derived initial transforms are written out when they are not collapsed (:229-250)
+      for (const auto& d : derived) {
+        const std::string name = prefix + std::to_string(d.first) + "DerivedInitialMovingTranslation.mat";
+        if (synx_write_linear_transform(name.c_str(), &d.second) != 0)
+          throw std::runtime_error(std::string("synx_write_linear_transform: ") + synx_last_error(nullptr));
+      }
     }
   }
   const std::string wi = std::to_string(warp_index);

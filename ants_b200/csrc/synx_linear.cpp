@@ -408,6 +408,67 @@ int synx_linear_field(const synx_linear* t, int invert, const synx_geom* g, floa
   return SYNX_OK;
 }
 
+int synx_initial_translation(const float* F, const synx_geom* gf, const float* M, const synx_geom* gm, int feature,
+                             synx_linear* out) {
+  const char* fn = "synx_initial_translation: ";
+  if (!gf || !gm || !out) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "null argument");
+  const int D = gf->dim;
+  if ((D != 2 && D != 3) || gm->dim != D)
+    return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "the images' dimensions differ or are not 2 or 3");
+  if (feature < 0 || feature > 2)
+    return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "feature must be 0 (centers), 1 (centers of mass) "
+                                                                "or 2 (origins)");
+  if (feature == 1 && (!F || !M)) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "images are needed");
+  // physical point of continuous index idx: origin + Dir diag(spacing) idx
+  auto point = [D](const synx_geom* g, const double idx[3], double p[3]) {
+    for (int r = 0; r < 3; ++r) {
+      p[r] = r < D ? g->origin[r] : 0.0;
+      if (r < D)
+        for (int c = 0; c < D; ++c) p[r] += g->direction[r * 3 + c] * g->spacing[c] * idx[c];
+    }
+  };
+  double cf[3] = {0, 0, 0}, cm[3] = {0, 0, 0};
+  for (int k = 0; k < 2; ++k) {
+    const synx_geom* g = k ? gm : gf;
+    double* c = k ? cm : cf;
+    if (feature == 2) {
+      for (int r = 0; r < D; ++r) c[r] = g->origin[r];
+    } else if (feature == 0) {
+      double idx[3] = {0, 0, 0};
+      for (int r = 0; r < D; ++r) idx[r] = (double)(g->size[r] - 1) / 2.0;
+      point(g, idx, c);
+    } else {
+      const float* img = k ? M : F;
+      const int64_t nx = g->size[0], ny = g->size[1], nz = D == 3 ? g->size[2] : 1;
+      double m0 = 0.0, m1[3] = {0, 0, 0};
+      size_t i = 0;
+      for (int64_t z = 0; z < nz; ++z)
+        for (int64_t y = 0; y < ny; ++y)
+          for (int64_t x = 0; x < nx; ++x, ++i) {
+            const double v = img[i];
+            const double idx[3] = {(double)x, (double)y, (double)z};
+            double p[3];
+            point(g, idx, p);
+            m0 += v;
+            for (int r = 0; r < D; ++r) m1[r] += v * p[r];
+          }
+      if (m0 == 0.0)
+        return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "the total mass of the " +
+                                                      (k ? "moving" : "fixed") + " image is zero");
+      for (int r = 0; r < D; ++r) c[r] = m1[r] / m0;
+    }
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->dim = D;
+  out->has_center = 1;
+  out->matrix[0] = out->matrix[4] = out->matrix[8] = 1.0;
+  for (int r = 0; r < D; ++r) {
+    out->center[r] = cf[r];
+    out->translation[r] = cm[r] - cf[r];
+  }
+  return SYNX_OK;
+}
+
 int synx_write_linear_transform(const char* path, const synx_linear* t) {
   const char* fn = "synx_write_linear_transform: ";
   if (!path || !t) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "null argument");

@@ -213,6 +213,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_read_linear_transform": (I, [C.c_char_p, I, I, P(SynxLinear)]),
         "synx_linear_field": (I, [P(SynxLinear), I, P(SynxGeom), V]),
         "synx_write_linear_transform": (I, [C.c_char_p, P(SynxLinear)]),
+        "synx_initial_translation": (I, [V, P(SynxGeom), V, P(SynxGeom), I, P(SynxLinear)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -706,6 +707,19 @@ def read_linear_transform(path, dim: int, index: int = 0) -> LinearTransform:
         _check(rc)
     m = np.array(list(t.matrix), dtype=np.float64).reshape(3, 3)[:dim, :dim]
     return LinearTransform(m, np.array(list(t.translation)[:dim]), np.array(list(t.center)[:dim]))
+
+
+def initial_translation(fixed, gf: Geom, moving, gm: Geom, feature: int) -> LinearTransform:
+    """The translation antsRegistration derives for -r [fixed,moving,feature]: 0 geometric centers,
+    1 centers of intensity mass, 2 origins (center = the fixed image's feature point)."""
+    a, b = gf.to_c(), gm.to_c()
+    F = None if fixed is None else np.ascontiguousarray(fixed, dtype=np.float32)
+    M = None if moving is None else np.ascontiguousarray(moving, dtype=np.float32)
+    t = SynxLinear()
+    _check(load_library().synx_initial_translation(None if F is None else _ptr(F), C.byref(a),
+                                                   None if M is None else _ptr(M), C.byref(b), feature, C.byref(t)))
+    d = gf.dim
+    return LinearTransform(np.eye(d), np.array(list(t.translation)[:d]), np.array(list(t.center)[:d]))
 
 
 def write_linear_transform(path, t: LinearTransform) -> None:

@@ -337,6 +337,16 @@ int synx_read_linear_transform(const char* path, int dim, int index, synx_linear
  * output. */
 int synx_linear_field(const synx_linear* transform, int invert, const synx_geom* grid, float* field_host);
 
+/* The translation antsRegistration derives from a pair of images for -r [fixed,moving,feature]
+ * (Examples/itkantsRegistrationHelper.h:1297-1360; ITK's CenteredTransformInitializer for 0 and 1):
+ * a rigid transform with identity rotation, center c_F and translation c_M - c_F, where c is per
+ * image 0: the geometric center (the physical point of continuous index (size-1)/2), 1: the center
+ * of intensity mass (sum of value * physical point over sum of value, raw intensities), 2: the
+ * origin.  Images are host memory (x fastest) and may be NULL for features 0 and 2.  SYNX_E_ARG for
+ * a zero total mass.  Host arithmetic in double. */
+int synx_initial_translation(const float* fixed_host, const synx_geom* fixed_geom, const float* moving_host,
+                             const synx_geom* moving_geom, int feature, synx_linear* out);
+
 /* Writes `transform` as an ITK AffineTransform_double_<dim>_<dim> file: MATLAB v4 (.mat,
  * little-endian double column vectors "AffineTransform_double_D_D" = A row-major then t, and
  * "fixed" = c), the form antsRegistration writes prefix0GenericAffine.mat in, or Insight text

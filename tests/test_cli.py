@@ -52,7 +52,7 @@ def test_nifti_roundtrip_scalar_and_vector(tmp_path):
     (["-d", "3", "-m", "CC[/nonexistent/f.nii.gz,/nonexistent/m.nii.gz,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10",
       "-f", "1", "-s", "0", "-o", "x"], "cannot open"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
-      "-r", "[f.nii.gz,m.nii.gz,1]"], "image-derived initial transforms"),
+      "-r", "[/nonexistent/f.nii.gz,/nonexistent/m.nii.gz,1]"], "cannot open"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
       "-r", "w.nii.gz"], "only linear transform files"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",

@@ -262,6 +262,48 @@ def test_has_center_flags(tmp_path):
         assert t.has_center == want, name
 
 
+@pytest.mark.parametrize("dim", [2, 3])
+def test_initial_translation_features(dim):
+    rng = np.random.default_rng(dim)
+    if dim == 3:
+        gf = Geom((17, 13, 11), (1.2, 0.9, 1.5), (-5.0, 3.0, 2.0), Rotation.from_euler("xyz", [0.2, -0.1, 0.3]).as_matrix())
+        gm = Geom((15, 16, 12), (1.0, 1.1, 1.3), (2.0, -1.0, 4.0), Rotation.from_euler("zyx", [0.1, 0.2, -0.1]).as_matrix())
+    else:
+        gf = Geom((23, 19), (1.1, 0.8), (2.0, -1.0), np.array([[np.cos(0.3), -np.sin(0.3)], [np.sin(0.3), np.cos(0.3)]]))
+        gm = Geom((21, 25), (0.9, 1.0), (-3.0, 4.0))
+    F = rng.uniform(0, 1, gf.shape).astype(np.float32)
+    M = rng.uniform(0, 2, gm.shape).astype(np.float32)
+
+    def centers(g, img, feature):
+        if feature == 2:
+            return np.asarray(g.origin)
+        P = physical_points(g).reshape(-1, dim)
+        if feature == 0:
+            return np.asarray(g.origin) + g.direction @ (np.asarray(g.spacing) * (np.asarray(g.size) - 1) / 2)
+        w = img.astype(np.float64).ravel()
+        return (P * w[:, None]).sum(0) / w.sum()
+
+    for feature in (0, 1, 2):
+        t = synx.initial_translation(F, gf, M, gm, feature)
+        cf, cm = centers(gf, F, feature), centers(gm, M, feature)
+        np.testing.assert_array_equal(t.matrix, np.eye(dim))
+        np.testing.assert_allclose(t.center, cf, atol=1e-9)
+        np.testing.assert_allclose(t.translation, cm - cf, atol=1e-9)
+    # features 0 and 2 need no intensities
+    t = synx.initial_translation(None, gf, None, gm, 0)
+    np.testing.assert_allclose(t.translation, centers(gm, M, 0) - centers(gf, F, 0), atol=1e-9)
+
+
+def test_initial_translation_errors():
+    g = Geom((8, 8))
+    with pytest.raises(SynxError, match="total mass"):
+        synx.initial_translation(np.zeros(g.shape, np.float32), g, np.ones(g.shape, np.float32), g, 1)
+    with pytest.raises(SynxError, match="feature must be"):
+        synx.initial_translation(None, g, None, g, 3)
+    with pytest.raises(SynxError, match="dimensions differ"):
+        synx.initial_translation(None, g, None, Geom((8, 8, 8)), 0)
+
+
 @pytest.fixture(scope="module")
 def apply_exe():
     from ants_b200 import build
@@ -276,3 +318,16 @@ def test_cli_rejects_unreadable_transforms(apply_exe, tmp_path, tname, needle):
                         str(tmp_path / tname)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 1
     assert needle in r.stderr
+
+
+def test_registration_cli_rejects_a_bad_feature(tmp_path):
+    from ants_b200 import build, nifti
+    build.build_all()
+    reg = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
+    g = Geom((8, 8))
+    nifti.write(tmp_path / "a.nii.gz", np.ones(g.shape, np.float32), g)
+    r = subprocess.run([reg, "-d", "2", "-m", f"CC[{tmp_path}/a.nii.gz,{tmp_path}/a.nii.gz,1,2]", "-t", "SyN[0.1,3,0]",
+                        "-c", "2", "-f", "1", "-s", "0", "-o", str(tmp_path / "x"),
+                        "-r", f"[{tmp_path}/a.nii.gz,{tmp_path}/a.nii.gz,3]"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    assert "feature must be" in r.stderr

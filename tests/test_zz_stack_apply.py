@@ -272,3 +272,36 @@ def test_registration_with_an_initial_moving_transform(exe, tmp_path, cuda):
         b, _ = nifti.read(f"{p}{out}.nii.gz", 2)
         bad = np.abs(a - b) > 1e-5
         assert bad.mean() < 1e-3, (out, int(bad.sum()))
+
+
+@pytest.mark.gpu
+def test_registration_with_a_derived_initial_translation(tmp_path, cuda):
+    """antsRegistration -r [fixed,moving,1]: the translation between the centers of intensity mass,
+    folded into the moving geometry; collapsed into 0GenericAffine.mat, or with -z 0 written as
+    0DerivedInitialMovingTranslation.mat, the SyN fields numbered 1 either way."""
+    from ants_b200 import synx
+    from ants_b200.synx import SyNParams
+    reg = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
+    size = (64, 60)
+    f, m = phantoms.pair_2d(size, seed=35)
+    g, gm = Geom(size), Geom(size, (1.0, 1.0), (1.5, -2.0))  # the moving image is shifted in space
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, gm)
+    t = synx.initial_translation(f, g, m, gm, 1)
+    L = Affine(np.eye(2), t.translation, t.center)
+    P = SyNParams(dim=2, learning_rate=0.2, cc_radius=2, iterations=(8, 4), shrink_factors=(2, 1),
+                  smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12)
+    rf, _, _, _ = O.syn_register(f, g, m, push_forward(gm, L.inverse()), P)
+    for z, names in (("1", ["0GenericAffine.mat"]), ("0", ["0DerivedInitialMovingTranslation.mat"])):
+        p = str(tmp_path / f"z{z}_")
+        r = run(reg, ["-d", "2", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]", "-t", "SyN[0.2,3,0]",
+                      "-c", "[8x4,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-z", z,
+                      "-r", f"[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1]", "-o", p])
+        assert r.returncode == 0, r.stderr
+        for n in names + ["1Warp.nii.gz", "1InverseWarp.nii.gz"]:
+            assert os.path.exists(p + n), n
+        back = synx.read_linear_transform(p + names[0], 2)
+        np.testing.assert_allclose(back.translation, t.translation, atol=1e-9)
+        np.testing.assert_allclose(back.center, t.center, atol=1e-9)
+        fwd, _ = nifti.read(p + "1Warp.nii.gz", 2)
+        assert float(np.sqrt(((planes(fwd) - rf) ** 2).sum(0).mean())) <= 0.05
