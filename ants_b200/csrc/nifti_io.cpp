@@ -130,6 +130,7 @@ Image read(const std::string& path) {
   img.components = (int)(n[4]);
   img.dim = (n[2] > 1) ? 3 : 2;
   if (n[3] != 1) throw std::runtime_error(path + ": time series are not supported");
+  if (n[5] != 1 || n[6] != 1) throw std::runtime_error(path + ": dimensions 6 and 7 are not supported");
   for (int k = 0; k < 3; ++k) img.spacing[k] = h.pixdim[k + 1] > 0 ? h.pixdim[k + 1] : 1.0;
   // RAS affine
   double A[3][4];
@@ -170,14 +171,29 @@ Image read(const std::string& path) {
     if (nrm <= 0) nrm = 1.0;
     for (int rr = 0; rr < 3; ++rr) img.direction[rr * 3 + c] = A[rr][c] / nrm;
   }
-  // payload
+  // payload: the element size comes from the datatype (bitpix must agree), and the data are read in
+  // bounded chunks, so a header that claims more data than the file holds fails on the short read
+  // instead of allocating what it claims
+  int bytes = 0;
+  switch (h.datatype) {
+    case 2: case 256: bytes = 1; break;
+    case 4: case 512: bytes = 2; break;
+    case 8: case 16: case 768: bytes = 4; break;
+    case 64: bytes = 8; break;
+    default: throw std::runtime_error(path + ": unsupported NIfTI datatype " + std::to_string(h.datatype));
+  }
+  if (h.bitpix != 8 * bytes) throw std::runtime_error(path + ": bitpix does not match the datatype");
   const long long count = img.voxels() * img.components;
+  if (!(h.vox_offset < (float)(1 << 26))) throw std::runtime_error(path + ": vox_offset out of range");
   const size_t off = (size_t)(h.vox_offset > 352 ? h.vox_offset : 352);
   std::vector<unsigned char> skip(off - sizeof(h));
   if (!skip.empty()) r.read(skip.data(), skip.size(), path);
-  const int bytes = h.bitpix / 8;
-  std::vector<unsigned char> raw((size_t)count * bytes);
-  r.read(raw.data(), raw.size(), path);
+  const size_t total = (size_t)count * (size_t)bytes, chunk = (size_t)1 << 26;
+  std::vector<unsigned char> raw;
+  for (size_t done = 0; done < total; done += std::min(chunk, total - done)) {
+    raw.resize(done + std::min(chunk, total - done));
+    r.read(raw.data() + done, raw.size() - done, path);
+  }
   img.data.resize((size_t)count);
   auto conv = [&](auto tag) {
     using T = decltype(tag);

@@ -78,3 +78,21 @@ def test_reproduces_the_registration_output(exe, tmp_path, cuda):
     a, _ = nifti.read(tmp_path / "aat.nii.gz", 2)
     b, _ = nifti.read(p + "warped.nii.gz", 2)
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("patch,needle", [
+    ({40: [3, 3000, 3000, 3000]}, "short read"),        # dim[]: claims 2.7e10 voxels in a small file
+    ({72: [8]}, "bitpix does not match"),                 # bitpix 8 with a float32 datatype
+    ({40: [7, 4, 4, 3, 1, 1, 2, 1]}, "dimensions 6 and 7"),
+])
+def test_corrupt_headers_fail_cleanly(exe, tmp_path, patch, needle):
+    # a NIfTI-1 header is read field by field: dim (int16[8]) at byte 40, bitpix (int16) at byte 72
+    g = Geom((5, 4, 3))
+    nifti.write(tmp_path / "ok.nii", np.ones(g.shape, np.float32), g)
+    raw = bytearray((tmp_path / "ok.nii").read_bytes())
+    for off, vals in patch.items():
+        raw[off:off + 2 * len(vals)] = np.asarray(vals, "<i2").tobytes()
+    (tmp_path / "bad.nii").write_bytes(bytes(raw))
+    r = run(exe, ["-d", "3", "-i", f"{tmp_path}/ok.nii", "-r", f"{tmp_path}/bad.nii", "-o", f"{tmp_path}/o.nii.gz"])
+    assert r.returncode == 1
+    assert needle in r.stderr
