@@ -485,8 +485,12 @@ class SyNStage:
     def _ck(self, rc):
         _check(rc, self.h)
 
-    def set_images(self, fixed, fixed_geom: Geom, moving, moving_geom: Geom) -> None:
-        """Host numpy float32 arrays (copied host->device) or CUDA tensors (device->device)."""
+    def set_images(self, fixed, fixed_geom: Geom, moving, moving_geom: Geom, moving_initial=None) -> None:
+        """Host numpy float32 arrays (copied host->device) or CUDA tensors (device->device).
+        `moving_initial`: a LinearTransform or a list of them (first applied first), the
+        antsRegistration -r initial moving transform; it is folded into the moving geometry."""
+        if moving_initial is not None:
+            moving_geom = fold_moving_geometry(moving_geom, moving_initial)
         gf, gm = fixed_geom.to_c(), moving_geom.to_c()
         if isinstance(fixed, np.ndarray):
             f = np.ascontiguousarray(fixed, dtype=np.float32)
@@ -689,6 +693,23 @@ class LinearTransform:
             t.translation[k] = float(self.translation[k])
             t.center[k] = float(self.center[k])
         return t
+
+
+def fold_moving_geometry(g: Geom, transforms) -> Geom:
+    """The moving image's geometry with initial linear transforms folded in: voxel i is placed at
+    Init^-1(p_i), so sampling the result at q reads the image at Init(q).  `transforms` is one
+    LinearTransform or a list applied first to last (Init = T_n o ... o T_1), the composite ITK's SyN
+    samples the moving image through (Init(x + psi_M(x)))."""
+    if isinstance(transforms, LinearTransform):
+        transforms = [transforms]
+    d = g.dim
+    M, b = np.eye(d), np.zeros(d)
+    for t in transforms:
+        A = np.asarray(t.matrix, float)
+        tb = np.asarray(t.translation, float) + np.asarray(t.center, float) - A @ np.asarray(t.center, float)
+        M, b = A @ M, A @ b + tb
+    Mi = np.linalg.inv(M)
+    return Geom(g.size, g.spacing, tuple(Mi @ np.asarray(g.origin) - Mi @ b), Mi @ g.direction)
 
 
 def count_linear_transforms(path, dim: int) -> int:

@@ -331,3 +331,20 @@ def test_registration_cli_rejects_a_bad_feature(tmp_path):
                         "-r", f"[{tmp_path}/a.nii.gz,{tmp_path}/a.nii.gz,3]"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 1
     assert "feature must be" in r.stderr
+
+
+def test_fold_moving_geometry_reads_the_image_at_init():
+    """Index of q in the folded geometry == index of Init(q) in the original (two transforms, first
+    applied first)."""
+    g = Geom((9, 8, 7), (1.1, 0.9, 1.2), (3.0, -2.0, 1.0), Rotation.from_euler("xyz", [0.1, 0.2, -0.1]).as_matrix())
+    T1 = LinearTransform(AFFINE3.reshape(3, 3), TRANS3, CENTER3)
+    T2 = LinearTransform(Rotation.from_euler("z", 0.3).as_matrix(), np.array([1.0, 0.5, -2.0]), np.array([4.0, 4.0, 4.0]))
+    gf = synx.fold_moving_geometry(g, [T1, T2])
+
+    def index_of(geom, q):
+        return np.linalg.solve(geom.direction * np.asarray(geom.spacing), q - np.asarray(geom.origin))
+
+    rng = np.random.default_rng(5)
+    for q in rng.uniform(-10, 20, (10, 3)):
+        init_q = apply(T2, apply(T1, q))
+        np.testing.assert_allclose(index_of(gf, q), index_of(g, init_q), atol=1e-9)
