@@ -76,6 +76,43 @@ def test_cc_identical_images_is_minus_one():
     assert np.abs(gF).max() < 1e-5 and np.abs(gM).max() < 1e-5
 
 
+def _bruteforce():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.cc_bruteforce
+
+
+@pytest.mark.parametrize("case", ["constant_fixed", "constant_moving", "half_flat", "radius_beyond_every_axis"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cc_edge_cases_match_bruteforce(case, dtype):
+    rng = np.random.default_rng(11)
+    shape, r, sp = (5, 6, 7), 2, (1.0, 1.2, 0.8)
+    F = rng.uniform(0, 1, shape).astype(np.float32)
+    M = rng.uniform(0, 1, shape).astype(np.float32)
+    if case == "constant_fixed":
+        F[:] = 0.5
+    elif case == "constant_moving":
+        M[:] = 2.0
+    elif case == "half_flat":
+        F[:, :, :3] = 0.25  # the variance guard holds on the flat side only
+    else:
+        shape, r = (3, 4, 5), 6
+        F, M = F[:3, :4, :5].copy(), M[:3, :4, :5].copy()
+    g = Geom(tuple(reversed(F.shape)), sp)
+    v, gF, gM, cc = O.cc_metric(F, M, g, r, dtype=dtype)
+    bv, bgF, bgM, bcc = _bruteforce()(F, M, r, sp)
+    tol = 1e-12 if dtype == np.float64 else 2e-6
+    assert abs(v - bv) < max(tol, 1e-12)
+    np.testing.assert_allclose(cc, bcc, atol=tol * 10)
+    scale = max(np.abs(bgF).max(), np.abs(bgM).max(), 1e-30)
+    np.testing.assert_allclose(gF, bgF, atol=tol * scale * 10, rtol=0)
+    np.testing.assert_allclose(gM, bgM, atol=tol * scale * 10, rtol=0)
+    if case.startswith("constant"):
+        assert v == -1.0 and not np.any(gF) and not np.any(gM)
+
+
 # ---- warp / compose / invert / resample -----------------------------------------------------------
 def test_warp_identity_and_integer_shift():
     rng = np.random.default_rng(4)
