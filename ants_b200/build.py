@@ -30,7 +30,7 @@ APPLY_CLI = os.path.join(HERE, "antsApplyTransforms_b200")
 LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu", "synx_server.cpp",
                "synx_linear.cpp"]
 LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh", "synx_phases.cuh", "synx_cc_tile.cuh", "synx_level.cuh",
-               "synx_level_body.cuh", "synx_host.h"]
+               "synx_level_body.cuh", "synx_host.h", "synx_nvtx.h"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
 APPLY_SOURCES = ["ants_apply_transforms.cpp", "nifti_io.cpp"]
 CLI_HEADERS = ["nifti_io.h", "ants_registration.h", "ants_apply_transforms.h", "cli_common.h"]

@@ -17,6 +17,7 @@
 
 #include "../../include/synx.h"
 #include "synx_host.h"
+#include "synx_nvtx.h"
 #include "synx_kernels.cuh"
 #include "synx_level.cuh"
 
@@ -748,6 +749,7 @@ LevelArgs make_level_args(synx_ctx* c, const GridInfo& g, int iters) {
 // Level set-up, enqueued on c->stream: pyramid smoothing of both images, resampling (or zeroing)
 // of the four half-fields, reset of the control block.
 int level_begin(synx_ctx* c, int level) {
+  synx::NvtxRange range("synx level setup", level);
   if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_run_level: images not set");
   if (level != c->cur_level + 1 || level >= c->P.n_levels)
     return set_err(c, SYNX_E_STATE, "synx_run_level: levels must run in order 0.." + std::to_string(c->P.n_levels - 1));
@@ -789,6 +791,7 @@ int level_begin(synx_ctx* c, int level) {
 // The level's iterations, enqueued on c->stream: the level kernel, graph replay of one iteration,
 // or plain launches.
 int level_iterate(synx_ctx* c, int level) {
+  synx::NvtxRange range("synx level iterate", level);
   const GridInfo& gl = c->lv[level];
   const int D = c->D;
   const int iters = c->P.iterations[level];
@@ -849,6 +852,7 @@ int level_iterate(synx_ctx* c, int level) {
 
 // Enqueue the read-back of the level's control block and log (host staging in the context).
 int level_readback(synx_ctx* c, int level) {
+  synx::NvtxRange range("synx level readback", level);
   const int iters = c->P.iterations[level];
   CUDA_TRY(c, cudaEventRecord(c->lev_ev[2], c->stream));
   CUDA_TRY(c, cudaGetLastError());
@@ -1012,6 +1016,7 @@ struct StreamSwap {
 // kernel serves share cooperative launches (one per dimension and CC radius); the others run
 // their own per-kernel path on the same stream.  One host synchronisation for the whole step.
 int batch_step(synx_batch* b, synx_ctx* const* cs, int n, cudaStream_t s, int* advanced) {
+  synx::NvtxRange range("synx batch step", n);
   if (advanced) *advanced = 0;
   if (!b || (n > 0 && !cs) || n < 0) return batch_err(b, SYNX_E_ARG, "synx_batch_step: bad arguments");
   std::vector<synx_ctx*> act;
