@@ -326,7 +326,8 @@ int allocate(synx_ctx* c) {
     // reuse
   } else {
     free_arena(c);
-    cudaError_t e = cudaMalloc((void**)&c->arena, sz);
+    cudaError_t e = c->P.test_inject == SYNX_INJECT_ALLOC_FAILURE ? cudaErrorMemoryAllocation
+                                                                 : cudaMalloc((void**)&c->arena, sz);
     if (e != cudaSuccess) {
       c->arena = nullptr;
       cudaGetLastError();
@@ -1197,7 +1198,7 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     return set_err(nullptr, SYNX_E_ARG, "synx_create: inverse iteration cap must be in 1..1000");
   if (p.update_variance < 0 || p.total_variance < 0)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: negative smoothing variance");
-  if (p.test_inject != 0 && p.test_inject != SYNX_INJECT_BARRIER_TIMEOUT)
+  if (p.test_inject != 0 && p.test_inject != SYNX_INJECT_BARRIER_TIMEOUT && p.test_inject != SYNX_INJECT_ALLOC_FAILURE)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: unknown test_inject value");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

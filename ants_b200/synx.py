@@ -26,6 +26,7 @@ SYNX_F_NO_PERSISTENT = 0x4
 SYNX_F_CC_FP32_SUMS = 0x8
 SYNX_F_FIELDS_FP16 = 0x10
 SYNX_INJECT_BARRIER_TIMEOUT = 1
+SYNX_INJECT_ALLOC_FAILURE = 2
 
 ERRORS = {-1: "invalid argument", -2: "bad state", -3: "CUDA error", -4: "out of device memory", -5: "unsupported"}
 

@@ -99,6 +99,10 @@ typedef struct synx_params {
  * and synx_run / synx_run_level return SYNX_E_CUDA with a barrier-timeout message.  The context
  * and the GPU stay usable. */
 #define SYNX_INJECT_BARRIER_TIMEOUT 1
+/* The context's device arena allocation reports failure without calling the device allocator, so
+ * synx_set_images returns SYNX_E_NOMEM as it would when the GPU is out of memory; the context can
+ * still be destroyed and other contexts are unaffected. */
+#define SYNX_INJECT_ALLOC_FAILURE 2
 
 /* Fill *p with antsRegistration's defaults for a SyN stage of dimension dim
  * (SyN[0.1,3,0], CC radius 4, one level, 1 iteration, shrink 1, sigma 0 vox). */
