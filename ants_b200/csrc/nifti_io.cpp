@@ -171,9 +171,9 @@ Image read(const std::string& path) {
     if (nrm <= 0) nrm = 1.0;
     for (int rr = 0; rr < 3; ++rr) img.direction[rr * 3 + c] = A[rr][c] / nrm;
   }
-  // payload: the element size comes from the datatype (bitpix must agree), and the data are read in
-  // bounded chunks, so a header that claims more data than the file holds fails on the short read
-  // instead of allocating what it claims
+  // payload: the element size comes from the datatype, as niftilib takes it (bitpix is not used), and
+  // the data are read in bounded chunks, so a header that claims more data than the file holds fails
+  // on the short read instead of allocating what it claims
   int bytes = 0;
   switch (h.datatype) {
     case 2: case 256: bytes = 1; break;
@@ -182,7 +182,6 @@ Image read(const std::string& path) {
     case 64: bytes = 8; break;
     default: throw std::runtime_error(path + ": unsupported NIfTI datatype " + std::to_string(h.datatype));
   }
-  if (h.bitpix != 8 * bytes) throw std::runtime_error(path + ": bitpix does not match the datatype");
   const long long count = img.voxels() * img.components;
   if (!(h.vox_offset < (float)(1 << 26))) throw std::runtime_error(path + ": vox_offset out of range");
   const size_t off = (size_t)(h.vox_offset > 352 ? h.vox_offset : 352);
