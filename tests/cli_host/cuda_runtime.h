@@ -1,0 +1,16 @@
+// Test infrastructure: host definitions of the few CUDA runtime calls the command lines make
+// (cudaMalloc/Free/Memcpy/Memset/SetDevice), so that tests/test_cli_host_plumbing.py can build
+// the command lines on a machine without a GPU.  Never part of the product.
+#pragma once
+#include <cstdlib>
+#include <cstring>
+typedef int cudaError_t;
+enum { cudaSuccess = 0, cudaErrorMemoryAllocation = 2 };
+enum cudaMemcpyKind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice, cudaMemcpyDefault };
+inline cudaError_t cudaMalloc(void** p, size_t n) { *p = std::malloc(n ? n : 1); return *p ? 0 : 2; }
+template <class T> inline cudaError_t cudaMalloc(T** p, size_t n) { return cudaMalloc((void**)p, n); }
+inline cudaError_t cudaFree(void* p) { std::free(p); return 0; }
+inline cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) { std::memmove(d, s, n); return 0; }
+inline cudaError_t cudaMemset(void* d, int v, size_t n) { std::memset(d, v, n); return 0; }
+inline cudaError_t cudaSetDevice(int) { return 0; }
+inline const char* cudaGetErrorString(cudaError_t) { return "host stand-in"; }

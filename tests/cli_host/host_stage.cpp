@@ -1,0 +1,64 @@
+// Test infrastructure: the stage entry points the registration command line calls, backed by
+// the CPU oracle's whole registration, so that its plumbing (initial transforms, output names,
+// written transforms, warped images) can be tested without a GPU.  Never part of the product.
+#include <cstring>
+#include <string>
+#include <vector>
+#include "synx.h"
+extern "C" int oracle_syn_register_f32(const float*, const synx_geom*, const float*, const synx_geom*, const synx_params*,
+                                       float*, float*, synx_geom*, int32_t*, int32_t*, double*, double*, int32_t*, int);
+extern "C" void oracle_shrink_geom(const synx_geom*, unsigned, synx_geom*);
+struct synx_ctx {
+  synx_params p;
+  std::vector<float> F, M, fwd, inv;
+  synx_geom gf, gm, go;
+  std::vector<int32_t> lv, it, ki;
+  std::vector<double> me, cv;
+  bool done = false;
+};
+extern "C" {
+int synx_params_default(synx_params* p, int dim) {
+  memset(p, 0, sizeof(*p));
+  p->dim = dim; p->n_levels = 1; p->learning_rate = 0.1; p->update_variance = 3.0; p->cc_radius = 4;
+  p->iterations[0] = 1; p->shrink_factors[0] = 1; p->convergence_threshold = 1e-6; p->convergence_window = 10;
+  p->preprocess = 1; p->winsor_upper = 1.0f; p->inv_max_iter = 20; p->inv_mean_tol = 0.001; p->inv_max_tol = 0.1;
+  return 0;
+}
+int synx_create(const synx_params* p, int, void*, synx_ctx** out) { *out = new synx_ctx; (*out)->p = *p; return 0; }
+int synx_destroy(synx_ctx* c) { delete c; return 0; }
+int synx_set_images(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm) {
+  c->gf = *gf; c->gm = *gm;
+  c->F.assign(F, F + gf->size[0] * gf->size[1] * gf->size[2]);
+  c->M.assign(M, M + gm->size[0] * gm->size[1] * gm->size[2]);
+  return 0;
+}
+int synx_run_level(synx_ctx* c, int level) {
+  if (c->done || level != c->p.n_levels - 1) return 0;  // the whole stage runs at the last level
+  synx_geom go;
+  oracle_shrink_geom(&c->gf, c->p.shrink_factors[c->p.n_levels - 1], &go);
+  const size_t N = go.size[0] * go.size[1] * go.size[2], D = c->p.dim;
+  std::vector<float> f(N * D), v(N * D);
+  const int cap = 100000;
+  c->lv.resize(cap); c->it.resize(cap); c->ki.resize(cap); c->me.resize(cap); c->cv.resize(cap);
+  int n = oracle_syn_register_f32(c->F.data(), &c->gf, c->M.data(), &c->gm, &c->p, f.data(), v.data(), &c->go,
+                                  c->lv.data(), c->it.data(), c->me.data(), c->cv.data(), c->ki.data(), cap);
+  for (auto* a : {&c->lv, &c->it, &c->ki}) a->resize(n);
+  c->me.resize(n); c->cv.resize(n);
+  c->fwd.resize(N * D); c->inv.resize(N * D);
+  for (size_t i = 0; i < N; ++i)
+    for (size_t k = 0; k < D; ++k) { c->fwd[i * D + k] = f[k * N + i]; c->inv[i * D + k] = v[k * N + i]; }
+  c->done = true;
+  return 0;
+}
+int synx_get_output_geom(const synx_ctx* c, synx_geom* g) { *g = c->go; return 0; }
+int synx_get_fields(synx_ctx* c, float* fw, float* iv) {
+  std::memcpy(fw, c->fwd.data(), 4 * c->fwd.size()); std::memcpy(iv, c->inv.data(), 4 * c->inv.size()); return 0; }
+int synx_get_log(synx_ctx* c, int32_t* level, int32_t* iter, double* metric, double* conv, int32_t* inv, int64_t cap, int64_t* count) {
+  *count = (int64_t)c->me.size();
+  for (int64_t i = 0; i < cap && i < *count; ++i) {
+    if (level) level[i] = c->lv[i]; if (iter) iter[i] = c->it[i]; if (metric) metric[i] = c->me[i];
+    if (conv) conv[i] = c->cv[i]; if (inv) inv[i] = c->ki[i];
+  }
+  return 0;
+}
+}

@@ -44,6 +44,10 @@ def test_rejects_bad_input(exe, args, needle):
 
 @pytest.mark.gpu
 def test_default_value_outside(exe, tmp_path, cuda):
+    check_default_value_outside(exe, tmp_path)
+
+
+def check_default_value_outside(exe, tmp_path):
     g = Geom((40, 36))
     img = np.full(g.shape, 5.0, np.float32)
     u = np.zeros(g.shape + (2,), np.float32)
@@ -61,6 +65,10 @@ def test_default_value_outside(exe, tmp_path, cuda):
 
 @pytest.mark.gpu
 def test_reproduces_the_registration_output(exe, tmp_path, cuda):
+    check_reproduces_the_registration_output(REG, exe, tmp_path)
+
+
+def check_reproduces_the_registration_output(reg, exe, tmp_path):
     # resampling the moving image through prefix0Warp gives antsRegistration's warped output
     size = (64, 60)
     f, m = phantoms.pair_2d(size, seed=31)
@@ -68,7 +76,7 @@ def test_reproduces_the_registration_output(exe, tmp_path, cuda):
     nifti.write(tmp_path / "f.nii.gz", f, g)
     nifti.write(tmp_path / "m.nii.gz", m, g)
     p = str(tmp_path / "r_")
-    r = subprocess.run([REG, "-d", "2", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]", "-t", "SyN[0.2,3,0]",
+    r = subprocess.run([reg, "-d", "2", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]", "-t", "SyN[0.2,3,0]",
                         "-c", "[8x4,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-o", f"[{p},{p}warped.nii.gz]"],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr

@@ -152,7 +152,7 @@ def cases(dim):
         "linear": ([("linear", A), ("linear", B)], gm, ["A.mat", "B.mat"]),
         # affine, field, affine: both ends folded
         "both_ends": ([("linear", B.inverse()), ("field", (a, g)), ("linear", A)], gm, ["[B.mat,1]", "a", "A.mat"]),
-    }, dict(a=a, b=b, inv=inv, A=A, B=B, g=g)
+    }, dict(a=a, b=b, inv=inv, A=A, B=B, g=g, gm=gm)
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -189,8 +189,12 @@ def run(exe, args):
 @pytest.mark.gpu
 @pytest.mark.parametrize("dim", [2, 3])
 def test_stacks_match_the_scheme(exe, tmp_path, cuda, dim):
+    check_stacks_match_the_scheme(exe, tmp_path, dim)
+
+
+def check_stacks_match_the_scheme(exe, tmp_path, dim):
     cs, parts = cases(dim)
-    g, gm = grids(dim)
+    g, gm = parts["g"], parts["gm"]  # the grid objects the cases refer to
     files = {"a": parts["a"], "b": parts["b"], "inv": parts["inv"]}
     for name, u in files.items():
         nifti.write(tmp_path / f"{name}.nii.gz", np.ascontiguousarray(np.moveaxis(u, 0, -1)), g, vector=True)
@@ -208,6 +212,7 @@ def test_stacks_match_the_scheme(exe, tmp_path, cuda, dim):
         return f"{tmp_path}/{tok}" + ("" if tok.endswith(".mat") else ".nii.gz")
 
     for name, (chain, gr, toks) in cs.items():
+        assert gr is g or gr is gm
         ref = tmp_path / ("fixed.nii.gz" if gr is g else "moving.nii.gz")
         ts = sum((["-t", spell(t)] for t in toks), [])
         want_field, want_img = emulate_cli(chain, gr, img, gi)
@@ -226,14 +231,25 @@ def test_stacks_match_the_scheme(exe, tmp_path, cuda, dim):
         assert bad.mean() < 2e-3, (name, int(bad.sum()))
 
 
+REG = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
+
+
 @pytest.mark.gpu
 def test_registration_with_an_initial_moving_transform(exe, tmp_path, cuda):
+    check_initial_moving_transform(REG, exe, tmp_path)
+
+
+@pytest.mark.gpu
+def test_registration_with_a_derived_initial_translation(exe, tmp_path, cuda):
+    check_derived_initial_translation(REG, tmp_path)
+
+
+def check_initial_moving_transform(reg, exe, tmp_path):
     """antsRegistration -r init.mat: the moving image is sampled at Init(x + psi_M(x)); the outputs are
     numbered as the reference numbers them (0GenericAffine.mat, 1Warp, 1InverseWarp), and the warped
     images agree with antsApplyTransforms through the standard stacks."""
     from ants_b200 import synx
     from ants_b200.synx import SyNParams
-    reg = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
     size = (64, 60)
     f, m = phantoms.pair_2d(size, seed=33)
     g = Geom(size)
@@ -274,14 +290,12 @@ def test_registration_with_an_initial_moving_transform(exe, tmp_path, cuda):
         assert bad.mean() < 1e-3, (out, int(bad.sum()))
 
 
-@pytest.mark.gpu
-def test_registration_with_a_derived_initial_translation(tmp_path, cuda):
+def check_derived_initial_translation(reg, tmp_path):
     """antsRegistration -r [fixed,moving,1]: the translation between the centers of intensity mass,
     folded into the moving geometry; collapsed into 0GenericAffine.mat, or with -z 0 written as
     0DerivedInitialMovingTranslation.mat, the SyN fields numbered 1 either way."""
     from ants_b200 import synx
     from ants_b200.synx import SyNParams
-    reg = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
     size = (64, 60)
     f, m = phantoms.pair_2d(size, seed=35)
     g, gm = Geom(size), Geom(size, (1.0, 1.0), (1.5, -2.0))  # the moving image is shifted in space
