@@ -233,6 +233,48 @@ void launch_warp_image(const float* img, const GridInfo& gi, const float* u, con
     k_warp_image<2><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
 }
 
+// Nearest-neighbour variant (antsApplyTransforms -n NearestNeighbor): ITK's
+// NearestNeighborInterpolateImageFunction reads, inside the buffer, the voxel at
+// RoundHalfIntegerUp(c) = floor(c + 0.5) per axis.  Inside the buffer -0.5 <= c < n - 0.5, so the
+// index is in [0, n - 1]; the clamp only absorbs the float rounding of c + 0.5 at the upper rim.
+__device__ __forceinline__ int nearest_index(float c, int n) {
+  const int i = (int)floorf(c + 0.5f);
+  return min(max(i, 0), n - 1);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_warp_image_nearest(const float* __restrict__ img, Dims di, Affine m,
+                                                            const float* __restrict__ u, Dims dv, int zb,
+                                                            float* __restrict__ out) {
+  const Coord3 c = coord3(dv, zb, 1);
+  if (!c.ok) return;
+  const int N = (int)dv.N, nxy = dv.nx * dv.ny;
+  for (int z = c.z0; z < c.z1; ++z) {
+    const int i = z * nxy + c.y * dv.nx + c.x;
+    float cx, cy, cz;
+    map_point<DIM, false>(m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f, cx, cy,
+                          cz);
+    float v = 0.0f;
+    if (inside_buffer<DIM>(di, cx, cy, cz)) {
+      const int x = nearest_index(cx, di.nx), y = nearest_index(cy, di.ny);
+      const int zz = DIM == 3 ? nearest_index(cz, di.nz) : 0;
+      v = __ldg(img + (zz * di.ny + y) * di.nx + x);
+    }
+    out[i] = v;
+  }
+}
+
+void launch_warp_image_nearest(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
+                               cudaStream_t s) {
+  count_launch();
+  Affine a = make_affine(gv, gi);
+  const Map3 m = map3(gv.d);
+  if (gv.d.dim == 3)
+    k_warp_image_nearest<3><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
+  else
+    k_warp_image_nearest<2><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
+}
+
 // ------------------------------------------------------------------------------------------
 // Gaussian smoothing of displacement fields: an xy kernel (one block per tile, slice and field)
 // and, in 3-D, a z kernel (one thread per column chunk).  The SyN epilogue (boundary zeroing,

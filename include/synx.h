@@ -256,6 +256,12 @@ int synx_smooth_image(const float* in_dev, float* out_dev, const synx_geom* g, d
  * displacement field; itkantsRegistrationHelper.hxx:2138, observer .h:342-381). */
 int synx_warp_image(const float* img_dev, const synx_geom* img_geom, const float* u_dev, const synx_geom* grid,
                     float* out_dev, void* stream);
+/* Same with nearest-neighbour sampling (antsApplyTransforms -n NearestNeighbor,
+ * Examples/make_interpolator_snip.tmpl:24-28): inside the image buffer, the voxel at
+ * floor(c + 0.5) per axis of the continuous index c (ITK's NearestNeighborInterpolateImageFunction),
+ * 0 outside.  For label images. */
+int synx_warp_image_nearest(const float* img_dev, const synx_geom* img_geom, const float* u_dev, const synx_geom* grid,
+                            float* out_dev, void* stream);
 
 /* Windowed CC on two images on the same grid: value (-mean cc), the fixed-to-middle update
  * direction (uses grad of `moving`) and the moving-to-middle one (uses grad of `fixed`)

@@ -54,6 +54,7 @@ def load() -> C.CDLL:
             f"oracle_preprocess_{suf}": (None, [V, V, C.c_int64, C.c_float, C.c_float]),
             f"oracle_smooth_image_{suf}": (None, [V, V, P(G), D, I]),
             f"oracle_warp_image_{suf}": (None, [V, P(G), V, P(G), V]),
+            f"oracle_warp_image_nearest_{suf}": (None, [V, P(G), V, P(G), V]),
             f"oracle_cc_{suf}": (D, [V, V, P(G), I, V, V, V]),
             f"oracle_smooth_field_{suf}": (None, [V, V, P(G), D]),
             f"oracle_scale_update_{suf}": (D, [V, P(G), D]),
@@ -121,11 +122,12 @@ def smooth_image(img, g, sigma, mm=False, dtype=np.float32):
     return out
 
 
-def warp_image(img, gi, u, gv, dtype=np.float32):
+def warp_image(img, gi, u, gv, dtype=np.float32, nearest=False):
     a, uu = _c(img, dtype), _c(u, dtype)
     out = np.empty(gv.shape, dtype)
     ga, gb = gi.to_c(), gv.to_c()
-    getattr(load(), f"oracle_warp_image_{_suf(dtype)}")(_p(a), C.byref(ga), _p(uu), C.byref(gb), _p(out))
+    name = "oracle_warp_image_nearest_" if nearest else "oracle_warp_image_"
+    getattr(load(), name + _suf(dtype))(_p(a), C.byref(ga), _p(uu), C.byref(gb), _p(out))
     return out
 
 

@@ -402,6 +402,31 @@ inline void warp_image(const T* img, const Geom& gi, const T* u, const Geom& gv,
   }
 }
 
+// Same warp with nearest-neighbour sampling, as antsApplyTransforms -n NearestNeighbor selects it
+// (Examples/make_interpolator_snip.tmpl:24-28): ITK's NearestNeighborInterpolateImageFunction
+// reads, inside the buffer, the voxel at RoundHalfIntegerUp(c) = floor(c + 0.5) per axis.
+template <class T>
+inline void warp_image_nearest(const T* img, const Geom& gi, const T* u, const Geom& gv, T* out) {
+  const int64_t N = gv.count();
+  const int64_t nx = gv.n[0], ny = gv.n[1];
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < N; ++i) {
+    double idx[3] = {(double)(i % nx), (double)((i / nx) % ny), (double)(i / (nx * ny))};
+    double p[3];
+    gv.index_to_point(idx, p);
+    for (int d = 0; d < gv.dim; ++d) p[d] += (double)u[d * N + i];
+    double c[3];
+    gi.point_to_cindex(p, c);
+    if (!inside_buffer(gi, c)) {
+      out[i] = (T)0;
+      continue;
+    }
+    int64_t k[3] = {0, 0, 0};
+    for (int d = 0; d < gi.dim; ++d) k[d] = std::min<int64_t>(std::max<int64_t>((int64_t)std::floor(c[d] + 0.5), 0), gi.n[d] - 1);
+    out[i] = img[(k[2] * gi.n[1] + k[1]) * gi.n[0] + k[0]];
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Neighbourhood cross-correlation value and derivatives.
 //

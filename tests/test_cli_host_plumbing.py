@@ -62,3 +62,8 @@ def test_initial_moving_transform(host_cli, tmp_path):
 
 def test_derived_initial_translation(host_cli, tmp_path):
     S.check_derived_initial_translation(host_cli["reg"], tmp_path)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_nearest_neighbor(host_cli, tmp_path, dim):
+    S.check_nearest_neighbor(host_cli["apply"], tmp_path, dim)

@@ -114,6 +114,31 @@ def test_cc_edge_cases_match_bruteforce(case, dtype):
 
 
 # ---- warp / compose / invert / resample -----------------------------------------------------------
+@pytest.mark.parametrize("dim", [2, 3])
+def test_warp_nearest_matches_a_restatement(dim):
+    """Nearest-neighbour warp: inside the buffer the voxel at floor(c + 0.5), 0 outside (numpy
+    restatement of ITK's NearestNeighborInterpolateImageFunction on an oblique grid pair)."""
+    from scipy.spatial.transform import Rotation
+    rng = np.random.default_rng(40 + dim)
+    if dim == 3:
+        gv = Geom((9, 8, 7), (1.1, 0.9, 1.2), (1.0, -1.0, 0.5), Rotation.from_euler("xyz", [0.2, -0.1, 0.15]).as_matrix())
+        gi = Geom((12, 11, 10), (0.8, 0.85, 0.9), (-1.0, -2.0, -1.5))
+    else:
+        gv = Geom((13, 11), (1.1, 0.9), (1.0, -1.0), np.array([[np.cos(0.2), -np.sin(0.2)], [np.sin(0.2), np.cos(0.2)]]))
+        gi = Geom((16, 15), (0.8, 0.85), (-1.0, -2.0))
+    img = rng.integers(0, 6, gi.shape).astype(np.float32)
+    u = (rng.standard_normal((dim,) + gv.shape) * 1.5).astype(np.float32)
+    got = O.warp_image(img, gi, u, gv, nearest=True)
+    axes = np.meshgrid(*[np.arange(n) for n in reversed(gv.size)], indexing="ij")
+    idx = np.stack(list(reversed(axes)), -1).astype(np.float64)
+    P = np.asarray(gv.origin) + (idx * np.asarray(gv.spacing)) @ gv.direction.T + np.moveaxis(u, 0, -1).astype(np.float64)
+    c = np.linalg.solve(gi.direction * np.asarray(gi.spacing), (P - np.asarray(gi.origin)).reshape(-1, dim).T).T
+    inside = np.all((c >= -0.5) & (c < np.asarray(gi.size) - 0.5), axis=1)
+    k = np.clip(np.floor(c + 0.5).astype(int), 0, np.asarray(gi.size) - 1)
+    want = np.where(inside, img[tuple(k[:, a] for a in reversed(range(dim)))], 0.0).reshape(gv.shape)
+    np.testing.assert_array_equal(got, want)
+    assert set(np.unique(got)) <= set(range(6))
+
 def test_warp_identity_and_integer_shift():
     rng = np.random.default_rng(4)
     img = rng.uniform(0, 1, (9, 10, 11)).astype(np.float32)

@@ -235,6 +235,35 @@ REG = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_nearest_neighbor_labels(exe, tmp_path, cuda, dim):
+    check_nearest_neighbor(exe, tmp_path, dim)
+
+
+def check_nearest_neighbor(exe, tmp_path, dim):
+    """-n NearestNeighbor through `-t field -t affine.mat`: the label image sampled at A(p + u(p)) with
+    ITK's nearest-neighbour rule; a point on a rounding tie may pick either voxel."""
+    cs, parts = cases(dim)
+    chain, gr, toks = cs["forward"]
+    g = parts["g"]
+    nifti.write(tmp_path / "a.nii.gz", np.ascontiguousarray(np.moveaxis(parts["a"], 0, -1)), g, vector=True)
+    parts["A"].write_mat(tmp_path / "A.mat")
+    nifti.write(tmp_path / "fixed.nii.gz", np.zeros(g.shape, np.float32), g)
+    gi = Geom((70, 64) if dim == 2 else (40, 36, 32), (0.8,) * dim, (-3.0,) * dim)
+    labels = np.random.default_rng(95 + dim).integers(0, 9, gi.shape).astype(np.float32)
+    nifti.write(tmp_path / "labels.nii.gz", labels, gi)
+    r = run(exe, ["-d", str(dim), "-r", f"{tmp_path}/fixed.nii.gz", "-i", f"{tmp_path}/labels.nii.gz",
+                  "-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/A.mat", "-n", "NearestNeighbor",
+                  "-o", f"{tmp_path}/o.nii.gz"])
+    assert r.returncode == 0, r.stderr
+    got, _ = nifti.read(tmp_path / "o.nii.gz", dim)
+    want = O.warp_image(labels, push_forward(gi, parts["A"].inverse()), parts["a"], g, nearest=True)
+    assert set(np.unique(got)) <= set(range(9))
+    bad = got != want
+    assert bad.mean() < 2e-3, int(bad.sum())
+
+
+@pytest.mark.gpu
 def test_registration_with_an_initial_moving_transform(exe, tmp_path, cuda):
     check_initial_moving_transform(REG, exe, tmp_path)
 
