@@ -638,6 +638,116 @@ def run_precision(args) -> int:
 
 
 # ---------------------------------------------------------------------------------------------
+APPLY_BYTES_PER_VOXEL = 20  # field 12 B + output 4 B + one sample of the input 4 B
+
+
+def run_apply(args) -> int:
+    """antsApplyTransforms through the standard stack `-t 1Warp.nii.gz -t 0GenericAffine.mat` onto a
+    182x218x182 reference grid.  The command line's scheme for this stack is one warp of the input
+    through the field, with the affine folded into the input's geometry (synx_warp_image), so a step
+    is that warp.  value = reference voxels per second with inputs resident (CUDA events on the
+    launching stream, L2 flushed between steps); e2e = the same with the input image and the field
+    copied host->device and the output device->host inside each timed step; roofline = the warp,
+    20 B per voxel (field 12, output 4, one input sample 4); cpu_baseline = the oracle's warp on all
+    host threads; the device output is checked against it."""
+    import torch
+    from ants_b200 import phantoms
+    from ants_b200 import synx as S
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = S.Geom(SIZE)                                        # the reference (fixed) grid, 1 mm
+    gi = S.Geom(SIZE, (1.0, 1.0, 1.0), (-2.0, 1.5, -1.0))   # the input (moving) image's own grid
+    rng = np.random.default_rng(0x5EED0000 + 5000)
+    _, moving = phantoms.pair_3d(SIZE, seed=0x5EED0000 + 5001)
+    img = np.ascontiguousarray(moving, dtype=np.float32)
+    u = np.ascontiguousarray(np.moveaxis(phantoms.smooth_field(g.shape, 8.0, 3.0, rng), -1, 0).astype(np.float32))
+    A = S.LinearTransform(np.array([[1.02, 0.03, -0.01], [-0.02, 0.98, 0.02], [0.01, -0.015, 1.01]]),
+                          np.array([1.5, -2.0, 0.75]), np.array([91.0, 109.0, 91.0]))
+    gi_fold = S.fold_moving_geometry(gi, A)  # sampling at q reads the input at A(q)
+    N = g.count
+    Id, Ud = torch.from_numpy(img).to(dev), torch.from_numpy(u).to(dev)
+    out = torch.empty(g.shape, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def step():
+        S.warp_image(Id, gi_fold, Ud, g, out, stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    launches0 = S.launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    launches = S.launch_count() - launches0
+    ms = [a.elapsed_time(b) for a, b in evs]
+    t = sum(ms) / 1000.0
+    value = N * args.steps / t
+    got = out.cpu().numpy()
+
+    # end to end: host input image and field in, warped image out, every step
+    img_h = torch.from_numpy(img).pin_memory()
+    u_h = torch.from_numpy(u).pin_memory()
+    out_h = torch.empty(g.shape, dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        Id.copy_(img_h, non_blocking=True)
+        Ud.copy_(u_h, non_blocking=True)
+        step()
+        out_h.copy_(out, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    t_e2e = sum(e2e_ms) / 1000.0
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = APPLY_BYTES_PER_VOXEL * N / (t / args.steps) / 1e9
+    cpu, mismatch = None, None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        n_cpu, t0 = 0, time.perf_counter()
+        while True:
+            ref = O.warp_image(img, gi_fold, u, g)
+            n_cpu += 1
+            dt = time.perf_counter() - t0
+            if dt >= 5.0 or n_cpu >= 50:
+                break
+        cpu = {"value": N * n_cpu / dt, "unit": "voxel/s", "cores": threads, "kind": "port",
+               "sample": f"{n_cpu} warps of the 182x218x182 workload by the oracle ({dt:.1f} s of CPU work)"}
+        mismatch = float((np.abs(got - ref) > 1e-5).mean())
+    line = {"metric": "antsApplyTransforms voxels/s (182x218x182, -t warp -t affine)", "value": value,
+            "unit": "voxel/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic: seeded phantom image, smooth field, fixed affine",
+            "config": {"workload": "warp of a 182x218x182 image through a displacement field and an affine "
+                                   "(folded into the input geometry), linear interpolation",
+                       "l2": "flushed between steps (256 MB)", "parity_mismatch_fraction_vs_oracle": mismatch},
+            "e2e": {"value": N * args.steps / t_e2e, "unit": "voxel/s", "h2d_bytes_per_step": int(img.nbytes + u.nbytes),
+                    "d2h_bytes_per_step": int(N * 4), "ms_per_step": 1000.0 * t_e2e / args.steps},
+            "roofline": {"kernel": "k_warp_image<3>", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": APPLY_BYTES_PER_VOXEL * N,
+                         "launch_ms": t / args.steps * 1000.0},
+            "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": int(launches)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -648,10 +758,10 @@ def main(argv=None) -> int:
     ap.add_argument("--plain-launches", action="store_true",
                     help="launch every kernel directly instead of replaying per-level CUDA graphs (the same "
                          "work; profilers see each kernel, which they do not inside graphs with conditional nodes)")
-    ap.add_argument("--config", default="single", choices=["single", "batched", "serving", "precision"],
+    ap.add_argument("--config", default="single", choices=["single", "batched", "serving", "precision", "apply"],
                     help="single: the 182x218x182 pair (default); batched: 32 pairs of uneven sizes, "
                          "batched vs sequential pairs/hour; serving: Poisson arrivals of a 2-D/3-D mix, "
-                         "p50/p99 latency")
+                         "p50/p99 latency; precision: the error study; apply: antsApplyTransforms warp + affine")
     ap.add_argument("--rates", default="0.5,2,5,10,20", help="serving: arrival rates (requests/s)")
     ap.add_argument("--window", type=float, default=12.0, help="serving: seconds of arrivals per rate")
     args = ap.parse_args(argv)
@@ -661,6 +771,8 @@ def main(argv=None) -> int:
         return run_serving(args)
     if args.config == "precision":
         return run_precision(args)
+    if args.config == "apply":
+        return run_apply(args)
 
     ws, rank, local = dist_env()
     from ants_b200 import phantoms, replicas
