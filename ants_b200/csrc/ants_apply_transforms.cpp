@@ -19,7 +19,8 @@
 //       applies its inverse.  The transforms of one file act as the composite the file holds: the
 //       last one first, or for [file,1] the inverse of the first one first (:1440-1451).
 //       HDF5 composite files (.h5) are not supported.
-//   -n/--interpolation Linear (the default) | NearestNeighbor (label images; others are rejected)
+//   -n/--interpolation Linear (the default) | NearestNeighbor | GenericLabel[Linear] (label images;
+//       others are rejected)
 //   -f/--default-value v (0): value where the point maps outside the input image
 //   -o/--output warped | [collapsed,1] | DisplacementField[collapsed]  (the collapsed form writes
 //       the single displacement field equivalent to the stack, on the reference grid, :1115-1131)
@@ -127,10 +128,13 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   if (opt.count("input-image-type") && one("input-image-type", "0") != "0" &&
       lower(one("input-image-type", "scalar")) != "scalar")
     throw std::runtime_error("only scalar input images are supported");
-  const std::string interp = lower(parse_call(one("interpolation", "Linear")).name);
-  if (interp != "linear" && interp != "nearestneighbor")
-    throw std::runtime_error("only Linear and NearestNeighbor interpolation are supported");
-  const bool nearest = interp == "nearestneighbor";
+  const OptionCall icall = parse_call(one("interpolation", "Linear"));
+  const std::string interp = lower(icall.name);
+  if (interp != "linear" && interp != "nearestneighbor" && interp != "genericlabel")
+    throw std::runtime_error("only Linear, NearestNeighbor and GenericLabel[Linear] interpolation are supported");
+  if (interp == "genericlabel" && !icall.params.empty() && lower(icall.params[0]) != "linear")
+    throw std::runtime_error("GenericLabel supports the Linear interpolator only");
+  const bool nearest = interp == "nearestneighbor", label = interp == "genericlabel";
   if (!opt.count("reference-image")) throw std::runtime_error("a reference image (-r) is required");
   if (!opt.count("output")) throw std::runtime_error("an output (-o) is required");
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
@@ -302,7 +306,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const long long Ni = in.voxels();
   DeviceBuffer di((size_t)Ni), dout((size_t)N);
   CLI_CK(cudaMemcpy(di.p, in.data.data(), 4 * (size_t)Ni, cudaMemcpyHostToDevice));
-  if (nearest) step_ok(synx_warp_image_nearest(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_nearest");
+  if (label) step_ok(synx_warp_image_label(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_label");
+  else if (nearest) step_ok(synx_warp_image_nearest(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_nearest");
   else step_ok(synx_warp_image(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image");
   nifti::Image res = ref;
   res.components = 1;

@@ -1661,6 +1661,18 @@ int synx_warp_image_nearest(const float* img, const synx_geom* gi, const float* 
   return SYNX_OK;
 }
 
+int synx_warp_image_label(const float* img, const synx_geom* gi, const float* u, const synx_geom* gv, float* out,
+                          void* stream) {
+  if (!img || !u || !out || !gi || !gv || !check_geom(gi, gi->dim) || !check_geom(gv, gi->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_warp_image_label: bad arguments");
+  GridInfo a, b;
+  geom_to_grid(*gi, a);
+  geom_to_grid(*gv, b);
+  launch_warp_image_label(img, a, u, b, out, (cudaStream_t)stream);
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
 int synx_cc_metric(const float* F, const float* M, const synx_geom* gg, int radius, float* gF, float* gM,
                    double* value, void* stream) {
   return synx_cc_metric_ex(F, M, gg, radius, 0, gF, gM, value, stream);

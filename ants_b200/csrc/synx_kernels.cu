@@ -264,6 +264,64 @@ __global__ void __launch_bounds__(256) k_warp_image_nearest(const float* __restr
   }
 }
 
+// Generic label interpolation (antsApplyTransforms -n GenericLabel[Linear]): ITK's
+// LabelImageGenericInterpolateImageFunction returns the label whose indicator image interpolates
+// highest; with linear interpolation that is the label with the largest sum of cell-corner weights,
+// ties going to the smaller label.  The cell is the linear interpolator's (clamp-to-edge), so every
+// corner offset is inside the image; at most 8 distinct labels per cell.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_warp_image_label(const float* __restrict__ img, Dims di, Affine m,
+                                                          const float* __restrict__ u, Dims dv, int zb,
+                                                          float* __restrict__ out) {
+  const Coord3 c = coord3(dv, zb, 1);
+  if (!c.ok) return;
+  const int N = (int)dv.N, nxy = dv.nx * dv.ny;
+  for (int z = c.z0; z < c.z1; ++z) {
+    const int i = z * nxy + c.y * dv.nx + c.x;
+    float cx, cy, cz;
+    map_point<DIM, false>(m, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f, cx, cy,
+                          cz);
+    float v = 0.0f;
+    if (inside_buffer<DIM>(di, cx, cy, cz)) {
+      const Cell cl = make_cell<DIM>(di, cx, cy, cz);
+      float lab[8], acc[8];
+      int n = 0;
+#pragma unroll
+      for (int k = 0; k < (DIM == 3 ? 8 : 4); ++k) {
+        const int bx = k & 1, by = (k >> 1) & 1, bz = (k >> 2) & 1;
+        const int o = cl.o000 + (bx ? cl.dx : 0) + (by ? cl.dy : 0) + (bz ? cl.dz : 0);
+        const float w = (bx ? cl.wx : 1.0f - cl.wx) * (by ? cl.wy : 1.0f - cl.wy) *
+                        (DIM == 3 ? (bz ? cl.wz : 1.0f - cl.wz) : 1.0f);
+        const float l = __ldg(img + o);
+        int j = 0;
+        while (j < n && lab[j] != l) ++j;
+        if (j == n) {
+          lab[n] = l;
+          acc[n] = 0.0f;
+          ++n;
+        }
+        acc[j] += w;
+      }
+      int best = 0;
+      for (int j = 1; j < n; ++j)
+        if (acc[j] > acc[best] || (acc[j] == acc[best] && lab[j] < lab[best])) best = j;
+      v = lab[best];
+    }
+    out[i] = v;
+  }
+}
+
+void launch_warp_image_label(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
+                             cudaStream_t s) {
+  count_launch();
+  Affine a = make_affine(gv, gi);
+  const Map3 m = map3(gv.d);
+  if (gv.d.dim == 3)
+    k_warp_image_label<3><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
+  else
+    k_warp_image_label<2><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
+}
+
 void launch_warp_image_nearest(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
                                cudaStream_t s) {
   count_launch();

@@ -191,6 +191,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_smooth_image": (I, [V, V, P(SynxGeom), D, I, V]),
         "synx_warp_image": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
         "synx_warp_image_nearest": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
+        "synx_warp_image_label": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
         "synx_cc_metric": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
         "synx_cc_metric_noalloc": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
         "synx_cc_metric_ex": (I, [V, V, P(SynxGeom), I, I, V, V, P(D), V]),
@@ -616,10 +617,13 @@ def smooth_image(img, out, g: Geom, sigma: float, sigma_in_mm: bool = False, str
                                             _stream(stream)))
 
 
-def warp_image(img, img_geom: Geom, u, grid: Geom, out, stream=None, nearest: bool = False) -> None:
-    """out(x) = img(x + u(x)) on `grid`, linear or (nearest=True) nearest-neighbour, 0 outside."""
+def warp_image(img, img_geom: Geom, u, grid: Geom, out, stream=None, nearest: bool = False,
+               label: bool = False) -> None:
+    """out(x) = img(x + u(x)) on `grid`, 0 outside: linear, nearest-neighbour (nearest=True) or
+    generic label interpolation over the linear interpolator (label=True)."""
     a, b = img_geom.to_c(), grid.to_c()
-    fn = load_library().synx_warp_image_nearest if nearest else load_library().synx_warp_image
+    lib = load_library()
+    fn = lib.synx_warp_image_label if label else lib.synx_warp_image_nearest if nearest else lib.synx_warp_image
     _check(fn(_ptr(img), C.byref(a), _ptr(u), C.byref(b), _ptr(out), _stream(stream)))
 
 

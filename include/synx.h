@@ -262,6 +262,12 @@ int synx_warp_image(const float* img_dev, const synx_geom* img_geom, const float
  * 0 outside.  For label images. */
 int synx_warp_image_nearest(const float* img_dev, const synx_geom* img_geom, const float* u_dev, const synx_geom* grid,
                             float* out_dev, void* stream);
+/* Same with generic label interpolation (antsApplyTransforms -n GenericLabel[Linear],
+ * Examples/make_interpolator_snip.tmpl:112-117; ITK's LabelImageGenericInterpolateImageFunction over
+ * the linear interpolator): inside the buffer, the label with the largest sum of linear cell-corner
+ * weights, a tie going to the smaller label; 0 outside. */
+int synx_warp_image_label(const float* img_dev, const synx_geom* img_geom, const float* u_dev, const synx_geom* grid,
+                          float* out_dev, void* stream);
 
 /* Windowed CC on two images on the same grid: value (-mean cc), the fixed-to-middle update
  * direction (uses grad of `moving`) and the moving-to-middle one (uses grad of `fixed`)

@@ -55,6 +55,7 @@ def load() -> C.CDLL:
             f"oracle_smooth_image_{suf}": (None, [V, V, P(G), D, I]),
             f"oracle_warp_image_{suf}": (None, [V, P(G), V, P(G), V]),
             f"oracle_warp_image_nearest_{suf}": (None, [V, P(G), V, P(G), V]),
+            f"oracle_warp_image_label_{suf}": (None, [V, P(G), V, P(G), V]),
             f"oracle_cc_{suf}": (D, [V, V, P(G), I, V, V, V]),
             f"oracle_smooth_field_{suf}": (None, [V, V, P(G), D]),
             f"oracle_scale_update_{suf}": (D, [V, P(G), D]),
@@ -122,11 +123,11 @@ def smooth_image(img, g, sigma, mm=False, dtype=np.float32):
     return out
 
 
-def warp_image(img, gi, u, gv, dtype=np.float32, nearest=False):
+def warp_image(img, gi, u, gv, dtype=np.float32, nearest=False, label=False):
     a, uu = _c(img, dtype), _c(u, dtype)
     out = np.empty(gv.shape, dtype)
     ga, gb = gi.to_c(), gv.to_c()
-    name = "oracle_warp_image_nearest_" if nearest else "oracle_warp_image_"
+    name = "oracle_warp_image_label_" if label else "oracle_warp_image_nearest_" if nearest else "oracle_warp_image_"
     getattr(load(), name + _suf(dtype))(_p(a), C.byref(ga), _p(uu), C.byref(gb), _p(out))
     return out
 

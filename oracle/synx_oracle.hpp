@@ -427,6 +427,55 @@ inline void warp_image_nearest(const T* img, const Geom& gi, const T* u, const G
   }
 }
 
+// Same warp with the generic label interpolation antsApplyTransforms -n GenericLabel[Linear] selects
+// (Examples/make_interpolator_snip.tmpl:112-117): ITK's LabelImageGenericInterpolateImageFunction
+// interpolates the indicator image of every label with the linear interpolator and returns the label
+// with the largest value, scanning its (sorted) label set and keeping a strictly larger value, so a
+// tie goes to the smaller label.  With linear interpolation the value of a label is the sum of the
+// weights of the cell corners that carry it; labels absent from the cell have value 0 and never win.
+template <class T>
+inline void warp_image_label(const T* img, const Geom& gi, const T* u, const Geom& gv, T* out) {
+  const int64_t N = gv.count();
+  const int64_t nx = gv.n[0], ny = gv.n[1];
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < N; ++i) {
+    double idx[3] = {(double)(i % nx), (double)((i / nx) % ny), (double)(i / (nx * ny))};
+    double p[3];
+    gv.index_to_point(idx, p);
+    for (int d = 0; d < gv.dim; ++d) p[d] += (double)u[d * N + i];
+    double c[3];
+    gi.point_to_cindex(p, c);
+    if (!inside_buffer(gi, c)) {
+      out[i] = (T)0;
+      continue;
+    }
+    LerpCell L;
+    lerp_cell(gi, c, L);
+    double lab[8], acc[8];
+    int n = 0;
+    const int corners = gi.dim == 3 ? 8 : 4;
+    for (int k = 0; k < corners; ++k) {
+      const int bx = k & 1, by = (k >> 1) & 1, bz = (k >> 2) & 1;
+      const int64_t x = bx ? L.i1[0] : L.i0[0], y = by ? L.i1[1] : L.i0[1], z = bz ? L.i1[2] : L.i0[2];
+      const double w = (bx ? L.w[0] : 1.0 - L.w[0]) * (by ? L.w[1] : 1.0 - L.w[1]) *
+                       (gi.dim == 3 ? (bz ? L.w[2] : 1.0 - L.w[2]) : 1.0);
+      const double v = (double)img[(z * gi.n[1] + y) * gi.n[0] + x];
+      int j = 0;
+      while (j < n && lab[j] != v) ++j;
+      if (j == n) {
+        lab[n] = v;
+        acc[n] = 0.0;
+        ++n;
+      }
+      acc[j] += w;
+    }
+    int best = 0;
+    for (int j = 1; j < n; ++j)
+      if (acc[j] > acc[best] || (acc[j] == acc[best] && lab[j] < lab[best])) best = j;
+    out[i] = (T)lab[best];
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Neighbourhood cross-correlation value and derivatives.
 //

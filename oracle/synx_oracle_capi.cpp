@@ -99,6 +99,10 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
                                T* out) {                                                             \
     warp_image_nearest(img, to_geom(gi), u, to_geom(gv), out);                                               \
   }                                                                                                  \
+  void oracle_warp_image_label_##SUF(const T* img, const synx_geom* gi, const T* u, const synx_geom* gv,   \
+                               T* out) {                                                             \
+    warp_image_label(img, to_geom(gi), u, to_geom(gv), out);                                               \
+  }                                                                                                  \
   double oracle_cc_##SUF(const T* F, const T* M, const synx_geom* g, int r, T* gF, T* gM, T* cc) {   \
     return cc_metric(F, M, to_geom(g), r, gF, gM, cc).value;                                         \
   }                                                                                                  \

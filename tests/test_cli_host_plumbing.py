@@ -64,6 +64,7 @@ def test_derived_initial_translation(host_cli, tmp_path):
     S.check_derived_initial_translation(host_cli["reg"], tmp_path)
 
 
+@pytest.mark.parametrize("interp", ["NearestNeighbor", "GenericLabel", "GenericLabel[Linear]"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_nearest_neighbor(host_cli, tmp_path, dim):
-    S.check_nearest_neighbor(host_cli["apply"], tmp_path, dim)
+def test_label_interpolation(host_cli, tmp_path, dim, interp):
+    S.check_label_interpolation(host_cli["apply"], tmp_path, dim, interp)

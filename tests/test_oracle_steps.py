@@ -138,6 +138,30 @@ def test_warp_nearest_matches_a_restatement(dim):
     want = np.where(inside, img[tuple(k[:, a] for a in reversed(range(dim)))], 0.0).reshape(gv.shape)
     np.testing.assert_array_equal(got, want)
     assert set(np.unique(got)) <= set(range(6))
+    # generic label interpolation: the label with the largest sum of linear corner weights (ties: the
+    # smaller label), restated per point with the linear interpolator's clamp-to-edge cell
+    got = O.warp_image(img, gi, u, gv, label=True, dtype=np.float64)
+    flat = got.ravel()
+    for q in np.flatnonzero(inside)[:400]:
+        cq = c[q]
+        f = np.floor(cq)
+        b = f.astype(int)
+        w = cq - f
+        lo = b.copy()
+        hi = b + 1
+        w = np.where(lo < 0, 0.0, w)
+        lo = np.maximum(lo, 0)
+        w = np.where(hi > np.asarray(gi.size) - 1, 0.0, w)
+        hi = np.minimum(hi, np.asarray(gi.size) - 1)
+        sums = {}
+        for corner in range(2 ** dim):
+            bits = [(corner >> a) & 1 for a in range(dim)]
+            k_ = [hi[a] if bits[a] else lo[a] for a in range(dim)]
+            wt = np.prod([w[a] if bits[a] else 1.0 - w[a] for a in range(dim)])
+            lab = float(img[tuple(k_[a] for a in reversed(range(dim)))])
+            sums[lab] = sums.get(lab, 0.0) + wt
+        best = max(sorted(sums), key=lambda L: sums[L])  # first maximum in increasing label order
+        assert flat[q] == best, (q, sums, flat[q])
 
 def test_warp_identity_and_integer_shift():
     rng = np.random.default_rng(4)

@@ -76,15 +76,16 @@ def test_warp_image(cuda, gi):
     assert bad.mean() < 1e-3, bad.sum()
 
 
+@pytest.mark.parametrize("mode", ["nearest", "label"])
 @pytest.mark.parametrize("gi", range(len(OBLIQUE)))
-def test_warp_image_nearest(cuda, gi):
+def test_warp_image_labels(cuda, gi, mode):
     gv = OBLIQUE[gi]
     gimg = other_grid(gv)
     img = np.random.default_rng(15 + gi).integers(0, 7, gimg.shape).astype(np.float32)
     u = field(gv.shape, 3.0, 4.0, 25 + gi)
-    ref = O.warp_image(img, gimg, u, gv, nearest=True)
+    ref = O.warp_image(img, gimg, u, gv, nearest=mode == "nearest", label=mode == "label")
     out = empty(gv.shape, cuda)
-    synx.warp_image(dev(img, cuda), gimg, dev(u, cuda), gv, out, nearest=True)
+    synx.warp_image(dev(img, cuda), gimg, dev(u, cuda), gv, out, nearest=mode == "nearest", label=mode == "label")
     # float vs double coordinates may round a tie or a rim point the other way
     bad = host(out) != ref
     assert bad.mean() < 1e-3, bad.sum()

@@ -235,14 +235,15 @@ REG = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("interp", ["NearestNeighbor", "GenericLabel[Linear]"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_nearest_neighbor_labels(exe, tmp_path, cuda, dim):
-    check_nearest_neighbor(exe, tmp_path, dim)
+def test_label_interpolation(exe, tmp_path, cuda, dim, interp):
+    check_label_interpolation(exe, tmp_path, dim, interp)
 
 
-def check_nearest_neighbor(exe, tmp_path, dim):
-    """-n NearestNeighbor through `-t field -t affine.mat`: the label image sampled at A(p + u(p)) with
-    ITK's nearest-neighbour rule; a point on a rounding tie may pick either voxel."""
+def check_label_interpolation(exe, tmp_path, dim, interp="NearestNeighbor"):
+    """-n NearestNeighbor / GenericLabel[Linear] through `-t field -t affine.mat`: the label image
+    sampled at A(p + u(p)); a point on a rounding tie may pick either label."""
     cs, parts = cases(dim)
     chain, gr, toks = cs["forward"]
     g = parts["g"]
@@ -253,11 +254,12 @@ def check_nearest_neighbor(exe, tmp_path, dim):
     labels = np.random.default_rng(95 + dim).integers(0, 9, gi.shape).astype(np.float32)
     nifti.write(tmp_path / "labels.nii.gz", labels, gi)
     r = run(exe, ["-d", str(dim), "-r", f"{tmp_path}/fixed.nii.gz", "-i", f"{tmp_path}/labels.nii.gz",
-                  "-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/A.mat", "-n", "NearestNeighbor",
+                  "-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/A.mat", "-n", interp,
                   "-o", f"{tmp_path}/o.nii.gz"])
     assert r.returncode == 0, r.stderr
     got, _ = nifti.read(tmp_path / "o.nii.gz", dim)
-    want = O.warp_image(labels, push_forward(gi, parts["A"].inverse()), parts["a"], g, nearest=True)
+    want = O.warp_image(labels, push_forward(gi, parts["A"].inverse()), parts["a"], g,
+                        nearest=interp == "NearestNeighbor", label=interp.startswith("GenericLabel"))
     assert set(np.unique(got)) <= set(range(9))
     bad = got != want
     assert bad.mean() < 2e-3, int(bad.sum())
