@@ -2,7 +2,6 @@
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 from ants_b200 import replicas
