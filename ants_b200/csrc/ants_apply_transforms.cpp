@@ -6,6 +6,7 @@
 // transforms before them (prefix0GenericAffine.mat).  Options follow
 // Examples/antsApplyTransforms.cxx:1063-1240:
 //   -d/--dimensionality 2|3      -i/--input image     -r/--reference-image image
+//   -e/--input-image-type 0|scalar (default) | 4|multichannel (each channel resampled in turn)
 //   -t/--transform file  (repeatable).  Order: a reference point is moved by the FIRST transform
 //       given, then by the second, and so on; the input is sampled where the last one puts it.
 //       This is the reference's order: its parser stores repeated options newest first
@@ -125,9 +126,12 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   };
   const int dim = std::atoi(one("dimensionality", "3").c_str());
   if (dim != 2 && dim != 3) throw std::runtime_error("--dimensionality must be 2 or 3");
-  if (opt.count("input-image-type") && one("input-image-type", "0") != "0" &&
-      lower(one("input-image-type", "scalar")) != "scalar")
-    throw std::runtime_error("only scalar input images are supported");
+  // input image type (:1053-1069): scalar, or multichannel, whose channels are resampled one by one
+  // (:516-535, :903-981); vector, tensor and time-series inputs are rejected
+  const std::string itype = lower(one("input-image-type", "0"));
+  const bool multichannel = itype == "4" || itype == "multichannel";
+  if (!(itype == "0" || itype == "scalar" || multichannel))
+    throw std::runtime_error("only scalar (0) and multichannel (4) input images are supported");
   const OptionCall icall = parse_call(one("interpolation", "Linear"));
   const std::string interp = lower(icall.name);
   if (interp != "linear" && interp != "nearestneighbor" && interp != "genericlabel")
@@ -291,7 +295,9 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   }
 
   nifti::Image in = nifti::read(one("input", ""));
-  if (in.components != 1) throw std::runtime_error("the input must be a scalar image");
+  if (!multichannel && in.components != 1)
+    throw std::runtime_error("the input must be a scalar image (-e 4 resamples a multichannel image)");
+  const int channels = in.components;
   synx_geom gi = to_geom(in, dim);
   if (tail_begin < chain.size()) {
     // sampling at q reads the input at L_post(q): the input's grid pulled back by L_post
@@ -305,14 +311,16 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     for (float& x : in.data) x -= defval;
   const long long Ni = in.voxels();
   DeviceBuffer di((size_t)Ni), dout((size_t)N);
-  CLI_CK(cudaMemcpy(di.p, in.data.data(), 4 * (size_t)Ni, cudaMemcpyHostToDevice));
-  if (label) step_ok(synx_warp_image_label(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_label");
-  else if (nearest) step_ok(synx_warp_image_nearest(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_nearest");
-  else step_ok(synx_warp_image(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image");
   nifti::Image res = ref;
-  res.components = 1;
-  res.data.resize((size_t)N);
-  CLI_CK(cudaMemcpy(res.data.data(), dout.p, 4 * (size_t)N, cudaMemcpyDeviceToHost));
+  res.components = channels;
+  res.data.resize((size_t)N * channels);
+  for (int c = 0; c < channels; ++c) {  // one channel (component plane) at a time
+    CLI_CK(cudaMemcpy(di.p, in.data.data() + (size_t)c * Ni, 4 * (size_t)Ni, cudaMemcpyHostToDevice));
+    if (label) step_ok(synx_warp_image_label(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_label");
+    else if (nearest) step_ok(synx_warp_image_nearest(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image_nearest");
+    else step_ok(synx_warp_image(di.p, &gi, w.p, &ge, dout.p, nullptr), "synx_warp_image");
+    CLI_CK(cudaMemcpy(res.data.data() + (size_t)c * N, dout.p, 4 * (size_t)N, cudaMemcpyDeviceToHost));
+  }
   if (defval != 0.0f)
     for (float& x : res.data) x += defval;
   nifti::write(out_path, res);

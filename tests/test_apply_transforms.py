@@ -33,6 +33,7 @@ def run(exe, args):
     (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz", "-t", "composite.h5"], "not supported"),
     (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz", "-n", "BSpline[3]"], "NearestNeighbor"),
     (["-d", "5", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz"], "dimensionality"),
+    (["-d", "3", "-e", "2", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz"], "multichannel (4)"),
     (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "Linear[x.mat,0]"], "not supported"),
     (["-d", "3", "-i", "a.nii.gz", "-r", "/nonexistent/r.nii.gz", "-o", "x.nii.gz"], "cannot open"),
 ])

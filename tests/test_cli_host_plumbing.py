@@ -68,3 +68,7 @@ def test_derived_initial_translation(host_cli, tmp_path):
 @pytest.mark.parametrize("dim", [2, 3])
 def test_label_interpolation(host_cli, tmp_path, dim, interp):
     S.check_label_interpolation(host_cli["apply"], tmp_path, dim, interp)
+
+
+def test_multichannel(host_cli, tmp_path):
+    S.check_multichannel(host_cli["apply"], tmp_path)

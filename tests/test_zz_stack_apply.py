@@ -235,6 +235,38 @@ REG = os.path.join(ROOT, "ants_b200", "antsRegistrationSyN_b200")
 
 
 @pytest.mark.gpu
+def test_multichannel_input(exe, tmp_path, cuda):
+    check_multichannel(exe, tmp_path)
+
+
+def check_multichannel(exe, tmp_path, dim=3):
+    """-e 4: every channel of a multichannel image resampled through `-t field -t affine.mat`, written
+    back as a multichannel image on the reference grid."""
+    cs, parts = cases(dim)
+    g = parts["g"]
+    nifti.write(tmp_path / "a.nii.gz", np.ascontiguousarray(np.moveaxis(parts["a"], 0, -1)), g, vector=True)
+    parts["A"].write_mat(tmp_path / "A.mat")
+    nifti.write(tmp_path / "fixed.nii.gz", np.zeros(g.shape, np.float32), g)
+    gi = Geom((40, 36, 32), (0.8,) * 3, (-3.0,) * 3)
+    chans = np.random.default_rng(97).uniform(0, 1, gi.shape + (3,)).astype(np.float32)
+    nifti.write(tmp_path / "mc.nii.gz", chans, gi, vector=True)
+    r = run(exe, ["-d", "3", "-e", "4", "-r", f"{tmp_path}/fixed.nii.gz", "-i", f"{tmp_path}/mc.nii.gz",
+                  "-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/A.mat", "-o", f"{tmp_path}/o.nii.gz"])
+    assert r.returncode == 0, r.stderr
+    got, go = nifti.read(tmp_path / "o.nii.gz", 3)
+    assert got.shape == g.shape + (3,) and go.size == g.size
+    gfold = push_forward(gi, parts["A"].inverse())
+    for c in range(3):
+        want = O.warp_image(np.ascontiguousarray(chans[..., c]), gfold, parts["a"], g)
+        bad = np.abs(got[..., c] - want) > 1e-4
+        assert bad.mean() < 2e-3, (c, int(bad.sum()))
+    # a multichannel image without -e 4 is refused
+    r = run(exe, ["-d", "3", "-r", f"{tmp_path}/fixed.nii.gz", "-i", f"{tmp_path}/mc.nii.gz",
+                  "-t", f"{tmp_path}/a.nii.gz", "-o", f"{tmp_path}/o2.nii.gz"])
+    assert r.returncode == 1 and "-e 4" in r.stderr
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("interp", ["NearestNeighbor", "GenericLabel[Linear]"])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_label_interpolation(exe, tmp_path, cuda, dim, interp):
