@@ -6,7 +6,8 @@
 // transforms before them (prefix0GenericAffine.mat).  Options follow
 // Examples/antsApplyTransforms.cxx:1063-1240:
 //   -d/--dimensionality 2|3      -i/--input image     -r/--reference-image image
-//   -e/--input-image-type 0|scalar (default) | 4|multichannel (each channel resampled in turn)
+//   -e/--input-image-type 0|scalar (default) | 3|time-series | 4|multichannel (each volume or channel
+//       resampled in turn)
 //   -t/--transform file  (repeatable).  Order: a reference point is moved by the FIRST transform
 //       given, then by the second, and so on; the input is sampled where the last one puts it.
 //       This is the reference's order: its parser stores repeated options newest first
@@ -126,12 +127,14 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   };
   const int dim = std::atoi(one("dimensionality", "3").c_str());
   if (dim != 2 && dim != 3) throw std::runtime_error("--dimensionality must be 2 or 3");
-  // input image type (:1053-1069): scalar, or multichannel, whose channels are resampled one by one
-  // (:516-535, :903-981); vector, tensor and time-series inputs are rejected
+  // input image type (:1053-1069): scalar, or multichannel / time series, whose channels or volumes
+  // are resampled one by one (:516-535, :903-981); vector and tensor inputs are rejected
   const std::string itype = lower(one("input-image-type", "0"));
   const bool multichannel = itype == "4" || itype == "multichannel";
-  if (!(itype == "0" || itype == "scalar" || multichannel))
-    throw std::runtime_error("only scalar (0) and multichannel (4) input images are supported");
+  const bool series = itype == "3" || itype == "time-series";
+  if (!(itype == "0" || itype == "scalar" || multichannel || series))
+    throw std::runtime_error("only scalar (0), time-series (3) and multichannel (4) input images are supported");
+  if (series && dim != 3) throw std::runtime_error("time-series input (-e 3) needs -d 3");
   const OptionCall icall = parse_call(one("interpolation", "Linear"));
   const std::string interp = lower(icall.name);
   if (interp != "linear" && interp != "nearestneighbor" && interp != "genericlabel")
@@ -239,7 +242,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       note = c.invert ? " (linear, inverse)" : " (linear)";
     } else {
       const nifti::Image f = nifti::read(c.file);
-      if (f.components != dim || f.dim != dim)
+      if (f.components != dim || f.dim != dim || f.time_series)
         throw std::runtime_error("'" + c.file + "' is not a " + std::to_string(dim) + "-D displacement field");
       const synx_geom gf = to_geom(f, dim);
       const long long Nf = f.voxels();
@@ -295,8 +298,10 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   }
 
   nifti::Image in = nifti::read(one("input", ""));
-  if (!multichannel && in.components != 1)
-    throw std::runtime_error("the input must be a scalar image (-e 4 resamples a multichannel image)");
+  if (series ? (in.components > 1 && !in.time_series) : multichannel ? in.time_series : in.components != 1)
+    throw std::runtime_error(series ? "the input is not a time series (-e 3)"
+                             : multichannel ? "the input is a time series (use -e 3)"
+                             : "the input must be a scalar image (-e 3 resamples a time series, -e 4 a multichannel image)");
   const int channels = in.components;
   synx_geom gi = to_geom(in, dim);
   if (tail_begin < chain.size()) {
@@ -313,6 +318,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   DeviceBuffer di((size_t)Ni), dout((size_t)N);
   nifti::Image res = ref;
   res.components = channels;
+  res.time_series = series;
+  res.time_step = in.time_step;
   res.data.resize((size_t)N * channels);
   for (int c = 0; c < channels; ++c) {  // one channel (component plane) at a time
     CLI_CK(cudaMemcpy(di.p, in.data.data() + (size_t)c * Ni, 4 * (size_t)Ni, cudaMemcpyHostToDevice));

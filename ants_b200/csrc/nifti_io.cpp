@@ -129,7 +129,12 @@ Image read(const std::string& path) {
   img.size[2] = n[2];
   img.components = (int)(n[4]);
   img.dim = (n[2] > 1) ? 3 : 2;
-  if (n[3] != 1) throw std::runtime_error(path + ": time series are not supported");
+  if (n[3] != 1) {  // a 4-D series: its volumes are held as component planes
+    if (n[4] != 1) throw std::runtime_error(path + ": time series of vector images are not supported");
+    img.time_series = true;
+    img.components = (int)n[3];
+    img.time_step = h.pixdim[4] > 0 ? h.pixdim[4] : 1.0;
+  }
   if (n[5] != 1 || n[6] != 1) throw std::runtime_error(path + ": dimensions 6 and 7 are not supported");
   for (int k = 0; k < 3; ++k) img.spacing[k] = h.pixdim[k + 1] > 0 ? h.pixdim[k + 1] : 1.0;
   // RAS affine
@@ -224,20 +229,22 @@ void write(const std::string& path, const Image& img) {
   std::memset(&h, 0, sizeof(h));
   h.sizeof_hdr = 348;
   h.regular = 'r';
-  const bool vec = img.components > 1;
-  h.dim[0] = vec ? 5 : (img.dim == 3 ? 3 : 2);
+  const bool series = img.time_series;
+  const bool vec = img.components > 1 && !series;
+  h.dim[0] = series ? 4 : vec ? 5 : (img.dim == 3 ? 3 : 2);
   h.dim[1] = (int16_t)img.size[0];
   h.dim[2] = (int16_t)img.size[1];
   h.dim[3] = (int16_t)(img.dim == 3 ? img.size[2] : 1);
-  h.dim[4] = 1;
-  h.dim[5] = (int16_t)img.components;
+  h.dim[4] = (int16_t)(series ? img.components : 1);
+  h.dim[5] = (int16_t)(series ? 1 : img.components);
   h.dim[6] = h.dim[7] = 1;
   if (vec) h.intent_code = 1007;  // NIFTI_INTENT_VECTOR
   h.datatype = 16;
   h.bitpix = 32;
   h.pixdim[0] = 1.0f;
   for (int k = 0; k < 3; ++k) h.pixdim[k + 1] = (float)(k < img.dim ? img.spacing[k] : 1.0);
-  h.pixdim[4] = h.pixdim[5] = h.pixdim[6] = h.pixdim[7] = 1.0f;
+  h.pixdim[4] = (float)(series ? img.time_step : 1.0);
+  h.pixdim[5] = h.pixdim[6] = h.pixdim[7] = 1.0f;
   h.vox_offset = 352.0f;
   h.scl_slope = 1.0f;
   h.xyzt_units = 2 | 8;  // mm, s

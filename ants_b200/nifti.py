@@ -22,11 +22,17 @@ def _open(path, mode):
     return gzip.open(path, mode) if str(path).endswith(".gz") else open(path, mode)
 
 
-def write(path, data: np.ndarray, geom: Geom, vector: bool = False) -> None:
+def write(path, data: np.ndarray, geom: Geom, vector: bool = False, time_series: bool = False,
+          time_step: float = 1.0) -> None:
     """data: scalar image in numpy order (z, y, x) / (y, x); or, with vector=True, a field in
-    interleaved layout grid.shape + (dim,) (the synx/ITK buffer layout)."""
+    interleaved layout grid.shape + (dim,) (the synx/ITK buffer layout); or, with time_series=True,
+    a 3-D series grid.shape + (volumes,) written as a 4-D image."""
     d = geom.dim
-    if vector:
+    if time_series:
+        planes = np.moveaxis(np.asarray(data, np.float32), -1, 0)  # volume slowest in the file
+        dims = [4, geom.size[0], geom.size[1], geom.size[2] if d == 3 else 1, planes.shape[0], 1, 1, 1]
+        intent = 0
+    elif vector:
         planes = np.moveaxis(np.asarray(data, np.float32), -1, 0)  # component slowest in the file
         dims = [5, geom.size[0], geom.size[1], geom.size[2] if d == 3 else 1, 1, d, 1, 1]
         intent = 1007
@@ -42,7 +48,7 @@ def write(path, data: np.ndarray, geom: Geom, vector: bool = False) -> None:
     A[:, :3] = D * np.array(sp)[None, :]
     A[:, 3] = org
     A[:2] *= -1.0  # LPS -> RAS
-    pixdim = [1.0] + sp + [1.0] * 4
+    pixdim = [1.0] + sp + [float(time_step) if time_series else 1.0] + [1.0] * 3
     hdr = _HDR.pack(348, b"", b"", 0, 0, b"r", 0, *dims, 0.0, 0.0, 0.0, intent, 16, 32, 0, *pixdim, 352.0, 1.0, 0.0,
                     0, b"\0", bytes([10]), 0.0, 0.0, 0.0, 0.0, 0, 0, b"synx", b"", 0, 1, 0.0, 0.0, 0.0,
                     A[0, 3], A[1, 3], A[2, 3], *A[0], *A[1], *A[2], b"", b"n+1\0")
@@ -54,7 +60,7 @@ def write(path, data: np.ndarray, geom: Geom, vector: bool = False) -> None:
 
 def read(path, dim: int | None = None):
     """Returns (array, Geom).  Scalar images come back in numpy order (z, y, x) / (y, x); vector
-    images in interleaved layout grid.shape + (components,)."""
+    images in interleaved layout grid.shape + (components,); 4-D series as grid.shape + (volumes,)."""
     with _open(path, "rb") as fh:
         raw = fh.read()
     f = _HDR.unpack(raw[:348])
@@ -69,7 +75,7 @@ def read(path, dim: int | None = None):
     nd = dims[0]
     n = [max(int(x), 1) for x in dims[1:nd + 1]] + [1] * (7 - nd)
     d = dim or (3 if n[2] > 1 else 2)
-    comps = n[4]
+    comps = n[4] * n[3]  # vector components, or the volumes of a 4-D series
     if sform_code > 0:
         A = srow.copy()
     else:

@@ -72,3 +72,7 @@ def test_label_interpolation(host_cli, tmp_path, dim, interp):
 
 def test_multichannel(host_cli, tmp_path):
     S.check_multichannel(host_cli["apply"], tmp_path)
+
+
+def test_time_series(host_cli, tmp_path):
+    S.check_time_series(host_cli["apply"], tmp_path)

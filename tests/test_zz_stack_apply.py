@@ -239,6 +239,45 @@ def test_multichannel_input(exe, tmp_path, cuda):
     check_multichannel(exe, tmp_path)
 
 
+@pytest.mark.gpu
+def test_time_series_input(exe, tmp_path, cuda):
+    check_time_series(exe, tmp_path)
+
+
+def check_time_series(exe, tmp_path):
+    """-e 3: every volume of a 4-D series resampled through `-t field -t affine.mat`, written back as a
+    4-D series on the reference grid with the input's time step."""
+    import struct
+    cs, parts = cases(3)
+    g = parts["g"]
+    nifti.write(tmp_path / "a.nii.gz", np.ascontiguousarray(np.moveaxis(parts["a"], 0, -1)), g, vector=True)
+    parts["A"].write_mat(tmp_path / "A.mat")
+    nifti.write(tmp_path / "fixed.nii.gz", np.zeros(g.shape, np.float32), g)
+    gi = Geom((40, 36, 32), (0.8,) * 3, (-3.0,) * 3)
+    vols = np.random.default_rng(98).uniform(0, 1, gi.shape + (3,)).astype(np.float32)
+    nifti.write(tmp_path / "ts.nii", vols, gi, time_series=True, time_step=2.5)
+    r = run(exe, ["-d", "3", "-e", "3", "-r", f"{tmp_path}/fixed.nii.gz", "-i", f"{tmp_path}/ts.nii",
+                  "-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/A.mat", "-o", f"{tmp_path}/o.nii"])
+    assert r.returncode == 0, r.stderr
+    raw = (tmp_path / "o.nii").read_bytes()
+    dims = struct.unpack("<8h", raw[40:56])
+    assert dims[0] == 4 and dims[4] == 3 and dims[5] == 1
+    assert struct.unpack("<f", raw[92:96])[0] == 2.5  # pixdim[4]
+    got, go = nifti.read(tmp_path / "o.nii", 3)
+    assert got.shape == g.shape + (3,) and go.size == g.size
+    gfold = push_forward(gi, parts["A"].inverse())
+    for t in range(3):
+        want = O.warp_image(np.ascontiguousarray(vols[..., t]), gfold, parts["a"], g)
+        bad = np.abs(got[..., t] - want) > 1e-4
+        assert bad.mean() < 2e-3, (t, int(bad.sum()))
+    base = ["-r", f"{tmp_path}/fixed.nii.gz", "-t", f"{tmp_path}/a.nii.gz", "-o", f"{tmp_path}/x.nii"]
+    for args, needle in ((["-d", "3", "-i", f"{tmp_path}/ts.nii"], "-e 3"),
+                         (["-d", "3", "-e", "4", "-i", f"{tmp_path}/ts.nii"], "use -e 3"),
+                         (["-d", "2", "-e", "3", "-i", f"{tmp_path}/ts.nii"], "needs -d 3")):
+        r = run(exe, args + base)
+        assert r.returncode == 1 and needle in r.stderr, (args, r.stderr)
+
+
 def check_multichannel(exe, tmp_path, dim=3):
     """-e 4: every channel of a multichannel image resampled through `-t field -t affine.mat`, written
     back as a multichannel image on the reference grid."""
