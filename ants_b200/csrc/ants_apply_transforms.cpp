@@ -26,6 +26,7 @@
 //   -f/--default-value v (0): value where the point maps outside the input image
 //   -o/--output warped | [collapsed,1] | DisplacementField[collapsed]  (the collapsed form writes
 //       the single displacement field equivalent to the stack, on the reference grid, :1115-1131)
+//   -u/--output-data-type char|uchar|short|int|float|double|default (a cast of the float result)
 //   --float 0|1 (computation is float32 either way)   -v/--verbose 0|1   --gpu N (not a reference option)
 //
 // GPU path.  The chain of transforms, in application order, is split into a leading run of
@@ -147,6 +148,13 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
   const int gpu = std::atoi(one("gpu", "0").c_str());
   const float defval = (float)std::atof(one("default-value", "0").c_str());
+  // output pixel type of the warped image (:1168-1181, :1460-1520): a cast of the float result;
+  // "default" is the computation type, float here
+  const std::map<std::string, int> out_types = {{"char", 256}, {"uchar", 2}, {"short", 4},  {"int", 8},
+                                                {"float", 16}, {"double", 64}, {"default", 16}};
+  const std::string out_type = lower(one("output-data-type", "default"));
+  if (!out_types.count(out_type))
+    throw std::runtime_error("--output-data-type must be char, uchar, short, int, float, double or default");
 
   // output form
   OptionCall o = parse_call(one("output", ""));
@@ -317,6 +325,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const long long Ni = in.voxels();
   DeviceBuffer di((size_t)Ni), dout((size_t)N);
   nifti::Image res = ref;
+  res.out_datatype = out_types.at(out_type);
   res.components = channels;
   res.time_series = series;
   res.time_step = in.time_step;

@@ -239,8 +239,16 @@ void write(const std::string& path, const Image& img) {
   h.dim[5] = (int16_t)(series ? 1 : img.components);
   h.dim[6] = h.dim[7] = 1;
   if (vec) h.intent_code = 1007;  // NIFTI_INTENT_VECTOR
-  h.datatype = 16;
-  h.bitpix = 32;
+  int out_bytes = 0;
+  switch (img.out_datatype) {
+    case 2: case 256: out_bytes = 1; break;
+    case 4: out_bytes = 2; break;
+    case 8: case 16: out_bytes = 4; break;
+    case 64: out_bytes = 8; break;
+    default: throw std::runtime_error(path + ": unsupported output datatype " + std::to_string(img.out_datatype));
+  }
+  h.datatype = (int16_t)img.out_datatype;
+  h.bitpix = (int16_t)(8 * out_bytes);
   h.pixdim[0] = 1.0f;
   for (int k = 0; k < 3; ++k) h.pixdim[k + 1] = (float)(k < img.dim ? img.spacing[k] : 1.0);
   h.pixdim[4] = (float)(series ? img.time_step : 1.0);
@@ -325,8 +333,31 @@ void write(const std::string& path, const Image& img) {
   if (!f) throw std::runtime_error("cannot write " + path);
   const char ext[4] = {0, 0, 0, 0};
   bool ok = gzwrite(f, &h, sizeof(h)) == (int)sizeof(h) && gzwrite(f, ext, 4) == 4;
+  // the payload in the output type: floats as they are, doubles widened, integers as a C++ cast of the
+  // value truncated toward zero (the reference's CastImageFilter), NaN as 0
+  std::vector<unsigned char> conv;
   const unsigned char* p = reinterpret_cast<const unsigned char*>(img.data.data());
-  size_t left = img.data.size() * sizeof(float);
+  if (img.out_datatype != 16) {
+    conv.resize(img.data.size() * (size_t)out_bytes);
+    for (size_t i = 0; i < img.data.size(); ++i) {
+      const float v = img.data[i];
+      unsigned char* q = conv.data() + i * (size_t)out_bytes;
+      if (img.out_datatype == 64) {
+        const double d = v;
+        std::memcpy(q, &d, 8);
+        continue;
+      }
+      const long long t = std::isfinite(v) && std::fabs(v) < 9.0e18f ? (long long)std::trunc(v) : 0;
+      switch (img.out_datatype) {
+        case 2: { const uint8_t x = (uint8_t)t; std::memcpy(q, &x, 1); break; }
+        case 256: { const int8_t x = (int8_t)t; std::memcpy(q, &x, 1); break; }
+        case 4: { const int16_t x = (int16_t)t; std::memcpy(q, &x, 2); break; }
+        default: { const int32_t x = (int32_t)t; std::memcpy(q, &x, 4); break; }
+      }
+    }
+    p = conv.data();
+  }
+  size_t left = img.data.size() * (size_t)out_bytes;
   while (ok && left > 0) {
     const unsigned chunk = (unsigned)std::min<size_t>(left, 1u << 30);
     ok = gzwrite(f, p, chunk) == (int)chunk;

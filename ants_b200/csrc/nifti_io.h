@@ -17,6 +17,8 @@ struct Image {
   double origin[3] = {0, 0, 0};     // LPS
   double direction[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};  // LPS, row-major
   std::vector<float> data;     // scalar: x fastest; vector: component planes (component slowest)
+  int out_datatype = 16;       // NIfTI datatype write() stores (reading leaves it float32): 2 uchar,
+                               // 4 int16, 8 int32, 16 float32, 64 float64, 256 int8
   bool time_series = false;    // a 4-D series: `components` volumes along dim[4] (stored like planes)
   double time_step = 1.0;      // pixdim[4] of a series
   long long voxels() const { return size[0] * size[1] * size[2]; }

@@ -76,3 +76,7 @@ def test_multichannel(host_cli, tmp_path):
 
 def test_time_series(host_cli, tmp_path):
     S.check_time_series(host_cli["apply"], tmp_path)
+
+
+def test_output_types(host_cli, tmp_path):
+    S.check_output_types(host_cli["apply"], tmp_path)

@@ -244,6 +244,37 @@ def test_time_series_input(exe, tmp_path, cuda):
     check_time_series(exe, tmp_path)
 
 
+@pytest.mark.gpu
+def test_output_data_types(exe, tmp_path, cuda):
+    check_output_types(exe, tmp_path)
+
+
+def check_output_types(exe, tmp_path):
+    """-u: the warped image stored as a cast of the float result (truncation toward zero for integer
+    types), with the matching NIfTI datatype code."""
+    import struct
+    g = Geom((30, 28))
+    img = (np.random.default_rng(99).uniform(-40, 300, g.shape)).astype(np.float32)
+    u = np.ascontiguousarray(np.moveaxis(field_on(g, 4.0, 2.0, 99), 0, -1))
+    nifti.write(tmp_path / "in.nii.gz", img, g)
+    nifti.write(tmp_path / "u.nii.gz", u, g, vector=True)
+    base = ["-d", "2", "-i", f"{tmp_path}/in.nii.gz", "-r", f"{tmp_path}/in.nii.gz", "-t", f"{tmp_path}/u.nii.gz"]
+    r = run(exe, base + ["-o", f"{tmp_path}/f.nii"])
+    assert r.returncode == 0, r.stderr
+    ref, _ = nifti.read(tmp_path / "f.nii", 2)
+    for name, code, cast in (("char", 256, np.int8), ("uchar", 2, np.uint8), ("short", 4, np.int16),
+                             ("int", 8, np.int32), ("double", 64, np.float64), ("default", 16, np.float32)):
+        r = run(exe, base + ["-u", name, "-o", f"{tmp_path}/{name}.nii"])
+        assert r.returncode == 0, (name, r.stderr)
+        raw = (tmp_path / f"{name}.nii").read_bytes()
+        assert struct.unpack("<h", raw[70:72])[0] == code, name  # datatype
+        got, _ = nifti.read(tmp_path / f"{name}.nii", 2)
+        want = ref.astype(np.float64) if cast in (np.float64, np.float32) else np.trunc(ref).astype(np.int64).astype(cast)
+        np.testing.assert_array_equal(got, np.asarray(want, np.float32), err_msg=name)
+    r = run(exe, base + ["-u", "long", "-o", f"{tmp_path}/x.nii"])
+    assert r.returncode == 1 and "output-data-type" in r.stderr
+
+
 def check_time_series(exe, tmp_path):
     """-e 3: every volume of a 4-D series resampled through `-t field -t affine.mat`, written back as a
     4-D series on the reference grid with the input's time step."""
