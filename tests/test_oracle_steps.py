@@ -318,3 +318,33 @@ def test_syn_fp32_tracks_fp64():
     np.testing.assert_allclose(m32, m64, atol=2e-3)
     # registration improves the similarity within each level
     assert m64[7] < m64[0] and m64[-1] < m64[8]
+
+
+
+def test_convergence_monitor_matches_a_restatement():
+    """The per-iteration convergence values the oracle logs, recomputed from its logged metrics: the
+    last `window` energies over the level's running sum of |energy|, fitted by one level of
+    multilevel B-spline approximation with a single-span linear B-spline on [0, 1] (each point
+    proposes phi_c = w_c z / sum w^2 for both control points; each control point is the w_c^2-weighted
+    mean of its proposals), value = minus the slope c1 - c0; infinite before a full window."""
+    from ants_b200 import phantoms
+    from ants_b200.synx import SyNParams
+    f, m = phantoms.pair_2d((48, 44), seed=12)
+    g = Geom((48, 44))
+    window = 5
+    P = SyNParams(dim=2, cc_radius=2, iterations=(9, 7), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0),
+                  convergence_threshold=-1.0, convergence_window=window)
+    _, _, _, log = O.syn_register(f, g, m, g, P, dtype=np.float64)
+    for level in (0, 1):
+        rows = [r for r in log if r["level"] == level]
+        energies = np.array([r["metric"] for r in rows])
+        for k, r in enumerate(rows):
+            if k + 1 < window:
+                assert r["convergence"] > 1e300
+                continue
+            z = energies[k + 1 - window:k + 1] / np.abs(energies[:k + 1]).sum()
+            t = np.linspace(0.0, 1.0, window)
+            w = np.stack([1.0 - t, t])                      # B-spline weights of both control points
+            proposals = w * z / (w ** 2).sum(0)             # each point's proposal for each control point
+            c = (w ** 2 * proposals).sum(1) / (w ** 2).sum(1)
+            assert abs(r["convergence"] - (-(c[1] - c[0]))) <= 1e-12 * max(1.0, abs(r["convergence"])), (level, k)
