@@ -348,3 +348,56 @@ def test_convergence_monitor_matches_a_restatement():
             proposals = w * z / (w ** 2).sum(0)             # each point's proposal for each control point
             c = (w ** 2 * proposals).sum(1) / (w ** 2).sum(1)
             assert abs(r["convergence"] - (-(c[1] - c[0]))) <= 1e-12 * max(1.0, abs(r["convergence"])), (level, k)
+
+
+
+def _lerp_planes(field, g, P):
+    """ITK's linear interpolation of component planes `field` on grid `g` at physical points P
+    (..., dim): 0 outside [-0.5, n - 0.5) per axis, clamp-to-edge inside the rim."""
+    dim = g.dim
+    c = np.linalg.solve(g.direction * np.asarray(g.spacing), (P - np.asarray(g.origin)).reshape(-1, dim).T).T
+    n = np.asarray(g.size)
+    inside = np.all((c >= -0.5) & (c < n - 0.5), axis=1)
+    f = np.floor(c)
+    lo = f.astype(int)
+    w = c - f
+    w = np.where(lo < 0, 0.0, w)
+    lo = np.clip(lo, 0, n - 1)  # inside the buffer lo <= n - 1 already; outside points are zeroed below
+    hi = lo + 1
+    w = np.where(hi > n - 1, 0.0, w)
+    hi = np.minimum(hi, n - 1)
+    out = np.zeros((field.shape[0], c.shape[0]))
+    for corner in range(2 ** dim):
+        bits = [(corner >> a) & 1 for a in range(dim)]
+        k = [np.where(bits[a], hi[:, a], lo[:, a]) for a in range(dim)]
+        wt = np.prod([w[:, a] if bits[a] else 1.0 - w[:, a] for a in range(dim)], axis=0)
+        for comp in range(field.shape[0]):
+            out[comp] += wt * field[comp][tuple(k[a] for a in reversed(range(dim)))]
+    out[:, ~inside] = 0.0
+    return out.reshape((field.shape[0],) + P.shape[:-1])
+
+
+def _points(g):
+    axes = np.meshgrid(*[np.arange(n) for n in reversed(g.size)], indexing="ij")
+    idx = np.stack(list(reversed(axes)), -1).astype(np.float64)
+    return np.asarray(g.origin) + (idx * np.asarray(g.spacing)) @ g.direction.T
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_compose_order_and_scaling_match_a_restatement(dim):
+    """compose(d, w) = w + s * d(x + w) with d interpolated at the displaced point (0 outside), on an
+    anisotropic grid with non-commuting random fields; scale_update returns u * eta / max ||u / h||."""
+    from ants_b200 import phantoms
+    rng = np.random.default_rng(60 + dim)
+    g = Geom((15, 12, 10)[:dim], (1.2, 0.9, 1.1)[:dim], (3.0, -2.0, 1.0)[:dim])
+    d = np.moveaxis(phantoms.smooth_field(g.shape, 2.0, 2.5, rng), -1, 0).astype(np.float64)
+    w = np.moveaxis(phantoms.smooth_field(g.shape, 3.0, 3.0, rng), -1, 0).astype(np.float64)
+    got = O.compose(d, w, g, scale=0.7, dtype=np.float64)
+    P = _points(g) + np.moveaxis(w, 0, -1)
+    want = w + 0.7 * _lerp_planes(d, g, P)
+    np.testing.assert_allclose(got, want, atol=1e-12)
+    assert np.abs(O.compose(w, d, g, dtype=np.float64) - O.compose(d, w, g, dtype=np.float64)).max() > 0.1
+    scaled, mx = O.scale_update(d, g, 0.25, dtype=np.float64)
+    norm = np.sqrt(((d / np.asarray(g.spacing).reshape((-1,) + (1,) * dim)) ** 2).sum(0)).max()
+    assert abs(mx - norm) <= 1e-12 * norm
+    np.testing.assert_allclose(scaled, d * (0.25 / norm), atol=1e-12)
