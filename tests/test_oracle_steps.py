@@ -401,3 +401,43 @@ def test_compose_order_and_scaling_match_a_restatement(dim):
     norm = np.sqrt(((d / np.asarray(g.spacing).reshape((-1,) + (1,) * dim)) ** 2).sum(0)).max()
     assert abs(mx - norm) <= 1e-12 * norm
     np.testing.assert_allclose(scaled, d * (0.25 / norm), atol=1e-12)
+
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_inversion_matches_a_restatement(dim):
+    """Fixed-point inversion: E = psi + phi(x + psi); stop when max ||E/h|| <= max_tol or its mean <=
+    mean_tol (tested before each sub-iteration, so the update after the last statistics is applied);
+    step psi -= eps * E with eps = 0.75 on the first sub-iteration and 0.5 after, each voxel's step
+    clamped to eps * max ||E/h||, boundary voxels held at 0."""
+    from ants_b200 import phantoms
+    rng = np.random.default_rng(70 + dim)
+    g = Geom((14, 12, 10)[:dim], (1.1, 0.9, 1.2)[:dim], (1.0, 2.0, -1.0)[:dim])
+    phi = np.moveaxis(phantoms.smooth_field(g.shape, 2.5, 2.0, rng), -1, 0).astype(np.float64)
+    sp = np.asarray(g.spacing).reshape((-1,) + (1,) * dim)
+    P = _points(g)
+    edge = np.zeros(g.shape, bool)
+    for a in range(dim):
+        sl = [slice(None)] * dim
+        sl[a] = 0
+        edge[tuple(sl)] = True
+        sl[a] = -1
+        edge[tuple(sl)] = True
+    for psi0, max_iter in ((np.zeros_like(phi), 20), (-0.5 * phi, 4)):
+        psi = psi0.copy()
+        mean_e = max_e = np.inf
+        it = 0
+        while it < max_iter and max_e > 0.1 and mean_e > 0.001:
+            it += 1
+            E = psi + _lerp_planes(phi, g, P + np.moveaxis(psi, 0, -1))
+            nrm = np.sqrt(((E / sp) ** 2).sum(0))
+            mean_e, max_e = nrm.mean(), nrm.max()
+            eps = 0.75 if it == 1 else 0.5
+            lim = eps * max_e
+            f = np.where(nrm > lim, lim / np.where(nrm > 0, nrm, 1.0), 1.0)
+            psi = psi - E * f * eps
+            psi[:, edge] = 0.0
+        got, it_got, mean_got, max_got = O.invert(phi, psi0, g, max_iter=max_iter, dtype=np.float64)
+        assert it_got == it
+        np.testing.assert_allclose(got, psi, atol=1e-10)
+        assert abs(mean_got - mean_e) < 1e-12 and abs(max_got - max_e) < 1e-12
