@@ -441,3 +441,32 @@ def test_inversion_matches_a_restatement(dim):
         assert it_got == it
         np.testing.assert_allclose(got, psi, atol=1e-10)
         assert abs(mean_got - mean_e) < 1e-12 and abs(max_got - max_e) < 1e-12
+
+
+
+@pytest.mark.parametrize("mm", [False, True])
+def test_pyramid_smoothing_matches_a_restatement(mm):
+    """Level smoothing of an image: per axis, the discrete Gaussian kernel of variance sigma^2 (in
+    voxels, or sigma^2 / h^2 for mm), max error 0.01 and max width 32, applied with replicated edges
+    (numpy restatement over the oracle's kernel, which the Bessel golden vectors pin)."""
+    rng = np.random.default_rng(80 + int(mm))
+    g = Geom((23, 19, 17), (1.1, 0.8, 1.4))
+    img = rng.uniform(0, 1, g.shape)
+    sigma = 1.7
+    got = O.smooth_image(img, g, sigma, mm=mm, dtype=np.float64)
+    want = img.copy()
+    for axis in range(3):  # x, y, z: numpy axes 2, 1, 0
+        var = sigma ** 2 / (g.spacing[axis] ** 2 if mm else 1.0)
+        k = O.gaussian_kernel(var, 0.01, 32)
+        R = len(k) // 2
+        ax = 2 - axis
+        pad = [(0, 0)] * 3
+        pad[ax] = (R, R)
+        padded = np.pad(want, pad, mode="edge")
+        out = np.zeros_like(want)
+        for j, kj in enumerate(k):
+            sl = [slice(None)] * 3
+            sl[ax] = slice(j, j + want.shape[ax])
+            out += kj * padded[tuple(sl)]
+        want = out
+    np.testing.assert_allclose(got, want, atol=1e-12)
