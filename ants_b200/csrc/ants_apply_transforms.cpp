@@ -36,15 +36,17 @@
 //   * the evaluation grid G has the reference grid's voxels at L_pre(p) (direction M*D, origin
 //     M*o + b for L_pre(p) = M p + b);
 //   * the input image is given the geometry under which sampling at q reads it at L_post(q).
-// The middle part is composed on G: the first field is copied onto G (synx_resample_field when
-// its own grid differs), every later transform's displacement is brought onto G (resampled, or
-// synx_linear_field for a linear transform) and composed, w <- w + u(x + w) (synx_compose).
-// The input is sampled once at L_post(x_G + w) (synx_warp_image).  Exact (one interpolation per
-// field, as ITK's composite) when the middle part is a single field, or fields that share G:
-// e.g. `-t 1Warp -t 0GenericAffine.mat` on the fixed grid and `-t [0GenericAffine.mat,1]
-// -t 1InverseWarp` on the moving grid.  A later middle transform is read through its copy on G:
-// a second interpolation for a field on another grid, and no displacement where the point has
-// left G.  The collapsed field, L_post(x_G + w) - p, is assembled on the host while it is written.
+// The middle part is composed on G, each transform acting on the current point x_G + w:
+//   * the first field: sampled on its own grid at G's points (a copy when its grid is G);
+//   * a later field on G: w <- w + d(x + w) (synx_compose);
+//   * a later field on another grid: d sampled on its own grid at x + w, one component at a time
+//     (synx_warp_image), then w <- d(x + w) + w (synx_field_affine_update);
+//   * a linear transform T(p) = A p + b: w <- (T(x) - x) + A w (synx_linear_field, then
+//     synx_field_affine_update).
+// The input is sampled once at L_post(x_G + w) (synx_warp_image).  Every transform is therefore
+// applied at the point itself, with one interpolation per field and the interpolators' own rule
+// outside a field's grid (no displacement), as ITK's composite applies them.  The collapsed field,
+// L_post(x_G + w) - p, is assembled on the host while it is written.
 #include "ants_apply_transforms.h"
 
 #include <cuda_runtime.h>
@@ -241,12 +243,12 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       continue;
     }
     std::string note;
-    // this transform's displacement on the evaluation grid, in tmp (in w for the first field)
-    float* dst = k == first_field ? w.p : tmp.p;
     if (c.is_linear) {
+      // after w: T(x + w) - x = (T(x) - x) + A w, exact wherever the point is
       std::vector<float> u((size_t)N * dim);
       step_ok(synx_linear_field(&c.linear, c.invert ? 1 : 0, &ge, u.data()), "synx_linear_field");
-      CLI_CK(cudaMemcpy(dst, u.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+      CLI_CK(cudaMemcpy(tmp.p, u.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+      step_ok(synx_field_affine_update(tmp.p, w.p, &ge, c.map.M, w.p, nullptr), "synx_field_affine_update");
       note = c.invert ? " (linear, inverse)" : " (linear)";
     } else {
       const nifti::Image f = nifti::read(c.file);
@@ -255,15 +257,26 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       const synx_geom gf = to_geom(f, dim);
       const long long Nf = f.voxels();
       if (same_grid(gf, ge)) {
-        CLI_CK(cudaMemcpy(dst, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+        // on the evaluation grid: the first field is copied, a later one composed (w + d(x + w))
+        CLI_CK(cudaMemcpy(k == first_field ? w.p : tmp.p, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+        if (k != first_field) step_ok(synx_compose(tmp.p, w.p, &ge, 1.0f, w.p, nullptr), "synx_compose");
       } else {
         DeviceBuffer src((size_t)Nf * dim);
         CLI_CK(cudaMemcpy(src.p, f.data.data(), 4 * (size_t)Nf * dim, cudaMemcpyHostToDevice));
-        step_ok(synx_resample_field(src.p, &gf, dst, &ge, nullptr), "synx_resample_field");
-        note = " (resampled)";
+        if (k == first_field) {
+          // sampled on its own grid at the evaluation grid's points
+          step_ok(synx_resample_field(src.p, &gf, w.p, &ge, nullptr), "synx_resample_field");
+        } else {
+          // sampled on its own grid at x + w, one component at a time, then added: w + d(x + w)
+          for (int cc = 0; cc < dim; ++cc)
+            step_ok(synx_warp_image(src.p + (size_t)cc * Nf, &gf, w.p, &ge, tmp.p + (size_t)cc * N, nullptr),
+                    "synx_warp_image");
+          const double I3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+          step_ok(synx_field_affine_update(tmp.p, w.p, &ge, I3, w.p, nullptr), "synx_field_affine_update");
+        }
+        note = " (own grid)";
       }
     }
-    if (k != first_field) step_ok(synx_compose(tmp.p, w.p, &ge, 1.0f, w.p, nullptr), "synx_compose");
     if (verbose) out << "  transform " << k << ": " << c.file << note << "\n";
   }
 

@@ -1673,6 +1673,15 @@ int synx_warp_image_label(const float* img, const synx_geom* gi, const float* u,
   return SYNX_OK;
 }
 
+int synx_field_affine_update(const float* u, const float* w, const synx_geom* g, const double* matrix, float* out,
+                             void* stream) {
+  if (!u || !w || !out || !g || !matrix || !check_geom(g, g->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_field_affine_update: bad arguments");
+  launch_field_affine_update(u, w, matrix, g->dim, g->size[0] * g->size[1] * g->size[2], out, (cudaStream_t)stream);
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
+}
+
 int synx_cc_metric(const float* F, const float* M, const synx_geom* gg, int radius, float* gF, float* gM,
                    double* value, void* stream) {
   return synx_cc_metric_ex(F, M, gg, radius, 0, gF, gM, value, stream);

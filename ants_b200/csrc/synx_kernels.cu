@@ -311,6 +311,41 @@ __global__ void __launch_bounds__(256) k_warp_image_label(const float* __restric
   }
 }
 
+// out = u + M w per voxel, fields as component planes (out may alias u or w: each voxel is read
+// before it is written, by the same thread).  A transform stack's composition step for a linear
+// transform (u = T(x) - x, M = A) or for a field sampled from its own grid (u = d(x + w), M = I).
+struct AffineUpdate {
+  float M[9];
+};
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_field_affine_update(const float* u, const float* w, AffineUpdate a,
+                                                             long long N, float* out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    float wv[3] = {w[i], w[N + i], DIM == 3 ? w[2 * N + i] : 0.0f};
+    float uv[3] = {u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f};
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+      float s = uv[r];
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) s = fmaf(a.M[r * 3 + k], wv[k], s);
+      out[r * N + i] = s;
+    }
+  }
+}
+
+void launch_field_affine_update(const float* u, const float* w, const double M[9], int dim, long long N, float* out,
+                                cudaStream_t s) {
+  count_launch();
+  AffineUpdate a;
+  for (int k = 0; k < 9; ++k) a.M[k] = (float)M[k];
+  const int blocks = grid_for(N, 256);
+  if (dim == 3)
+    k_field_affine_update<3><<<blocks, 256, 0, s>>>(u, w, a, N, out);
+  else
+    k_field_affine_update<2><<<blocks, 256, 0, s>>>(u, w, a, N, out);
+}
+
 void launch_warp_image_label(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
                              cudaStream_t s) {
   count_launch();

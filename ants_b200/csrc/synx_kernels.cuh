@@ -74,6 +74,8 @@ void launch_warp_image_nearest(const float* img, const GridInfo& gi, const float
                                cudaStream_t s);
 void launch_warp_image_label(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
                              cudaStream_t s);
+void launch_field_affine_update(const float* u, const float* w, const double M[9], int dim, long long N, float* out,
+                                cudaStream_t s);
 
 // Returns the number of blocks the CC launch uses (partials needed).
 int cc_blocks(const GridInfo& g, int radius);

@@ -303,6 +303,13 @@ int synx_smooth_field(const float* in_dev, float* out_dev, const synx_geom* g, d
  * Utilities/itkComposeDiffeomorphismsImageFilter.hxx:70-105). */
 int synx_compose(const float* d_dev, const float* w_dev, const synx_geom* g, float scale, float* out_dev,
                  void* stream);
+/* out = u + M w at every voxel of `g` (component planes; out may alias u or w; M row-major 3x3, its
+ * leading dim x dim block used).  The composition step of a transform stack where compose's
+ * interpolation does not apply: a linear transform T(p) = A p + b after w, T(x + w) - x =
+ * (T(x) - x) + A w with u = synx_linear_field(T) and M = A; and a field d on another grid,
+ * w + d(x + w) with u sampled from d's own grid by synx_warp_image per component and M = I. */
+int synx_field_affine_update(const float* u_dev, const float* w_dev, const synx_geom* g, const double* matrix,
+                             float* out_dev, void* stream);
 
 /* Fixed-point inverse of phi, warm-started from psi_inout (ITK
  * InvertDisplacementFieldImageFilter; twin itkANTSImageRegistrationOptimizer.h:1845-1988).

@@ -99,15 +99,26 @@ def emulate_cli(chain, gr: Geom, img=None, gi=None):
         L = chain[k][1]
         post.M, post.b = L.M @ post.M, L.M @ post.b + L.b
     ge = push_forward(gr, pre)
+
+    def same(a, b):
+        return (a.size == b.size and np.array_equal(a.spacing, b.spacing) and np.array_equal(a.origin, b.origin)
+                and np.array_equal(a.direction, b.direction))
+
     w = np.zeros((dim,) + gr.shape, np.float32)
     for k in range(lead_end, tail_begin):
         kind, obj = chain[k]
         if kind == "field":
             d, gd = obj
-            u = O.resample_field(d, gd, ge)
-        else:
-            u = (obj.apply(points(ge)) - points(ge)).astype(np.float32)
-        w = u if k == lead_end else O.compose(u, w, ge)
+            if k == lead_end:  # the first field, sampled at the evaluation grid's points
+                w = d.copy() if same(gd, ge) else O.resample_field(d, gd, ge)
+            elif same(gd, ge):  # w + d(x + w)
+                w = O.compose(d, w, ge)
+            else:  # d sampled on its own grid at x + w, then added
+                w = (w + np.stack([O.warp_image(np.ascontiguousarray(d[c]), gd, w, ge) for c in range(dim)])
+                     ).astype(np.float32)
+        else:  # T(x + w) - x = (T(x) - x) + A w
+            P = points(ge)
+            w = (obj.apply(P) - P + np.tensordot(obj.M, w, axes=1)).astype(np.float32)
     P = points(gr)
     collapsed = (post.apply(pre.apply(P) + w) - P).astype(np.float32)
     warped = None
@@ -140,6 +151,7 @@ def cases(dim):
     g, gm = grids(dim)
     a, b = field_on(g, 4.0, 2.0, 60 + dim), field_on(g, 5.0, 2.5, 70 + dim)
     inv = field_on(g, 4.0, 2.0, 80 + dim)  # an inverse warp lives on the fixed grid too
+    c = field_on(gm, 4.0, 2.0, 85 + dim)   # a field on the moving grid
     A, B = affine(dim, 0), affine(dim, 1)
     return {
         # two fields on the reference grid: a first, then b
@@ -152,7 +164,11 @@ def cases(dim):
         "linear": ([("linear", A), ("linear", B)], gm, ["A.mat", "B.mat"]),
         # affine, field, affine: both ends folded
         "both_ends": ([("linear", B.inverse()), ("field", (a, g)), ("linear", A)], gm, ["[B.mat,1]", "a", "A.mat"]),
-    }, dict(a=a, b=b, inv=inv, A=A, B=B, g=g, gm=gm)
+        # an affine between two fields: applied at the displaced point, T(x + w) - x = (T(x) - x) + A w
+        "sandwiched": ([("field", (a, g)), ("linear", A), ("field", (b, g))], g, ["a", "A.mat", "b"]),
+        # a later field on another grid than the evaluation grid: sampled on its own grid at x + w
+        "other_grid": ([("field", (a, g)), ("field", (c, gm))], g, ["a", "c"]),
+    }, dict(a=a, b=b, c=c, inv=inv, A=A, B=B, g=g, gm=gm)
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -195,9 +211,9 @@ def test_stacks_match_the_scheme(exe, tmp_path, cuda, dim):
 def check_stacks_match_the_scheme(exe, tmp_path, dim):
     cs, parts = cases(dim)
     g, gm = parts["g"], parts["gm"]  # the grid objects the cases refer to
-    files = {"a": parts["a"], "b": parts["b"], "inv": parts["inv"]}
-    for name, u in files.items():
-        nifti.write(tmp_path / f"{name}.nii.gz", np.ascontiguousarray(np.moveaxis(u, 0, -1)), g, vector=True)
+    files = {"a": (parts["a"], g), "b": (parts["b"], g), "inv": (parts["inv"], g), "c": (parts["c"], gm)}
+    for name, (u, gu) in files.items():
+        nifti.write(tmp_path / f"{name}.nii.gz", np.ascontiguousarray(np.moveaxis(u, 0, -1)), gu, vector=True)
     parts["A"].write_mat(tmp_path / "A.mat")
     parts["B"].write_mat(tmp_path / "B.mat")
     nifti.write(tmp_path / "fixed.nii.gz", np.zeros(g.shape, np.float32), g)
@@ -224,10 +240,10 @@ def check_stacks_match_the_scheme(exe, tmp_path, dim):
         # may fall either side, so a small share of voxels may differ (as in the step tests)
         bad = np.abs(got - want_img) > 1e-4
         assert bad.mean() < 2e-3, (name, int(bad.sum()))
-        r = run(exe, ["-d", str(dim), "-r", str(ref), *ts, "-o", f"[{tmp_path}/c.nii.gz,1]"])
+        r = run(exe, ["-d", str(dim), "-r", str(ref), *ts, "-o", f"[{tmp_path}/collapsed.nii.gz,1]"])
         assert r.returncode == 0, (name, r.stderr)
-        c, _ = nifti.read(tmp_path / "c.nii.gz", dim)
-        bad = np.abs(planes(c) - want_field) > 1e-4
+        collapsed, _ = nifti.read(tmp_path / "collapsed.nii.gz", dim)
+        bad = np.abs(planes(collapsed) - want_field) > 1e-4
         assert bad.mean() < 2e-3, (name, int(bad.sum()))
 
 
