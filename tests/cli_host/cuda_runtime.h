@@ -14,3 +14,10 @@ inline cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) 
 inline cudaError_t cudaMemset(void* d, int v, size_t n) { std::memset(d, v, n); return 0; }
 inline cudaError_t cudaSetDevice(int) { return 0; }
 inline const char* cudaGetErrorString(cudaError_t) { return "host stand-in"; }
+typedef void* cudaStream_t;
+enum { cudaStreamNonBlocking = 1 };
+inline cudaError_t cudaStreamCreateWithFlags(cudaStream_t* s, unsigned) { *s = (cudaStream_t)0x1; return 0; }
+inline cudaError_t cudaStreamDestroy(cudaStream_t) { return 0; }
+inline cudaError_t cudaGetDeviceCount(int* n) { *n = 1; return 0; }
+inline cudaError_t cudaGetLastError() { return 0; }
+inline cudaError_t cudaMemGetInfo(size_t* free_b, size_t* total_b) { *free_b = (size_t)1 << 34; *total_b = (size_t)1 << 35; return 0; }

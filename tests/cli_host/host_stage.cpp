@@ -1,6 +1,8 @@
-// Test infrastructure: the stage entry points the registration command line calls, backed by
-// the CPU oracle's whole registration, so that its plumbing (initial transforms, output names,
-// written transforms, warped images) can be tested without a GPU.  Never part of the product.
+// Test infrastructure: the stage and batch entry points the registration command line and the
+// serving loop call, backed by the CPU oracle's whole registration (run when a stage reaches its
+// last level), so that their plumbing (initial transforms, output names, written transforms, warped
+// images; admission, pooling and request lifecycle) can be tested without a GPU.  The footprint is
+// a stand-in that grows with both images.  Never part of the product.
 #include <cstring>
 #include <string>
 #include <vector>
@@ -15,7 +17,12 @@ struct synx_ctx {
   std::vector<int32_t> lv, it, ki;
   std::vector<double> me, cv;
   bool done = false;
+  int level = 0;  // next level a batch step runs
 };
+struct synx_batch {
+  int device;
+};
+static int g_created = 0;  // contexts created, so a test can see pooled contexts being reused
 extern "C" {
 int synx_params_default(synx_params* p, int dim) {
   memset(p, 0, sizeof(*p));
@@ -24,12 +31,20 @@ int synx_params_default(synx_params* p, int dim) {
   p->preprocess = 1; p->winsor_upper = 1.0f; p->inv_max_iter = 20; p->inv_mean_tol = 0.001; p->inv_max_tol = 0.1;
   return 0;
 }
-int synx_create(const synx_params* p, int, void*, synx_ctx** out) { *out = new synx_ctx; (*out)->p = *p; return 0; }
+int synx_create(const synx_params* p, int, void*, synx_ctx** out) {
+  *out = new synx_ctx;
+  (*out)->p = *p;
+  ++g_created;
+  return 0;
+}
+int host_stage_created() { return g_created; }
 int synx_destroy(synx_ctx* c) { delete c; return 0; }
 int synx_set_images(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm) {
   c->gf = *gf; c->gm = *gm;
   c->F.assign(F, F + gf->size[0] * gf->size[1] * gf->size[2]);
   c->M.assign(M, M + gm->size[0] * gm->size[1] * gm->size[2]);
+  c->done = false;
+  c->level = 0;
   return 0;
 }
 int synx_run_level(synx_ctx* c, int level) {
@@ -59,6 +74,29 @@ int synx_get_log(synx_ctx* c, int32_t* level, int32_t* iter, double* metric, dou
     if (level) level[i] = c->lv[i]; if (iter) iter[i] = c->it[i]; if (metric) metric[i] = c->me[i];
     if (conv) conv[i] = c->cv[i]; if (inv) inv[i] = c->ki[i];
   }
+  return 0;
+}
+}
+
+extern "C" {
+int synx_batch_create(int device, synx_batch** out) { *out = new synx_batch{device}; return 0; }
+int synx_batch_destroy(synx_batch* b) { delete b; return 0; }
+const char* synx_batch_last_error(const synx_batch*) { return ""; }
+int synx_batch_step(synx_batch*, synx_ctx* const* cs, int n, void*, int* advanced) {
+  int a = 0;
+  for (int i = 0; i < n; ++i) {
+    synx_ctx* c = cs[i];
+    if (c->level >= c->p.n_levels) continue;
+    synx_run_level(c, c->level);
+    ++c->level;
+    ++a;
+  }
+  if (advanced) *advanced = a;
+  return 0;
+}
+int synx_footprint(const synx_params* p, const synx_geom* gf, const synx_geom* gm, int64_t* bytes) {
+  const int64_t nf = gf->size[0] * gf->size[1] * gf->size[2], nm = gm->size[0] * gm->size[1] * gm->size[2];
+  *bytes = 4 * (nf + nm) + 40 * nf * p->dim;
   return 0;
 }
 }
