@@ -1,5 +1,7 @@
-"""antsApplyTransforms_b200 transform stacks: order, linear transforms folded into grid geometry,
-and the collapsed field.
+"""antsApplyTransforms_b200 transform stacks -- order, linear transforms folded into grid geometry,
+every transform applied at the displaced point, the collapsed field -- and the command lines' other
+options: label interpolation, multichannel and time-series inputs, output types, and
+antsRegistrationSyN_b200's initial moving transforms.
 
 The reference applies the FIRST -t to a reference point first (its parser stores repeated options
 newest first, Utilities/antsCommandLineOption.cxx:42,64, and an ITK composite applies the transform
@@ -9,10 +11,11 @@ added last first), so `-t 1Warp -t 0GenericAffine.mat` samples the input at A(p 
 own grid (the oracle's warp, the interpolation ITK's displacement-field transform uses), each linear
 transform applied analytically.  `emulate_cli` is the command line's scheme restated with the
 oracle's step functions: leading linear transforms folded into the evaluation grid, trailing ones
-into the input image's geometry, the middle composed on the evaluation grid.  CPU tests check the
-scheme against the composite on the stacks where it is exact; GPU tests check the command line
-against the scheme.  This file is collected last, after the allocation-free entry point's, so that
-a run which stops at the first failure has already run every other test.
+into the input image's geometry, the middle applied transform by transform at the displaced point.
+CPU tests check the scheme against the composite on every tested stack shape; GPU tests (and, through
+host stand-ins, tests/test_cli_host_plumbing.py) check the command lines against the scheme.  This
+file is collected after the tests already verified on the device, so that a run which stops at the
+first failure has already run them.
 """
 import os
 import subprocess
@@ -172,7 +175,7 @@ def cases(dim):
 
 
 @pytest.mark.parametrize("dim", [2, 3])
-def test_scheme_is_the_composite_on_exact_stacks(dim):
+def test_scheme_is_the_composite(dim):
     cs, _ = cases(dim)
     for name, (chain, gr, _) in cs.items():
         want = chain_displacement(chain, gr)
