@@ -2,7 +2,8 @@
 //
 // Accepted options (the reference's syntax, Examples/antsRegistration.cxx:30-548, parsed as in
 // Examples/antsRegistrationTemplateHeader.h:545-651, :801-815, :1081-1087):
-//   -d/--dimensionality 2|3        --float 0|1 (computation is float32 either way)
+//   -d/--dimensionality 2|3        --float 0|1 (computation is float32 either way; the output files
+//       are float32 with --float 1 and float64 by default, as the reference writes them)
 //   -m/--metric CC[fixed,moving,weight,radius]
 //   -t/--transform SyN[gradientStep,updateFieldVariance,totalFieldVariance]
 //   -c/--convergence [NxNx...,threshold,window] or NxNx...
@@ -295,13 +296,20 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       }
     }
   }
+  // output files in the precision the reference writes them: float with --float 1, double by default
+  // (antsRegistration.cxx:488-491); the values are computed in float either way
+  const int out_type = flag("float", false) ? 16 : 64;
+  auto typed = [out_type](nifti::Image im) {
+    im.out_datatype = out_type;
+    return im;
+  };
   const std::string wi = std::to_string(warp_index);
-  nifti::write(prefix + wi + "Warp.nii.gz", field_image(go, fwd));
-  nifti::write(prefix + wi + "InverseWarp.nii.gz", field_image(go, inv));
-  if (!warped.empty()) nifti::write(warped, like(fixed, warp_on_device(moving, gm, fwd, go)));
+  nifti::write(prefix + wi + "Warp.nii.gz", typed(field_image(go, fwd)));
+  nifti::write(prefix + wi + "InverseWarp.nii.gz", typed(field_image(go, inv)));
+  if (!warped.empty()) nifti::write(warped, typed(like(fixed, warp_on_device(moving, gm, fwd, go))));
   if (!inv_warped.empty()) {
     std::vector<float> inv_on_moving = resample_on_device(inv, go, gm);
-    nifti::write(inv_warped, like(moving, warp_on_device(fixed, gf, inv_on_moving, gm)));
+    nifti::write(inv_warped, typed(like(moving, warp_on_device(fixed, gf, inv_on_moving, gm))));
   }
   if (verbose) {
     const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

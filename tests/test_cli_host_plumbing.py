@@ -80,3 +80,7 @@ def test_time_series(host_cli, tmp_path):
 
 def test_output_types(host_cli, tmp_path):
     S.check_output_types(host_cli["apply"], tmp_path)
+
+
+def test_output_precision(host_cli, tmp_path):
+    S.check_output_precision(host_cli["reg"], tmp_path)

@@ -442,6 +442,34 @@ def check_initial_moving_transform(reg, exe, tmp_path):
         assert bad.mean() < 1e-3, (out, int(bad.sum()))
 
 
+@pytest.mark.gpu
+def test_registration_output_precision(tmp_path, cuda):
+    check_output_precision(REG, tmp_path)
+
+
+def check_output_precision(reg, tmp_path):
+    """The registration's fields and warped image are written as float64 by default and as float32 with
+    --float 1, as the reference writes them; the values are the same float results either way."""
+    import struct
+    size = (40, 36)
+    f, m = phantoms.pair_2d(size, seed=37)
+    g = Geom(size)
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    vals = {}
+    for flt, code in (("0", 64), ("1", 16)):
+        p = str(tmp_path / f"p{flt}_")
+        r = run(reg, ["-d", "2", "--float", flt, "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]",
+                      "-t", "SyN[0.2,3,0]", "-c", "[4x2,1e-12,10]", "-f", "2x1", "-s", "1x0vox",
+                      "-o", f"[{p},{p}warped.nii]"])
+        assert r.returncode == 0, r.stderr
+        raw = (tmp_path / f"p{flt}_warped.nii").read_bytes()
+        assert struct.unpack("<h", raw[70:72])[0] == code
+        vals[flt] = (nifti.read(p + "0Warp.nii.gz", 2)[0], nifti.read(p + "warped.nii", 2)[0])
+    np.testing.assert_array_equal(vals["0"][0], vals["1"][0])
+    np.testing.assert_array_equal(vals["0"][1], vals["1"][1])
+
+
 def check_derived_initial_translation(reg, tmp_path):
     """antsRegistration -r [fixed,moving,1]: the translation between the centers of intensity mass,
     folded into the moving geometry; collapsed into 0GenericAffine.mat, or with -z 0 written as
