@@ -27,7 +27,9 @@
 //   -o/--output warped | [collapsed,1] | DisplacementField[collapsed]  (the collapsed form writes
 //       the single displacement field equivalent to the stack, on the reference grid, :1115-1131)
 //   -u/--output-data-type char|uchar|short|int|float|double|default (a cast of the float result)
-//   --float 0|1 (computation is float32 either way)   -v/--verbose 0|1   --gpu N (not a reference option)
+//   --float 0|1 (computation is float32 either way; output files, the collapsed field and the
+//       default output type, are float64 unless --float 1, as the reference writes them)
+//   -v/--verbose 0|1   --gpu N (not a reference option)
 //
 // GPU path.  The chain of transforms, in application order, is split into a leading run of
 // linear transforms L_pre, a middle part from the first field to the last field, and a trailing
@@ -150,10 +152,14 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
   const int gpu = std::atoi(one("gpu", "0").c_str());
   const float defval = (float)std::atof(one("default-value", "0").c_str());
-  // output pixel type of the warped image (:1168-1181, :1460-1520): a cast of the float result;
-  // "default" is the computation type, float here
-  const std::map<std::string, int> out_types = {{"char", 256}, {"uchar", 2}, {"short", 4},  {"int", 8},
-                                                {"float", 16}, {"double", 64}, {"default", 16}};
+  // the reference computes in double unless --float 1 (:1237-1240, :1384-1405); its collapsed field and
+  // the "default" output type are that type, so the files here are float64 unless --float 1 (the values
+  // are computed in float either way)
+  const std::string fl = lower(one("float", "0"));
+  const int real_type = (fl == "1" || fl == "true") ? 16 : 64;
+  // output pixel type of the warped image (:1168-1181, :1460-1520): a cast of the float result
+  const std::map<std::string, int> out_types = {{"char", 256}, {"uchar", 2}, {"short", 4},     {"int", 8},
+                                                {"float", 16}, {"double", 64}, {"default", real_type}};
   const std::string out_type = lower(one("output-data-type", "default"));
   if (!out_types.count(out_type))
     throw std::runtime_error("--output-data-type must be char, uchar, short, int, float, double or default");
@@ -282,6 +288,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
 
   if (collapse) {
     nifti::Image fo;
+    fo.out_datatype = real_type;
     fo.dim = dim;
     fo.components = dim;
     for (int k = 0; k < 3; ++k) {

@@ -282,7 +282,8 @@ def check_output_types(exe, tmp_path):
     assert r.returncode == 0, r.stderr
     ref, _ = nifti.read(tmp_path / "f.nii", 2)
     for name, code, cast in (("char", 256, np.int8), ("uchar", 2, np.uint8), ("short", 4, np.int16),
-                             ("int", 8, np.int32), ("double", 64, np.float64), ("default", 16, np.float32)):
+                             ("int", 8, np.int32), ("double", 64, np.float64), ("float", 16, np.float32),
+                             ("default", 64, np.float64)):  # default: the reference's computation type, double
         r = run(exe, base + ["-u", name, "-o", f"{tmp_path}/{name}.nii"])
         assert r.returncode == 0, (name, r.stderr)
         raw = (tmp_path / f"{name}.nii").read_bytes()
@@ -290,6 +291,13 @@ def check_output_types(exe, tmp_path):
         got, _ = nifti.read(tmp_path / f"{name}.nii", 2)
         want = ref.astype(np.float64) if cast in (np.float64, np.float32) else np.trunc(ref).astype(np.int64).astype(cast)
         np.testing.assert_array_equal(got, np.asarray(want, np.float32), err_msg=name)
+    # with --float 1 the default type, and the collapsed field, are float
+    r = run(exe, base + ["--float", "1", "-o", f"{tmp_path}/f1.nii"])
+    assert r.returncode == 0 and struct.unpack("<h", (tmp_path / "f1.nii").read_bytes()[70:72])[0] == 16
+    for flt, code in (("0", 64), ("1", 16)):
+        r = run(exe, ["-d", "2", "-r", f"{tmp_path}/in.nii.gz", "-t", f"{tmp_path}/u.nii.gz", "--float", flt,
+                      "-o", f"[{tmp_path}/col{flt}.nii,1]"])
+        assert r.returncode == 0 and struct.unpack("<h", (tmp_path / f"col{flt}.nii").read_bytes()[70:72])[0] == code
     r = run(exe, base + ["-u", "long", "-o", f"{tmp_path}/x.nii"])
     assert r.returncode == 1 and "output-data-type" in r.stderr
 
