@@ -26,6 +26,7 @@
 //   -f/--default-value v (0): value where the point maps outside the input image
 //   -o/--output warped | [collapsed,1] | DisplacementField[collapsed]  (the collapsed form writes
 //       the single displacement field equivalent to the stack, on the reference grid, :1115-1131)
+//       | Linear[collapsed.mat,invert]  (an all-linear stack as one affine transform file)
 //   -u/--output-data-type char|uchar|short|int|float|double|default (a cast of the float result)
 //   --float 0|1 (computation is float32 either way; output files, the collapsed field and the
 //       default output type, are float64 unless --float 1, as the reference writes them)
@@ -147,8 +148,9 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   if (interp == "genericlabel" && !icall.params.empty() && lower(icall.params[0]) != "linear")
     throw std::runtime_error("GenericLabel supports the Linear interpolator only");
   const bool nearest = interp == "nearestneighbor", label = interp == "genericlabel";
-  if (!opt.count("reference-image")) throw std::runtime_error("a reference image (-r) is required");
   if (!opt.count("output")) throw std::runtime_error("an output (-o) is required");
+  const bool linear_out = lower(parse_call(one("output", "")).name) == "linear";
+  if (!linear_out && !opt.count("reference-image")) throw std::runtime_error("a reference image (-r) is required");
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
   const int gpu = std::atoi(one("gpu", "0").c_str());
   const float defval = (float)std::atof(one("default-value", "0").c_str());
@@ -176,12 +178,15 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     out_path = o.params[0];
     collapse = o.params.size() > 1 && (o.params[1] == "1" || lower(o.params[1]) == "true");
     if (!collapse) throw std::runtime_error("-o [file,0] is not a supported output form");
-  } else if (lower(o.name) == "linear" || lower(o.name) == "compositetransform") {
+  } else if (linear_out) {
+    if (o.params.empty() || o.params.size() > 2) throw std::runtime_error("Linear[file.mat,invert] needs a file name");
+    out_path = o.params[0];
+  } else if (lower(o.name) == "compositetransform") {
     throw std::runtime_error("-o " + o.name + "[...] is not supported (displacement fields only)");
   } else {
     out_path = o.name;
   }
-  if (!collapse && !opt.count("input")) throw std::runtime_error("an input image (-i) is required");
+  if (!collapse && !linear_out && !opt.count("input")) throw std::runtime_error("an input image (-i) is required");
 
   // the chain in application order: command-line order, each file's transforms as its composite
   std::vector<ChainItem> chain;
@@ -216,6 +221,37 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     ChainItem c;
     c.file = file;
     chain.push_back(c);
+  }
+
+  if (linear_out) {
+    // -o Linear[file.mat,invert] (:640-680): an all-linear stack collapsed into one affine, written as
+    // an ITK transform file.  Like CollapseLinearTransforms (itkantsRegistrationHelper.hxx:3773-3825) the
+    // center is that of the first transform that acts and has one; the inverse is written, as the
+    // reference builds it, with the inverse matrix, offset -M^-1 b and center 0.  No device work.
+    Map total;
+    double center[3] = {0.0, 0.0, 0.0};
+    bool have_center = false;
+    for (const ChainItem& c : chain) {
+      if (!c.is_linear)
+        throw std::runtime_error("'" + c.file + "' is a displacement field: only linear stacks collapse to Linear[...]");
+      total = mul(c.map, total);
+      if (!have_center && c.linear.has_center) {
+        for (int k = 0; k < 3; ++k) center[k] = c.linear.center[k];
+        have_center = true;
+      }
+    }
+    synx_linear t;
+    if (o.params.size() > 1 && o.params[1] != "0" && lower(o.params[1]) != "false") {
+      Map inv;
+      if (!inverse(total, inv)) throw std::runtime_error("the collapsed linear transform is singular, no inverse");
+      const double zero[3] = {0.0, 0.0, 0.0};
+      t = linear_of(inv, dim, zero);
+    } else {
+      t = linear_of(total, dim, center);
+    }
+    step_ok(synx_write_linear_transform(out_path.c_str(), &t), "synx_write_linear_transform");
+    if (verbose) out << "wrote the collapsed linear transform " << out_path << "\n";
+    return EXIT_SUCCESS;
   }
 
   // split: leading linear run, middle (first field .. last field), trailing linear run

@@ -34,7 +34,7 @@ def run(exe, args):
     (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz", "-n", "BSpline[3]"], "NearestNeighbor"),
     (["-d", "5", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz"], "dimensionality"),
     (["-d", "3", "-e", "2", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz"], "multichannel (4)"),
-    (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "Linear[x.mat,0]"], "not supported"),
+    (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "CompositeTransform[x.h5]"], "not supported"),
     (["-d", "3", "-i", "a.nii.gz", "-r", "/nonexistent/r.nii.gz", "-o", "x.nii.gz"], "cannot open"),
 ])
 def test_rejects_bad_input(exe, args, needle):
@@ -104,3 +104,45 @@ def test_corrupt_headers_fail_cleanly(exe, tmp_path, patch, needle):
     r = run(exe, ["-d", "3", "-i", f"{tmp_path}/ok.nii", "-r", f"{tmp_path}/bad.nii", "-o", f"{tmp_path}/o.nii.gz"])
     assert r.returncode == 1
     assert needle in r.stderr
+
+
+
+def test_collapse_linear_stack(exe, tmp_path):
+    """-o Linear[out.mat,invert]: an all-linear stack (first -t acting first) written as one affine;
+    the center is that of the first transform acting (CollapseLinearTransforms); the inverse is
+    written with center 0, as the reference builds it.  No GPU is involved."""
+    from scipy.spatial.transform import Rotation
+
+    from ants_b200 import synx
+    from ants_b200.synx import LinearTransform
+    A = LinearTransform(np.array([[1.05, 0.08, -0.03], [-0.06, 0.97, 0.04], [0.02, -0.05, 1.02]]),
+                        np.array([2.5, -1.25, 3.0]), np.array([10.0, -4.0, 7.5]))
+    B = LinearTransform(Rotation.from_euler("xyz", [0.1, -0.2, 0.3]).as_matrix(), np.array([1.0, 2.0, -0.5]),
+                        np.array([3.0, 3.0, 3.0]))
+    synx.write_linear_transform(tmp_path / "A.mat", A)
+    synx.write_linear_transform(tmp_path / "B.txt", B)
+
+    def mp(t):
+        return t.matrix, t.translation + t.center - t.matrix @ t.center
+
+    (MA, bA), (MB, bB) = mp(A), mp(B)
+    M, b = MB @ MA, MB @ bA + bB  # A acts first, then B
+    for inv, name in (("0", "c.mat"), ("1", "ci.mat")):
+        r = run(exe, ["-d", "3", "-t", f"{tmp_path}/A.mat", "-t", f"{tmp_path}/B.txt", "-o",
+                      f"Linear[{tmp_path}/{name},{inv}]"])
+        assert r.returncode == 0, r.stderr
+        t = synx.read_linear_transform(tmp_path / name, 3)
+        Mt, bt = mp(t)
+        if inv == "0":
+            np.testing.assert_allclose(Mt, M, atol=1e-12)
+            np.testing.assert_allclose(bt, b, atol=1e-10)
+            np.testing.assert_array_equal(t.center, A.center)
+        else:
+            np.testing.assert_allclose(Mt, np.linalg.inv(M), atol=1e-12)
+            np.testing.assert_allclose(bt, -np.linalg.inv(M) @ b, atol=1e-10)
+            np.testing.assert_array_equal(t.center, 0.0)
+    synx.write_linear_transform(tmp_path / "u.mat", A)
+    g = Geom((4, 4, 4))
+    nifti.write(tmp_path / "f.nii.gz", np.zeros(g.shape + (3,), np.float32), g, vector=True)
+    r = run(exe, ["-d", "3", "-t", f"{tmp_path}/f.nii.gz", "-t", f"{tmp_path}/u.mat", "-o", f"Linear[{tmp_path}/x.mat]"])
+    assert r.returncode == 1 and "displacement field" in r.stderr
