@@ -9,7 +9,7 @@
 //   -c/--convergence [NxNx...,threshold,window] or NxNx...
 //   -f/--shrink-factors NxNx...     -s/--smoothing-sigmas NxNx...[vox|mm]
 //   -o/--output prefix | [prefix,warpedImage,inverseWarpedImage]
-//   -w/--winsorize-image-intensities [lower,upper]   -u/--use-histogram-matching 0
+//   -w/--winsorize-image-intensities [lower,upper]   -u/--use-histogram-matching 0|1
 //   -v/--verbose 0|1   --random-seed N (accepted, no effect: the stage is deterministic)
 //   --gpu N (device index; not a reference option)
 //   -r/--initial-moving-transform file | [file,useInverse] | identity | [fixed,moving,feature]
@@ -94,9 +94,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   if (flag("write-composite-transform", false))
     throw std::runtime_error("option --write-composite-transform 1 (HDF5 composite output) is not supported");
   const bool collapse = flag("collapse-output-transforms", true);
-  if (opt.count("use-histogram-matching") && (one("use-histogram-matching", "0") == "1" ||
-                                              lower(one("use-histogram-matching", "0")) == "true"))
-    throw std::runtime_error("--use-histogram-matching 1 is not supported");
+  const bool histogram_matching = flag("use-histogram-matching", false);
   if (opt.count("interpolation") && lower(one("interpolation", "Linear")) != "linear")
     throw std::runtime_error("only Linear interpolation is supported for the warped outputs");
 
@@ -210,6 +208,9 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     p.shrink_factors[l] = shrink[l];
     p.smoothing_sigmas[l] = sigmas[l];
   }
+  // the moving image matched to the fixed one after the window (PreprocessImage,
+  // Examples/itkantsRegistrationHelper.hxx:1135-1143)
+  p.histogram_match = histogram_matching ? 1 : 0;
   if (opt.count("winsorize-image-intensities")) {
     OptionCall w = parse_call(one("winsorize-image-intensities", ""));
     if (w.params.size() > 0) p.winsor_lower = (float)std::atof(w.params[0].c_str());

@@ -238,6 +238,10 @@ int set_err(synx_ctx* c, int code, const std::string& msg) {
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Device scratch of histogram_match_dev: `levels` bins and the min/max pair, then the per-block sums.
+size_t hm_sums_offset(int levels) { return (4 * (size_t)levels + 8 + 15) & ~(size_t)15; }
+size_t hm_scratch_bytes(int levels) { return hm_sums_offset(levels) + 8 * (size_t)HM_STATS_BLOCKS; }
+
 void drop_graphs(synx_ctx* c) {
   for (auto& g : c->gexec_lv) {
     if (g) cudaGraphExecDestroy(g);
@@ -305,7 +309,7 @@ ArenaPlan arena_plan(const synx_ctx* c) {
   a.Cu = add(4 * 3 * coeff_cap), a.Ct = add(4 * 3 * coeff_cap), a.Ci = add(8 * 3 * coeff_cap);
   a.Ctl = add(sizeof(IterCtl));
   a.Lm = add(8 * (size_t)max_iters), a.Lc = add(8 * (size_t)max_iters), a.Li = add(4 * (size_t)max_iters);
-  a.H = add(4 * 258);
+  a.H = add(std::max((size_t)4 * 258, hm_scratch_bytes(256)));
   a.total = sz;
   a.ccb = ccb;
   a.invb = invb;
@@ -373,6 +377,120 @@ int allocate(synx_ctx* c) {
   return SYNX_OK;
 }
 
+// Quantile of a histogram with equal bins [lo + b*bw, lo + (b+1)*bw), interpolated inside the bin
+// that reaches p: ITK's Histogram::Quantile (ITK 5.4.6, the version SuperBuild/External_ITKv5.cmake:155
+// pins), accumulating from the first bin below p = 0.5 and from the last one above.
+double hist_quantile(const std::vector<unsigned>& h, double lo, double bw, double p) {
+  const int nb = (int)h.size();
+  double total = 0.0;
+  for (unsigned v : h) total += (double)v;
+  auto bmin = [&](int b) { return lo + b * bw; };
+  auto bmax = [&](int b) { return lo + (b + 1) * bw; };
+  double cum = 0, pn = 0, pprev = 0, fn = 0;
+  if (p < 0.5) {
+    int k = 0;
+    do {
+      fn = h[k];
+      cum += fn;
+      pprev = pn;
+      pn = cum / total;
+      ++k;
+    } while (k < nb && pn < p);
+    return bmin(k - 1) + ((p - pprev) / (fn / total)) * (bmax(k - 1) - bmin(k - 1));
+  }
+  int k = nb - 1, m = 0;
+  pn = 1.0;
+  do {
+    fn = h[k];
+    cum += fn;
+    pprev = pn;
+    pn = 1.0 - cum / total;
+    --k;
+    ++m;
+  } while (m < nb && pn > p);
+  return bmax(k + 1) - ((pprev - p) / (fn / total)) * (bmax(k + 1) - bmin(k + 1));
+}
+
+struct ImageStats {
+  float mn, mx, mean;
+};
+
+// Min, max and mean of one image (the mean cast to float, as ITK casts it to the pixel type).  The
+// per-block sums come back and are added in block order, so the result does not depend on timing.
+int image_stats(synx_ctx* c, const float* x, long long n, void* scratch, int levels, cudaStream_t s, ImageStats& st) {
+  unsigned* mm = (unsigned*)scratch + levels;
+  double* part = (double*)((char*)scratch + hm_sums_offset(levels));
+  unsigned init[2] = {float_to_ordered(FLT_MAX), float_to_ordered(-FLT_MAX)};
+  CUDA_TRY(c, cudaMemcpyAsync(mm, init, 8, cudaMemcpyHostToDevice, s));
+  launch_stats(x, n, part, HM_STATS_BLOCKS, mm, s);
+  unsigned hm[2];
+  std::vector<double> hp(HM_STATS_BLOCKS);
+  CUDA_TRY(c, cudaMemcpyAsync(hm, mm, 8, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(hp.data(), part, 8 * (size_t)HM_STATS_BLOCKS, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  double sum = 0.0;
+  for (double v : hp) sum += v;
+  st.mn = ordered_to_float(hm[0]);
+  st.mx = ordered_to_float(hm[1]);
+  st.mean = (float)(sum / (double)n);
+  return SYNX_OK;
+}
+
+// Histogram matching of `src` to `ref` (ITK's HistogramMatchingImageFilter; PreprocessImage runs it
+// with 256 levels, 12 match points and the threshold at the mean, Examples/itkantsRegistrationHelper.hxx:111-122).
+// Statistics and thresholded histograms of both images on the device; the table of match points
+// on the host in double (points + 2 rows: the thresholds, the quantiles j/(points+1), the maxima;
+// slope 0 between coincident source points; below the first point the line through the minima,
+// above the last the one through the maxima); one mapping pass writes `out` (may be `src`).
+int histogram_match_dev(synx_ctx* c, const float* src, long long ns, const float* ref, long long nr, int levels,
+                        int points, bool thr_mean, float* out, void* scratch, cudaStream_t s) {
+  ImageStats a, b;
+  int rc = image_stats(c, src, ns, scratch, levels, s, a);
+  if (rc) return rc;
+  rc = image_stats(c, ref, nr, scratch, levels, s, b);
+  if (rc) return rc;
+  unsigned* bins = (unsigned*)scratch;
+  auto histogram = [&](const float* x, long long n, const ImageStats& st, double thr,
+                       std::vector<unsigned>& h) -> int {
+    CUDA_TRY(c, cudaMemsetAsync(bins, 0, 4 * (size_t)levels, s));
+    launch_histogram_range(x, n, (double)st.mn, (double)st.mx, levels, thr, (double)st.mx, bins, s);
+    h.assign(levels, 0u);
+    CUDA_TRY(c, cudaMemcpyAsync(h.data(), bins, 4 * (size_t)levels, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+    return SYNX_OK;
+  };
+  const double sthr = thr_mean ? (double)a.mean : (double)a.mn, rthr = thr_mean ? (double)b.mean : (double)b.mn;
+  std::vector<unsigned> hs, hr;
+  if ((rc = histogram(src, ns, a, sthr, hs))) return rc;
+  if ((rc = histogram(ref, nr, b, rthr, hr))) return rc;
+  const double bws = ((double)a.mx - (double)a.mn) / levels, bwr = ((double)b.mx - (double)b.mn) / levels;
+  HistMatchMap t = {};
+  t.points = points;
+  t.src[0] = sthr;
+  t.ref[0] = rthr;
+  t.src[points + 1] = (double)a.mx;
+  t.ref[points + 1] = (double)b.mx;
+  const double delta = 1.0 / ((double)points + 1.0);
+  for (int j = 1; j <= points; ++j) {
+    t.src[j] = hist_quantile(hs, (double)a.mn, bws, j * delta);
+    t.ref[j] = hist_quantile(hr, (double)b.mn, bwr, j * delta);
+  }
+  for (int j = 0; j <= points; ++j) {
+    const double den = t.src[j + 1] - t.src[j];
+    t.grad[j] = den != 0.0 ? (t.ref[j + 1] - t.ref[j]) / den : 0.0;
+  }
+  t.src_min = (double)a.mn;
+  t.src_max = (double)a.mx;
+  t.ref_min = (double)b.mn;
+  t.ref_max = (double)b.mx;
+  const double dlo = t.src[0] - t.src_min, dhi = t.src[points + 1] - t.src_max;
+  t.lower_grad = dlo != 0.0 ? (t.ref[0] - t.ref_min) / dlo : 0.0;
+  t.upper_grad = dhi != 0.0 ? (t.ref[points + 1] - t.ref_max) / dhi : 0.0;
+  launch_histogram_map(src, out, ns, t, s);
+  CUDA_TRY(c, cudaGetLastError());
+  return SYNX_OK;
+}
+
 // Preprocess one image in place on the device: histogram quantiles -> window -> [0, 1].
 int preprocess(synx_ctx* c, float* img, long long n) {
   unsigned init[2] = {float_to_ordered(FLT_MAX), float_to_ordered(-FLT_MAX)};
@@ -392,33 +510,7 @@ int preprocess(synx_ctx* c, float* img, long long n) {
   CUDA_TRY(c, cudaMemcpyAsync(hh.data(), c->hist, 4 * nb, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   const double bw = ((double)hi - (double)mn) / nb;
-  auto bmin = [&](int b) { return (double)mn + b * bw; };
-  auto bmax = [&](int b) { return (double)mn + (b + 1) * bw; };
-  auto quantile = [&](double p) -> double {
-    double total = (double)n, cum = 0, pn = 0, pprev = 0, fn = 0;
-    if (p < 0.5) {
-      int k = 0;
-      do {
-        fn = hh[k];
-        cum += fn;
-        pprev = pn;
-        pn = cum / total;
-        ++k;
-      } while (k < nb && pn < p);
-      return bmin(k - 1) + ((p - pprev) / (fn / total)) * (bmax(k - 1) - bmin(k - 1));
-    }
-    int k = nb - 1, m = 0;
-    pn = 1.0;
-    do {
-      fn = hh[k];
-      cum += fn;
-      pprev = pn;
-      pn = 1.0 - cum / total;
-      --k;
-      ++m;
-    } while (m < nb && pn > p);
-    return bmax(k + 1) - ((pprev - p) / (fn / total)) * (bmax(k + 1) - bmin(k + 1));
-  };
+  auto quantile = [&](double p) { return hist_quantile(hh, (double)mn, bw, p); };
   const float wlo = (float)quantile(c->P.winsor_lower), whi = (float)quantile(c->P.winsor_upper);
   const double scale = 1.0 / ((double)whi - (double)wlo);
   const double shift = -(double)wlo * scale;
@@ -1200,6 +1292,8 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     return set_err(nullptr, SYNX_E_ARG, "synx_create: negative smoothing variance");
   if (p.test_inject != 0 && p.test_inject != SYNX_INJECT_BARRIER_TIMEOUT && p.test_inject != SYNX_INJECT_ALLOC_FAILURE)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: unknown test_inject value");
+  if (p.histogram_match != 0 && p.histogram_match != 1)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: histogram_match must be 0 or 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -1274,6 +1368,10 @@ static int set_images_common(synx_ctx* c, const float* F, const synx_geom* gf, c
     rc = preprocess(c, c->F0, c->NF);
     if (rc) return rc;
     rc = preprocess(c, c->M0, c->NM);
+    if (rc) return rc;
+  }
+  if (c->P.histogram_match) {
+    rc = histogram_match_dev(c, c->M0, c->NM, c->F0, c->NF, 256, 12, true, c->M0, c->hist, c->stream);
     if (rc) return rc;
   }
   c->images_set = true;
@@ -1671,6 +1769,21 @@ int synx_warp_image_label(const float* img, const synx_geom* gi, const float* u,
   launch_warp_image_label(img, a, u, b, out, (cudaStream_t)stream);
   STEP_TRY(cudaGetLastError());
   return SYNX_OK;
+}
+
+int synx_histogram_match(const float* src, int64_t n_src, const float* ref, int64_t n_ref, int32_t levels,
+                         int32_t match_points, int32_t threshold_at_mean, float* out, void* stream) {
+  if (!src || !ref || !out || n_src < 1 || n_ref < 1 || levels < 1 || levels > 4096 || match_points < 1 ||
+      match_points > HM_MAX_POINTS || (threshold_at_mean != 0 && threshold_at_mean != 1))
+    return set_err(nullptr, SYNX_E_ARG, "synx_histogram_match: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  void* scratch = nullptr;
+  STEP_TRY(cudaMalloc(&scratch, hm_scratch_bytes(levels)));
+  const int rc = histogram_match_dev(nullptr, src, n_src, ref, n_ref, levels, match_points, threshold_at_mean != 0, out,
+                                     scratch, s);
+  cudaStreamSynchronize(s);
+  cudaFree(scratch);
+  return rc;
 }
 
 int synx_field_affine_update(const float* u, const float* w, const synx_geom* g, const double* matrix, float* out,

@@ -977,6 +977,90 @@ void launch_window(const float* in, float* out, long long n, float wlo, float wh
 }
 
 // ------------------------------------------------------------------------------------------
+// Histogram matching (ITK's HistogramMatchingImageFilter): an image's min, max and per-block
+// double sums (a fixed grid, so the mean's summation order is the same on every run), the
+// histogram of the voxels inside [vlo, vhi], and the piecewise-linear map through the table of
+// match points.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_stats(const float* __restrict__ x, long long n, double* part, unsigned* mm) {
+  __shared__ double ws[8];
+  double sum = 0.0;
+  float lo = FLT_MAX, hi = -FLT_MAX;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    sum += (double)v;
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    lo = fminf(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_down_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    ws[threadIdx.x >> 5] = sum;
+    atomicMin(&mm[0], d_float_to_ordered(lo));
+    atomicMax(&mm[1], d_float_to_ordered(hi));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+    part[blockIdx.x] = t;
+  }
+}
+void launch_stats(const float* x, long long n, double* part, int nblocks, unsigned* mm, cudaStream_t s) {
+  count_launch();
+  k_stats<<<nblocks, 256, 0, s>>>(x, n, part, mm);
+}
+
+__global__ void __launch_bounds__(256) k_hist_range(const float* __restrict__ x, long long n, double lo, double bw,
+                                                    int nb, double vlo, double vhi, unsigned* hist) {
+  extern __shared__ unsigned sh[];
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) sh[b] = 0u;
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = (double)x[i];
+    if (!(v >= vlo && v <= vhi)) continue;  // also drops NaN
+    int b = bw > 0.0 ? (int)((v - lo) / bw) : 0;
+    b = min(max(b, 0), nb - 1);
+    atomicAdd(&sh[b], 1u);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    if (sh[b]) atomicAdd(&hist[b], sh[b]);
+}
+void launch_histogram_range(const float* x, long long n, double lo, double hi, int nbins, double vlo, double vhi,
+                            unsigned* hist, cudaStream_t s) {
+  count_launch();
+  const double bw = (hi - lo) / nbins;
+  k_hist_range<<<grid_for(n, 256), 256, nbins * sizeof(unsigned), s>>>(x, n, lo, bw, nbins, vlo, vhi, hist);
+}
+
+// Unfused double arithmetic (no FMA contraction), as the host computes the same map.
+__global__ void __launch_bounds__(256) k_hist_map(const float* in, float* out, long long n,
+                                                  HistMatchMap t) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = (double)in[i];
+    int j = 0;
+    while (j < t.points + 2 && !(v < t.src[j])) ++j;
+    double r;
+    if (j == 0)
+      r = __dadd_rn(t.ref_min, __dmul_rn(__dsub_rn(v, t.src_min), t.lower_grad));
+    else if (j == t.points + 2)
+      r = __dadd_rn(t.ref_max, __dmul_rn(__dsub_rn(v, t.src_max), t.upper_grad));
+    else
+      r = __dadd_rn(t.ref[j - 1], __dmul_rn(__dsub_rn(v, t.src[j - 1]), t.grad[j - 1]));
+    out[i] = (float)r;
+  }
+}
+void launch_histogram_map(const float* in, float* out, long long n, const HistMatchMap& t, cudaStream_t s) {
+  count_launch();
+  k_hist_map<<<grid_for(n, 256), 256, 0, s>>>(in, out, n, t);
+}
+
+// ------------------------------------------------------------------------------------------
 // Layout conversion.
 // ------------------------------------------------------------------------------------------
 __global__ void k_interleave(const float* __restrict__ planes, float* __restrict__ inter, long long N, int D) {

@@ -141,6 +141,20 @@ void launch_conv_image_axis(const float* in, float* out, const GridInfo& g, int 
 // Intensity statistics / window.
 void launch_minmax(const float* x, long long n, unsigned* mm /* [2]: ordered-int min, max */, cudaStream_t s);
 void launch_histogram(const float* x, long long n, float lo, float hi, int nbins, unsigned* hist, cudaStream_t s);
+// Histogram matching: the table of match points (rows src/ref, points + 2 of them; slopes of
+// the points + 1 segments between them; the lines below the first and above the last point).
+constexpr int HM_MAX_POINTS = 62;
+constexpr int HM_STATS_BLOCKS = 592;  // fixed grid of the statistics pass (4 x 148 SMs)
+struct HistMatchMap {
+  int points;
+  double src[HM_MAX_POINTS + 2], ref[HM_MAX_POINTS + 2], grad[HM_MAX_POINTS + 1];
+  double src_min, src_max, ref_min, ref_max, lower_grad, upper_grad;
+};
+void launch_stats(const float* x, long long n, double* part /* [nblocks] */, int nblocks, unsigned* mm,
+                  cudaStream_t s);
+void launch_histogram_range(const float* x, long long n, double lo, double hi, int nbins, double vlo, double vhi,
+                            unsigned* hist, cudaStream_t s);
+void launch_histogram_map(const float* in, float* out, long long n, const HistMatchMap& t, cudaStream_t s);
 void launch_window(const float* in, float* out, long long n, float wlo, float whi, double scale, double shift,
                    cudaStream_t s);
 

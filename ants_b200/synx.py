@@ -77,7 +77,8 @@ class SynxParams(C.Structure):
         ("persistent_blocks", C.c_int32),
         ("persistent_max_voxels", C.c_int32),
         ("test_inject", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("histogram_match", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -192,6 +193,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_warp_image": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
         "synx_warp_image_nearest": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
         "synx_warp_image_label": (I, [V, P(SynxGeom), V, P(SynxGeom), V, V]),
+        "synx_histogram_match": (I, [V, C.c_int64, V, C.c_int64, C.c_int32, C.c_int32, C.c_int32, V, V]),
         "synx_cc_metric": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
         "synx_cc_metric_noalloc": (I, [V, V, P(SynxGeom), I, V, V, P(D), V]),
         "synx_cc_metric_ex": (I, [V, V, P(SynxGeom), I, I, V, V, P(D), V]),
@@ -271,6 +273,7 @@ class SyNParams:
     persistent_blocks: int = 0  # launch shape of the persistent level kernel (0: automatic)
     persistent_max_voxels: int = 0  # largest level it runs (0: automatic)
     test_inject: int = 0  # SYNX_INJECT_* (failure-detection tests)
+    histogram_match: bool = False  # --use-histogram-matching 1: the moving image matched to the fixed one
 
     def to_c(self) -> SynxParams:
         n = len(self.iterations)
@@ -302,6 +305,7 @@ class SyNParams:
         p.persistent_blocks = self.persistent_blocks
         p.persistent_max_voxels = self.persistent_max_voxels
         p.test_inject = self.test_inject
+        p.histogram_match = int(self.histogram_match)
         return p
 
 
@@ -625,6 +629,14 @@ def warp_image(img, img_geom: Geom, u, grid: Geom, out, stream=None, nearest: bo
     lib = load_library()
     fn = lib.synx_warp_image_label if label else lib.synx_warp_image_nearest if nearest else lib.synx_warp_image
     _check(fn(_ptr(img), C.byref(a), _ptr(u), C.byref(b), _ptr(out), _stream(stream)))
+
+
+def histogram_match(src, ref, out, levels: int = 256, match_points: int = 12, threshold_at_mean: bool = True,
+                    stream=None) -> None:
+    """out = src with its histogram matched to ref's (device float tensors; out may be src).  The
+    defaults are those antsRegistration's --use-histogram-matching 1 runs with."""
+    _check(load_library().synx_histogram_match(_ptr(src), int(src.numel()), _ptr(ref), int(ref.numel()), levels,
+                                               match_points, int(threshold_at_mean), _ptr(out), _stream(stream)))
 
 
 def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None, fp32_sums: bool = False) -> float:

@@ -84,7 +84,9 @@ typedef struct synx_params {
   int32_t persistent_blocks;     /* grid of the persistent level kernel; 0: automatic */
   int32_t persistent_max_voxels; /* largest level run by it; 0: automatic (400,000) */
   int32_t test_inject;           /* 0; SYNX_INJECT_* makes a failure happen for tests */
-  int32_t reserved[5];
+  int32_t histogram_match;       /* 1: after the window, match the moving image's histogram to the fixed
+                                    one's (--use-histogram-matching 1; synx_histogram_match) */
+  int32_t reserved[4];
 } synx_params;
 
 #define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
@@ -268,6 +270,17 @@ int synx_warp_image_nearest(const float* img_dev, const synx_geom* img_geom, con
  * weights, a tie going to the smaller label; 0 outside. */
 int synx_warp_image_label(const float* img_dev, const synx_geom* img_geom, const float* u_dev, const synx_geom* grid,
                           float* out_dev, void* stream);
+
+/* Histogram matching of `src` to `ref` (device float arrays of n_src and n_ref voxels); `out` may be
+ * `src`.  Replaces ITK's HistogramMatchingImageFilter as PreprocessImage runs it for
+ * --use-histogram-matching 1 (Examples/itkantsRegistrationHelper.hxx:111-122: levels 256,
+ * match_points 12, threshold_at_mean 1).  Each image's histogram holds the voxels in
+ * [threshold, max] (threshold: the mean, or the min with threshold_at_mean 0) in `levels` equal
+ * bins over [min, max]; the match points are the thresholds, the quantiles j/(match_points+1) and
+ * the maxima, and each voxel is mapped through the piecewise-linear function between them.
+ * levels in 1..4096, match_points in 1..62.  Synchronises the stream. */
+int synx_histogram_match(const float* src_dev, int64_t n_src, const float* ref_dev, int64_t n_ref, int32_t levels,
+                         int32_t match_points, int32_t threshold_at_mean, float* out_dev, void* stream);
 
 /* Windowed CC on two images on the same grid: value (-mean cc), the fixed-to-middle update
  * direction (uses grad of `moving`) and the moving-to-middle one (uses grad of `fixed`)

@@ -52,6 +52,8 @@ def load() -> C.CDLL:
     for suf in ("f32", "f64"):
         sigs.update({
             f"oracle_preprocess_{suf}": (None, [V, V, C.c_int64, C.c_float, C.c_float]),
+            f"oracle_histogram_match_{suf}": (None, [V, C.c_int64, V, C.c_int64, I, I, I, V]),
+            f"oracle_histogram_match_table_{suf}": (None, [V, C.c_int64, V, C.c_int64, I, I, I, V, V, V, V]),
             f"oracle_smooth_image_{suf}": (None, [V, V, P(G), D, I]),
             f"oracle_warp_image_{suf}": (None, [V, P(G), V, P(G), V]),
             f"oracle_warp_image_nearest_{suf}": (None, [V, P(G), V, P(G), V]),
@@ -113,6 +115,26 @@ def preprocess(img, qlo=0.0, qhi=1.0, dtype=np.float32):
     out = np.empty_like(a)
     getattr(load(), f"oracle_preprocess_{_suf(dtype)}")(_p(a), _p(out), a.size, qlo, qhi)
     return out
+
+
+def histogram_match(src, ref, levels=256, points=12, threshold_at_mean=True, dtype=np.float32):
+    """src with its histogram matched to ref's (ITK's HistogramMatchingImageFilter restated)."""
+    a, b = _c(src, dtype), _c(ref, dtype)
+    out = np.empty_like(a)
+    getattr(load(), f"oracle_histogram_match_{_suf(dtype)}")(_p(a), a.size, _p(b), b.size, levels, points,
+                                                             int(threshold_at_mean), _p(out))
+    return out
+
+
+def histogram_match_table(src, ref, levels=256, points=12, threshold_at_mean=True, dtype=np.float32):
+    """The match-point table: (source points, reference points, slopes, ends) with ends = (source
+    min, source max, reference min, reference max, lower slope, upper slope)."""
+    a, b = _c(src, dtype), _c(ref, dtype)
+    ts, tr, gr, ends = np.zeros(points + 2), np.zeros(points + 2), np.zeros(points + 1), np.zeros(6)
+    getattr(load(), f"oracle_histogram_match_table_{_suf(dtype)}")(_p(a), a.size, _p(b), b.size, levels, points,
+                                                                   int(threshold_at_mean), _p(ts), _p(tr), _p(gr),
+                                                                   _p(ends))
+    return ts, tr, gr, ends
 
 
 def smooth_image(img, g, sigma, mm=False, dtype=np.float32):

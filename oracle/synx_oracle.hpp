@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -312,6 +313,46 @@ inline Geom shrink_geom(const Geom& in, const unsigned f[3]) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Histogram quantile with linear interpolation inside the bin that reaches p, as ITK's
+// Histogram::Quantile computes it (ITK 5.4.6, Modules/Numerics/Statistics/include/itkHistogram.hxx;
+// the version is pinned in SuperBuild/External_ITKv5.cmake:155).  Equal-width bins: bin b spans
+// [lo + b*bw, lo + (b+1)*bw).  Below p = 0.5 the frequencies are accumulated from the first bin
+// upward, otherwise from the last bin downward.
+// ------------------------------------------------------------------------------------------
+inline double histogram_quantile(const std::vector<double>& freq, double lo, double bw, double p) {
+  const int nb = (int)freq.size();
+  double total = 0.0;
+  for (double f : freq) total += f;
+  auto bin_min = [&](int b) { return lo + b * bw; };
+  auto bin_max = [&](int b) { return lo + (b + 1) * bw; };
+  double cum = 0.0, pn = 0.0, pprev = 0.0, fn = 0.0;
+  if (p < 0.5) {
+    int n = 0;
+    do {
+      fn = freq[n];
+      cum += fn;
+      pprev = pn;
+      pn = cum / total;
+      ++n;
+    } while (n < nb && pn < p);
+    double prop = fn / total;
+    return bin_min(n - 1) + ((p - pprev) / prop) * (bin_max(n - 1) - bin_min(n - 1));
+  }
+  int n = nb - 1, m = 0;
+  pn = 1.0;
+  do {
+    fn = freq[n];
+    cum += fn;
+    pprev = pn;
+    pn = 1.0 - cum / total;
+    --n;
+    ++m;
+  } while (m < nb && pn > p);
+  double prop = fn / total;
+  return bin_max(n + 1) - ((pprev - p) / prop) * (bin_max(n + 1) - bin_min(n + 1));
+}
+
+// ------------------------------------------------------------------------------------------
 // Intensity preprocessing (PreprocessImage, Examples/itkantsRegistrationHelper.hxx:76-136):
 // 256-bin histogram with automatic min/max and marginal scale 10 (the upper bound is raised by
 // (max-min)/256/10), quantiles -> intensity window -> linear map to [0, 1] with clamping.
@@ -333,35 +374,7 @@ inline void preprocess_image(const T* in, T* out, int64_t N, float qlo, float qh
     b = std::min(std::max(b, 0), nb - 1);
     freq[b] += 1.0;
   }
-  auto bin_min = [&](int b) { return (double)mn + b * bw; };
-  auto bin_max = [&](int b) { return (double)mn + (b + 1) * bw; };
-  auto quantile = [&](double p) -> double {
-    double total = (double)N, cum = 0.0, pn = 0.0, pprev = 0.0, fn = 0.0;
-    if (p < 0.5) {
-      int n = 0;
-      do {
-        fn = freq[n];
-        cum += fn;
-        pprev = pn;
-        pn = cum / total;
-        ++n;
-      } while (n < nb && pn < p);
-      double prop = fn / total;
-      return bin_min(n - 1) + ((p - pprev) / prop) * (bin_max(n - 1) - bin_min(n - 1));
-    }
-    int n = nb - 1, m = 0;
-    pn = 1.0;
-    do {
-      fn = freq[n];
-      cum += fn;
-      pprev = pn;
-      pn = 1.0 - cum / total;
-      --n;
-      ++m;
-    } while (m < nb && pn > p);
-    double prop = fn / total;
-    return bin_max(n + 1) - ((pprev - p) / prop) * (bin_max(n + 1) - bin_min(n + 1));
-  };
+  auto quantile = [&](double p) { return histogram_quantile(freq, (double)mn, bw, p); };
   float wlo = (float)quantile(qlo), whi = (float)quantile(qhi);
   double scale = (1.0 - 0.0) / ((double)whi - (double)wlo);
   double shift = 0.0 - (double)wlo * scale;
@@ -823,6 +836,113 @@ inline double convergence_value(const std::vector<double>& energies, double tota
 // Examples/itkantsRegistrationHelper.hxx:1983-2164, final fields composed as in
 // Examples/antsDisplacementAndVelocityFieldRegistrationCommandIterationUpdate.h:415-432).
 // ------------------------------------------------------------------------------------------
+// ------------------------------------------------------------------------------------------
+// Histogram matching (--use-histogram-matching 1): PreprocessImage matches the windowed moving
+// image to the preprocessed fixed one with ITK's HistogramMatchingImageFilter, 256 histogram
+// levels, 12 match points, threshold at the mean intensity
+// (Examples/itkantsRegistrationHelper.hxx:111-122, called at :1135-1143).  The filter's algorithm
+// (ITK 5.4.6, Modules/Filtering/ImageIntensity/include/itkHistogramMatchingImageFilter.hxx):
+//  * per image: min, max and mean (a double sum in voxel order, the mean cast to the pixel type);
+//  * per image: a histogram of `levels` equal bins spanning [min, max] of the voxels in
+//    [threshold, max], the threshold being the mean (or the min without thresholding);
+//  * a table of match points: row 0 the thresholds, rows 1..points the quantiles j/(points+1)
+//    of the two histograms, the last row the maxima; the slope between consecutive points,
+//    0 where two source points coincide; below the first point the line through
+//    (source min, reference min), above the last the one through the maxima;
+//  * each source voxel s mapped through that piecewise-linear function, in double, then cast.
+// ------------------------------------------------------------------------------------------
+struct HistogramMatchTable {
+  int points = 0;                      // match points; the table has points + 2 rows
+  std::vector<double> src, ref, grad;  // rows of the table; slopes of the points + 1 segments
+  double src_min = 0, src_max = 0, ref_min = 0, ref_max = 0, lower_grad = 0, upper_grad = 0;
+};
+
+template <class T>
+inline void intensity_stats(const T* x, int64_t n, T& mn, T& mx, T& mean) {
+  mn = std::numeric_limits<T>::max();
+  mx = std::numeric_limits<T>::lowest();
+  double sum = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    sum += (double)x[i];
+    if (x[i] < mn) mn = x[i];
+    if (x[i] > mx) mx = x[i];
+  }
+  mean = (T)(sum / (double)n);
+}
+
+// Frequencies of the voxels in [vlo, vhi], `levels` equal bins over [lo, hi]; the top value
+// falls in the last bin.
+template <class T>
+inline std::vector<double> thresholded_histogram(const T* x, int64_t n, double lo, double hi, double vlo, double vhi,
+                                                 int levels) {
+  std::vector<double> freq(levels, 0.0);
+  const double bw = (hi - lo) / levels;
+  for (int64_t i = 0; i < n; ++i) {
+    const double v = (double)x[i];
+    if (!(v >= vlo && v <= vhi)) continue;
+    int b = bw > 0 ? (int)((v - lo) / bw) : 0;
+    b = std::min(std::max(b, 0), levels - 1);
+    freq[b] += 1.0;
+  }
+  return freq;
+}
+
+template <class T>
+inline HistogramMatchTable histogram_match_table(const T* src, int64_t ns, const T* ref, int64_t nr, int levels,
+                                                 int points, bool threshold_at_mean) {
+  T smin, smax, smean, rmin, rmax, rmean;
+  intensity_stats(src, ns, smin, smax, smean);
+  intensity_stats(ref, nr, rmin, rmax, rmean);
+  const double sthr = threshold_at_mean ? (double)smean : (double)smin;
+  const double rthr = threshold_at_mean ? (double)rmean : (double)rmin;
+  const auto hs = thresholded_histogram(src, ns, (double)smin, (double)smax, sthr, (double)smax, levels);
+  const auto hr = thresholded_histogram(ref, nr, (double)rmin, (double)rmax, rthr, (double)rmax, levels);
+  const double bws = ((double)smax - (double)smin) / levels, bwr = ((double)rmax - (double)rmin) / levels;
+  HistogramMatchTable t;
+  t.points = points;
+  t.src.assign(points + 2, 0.0);
+  t.ref.assign(points + 2, 0.0);
+  t.src[0] = sthr;
+  t.ref[0] = rthr;
+  t.src[points + 1] = (double)smax;
+  t.ref[points + 1] = (double)rmax;
+  const double delta = 1.0 / ((double)points + 1.0);
+  for (int j = 1; j <= points; ++j) {
+    t.src[j] = histogram_quantile(hs, (double)smin, bws, j * delta);
+    t.ref[j] = histogram_quantile(hr, (double)rmin, bwr, j * delta);
+  }
+  t.grad.assign(points + 1, 0.0);
+  for (int j = 0; j <= points; ++j) {
+    const double den = t.src[j + 1] - t.src[j];
+    t.grad[j] = den != 0.0 ? (t.ref[j + 1] - t.ref[j]) / den : 0.0;
+  }
+  t.src_min = (double)smin;
+  t.src_max = (double)smax;
+  t.ref_min = (double)rmin;
+  t.ref_max = (double)rmax;
+  const double dlo = t.src[0] - t.src_min;
+  t.lower_grad = dlo != 0.0 ? (t.ref[0] - t.ref_min) / dlo : 0.0;
+  const double dhi = t.src[points + 1] - t.src_max;
+  t.upper_grad = dhi != 0.0 ? (t.ref[points + 1] - t.ref_max) / dhi : 0.0;
+  return t;
+}
+
+// The piecewise-linear map of one source value.
+inline double histogram_match_value(const HistogramMatchTable& t, double s) {
+  int j = 0;
+  while (j < t.points + 2 && !(s < t.src[j])) ++j;
+  if (j == 0) return t.ref_min + (s - t.src_min) * t.lower_grad;
+  if (j == t.points + 2) return t.ref_max + (s - t.src_max) * t.upper_grad;
+  return t.ref[j - 1] + (s - t.src[j - 1]) * t.grad[j - 1];
+}
+
+template <class T>
+inline void histogram_match(const T* src, int64_t ns, const T* ref, int64_t nr, int levels, int points,
+                            bool threshold_at_mean, T* out) {
+  const HistogramMatchTable t = histogram_match_table(src, ns, ref, nr, levels, points, threshold_at_mean);
+  for (int64_t i = 0; i < ns; ++i) out[i] = (T)histogram_match_value(t, (double)src[i]);
+}
+
 struct SynParams {
   double eta = 0.1, var_update = 3.0, var_total = 0.0;
   int radius = 4;
@@ -835,6 +955,7 @@ struct SynParams {
   int conv_window = 10;
   bool preprocess = true;
   float q_lo = 0.0f, q_hi = 1.0f;
+  bool histogram_match = false;  // the moving image matched to the fixed one after the window
 };
 
 struct SynLog {
@@ -896,6 +1017,7 @@ inline void syn_register(const T* F_in, const Geom& gF, const T* M_in, const Geo
     std::memcpy(F.data(), F_in, sizeof(T) * NF);
     std::memcpy(M.data(), M_in, sizeof(T) * NM);
   }
+  if (P.histogram_match) histogram_match(M.data(), NM, F.data(), NF, 256, 12, true, M.data());
   SynState<T> S;
   std::vector<T> Fs(NF), Ms(NM);
   for (int l = 0; l < P.n_levels; ++l) {

@@ -50,6 +50,7 @@ static SynParams to_params(const synx_params* p) {
   P.preprocess = p->preprocess != 0;
   P.q_lo = p->winsor_lower;
   P.q_hi = p->winsor_upper;
+  P.histogram_match = p->histogram_match != 0;
   return P;
 }
 
@@ -87,6 +88,21 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
 #define ORACLE_TYPED(SUF, T)                                                                         \
   void oracle_preprocess_##SUF(const T* in, T* out, int64_t n, float qlo, float qhi) {               \
     preprocess_image(in, out, n, qlo, qhi);                                                          \
+  }                                                                                                  \
+  void oracle_histogram_match_##SUF(const T* src, int64_t ns, const T* ref, int64_t nr, int levels,    \
+                                    int points, int thr_mean, T* out) {                              \
+    histogram_match(src, ns, ref, nr, levels, points, thr_mean != 0, out);                           \
+  }                                                                                                  \
+  /* table rows src[points+2], ref[points+2], slopes grad[points+1]; ends: src min, src max, */       \
+  /* ref min, ref max, lower slope, upper slope */                                                   \
+  void oracle_histogram_match_table_##SUF(const T* src, int64_t ns, const T* ref, int64_t nr,         \
+                                          int levels, int points, int thr_mean, double* tsrc,        \
+                                          double* tref, double* grad, double* ends) {                \
+    HistogramMatchTable t = histogram_match_table(src, ns, ref, nr, levels, points, thr_mean != 0);   \
+    for (int j = 0; j < points + 2; ++j) tsrc[j] = t.src[j], tref[j] = t.ref[j];                     \
+    for (int j = 0; j < points + 1; ++j) grad[j] = t.grad[j];                                        \
+    const double e[6] = {t.src_min, t.src_max, t.ref_min, t.ref_max, t.lower_grad, t.upper_grad};    \
+    for (int k = 0; k < 6; ++k) ends[k] = e[k];                                                      \
   }                                                                                                  \
   void oracle_smooth_image_##SUF(const T* in, T* out, const synx_geom* g, double sigma, int mm) {    \
     smooth_image(in, out, to_geom(g), sigma, mm != 0);                                               \

@@ -84,3 +84,16 @@ def test_output_types(host_cli, tmp_path):
 
 def test_output_precision(host_cli, tmp_path):
     S.check_output_precision(host_cli["reg"], tmp_path)
+
+
+def test_histogram_matching(host_cli, tmp_path):
+    import numpy as np
+
+    import oracle as O
+    import test_zz_histogram_match_gpu as H
+
+    def stage_fields(f, gf, m, gm, P):
+        fwd, inv, _, _ = O.syn_register(f, gf, m, gm, P)
+        return np.moveaxis(fwd, 0, -1), np.moveaxis(inv, 0, -1)
+
+    H.check_cli_histogram_matching(host_cli["reg"], tmp_path, stage_fields)
