@@ -247,6 +247,26 @@ def _ptr(a) -> int:
     return a.data_ptr()
 
 
+def _dev(t, numel: int, name: str) -> int:
+    """Device pointer of a contiguous float32 CUDA tensor with at least `numel` values.  Anything else
+    is refused here: a host pointer or a short buffer reaching a kernel would be a memory fault."""
+    if isinstance(t, np.ndarray) or not getattr(t, "is_cuda", False):
+        raise SynxError(f"{name}: a CUDA tensor is required")
+    if str(t.dtype) != "torch.float32" or not t.is_contiguous():
+        raise SynxError(f"{name}: a contiguous float32 tensor is required")
+    if t.numel() < numel:
+        raise SynxError(f"{name}: {t.numel()} values, the geometry needs {numel}")
+    return t.data_ptr()
+
+
+def _host(a, numel: int, name: str) -> np.ndarray:
+    """A C-contiguous float32 copy (or view) of a host array with exactly `numel` values."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.size != numel:
+        raise SynxError(f"{name}: {a.size} values, the geometry needs {numel}")
+    return a
+
+
 # ---- stage parameters --------------------------------------------------------------------------
 @dataclass
 class SyNParams:
@@ -369,8 +389,8 @@ class Server:
         """Queue a request; `out` = (forward, inverse) float32 host arrays of shape
         fixed_geom.shape + (dim,) to receive the fields (allocated here when omitted; pass pinned
         arrays for faster copies)."""
-        f = np.ascontiguousarray(fixed, dtype=np.float32)
-        m = np.ascontiguousarray(moving, dtype=np.float32)
+        f = _host(fixed, fixed_geom.count, "fixed")
+        m = _host(moving, moving_geom.count, "moving")
         shp = tuple(fixed_geom.shape) + (params.dim,)
         if out is None:
             fwd = np.empty(shp, np.float32)
@@ -500,12 +520,13 @@ class SyNStage:
             moving_geom = fold_moving_geometry(moving_geom, moving_initial)
         gf, gm = fixed_geom.to_c(), moving_geom.to_c()
         if isinstance(fixed, np.ndarray):
-            f = np.ascontiguousarray(fixed, dtype=np.float32)
-            m = np.ascontiguousarray(moving, dtype=np.float32)
+            f = _host(fixed, fixed_geom.count, "fixed")
+            m = _host(moving, moving_geom.count, "moving")
             self._keep = (f, m)
             self._ck(self.lib.synx_set_images(self.h, _ptr(f), C.byref(gf), _ptr(m), C.byref(gm)))
         else:
-            self._ck(self.lib.synx_set_images_device(self.h, _ptr(fixed), C.byref(gf), _ptr(moving), C.byref(gm)))
+            self._ck(self.lib.synx_set_images_device(self.h, _dev(fixed, fixed_geom.count, "fixed"), C.byref(gf),
+                                                     _dev(moving, moving_geom.count, "moving"), C.byref(gm)))
 
     def run(self) -> None:
         self._ck(self.lib.synx_run(self.h))
@@ -532,7 +553,9 @@ class SyNStage:
         return fwd, inv
 
     def fields_device(self, fwd, inv) -> None:
-        self._ck(self.lib.synx_get_fields_device(self.h, _ptr(fwd), _ptr(inv)))
+        g = self.output_geom()
+        n = g.dim * g.count
+        self._ck(self.lib.synx_get_fields_device(self.h, _dev(fwd, n, "fwd"), _dev(inv, n, "inv")))
 
     def half_fields(self) -> tuple:
         g = self.output_geom()
@@ -542,7 +565,7 @@ class SyNStage:
         return tuple(out)
 
     def set_half_fields(self, phi_f, psi_f, phi_m, psi_m, grid: Geom) -> None:
-        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (phi_f, psi_f, phi_m, psi_m)]
+        arrs = [_host(a, grid.dim * grid.count, "half field") for a in (phi_f, psi_f, phi_m, psi_m)]
         g = grid.to_c()
         self._ck(self.lib.synx_set_half_fields(self.h, *[_ptr(a) for a in arrs], C.byref(g)))
 
@@ -617,7 +640,8 @@ def _stream(stream) -> C.c_void_p:
 
 def smooth_image(img, out, g: Geom, sigma: float, sigma_in_mm: bool = False, stream=None) -> None:
     gc = g.to_c()
-    _check(load_library().synx_smooth_image(_ptr(img), _ptr(out), C.byref(gc), sigma, int(sigma_in_mm),
+    _check(load_library().synx_smooth_image(_dev(img, g.count, "img"), _dev(out, g.count, "out"), C.byref(gc),
+                                            sigma, int(sigma_in_mm),
                                             _stream(stream)))
 
 
@@ -628,15 +652,18 @@ def warp_image(img, img_geom: Geom, u, grid: Geom, out, stream=None, nearest: bo
     a, b = img_geom.to_c(), grid.to_c()
     lib = load_library()
     fn = lib.synx_warp_image_label if label else lib.synx_warp_image_nearest if nearest else lib.synx_warp_image
-    _check(fn(_ptr(img), C.byref(a), _ptr(u), C.byref(b), _ptr(out), _stream(stream)))
+    _check(fn(_dev(img, img_geom.count, "img"), C.byref(a), _dev(u, grid.dim * grid.count, "u"), C.byref(b),
+              _dev(out, grid.count, "out"), _stream(stream)))
 
 
 def histogram_match(src, ref, out, levels: int = 256, match_points: int = 12, threshold_at_mean: bool = True,
                     stream=None) -> None:
     """out = src with its histogram matched to ref's (device float tensors; out may be src).  The
     defaults are those antsRegistration's --use-histogram-matching 1 runs with."""
-    _check(load_library().synx_histogram_match(_ptr(src), int(src.numel()), _ptr(ref), int(ref.numel()), levels,
-                                               match_points, int(threshold_at_mean), _ptr(out), _stream(stream)))
+    n = int(src.numel())
+    _check(load_library().synx_histogram_match(_dev(src, n, "src"), n, _dev(ref, 1, "ref"), int(ref.numel()), levels,
+                                               match_points, int(threshold_at_mean), _dev(out, n, "out"),
+                                               _stream(stream)))
 
 
 def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None, fp32_sums: bool = False) -> float:
@@ -644,7 +671,9 @@ def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None, fp32_sums: bool =
     gc = g.to_c()
     v = C.c_double()
     flags = SYNX_F_CC_FP32_SUMS if fp32_sums else 0
-    _check(load_library().synx_cc_metric_ex(_ptr(F), _ptr(M), C.byref(gc), radius, flags, _ptr(gF), _ptr(gM),
+    n = g.count
+    _check(load_library().synx_cc_metric_ex(_dev(F, n, "F"), _dev(M, n, "M"), C.byref(gc), radius, flags,
+                                            _dev(gF, g.dim * n, "gF"), _dev(gM, g.dim * n, "gM"),
                                             C.byref(v), _stream(stream)))
     return v.value
 
@@ -656,7 +685,9 @@ def cc_metric_noalloc(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
     lib = load_library()
     gc = g.to_c()
     v = C.c_double()
-    rc = lib.synx_cc_metric_noalloc(_ptr(F), _ptr(M), C.byref(gc), radius, _ptr(gF), _ptr(gM), C.byref(v),
+    n = g.count
+    rc = lib.synx_cc_metric_noalloc(_dev(F, n, "F"), _dev(M, n, "M"), C.byref(gc), radius, _dev(gF, g.dim * n, "gF"),
+                                    _dev(gM, g.dim * n, "gM"), C.byref(v),
                                     _stream(stream))
     if rc != 0:
         raise SynxError(f"synx error {rc} ({ERRORS.get(rc, '?')}): {lib.synx_noalloc_last_error().decode()}")
@@ -666,26 +697,33 @@ def cc_metric_noalloc(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
 def smooth_field(u, out, g: Geom, variance: float, stream=None) -> float:
     gc = g.to_c()
     mx = C.c_double()
-    _check(load_library().synx_smooth_field(_ptr(u), _ptr(out), C.byref(gc), variance, C.byref(mx), _stream(stream)))
+    n = g.dim * g.count
+    _check(load_library().synx_smooth_field(_dev(u, n, "u"), _dev(out, n, "out"), C.byref(gc), variance, C.byref(mx),
+                                            _stream(stream)))
     return mx.value
 
 
 def compose(d, w, g: Geom, out, scale: float = 1.0, stream=None) -> None:
     gc = g.to_c()
-    _check(load_library().synx_compose(_ptr(d), _ptr(w), C.byref(gc), scale, _ptr(out), _stream(stream)))
+    n = g.dim * g.count
+    _check(load_library().synx_compose(_dev(d, n, "d"), _dev(w, n, "w"), C.byref(gc), scale, _dev(out, n, "out"),
+                                       _stream(stream)))
 
 
 def invert_field(phi, psi, g: Geom, max_iter=20, mean_tol=0.001, max_tol=0.1, stream=None) -> int:
     gc = g.to_c()
     it = C.c_int()
-    _check(load_library().synx_invert_field(_ptr(phi), _ptr(psi), C.byref(gc), max_iter, mean_tol, max_tol,
+    n = g.dim * g.count
+    _check(load_library().synx_invert_field(_dev(phi, n, "phi"), _dev(psi, n, "psi"), C.byref(gc), max_iter, mean_tol,
+                                            max_tol,
                                             C.byref(it), _stream(stream)))
     return it.value
 
 
 def resample_field(u, gi: Geom, out, go: Geom, stream=None) -> None:
     a, b = gi.to_c(), go.to_c()
-    _check(load_library().synx_resample_field(_ptr(u), C.byref(a), _ptr(out), C.byref(b), _stream(stream)))
+    _check(load_library().synx_resample_field(_dev(u, gi.dim * gi.count, "u"), C.byref(a),
+                                              _dev(out, go.dim * go.count, "out"), C.byref(b), _stream(stream)))
 
 
 @dataclass
