@@ -90,7 +90,7 @@ def test_histogram_matching(host_cli, tmp_path):
     import numpy as np
 
     import oracle as O
-    import test_zz_histogram_match_gpu as H
+    import test_zz_u_histogram_match_gpu as H
 
     def stage_fields(f, gf, m, gm, P):
         fwd, inv, _, _ = O.syn_register(f, gf, m, gm, P)

@@ -6,7 +6,7 @@ mean intensity (Examples/itkantsRegistrationHelper.hxx:111-122, called at :1135-
 part of the reference tree, so the oracle's restatement (ITK 5.4.6, the version
 SuperBuild/External_ITKv5.cmake:155 pins) is checked here against a second, vectorised numpy
 restatement and against the properties the filter's construction guarantees.  The device kernels
-are checked against the oracle in test_zz_histogram_match_gpu.py.
+are checked against the oracle in test_zz_u_histogram_match_gpu.py.
 """
 import numpy as np
 import pytest
