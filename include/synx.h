@@ -84,8 +84,9 @@ typedef struct synx_params {
   int32_t persistent_blocks;     /* grid of the persistent level kernel; 0: automatic */
   int32_t persistent_max_voxels; /* largest level run by it; 0: automatic (400,000) */
   int32_t test_inject;           /* 0; SYNX_INJECT_* makes a failure happen for tests */
-  int32_t histogram_match;       /* 1: after the window, match the moving image's histogram to the fixed
-                                    one's (--use-histogram-matching 1; synx_histogram_match) */
+  int32_t histogram_match;       /* 1: match the moving image's histogram to the fixed one's after the
+                                    window, or on the images as given when preprocess is 0
+                                    (--use-histogram-matching 1; synx_histogram_match) */
   int32_t reserved[4];
 } synx_params;
 
