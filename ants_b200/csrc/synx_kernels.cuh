@@ -143,7 +143,7 @@ void launch_minmax(const float* x, long long n, unsigned* mm /* [2]: ordered-int
 void launch_histogram(const float* x, long long n, float lo, float hi, int nbins, unsigned* hist, cudaStream_t s);
 // Histogram matching: the table of match points (rows src/ref, points + 2 of them; slopes of
 // the points + 1 segments between them; the lines below the first and above the last point).
-constexpr int HM_MAX_POINTS = 62;
+constexpr int HM_MAX_POINTS = 64;
 constexpr int HM_STATS_BLOCKS = 592;  // fixed grid of the statistics pass (4 x 148 SMs)
 struct HistMatchMap {
   int points;

@@ -279,7 +279,8 @@ int synx_warp_image_label(const float* img_dev, const synx_geom* img_geom, const
  * [threshold, max] (threshold: the mean, or the min with threshold_at_mean 0) in `levels` equal
  * bins over [min, max]; the match points are the thresholds, the quantiles j/(match_points+1) and
  * the maxima, and each voxel is mapped through the piecewise-linear function between them.
- * levels in 1..4096, match_points in 1..62.  Synchronises the stream. */
+ * levels in 1..4096, match_points in 1..64 (ImageMath HistogramMatch runs 255 and 64 by default,
+ * Examples/ImageMath_Templates.hxx:1758-1789).  Synchronises the stream. */
 int synx_histogram_match(const float* src_dev, int64_t n_src, const float* ref_dev, int64_t n_ref, int32_t levels,
                          int32_t match_points, int32_t threshold_at_mean, float* out_dev, void* stream);
 

@@ -87,7 +87,7 @@ def images(case):
 
 
 @pytest.mark.parametrize("case", ["2d", "3d"])
-@pytest.mark.parametrize("levels,points,thr_mean", [(256, 12, True), (256, 12, False), (64, 5, True), (7, 1, True)])
+@pytest.mark.parametrize("levels,points,thr_mean", [(256, 12, True), (256, 12, False), (64, 5, True), (7, 1, True), (255, 64, False)])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_oracle_matches_numpy_restatement(case, levels, points, thr_mean, dtype):
     ref, src = images(case)

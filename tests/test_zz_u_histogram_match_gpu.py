@@ -28,7 +28,7 @@ def remapped_pair(size, seed):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["2d", "3d"])
-@pytest.mark.parametrize("levels,points,thr_mean", [(256, 12, True), (256, 12, False), (64, 5, True), (7, 1, True)])
+@pytest.mark.parametrize("levels,points,thr_mean", [(256, 12, True), (256, 12, False), (64, 5, True), (7, 1, True), (255, 64, False)])
 def test_device_matches_oracle(cuda, case, levels, points, thr_mean):
     import torch
     ref, src = images(case)
