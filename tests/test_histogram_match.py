@@ -155,3 +155,20 @@ def test_registration_applies_it_to_the_moving_image_after_the_window():
     np.testing.assert_array_equal(a[1], b[1])
     c = O.syn_register(ref_raw, g, m, g, SyNParams(**{**P.__dict__, "histogram_match": False}))
     assert not np.array_equal(a[0], c[0])  # the option changes the registration
+
+
+def test_constant_images():
+    # zero-width bins: every quantile is the constant, every slope 0, and the source maps to the
+    # reference's maximum (no table point lies above it)
+    src = np.full((10, 12), 0.25, np.float32)
+    ref = np.linspace(0, 1, 120, dtype=np.float32).reshape(10, 12)
+    ts, tr, gr, ends = O.histogram_match_table(src, ref)
+    assert np.all(ts == np.float32(0.25)) and np.all(gr == 0) and ends[4] == 0 and ends[5] == 0
+    out = O.histogram_match(src, ref)
+    np.testing.assert_array_equal(out, np.full_like(src, ref.max()))
+    np.testing.assert_array_equal(out, np_match(src, ref))
+    # a constant reference: all reference points coincide, so everything at or above the source's
+    # mean maps onto that constant and the lower line runs flat from the reference minimum
+    out = O.histogram_match(ref, np.full_like(ref, 0.5))
+    np.testing.assert_array_equal(out, np_match(ref, np.full_like(ref, 0.5)))
+    assert np.all(out == np.float32(0.5))

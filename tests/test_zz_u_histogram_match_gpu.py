@@ -115,3 +115,21 @@ def test_cli_histogram_matching(cuda, tmp_path):
             return st.fields()
 
     check_cli_histogram_matching(build.CLI, tmp_path, stage_fields)
+
+
+@pytest.mark.gpu
+def test_device_edge_cases(cuda):
+    import torch
+    from ants_b200.synx import SynxError
+    # a constant source (zero-width bins) and a constant reference, as in the oracle's own tests
+    src = np.full((10, 12), 0.25, np.float32)
+    ref = np.linspace(0, 1, 120, dtype=np.float32).reshape(10, 12)
+    for a, b in ((src, ref), (ref, np.full_like(ref, 0.5))):
+        s, r = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+        out = torch.empty_like(s)
+        synx.histogram_match(s, r, out)
+        np.testing.assert_array_equal(out.cpu().numpy(), O.histogram_match(a, b))
+    # an empty source is refused by the library, not launched
+    e = torch.empty(0, device=cuda)
+    with pytest.raises(SynxError):
+        synx.histogram_match(e, torch.from_numpy(ref).to(cuda), e)
