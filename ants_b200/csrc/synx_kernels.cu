@@ -68,19 +68,61 @@ GridInfo make_grid(int dim, const int64_t size[3], const double sp[3], const dou
   return g;
 }
 
-Affine make_affine(const GridInfo& src, const GridInfo& dst) {
-  Affine a;
-  double dorg[3] = {src.org[0] - dst.org[0], src.org[1] - dst.org[1], src.org[2] - dst.org[2]};
+// Grids of one pyramid share the fixed image's direction cosines.  Between such grids the
+// index map is formed in their common frame, B = diag(sp_src / sp_dst) with exact zeros and
+// t = D^-1 (org_src - org_dst) / sp_dst, so that an even shrink factor's half-voxel rim points
+// (c = -0.5, c = n - 0.5) come out exact instead of carrying the rotation's rounding noise
+// into ITK's inside-buffer test.  Other grid pairs go through the physical frame.
+static bool same_direction(const GridInfo& a, const GridInfo& b) {
+  const int dim = a.d.dim;
+  if (dim != b.d.dim) return false;
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c)
+      if (a.dir[r * 3 + c] != b.dir[r * 3 + c]) return false;
+  return true;
+}
+
+void index_map(const GridInfo& src, const GridInfo& dst, double t[3], double B[9]) {
+  const int dim = src.d.dim;
+  const double dorg[3] = {src.org[0] - dst.org[0], src.org[1] - dst.org[1], dim == 3 ? src.org[2] - dst.org[2] : 0.0};
+  if (same_direction(src, dst)) {
+    double D[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, Di[9];
+    for (int r = 0; r < dim; ++r)
+      for (int c = 0; c < dim; ++c) D[r * 3 + c] = src.dir[r * 3 + c];
+    inv3(D, Di);
+    for (int r = 0; r < 3; ++r) {
+      const bool on = r < dim;
+      for (int c = 0; c < 3; ++c) B[r * 3 + c] = (r == c && on) ? src.sp[r] / dst.sp[r] : 0.0;
+      t[r] = on ? (Di[r * 3 + 0] * dorg[0] + Di[r * 3 + 1] * dorg[1] + Di[r * 3 + 2] * dorg[2]) / dst.sp[r] : 0.0;
+    }
+    return;
+  }
   for (int r = 0; r < 3; ++r) {
-    double t = 0.0;
+    double tt = 0.0;
     for (int c = 0; c < 3; ++c) {
-      t += dst.p2i[r * 3 + c] * dorg[c];
+      tt += dst.p2i[r * 3 + c] * dorg[c];
       double b = 0.0;
       for (int k = 0; k < 3; ++k) b += dst.p2i[r * 3 + k] * src.i2p[k * 3 + c];
-      a.B[r * 3 + c] = (float)b;
+      B[r * 3 + c] = b;
+    }
+    t[r] = tt;
+  }
+  if (dim == 2) {
+    t[2] = 0.0;
+    B[2] = B[5] = B[6] = B[7] = B[8] = 0.0;
+  }
+}
+
+Affine make_affine(const GridInfo& src, const GridInfo& dst) {
+  Affine a;
+  double t[3], B[9];
+  index_map(src, dst, t, B);
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) {
+      a.B[r * 3 + c] = (float)B[r * 3 + c];
       a.A[r * 3 + c] = (float)dst.p2i[r * 3 + c];
     }
-    a.t[r] = (float)t;
+    a.t[r] = (float)t[r];
   }
   return a;
 }
@@ -839,18 +881,63 @@ struct Ptr4 {
   float* p[4];
 };
 
+// Index map in double: c = ((t + B0 x) + B1 y) + B2 z, each operation rounded on its own (no
+// fused multiply-add), so the inside-buffer decision at a half-voxel rim tie is the one the
+// host-side map's exact arithmetic gives.  Once per level and field, so the FP64 cost is nil.
+struct MapD {
+  double t[3];
+  double B[9];
+};
+
+__device__ __forceinline__ double map_axis_d(const MapD& m, int r, double x, double y, double z) {
+  double v = __dadd_rn(m.t[r], __dmul_rn(m.B[r * 3 + 0], x));
+  v = __dadd_rn(v, __dmul_rn(m.B[r * 3 + 1], y));
+  return __dadd_rn(v, __dmul_rn(m.B[r * 3 + 2], z));
+}
+
+// Clamp-to-edge cell from a double continuous index (weights rounded to float once).
+__device__ __forceinline__ void axis_cell_d(double c, int n, int& i0, int& i1, float& w) {
+  const double f = floor(c);
+  int b = (int)f;
+  double wd = c - f;
+  if (b < 0) {
+    b = 0;
+    wd = 0.0;
+  }
+  int u = b + 1;
+  if (u > n - 1) {
+    u = n - 1;
+    wd = 0.0;
+  }
+  i0 = b;
+  i1 = u;
+  w = (float)wd;
+}
+
 template <int DIM>
-__global__ void __launch_bounds__(256) k_resample(Ptr4c in, Dims di, Ptr4 out, Dims dout, int zb, Affine m, int nf) {
+__global__ void __launch_bounds__(256) k_resample(Ptr4c in, Dims di, Ptr4 out, Dims dout, int zb, MapD m, int nf) {
   const Coord3 c3 = coord3(dout, zb, 1);
   if (!c3.ok) return;
   const int No = (int)dout.N, Ni = (int)di.N, nxy = dout.nx * dout.ny;
   for (int z = c3.z0; z < c3.z1; ++z) {
     const int i = z * nxy + c3.y * dout.nx + c3.x;
-    float cx, cy, cz;
-    map_point<DIM>(m, (float)c3.x, (float)c3.y, (float)z, 0.0f, 0.0f, 0.0f, cx, cy, cz);
-    const bool ok = inside_buffer<DIM>(di, cx, cy, cz);
+    const double fx = (double)c3.x, fy = (double)c3.y, fz = (double)z;
+    const double cx = map_axis_d(m, 0, fx, fy, fz), cy = map_axis_d(m, 1, fx, fy, fz);
+    const double cz = DIM == 3 ? map_axis_d(m, 2, fx, fy, fz) : 0.0;
+    bool ok = (cx >= -0.5) && (cx < (double)di.nx - 0.5) && (cy >= -0.5) && (cy < (double)di.ny - 0.5);
+    if (DIM == 3) ok = ok && (cz >= -0.5) && (cz < (double)di.nz - 0.5);
     Cell c{};
-    if (ok) c = make_cell<DIM>(di, cx, cy, cz);
+    if (ok) {
+      int x0, x1, y0, y1, z0 = 0, z1 = 0;
+      axis_cell_d(cx, di.nx, x0, x1, c.wx);
+      axis_cell_d(cy, di.ny, y0, y1, c.wy);
+      if (DIM == 3) axis_cell_d(cz, di.nz, z0, z1, c.wz);
+      const int sy = di.nx, sz = di.nx * di.ny;
+      c.o000 = z0 * sz + y0 * sy + x0;
+      c.dx = x1 - x0;
+      c.dy = (y1 - y0) * sy;
+      c.dz = (z1 - z0) * sz;
+    }
     for (int f = 0; f < nf; ++f)
 #pragma unroll
       for (int k = 0; k < DIM; ++k) out.p[f][k * No + i] = ok ? lerp_at<DIM>(in.p[f] + k * Ni, c) : 0.0f;
@@ -880,7 +967,8 @@ void launch_resample_fields(const float* const* in, const GridInfo& gi, float* c
     pi.p[f] = in[f];
     po.p[f] = out[f];
   }
-  Affine a = make_affine(go, gi);
+  MapD a;
+  index_map(go, gi, a.t, a.B);
   const Map3 m = map3(go.d);
   if (go.d.dim == 3)
     k_resample<3><<<m.grid, 256, 0, s>>>(pi, gi.d, po, go.d, m.zb, a, nfields);

@@ -56,6 +56,9 @@ struct GridInfo {
 GridInfo make_grid(int dim, const int64_t size[3], const double sp[3], const double org[3], const double dir[9]);
 // c = t + B i + A u mapping voxel i of `src` displaced by u into continuous index of `dst`.
 Affine make_affine(const GridInfo& src, const GridInfo& dst);
+// The index part of that map in double (c = t + B i); exact zeros off the diagonal when both
+// grids share their direction cosines.
+void index_map(const GridInfo& src, const GridInfo& dst, double t[3], double B[9]);
 
 struct PartialBufs {
   double* sum;       // per-block partial sums

@@ -1,16 +1,18 @@
 // Allocation-free entry point for the neighbourhood-CC step.
 //
-// Some callers of this library cannot call cudaMalloc: a pipeline that is being recorded into
-// a CUDA graph (a device allocation is not a stream operation, so it cannot be captured, and it
-// synchronises the device), a host that runs registration inside a device-memory budget owned
-// by another runtime (a serving process, a plug-in inside a viewer or a deep-learning
-// framework's caching allocator), or a latency-bound loop that must not stall its other streams
-// on an allocation.  synx_cc_metric() allocates a small control block and the per-block partial
-// sums of the metric on every call; synx_cc_metric_noalloc() runs the same kernel with that
-// scratch taken from a fixed array in device memory instead.
+// Some callers of this library cannot call cudaMalloc: a plug-in whose host application (a
+// viewer, a deep-learning framework with its own caching allocator, a serving process) owns the
+// GPU's memory and its budget, or a latency-bound loop that cannot afford the device-wide
+// synchronisation a cudaMalloc/cudaFree pair can cause.  synx_cc_metric() allocates a small
+// control block and the per-block partial sums of the metric on every call;
+// synx_cc_metric_noalloc() runs the same kernel with that scratch taken from a fixed array in
+// device memory instead.
 //
 // The array below is part of the library image: every GPU on which the library is used keeps
-// it (about 260 KB) until the process exits.  All calls on a device share it.
+// it (about 260 KB) until the process exits.  All calls on a device share it and find the last
+// call's contents there; the control block is cleared on the stream before every launch.  The
+// first call on a device looks up the array's device address (cudaGetSymbolAddress), so that
+// first call should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cstring>

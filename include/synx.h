@@ -294,17 +294,19 @@ int synx_cc_metric(const float* fixed_dev, const float* moving_dev, const synx_g
 int synx_cc_metric_ex(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius, int flags,
                       float* grad_fixed_dev, float* grad_moving_dev, double* value, void* cuda_stream);
 
-/* Same computation as synx_cc_metric, for callers that cannot allocate device memory (a
- * pipeline being captured into a CUDA graph, a host whose device memory is owned by another
- * allocator, a loop that must not stall on an allocation).  No counterpart in the reference.
+/* Same computation as synx_cc_metric, for callers that must not allocate device memory: a
+ * plug-in whose host application (a viewer, a framework with its own caching allocator, a
+ * serving process) owns the GPU's memory budget, or a latency-bound loop that cannot afford the
+ * device-wide synchronisation of a cudaMalloc/cudaFree pair.  No counterpart in the reference.
  * It calls no cudaMalloc/cudaFree: the kernel's scratch (control block and per-block partial
  * sums, about 260 KB) is a fixed array in device memory that each GPU using the library holds
  * until the process exits.  Limit: grids needing more than 32768 CC blocks (for example more
  * than 8192 x 1024 voxels per slice) are rejected with SYNX_E_ARG.  The first call on a device
- * looks the array's device address up (make it before any stream capture).  All calls on a
- * device share the array: calls that overlap on the GPU (other streams, other host threads)
- * race.  value_host may be NULL; otherwise the call waits for its stream to read the value.
- * Errors are reported by synx_noalloc_last_error(). */
+ * looks the array's device address up, so make that first call before any stream capture.  All
+ * calls on a device share the array and find the previous call's contents in it (the control
+ * block is cleared before each launch): calls that overlap on the GPU (other streams, other
+ * host threads) race.  value_host may be NULL; otherwise the call waits for its stream to read
+ * the value.  Errors are reported by synx_noalloc_last_error(). */
 int synx_cc_metric_noalloc(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
                            float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
 const char* synx_noalloc_last_error(void);

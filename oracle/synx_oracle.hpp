@@ -780,18 +780,93 @@ inline int invert_field(const T* phi, T* psi, const Geom& g, int max_iter = 20, 
   return it - 1;
 }
 
+// ------------------------------------------------------------------------------------------
+// Index map between two grids: voxel index i of `src` lands at continuous index
+// c = t + B i of `dst`.  Grids of one registration pyramid share the fixed image's direction
+// cosines, and then the map is formed in the grids' common frame: B = diag(sp_src / sp_dst)
+// with exact zeros off the diagonal, t = D^-1 (org_src - org_dst) / sp_dst.  Formed through
+// the physical frame instead, B picks up ~1e-17 off-diagonal terms from the rotation, and a
+// shrink by an even factor puts the finer grid's rim voxels exactly on the coarser grid's
+// half-voxel buffer bounds (c = -0.5 and c = n - 0.5, the ShrinkImageFilter centring of
+// Examples/itkantsRegistrationHelper.hxx:16-39), where that noise decides inside or outside.
+// In the common frame those rim points come out exact for power-of-two shrink factors, so the
+// buffer rule (inside at -0.5, outside at n - 0.5) is applied to the exact point.  The same
+// t and B, evaluated as ((t + B0 x) + B1 y) + B2 z in double, are what the device library's
+// level resampling uses.
+// ------------------------------------------------------------------------------------------
+inline bool same_direction(const Geom& a, const Geom& b) {
+  if (a.dim != b.dim) return false;
+  for (int r = 0; r < a.dim; ++r)
+    for (int c = 0; c < a.dim; ++c)
+      if (a.dir[r * 3 + c] != b.dir[r * 3 + c]) return false;
+  return true;
+}
+
+inline void index_map(const Geom& src, const Geom& dst, double t[3], double B[9]) {
+  const double dorg[3] = {src.org[0] - dst.org[0], src.org[1] - dst.org[1],
+                          src.dim == 3 ? src.org[2] - dst.org[2] : 0.0};
+  if (same_direction(src, dst)) {
+    double D[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, Di[9];
+    for (int r = 0; r < src.dim; ++r)
+      for (int c = 0; c < src.dim; ++c) D[r * 3 + c] = src.dir[r * 3 + c];
+    const double* a = D;
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    const double id = 1.0 / det;
+    Di[0] = (a[4] * a[8] - a[5] * a[7]) * id;
+    Di[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    Di[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    Di[3] = (a[5] * a[6] - a[3] * a[8]) * id;
+    Di[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    Di[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    Di[6] = (a[3] * a[7] - a[4] * a[6]) * id;
+    Di[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    Di[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    for (int r = 0; r < 3; ++r) {
+      const bool on = r < src.dim;
+      for (int c = 0; c < 3; ++c) B[r * 3 + c] = (r == c && on) ? src.sp[r] / dst.sp[r] : 0.0;
+      t[r] = on ? (Di[r * 3 + 0] * dorg[0] + Di[r * 3 + 1] * dorg[1] + Di[r * 3 + 2] * dorg[2]) / dst.sp[r] : 0.0;
+    }
+    return;
+  }
+  for (int r = 0; r < 3; ++r) {
+    double tt = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      tt += dst.p2i[r * 3 + c] * dorg[c];
+      double b = 0.0;
+      for (int k = 0; k < 3; ++k) b += dst.p2i[r * 3 + k] * src.i2p[k * 3 + c];
+      B[r * 3 + c] = b;
+    }
+    t[r] = tt;
+  }
+  if (src.dim == 2) {
+    t[2] = 0.0;
+    B[2] = B[5] = B[6] = B[7] = B[8] = 0.0;
+  }
+}
+
+inline void apply_index_map(const double t[3], const double B[9], const double idx[3], double c[3]) {
+  for (int r = 0; r < 3; ++r) {
+    double v = t[r] + B[r * 3 + 0] * idx[0];
+    v = v + B[r * 3 + 1] * idx[1];
+    c[r] = v + B[r * 3 + 2] * idx[2];
+  }
+}
+
 // Resample a vector field onto another grid (DisplacementFieldTransformParametersAdaptor at
 // each level, Examples/itkantsRegistrationHelper.hxx:2028-2055): linear, 0 outside.
 template <class T>
 inline void resample_field(const T* in, const Geom& gi, T* out, const Geom& go) {
   const int64_t No = go.count(), Ni = gi.count(), nx = go.n[0], ny = go.n[1];
   const int D = go.dim;
+  double mt[3], mB[9];
+  index_map(go, gi, mt, mB);
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < No; ++i) {
     double idx[3] = {(double)(i % nx), (double)((i / nx) % ny), (double)(i / (nx * ny))};
-    double p[3], c[3];
-    go.index_to_point(idx, p);
-    gi.point_to_cindex(p, c);
+    double c[3];
+    apply_index_map(mt, mB, idx, c);
+    if (D == 2) c[2] = 0.0;
     if (!inside_buffer(gi, c)) {
       for (int k = 0; k < D; ++k) out[k * No + i] = (T)0;
       continue;

@@ -3,9 +3,7 @@
 Every other parity test places its grids axis-aligned, so the gathers run their diagonal index-map
 path; here the grids are rotated (and anisotropic), so the warp, composition, resampling, inversion,
 CC derivative conversion (index-axis derivatives rotated into physical axes) and a whole stage run
-the general path against the oracle.  Tolerances are those of the axis-aligned tests.  This file is
-collected after the allocation-free entry point's, so that a run which stops at the first failure has
-already run the tests before it.
+the general path against the oracle.  Tolerances are those of the axis-aligned tests.
 """
 import numpy as np
 import pytest

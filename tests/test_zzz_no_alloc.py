@@ -1,11 +1,13 @@
 """The allocation-free CC entry point (synx_cc_metric_noalloc).
 
-It exists for callers that cannot allocate device memory -- a pipeline being captured into a CUDA
-graph, a host whose GPU memory belongs to another allocator, a loop that must not stall on an
-allocation -- and keeps the kernel's scratch in a fixed array inside libsynx instead.  The GPU test
-calls it twice in a row through the C ABI and checks each result against synx_cc_metric on the same
-inputs, with the tolerances of the CC parity tests; this file is collected last so that a run which
-stops at the first failure has already run every other test.
+It serves callers that must not allocate device memory themselves: a plug-in whose host
+application (a viewer, a deep-learning framework with its own caching allocator, a serving process)
+owns the GPU's memory and its budget, or a latency-bound loop that cannot afford the device-wide
+synchronisation a cudaMalloc/cudaFree pair can cause.  It keeps the CC kernel's scratch in a fixed
+array inside libsynx instead.  The GPU test calls it twice in a row through the C ABI and checks each
+result against synx_cc_metric on the same inputs, with the tolerances of the CC parity tests.  The
+file name sorts after every other test file, so pytest collects it last and a run which stops at the
+first failure has already run every other test.
 """
 import ctypes as C
 
