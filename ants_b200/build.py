@@ -25,6 +25,8 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 
 LIB = os.path.join(HERE, "libsynx.so")
 CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
+# the C++ library entry `ants::antsRegistration(std::vector<std::string>, std::ostream*)`
+REG_LIB = os.path.join(HERE, "libantsRegistration_b200.so")
 APPLY_CLI = os.path.join(HERE, "antsApplyTransforms_b200")
 
 LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu", "synx_server.cpp",
@@ -105,9 +107,24 @@ def _build_exe(target: str, sources: list[str], force: bool) -> str | None:
     return target
 
 
+def build_reg_lib(force: bool = False) -> str | None:
+    """libantsRegistration_b200.so: the command line without its main(), exporting the reference's
+    library symbol ants::antsRegistration for wrappers."""
+    srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in CLI_HEADERS] + [LIB]
+    if not force and not _stale(REG_LIB, deps):
+        return REG_LIB
+    cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", "-fPIC", "-shared", "-DSYNX_CLI_NO_MAIN", "-I", INCLUDE,
+           "-I", "/usr/local/cuda/include", "-o", REG_LIB, *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN",
+           "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,/usr/local/cuda/lib64", "-lz"]
+    _run(cmd)
+    return REG_LIB
+
+
 def build_cli(force: bool = False) -> str | None:
-    """antsRegistrationSyN_b200 and antsApplyTransforms_b200."""
+    """antsRegistrationSyN_b200, antsApplyTransforms_b200 and libantsRegistration_b200.so."""
     _build_exe(APPLY_CLI, APPLY_SOURCES, force)
+    build_reg_lib(force)
     return _build_exe(CLI, CLI_SOURCES, force)
 
 

@@ -100,6 +100,15 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
 
   const int dim = std::atoi(one("dimensionality", "3").c_str());
   if (dim != 2 && dim != 3) throw std::runtime_error("--dimensionality must be 2 or 3");
+  // The reference computes in double unless --float 1 (antsRegistration.cxx:488-491, :707-722).
+  // This stage computes in float32 (FP64 only in the CC window sums and the global reductions),
+  // so a double request is honoured for the written files only, and said so on stderr.
+  const bool use_float = flag("float", false);
+  if (!use_float)
+    std::cerr << "antsRegistrationSyN_b200: WARNING: double precision requested (--float 0, the reference's "
+                 "default); this stage computes in float32 and writes its results widened to float64. Pass "
+                 "--float 1 to request float32 explicitly."
+              << std::endl;
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
 
   // initial moving transforms: linear files (or identity), in the order they act on a point (the
@@ -299,7 +308,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   }
   // output files in the precision the reference writes them: float with --float 1, double by default
   // (antsRegistration.cxx:488-491); the values are computed in float either way
-  const int out_type = flag("float", false) ? 16 : 64;
+  const int out_type = use_float ? 16 : 64;
   auto typed = [out_type](nifti::Image im) {
     im.out_datatype = out_type;
     return im;
@@ -333,7 +342,17 @@ int antsRegistration(std::vector<std::string> args, std::ostream* out) {
 
 }  // namespace ants_b200
 
+namespace ants {
+
+int antsRegistration(std::vector<std::string> args, std::ostream* out_stream) {
+  return ants_b200::antsRegistration(std::move(args), out_stream);
+}
+
+}  // namespace ants
+
+#ifndef SYNX_CLI_NO_MAIN
 int main(int argc, char** argv) {
   std::vector<std::string> args(argv + 1, argv + argc);
-  return ants_b200::antsRegistration(args, &std::cout);
+  return ants::antsRegistration(args, &std::cout);
 }
+#endif

@@ -15,3 +15,9 @@ namespace ants_b200 {
 int antsRegistration(std::vector<std::string> args, std::ostream* out);
 
 }  // namespace ants_b200
+
+// The reference's own library symbol, `ants::antsRegistration` (Examples/include/antsRegistration.h:7-9,
+// body Examples/antsRegistration.cxx:554-777), declared in include/antsRegistration.h, so that a
+// wrapper compiled against the reference's header links against libantsRegistration_b200.so
+// unchanged.  Forwards to ants_b200::antsRegistration.
+#include "antsRegistration.h"
