@@ -30,7 +30,7 @@ REG_LIB = os.path.join(HERE, "libantsRegistration_b200.so")
 APPLY_CLI = os.path.join(HERE, "antsApplyTransforms_b200")
 
 LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu", "synx_server.cpp",
-               "synx_linear.cpp"]
+               "synx_linear.cpp", "synx_tune.cpp"]
 LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh", "synx_phases.cuh", "synx_cc_tile.cuh", "synx_level.cuh",
                "synx_level_body.cuh", "synx_host.h", "synx_nvtx.h"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
@@ -89,7 +89,8 @@ def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
             list(ex.map(_run, jobs))
     objs = [o for _, o, _ in _objects()]
     if force or jobs or _stale(LIB, objs):
-        _run([_nvcc(), *ARCH, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *objs, "-lcudart", "-Xcompiler", "-pthread"])
+        _run([_nvcc(), *ARCH, "-ccbin", _host_cxx(), "-shared", "-o", LIB, *objs, "-lcudart", "-ldl", "-Xcompiler",
+              "-pthread"])
     return LIB
 
 

@@ -55,12 +55,22 @@ static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, flo
 // z-chunk of one CC block.  Each block first fills its z window (2R slices, column updates only,
 // about a third of a full slice's work each), then marches its chunk; 2 blocks are resident per
 // SM.  The chunk count minimises waves x (chunk + warm-up cost), so the last wave is not mostly
-// empty (e.g. 182 slices over 6 x 28 tiles: 7 chunks, 1176 blocks = 3.97 waves of 296).
-static int cc_zchunk(const GridInfo& g, int radius) {
+// empty (e.g. 182 slices over 6 x 28 tiles: 7 chunks, 1176 blocks = 3.97 waves of 296).  A tile
+// plan may fix the number of chunks instead (at most nz / R, chunks of at least R slices).
+static int cc_max_chunks(const GridInfo& g, int radius) {
+  return g.d.dim == 2 ? 1 : std::max(1, g.d.nz / std::max(radius, 1));
+}
+
+static int cc_zchunk(const GridInfo& g, int radius, int chunks = 0) {
   if (g.d.dim == 2) return 1;
+  const int nz = g.d.nz;
+  const int max_chunks = cc_max_chunks(g, radius);
+  if (chunks > 0) {
+    chunks = std::min(chunks, max_chunks);
+    return (nz + chunks - 1) / chunks;
+  }
   const int bxy = ((g.d.nx + 31) / 32) * ((g.d.ny + 7) / 8);
-  const int nz = g.d.nz, slots = 2 * 148;
-  const int max_chunks = std::max(1, nz / std::max(radius, 1));  // chunks of at least R slices
+  const int slots = 2 * 148;
   int best_zc = nz;
   double best = 1e30;
   for (int c = 1; c <= max_chunks; ++c) {
@@ -76,10 +86,14 @@ static int cc_zchunk(const GridInfo& g, int radius) {
   return best_zc;
 }
 
-int cc_blocks(const GridInfo& g, int radius) {
+int cc_blocks(const GridInfo& g, int radius, int chunks) {
   const int bx = (g.d.nx + 31) / 32, by = (g.d.ny + 7) / 8;
-  const int zc = cc_zchunk(g, radius);
+  const int zc = cc_zchunk(g, radius, chunks);
   return bx * by * ((g.d.nz + zc - 1) / zc);
+}
+
+int cc_blocks_max(const GridInfo& g, int radius) {
+  return cc_blocks(g, radius, cc_max_chunks(g, radius));
 }
 
 size_t cc_smem_bytes(int dim, int radius) {
@@ -120,7 +134,7 @@ bool cc_radius_supported(int dim, int radius) {
   return radius >= 1 && radius <= 7 && cc_smem_bytes(dim, radius) <= 227 * 1024;
 }
 
-CCParams make_cc_params(const GridInfo& g, int radius) {
+CCParams make_cc_params(const GridInfo& g, int radius, int chunks) {
   CCParams P;
   for (int k = 0; k < 3; ++k) P.h[k] = (float)g.sp[k];
   bool ident = true;
@@ -130,14 +144,14 @@ CCParams make_cc_params(const GridInfo& g, int radius) {
   }
   P.identity_dir = ident ? 1 : 0;
   P.eps = 1.1920928955078125e-07;  // FLT_EPSILON: the reference metric's float guard
-  P.ZC = cc_zchunk(g, radius);
+  P.ZC = cc_zchunk(g, radius, chunks);
   return P;
 }
 
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out, bool fp32_sums) {
+               IterCtl* ctl, cudaStream_t s, float* cc_out, bool fp32_sums, int chunks) {
   add_launch_count(1);
-  const CCParams P = make_cc_params(g, radius);
+  const CCParams P = make_cc_params(g, radius, chunks);
   dim3 grid((g.d.nx + 31) / 32, (g.d.ny + 7) / 8, (g.d.nz + P.ZC - 1) / P.ZC);
 #define SYNX_CC_CASE(RR)                                                                         \
   case RR:                                                                                       \

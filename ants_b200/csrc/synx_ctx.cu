@@ -206,6 +206,8 @@ struct synx_ctx {
   IterCtl h_ctl{};
   std::vector<double> h_lm, h_lc;
   std::vector<int> h_li;
+  // tile plan per level (stage parameters, then the tuning table, then the cost models)
+  LevelPlan plan[SYNX_MAX_LEVELS] = {};
   // canonical buffer assignment (level changes swap field and work buffers)
   float* canon[8] = {};
   // graphs: one executable per level, valid while the arena and grids are unchanged
@@ -286,7 +288,7 @@ ArenaPlan arena_plan(const synx_ctx* c) {
   const long long Nmax = c->Nmax, NI = std::max(c->NF, c->NM);
   int ccb = 0, invb = 0;
   for (auto& g : c->lv) {
-    ccb = std::max(ccb, cc_blocks(g, c->P.cc_radius));
+    ccb = std::max(ccb, cc_blocks_max(g, c->P.cc_radius));  // any chunk count a tile plan picks
     invb = std::max(invb, inv_blocks(g));
   }
   invb = std::max(invb, 2048);
@@ -592,7 +594,9 @@ void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const
   const float* k[3] = {coeff_base, coeff_base + c->coeff_cap, coeff_base + 2 * c->coeff_cap};
   if (smooth3_supported(c->D, R)) {
     const float* kh[3] = {host_base, host_base + c->coeff_cap, host_base + 2 * c->coeff_cap};
-    launch_smooth_field(in, out, orig, tmp, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream);
+    const int rows = c->cur_level >= 0 ? c->plan[c->cur_level].smooth_rows : 8;
+    const SmoothPlan sp{rows > 0 ? rows : 0, 0};
+    launch_smooth_field(in, out, orig, tmp, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream, &sp);
     return;
   }
   const int D = c->D;
@@ -628,7 +632,7 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
   launch_warp_pair(c->Fs, c->gF, c->psiF, c->Ms, c->gM, c->psiM, g, c->Ft, c->Mt, c->ctl, s);
   int e0 = profile ? ev() : -1;
   launch_cc(c->Ft, c->Mt, g, c->P.cc_radius, c->gFu, c->gMu, c->cc_partials, c->ctl, s, nullptr,
-            (c->P.flags & SYNX_F_CC_FP32_SUMS) != 0);
+            (c->P.flags & SYNX_F_CC_FP32_SUMS) != 0, c->plan[c->cur_level].cc_chunks);
   if (profile) c->ev_pairs_cc.push_back({e0, ev()});
   // update-field smoothing, SyN epilogue (boundary zero, blend) and max ||u/spacing||
   const float* upd[2] = {c->t1F, c->t1M};
@@ -745,10 +749,10 @@ long long level_inv_units(const GridInfo& g) {
 
 // Whether a level runs in the level kernel (alone or in a batch): the options it implements, and
 // a level small enough that launch latency, not bandwidth, dominates the per-kernel path.
-bool persistent_eligible(synx_ctx* c, const GridInfo& g, bool profile) {
+// Whether the level kernel implements the stage's options on grid g (whatever its size).
+bool persistent_capable(synx_ctx* c, const GridInfo& g, bool profile) {
   if (profile || (c->P.flags & (SYNX_F_NO_PERSISTENT | SYNX_F_CC_FP32_SUMS | SYNX_F_FIELDS_FP16))) return false;
-  const long long max_vox = c->P.persistent_max_voxels > 0 ? c->P.persistent_max_voxels : kPersistentMaxVoxels;
-  if (g.d.N > max_vox || c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
+  if (c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
   int rs = 1;
   for (int a = 0; a < c->D; ++a) rs = std::max(rs, c->R_upd[a]);
   if (rs > kLevelMaxSmoothRadius) return false;
@@ -756,8 +760,43 @@ bool persistent_eligible(synx_ctx* c, const GridInfo& g, bool profile) {
   return level_inv_units(g) <= c->inv_cap;
 }
 
-bool use_persistent(synx_ctx* c, const GridInfo& g, bool profile, int* blocks) {
-  if (!persistent_eligible(c, g, profile)) return false;
+bool persistent_eligible(synx_ctx* c, const GridInfo& g, bool profile) {
+  const long long max_vox = c->P.persistent_max_voxels > 0 ? c->P.persistent_max_voxels : kPersistentMaxVoxels;
+  return g.d.N <= max_vox && persistent_capable(c, g, profile);
+}
+
+// Radius of the update-field smoothing kernel on a level grid (the widest axis).
+int level_smooth_radius(const synx_ctx* c, const GridInfo& g) {
+  int rs = 1;
+  for (int a = 0; a < c->D; ++a) {
+    const int n = a == 0 ? g.d.nx : (a == 1 ? g.d.ny : g.d.nz);
+    rs = std::max(rs, (int)gauss_kernel(c->P.update_variance, 0.001, (size_t)n).size() / 2);
+  }
+  return rs;
+}
+
+// The tile plan of a level: the tuning table's entry for its grid (unless the stage opts out),
+// overridden by explicit stage parameters; without either, the cost models (slab smoothing with
+// 8-row tiles, the CC chunk model, the persistent kernel up to the size threshold).
+LevelPlan resolve_plan(synx_ctx* c, int level) {
+  const GridInfo& g = c->lv[level];
+  LevelPlan p{-1, 8, 0};
+  LevelPlan t{};
+  if (c->P.tuning == 0 &&
+      tuning_lookup(c->D, c->P.cc_radius, level_smooth_radius(c, g), g.d.nx, g.d.ny, g.d.nz, &t))
+    p = t;
+  if (c->P.smooth_tile_rows != 0) p.smooth_rows = c->P.smooth_tile_rows;
+  if (c->P.flags & SYNX_F_SMOOTH_TWO_PASS) p.smooth_rows = -1;
+  if (c->P.cc_z_chunks > 0) p.cc_chunks = c->P.cc_z_chunks;
+  if (c->P.persistent_max_voxels > 0) p.persistent = -1;  // an explicit size threshold decides
+  return p;
+}
+
+bool use_persistent(synx_ctx* c, int level, const GridInfo& g, bool profile, int* blocks) {
+  const int choice = c->plan[level].persistent;
+  const bool ok = choice == 1 ? persistent_capable(c, g, profile)
+                              : (choice == 0 ? false : persistent_eligible(c, g, profile));
+  if (!ok) return false;
   if (c->coop_max <= 0) c->coop_max = level_max_blocks(c->D, c->P.cc_radius, kLevelMaxSmoothRadius, c->device);
   if (c->coop_max <= 0) return false;
   // every co-resident block: the phases are latency-bound at these sizes, so more warps in
@@ -854,6 +893,7 @@ int level_begin(synx_ctx* c, int level) {
   if (rc) return rc;
   rc = upload_level_kernels(c, level);
   if (rc) return rc;
+  c->plan[level] = resolve_plan(c, level);
   if (level == 0) {
     for (float* f : {c->phiF, c->psiF, c->phiM, c->psiM})
       CUDA_TRY(c, cudaMemsetAsync(f, 0, 4 * (size_t)D * gl.d.N, c->stream));
@@ -891,7 +931,7 @@ int level_iterate(synx_ctx* c, int level) {
   const bool profile = (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0;
   const bool graphs = (c->P.flags & SYNX_F_USE_GRAPHS) != 0 && !profile;
   int coop_blocks = 0;
-  const bool persistent = iters > 0 && use_persistent(c, gl, profile, &coop_blocks);
+  const bool persistent = iters > 0 && use_persistent(c, level, gl, profile, &coop_blocks);
   if (persistent) {
     // every iteration of this level in one cooperative launch
     LevelArgs A = make_level_args(c, gl, iters);
@@ -1294,6 +1334,11 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     return set_err(nullptr, SYNX_E_ARG, "synx_create: unknown test_inject value");
   if (p.histogram_match != 0 && p.histogram_match != 1)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: histogram_match must be 0 or 1");
+  if (p.tuning != 0 && p.tuning != 1) return set_err(nullptr, SYNX_E_ARG, "synx_create: tuning must be 0 or 1");
+  if (p.smooth_tile_rows != 0 && p.smooth_tile_rows != 8 && p.smooth_tile_rows != 16 && p.smooth_tile_rows != -1)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: smooth_tile_rows must be 0, 8, 16 or -1");
+  if (p.cc_z_chunks < 0 || p.cc_z_chunks > 4096)
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: cc_z_chunks must be in 0..4096");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -1317,6 +1362,7 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
     }
     c->own_stream = true;
   }
+  if (p.tuning == 0) tuning_ensure_loaded();
   cudaError_t e = cc_prepare(p.dim, p.cc_radius);
   if (e == cudaSuccess) e = smooth3_prepare();
   for (auto& ev : c->lev_ev)
@@ -1632,6 +1678,32 @@ int synx_get_level_profile(synx_ctx* c, int level, double* setup_ms, double* ite
   if (iterations) *iterations = l.iterations;
   if (inverse_subiterations) *inverse_subiterations = l.inv_sub;
   if (voxels) *voxels = l.voxels;
+  return SYNX_OK;
+}
+
+int synx_level_plan(synx_ctx* c, int level, int32_t* persistent, int32_t* smooth_rows, int32_t* cc_z_chunks) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if (!c->images_set) return set_err(c, SYNX_E_STATE, "synx_level_plan: images not set");
+  if (level < 0 || level >= c->P.n_levels) return set_err(c, SYNX_E_ARG, "synx_level_plan: bad level");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  // the smoothing radii of that level decide eligibility: computed as level_begin would
+  const int saved[3] = {c->R_upd[0], c->R_upd[1], c->R_upd[2]};
+  const GridInfo& g = c->lv[level];
+  for (int a = 0; a < c->D; ++a) {
+    const int n = a == 0 ? g.d.nx : (a == 1 ? g.d.ny : g.d.nz);
+    c->R_upd[a] = (int)gauss_kernel(c->P.update_variance, 0.001, (size_t)n).size() / 2;
+  }
+  const LevelPlan p = resolve_plan(c, level);
+  const LevelPlan keep = c->plan[level];
+  c->plan[level] = p;
+  int blocks = 0;
+  const bool pers = c->P.iterations[level] > 0 &&
+                    use_persistent(c, level, g, (c->P.flags & SYNX_F_PROFILE_EVENTS) != 0, &blocks);
+  c->plan[level] = keep;
+  for (int a = 0; a < 3; ++a) c->R_upd[a] = saved[a];
+  if (persistent) *persistent = pers ? 1 : 0;
+  if (smooth_rows) *smooth_rows = p.smooth_rows;
+  if (cc_z_chunks) *cc_z_chunks = p.cc_chunks;
   return SYNX_OK;
 }
 

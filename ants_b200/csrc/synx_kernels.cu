@@ -450,6 +450,81 @@ __global__ void __launch_bounds__(256, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth
   }
 }
 
+// Fused 3-D smoothing: xy and z in one pass over a slab.  A block owns a 32 x TY tile of columns of
+// one half-field and a chunk of ZC output slices.  It convolves slices z0 - R .. z1 - 1 + R in xy
+// (the xy kernel's shared-memory halo tile, replicate edges) and keeps the last 2R + 1 xy-smoothed
+// slices in a shared-memory ring whose slots are thread-private (each thread's ring entries are its
+// own outputs, so the ring needs no barrier); every output slice is then convolved along z from the
+// ring, with the SyN epilogue and the max norm.  The xy intermediate never reaches global memory
+// (48 B per voxel of traffic less than the two-kernel path), at the price of recomputing the 2R halo
+// slices of each chunk.  The arithmetic and its order are those of the two-kernel path: the same bits.
+template <int R, int TY>
+__global__ void __launch_bounds__(256) k_smooth_slab(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  if (ctl != nullptr && ctl->stop) return;
+  constexpr int K = 2 * R + 1, RPT = TY / 8;
+  extern __shared__ __align__(16) float sms[];
+  float* ring = sms + smooth3_smem_floats(3, R, TY);  // [K][3][RPT][256]
+  __shared__ float red[32];
+  const int nzc = gridDim.z / a.halves;
+  const int h = blockIdx.z / nzc;
+  const int zc = blockIdx.z - h * nzc;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
+  const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int ox = blockIdx.x * 32 + tx, oy0 = blockIdx.y * TY + ty * RPT;
+  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+  const bool xedge = ox == 0 || ox == nx - 1;
+  float mx = 0.0f;
+  int sq = 0;  // ring slot of slice zs: (zs - z0 + R) mod K
+  for (int zs = z0 - R; zs < z1 + R; ++zs) {
+    float y[3][RPT];
+    smooth_xy_compute<3, R, TY>(a, d, blockIdx.x, blockIdx.y, min(max(zs, 0), nz - 1), h, sms, y);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) ring[((sq * 3 + c) * RPT + r) * 256 + tid] = y[c][r];
+    sq = sq == K - 1 ? 0 : sq + 1;  // now the slot of slice zs + 1, i.e. of slice z - R below
+    const int z = zs - R;  // output slice whose window z - R .. z + R is complete
+    if (z >= z0 && ox < nx) {
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        const int oy = oy0 + r;
+        if (oy >= ny) break;
+        const int i = z * nxy + oy * nx + ox;
+        const bool edge = a.epilogue && (xedge || oy == 0 || oy == ny - 1 || z == 0 || z == nz - 1);
+        float nrm2 = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float acc = 0.0f;
+          int s2 = sq;
+#pragma unroll
+          for (int j = 0; j < K; ++j) {
+            acc = fmaf(a.k[2][j], ring[((s2 * 3 + c) * RPT + r) * 256 + tid], acc);
+            s2 = s2 == K - 1 ? 0 : s2 + 1;
+          }
+          if (a.epilogue) {
+            if (edge) acc = 0.0f;
+            else if (a.w2 != 0.0f) acc = acc * a.w1 + org[c * N + i] * a.w2;
+          }
+          const float qv = acc * a.ih[c];
+          nrm2 += qv * qv;
+          dst[c * N + i] = acc;
+        }
+        mx = fmaxf(mx, sqrtf(nrm2));
+      }
+    }
+  }
+  if (a.do_max) {
+    const float bm = block_max_f(mx, red);
+    if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
+  }
+}
+
+size_t smooth_slab_smem_bytes(int R, int TY) {
+  return (smooth3_smem_floats(3, R, TY) + (size_t)(2 * R + 1) * 3 * (TY / 8) * 256) * sizeof(float);
+}
+
 static int smooth3_radius(int dim, const int R[3]) {
   int r = 0;
   for (int a = 0; a < dim; ++a) r = std::max(r, R[a]);
@@ -469,6 +544,12 @@ static cudaError_t smooth3_attr_both() {
                              (int)(smooth3_smem_floats(2, R, kSmoothTileY) * 4));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_smooth_z<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_z_smem_bytes(R));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_smooth_slab<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smooth_slab_smem_bytes(R, 8));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_smooth_slab<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smooth_slab_smem_bytes(R, 16));
   return e;
 }
 
@@ -534,10 +615,75 @@ int smooth_z_chunk(const Dims& d, int halves, int RR, int slots) {
   return best_zc;
 }
 
+// Slab plan of the fused 3-D smoothing: tile rows (8 or 16) and output slices per block; 0 = the
+// two-kernel path.  The chunk is chosen by waves of resident blocks times the slices a block
+// convolves in xy (its chunk plus the 2R halo slices), unless a plan fixes it.
+static int slab_chunk(const Dims& d, int halves, int R, int TY) {
+  const size_t smem = smooth_slab_smem_bytes(R, TY);
+  int per_sm = (int)std::min<size_t>(8, (227 * 1024) / (smem + 1024));
+  if (per_sm < 1) per_sm = 1;
+  const int slots = 148 * per_sm;
+  const int cols = ((d.nx + 31) / 32) * ((d.ny + TY - 1) / TY) * halves;
+  int best_zc = d.nz;
+  double best = -1.0;
+  for (int zc = 1; zc <= d.nz; ++zc) {
+    const long long blocks = (long long)cols * ((d.nz + zc - 1) / zc);
+    const double cost = (double)((blocks + slots - 1) / slots) * (zc + 2 * R);
+    if (best < 0 || cost < best) {
+      best = cost;
+      best_zc = zc;
+    }
+  }
+  return best_zc;
+}
+
+static void launch_smooth_slab(const Smooth3Args& a0, const GridInfo& g, int RR, int TY, int ZC, IterCtl* ctl,
+                               cudaStream_t s) {
+  Smooth3Args a = a0;
+  a.ZC = ZC > 0 ? std::min(ZC, g.d.nz) : slab_chunk(g.d, a.halves, RR, TY);
+  const dim3 grid((g.d.nx + 31) / 32, (g.d.ny + TY - 1) / TY, ((g.d.nz + a.ZC - 1) / a.ZC) * a.halves);
+  const size_t smem = smooth_slab_smem_bytes(RR, TY);
+  count_launch();
+#define SYNX_SSLAB(RV)                                                              \
+  case RV:                                                                          \
+    if (TY == 16)                                                                   \
+      k_smooth_slab<RV, 16><<<grid, 256, smooth_slab_smem_bytes(RV, 16), s>>>(a, g.d, ctl); \
+    else                                                                            \
+      k_smooth_slab<RV, 8><<<grid, 256, smooth_slab_smem_bytes(RV, 8), s>>>(a, g.d, ctl);   \
+    break;
+  (void)smem;
+  switch (RR) {
+    SYNX_SSLAB(1)
+    SYNX_SSLAB(2)
+    SYNX_SSLAB(3)
+    SYNX_SSLAB(4)
+    SYNX_SSLAB(5)
+    SYNX_SSLAB(6)
+    SYNX_SSLAB(7)
+    SYNX_SSLAB(8)
+    SYNX_SSLAB(9)
+    SYNX_SSLAB(10)
+    SYNX_SSLAB(11)
+    SYNX_SSLAB(12)
+    default:
+      break;
+  }
+#undef SYNX_SSLAB
+}
+
+SmoothPlan g_smooth_plan{8, 0};
+
 void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
                          int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
-                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s) {
+                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s, const SmoothPlan* plan) {
   const int dim = g.d.dim;
+  const SmoothPlan P = plan ? *plan : g_smooth_plan;
+  if (dim == 3 && P.slab_ty > 0) {
+    int RR = 1;
+    Smooth3Args a = make_smooth_args(in, out, orig, halves, g, khost, R, epilogue, w1, w2, maxnorm, &RR);
+    launch_smooth_slab(a, g, RR, P.slab_ty, P.slab_zc, ctl, s);
+    return;
+  }
   int RR = 1;
   Smooth3Args a = make_smooth_args(in, dim == 3 ? tmp : out, orig, halves, g, khost, R, epilogue, w1, w2, maxnorm, &RR);
   // xy tiles are 32 x kSmoothTileY; the z pass below keeps 32 x 8 columns

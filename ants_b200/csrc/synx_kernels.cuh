@@ -80,15 +80,18 @@ void launch_warp_image_label(const float* img, const GridInfo& gi, const float* 
 void launch_field_affine_update(const float* u, const float* w, const double M[9], int dim, long long N, float* out,
                                 cudaStream_t s);
 
-// Returns the number of blocks the CC launch uses (partials needed).
-int cc_blocks(const GridInfo& g, int radius);
+// Returns the number of blocks the CC launch uses (partials needed); chunks > 0 fixes the number
+// of z chunks (at most nz / radius), 0 takes the cost model's.
+int cc_blocks(const GridInfo& g, int radius, int chunks = 0);
+// The most blocks any chunk count can give on g.
+int cc_blocks_max(const GridInfo& g, int radius);
 size_t cc_smem_bytes(int dim, int radius);
 bool cc_radius_supported(int dim, int radius);
 // Raise the dynamic shared-memory limit of the CC kernel (once per device, outside capture).
 cudaError_t cc_prepare(int dim, int radius);
 // fp32_sums: window sums and variance terms in float (the precision study's variant).
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr, bool fp32_sums = false);
+               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr, bool fp32_sums = false, int chunks = 0);
 // Round nf fields of n floats each to the nearest half-precision value, in place (the
 // precision study's FP16 field storage).
 void launch_round_half(float* const* f, int nf, long long n, cudaStream_t s);
@@ -99,10 +102,20 @@ void launch_round_half(float* const* f, int nf, long long n, cudaStream_t s);
 // (w2 != 0); `maxnorm` reduces max ||u/spacing|| into ctl->maxnorm[h].  Radii up to 12.
 bool smooth3_supported(int dim, const int R[3]);
 cudaError_t smooth3_prepare();
-// In 3-D the xy pass writes `tmp` (same shape as `out`), which the z pass reads.
+// How a 3-D field is smoothed: slab_ty > 0 runs the fused slab kernel with 32 x slab_ty column
+// tiles (8 or 16) and slab_zc output slices per block (0: chosen by a waves x work model);
+// slab_ty = 0 runs the xy kernel and then the z kernel through `tmp`.
+struct SmoothPlan {
+  int slab_ty;
+  int slab_zc;
+};
+extern SmoothPlan g_smooth_plan;  // the default plan
+// In 3-D on the two-kernel path the xy pass writes `tmp` (same shape as `out`), which the z pass
+// reads.  plan = null uses g_smooth_plan.
 void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
                          int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
-                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s);
+                         float w1, float w2, bool maxnorm, IterCtl* ctl, cudaStream_t s,
+                         const SmoothPlan* plan = nullptr);
 
 // Separable smoothing of `halves` fields (each dim components) along one axis.
 // `last` applies the SyN epilogue: zero boundary, blend with `orig` (w2 != 0), and the max

@@ -61,7 +61,7 @@ int level_zb(const Dims& d, int halves);
 
 // Helpers shared with the standalone launchers (synx_kernels.cu, synx_cc.cu).
 bool affine_diag_host(const Affine& m);
-CCParams make_cc_params(const GridInfo& g, int radius);
+CCParams make_cc_params(const GridInfo& g, int radius, int chunks = 0);
 Smooth3Args make_smooth_args(const float* const* in, float* const* out, const float* const* orig, int halves,
                              const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue, float w1,
                              float w2, bool maxnorm, int* radius);

@@ -293,16 +293,16 @@ __host__ __device__ inline size_t smooth3_smem_floats(int dim, int R, int TY = 8
   return (size_t)dim * HY * HXP + (size_t)dim * HY * 32;
 }
 
-// xy part for one (32 x TY tile, slice z, field h): halo tile of every component staged in shared
-// memory with replicate-edge indices, convolved along x (each work item makes four consecutive
-// outputs from float4 loads) and then along y (each thread makes TY/8 consecutive rows of one
-// column from registers).  Taller tiles convolve fewer halo rows along x per output (TY + 2R
-// rows for TY outputs).  In 3-D the xy-smoothed values go to `out` for the z part; in 2-D this
-// is the whole filter and the SyN epilogue runs here (max norm returned).  All threads of the
-// block must call it; `sm` holds smooth3_smem_floats(DIM, R, TY) floats.
-template <int DIM, int R, int TY = 8>
-__device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
-                                                float* sm) {
+// xy smoothing of one (32 x TY tile, slice z, field h): halo tile of every component staged in
+// shared memory with replicate-edge indices, convolved along x (each work item makes four
+// consecutive outputs from float4 loads) and then along y (each thread makes TY/8 consecutive rows
+// of one column from registers).  Taller tiles convolve fewer halo rows along x per output (TY + 2R
+// rows for TY outputs).
+// The xy convolution of one (32 x TY tile, slice z, field h): thread (tx, ty) gets the outputs at
+// x = bx*32 + tx, y = by*TY + ty*(TY/8) + r in y[c][r].  All threads of the block must call it.
+template <int DIM, int R, int TY>
+__device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
+                                                  float* sm, float (&y)[DIM][TY / 8]) {
   static_assert(TY % 8 == 0, "8 warps share the tile rows");
   constexpr int K = 2 * R + 1, RPT = TY / 8;
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
@@ -311,7 +311,6 @@ __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims
   float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
   const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
   const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
-  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const int x0 = bx * 32, y0 = by * TY;
   const float* plane = src + z * nxy;
@@ -347,8 +346,7 @@ __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims
     reinterpret_cast<float4*>(xsum + row * 32)[q] = make_float4(o[0], o[1], o[2], o[3]);
   }
   __syncthreads();
-  const int ox = x0 + tx, ty0 = ty * RPT;
-  float y[DIM][RPT];
+  const int ty0 = ty * RPT;
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
     const float* col = xsum + (c * HY + ty0) * 32 + tx;
@@ -364,6 +362,23 @@ __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims
     }
   }
   __syncthreads();  // the tile and xsum may be reused by the caller's next tile
+}
+
+// xy part for one (32 x TY tile, slice z, field h), written out: in 3-D the xy-smoothed values go
+// to `out` for the z part; in 2-D this is the whole filter and the SyN epilogue runs here (max norm
+// returned).  All threads of the block must call it; `sm` holds smooth3_smem_floats(DIM, R, TY)
+// floats.
+template <int DIM, int R, int TY = 8>
+__device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
+                                                float* sm) {
+  constexpr int RPT = TY / 8;
+  float y[DIM][RPT];
+  smooth_xy_compute<DIM, R, TY>(a, d, bx, by, z, h, sm, y);
+  const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
+  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int x0 = bx * 32, y0 = by * TY;
+  const int ox = x0 + tx, ty0 = ty * RPT;
   float mx = 0.0f;
   if (ox >= nx) return mx;
   const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];

@@ -25,6 +25,7 @@ SYNX_F_USE_GRAPHS = 0x2
 SYNX_F_NO_PERSISTENT = 0x4
 SYNX_F_CC_FP32_SUMS = 0x8
 SYNX_F_FIELDS_FP16 = 0x10
+SYNX_F_SMOOTH_TWO_PASS = 0x20
 SYNX_INJECT_BARRIER_TIMEOUT = 1
 SYNX_INJECT_ALLOC_FAILURE = 2
 
@@ -78,7 +79,10 @@ class SynxParams(C.Structure):
         ("persistent_max_voxels", C.c_int32),
         ("test_inject", C.c_int32),
         ("histogram_match", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("smooth_tile_rows", C.c_int32),
+        ("cc_z_chunks", C.c_int32),
+        ("tuning", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
 
@@ -219,6 +223,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_linear_field": (I, [P(SynxLinear), I, P(SynxGeom), V]),
         "synx_write_linear_transform": (I, [C.c_char_p, P(SynxLinear)]),
         "synx_initial_translation": (I, [V, P(SynxGeom), V, P(SynxGeom), I, P(SynxLinear)]),
+        "synx_tuning_load": (I, [C.c_char_p]),
+        "synx_tuning_path": (C.c_char_p, []),
+        "synx_level_plan": (I, [V, I, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -294,6 +301,9 @@ class SyNParams:
     persistent_max_voxels: int = 0  # largest level it runs (0: automatic)
     test_inject: int = 0  # SYNX_INJECT_* (failure-detection tests)
     histogram_match: bool = False  # --use-histogram-matching 1: the moving image matched to the fixed one
+    smooth_tile_rows: int = 0  # 3-D update smoothing: 8/16 slab tiles, -1 two kernels, 0 tuned table / model
+    cc_z_chunks: int = 0  # CC kernel z chunks, 0 tuned table / model
+    tuning: int = 0  # 0: per-level plans from the tuning table; 1: built-in cost models only
 
     def to_c(self) -> SynxParams:
         n = len(self.iterations)
@@ -326,6 +336,9 @@ class SyNParams:
         p.persistent_max_voxels = self.persistent_max_voxels
         p.test_inject = self.test_inject
         p.histogram_match = int(self.histogram_match)
+        p.smooth_tile_rows = int(self.smooth_tile_rows)
+        p.cc_z_chunks = int(self.cc_z_chunks)
+        p.tuning = int(self.tuning)
         return p
 
 
@@ -589,6 +602,13 @@ class SyNStage:
         return {"inverse_ms": a.value, "inverse_launches": b.value, "inverse_voxels": c_.value, "cc_ms": d.value,
                 "cc_launches": e.value, "cc_voxels": f.value}
 
+    def level_plan(self, level: int) -> dict:
+        """The tile plan `level` runs with: persistent level kernel or not, smoothing tile rows (-1:
+        xy and z kernels), CC z chunks (0: cost model)."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        self._ck(self.lib.synx_level_plan(self.h, level, C.byref(a), C.byref(b), C.byref(c)))
+        return {"persistent": a.value, "smooth_rows": b.value, "cc_z_chunks": c.value}
+
     def reset_profile(self) -> None:
         self._ck(self.lib.synx_reset_profile(self.h))
 
@@ -624,6 +644,19 @@ def gaussian_kernel(variance: float, max_error: float, max_width: int) -> np.nda
     out = np.zeros(n.value, np.float64)
     _check(lib.synx_gaussian_kernel(variance, max_error, max_width, _ptr(out), n.value, C.byref(n)))
     return out
+
+
+def tuning_load(path: str | None = None) -> int:
+    """(Re)load the tile-plan table; None reloads the default ($SYNX_TUNING_TABLE or
+    tuning_b200.txt beside libsynx.so).  Returns the number of entries."""
+    n = load_library().synx_tuning_load(path.encode() if path else None)
+    if n < 0:
+        _check(n)
+    return n
+
+
+def tuning_path() -> str:
+    return load_library().synx_tuning_path().decode()
 
 
 def shrink_geom(g: Geom, factor: int) -> Geom:

@@ -20,7 +20,8 @@ A voxel-iteration is one voxel of a level grid processed by one full SyN iterati
               iteration, the compulsory traffic of each step (BYTES_PER_ITER_VOXEL below);
               `achieved_whole_step` applies the same model to all levels over the step time.
   --impl reference -- the CPU path (the oracle restatement of the reference arithmetic, all host
-              threads) on a bounded sample of the same workload: one full-resolution iteration per step.
+              threads) on the same workload: the K timed steps together run one complete registration,
+              each advancing it by up to ceil(240 / K) SyN iterations.
 
 Multi-GPU (torchrun): independent replicas, one pair per rank (no data-path collective);
 value = voxel-iterations of all ranks / max over ranks of the timed region.
@@ -62,6 +63,16 @@ ROOF_LEVEL = 3  # the 182x218x182 level: one iteration graph per replay
 # DRAM bytes (read + write) of one replay of that iteration graph, from the ncu capture summarised
 # in profiles/iteration_graph_182x218x182.md
 ITER_GRAPH_TRAFFIC_BYTES = 3.820e9  # 2.419 GB read + 1.401 GB written (mean of two replays)
+
+
+DATA = "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field"
+
+
+def workload_config(iterations_per_level, voxel_iterations, replicas_n):
+    """The `config` object both arms print: the workload and what one registration of it ran."""
+    return {"workload": WORKLOAD, "iterations_run_per_level": list(iterations_per_level),
+            "voxel_iterations_per_registration": int(voxel_iterations), "l2": "flushed between steps (256 MB)",
+            "parallelism": f"replicas x{replicas_n}"}
 
 
 def dist_env():
@@ -214,21 +225,49 @@ def cpu_sample(fixed, moving, g, threads: int, min_seconds: float = 0.0, max_ite
     return g.count * n / dt, dt, n
 
 
+SCHEDULE_MAX_ITERATIONS = sum(STAGE["iterations"])  # 240: the schedule's iterations without early stops
+
+
 def run_reference(args, fixed, moving, g):
+    """The CPU path on the same configuration as the device arm: the K timed steps together run ONE
+    complete registration of the 182x218x182 pair with the full schedule (preprocessing, the four
+    levels with their set-ups and the convergence monitor at 1e-12, the final composition).  Each
+    step advances that registration by up to ceil(240 / K) SyN iterations (240 = the schedule's
+    iterations without early stops), so the registration is complete within the K steps; steps left
+    after it completes do nothing.  The W warm-up steps advance a separate registration the same way.
+    value = voxel-iterations of the complete registration / the sum of the K step times, the same
+    quantity the device arm reports per registration."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ants_b200.synx import SyNParams
     threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    P = SyNParams(dim=3, **STAGE)
+    per_step = -(-SCHEDULE_MAX_ITERATIONS // max(args.steps, 1))
+    warm = O.SynRun(fixed, g, moving, g, P)
     for _ in range(args.warmup):
-        cpu_sample(fixed, moving, g, threads)
-    times = []
+        warm.advance(per_step)
+    warm.close()
+    run = O.SynRun(fixed, g, moving, g, P)
+    times, vox = [], 0
     for _ in range(args.steps):
-        _, dt, _ = cpu_sample(fixed, moving, g, threads)
-        times.append(dt)
+        t0 = time.perf_counter()
+        vox += run.advance(per_step)
+        times.append(time.perf_counter() - t0)
+    assert run.done, "the complete registration did not finish within the timed steps"
+    levels = run.levels()
+    run.close()
     total = sum(times)
-    value = g.count * args.steps / total
-    sample = "one full-resolution (182x218x182) SyN-CC iteration from zero fields per step"
+    value = vox / total
+    sample = (f"one complete registration of the workload split over the {args.steps} timed steps "
+              f"(up to {per_step} SyN iterations per step); {threads} host threads, CPU restatement of the "
+              f"reference arithmetic, {total:.1f} s")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": sample},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": DATA, "config": workload_config([lv[2] for lv in levels], vox, 1),
+            "cpu_level_seconds": [round(lv[1], 3) for lv in levels],
+            "cpu_level_voxel_iterations": [lv[0] for lv in levels],
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -904,10 +943,9 @@ def main(argv=None) -> int:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field",
-            "config": {"workload": WORKLOAD, "iterations_run_per_level": [its.get(l, 0) for l in range(4)],
-                       "voxel_iterations_per_step": vox_iters // args.steps, "l2": "flushed between steps (256 MB)",
-                       "parallelism": f"replicas x{ws}", "cuda_graphs": not args.plain_launches},
+            "data": DATA,
+            "config": workload_config([its.get(l, 0) for l in range(4)], vox_iters // args.steps, ws),
+            "cuda_graphs": not args.plain_launches,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(Fh.nbytes + Mh.nbytes),
                     "d2h_bytes_per_step": int(fwd_h.nbytes + inv_h.nbytes),
                     "ms_per_step": 1000.0 * t_e2e / args.steps},

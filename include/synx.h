@@ -87,7 +87,14 @@ typedef struct synx_params {
   int32_t histogram_match;       /* 1: match the moving image's histogram to the fixed one's after the
                                     window, or on the images as given when preprocess is 0
                                     (--use-histogram-matching 1; synx_histogram_match) */
-  int32_t reserved[4];
+  /* Tile plan of the per-kernel path (none of these changes the results beyond rounding order; the
+   * smoothing choice not at all).  0 = the tuning table's entry for the level grid (see
+   * synx_tuning_load), or the built-in cost models when the table has none. */
+  int32_t smooth_tile_rows;      /* 3-D update smoothing: 8 or 16 = fused slab kernel with 32 x rows
+                                    column tiles; -1 = xy kernel + z kernel through a temporary */
+  int32_t cc_z_chunks;           /* z chunks of the CC kernel's column walks (>= 1), 0 = table/model */
+  int32_t tuning;                /* 0: use the tuning table; 1: built-in cost models only */
+  int32_t reserved[1];
 } synx_params;
 
 #define SYNX_F_PROFILE_EVENTS 0x1 /* time the dominant kernel class with CUDA events */
@@ -96,6 +103,8 @@ typedef struct synx_params {
 /* Precision-study variants (not antsRegistration behaviour; both run the per-kernel path): */
 #define SYNX_F_CC_FP32_SUMS 0x8  /* CC window sums and variance terms in float instead of double */
 #define SYNX_F_FIELDS_FP16 0x10  /* half-fields rounded to half precision wherever they are stored */
+#define SYNX_F_SMOOTH_TWO_PASS 0x20 /* 3-D field smoothing as an xy kernel and a z kernel through a
+                                       temporary instead of the fused slab kernel (same results) */
 
 /* Failure injection for tests (host-side; nothing faults): the level kernel's grid barrier waits for
  * one block more than it launched, with a short poll limit, so the wait runs out, the kernel ends
@@ -283,6 +292,20 @@ int synx_warp_image_label(const float* img_dev, const synx_geom* img_geom, const
  * Examples/ImageMath_Templates.hxx:1758-1789).  Synchronises the stream. */
 int synx_histogram_match(const float* src_dev, int64_t n_src, const float* ref_dev, int64_t n_ref, int32_t levels,
                          int32_t match_points, int32_t threshold_at_mean, float* out_dev, void* stream);
+
+/* Tile plans chosen by the project's autotuner (python -m ants_b200.autotune): a text table of
+ * measured winners per level grid, one line per (dim, nx, ny, nz, CC radius, smoothing radius) with
+ * the chosen persistent-kernel use, smoothing tile rows and CC z chunks.  Loaded once per process at
+ * the first synx_create from $SYNX_TUNING_TABLE or, if unset, tuning_b200.txt beside libsynx.so.
+ * synx_tuning_load(path) (re)loads a table explicitly (an unreadable path is SYNX_E_ARG); NULL
+ * reloads the default (absent: an empty table); returns the number of entries.  A level grid without an exact entry takes the entry of the
+ * nearest size (same dim and radii, voxel count within a factor of 1.5), else the cost models.
+ * No counterpart in the reference (ITK has no device tiles). */
+int synx_tuning_load(const char* path);
+const char* synx_tuning_path(void);
+/* The plan level `level` of a context runs with (after synx_set_images): persistent = 1 if the
+ * level runs in the persistent level kernel, smoothing tile rows (or -1), CC z chunks. */
+int synx_level_plan(synx_ctx* ctx, int level, int32_t* persistent, int32_t* smooth_rows, int32_t* cc_z_chunks);
 
 /* Windowed CC on two images on the same grid: value (-mean cc), the fixed-to-middle update
  * direction (uses grad of `moving`) and the moving-to-middle one (uses grad of `fixed`)

@@ -48,6 +48,11 @@ def load() -> C.CDLL:
         "oracle_set_threads": (None, [I]),
         "oracle_gaussian_kernel": (I, [D, D, I, V, I]),
         "oracle_shrink_geom": (None, [P(G), C.c_uint, P(G)]),
+        "oracle_run_create_f32": (V, [V, P(G), V, P(G), P(Pm)]),
+        "oracle_run_advance_f32": (C.c_int64, [V, C.c_int64]),
+        "oracle_run_done_f32": (I, [V]),
+        "oracle_run_levels_f32": (I, [V, V, V, V, I]),
+        "oracle_run_destroy_f32": (None, [V]),
     }
     for suf in ("f32", "f64"):
         sigs.update({
@@ -241,3 +246,42 @@ def syn_register(F, gF, M, gM, params, dtype=np.float32):
     log = [dict(level=int(lv[i]), iteration=int(it[i]), metric=float(me[i]), convergence=float(cv[i]),
                 inverse_iterations=int(ki[i])) for i in range(min(n, cap))]
     return fwd, inv, Geom.from_c(go), log
+
+
+class SynRun:
+    """A float32 stage run that is advanced a bounded number of SyN iterations at a time (level
+    set-ups and the final composition included), so that one complete registration can be split
+    over several timed steps.  Running it to the end computes what syn_register computes."""
+
+    def __init__(self, F, gF, M, gM, params):
+        self._keep = (_c(F, np.float32), _c(M, np.float32), gF.to_c(), gM.to_c(), params.to_c())
+        f, m, ga, gb, pc = self._keep
+        self.n_levels = int(params.n_levels) if hasattr(params, "n_levels") else len(params.iterations)
+        self.h = load().oracle_run_create_f32(_p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc))
+
+    def advance(self, n: int) -> int:
+        return int(load().oracle_run_advance_f32(self.h, n))
+
+    @property
+    def done(self) -> bool:
+        return bool(load().oracle_run_done_f32(self.h))
+
+    def levels(self):
+        """[(voxel-iterations, seconds in iterations, iterations run)] per level."""
+        L = self.n_levels
+        vi = np.zeros(L, np.int64)
+        sec = np.zeros(L)
+        it = np.zeros(L, np.int32)
+        load().oracle_run_levels_f32(self.h, _p(vi), _p(sec), _p(it), L)
+        return [(int(a), float(b), int(c)) for a, b, c in zip(vi, sec, it)]
+
+    def close(self):
+        if self.h:
+            load().oracle_run_destroy_f32(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -36,6 +36,14 @@
 
 namespace synx_oracle {
 
+inline double omp_seconds() {
+#ifdef _OPENMP
+  return omp_get_wtime();
+#else
+  return 0.0;
+#endif
+}
+
 // ------------------------------------------------------------------------------------------
 // Geometry: ITK image information (index -> physical point p = origin + D * diag(sp) * idx).
 // ------------------------------------------------------------------------------------------
@@ -1080,22 +1088,47 @@ inline void syn_iteration(const T* Fs, const Geom& gF, const T* Ms, const Geom& 
   if (inv_iters) *inv_iters = k;
 }
 
+// A stage run that can be advanced a bounded number of SyN iterations at a time (the CPU
+// baseline splits one complete registration over its timed steps).  Level set-up (image
+// smoothing, field resampling) happens when the first iteration of a level is due; the final
+// composition when the last level ends.  Running it to the end is syn_register.
 template <class T>
-inline void syn_register(const T* F_in, const Geom& gF, const T* M_in, const Geom& gM, const SynParams& P,
-                         std::vector<T>& fwd, std::vector<T>& inv, Geom& gOut, SynLog* log = nullptr) {
-  const int64_t NF = gF.count(), NM = gM.count();
-  std::vector<T> F(NF), M(NM);
-  if (P.preprocess) {
-    preprocess_image(F_in, F.data(), NF, P.q_lo, P.q_hi);
-    preprocess_image(M_in, M.data(), NM, P.q_lo, P.q_hi);
-  } else {
-    std::memcpy(F.data(), F_in, sizeof(T) * NF);
-    std::memcpy(M.data(), M_in, sizeof(T) * NM);
-  }
-  if (P.histogram_match) histogram_match(M.data(), NM, F.data(), NF, 256, 12, true, M.data());
+struct SynRun {
+  SynParams P;
+  Geom gF, gM;
+  std::vector<T> F, M, Fs, Ms;
   SynState<T> S;
-  std::vector<T> Fs(NF), Ms(NM);
-  for (int l = 0; l < P.n_levels; ++l) {
+  int level = -1;   // current level (-1: none set up yet)
+  int k = 0;        // iterations run in the current level
+  bool level_done = true;
+  bool done = false;
+  std::vector<double> energies;
+  double total_abs = 0.0;
+  std::vector<T> fwd, inv;
+  SynLog log;
+  std::vector<int64_t> level_voxels;
+  std::vector<double> level_seconds;
+
+  SynRun(const T* F_in, const Geom& gF_, const T* M_in, const Geom& gM_, const SynParams& P_)
+      : P(P_), gF(gF_), gM(gM_) {
+    const int64_t NF = gF.count(), NM = gM.count();
+    F.resize(NF);
+    M.resize(NM);
+    if (P.preprocess) {
+      preprocess_image(F_in, F.data(), NF, P.q_lo, P.q_hi);
+      preprocess_image(M_in, M.data(), NM, P.q_lo, P.q_hi);
+    } else {
+      std::memcpy(F.data(), F_in, sizeof(T) * NF);
+      std::memcpy(M.data(), M_in, sizeof(T) * NM);
+    }
+    if (P.histogram_match) histogram_match(M.data(), NM, F.data(), NF, 256, 12, true, M.data());
+    Fs.resize(NF);
+    Ms.resize(NM);
+    level_voxels.assign(P.n_levels, 0);
+    level_seconds.assign(P.n_levels, 0.0);
+  }
+
+  void setup_level(int l) {
     unsigned f[3];
     shrink_factors_per_dim(gF.dim, P.shrink[l], gF.sp, f);
     Geom gl = shrink_geom(gF, f);
@@ -1118,32 +1151,72 @@ inline void syn_register(const T* F_in, const Geom& gF, const T* M_in, const Geo
       }
       S.g = gl;
     }
-    std::vector<double> energies;
-    double total_abs = 0.0;
-    for (int k = 1; k <= P.iters[l]; ++k) {
+    level = l;
+    k = 0;
+    level_done = false;
+    energies.clear();
+    total_abs = 0.0;
+  }
+
+  void finish() {
+    const int64_t N = S.g.count();
+    const int D = S.g.dim;
+    fwd.assign((size_t)N * D, (T)0);
+    inv.assign((size_t)N * D, (T)0);
+    compose(S.psiM.data(), S.phiF.data(), S.g, fwd.data());
+    compose(S.psiF.data(), S.phiM.data(), S.g, inv.data());
+    done = true;
+  }
+
+  // Runs up to n SyN iterations (with the level set-ups they need, and the final composition once
+  // the last level ends).  Returns the voxel-iterations run.
+  int64_t advance(int64_t n) {
+    int64_t vi = 0;
+    while (!done && n > 0) {
+      if (level_done) {
+        if (level + 1 >= P.n_levels) {
+          finish();
+          break;
+        }
+        setup_level(level + 1);
+        if (P.iters[level] <= 0) {
+          level_done = true;
+          continue;
+        }
+      }
       double metric = 0.0;
       int ki = 0;
+      const double t0 = omp_seconds();
       syn_iteration(Fs.data(), gF, Ms.data(), gM, P, S, &metric, &ki);
+      level_seconds[level] += omp_seconds() - t0;
+      ++k;
+      --n;
+      vi += S.g.count();
+      level_voxels[level] += S.g.count();
       energies.push_back(metric);
       total_abs += std::fabs(metric);
-      double cv = convergence_value(energies, total_abs, P.conv_window);
-      if (log) {
-        log->level.push_back(l);
-        log->iter.push_back(k);
-        log->metric.push_back(metric);
-        log->conv.push_back(cv);
-        log->inv_iters.push_back(ki);
-      }
-      if (cv < P.conv_thresh) break;
+      const double cv = convergence_value(energies, total_abs, P.conv_window);
+      log.level.push_back(level);
+      log.iter.push_back(k);
+      log.metric.push_back(metric);
+      log.conv.push_back(cv);
+      log.inv_iters.push_back(ki);
+      if (cv < P.conv_thresh || k >= P.iters[level]) level_done = true;
     }
+    if (!done && level_done && level + 1 >= P.n_levels) finish();
+    return vi;
   }
-  const int64_t N = S.g.count();
-  const int D = S.g.dim;
-  fwd.assign((size_t)N * D, (T)0);
-  inv.assign((size_t)N * D, (T)0);
-  compose(S.psiM.data(), S.phiF.data(), S.g, fwd.data());
-  compose(S.psiF.data(), S.phiM.data(), S.g, inv.data());
-  gOut = S.g;
+};
+
+template <class T>
+inline void syn_register(const T* F_in, const Geom& gF, const T* M_in, const Geom& gM, const SynParams& P,
+                         std::vector<T>& fwd, std::vector<T>& inv, Geom& gOut, SynLog* log = nullptr) {
+  SynRun<T> R(F_in, gF, M_in, gM, P);
+  while (!R.done) R.advance(INT64_MAX);
+  fwd.swap(R.fwd);
+  inv.swap(R.inv);
+  gOut = R.S.g;
+  if (log) *log = R.log;
 }
 
 }  // namespace synx_oracle

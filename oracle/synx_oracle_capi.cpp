@@ -186,4 +186,27 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
 ORACLE_TYPED(f32, float)
 ORACLE_TYPED(f64, double)
 
+/* A float stage run advanced in bounded pieces (the CPU baseline's timed steps).  advance returns
+   the voxel-iterations it ran; the run is done once the final composition has been made. */
+void* oracle_run_create_f32(const float* F, const synx_geom* gF, const float* M, const synx_geom* gM,
+                            const synx_params* p) {
+  return new SynRun<float>(F, to_geom(gF), M, to_geom(gM), to_params(p));
+}
+int64_t oracle_run_advance_f32(void* h, int64_t n) { return static_cast<SynRun<float>*>(h)->advance(n); }
+int oracle_run_done_f32(void* h) { return static_cast<SynRun<float>*>(h)->done ? 1 : 0; }
+/* Per level: voxel-iterations run and seconds spent in its iterations; returns the record count. */
+int oracle_run_levels_f32(void* h, int64_t* voxel_iters, double* seconds, int32_t* iterations, int cap) {
+  auto* R = static_cast<SynRun<float>*>(h);
+  const int L = R->P.n_levels;
+  for (int l = 0; l < L && l < cap; ++l) {
+    voxel_iters[l] = R->level_voxels[l];
+    seconds[l] = R->level_seconds[l];
+    int n = 0;
+    for (int v : R->log.level) n += v == l;
+    iterations[l] = n;
+  }
+  return L;
+}
+void oracle_run_destroy_f32(void* h) { delete static_cast<SynRun<float>*>(h); }
+
 }  // extern "C"

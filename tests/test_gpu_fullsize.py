@@ -1,7 +1,8 @@
-"""Size-independent properties at the full 182x218x182 size of the single-pair workload (the
-oracle is too slow there): the CC value and both update directions are invariant to an affine
-intensity change of the fixed image, update smoothing is linear, a registration repeats bit for
-bit, and its forward and inverse fields compose to (nearly) the identity."""
+"""Properties at the full 182x218x182 size of the single-pair workload (the whole-stage comparison
+with the oracle at this size is in test_zz_v_parity_configs.py): the CC value and both update
+directions are invariant to an affine intensity change of the fixed image, update smoothing is
+linear and matches the oracle, a registration repeats bit for bit, and its forward and inverse
+fields compose to (nearly) the identity."""
 import numpy as np
 import pytest
 import torch
@@ -49,6 +50,17 @@ def test_update_smoothing_is_linear(cuda):
     synx.smooth_field(2.0 * u - 0.5 * v, sw, g, 3.0)
     err = (sw - (2.0 * su - 0.5 * sv)).abs().max().item()
     assert err < 1e-5 * max(1.0, sw.abs().max().item())
+
+
+def test_update_smoothing_matches_oracle_at_full_size(cuda):
+    # the slab smoothing kernel walks z in chunks at this size: compare it with the oracle
+    import oracle as O
+    g = Geom(SIZE)
+    u = np.random.default_rng(6).standard_normal((3,) + g.shape).astype(np.float32)
+    ref = O.smooth_field(u, g, 3.0)
+    out = torch.empty((3,) + g.shape, device="cuda")
+    synx.smooth_field(torch.from_numpy(u).cuda(), out, g, 3.0)
+    np.testing.assert_allclose(out.cpu().numpy(), ref, atol=2e-6, rtol=0)
 
 
 def test_registration_repeats_and_fields_are_inverse(cuda, pair):

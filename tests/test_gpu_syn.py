@@ -14,7 +14,7 @@ import pytest
 
 import oracle as O
 from ants_b200 import phantoms
-from ants_b200.synx import SYNX_F_NO_PERSISTENT, SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage
+from ants_b200.synx import SYNX_F_NO_PERSISTENT, SYNX_F_SMOOTH_TWO_PASS, SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage
 
 pytestmark = pytest.mark.gpu
 
@@ -179,3 +179,23 @@ def test_run_level_order_enforced(cuda):
         st.run_level(0)
         st.run_level(1)
         assert st.output_geom().size == (32, 32)
+
+
+@pytest.mark.parametrize("uvar", [3.0, 0.3, 8.0])
+def test_slab_smoothing_matches_two_pass_bit_for_bit(cuda, uvar):
+    # the fused slab smoothing (xy and z in one kernel) and the two-kernel path through a temporary
+    # do the same arithmetic in the same order: whole registrations agree bit for bit
+    f, m = make_pair(3, (41, 37, 33), seed=13)
+    g = Geom((41, 37, 33))
+    outs = []
+    for extra in (0, SYNX_F_SMOOTH_TWO_PASS):
+        P = SyNParams(dim=3, cc_radius=3, update_variance=uvar, iterations=(5, 3), shrink_factors=(2, 1),
+                      smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12,
+                      flags=SYNX_F_USE_GRAPHS | SYNX_F_NO_PERSISTENT | extra)
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.run()
+            outs.append((st.fields(), [r.metric for r in st.log()]))
+    np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
+    np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
+    assert outs[0][1] == outs[1][1]
