@@ -16,14 +16,15 @@
 //       (repeatable, the first given acting first; linear .mat/.txt files, or the translation derived
 //       from two images: feature 0 geometric centers, 1 centers of mass, 2 origins)
 //   -z/--collapse-output-transforms 0|1 (default 1)   -a/--write-composite-transform 0
+//   -x/--masks [fixedMask,movingMask] | fixedMask (metric masks; a name that is not a file = no mask)
 // Output: prefix0Warp.nii.gz and prefix0InverseWarp.nii.gz (antsRegistrationTemplateHeader.cxx:74-90
 // names for SyN); with initial transforms, prefix0GenericAffine.mat (them, collapsed) and
 // prefix1Warp / prefix1InverseWarp, or without collapsing prefix<n>Warp after the n initial
 // transforms; plus the warped images when requested.  The initial transform is folded into the
 // moving image's geometry (an index <-> physical map the device functions take in general form),
 // which samples the moving image at Init(x + psi_M(x)) exactly.  With -z 0, derived translations are
-// written as prefix<n>DerivedInitialMovingTranslation.mat.  Other stages, metrics, masks,
-// initial fixed transforms and HDF5 composite output are rejected with EXIT_FAILURE.
+// written as prefix<n>DerivedInitialMovingTranslation.mat.  Other stages, metrics, initial fixed
+// transforms and HDF5 composite output are rejected with EXIT_FAILURE.
 #include "ants_registration.h"
 
 #include <cuda_runtime.h>
@@ -83,9 +84,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     auto it = opt.find(n);
     return it == opt.end() ? def : it->second.back();
   };
-  for (const char* bad : {"masks", "initial-fixed-transform", "restore-state", "save-state", "restrict-deformation"})
-    if (opt.count(bad) && !(std::string(bad) == "masks" && opt[bad].back() == "[NULL,NULL]"))
-      throw std::runtime_error(std::string("option --") + bad + " is not supported by this SyN+CC stage");
+  for (const char* bad : {"initial-fixed-transform", "restore-state", "save-state", "restrict-deformation"})
+    if (opt.count(bad)) throw std::runtime_error(std::string("option --") + bad + " is not supported by this SyN+CC stage");
   auto flag = [&](const std::string& n, bool def) {
     if (!opt.count(n)) return def;
     const std::string v = lower(one(n, ""));
@@ -245,12 +245,48 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       out << "  initial moving transform: " << init.size()
           << " linear transform(s), folded into the moving image geometry" << std::endl;
   }
+  // -x [fixedMask,movingMask] or -x fixedMask (antsRegistrationTemplateHeader.h:363-425): a file that
+  // does not exist (NULL, for instance) means no mask for that image; one stage, so one -x
+  nifti::Image mask_f, mask_m;
+  bool have_mask_f = false, have_mask_m = false;
+  if (opt.count("masks")) {
+    if (opt["masks"].size() != 1) throw std::runtime_error("one --masks option per stage: this is one stage");
+    OptionCall x = parse_call(opt["masks"][0]);
+    std::vector<std::string> names = x.params.empty() ? std::vector<std::string>{x.name} : x.params;
+    auto exists = [](const std::string& f) {
+      FILE* fh = std::fopen(f.c_str(), "rb");
+      if (fh) std::fclose(fh);
+      return fh != nullptr;
+    };
+    if (!names.empty() && exists(names[0])) {
+      mask_f = nifti::read(names[0]);
+      have_mask_f = true;
+    }
+    if (names.size() > 1 && exists(names[1])) {
+      mask_m = nifti::read(names[1]);
+      have_mask_m = true;
+    }
+    if ((have_mask_f && mask_f.components != 1) || (have_mask_m && mask_m.components != 1))
+      throw std::runtime_error("scalar mask images expected");
+  }
   synx_ctx* ctx = nullptr;
   if (synx_create(&p, gpu, nullptr, &ctx) != 0) throw std::runtime_error(std::string("synx_create: ") + synx_last_error(nullptr));
   struct Guard {
     synx_ctx* c;
     ~Guard() { synx_destroy(c); }
   } guard{ctx};
+  if (have_mask_f || have_mask_m) {
+    const synx_geom gmf = have_mask_f ? to_geom(mask_f, dim) : synx_geom{};
+    // the moving mask is sampled through the same transforms as the moving image
+    synx_geom gmm = have_mask_m ? to_geom(mask_m, dim) : synx_geom{};
+    if (have_mask_m && !init.empty()) gmm = push_forward(gmm, init_inverse);
+    if (synx_set_masks(ctx, have_mask_f ? mask_f.data.data() : nullptr, have_mask_f ? &gmf : nullptr,
+                       have_mask_m ? mask_m.data.data() : nullptr, have_mask_m ? &gmm : nullptr) != 0)
+      throw std::runtime_error(std::string("synx_set_masks: ") + synx_last_error(ctx));
+    if (verbose)
+      out << "  metric masks: fixed " << (have_mask_f ? "yes" : "no") << ", moving " << (have_mask_m ? "yes" : "no")
+          << std::endl;
+  }
   auto t0 = std::chrono::steady_clock::now();
   if (synx_set_images(ctx, fixed.data.data(), &gf, moving.data.data(), &gm) != 0)
     throw std::runtime_error(std::string("synx_set_images: ") + synx_last_error(ctx));

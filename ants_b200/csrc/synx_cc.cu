@@ -10,20 +10,25 @@ namespace synx {
 
 // Standalone CC kernel: one tile per block, deterministic metric reduction (block partials,
 // the last block sums them in order).
-template <int R, int DIM, typename T>
+// With metric masks (MASKED) the partials hold each block's cc sum and, after them, its count of
+// valid voxels; the value is -sum / count.
+template <int R, int DIM, typename T, bool MASKED = false>
 __global__ void __launch_bounds__(256)
     k_cc(const float* __restrict__ Ft, const float* __restrict__ Mt, Dims d, CCParams P, float* __restrict__ gF,
          float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out) {
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
+  __shared__ double vcount;
   __shared__ int am_last;
   const int tid = threadIdx.x;
-  const double bs = cc_tile<R, DIM, T>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw, red);
+  const double bs = cc_tile<R, DIM, T, MASKED>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y, blockIdx.z,
+                                               smem_raw, red, &vcount);
   const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
   const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (tid == 0) {
     partials[bid] = bs;
+    if (MASKED) partials[nblocks + bid] = vcount;
     __threadfence();
     unsigned t = atomicAdd(&ctl->cc_counter, 1u);
     am_last = (t == nblocks - 1);
@@ -31,12 +36,20 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   if (am_last) {
     __threadfence();
-    double s = 0.0;
-    for (unsigned b = tid; b < nblocks; b += 256) s += __ldcg(partials + b);
+    double s = 0.0, n = 0.0;
+    for (unsigned b = tid; b < nblocks; b += 256) {
+      s += __ldcg(partials + b);
+      if (MASKED) n += __ldcg(partials + nblocks + b);
+    }
     s = block_sum_d(s, red);
+    if (MASKED) {
+      __syncthreads();
+      n = block_sum_d(n, red);
+    }
     if (tid == 0) {
+      const double cnt = MASKED ? n : (double)d.N;
       ctl->cc_sum = s;
-      ctl->metric = -s / (double)d.N;
+      ctl->metric = cnt > 0.0 ? -s / cnt : 0.0;
       ctl->cc_counter = 0u;
     }
   }
@@ -45,7 +58,10 @@ __global__ void __launch_bounds__(256)
 template <int R, int DIM>
 static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, float* gF, float* gM, double* partials,
                         IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P, bool fp32) {
-  if (fp32)
+  if (P.valid != nullptr)
+    k_cc<R, DIM, double, true><<<grid, 256, CCShape<R, DIM, double, true>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials,
+                                                                                     ctl, cc_out);
+  else if (fp32)
     k_cc<R, DIM, float><<<grid, 256, CCShape<R, DIM, float>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
   else
     k_cc<R, DIM, double><<<grid, 256, CCShape<R, DIM, double>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl,
@@ -96,17 +112,21 @@ int cc_blocks_max(const GridInfo& g, int radius) {
   return cc_blocks(g, radius, cc_max_chunks(g, radius));
 }
 
-size_t cc_smem_bytes(int dim, int radius) {
-  // CCShape<R, DIM, double>::smem for a run-time radius
+size_t cc_smem_bytes(int dim, int radius, bool masked) {
+  // CCShape<R, DIM, double, masked>::smem for a run-time radius
   const size_t TX = 32, TY = 8, HX = TX + 2 * radius, HY = TY + 2 * radius, HC = HX * HY;
   const size_t RD = dim == 3 ? 2 * radius + 1 : 1;
-  return RD * HC * 8 + 5 * HY * (HX | 1) * 8 + 5 * HY * (TX + 1) * 8;
+  const size_t nq = masked ? 6 : 5;
+  return RD * HC * 8 + nq * HY * (HX | 1) * 8 + nq * HY * (TX + 1) * 8 + (masked ? RD * HC : 0);
 }
 
 template <int R, int DIM>
 static cudaError_t cc_prepare_t() {
   cudaError_t e = cudaFuncSetAttribute(k_cc<R, DIM, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)CCShape<R, DIM, double>::smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_cc<R, DIM, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)CCShape<R, DIM, double, true>::smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_cc<R, DIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)CCShape<R, DIM, float>::smem);
@@ -131,7 +151,7 @@ cudaError_t cc_prepare(int dim, int radius) {
 }
 
 bool cc_radius_supported(int dim, int radius) {
-  return radius >= 1 && radius <= 7 && cc_smem_bytes(dim, radius) <= 227 * 1024;
+  return radius >= 1 && radius <= 7 && cc_smem_bytes(dim, radius, true) <= 227 * 1024;
 }
 
 CCParams make_cc_params(const GridInfo& g, int radius, int chunks) {
@@ -144,14 +164,16 @@ CCParams make_cc_params(const GridInfo& g, int radius, int chunks) {
   }
   P.identity_dir = ident ? 1 : 0;
   P.eps = 1.1920928955078125e-07;  // FLT_EPSILON: the reference metric's float guard
+  P.valid = nullptr;
   P.ZC = cc_zchunk(g, radius, chunks);
   return P;
 }
 
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out, bool fp32_sums, int chunks) {
+               IterCtl* ctl, cudaStream_t s, float* cc_out, bool fp32_sums, int chunks, const unsigned char* valid) {
   add_launch_count(1);
-  const CCParams P = make_cc_params(g, radius, chunks);
+  CCParams P = make_cc_params(g, radius, chunks);
+  P.valid = valid;
   dim3 grid((g.d.nx + 31) / 32, (g.d.ny + 7) / 8, (g.d.nz + P.ZC - 1) / P.ZC);
 #define SYNX_CC_CASE(RR)                                                                         \
   case RR:                                                                                       \

@@ -34,6 +34,7 @@ struct CCParams {
   int identity_dir;
   double eps;
   int ZC;          // z-chunk per block
+  const unsigned char* valid;  // metric masks: nonzero = valid voxel (MASKED tiles only)
 };
 
 __device__ __forceinline__ int pmod(int a, int m) {
@@ -47,17 +48,20 @@ __device__ __forceinline__ float grad1(float vm, float v0, float vp, int pos, in
   return (vp - vm) / (2.0f * h);
 }
 
-template <int R, int DIM, typename T = double>
+// With metric masks (MASKED) a sixth quantity, the count of valid voxels, is box-summed beside the
+// five sums, and a byte ring holds the validity of the ring's slices.
+template <int R, int DIM, typename T = double, bool MASKED = false>
 struct CCShape {
   static constexpr int TX = 32, TY = 8;
   static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HC = HX * HY;
   static constexpr int RZ = DIM == 3 ? R : 0;
   static constexpr int RD = 2 * RZ + 1;
   static constexpr int CPT = (HC + 255) / 256;
+  static constexpr int NQ = MASKED ? 6 : 5;
   static constexpr int CSP = HX | 1;   // row pitch of the column sums (odd)
   static constexpr int XSP = TX + 1;   // row pitch of the x box sums (odd)
-  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)5 * HY * CSP * sizeof(T) +
-                                 (size_t)5 * HY * XSP * sizeof(T);
+  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)NQ * HY * CSP * sizeof(T) +
+                                 (size_t)NQ * HY * XSP * sizeof(T) + (MASKED ? (size_t)RD * HC : 0);
 };
 
 // One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
@@ -74,18 +78,20 @@ __device__ __forceinline__ float rcp_rn<float>(float x) {
   return __frcp_rn(x);
 }
 
-template <int R, int DIM, typename T = double>
+template <int R, int DIM, typename T = double, bool MASKED = false>
 __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const float* __restrict__ Mt, const Dims& d,
                                           const CCParams& P, float* __restrict__ gF, float* __restrict__ gM,
                                           float* __restrict__ cc_out, int bx, int by, int bz,
-                                          unsigned char* smem_raw, double* red) {
-  using S = CCShape<R, DIM, T>;
+                                          unsigned char* smem_raw, double* red, double* valid_count = nullptr) {
+  using S = CCShape<R, DIM, T, MASKED>;
   constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
-  constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY;
+  constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY, NQ = S::NQ;
   float2* ring = reinterpret_cast<float2*>(smem_raw);
-  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [5][HY][CSP]; reused as ys [5][TY][TX] after the x pass
-  T* xs = cs + 5 * HY * CSP;                      // [5][HY][XSP]
+  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [NQ][HY][CSP]; reused as ys [NQ][TY][TX] after the x pass
+  T* xs = cs + NQ * HY * CSP;                     // [NQ][HY][XSP]
   T* ys = cs;
+  unsigned char* vring = reinterpret_cast<unsigned char*>(xs + NQ * HY * XSP);  // [RD][HC] (MASKED)
+  const unsigned char* __restrict__ valid = P.valid;
 
   const int tid = threadIdx.x;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
@@ -107,13 +113,11 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     sofs[c] = hy * CSP + hx;
   }
   // sliding-window tasks: x pass (quantity, half, halo row), y pass (quantity, output column)
-  const int xrow = tid % HY, xhalf = (tid / HY) & 1, xq = tid / (2 * HY);
-  const int ycol = tid & 31, yq = tid >> 5;
-  T acc[CPT][5];
+  T acc[CPT][NQ];
 #pragma unroll
   for (int c = 0; c < CPT; ++c)
 #pragma unroll
-    for (int q = 0; q < 5; ++q) acc[c][q] = T(0);
+    for (int q = 0; q < NQ; ++q) acc[c][q] = T(0);
 
   // warm-up: slices z0-RZ .. z0+RZ-1
   for (int zs = z0 - RZ; zs < z0 + RZ; ++zs) {
@@ -124,23 +128,29 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       int col = tid + c * 256;
       if (col < HC) {
         float2 v = make_float2(0.0f, 0.0f);
+        unsigned char vb = 0;
         if (zin && gval[c]) {
           long long o = (long long)zs * nxy + gofs[c];
           v.x = __ldg(Ft + o);
           v.y = __ldg(Mt + o);
-          const T f = v.x, m = v.y;
-          acc[c][0] += f;
-          acc[c][1] += m;
-          acc[c][2] += f * f;
-          acc[c][3] += m * m;
-          acc[c][4] += f * m;
+          vb = MASKED ? __ldg(valid + o) : 1;
+          if (vb) {
+            const T f = v.x, m = v.y;
+            acc[c][0] += f;
+            acc[c][1] += m;
+            acc[c][2] += f * f;
+            acc[c][3] += m * m;
+            acc[c][4] += f * m;
+            if (MASKED) acc[c][NQ - 1] += T(1);
+          }
         }
         ring[slot * HC + col] = v;
+        if (MASKED) vring[slot * HC + col] = vb;
       }
     }
   }
 
-  double cc_acc = 0.0;
+  double cc_acc = 0.0, n_valid = 0.0;
   const int tx = tid & 31, ty = tid >> 5;
   const int ox = x0 + tx, oy = y0 + ty;
   const bool out_ok = ox < nx && oy < ny;
@@ -150,12 +160,15 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   // the (F, M) values of the slice entering the z window are loaded one slice ahead, so the
   // loads overlap the previous slice's box sums and CC terms
   float2 nv[CPT];
+  unsigned char nvb[CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) {
     nv[c] = make_float2(0.0f, 0.0f);
+    nvb[c] = 0;
     if (z0 < z1 && z0 + RZ < nz && gval[c]) {
       const long long o = (long long)(z0 + RZ) * nxy + gofs[c];
       nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
+      if (MASKED) nvb[c] = __ldg(valid + o);
     }
   }
   for (int zc = z0; zc < z1; ++zc) {
@@ -169,7 +182,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     for (int c = 0; c < CPT; ++c) {
       int col = tid + c * 256;
       if (col < HC) {
-        if (sub && gval[c]) {
+        if (sub && gval[c] && (!MASKED || vring[slot * HC + col])) {
           float2 o = ring[slot * HC + col];
           const T f = o.x, m = o.y;
           acc[c][0] -= f;
@@ -177,29 +190,37 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
           acc[c][2] -= f * f;
           acc[c][3] -= m * m;
           acc[c][4] -= f * m;
+          if (MASKED) acc[c][NQ - 1] -= T(1);
         }
         const float2 v = nv[c];  // zero outside the volume
-        if (zin && gval[c]) {
+        const unsigned char vb = MASKED ? nvb[c] : 1;
+        if (zin && gval[c] && vb) {
           const T f = v.x, m = v.y;
           acc[c][0] += f;
           acc[c][1] += m;
           acc[c][2] += f * f;
           acc[c][3] += m * m;
           acc[c][4] += f * m;
+          if (MASKED) acc[c][NQ - 1] += T(1);
         }
         ring[slot * HC + col] = v;
+        if (MASKED) vring[slot * HC + col] = (zin && gval[c]) ? vb : 0;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) cs[q * HY * CSP + sofs[c]] = acc[c][q];
+        for (int q = 0; q < NQ; ++q) cs[q * HY * CSP + sofs[c]] = acc[c][q];
         nv[c] = make_float2(0.0f, 0.0f);
+        if (MASKED) nvb[c] = 0;
         if (znext && gval[c]) {
           const long long o = (long long)(ze + 1) * nxy + gofs[c];
           nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
+          if (MASKED) nvb[c] = __ldg(valid + o);
         }
       }
     }
     __syncthreads();
-    // x box sums, sliding along the row: outputs 16 h .. 16 h + 15 of one halo row
-    if (xq < 5) {
+    // x box sums, sliding along the row: outputs 16 h .. 16 h + 15 of one halo row (one task per
+    // quantity, half and halo row)
+    for (int task = tid; task < NQ * 2 * HY; task += 256) {
+      const int xrow = task % HY, xhalf = (task / HY) & 1, xq = task / (2 * HY);
       const T* src = cs + xq * HY * CSP + xrow * CSP + 16 * xhalf;
       T* dst = xs + xq * HY * XSP + xrow * XSP + 16 * xhalf;
       T s = T(0);
@@ -214,8 +235,10 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       }
     }
     __syncthreads();
-    // y box sums, sliding down one output column over the TY output rows
-    if (yq < 5) {
+    // y box sums, sliding down one output column over the TY output rows (one task per quantity
+    // and output column)
+    for (int task = tid; task < NQ * 32; task += 256) {
+      const int ycol = task & 31, yq = task >> 5;
       const T* src = xs + yq * HY * XSP + ycol;
       T* dst = ys + yq * TY * TX + ycol;
       T s = T(0);
@@ -230,18 +253,26 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       }
     }
     __syncthreads();
-    if (out_ok) {
-      T Sq[5];
+    const int cidx = (ty + R) * HX + (tx + R);
+    const bool center_ok = out_ok && (!MASKED || vring[pmod(zc, RD) * HC + cidx]);
+    if (MASKED && out_ok && !center_ok) {  // a masked-out voxel: no value, no update
+      const long long oi = (long long)zc * nxy + (long long)oy * nx + ox;
 #pragma unroll
-      for (int q = 0; q < 5; ++q) Sq[q] = ys[q * TY * TX + ty * TX + tx];
+      for (int dd = 0; dd < DIM; ++dd) gF[dd * N + oi] = gM[dd * N + oi] = 0.0f;
+      if (cc_out != nullptr) cc_out[oi] = 0.0f;
+    }
+    if (center_ok) {
+      T Sq[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) Sq[q] = ys[q * TY * TX + ty * TX + tx];
       const T czn = (T)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
-      const T n = cxn * cyn * czn;
+      const T n = MASKED ? Sq[NQ - 1] : cxn * cyn * czn;
+      if (MASKED) n_valid += 1.0;
       const T inv_n = rcp_rn(n);
       const T mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
       const T sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
       const T sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
       const T sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
-      const int cidx = (ty + R) * HX + (tx + R);
       const float2* rc = ring + pmod(zc, RD) * HC;
       const float2 v0 = rc[cidx];
       const T fh = (T)v0.x - mF, mh = (T)v0.y - mM;
@@ -293,6 +324,11 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       if (cc_out != nullptr) cc_out[oi] = (float)cc;
     }
     __syncthreads();
+  }
+  if (MASKED) {
+    const double nv = block_sum_d(n_valid, red);
+    if (tid == 0 && valid_count) *valid_count = nv;
+    __syncthreads();  // red is reused below
   }
   return block_sum_d(cc_acc, red);
 }

@@ -208,6 +208,12 @@ struct synx_ctx {
   std::vector<int> h_li;
   // tile plan per level (stage parameters, then the tuning table, then the cost models)
   LevelPlan plan[SYNX_MAX_LEVELS] = {};
+  // metric masks (synx_set_masks): one byte per voxel on their own grids, null for none; the
+  // per-iteration validity of the virtual voxels lives in the arena
+  unsigned char* maskF = nullptr;
+  unsigned char* maskM = nullptr;
+  GridInfo gmF{}, gmM{};
+  unsigned char* valid = nullptr;
   // canonical buffer assignment (level changes swap field and work buffers)
   float* canon[8] = {};
   // graphs: one executable per level, valid while the arena and grids are unchanged
@@ -277,7 +283,7 @@ long long level_inv_units(const GridInfo& g);
 
 // Byte offsets of everything a context keeps on the device, for its images and schedule.
 struct ArenaPlan {
-  size_t F0, M0, Fs, Ms, Tmp, Field[4], Ft, Mt, Work[6], CC, IS, IM, Cu, Ct, Ci, Ctl, Lm, Lc, Li, H;
+  size_t F0, M0, Fs, Ms, Tmp, Field[4], Ft, Mt, Work[6], CC, IS, IM, Cu, Ct, Ci, Ctl, Lm, Lc, Li, H, V;
   size_t total;
   int ccb, invb, coeff_cap, max_iters;
 };
@@ -307,11 +313,13 @@ ArenaPlan arena_plan(const synx_ctx* c) {
   for (int k = 0; k < 4; ++k) a.Field[k] = add(4 * (size_t)D * Nmax);
   a.Ft = add(4 * Nmax), a.Mt = add(4 * Nmax);
   for (int k = 0; k < 6; ++k) a.Work[k] = add(4 * (size_t)D * Nmax);
-  a.CC = add(8 * (size_t)ccb), a.IS = add(8 * 2 * (size_t)invb), a.IM = add(4 * 2 * (size_t)invb);
+  // CC partials: the block sums and, with metric masks, the blocks' valid counts after them
+  a.CC = add(8 * 2 * (size_t)ccb), a.IS = add(8 * 2 * (size_t)invb), a.IM = add(4 * 2 * (size_t)invb);
   a.Cu = add(4 * 3 * coeff_cap), a.Ct = add(4 * 3 * coeff_cap), a.Ci = add(8 * 3 * coeff_cap);
   a.Ctl = add(sizeof(IterCtl));
   a.Lm = add(8 * (size_t)max_iters), a.Lc = add(8 * (size_t)max_iters), a.Li = add(4 * (size_t)max_iters);
   a.H = add(std::max((size_t)4 * 258, hm_scratch_bytes(256)));
+  a.V = add((size_t)Nmax);  // metric-mask validity, one byte per voxel of the largest level
   a.total = sz;
   a.ccb = ccb;
   a.invb = invb;
@@ -375,6 +383,7 @@ int allocate(synx_ctx* c) {
   c->logdev.inv_iters = (int*)(a + oLi);
   c->logdev.cap = max_iters;
   c->hist = (unsigned*)(a + oH);
+  c->valid = (unsigned char*)(a + pl.V);
   CUDA_TRY(c, cudaMemsetAsync(c->ctl, 0, sizeof(IterCtl), c->stream));
   return SYNX_OK;
 }
@@ -630,9 +639,11 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
     return idx;
   };
   launch_warp_pair(c->Fs, c->gF, c->psiF, c->Ms, c->gM, c->psiM, g, c->Ft, c->Mt, c->ctl, s);
+  const bool masked = c->maskF != nullptr || c->maskM != nullptr;
+  if (masked) launch_mask_validity(c->maskF, c->gmF, c->psiF, c->maskM, c->gmM, c->psiM, g, c->valid, c->ctl, s);
   int e0 = profile ? ev() : -1;
   launch_cc(c->Ft, c->Mt, g, c->P.cc_radius, c->gFu, c->gMu, c->cc_partials, c->ctl, s, nullptr,
-            (c->P.flags & SYNX_F_CC_FP32_SUMS) != 0, c->plan[c->cur_level].cc_chunks);
+            (c->P.flags & SYNX_F_CC_FP32_SUMS) != 0, c->plan[c->cur_level].cc_chunks, masked ? c->valid : nullptr);
   if (profile) c->ev_pairs_cc.push_back({e0, ev()});
   // update-field smoothing, SyN epilogue (boundary zero, blend) and max ||u/spacing||
   const float* upd[2] = {c->t1F, c->t1M};
@@ -752,6 +763,7 @@ long long level_inv_units(const GridInfo& g) {
 // Whether the level kernel implements the stage's options on grid g (whatever its size).
 bool persistent_capable(synx_ctx* c, const GridInfo& g, bool profile) {
   if (profile || (c->P.flags & (SYNX_F_NO_PERSISTENT | SYNX_F_CC_FP32_SUMS | SYNX_F_FIELDS_FP16))) return false;
+  if (c->maskF || c->maskM) return false;  // metric masks run the per-kernel path
   if (c->P.total_variance > 0.0 || !(c->P.update_variance > 0.0)) return false;
   int rs = 1;
   for (int a = 0; a < c->D; ++a) rs = std::max(rs, c->R_upd[a]);
@@ -1381,6 +1393,8 @@ int synx_destroy(synx_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_arena(ctx);
+  if (ctx->maskF) cudaFree(ctx->maskF);
+  if (ctx->maskM) cudaFree(ctx->maskM);
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   for (auto e : ctx->lev_ev)
     if (e) cudaEventDestroy(e);
@@ -1429,6 +1443,38 @@ static int set_images_common(synx_ctx* c, const float* F, const synx_geom* gf, c
   c->log_inv.clear();
   CUDA_TRY(c, cudaGetLastError());
   return SYNX_OK;
+}
+
+int synx_set_masks(synx_ctx* c, const float* fixed_mask, const synx_geom* gfm, const float* moving_mask,
+                   const synx_geom* gmm) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  if ((fixed_mask && !check_geom(gfm, c->D)) || (moving_mask && !check_geom(gmm, c->D)))
+    return set_err(c, SYNX_E_ARG, "synx_set_masks: mask geometry does not match the stage dimension or is invalid");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  auto upload = [&](const float* m, const synx_geom* gm, unsigned char** dst, GridInfo* gi) -> int {
+    if (*dst) {
+      cudaFree(*dst);
+      *dst = nullptr;
+    }
+    if (!m) return SYNX_OK;
+    geom_to_grid(*gm, *gi);
+    const size_t n = (size_t)gi->d.N;
+    std::vector<unsigned char> b(n);
+    for (size_t i = 0; i < n; ++i) b[i] = m[i] != 0.0f ? 1 : 0;
+    cudaError_t e = cudaMalloc((void**)dst, n);
+    if (e != cudaSuccess) {
+      *dst = nullptr;
+      cudaGetLastError();
+      return set_err(c, SYNX_E_NOMEM, std::string("synx_set_masks: ") + cudaGetErrorString(e));
+    }
+    CUDA_TRY(c, cudaMemcpy(*dst, b.data(), n, cudaMemcpyHostToDevice));
+    return SYNX_OK;
+  };
+  int rc = upload(fixed_mask, gfm, &c->maskF, &c->gmF);
+  if (!rc) rc = upload(moving_mask, gmm, &c->maskM, &c->gmM);
+  drop_graphs(c);  // the iteration's launches change with the masks
+  return rc;
 }
 
 int synx_set_images(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm) {
@@ -1870,6 +1916,28 @@ int synx_field_affine_update(const float* u, const float* w, const synx_geom* g,
 int synx_cc_metric(const float* F, const float* M, const synx_geom* gg, int radius, float* gF, float* gM,
                    double* value, void* stream) {
   return synx_cc_metric_ex(F, M, gg, radius, 0, gF, gM, value, stream);
+}
+
+int synx_cc_metric_masked(const float* F, const float* M, const uint8_t* valid, const synx_geom* gg, int radius,
+                          float* gF, float* gM, double* value, void* stream) {
+  if (!F || !M || !valid || !gF || !gM || !gg || !check_geom(gg, gg->dim))
+    return set_err(nullptr, SYNX_E_ARG, "synx_cc_metric_masked: bad arguments");
+  if (!cc_radius_supported(gg->dim, radius))
+    return set_err(nullptr, SYNX_E_UNSUPPORTED, "synx_cc_metric_masked: radius");
+  cudaStream_t s = (cudaStream_t)stream;
+  GridInfo g;
+  geom_to_grid(*gg, g);
+  STEP_TRY(cc_prepare(gg->dim, radius));
+  TempCtl t;
+  STEP_TRY(t.alloc(2 * cc_blocks(g, radius)));  // block sums, then block counts
+  STEP_TRY(cudaMemsetAsync(t.ctl, 0, sizeof(IterCtl), s));
+  launch_cc(F, M, g, radius, gF, gM, t.part, t.ctl, s, nullptr, false, 0, valid);
+  IterCtl h;
+  STEP_TRY(cudaMemcpyAsync(&h, t.ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, s));
+  STEP_TRY(cudaStreamSynchronize(s));
+  if (value) *value = h.metric;
+  STEP_TRY(cudaGetLastError());
+  return SYNX_OK;
 }
 
 int synx_cc_metric_ex(const float* F, const float* M, const synx_geom* gg, int radius, int flags, float* gF, float* gM,

@@ -410,6 +410,49 @@ void launch_warp_image_nearest(const float* img, const GridInfo& gi, const float
     k_warp_image_nearest<2><<<m.grid, 256, 0, s>>>(img, gi.d, a, u, gv.d, m.zb, out);
 }
 
+// Metric-mask validity of the virtual voxels (antsRegistration -x [fixedMask,movingMask]): SyN
+// resamples each mask into the virtual domain through its image's inverse half-field, nearest
+// neighbour with 0 outside (ITK's NearestNeighborInterpolateImageFunction: the voxel at
+// floor(c + 0.5) inside the buffer), and a voxel is valid where both are nonzero.  A null mask
+// counts as inside everywhere.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_mask_validity(const unsigned char* __restrict__ mF, Dims dF, Affine aF,
+                                                       const float* __restrict__ psiF,
+                                                       const unsigned char* __restrict__ mM, Dims dM, Affine aM,
+                                                       const float* __restrict__ psiM, Dims dv, int zb,
+                                                       unsigned char* __restrict__ valid, IterCtl* ctl) {
+  if (ctl != nullptr && ctl->stop) return;
+  const Coord3 c = coord3(dv, zb, 1);
+  if (!c.ok) return;
+  const int N = (int)dv.N, nxy = dv.nx * dv.ny;
+  auto inside = [&](const unsigned char* m, const Dims& dm, const Affine& a, const float* u, int i, int z) -> bool {
+    if (m == nullptr) return true;
+    float cx, cy, cz;
+    map_point<DIM, false>(a, (float)c.x, (float)c.y, (float)z, u[i], u[N + i], DIM == 3 ? u[2 * N + i] : 0.0f, cx,
+                          cy, cz);
+    if (!inside_buffer<DIM>(dm, cx, cy, cz)) return false;
+    const int x = nearest_index(cx, dm.nx), y = nearest_index(cy, dm.ny);
+    const int zz = DIM == 3 ? nearest_index(cz, dm.nz) : 0;
+    return __ldg(m + (zz * dm.ny + y) * dm.nx + x) != 0;
+  };
+  for (int z = c.z0; z < c.z1; ++z) {
+    const int i = z * nxy + c.y * dv.nx + c.x;
+    valid[i] = (inside(mF, dF, aF, psiF, i, z) && inside(mM, dM, aM, psiM, i, z)) ? 1 : 0;
+  }
+}
+
+void launch_mask_validity(const unsigned char* mF, const GridInfo& gmF, const float* psiF, const unsigned char* mM,
+                          const GridInfo& gmM, const float* psiM, const GridInfo& gv, unsigned char* valid,
+                          IterCtl* ctl, cudaStream_t s) {
+  count_launch();
+  const Affine aF = make_affine(gv, gmF), aM = make_affine(gv, gmM);
+  const Map3 m = map3(gv.d);
+  if (gv.d.dim == 3)
+    k_mask_validity<3><<<m.grid, 256, 0, s>>>(mF, gmF.d, aF, psiF, mM, gmM.d, aM, psiM, gv.d, m.zb, valid, ctl);
+  else
+    k_mask_validity<2><<<m.grid, 256, 0, s>>>(mF, gmF.d, aF, psiF, mM, gmM.d, aM, psiM, gv.d, m.zb, valid, ctl);
+}
+
 // ------------------------------------------------------------------------------------------
 // Gaussian smoothing of displacement fields: an xy kernel (one block per tile, slice and field)
 // and, in 3-D, a z kernel (one thread per column chunk).  The SyN epilogue (boundary zeroing,

@@ -77,6 +77,11 @@ void launch_warp_image_nearest(const float* img, const GridInfo& gi, const float
                                cudaStream_t s);
 void launch_warp_image_label(const float* img, const GridInfo& gi, const float* u, const GridInfo& gv, float* out,
                              cudaStream_t s);
+// Metric-mask validity (one byte per voxel of gv): both masks, warped nearest-neighbour through
+// their half-fields, nonzero; a null mask is inside everywhere.
+void launch_mask_validity(const unsigned char* mF, const GridInfo& gmF, const float* psiF, const unsigned char* mM,
+                          const GridInfo& gmM, const float* psiM, const GridInfo& gv, unsigned char* valid,
+                          IterCtl* ctl, cudaStream_t s);
 void launch_field_affine_update(const float* u, const float* w, const double M[9], int dim, long long N, float* out,
                                 cudaStream_t s);
 
@@ -85,13 +90,15 @@ void launch_field_affine_update(const float* u, const float* w, const double M[9
 int cc_blocks(const GridInfo& g, int radius, int chunks = 0);
 // The most blocks any chunk count can give on g.
 int cc_blocks_max(const GridInfo& g, int radius);
-size_t cc_smem_bytes(int dim, int radius);
+size_t cc_smem_bytes(int dim, int radius, bool masked = false);
 bool cc_radius_supported(int dim, int radius);
 // Raise the dynamic shared-memory limit of the CC kernel (once per device, outside capture).
 cudaError_t cc_prepare(int dim, int radius);
 // fp32_sums: window sums and variance terms in float (the precision study's variant).
+// valid (metric masks): one byte per voxel, nonzero = valid; `partials` then needs twice the blocks.
 void launch_cc(const float* Ft, const float* Mt, const GridInfo& g, int radius, float* gF, float* gM, double* partials,
-               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr, bool fp32_sums = false, int chunks = 0);
+               IterCtl* ctl, cudaStream_t s, float* cc_out = nullptr, bool fp32_sums = false, int chunks = 0,
+               const unsigned char* valid = nullptr);
 // Round nf fields of n floats each to the nearest half-precision value, in place (the
 // precision study's FP16 field storage).
 void launch_round_half(float* const* f, int nf, long long n, cudaStream_t s);

@@ -223,6 +223,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_linear_field": (I, [P(SynxLinear), I, P(SynxGeom), V]),
         "synx_write_linear_transform": (I, [C.c_char_p, P(SynxLinear)]),
         "synx_initial_translation": (I, [V, P(SynxGeom), V, P(SynxGeom), I, P(SynxLinear)]),
+        "synx_set_masks": (I, [V, V, P(SynxGeom), V, P(SynxGeom)]),
+        "synx_cc_metric_masked": (I, [V, V, V, P(SynxGeom), I, V, V, P(D), V]),
         "synx_tuning_load": (I, [C.c_char_p]),
         "synx_tuning_path": (C.c_char_p, []),
         "synx_level_plan": (I, [V, I, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
@@ -525,6 +527,26 @@ class SyNStage:
     def _ck(self, rc):
         _check(rc, self.h)
 
+    def set_masks(self, fixed_mask=None, fixed_mask_geom: Geom | None = None, moving_mask=None,
+                  moving_mask_geom: Geom | None = None) -> None:
+        """Metric masks (antsRegistration -x): host arrays, nonzero = inside, on their own grids;
+        None for none.  They stay set across set_images calls."""
+        args = []
+        keep = []
+        for m, gm in ((fixed_mask, fixed_mask_geom), (moving_mask, moving_mask_geom)):
+            if m is None:
+                args += [None, None]
+                continue
+            if gm is None:
+                raise SynxError("a mask needs its geometry")
+            a = np.ascontiguousarray(m, dtype=np.float32)
+            if a.size != gm.count:
+                raise SynxError("mask size does not match its geometry")
+            gc = gm.to_c()
+            keep += [a, gc]
+            args += [_ptr(a), C.byref(gc)]
+        self._ck(self.lib.synx_set_masks(self.h, *args))
+
     def set_images(self, fixed, fixed_geom: Geom, moving, moving_geom: Geom, moving_initial=None) -> None:
         """Host numpy float32 arrays (copied host->device) or CUDA tensors (device->device).
         `moving_initial`: a LinearTransform or a list of them (first applied first), the
@@ -708,6 +730,21 @@ def cc_metric(F, M, g: Geom, radius: int, gF, gM, stream=None, fp32_sums: bool =
     _check(load_library().synx_cc_metric_ex(_dev(F, n, "F"), _dev(M, n, "M"), C.byref(gc), radius, flags,
                                             _dev(gF, g.dim * n, "gF"), _dev(gM, g.dim * n, "gM"),
                                             C.byref(v), _stream(stream)))
+    return v.value
+
+
+def cc_metric_masked(F, M, valid, g: Geom, radius: int, gF, gM, stream=None) -> float:
+    """CC over the valid voxels only; `valid` is a contiguous uint8 CUDA tensor (nonzero = valid)."""
+    if isinstance(valid, np.ndarray) or not getattr(valid, "is_cuda", False):
+        raise SynxError("valid: a CUDA tensor is required")
+    if str(valid.dtype) != "torch.uint8" or not valid.is_contiguous() or valid.numel() < g.count:
+        raise SynxError("valid: a contiguous uint8 tensor with one byte per voxel is required")
+    gc = g.to_c()
+    v = C.c_double()
+    n = g.count
+    _check(load_library().synx_cc_metric_masked(_dev(F, n, "F"), _dev(M, n, "M"), valid.data_ptr(), C.byref(gc),
+                                                radius, _dev(gF, g.dim * n, "gF"), _dev(gM, g.dim * n, "gM"),
+                                                C.byref(v), _stream(stream)))
     return v.value
 
 

@@ -293,6 +293,15 @@ int synx_warp_image_label(const float* img_dev, const synx_geom* img_geom, const
 int synx_histogram_match(const float* src_dev, int64_t n_src, const float* ref_dev, int64_t n_ref, int32_t levels,
                          int32_t match_points, int32_t threshold_at_mean, float* out_dev, void* stream);
 
+/* Metric masks of the stage (antsRegistration -x [fixedMask,movingMask], Examples/antsRegistration.cxx:
+ * 471-480, set on the metric at Examples/itkantsRegistrationHelper.hxx:863-890, :1159-1166): host
+ * arrays on their own grids, nonzero = inside; NULL for none (both NULL clears them).  Each mask is
+ * resampled into the virtual domain through its image's inverse half-field (nearest neighbour, 0
+ * outside) every iteration; CC sums, counts, values and updates then cover only the voxels inside
+ * both.  Masks stay set across synx_set_images; a masked stage runs the per-kernel path. */
+int synx_set_masks(synx_ctx* ctx, const float* fixed_mask, const synx_geom* fixed_mask_geom,
+                   const float* moving_mask, const synx_geom* moving_mask_geom);
+
 /* Tile plans chosen by the project's autotuner (python -m ants_b200.autotune): a text table of
  * measured winners per level grid, one line per (dim, nx, ny, nz, CC radius, smoothing radius) with
  * the chosen persistent-kernel use, smoothing tile rows and CC z chunks.  Loaded once per process at
@@ -313,6 +322,12 @@ int synx_level_plan(synx_ctx* ctx, int level, int32_t* persistent, int32_t* smoo
  * ImageRegistration/itkCrossCorrelationRegistrationFunction.cxx:179-504). */
 int synx_cc_metric(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
                    float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
+/* CC over the valid voxels only: valid_dev holds one byte per voxel (nonzero = valid, as the
+ * metric masks make it); invalid voxels add nothing to the window sums or counts and get no
+ * value and zero updates; the value is -mean cc over the valid voxels. */
+int synx_cc_metric_masked(const float* fixed_dev, const float* moving_dev, const uint8_t* valid_dev,
+                          const synx_geom* g, int radius, float* grad_fixed_dev, float* grad_moving_dev,
+                          double* value_host, void* stream);
 /* Same with flags: SYNX_F_CC_FP32_SUMS selects float window sums (precision study). */
 int synx_cc_metric_ex(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius, int flags,
                       float* grad_fixed_dev, float* grad_moving_dev, double* value, void* cuda_stream);

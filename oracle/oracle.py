@@ -64,6 +64,9 @@ def load() -> C.CDLL:
             f"oracle_warp_image_nearest_{suf}": (None, [V, P(G), V, P(G), V]),
             f"oracle_warp_image_label_{suf}": (None, [V, P(G), V, P(G), V]),
             f"oracle_cc_{suf}": (D, [V, V, P(G), I, V, V, V]),
+            f"oracle_cc_masked_{suf}": (D, [V, V, P(G), I, V, V, V, V]),
+            f"oracle_syn_register_masked_{suf}": (I, [V, P(G), V, P(G), P(Pm), V, P(G), V, P(G), V, V, P(G), V, V,
+                                                        V, V, V, I]),
             f"oracle_smooth_field_{suf}": (None, [V, V, P(G), D]),
             f"oracle_scale_update_{suf}": (D, [V, P(G), D]),
             f"oracle_compose_{suf}": (None, [V, V, P(G), V, D]),
@@ -159,14 +162,20 @@ def warp_image(img, gi, u, gv, dtype=np.float32, nearest=False, label=False):
     return out
 
 
-def cc_metric(F, M, g, radius, dtype=np.float32):
-    """Returns (value, grad_fixed_update, grad_moving_update, local_cc)."""
+def cc_metric(F, M, g, radius, dtype=np.float32, valid=None):
+    """Returns (value, grad_fixed_update, grad_moving_update, local_cc).  `valid` (bool per voxel):
+    the metric masks' validity; invalid voxels are left out of the window sums and get no value."""
     f, m = _c(F, dtype), _c(M, dtype)
     gF = np.empty((g.dim,) + g.shape, dtype)
     gM = np.empty_like(gF)
     cc = np.empty(g.shape, dtype)
     gc = g.to_c()
-    v = getattr(load(), f"oracle_cc_{_suf(dtype)}")(_p(f), _p(m), C.byref(gc), radius, _p(gF), _p(gM), _p(cc))
+    if valid is None:
+        v = getattr(load(), f"oracle_cc_{_suf(dtype)}")(_p(f), _p(m), C.byref(gc), radius, _p(gF), _p(gM), _p(cc))
+    else:
+        vb = np.ascontiguousarray(valid, dtype=np.uint8)
+        v = getattr(load(), f"oracle_cc_masked_{_suf(dtype)}")(_p(f), _p(m), C.byref(gc), radius, _p(vb), _p(gF),
+                                                               _p(gM), _p(cc))
     return v, gF, gM, cc
 
 
@@ -222,8 +231,10 @@ def syn_iteration(Fs, gF, Ms, gM, params, g, phiF, psiF, phiM, psiM, dtype=np.fl
     return v, flds, k.value
 
 
-def syn_register(F, gF, M, gM, params, dtype=np.float32):
-    """Full stage: returns (forward, inverse, out_geom, log) with fields as component planes."""
+def syn_register(F, gF, M, gM, params, dtype=np.float32, fixed_mask=None, fixed_mask_geom=None, moving_mask=None,
+                 moving_mask_geom=None):
+    """Full stage: returns (forward, inverse, out_geom, log) with fields as component planes.  Metric
+    masks (nonzero = inside) on their own grids (default: the image's grid) are optional."""
     from ants_b200.synx import Geom, SynxGeom
     f, m = _c(F, dtype), _c(M, dtype)
     g_last = gF
@@ -240,9 +251,20 @@ def syn_register(F, gF, M, gM, params, dtype=np.float32):
     go = SynxGeom()
     pc = params.to_c()
     ga, gb = gF.to_c(), gM.to_c()
-    n = getattr(load(), f"oracle_syn_register_{_suf(dtype)}")(_p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc),
-                                                              _p(fwd), _p(inv), C.byref(go), _p(lv), _p(it), _p(me),
-                                                              _p(cv), _p(ki), cap)
+    if fixed_mask is None and moving_mask is None:
+        n = getattr(load(), f"oracle_syn_register_{_suf(dtype)}")(_p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc),
+                                                                  _p(fwd), _p(inv), C.byref(go), _p(lv), _p(it),
+                                                                  _p(me), _p(cv), _p(ki), cap)
+    else:
+        mf = _c(fixed_mask, dtype) if fixed_mask is not None else None
+        mm = _c(moving_mask, dtype) if moving_mask is not None else None
+        gmf = (fixed_mask_geom or gF).to_c() if mf is not None else None
+        gmm = (moving_mask_geom or gM).to_c() if mm is not None else None
+        n = getattr(load(), f"oracle_syn_register_masked_{_suf(dtype)}")(
+            _p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc), _p(mf) if mf is not None else None,
+            C.byref(gmf) if gmf is not None else None, _p(mm) if mm is not None else None,
+            C.byref(gmm) if gmm is not None else None, _p(fwd), _p(inv), C.byref(go), _p(lv), _p(it), _p(me),
+            _p(cv), _p(ki), cap)
     log = [dict(level=int(lv[i]), iteration=int(it[i]), metric=float(me[i]), convergence=float(cv[i]),
                 inverse_iterations=int(ki[i])) for i in range(min(n, cap))]
     return fwd, inv, Geom.from_c(go), log

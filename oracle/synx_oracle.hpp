@@ -512,6 +512,13 @@ inline void warp_image_label(const T* img, const Geom& gi, const T* u, const Geo
 //     SyN evaluates it once per half with the roles swapped (fixed-to-middle update uses
 //     grad of the warped moving image, moving-to-middle uses grad of the warped fixed image);
 //   * value = -mean(cc) over the grid.
+// Metric masks (antsRegistration -x [fixedMask,movingMask], Examples/antsRegistration.cxx:471-480,
+// set on the metric at Examples/itkantsRegistrationHelper.hxx:1159-1166): SyN resamples each mask
+// into the virtual domain through the same half-field as its image, nearest-neighbour with 0
+// outside, and a virtual voxel is valid where both warped masks are nonzero.  Invalid voxels add
+// nothing to the window sums or to n (the count of valid voxels in the window, ITK's Qcount), and
+// an invalid centre has no cc and no derivative; the value is -mean(cc) over the valid centres.
+// (ITK's mask handling in SyN and in the metric's scan is restated as recalled: unpinned.)
 // grad: ITK CentralDifferenceImageFunction at grid points, i.e. (I(x+h/2) - I(x-h/2)) / h with
 // linear interpolation and the buffer rule above: (I[x+1]-I[x-1])/(2h) inside, 0.5(I[1]-I[0])/h
 // at index 0 (x-h/2 lies on the buffer rim), 0 at the last index (x+h/2 is outside), then
@@ -537,23 +544,28 @@ inline double grad_axis(const T* I, const Geom& g, int64_t x, int64_t y, int64_t
 
 template <class T>
 inline CCResult cc_metric(const T* F, const T* M, const Geom& g, int r, T* gradF_upd, T* gradM_upd,
-                          T* cc_out = nullptr, double eps = 1.1920928955078125e-07) {
+                          T* cc_out = nullptr, double eps = 1.1920928955078125e-07,
+                          const unsigned char* valid = nullptr) {
   const int64_t nx = g.n[0], ny = g.n[1], nz = g.n[2], N = g.count();
   const int rz = g.dim == 3 ? r : 0;
-  // separable running box sums in double: 5 quantities
-  std::vector<double> q[5], t[5];
-  for (int k = 0; k < 5; ++k) {
+  // separable running box sums in double: 5 quantities, and with metric masks a sixth, the number
+  // of valid voxels in the window (invalid voxels add nothing to any sum)
+  const int NQ = valid ? 6 : 5;
+  std::vector<double> q[6], t[6];
+  for (int k = 0; k < NQ; ++k) {
     q[k].resize(N);
     t[k].resize(N);
   }
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < N; ++i) {
-    double f = (double)F[i], m = (double)M[i];
+    const double v = valid ? (valid[i] ? 1.0 : 0.0) : 1.0;
+    double f = v != 0.0 ? (double)F[i] : 0.0, m = v != 0.0 ? (double)M[i] : 0.0;
     q[0][i] = f;
     q[1][i] = m;
     q[2][i] = f * f;
     q[3][i] = m * m;
     q[4][i] = f * m;
+    if (valid) q[5][i] = v;
   }
   auto box_axis = [&](std::vector<double>* src, std::vector<double>* dst, int axis, int rad) {
     const int64_t stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
@@ -566,7 +578,7 @@ inline CCResult cc_metric(const T* F, const T* M, const Geom& g, int r, T* gradF
           int64_t base = z * nx * ny + y * nx + x;
           int64_t line0 = base - pos * stride;
           int64_t lo = std::max<int64_t>(pos - rad, 0), hi = std::min<int64_t>(pos + rad, len - 1);
-          for (int k = 0; k < 5; ++k) {
+          for (int k = 0; k < NQ; ++k) {
             double s = 0.0;
             for (int64_t j = lo; j <= hi; ++j) s += src[k][line0 + j * stride];
             dst[k][base] = s;
@@ -579,16 +591,24 @@ inline CCResult cc_metric(const T* F, const T* M, const Geom& g, int r, T* gradF
   std::vector<double>* S = g.dim == 3 ? t : q;
   double sum_cc = 0.0;
   std::vector<double> slice_cc(nz, 0.0);
+  std::vector<int64_t> slice_n(nz, 0);
 #pragma omp parallel for schedule(static)
   for (int64_t z = 0; z < nz; ++z) {
     double acc = 0.0;
+    int64_t cnt = 0;
     for (int64_t y = 0; y < ny; ++y)
       for (int64_t x = 0; x < nx; ++x) {
         int64_t i = z * nx * ny + y * nx + x;
+        if (valid && !valid[i]) {  // a masked-out voxel: no value, no update
+          if (cc_out) cc_out[i] = (T)0;
+          for (int d = 0; d < g.dim; ++d) gradF_upd[d * N + i] = gradM_upd[d * N + i] = (T)0;
+          continue;
+        }
+        ++cnt;
         double cx = (double)(std::min<int64_t>(x + r, nx - 1) - std::max<int64_t>(x - r, 0) + 1);
         double cy = (double)(std::min<int64_t>(y + r, ny - 1) - std::max<int64_t>(y - r, 0) + 1);
         double cz = (double)(std::min<int64_t>(z + rz, nz - 1) - std::max<int64_t>(z - rz, 0) + 1);
-        double n = cx * cy * cz;
+        double n = valid ? S[5][i] : cx * cy * cz;
         double sF = S[0][i], sM = S[1][i], sFF2 = S[2][i], sMM2 = S[3][i], sFM2 = S[4][i];
         double mF = sF / n, mM = sM / n;
         double sFF = sFF2 - mF * sF - mF * sF + n * mF * mF;
@@ -623,9 +643,14 @@ inline CCResult cc_metric(const T* F, const T* M, const Geom& g, int r, T* gradF
         }
       }
     slice_cc[z] = acc;
+    slice_n[z] = cnt;
   }
-  for (int64_t z = 0; z < nz; ++z) sum_cc += slice_cc[z];
-  return CCResult{-sum_cc / (double)N, sum_cc};
+  int64_t n_valid = 0;
+  for (int64_t z = 0; z < nz; ++z) {
+    sum_cc += slice_cc[z];
+    n_valid += slice_n[z];
+  }
+  return CCResult{n_valid > 0 ? -sum_cc / (double)n_valid : 0.0, sum_cc};
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1050,7 +1075,29 @@ template <class T>
 struct SynState {
   Geom g;  // current level grid
   std::vector<T> phiF, psiF, phiM, psiM;
+  // metric masks on their own grids (nonzero = inside), or null
+  const T* maskF = nullptr;
+  const T* maskM = nullptr;
+  Geom gmF, gmM;
 };
+
+// Validity of the virtual voxels under the metric masks: both masks, warped nearest-neighbour
+// through the half-fields (fixed mask at x + psiF(x), moving mask at x + psiM(x)), nonzero.
+template <class T>
+inline void mask_validity(const SynState<T>& S, std::vector<unsigned char>& valid) {
+  const Geom& g = S.g;
+  const int64_t N = g.count();
+  valid.assign(N, 1);
+  std::vector<T> w(N);
+  if (S.maskF) {
+    warp_image_nearest(S.maskF, S.gmF, S.psiF.data(), g, w.data());
+    for (int64_t i = 0; i < N; ++i) valid[i] = valid[i] && w[i] != (T)0;
+  }
+  if (S.maskM) {
+    warp_image_nearest(S.maskM, S.gmM, S.psiM.data(), g, w.data());
+    for (int64_t i = 0; i < N; ++i) valid[i] = valid[i] && w[i] != (T)0;
+  }
+}
 
 template <class T>
 inline void syn_iteration(const T* Fs, const Geom& gF, const T* Ms, const Geom& gM, const SynParams& P,
@@ -1061,8 +1108,11 @@ inline void syn_iteration(const T* Fs, const Geom& gF, const T* Ms, const Geom& 
   std::vector<T> Ft(N), Mt(N), uF((size_t)N * D), uM((size_t)N * D), sF((size_t)N * D), sM((size_t)N * D);
   warp_image(Fs, gF, S.psiF.data(), g, Ft.data());
   warp_image(Ms, gM, S.psiM.data(), g, Mt.data());
+  std::vector<unsigned char> valid;
+  if (S.maskF || S.maskM) mask_validity(S, valid);
   CCResult r = cc_metric(Ft.data(), Mt.data(), g, P.radius, uF.data(), uM.data(),
-                         scratch_cc ? scratch_cc->data() : nullptr);
+                         scratch_cc ? scratch_cc->data() : nullptr, 1.1920928955078125e-07,
+                         valid.empty() ? nullptr : valid.data());
   smooth_field(uF.data(), sF.data(), g, P.var_update);
   smooth_field(uM.data(), sM.data(), g, P.var_update);
   scale_update(sF.data(), g, P.eta);
@@ -1108,6 +1158,22 @@ struct SynRun {
   SynLog log;
   std::vector<int64_t> level_voxels;
   std::vector<double> level_seconds;
+
+  std::vector<T> maskF, maskM;
+
+  // Metric masks (nonzero = inside) on their own grids; null for none.  Call before advancing.
+  void set_masks(const T* mF, const Geom* gmF, const T* mM, const Geom* gmM) {
+    if (mF && gmF) {
+      maskF.assign(mF, mF + gmF->count());
+      S.maskF = maskF.data();
+      S.gmF = *gmF;
+    }
+    if (mM && gmM) {
+      maskM.assign(mM, mM + gmM->count());
+      S.maskM = maskM.data();
+      S.gmM = *gmM;
+    }
+  }
 
   SynRun(const T* F_in, const Geom& gF_, const T* M_in, const Geom& gM_, const SynParams& P_)
       : P(P_), gF(gF_), gM(gM_) {
@@ -1210,8 +1276,11 @@ struct SynRun {
 
 template <class T>
 inline void syn_register(const T* F_in, const Geom& gF, const T* M_in, const Geom& gM, const SynParams& P,
-                         std::vector<T>& fwd, std::vector<T>& inv, Geom& gOut, SynLog* log = nullptr) {
+                         std::vector<T>& fwd, std::vector<T>& inv, Geom& gOut, SynLog* log = nullptr,
+                         const T* maskF = nullptr, const Geom* gmF = nullptr, const T* maskM = nullptr,
+                         const Geom* gmM = nullptr) {
   SynRun<T> R(F_in, gF, M_in, gM, P);
+  R.set_masks(maskF, gmF, maskM, gmM);
   while (!R.done) R.advance(INT64_MAX);
   fwd.swap(R.fwd);
   inv.swap(R.inv);

@@ -122,6 +122,11 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
   double oracle_cc_##SUF(const T* F, const T* M, const synx_geom* g, int r, T* gF, T* gM, T* cc) {   \
     return cc_metric(F, M, to_geom(g), r, gF, gM, cc).value;                                         \
   }                                                                                                  \
+  /* CC over the valid voxels only (valid: one byte per voxel, nonzero = valid). */                  \
+  double oracle_cc_masked_##SUF(const T* F, const T* M, const synx_geom* g, int r,                   \
+                                const unsigned char* valid, T* gF, T* gM, T* cc) {                   \
+    return cc_metric(F, M, to_geom(g), r, gF, gM, cc, 1.1920928955078125e-07, valid).value;          \
+  }                                                                                                  \
   void oracle_smooth_field_##SUF(const T* in, T* out, const synx_geom* g, double var) {              \
     smooth_field(in, out, to_geom(g), var);                                                          \
   }                                                                                                  \
@@ -160,15 +165,36 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
   }                                                                                                  \
   /* Full stage.  fwd/inv must hold the last level grid (query it with oracle_shrink_geom);       \
      log arrays hold log_cap records; returns the number of records. */                             \
+  int oracle_syn_register_masked_##SUF(const T* F, const synx_geom* gF, const T* M, const synx_geom* gM, \
+                                       const synx_params* p, const T* maskF, const synx_geom* gmF,   \
+                                       const T* maskM, const synx_geom* gmM, T* fwd, T* inv,         \
+                                       synx_geom* gout, int32_t* log_level, int32_t* log_iter,       \
+                                       double* log_metric, double* log_conv, int32_t* log_inv,       \
+                                       int log_cap);                                                 \
   int oracle_syn_register_##SUF(const T* F, const synx_geom* gF, const T* M, const synx_geom* gM,    \
                                 const synx_params* p, T* fwd, T* inv, synx_geom* gout,               \
                                 int32_t* log_level, int32_t* log_iter, double* log_metric,           \
                                 double* log_conv, int32_t* log_inv, int log_cap) {                   \
+    return oracle_syn_register_masked_##SUF(F, gF, M, gM, p, nullptr, nullptr, nullptr, nullptr, fwd,   \
+                                            inv, gout, log_level, log_iter, log_metric, log_conv,    \
+                                            log_inv, log_cap);                                       \
+  }                                                                                                  \
+  /* The same with metric masks (null for none), each on its own grid. */                           \
+  int oracle_syn_register_masked_##SUF(const T* F, const synx_geom* gF, const T* M, const synx_geom* gM, \
+                                       const synx_params* p, const T* maskF, const synx_geom* gmF,   \
+                                       const T* maskM, const synx_geom* gmM, T* fwd, T* inv,         \
+                                       synx_geom* gout, int32_t* log_level, int32_t* log_iter,       \
+                                       double* log_metric, double* log_conv, int32_t* log_inv,       \
+                                       int log_cap) {                                                \
     SynParams P = to_params(p);                                                                      \
     std::vector<T> f, v;                                                                             \
     Geom go;                                                                                         \
     SynLog L;                                                                                        \
-    syn_register(F, to_geom(gF), M, to_geom(gM), P, f, v, go, &L);                                   \
+    Geom a, b;                                                                                       \
+    if (gmF) a = to_geom(gmF);                                                                       \
+    if (gmM) b = to_geom(gmM);                                                                       \
+    syn_register(F, to_geom(gF), M, to_geom(gM), P, f, v, go, &L, maskF, gmF ? &a : nullptr, maskM,  \
+                 gmM ? &b : nullptr);                                                                \
     std::copy(f.begin(), f.end(), fwd);                                                              \
     std::copy(v.begin(), v.end(), inv);                                                              \
     from_geom(go, gout);                                                                             \

@@ -7,13 +7,17 @@
 #include <string>
 #include <vector>
 #include "synx.h"
-extern "C" int oracle_syn_register_f32(const float*, const synx_geom*, const float*, const synx_geom*, const synx_params*,
-                                       float*, float*, synx_geom*, int32_t*, int32_t*, double*, double*, int32_t*, int);
+extern "C" int oracle_syn_register_masked_f32(const float*, const synx_geom*, const float*, const synx_geom*,
+                                              const synx_params*, const float*, const synx_geom*, const float*,
+                                              const synx_geom*, float*, float*, synx_geom*, int32_t*, int32_t*,
+                                              double*, double*, int32_t*, int);
 extern "C" void oracle_shrink_geom(const synx_geom*, unsigned, synx_geom*);
 struct synx_ctx {
   synx_params p;
   std::vector<float> F, M, fwd, inv;
   synx_geom gf, gm, go;
+  std::vector<float> mF, mM;  // metric masks (empty: none)
+  synx_geom gmF, gmM;
   std::vector<int32_t> lv, it, ki;
   std::vector<double> me, cv;
   bool done = false;
@@ -47,6 +51,13 @@ int synx_set_images(synx_ctx* c, const float* F, const synx_geom* gf, const floa
   c->level = 0;
   return 0;
 }
+int synx_set_masks(synx_ctx* c, const float* mf, const synx_geom* gmf, const float* mm, const synx_geom* gmm) {
+  c->mF.clear();
+  c->mM.clear();
+  if (mf) { c->gmF = *gmf; c->mF.assign(mf, mf + gmf->size[0] * gmf->size[1] * gmf->size[2]); }
+  if (mm) { c->gmM = *gmm; c->mM.assign(mm, mm + gmm->size[0] * gmm->size[1] * gmm->size[2]); }
+  return 0;
+}
 int synx_run_level(synx_ctx* c, int level) {
   if (c->done || level != c->p.n_levels - 1) return 0;  // the whole stage runs at the last level
   synx_geom go;
@@ -55,8 +66,11 @@ int synx_run_level(synx_ctx* c, int level) {
   std::vector<float> f(N * D), v(N * D);
   const int cap = 100000;
   c->lv.resize(cap); c->it.resize(cap); c->ki.resize(cap); c->me.resize(cap); c->cv.resize(cap);
-  int n = oracle_syn_register_f32(c->F.data(), &c->gf, c->M.data(), &c->gm, &c->p, f.data(), v.data(), &c->go,
-                                  c->lv.data(), c->it.data(), c->me.data(), c->cv.data(), c->ki.data(), cap);
+  int n = oracle_syn_register_masked_f32(c->F.data(), &c->gf, c->M.data(), &c->gm, &c->p,
+                                         c->mF.empty() ? nullptr : c->mF.data(), c->mF.empty() ? nullptr : &c->gmF,
+                                         c->mM.empty() ? nullptr : c->mM.data(), c->mM.empty() ? nullptr : &c->gmM,
+                                         f.data(), v.data(), &c->go, c->lv.data(), c->it.data(), c->me.data(),
+                                         c->cv.data(), c->ki.data(), cap);
   for (auto* a : {&c->lv, &c->it, &c->ki}) a->resize(n);
   c->me.resize(n); c->cv.resize(n);
   c->fwd.resize(N * D); c->inv.resize(N * D);

@@ -87,6 +87,46 @@ def cc_bruteforce(F: np.ndarray, M: np.ndarray, r: int, spacing: tuple, eps: flo
     return -ccs.mean(), gF, gM, ccs
 
 
+def cc_bruteforce_masked(F: np.ndarray, M: np.ndarray, valid: np.ndarray, r: int, spacing: tuple,
+                         eps: float = 1.1920928955078125e-07):
+    """The same over the valid voxels only: invalid voxels are left out of every window sum and of the
+    count n, and an invalid centre has no cc and no derivative; value = -mean cc over valid centres."""
+    d = F.ndim
+    gF = np.zeros((d,) + F.shape)
+    gM = np.zeros((d,) + F.shape)
+    ccs = np.zeros(F.shape)
+    total, count = 0.0, 0
+    for idx in np.ndindex(F.shape):
+        if not valid[idx]:
+            continue
+        sl = tuple(slice(max(i - r, 0), min(i + r, n - 1) + 1) for i, n in zip(idx, F.shape))
+        keep = valid[sl].ravel().astype(bool)
+        f = F[sl].astype(np.float64).ravel()[keep]
+        m = M[sl].astype(np.float64).ravel()[keep]
+        n = f.size
+        sF, sM = f.sum(), m.sum()
+        mF, mM = sF / n, sM / n
+        sFF = (f * f).sum() - 2 * mF * sF + n * mF * mF
+        sMM = (m * m).sum() - 2 * mM * sM + n * mM * mM
+        sFM = (f * m).sum() - mM * sF - mF * sM + n * mM * mF
+        fh = float(F[idx]) - mF
+        mh = float(M[idx]) - mM
+        cc, aF, aM = 1.0, 0.0, 0.0
+        if sFF > eps and sMM > eps:
+            cc = sFM * sFM / (sFF * sMM)
+            coef = 2 * sFM / (sFF * sMM)
+            aF = coef * (fh - sFM / sMM * mh)
+            aM = coef * (mh - sFM / sFF * fh)
+        ccs[idx] = cc
+        total += cc
+        count += 1
+        for comp in range(d):
+            ax = d - 1 - comp
+            gF[comp][idx] = aF * grad_axis(M, idx, ax, spacing[comp])
+            gM[comp][idx] = aM * grad_axis(F, idx, ax, spacing[comp])
+    return (-total / count if count else 0.0), gF, gM, ccs
+
+
 def main() -> None:
     kernels = []
     for var in (0.25, 0.5, 1.0, 2.0, 3.0, 4.5, 9.0):

@@ -46,7 +46,7 @@ def test_nifti_roundtrip_scalar_and_vector(tmp_path):
      "must match the levels"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-f", "1", "-s", "0", "-o", "x"], "no convergence"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
-      "-x", "[mask.nii.gz]"], "not supported"),
+      "--restore-state", "state.h5"], "not supported"),
     (["-d", "4", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x"],
      "dimensionality"),
     (["-d", "3", "-m", "CC[/nonexistent/f.nii.gz,/nonexistent/m.nii.gz,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10",

@@ -97,3 +97,17 @@ def test_histogram_matching(host_cli, tmp_path):
         return np.moveaxis(fwd, 0, -1), np.moveaxis(inv, 0, -1)
 
     H.check_cli_histogram_matching(host_cli["reg"], tmp_path, stage_fields)
+
+
+def test_masks(host_cli, tmp_path):
+    import numpy as np
+
+    import oracle as O
+    import test_zz_t_masks as X
+
+    def stage_fields(f, gf, m, gm, P, mf, mm):
+        fwd, inv, _, _ = O.syn_register(f, gf, m, gm, P, fixed_mask=mf, fixed_mask_geom=gf, moving_mask=mm,
+                                        moving_mask_geom=gm)
+        return np.moveaxis(fwd, 0, -1), np.moveaxis(inv, 0, -1)
+
+    X.check_cli_masks(host_cli["reg"], tmp_path, stage_fields)

@@ -76,6 +76,14 @@ def test_cc_identical_images_is_minus_one():
     assert np.abs(gF).max() < 1e-5 and np.abs(gM).max() < 1e-5
 
 
+def _golden_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def _bruteforce():
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
@@ -470,3 +478,35 @@ def test_pyramid_smoothing_matches_a_restatement(mm):
             out += kj * padded[tuple(sl)]
         want = out
     np.testing.assert_allclose(got, want, atol=1e-12)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("shape,r,sp", [((6, 7, 8), 2, (1.0, 1.2, 0.8)), ((9, 11), 1, (1.0, 0.7))])
+def test_masked_cc_matches_bruteforce(dtype, shape, r, sp):
+    # metric masks: the window sums and counts over valid voxels only (a blob of invalid voxels, and a
+    # ragged rim)
+    rng = np.random.default_rng(17)
+    F = rng.uniform(0, 1, shape).astype(np.float32)
+    M = (0.7 * np.roll(F, 1, axis=-1) + 0.2 * rng.uniform(0, 1, shape)).astype(np.float32)
+    valid = rng.uniform(0, 1, shape) > 0.3
+    valid[(slice(0, 2),) * len(shape)] = False
+    g = Geom(tuple(reversed(shape)), sp[: len(shape)])
+    v, gF, gM, cc = O.cc_metric(F, M, g, r, dtype=dtype, valid=valid)
+    bv, bgF, bgM, bcc = _golden_module().cc_bruteforce_masked(F, M, valid, r, sp[: len(shape)])
+    tol = 1e-12 if dtype == np.float64 else 2e-6
+    assert abs(v - bv) < max(tol, 1e-12)
+    np.testing.assert_allclose(np.where(valid, cc, 0), bcc, atol=tol * 10)
+    np.testing.assert_allclose(gF, bgF, atol=tol * 10)
+    np.testing.assert_allclose(gM, bgM, atol=tol * 10)
+
+
+def test_all_valid_mask_is_the_unmasked_metric():
+    rng = np.random.default_rng(18)
+    F = rng.uniform(0, 1, (8, 9, 10)).astype(np.float32)
+    M = rng.uniform(0, 1, (8, 9, 10)).astype(np.float32)
+    g = Geom((10, 9, 8))
+    a = O.cc_metric(F, M, g, 2)
+    b = O.cc_metric(F, M, g, 2, valid=np.ones(F.shape, bool))
+    assert a[0] == b[0]
+    for x, y in zip(a[1:], b[1:]):
+        np.testing.assert_array_equal(x, y)
