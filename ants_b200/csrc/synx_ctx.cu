@@ -214,6 +214,7 @@ struct synx_ctx {
   unsigned char* maskM = nullptr;
   GridInfo gmF{}, gmM{};
   unsigned char* valid = nullptr;
+  int* inv_list[2] = {nullptr, nullptr};  // deferred voxels of the single-pass inverse, per half
   // canonical buffer assignment (level changes swap field and work buffers)
   float* canon[8] = {};
   // graphs: one executable per level, valid while the arena and grids are unchanged
@@ -283,7 +284,7 @@ long long level_inv_units(const GridInfo& g);
 
 // Byte offsets of everything a context keeps on the device, for its images and schedule.
 struct ArenaPlan {
-  size_t F0, M0, Fs, Ms, Tmp, Field[4], Ft, Mt, Work[6], CC, IS, IM, Cu, Ct, Ci, Ctl, Lm, Lc, Li, H, V;
+  size_t F0, M0, Fs, Ms, Tmp, Field[4], Ft, Mt, Work[6], CC, IS, IM, Cu, Ct, Ci, Ctl, Lm, Lc, Li, H, V, IL[2];
   size_t total;
   int ccb, invb, coeff_cap, max_iters;
 };
@@ -320,6 +321,8 @@ ArenaPlan arena_plan(const synx_ctx* c) {
   a.Lm = add(8 * (size_t)max_iters), a.Lc = add(8 * (size_t)max_iters), a.Li = add(4 * (size_t)max_iters);
   a.H = add(std::max((size_t)4 * 258, hm_scratch_bytes(256)));
   a.V = add((size_t)Nmax);  // metric-mask validity, one byte per voxel of the largest level
+  // the single-pass inverse's deferred-voxel lists, one per half, room for every voxel
+  for (int k = 0; k < 2; ++k) a.IL[k] = add(4 * (size_t)Nmax);
   a.total = sz;
   a.ccb = ccb;
   a.invb = invb;
@@ -384,6 +387,7 @@ int allocate(synx_ctx* c) {
   c->logdev.cap = max_iters;
   c->hist = (unsigned*)(a + oH);
   c->valid = (unsigned char*)(a + pl.V);
+  for (int k = 0; k < 2; ++k) c->inv_list[k] = (int*)(a + pl.IL[k]);
   CUDA_TRY(c, cudaMemsetAsync(c->ctl, 0, sizeof(IterCtl), c->stream));
   return SYNX_OK;
 }
@@ -691,13 +695,29 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
   int e1 = profile ? ev() : -1;
   // the CC derivative buffers are free until the next iteration: they carry the inverse residual
   float* ecache[2] = {c->gFu, c->gMu};
+  // single-pass form (one streaming pass per sub-iteration plus a short pass over the deferred
+  // voxels) unless the stage asks for the two-pass form; both give the same bits
+  const bool single = (c->P.flags & SYNX_F_INV_TWO_PASS) == 0;
+  int* lists[2] = {c->inv_list[0], c->inv_list[1]};
   auto inversion = [&](int phase, const float* const* phi, float* const* psi) -> cudaError_t {
     const double mt = c->P.inv_mean_tol, xt = c->P.inv_max_tol;
+    auto sub = [&](int k, cudaStream_t st) {
+      if (single) {
+        launch_invert_spec(phi, psi, 2, g, k, mi, mt, xt, c->ctl, phase, pb, st, true, ecache, lists);
+        launch_invert_fix(phi, psi, 2, g, k, mi, c->ctl, phase, st, true, ecache, lists);
+      } else {
+        launch_invert_step(phi, psi, 2, g, k, mi, mt, xt, c->ctl, phase, pb, st, true, ecache);
+      }
+    };
+    auto control = [&](cudaGraphConditionalHandle h, bool init, cudaStream_t st) {
+      if (single) launch_inv_spec_control(c->ctl, phase, h, mi, init, st);
+      else launch_inv_loop_control(c->ctl, phase, h, mi, init, st);
+    };
     if (!loops) {
-      for (int k = 0; k <= mi; ++k) launch_invert_step(phi, psi, 2, g, k, mi, mt, xt, c->ctl, phase, pb, s, true, ecache);
+      for (int k = 0; k < (single ? mi : mi + 1); ++k) sub(k, s);
       return cudaSuccess;
     }
-    launch_invert_step(phi, psi, 2, g, 0, mi, mt, xt, c->ctl, phase, pb, s, true, ecache);
+    sub(0, s);
     cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
     cudaGraph_t cg = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -707,7 +727,7 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
     if (st != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
     cudaGraphConditionalHandle h = 0;
     if ((e = cudaGraphConditionalHandleCreate(&h, cg, 0, 0)) != cudaSuccess) return e;
-    launch_inv_loop_control(c->ctl, phase, h, mi, true, s);
+    control(h, true, s);
     if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd)) != cudaSuccess) return e;
     cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
     np.conditional.handle = h;
@@ -720,8 +740,8 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
     if ((e = cudaStreamBeginCaptureToGraph(c->aux, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                            cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return e;
-    launch_invert_step(phi, psi, 2, g, -1, mi, mt, xt, c->ctl, phase, pb, c->aux, true, ecache);
-    launch_inv_loop_control(c->ctl, phase, h, mi, false, c->aux);
+    sub(-1, c->aux);
+    control(h, false, c->aux);
     cudaGraph_t body = nullptr;
     return cudaStreamEndCapture(c->aux, &body);
   };
@@ -2069,7 +2089,23 @@ int synx_invert_field(const float* phi, float* psi, const synx_geom* gg, int max
   PartialBufs pb{t.part, t.pmax, nb};
   const float* pp[1] = {phi};
   float* ps[1] = {psi};
-  for (int k = 0; k <= max_iter; ++k) launch_invert_step(pp, ps, 1, g, k, max_iter, mean_tol, max_tol, t.ctl, 0, pb, s);
+  // the single-pass form: residual cache and deferred-voxel list for the one half
+  struct Scratch {
+    float* ec = nullptr;
+    int* list = nullptr;
+    ~Scratch() {
+      if (ec) cudaFree(ec);
+      if (list) cudaFree(list);
+    }
+  } sc;
+  STEP_TRY(cudaMalloc((void**)&sc.ec, 4 * (size_t)g.d.dim * g.d.N));
+  STEP_TRY(cudaMalloc((void**)&sc.list, 4 * (size_t)g.d.N));
+  float* ecs[1] = {sc.ec};
+  int* lists[1] = {sc.list};
+  for (int k = 0; k < max_iter; ++k) {
+    launch_invert_spec(pp, ps, 1, g, k, max_iter, mean_tol, max_tol, t.ctl, 0, pb, s, true, ecs, lists);
+    launch_invert_fix(pp, ps, 1, g, k, max_iter, t.ctl, 0, s, true, ecs, lists);
+  }
   IterCtl h;
   STEP_TRY(cudaMemcpyAsync(&h, t.ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, s));
   STEP_TRY(cudaStreamSynchronize(s));

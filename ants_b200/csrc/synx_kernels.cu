@@ -213,6 +213,9 @@ __global__ void k_zero_ctl_level(IterCtl* ctl) {
       ctl->inv[p][h].counter = 0u;
       ctl->inv[p][h].iters = 0;
       ctl->inv[p][h].exec[0] = ctl->inv[p][h].exec[1] = 0;
+      ctl->inv[p][h].mrun = 0u;
+      ctl->inv[p][h].lcount = 0u;
+      ctl->inv[p][h].fcount = 0u;
     }
 }
 void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s) {
@@ -1022,6 +1025,266 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
     if (dg) k_invert_step<2, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
     else k_invert_step<2, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   }
+}
+
+// ------------------------------------------------------------------------------------------
+// Single-pass fixed-point inverse.  Sub-iteration k (k_invert_spec) evaluates the residual E_k of
+// the iterate psi_k, its statistics, and the update of iteration k in the same pass:
+// psi_{k+1} = psi_k + (-E_k f) eps_k with f = lim / ||E_k / h|| where that exceeds lim and 1
+// elsewhere, lim = eps_k max ||E_k / h|| (ITK's clamp; eps 0.75 then 0.5; boundary voxels pinned
+// to 0).  lim needs the maximum over the whole field, known only when the pass ends, but f = 1
+// wherever ||E_k / h|| <= eps_k M for any lower bound M of that maximum.  Every thread keeps such
+// a bound (its own running maximum and, through a global atomic maximum read at each tile, what the
+// other blocks have seen so far) and updates those voxels at once; the rest keep psi_k, store E_k
+// in the residual cache and append their index to a list, and k_invert_fix applies their updates
+// with the final lim.  The two passes perform exactly the two-pass form's operations on the same
+// values, so the results are bit-identical; the field is streamed once per sub-iteration instead of
+// twice.  Control: S(k) runs when k = 0 or S(k-1) found the half not converged (exec[k & 1]); its
+// last block decides exec[(k + 1) & 1] from the statistics and k + 1 < max_iter.
+// ------------------------------------------------------------------------------------------
+struct InvList {
+  int* idx[2];
+};
+
+template <int DIM, bool DIAG>
+__device__ __forceinline__ void invert_spec_tile(const InvArgs& a, int h, int bx, int by, int bz, float eps,
+                                                 double& acc, float& mx, unsigned* gbound, int* __restrict__ list,
+                                                 unsigned* lcount) {
+  const Dims& d = a.g;
+  const int x = bx * 32 + (threadIdx.x & 31), y = by * 8 + (threadIdx.x >> 5);
+  // every lane of the warp arrives here; the lanes inside the grid walk the same slices below, so
+  // they form one active set for the warp-wide list reservation and maximum
+  const bool inside = x < d.nx && y < d.ny;
+  const unsigned act = __ballot_sync(0xffffffffu, inside);
+  if (!inside) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
+  const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
+  float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
+  float* __restrict__ ec = h ? a.ecache.p[1] : a.ecache.p[0];
+  const int z0 = bz * a.zb, z1 = min(z0 + a.zb, d.nz);
+  const int N = (int)d.N, nxy = d.nx * d.ny;
+  const float fx = (float)x, fy = (float)y;
+  const bool xyedge = x == 0 || x == d.nx - 1 || y == 0 || y == d.ny - 1;
+  const unsigned seen = __ldcg(gbound);
+  float bound = fmaxf(mx, __uint_as_float(seen));
+  const int i0 = z0 * nxy + y * d.nx + x;
+  float pn[3] = {0.0f, 0.0f, 0.0f};
+  if (z0 < z1) {
+    pn[0] = psi[i0];
+    pn[1] = psi[N + i0];
+    pn[2] = DIM == 3 ? psi[2 * N + i0] : 0.0f;
+  }
+  for (int z = z0; z < z1; ++z) {
+    const int i = z * nxy + y * d.nx + x;
+    float p[3] = {pn[0], pn[1], pn[2]};
+    if (z + 1 < z1) {
+      pn[0] = psi[i + nxy];
+      pn[1] = psi[N + i + nxy];
+      pn[2] = DIM == 3 ? psi[2 * N + i + nxy] : 0.0f;
+    }
+    float e[3];
+    inv_residual<DIM, DIAG>(phi, d, a.A, fx, fy, (float)z, p, e);
+    float s2 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const float v = e[c] * a.ih[c];
+      s2 += v * v;
+    }
+    const float nrm = sqrtf(s2);
+    acc += (double)nrm;
+    mx = fmaxf(mx, nrm);
+    bound = fmaxf(bound, nrm);
+    const bool edge = xyedge || (DIM == 3 && (z == 0 || z == d.nz - 1));
+    const bool now = edge || nrm <= eps * bound;  // f = 1 here whatever the final maximum
+    if (now) {
+      const float f = 1.0f;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) p[c] = edge ? 0.0f : p[c] + ((-e[c]) * f) * eps;
+      psi[i] = p[0];
+      psi[N + i] = p[1];
+      if (DIM == 3) psi[2 * N + i] = p[2];
+    } else {
+      ec[i] = e[0];
+      ec[N + i] = e[1];
+      if (DIM == 3) ec[2 * N + i] = e[2];
+    }
+    // deferred voxels: list slots reserved once per warp
+    const unsigned def = __ballot_sync(act, !now);
+    if (def) {
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(lcount, (unsigned)__popc(def));
+      base = __shfl_sync(act, base, leader);
+      if (!now) list[base + __popc(def & ((1u << lane) - 1u))] = i;
+    }
+  }
+  // share the warp's maximum with the other blocks (non-negative floats order as their bits)
+  const unsigned wmax = __reduce_max_sync(act, __float_as_uint(mx));
+  if (lane == leader && wmax > seen) atomicMax(gbound, wmax);
+}
+
+template <int DIM, bool DIAG>
+__global__ void __launch_bounds__(256, 4) k_invert_spec(const InvArgs a, InvLaunch L, IterCtl* ctl,
+                                                        double* __restrict__ psum, float* __restrict__ pmax, int pcap,
+                                                        InvList list) {
+  if (L.stop_aware && ctl->stop) return;
+  __shared__ double redd[32];
+  __shared__ float redf[32];
+  __shared__ int am_last;
+  const int nb = gridDim.x / L.halves;
+  const int h = blockIdx.x / nb;
+  const int bid = blockIdx.x - h * nb;
+  InvCtl& C = ctl->inv[L.phase][h];
+  const int k = L.k >= 0 ? L.k : *(volatile const int*)&ctl->inv[L.phase][0].kdev;
+  if (k > 0 && !*(volatile const int*)&C.exec[k & 1]) {
+    if (bid == 0 && threadIdx.x == 0) C.exec[(k + 1) & 1] = 0;
+    return;
+  }
+  const float eps = k == 0 ? 0.75f : 0.5f;
+  double acc = 0.0;
+  float mxl = 0.0f;
+  const int ntiles = L.tx * L.ty * L.tz;
+  for (int t = bid; t < ntiles; t += nb) {
+    const int bx = t % L.tx, r = t / L.tx;
+    invert_spec_tile<DIM, DIAG>(a, h, bx, r % L.ty, r / L.ty, eps, acc, mxl, &C.mrun, list.idx[h], &C.lcount);
+  }
+  const double bs = block_sum_d(acc, redd);
+  const float bm = block_max_f(mxl, redf);
+  if (threadIdx.x == 0) {
+    psum[h * pcap + bid] = bs;
+    pmax[h * pcap + bid] = bm;
+    __threadfence();
+    const unsigned t = atomicAdd(&C.counter, 1u);
+    am_last = (t == (unsigned)nb - 1);
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double sm = 0.0;
+    float m = 0.0f;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      sm += __ldcg(psum + h * pcap + b);
+      m = fmaxf(m, __ldcg(pmax + h * pcap + b));
+    }
+    sm = block_sum_d(sm, redd);
+    m = block_max_f(m, redf);
+    if (threadIdx.x == 0) {
+      const double mean = sm / (double)a.g.N;
+      C.maxk[k & 1] = m;
+      C.mean[(k + 1) & 1] = mean;
+      C.maxv[(k + 1) & 1] = m;
+      C.exec[(k + 1) & 1] = (k + 1 < L.max_iter && (double)m > L.max_tol && mean > L.mean_tol) ? 1 : 0;
+      C.iters = k + 1;
+      C.counter = 0u;
+    }
+  }
+}
+
+// The deferred updates of sub-iteration k: psi = psi + (-E f) eps with the final clamp.  The last
+// block to finish clears the list and the running bound for the next sub-iteration.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_invert_fix(const InvArgs a, InvLaunch L, IterCtl* ctl, InvList list) {
+  if (L.stop_aware && ctl->stop) return;
+  __shared__ int am_last;
+  const int nb = gridDim.x / L.halves;
+  const int h = blockIdx.x / nb;
+  const int bid = blockIdx.x - h * nb;
+  InvCtl& C = ctl->inv[L.phase][h];
+  const int k = L.k >= 0 ? L.k : *(volatile const int*)&ctl->inv[L.phase][0].kdev;
+  if (k > 0 && !*(volatile const int*)&C.exec[k & 1]) return;
+  const float eps = k == 0 ? 0.75f : 0.5f;
+  const float lim = eps * *(volatile const float*)&C.maxk[k & 1];
+  const unsigned n = *(volatile const unsigned*)&C.lcount;
+  const int N = (int)a.g.N;
+  float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
+  const float* __restrict__ ec = h ? a.ecache.p[1] : a.ecache.p[0];
+  const int* __restrict__ idx = list.idx[h];
+  for (unsigned j = (unsigned)bid * blockDim.x + threadIdx.x; j < n; j += (unsigned)nb * blockDim.x) {
+    const int i = idx[j];
+    float e[3], p[3];
+    e[0] = ec[i];
+    e[1] = ec[N + i];
+    e[2] = DIM == 3 ? ec[2 * N + i] : 0.0f;
+    p[0] = psi[i];
+    p[1] = psi[N + i];
+    p[2] = DIM == 3 ? psi[2 * N + i] : 0.0f;
+    float s2 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const float v = e[c] * a.ih[c];
+      s2 += v * v;
+    }
+    const float nrm = sqrtf(s2);
+    const float f = nrm > lim ? lim / nrm : 1.0f;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) p[c] = p[c] + ((-e[c]) * f) * eps;
+    psi[i] = p[0];
+    psi[N + i] = p[1];
+    if (DIM == 3) psi[2 * N + i] = p[2];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    am_last = atomicAdd(&C.fcount, 1u) == (unsigned)nb - 1;
+  }
+  __syncthreads();
+  if (am_last && threadIdx.x == 0) {
+    C.lcount = 0u;
+    C.mrun = 0u;
+    C.fcount = 0u;
+  }
+}
+
+void launch_invert_spec(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
+                        double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
+                        bool stop_aware, float* const* ecache, int* const* list) {
+  count_launch();
+  const Map3 m2 = map3(g.d, 2, kInvTarget);
+  const int tz = (int)m2.grid.z / 2;
+  const int ntiles = (int)m2.grid.x * (int)m2.grid.y * tz;
+  const int nb = std::max(1, std::min({ntiles, kInvBlocksPerHalf, pb.capacity}));
+  const InvArgs a = make_inv_args(phi, psi, halves, g, m2.zb, ecache);
+  InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, (int)m2.grid.x, (int)m2.grid.y, tz, mean_tol, max_tol};
+  const InvList il{{list[0], halves > 1 ? list[1] : list[0]}};
+  const bool dg = affine_diag(make_affine(g, g));
+  const dim3 grid((unsigned)(nb * halves));
+  if (g.d.dim == 3) {
+    if (dg) k_invert_spec<3, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+    else k_invert_spec<3, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+  } else {
+    if (dg) k_invert_spec<2, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+    else k_invert_spec<2, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+  }
+}
+
+constexpr int kInvFixBlocksPerHalf = 148;
+
+void launch_invert_fix(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
+                       IterCtl* ctl, int phase, cudaStream_t s, bool stop_aware, float* const* ecache,
+                       int* const* list) {
+  count_launch();
+  const InvArgs a = make_inv_args(phi, psi, halves, g, 1, ecache);
+  InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, 0, 0, 0, 0.0, 0.0};
+  const InvList il{{list[0], halves > 1 ? list[1] : list[0]}};
+  const dim3 grid((unsigned)(kInvFixBlocksPerHalf * halves));
+  if (g.d.dim == 3)
+    k_invert_fix<3><<<grid, 256, 0, s>>>(a, L, ctl, il);
+  else
+    k_invert_fix<2><<<grid, 256, 0, s>>>(a, L, ctl, il);
+}
+
+__global__ void k_inv_spec_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, int init) {
+  InvCtl* C = ctl->inv[phase];
+  const int next = init ? 1 : C[0].kdev + 1;
+  const int s = next & 1;
+  const unsigned go = (!ctl->stop && next < max_iter && (C[0].exec[s] || C[1].exec[s])) ? 1u : 0u;
+  C[0].kdev = next;
+  cudaGraphSetConditional(handle, go);
+}
+
+void launch_inv_spec_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, bool init,
+                             cudaStream_t s) {
+  count_launch();
+  k_inv_spec_control<<<1, 1, 0, s>>>(ctl, phase, handle, max_iter, init ? 1 : 0);
 }
 
 __global__ void k_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter,

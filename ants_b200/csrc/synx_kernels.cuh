@@ -18,6 +18,14 @@ struct InvCtl {
   unsigned counter;
   int kdev;  // sub-iteration index for launches that read it from the device (graph loop bodies)
   int pad;
+  // single-pass form: a running lower bound of the residual maximum (float bits), the deferred
+  // voxels' list length, the arrival counter of the deferred-update pass, and per sub-iteration
+  // parity the residual maximum the deferred updates clamp against
+  unsigned mrun;
+  unsigned lcount;
+  unsigned fcount;
+  float maxk[2];
+  int pad2;
 };
 
 constexpr int kMaxWindow = 64;
@@ -144,6 +152,22 @@ int inv_blocks(const GridInfo& g);
 void launch_invert_step(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
                         double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
                         bool stop_aware = true, float* const* ecache = nullptr);
+// Single-pass fixed-point inverse: sub-iteration k evaluates the residual of the iterate, its
+// statistics and the update in one pass over the field (launch_invert_spec), deferring the voxels
+// whose clamp factor is not yet known to a short second pass (launch_invert_fix) over a list of
+// their indices (`list`: per half, room for every voxel of g).  `ecache` (required) holds the
+// deferred voxels' residuals.  k < 0: graph loop body (index from the control block).
+void launch_invert_spec(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
+                        double mean_tol, double max_tol, IterCtl* ctl, int phase, PartialBufs pb, cudaStream_t s,
+                        bool stop_aware, float* const* ecache, int* const* list);
+void launch_invert_fix(const float* const* phi, float* const* psi, int halves, const GridInfo& g, int k, int max_iter,
+                       IterCtl* ctl, int phase, cudaStream_t s, bool stop_aware, float* const* ecache,
+                       int* const* list);
+// Loop control of the single-pass form's WHILE node: init (after sub-iteration 0) sets kdev = 1,
+// the step form advances kdev; both set the condition to "level running, kdev < max_iter and some
+// half continues", so the loop ends within max_iter bodies.
+void launch_inv_spec_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, bool init,
+                             cudaStream_t s);
 // Loop control of a fixed-point inverse captured as a conditional WHILE graph node: init (after
 // the k = 0 statistics launch) sets kdev = 1 and the loop condition to "level still running";
 // the step form (the loop body's second kernel) advances kdev and sets the condition to "some

@@ -91,6 +91,8 @@ def test_footprint_without_a_gpu():
     big = footprint(P, Geom((182, 218, 182)), Geom((182, 218, 182)))
     small = footprint(P, Geom((91, 109, 91)), Geom((91, 109, 91)))
     n = 182 * 218 * 182
-    # 4 half-fields + 6 work fields of 3 components, 2 warped images, 5 image buffers: 37 floats/voxel
-    assert 37 * 4 * n <= big < 37 * 4 * n * 1.05
+    # 4 half-fields + 6 work fields of 3 components, 2 warped images, 5 image buffers: 37 floats/voxel,
+    # plus the inverse's two deferred-voxel lists (2 ints) and the metric-mask validity (1 byte)
+    per_voxel = 37 * 4 + 2 * 4 + 1
+    assert per_voxel * n <= big < per_voxel * n * 1.05
     assert small < big / 7

@@ -14,7 +14,8 @@ import pytest
 
 import oracle as O
 from ants_b200 import phantoms
-from ants_b200.synx import SYNX_F_NO_PERSISTENT, SYNX_F_SMOOTH_TWO_PASS, SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage
+from ants_b200.synx import (SYNX_F_INV_TWO_PASS, SYNX_F_NO_PERSISTENT, SYNX_F_SMOOTH_TWO_PASS, SYNX_F_USE_GRAPHS, Geom,
+                            SyNParams, SyNStage)
 
 pytestmark = pytest.mark.gpu
 
@@ -199,3 +200,26 @@ def test_slab_smoothing_matches_two_pass_bit_for_bit(cuda, uvar):
     np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
     np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
     assert outs[0][1] == outs[1][1]
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("dim,size", [(3, (38, 35, 31)), (2, (90, 77))])
+def test_single_pass_inverse_matches_two_pass_bit_for_bit(cuda, dim, size, graphs):
+    # the single-pass fixed-point inverse (residual, statistics and update in one pass; clamped voxels
+    # deferred to a short pass over a list) performs the two-pass form's operations on the same values:
+    # whole registrations agree bit for bit, including the cold-started first inversions that iterate
+    f, m = make_pair(dim, size, seed=19)
+    g = Geom(size)
+    outs = []
+    for extra in (0, SYNX_F_INV_TWO_PASS):
+        P = SyNParams(dim=dim, cc_radius=3 if dim == 3 else 2, iterations=(6, 4), shrink_factors=(2, 1),
+                      smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12,
+                      flags=(SYNX_F_USE_GRAPHS if graphs else 0) | SYNX_F_NO_PERSISTENT | extra)
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.run()
+            outs.append((st.fields(), [(r.metric, r.inverse_iterations) for r in st.log()]))
+    np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
+    np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
+    assert outs[0][1] == outs[1][1]
+    assert max(k for _, k in outs[0][1]) > 4  # some inversions iterate more than once
