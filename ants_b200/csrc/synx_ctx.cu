@@ -607,7 +607,7 @@ void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const
   const float* k[3] = {coeff_base, coeff_base + c->coeff_cap, coeff_base + 2 * c->coeff_cap};
   if (smooth3_supported(c->D, R)) {
     const float* kh[3] = {host_base, host_base + c->coeff_cap, host_base + 2 * c->coeff_cap};
-    const int rows = c->cur_level >= 0 ? c->plan[c->cur_level].smooth_rows : 8;
+    const int rows = c->cur_level >= 0 ? c->plan[c->cur_level].smooth_rows : -1;
     const SmoothPlan sp{rows > 0 ? rows : 0, 0};
     launch_smooth_field(in, out, orig, tmp, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream, &sp);
     return;
@@ -808,11 +808,11 @@ int level_smooth_radius(const synx_ctx* c, const GridInfo& g) {
 }
 
 // The tile plan of a level: the tuning table's entry for its grid (unless the stage opts out),
-// overridden by explicit stage parameters; without either, the cost models (slab smoothing with
-// 8-row tiles, the CC chunk model, the persistent kernel up to the size threshold).
+// overridden by explicit stage parameters; without either, the cost models (xy and z smoothing
+// kernels, the CC chunk model, the persistent kernel up to the size threshold).
 LevelPlan resolve_plan(synx_ctx* c, int level) {
   const GridInfo& g = c->lv[level];
-  LevelPlan p{-1, 8, 0};
+  LevelPlan p{-1, -1, 0};
   LevelPlan t{};
   if (c->P.tuning == 0 &&
       tuning_lookup(c->D, c->P.cc_radius, level_smooth_radius(c, g), g.d.nx, g.d.ny, g.d.nz, &t))

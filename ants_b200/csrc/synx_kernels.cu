@@ -717,7 +717,10 @@ static void launch_smooth_slab(const Smooth3Args& a0, const GridInfo& g, int RR,
 #undef SYNX_SSLAB
 }
 
-SmoothPlan g_smooth_plan{8, 0};
+// Default: the xy and z kernels.  The autotuner measured the slab kernel slower at every level of
+// the 182x218x182 pyramid (a block's slices are convolved one after another, three barriers each,
+// with too few blocks in flight), so it runs only where a tuning table picks it.
+SmoothPlan g_smooth_plan{0, 0};
 
 void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
                          int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,

@@ -104,7 +104,8 @@ typedef struct synx_params {
 #define SYNX_F_CC_FP32_SUMS 0x8  /* CC window sums and variance terms in float instead of double */
 #define SYNX_F_FIELDS_FP16 0x10  /* half-fields rounded to half precision wherever they are stored */
 #define SYNX_F_SMOOTH_TWO_PASS 0x20 /* 3-D field smoothing as an xy kernel and a z kernel through a
-                                       temporary instead of the fused slab kernel (same results) */
+                                       temporary even where a tuning table picks the fused slab
+                                       kernel (same results) */
 #define SYNX_F_INV_TWO_PASS 0x40    /* fixed-point inverse with a statistics pass and an update pass per
                                        sub-iteration instead of the single-pass form (same results) */
 

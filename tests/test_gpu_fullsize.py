@@ -53,7 +53,7 @@ def test_update_smoothing_is_linear(cuda):
 
 
 def test_update_smoothing_matches_oracle_at_full_size(cuda):
-    # the slab smoothing kernel walks z in chunks at this size: compare it with the oracle
+    # the xy and z smoothing kernels at full size (the z kernel walks columns in chunks): the oracle
     import oracle as O
     g = Geom(SIZE)
     u = np.random.default_rng(6).standard_normal((3,) + g.shape).astype(np.float32)

@@ -182,16 +182,18 @@ def test_run_level_order_enforced(cuda):
         assert st.output_geom().size == (32, 32)
 
 
+@pytest.mark.parametrize("rows", [8, 16])
 @pytest.mark.parametrize("uvar", [3.0, 0.3, 8.0])
-def test_slab_smoothing_matches_two_pass_bit_for_bit(cuda, uvar):
-    # the fused slab smoothing (xy and z in one kernel) and the two-kernel path through a temporary
-    # do the same arithmetic in the same order: whole registrations agree bit for bit
+def test_slab_smoothing_matches_two_pass_bit_for_bit(cuda, uvar, rows):
+    # the fused slab smoothing (xy and z in one kernel, a tuning-table option) and the two-kernel path
+    # through a temporary (the default) do the same arithmetic in the same order: whole registrations
+    # agree bit for bit
     f, m = make_pair(3, (41, 37, 33), seed=13)
     g = Geom((41, 37, 33))
     outs = []
-    for extra in (0, SYNX_F_SMOOTH_TWO_PASS):
+    for tile_rows, extra in ((rows, 0), (rows, SYNX_F_SMOOTH_TWO_PASS)):
         P = SyNParams(dim=3, cc_radius=3, update_variance=uvar, iterations=(5, 3), shrink_factors=(2, 1),
-                      smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12,
+                      smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12, smooth_tile_rows=tile_rows,
                       flags=SYNX_F_USE_GRAPHS | SYNX_F_NO_PERSISTENT | extra)
         with SyNStage(P) as st:
             st.set_images(f, g, m, g)
