@@ -8,9 +8,9 @@ level grid keeps the candidate with the least time per iteration.  Candidates:
 
 * the persistent level kernel (every phase of every iteration in one cooperative launch), where the
   level kernel implements the stage's options;
-* the per-kernel path with the update smoothing as the fused slab kernel (8- or 16-row column tiles)
-  or as an xy kernel plus a z kernel, crossed with the CC kernel's z chunk count (its cost model, or
-  1, 2, 4, 8, 16 chunks where the depth allows);
+* the per-kernel path with the update smoothing as the fused slab kernel (8- or 16-row column tiles),
+  as an xy kernel plus a z kernel, or as the pipelined xy kernel (32- or 64-row tiles) plus the z
+  kernel, crossed with the CC kernel's z chunk count (its cost model, or 4 or 8 chunks);
 * the built-in cost models (the plan without a table), timed for comparison.
 
     python -m ants_b200.autotune --out ants_b200/tuning_b200.txt [--workloads single,batched,...]
@@ -77,8 +77,8 @@ def candidates(dim):
     if dim == 2:
         cands.append(("kernels", dict(tuning=1, flags=S.SYNX_F_NO_PERSISTENT)))
         return cands
-    for rows in (8, 16, -1):
-        for chunks in (0, 1, 2, 4, 8, 16):
+    for rows in (8, 16, -1, -2, -3):
+        for chunks in (0, 4, 8):
             cands.append((f"kernels rows={rows} chunks={chunks}",
                           dict(tuning=1, flags=S.SYNX_F_NO_PERSISTENT, smooth_tile_rows=rows, cc_z_chunks=chunks)))
     return cands

@@ -608,7 +608,9 @@ void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const
   if (smooth3_supported(c->D, R)) {
     const float* kh[3] = {host_base, host_base + c->coeff_cap, host_base + 2 * c->coeff_cap};
     const int rows = c->cur_level >= 0 ? c->plan[c->cur_level].smooth_rows : -1;
-    const SmoothPlan sp{rows > 0 ? rows : 0, 0};
+    // tile rows > 0: the slab kernel; -1: xy kernel + z kernel; -2 / -3: pipelined xy kernel with
+    // 32 / 64-row tiles + z kernel
+    const SmoothPlan sp{rows > 0 ? rows : 0, 0, rows == -2 ? 32 : (rows == -3 ? 64 : 0)};
     launch_smooth_field(in, out, orig, tmp, 2, g, kh, R, epilogue, w1, w2, maxnorm, c->ctl, c->stream, &sp);
     return;
   }
@@ -818,7 +820,7 @@ LevelPlan resolve_plan(synx_ctx* c, int level) {
       tuning_lookup(c->D, c->P.cc_radius, level_smooth_radius(c, g), g.d.nx, g.d.ny, g.d.nz, &t))
     p = t;
   if (c->P.smooth_tile_rows != 0) p.smooth_rows = c->P.smooth_tile_rows;
-  if (c->P.flags & SYNX_F_SMOOTH_TWO_PASS) p.smooth_rows = -1;
+  if ((c->P.flags & SYNX_F_SMOOTH_TWO_PASS) && p.smooth_rows > 0) p.smooth_rows = -1;
   if (c->P.cc_z_chunks > 0) p.cc_chunks = c->P.cc_z_chunks;
   if (c->P.persistent_max_voxels > 0) p.persistent = -1;  // an explicit size threshold decides
   return p;
@@ -1367,8 +1369,9 @@ int synx_create(const synx_params* params, int device, void* cuda_stream, synx_c
   if (p.histogram_match != 0 && p.histogram_match != 1)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: histogram_match must be 0 or 1");
   if (p.tuning != 0 && p.tuning != 1) return set_err(nullptr, SYNX_E_ARG, "synx_create: tuning must be 0 or 1");
-  if (p.smooth_tile_rows != 0 && p.smooth_tile_rows != 8 && p.smooth_tile_rows != 16 && p.smooth_tile_rows != -1)
-    return set_err(nullptr, SYNX_E_ARG, "synx_create: smooth_tile_rows must be 0, 8, 16 or -1");
+  if (p.smooth_tile_rows != 0 && p.smooth_tile_rows != 8 && p.smooth_tile_rows != 16 &&
+      (p.smooth_tile_rows < -3 || p.smooth_tile_rows > -1))
+    return set_err(nullptr, SYNX_E_ARG, "synx_create: smooth_tile_rows must be 0, 8, 16, -1, -2 or -3");
   if (p.cc_z_chunks < 0 || p.cc_z_chunks > 4096)
     return set_err(nullptr, SYNX_E_ARG, "synx_create: cc_z_chunks must be in 0..4096");
   int ndev = 0;

@@ -13,7 +13,8 @@ int set_global_error(int code, const std::string& msg);
 // kernel instead), as the autotuner's table records it.
 struct LevelPlan {
   int persistent;   // 1: persistent level kernel (when eligible), 0: per-kernel path, -1: size threshold
-  int smooth_rows;  // 3-D update smoothing: 8 / 16 slab tile rows, -1: xy + z kernels
+  int smooth_rows;  // 3-D update smoothing: 8 / 16 slab tile rows, -1: xy + z kernels, -2 / -3: pipelined
+                    // xy kernel (32 / 64-row tiles) + z kernel
   int cc_chunks;    // z chunks of the CC kernel, 0: its cost model
 };
 

@@ -479,6 +479,58 @@ __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, 
   }
 }
 
+// 3-D xy smoothing over a chunk of ZC slices per block, the halo tiles double-buffered: the tile of
+// the next slice is copied in with cp.async while the current one is convolved, so the load latency
+// overlaps the arithmetic instead of stalling each block between its barriers.  Writes the
+// xy-smoothed fields for the z kernel; the arithmetic is k_smooth_xy's (the same bits).
+template <int R, int TY>
+__global__ void __launch_bounds__(256) k_smooth_xy_pipe(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  if (ctl != nullptr && ctl->stop) return;
+  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R, RPT = TY / 8;
+  constexpr int TILE = 3 * HY * HXP;
+  extern __shared__ __align__(16) float smp[];
+  float* xsum = smp + 2 * TILE;
+  const int nzc = gridDim.z / a.halves;
+  const int h = blockIdx.z / nzc, zc = blockIdx.z - h * nzc;
+  const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, d.nz);
+  if (z0 >= z1) return;  // the same for every thread of the block
+  const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
+  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int ox = blockIdx.x * 32 + tx, oy0 = blockIdx.y * TY + ty * RPT;
+  smooth_xy_load_tile<3, R, TY, true>(a, d, blockIdx.x, blockIdx.y, z0, h, smp);
+  cp_async_commit();
+  for (int z = z0; z < z1; ++z) {
+    const int k = z - z0;
+    if (z + 1 < z1) {
+      // buffer (k + 1) & 1 was last read by the convolution of slice z - 1, which ended in a barrier
+      smooth_xy_load_tile<3, R, TY, true>(a, d, blockIdx.x, blockIdx.y, z + 1, h, smp + ((k + 1) & 1) * TILE);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    float y[3][RPT];
+    smooth_xy_convolve<3, R, TY>(a, smp + (k & 1) * TILE, xsum, y);
+    if (ox < nx) {
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        const int oy = oy0 + r;
+        if (oy >= ny) break;
+        const int i = z * nxy + oy * nx + ox;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[c * N + i] = y[c][r];
+      }
+    }
+  }
+}
+
+size_t smooth_xy_pipe_smem_bytes(int R, int TY) {
+  const int HXP = (32 + 2 * R + 3) & ~3, HY = TY + 2 * R;
+  return (size_t)(2 * 3 * HY * HXP + 3 * HY * 32) * sizeof(float);
+}
+
 template <int R>
 // the ring lives in shared memory ((2R+1) x 3 x 256 floats, smooth_z_smem_bytes), so few registers
 // are needed: 5 resident blocks per SM up to R = 6 (40 KB of ring each), 3 up to R = 12
@@ -590,6 +642,12 @@ static cudaError_t smooth3_attr_both() {
                              (int)(smooth3_smem_floats(2, R, kSmoothTileY) * 4));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_smooth_z<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_z_smem_bytes(R));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_smooth_xy_pipe<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smooth_xy_pipe_smem_bytes(R, 32));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_smooth_xy_pipe<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smooth_xy_pipe_smem_bytes(R, 64));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_smooth_slab<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smooth_slab_smem_bytes(R, 8));
@@ -720,7 +778,7 @@ static void launch_smooth_slab(const Smooth3Args& a0, const GridInfo& g, int RR,
 // Default: the xy and z kernels.  The autotuner measured the slab kernel slower at every level of
 // the 182x218x182 pyramid (a block's slices are convolved one after another, three barriers each,
 // with too few blocks in flight), so it runs only where a tuning table picks it.
-SmoothPlan g_smooth_plan{0, 0};
+SmoothPlan g_smooth_plan{0, 0, 0};
 
 void launch_smooth_field(const float* const* in, float* const* out, const float* const* orig, float* const* tmp,
                          int halves, const GridInfo& g, const float* const khost[3], const int R[3], bool epilogue,
@@ -737,6 +795,52 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   Smooth3Args a = make_smooth_args(in, dim == 3 ? tmp : out, orig, halves, g, khost, R, epilogue, w1, w2, maxnorm, &RR);
   // xy tiles are 32 x kSmoothTileY; the z pass below keeps 32 x 8 columns
   const int gx = (g.d.nx + 31) / 32, gy = (g.d.ny + 7) / 8;
+  if (dim == 3 && (P.xy_ty == 32 || P.xy_ty == 64)) {
+    // the pipelined xy kernel: chunks of slices per block by waves of resident blocks times the
+    // slices a block walks (plus one for the pipeline's fill)
+    const int TY = P.xy_ty;
+    const size_t smem = smooth_xy_pipe_smem_bytes(RR, TY);
+    const int per_sm = std::max(1, (int)std::min<size_t>(8, (227 * 1024) / (smem + 1024)));
+    const int cols = gx * ((g.d.ny + TY - 1) / TY) * halves;
+    int best_zc = g.d.nz;
+    double best = -1.0;
+    for (int zc = 1; zc <= g.d.nz; ++zc) {
+      const long long blocks = (long long)cols * ((g.d.nz + zc - 1) / zc);
+      const double cost = (double)((blocks + 148 * per_sm - 1) / (148 * per_sm)) * (zc + 1);
+      if (best < 0 || cost < best) {
+        best = cost;
+        best_zc = zc;
+      }
+    }
+    Smooth3Args ap = a;
+    ap.ZC = best_zc;
+    const dim3 gp(gx, (g.d.ny + TY - 1) / TY, ((g.d.nz + best_zc - 1) / best_zc) * halves);
+    count_launch();
+#define SYNX_SXYP(RV)                                                                           \
+  case RV:                                                                                      \
+    if (TY == 64)                                                                               \
+      k_smooth_xy_pipe<RV, 64><<<gp, 256, smooth_xy_pipe_smem_bytes(RV, 64), s>>>(ap, g.d, ctl); \
+    else                                                                                        \
+      k_smooth_xy_pipe<RV, 32><<<gp, 256, smooth_xy_pipe_smem_bytes(RV, 32), s>>>(ap, g.d, ctl); \
+    break;
+    switch (RR) {
+      SYNX_SXYP(1)
+      SYNX_SXYP(2)
+      SYNX_SXYP(3)
+      SYNX_SXYP(4)
+      SYNX_SXYP(5)
+      SYNX_SXYP(6)
+      SYNX_SXYP(7)
+      SYNX_SXYP(8)
+      SYNX_SXYP(9)
+      SYNX_SXYP(10)
+      SYNX_SXYP(11)
+      SYNX_SXYP(12)
+      default:
+        break;
+    }
+#undef SYNX_SXYP
+  } else {
   const dim3 gxy(gx, (g.d.ny + kSmoothTileY - 1) / kSmoothTileY, g.d.nz * halves);
   const size_t smem = smooth3_smem_floats(dim, RR, kSmoothTileY) * 4;
   count_launch();
@@ -764,6 +868,7 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
       break;
   }
 #undef SYNX_SXY
+  }
   if (dim != 3) return;
   // z pass: tmp -> out with the epilogue
   a.in = Ptr2c{{tmp[0], halves > 1 ? tmp[1] : tmp[0]}};

@@ -119,10 +119,12 @@ bool smooth3_supported(int dim, const int R[3]);
 cudaError_t smooth3_prepare();
 // How a 3-D field is smoothed: slab_ty > 0 runs the fused slab kernel with 32 x slab_ty column
 // tiles (8 or 16) and slab_zc output slices per block (0: chosen by a waves x work model);
-// slab_ty = 0 runs the xy kernel and then the z kernel through `tmp`.
+// slab_ty = 0 runs an xy kernel and then the z kernel through `tmp`.
 struct SmoothPlan {
   int slab_ty;
   int slab_zc;
+  int xy_ty;  // two-kernel path: 0 = the xy kernel (one slice per block), 32 / 64 = the pipelined xy
+              // kernel (double-buffered tiles over a chunk of slices) with 32 x xy_ty tiles
 };
 extern SmoothPlan g_smooth_plan;  // the default plan
 // In 3-D on the two-kernel path the xy pass writes `tmp` (same shape as `out`), which the z pass

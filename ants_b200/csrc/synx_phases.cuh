@@ -300,15 +300,22 @@ __host__ __device__ inline size_t smooth3_smem_floats(int dim, int R, int TY = 8
 // rows for TY outputs).
 // The xy convolution of one (32 x TY tile, slice z, field h): thread (tx, ty) gets the outputs at
 // x = bx*32 + tx, y = by*TY + ty*(TY/8) + r in y[c][r].  All threads of the block must call it.
-template <int DIM, int R, int TY>
-__device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
-                                                  float* sm, float (&y)[DIM][TY / 8]) {
-  static_assert(TY % 8 == 0, "8 warps share the tile rows");
-  constexpr int K = 2 * R + 1, RPT = TY / 8;
+// Halo tile of one (32 x TY tile, slice z, field h) into shared memory (replicate-edge indices):
+// plain loads, or with ASYNC cp.async copies that the caller commits and waits for.
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(NPENDING) : "memory");
+}
+
+template <int DIM, int R, int TY, bool ASYNC>
+__device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
+                                                    float* tile) {
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
-  constexpr int NQ = (2 * R + 3) / 4 + 1;  // float4 loads covering 4 + 2R taps
-  float* tile = sm;                    // [DIM][HY][HXP]
-  float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
   const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
   const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
@@ -320,9 +327,27 @@ __device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Di
     const float* line = plane + c * N + gy * nx;
     float* trow = tile + row * HXP;
 #pragma unroll
-    for (int hx = tx; hx < HX; hx += 32) trow[hx] = __ldg(line + min(max(x0 - R + hx, 0), nx - 1));
+    for (int hx = tx; hx < HX; hx += 32) {
+      const float* g = line + min(max(x0 - R + hx, 0), nx - 1);
+      if (ASYNC)
+        cp_async4(trow + hx, g);
+      else
+        trow[hx] = __ldg(g);
+    }
   }
-  __syncthreads();
+}
+
+// x and y convolution of a loaded halo tile: thread (tx, ty) gets the outputs at x = bx*32 + tx,
+// y = by*TY + ty*(TY/8) + r in y[c][r].  All threads of the block call it; it ends with the
+// tile read and xsum free again.
+template <int DIM, int R, int TY>
+__device__ __forceinline__ void smooth_xy_convolve(const Smooth3Args& a, const float* tile, float* xsum,
+                                                   float (&y)[DIM][TY / 8]) {
+  static_assert(TY % 8 == 0, "8 warps share the tile rows");
+  constexpr int K = 2 * R + 1, RPT = TY / 8;
+  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
+  constexpr int NQ = (2 * R + 3) / 4 + 1;  // float4 loads covering 4 + 2R taps
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   for (int it = tid; it < DIM * HY * 8; it += 256) {
     const int row = it >> 3, q = it & 7;
     const float4* t4 = reinterpret_cast<const float4*>(tile + row * HXP) + q;
@@ -362,6 +387,17 @@ __device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Di
     }
   }
   __syncthreads();  // the tile and xsum may be reused by the caller's next tile
+}
+
+template <int DIM, int R, int TY>
+__device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
+                                                  float* sm, float (&y)[DIM][TY / 8]) {
+  constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
+  float* tile = sm;                     // [DIM][HY][HXP]
+  float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
+  smooth_xy_load_tile<DIM, R, TY, false>(a, d, bx, by, z, h, tile);
+  __syncthreads();
+  smooth_xy_convolve<DIM, R, TY>(a, tile, xsum, y);
 }
 
 // xy part for one (32 x TY tile, slice z, field h), written out: in 3-D the xy-smoothed values go
@@ -490,14 +526,25 @@ __device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, cons
     for (int c = 0; c < 3; ++c) slot(u, c) = __ldg(col + c * N + zs * nxy);
   }
   const bool xyedge = ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1;
+  // the slices entering the window are loaded two outputs ahead (q0: slice z + R, q1: z + R + 1),
+  // so each load's latency overlaps two outputs' convolutions
+  float q0[3], q1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    q0[c] = z0 < z1 ? __ldg(col + c * N + min(z0 + R, nz - 1) * nxy) : 0.0f;
+    q1[c] = z0 + 1 < z1 ? __ldg(col + c * N + min(z0 + 1 + R, nz - 1) * nxy) : 0.0f;
+  }
   for (int zb = z0; zb < z1; zb += RD) {
 #pragma unroll
     for (int u = 0; u < RD; ++u) {
       const int z = zb + u;
       if (z < z1) {
-        const int zs = min(z + R, nz - 1);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) slot((u + 2 * R) % RD, c) = __ldg(col + c * N + zs * nxy);
+        for (int c = 0; c < 3; ++c) {
+          slot((u + 2 * R) % RD, c) = q0[c];
+          q0[c] = q1[c];
+          if (z + 2 < z1) q1[c] = __ldg(col + c * N + min(z + 2 + R, nz - 1) * nxy);
+        }
         const int i = z * nxy + oy * nx + ox;
         const bool edge = a.epilogue && (xyedge || z == 0 || z == nz - 1);
         float nrm2 = 0.0f;

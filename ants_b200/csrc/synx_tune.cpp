@@ -7,7 +7,8 @@
 //   dim nx ny nz r_cc r_smooth  persistent smooth_rows cc_z_chunks  ms_best ms_default
 //
 // persistent: 1 = the persistent level kernel, 0 = the per-kernel path; smooth_rows: 8 or 16 (the
-// fused slab smoothing kernel's tile rows) or -1 (xy and z kernels); cc_z_chunks: z chunks of the
+// fused slab smoothing kernel's tile rows), -1 (xy and z kernels) or -2 / -3 (the pipelined xy kernel
+// with 32- / 64-row tiles, and the z kernel); cc_z_chunks: z chunks of the
 // CC kernel (0 = its cost model).  The two times are informational.  The table is read once per
 // process (first synx_create) from $SYNX_TUNING_TABLE or tuning_b200.txt beside libsynx.so.
 #include <dlfcn.h>
@@ -67,7 +68,8 @@ int load_locked(const std::string& path) {
                               &e.r_smooth, &e.plan.persistent, &e.plan.smooth_rows, &e.plan.cc_chunks, &a, &b);
     if (n < 9 || (e.dim != 2 && e.dim != 3) || e.nx < 1 || e.ny < 1 || e.nz < 1) continue;
     if (e.plan.persistent != 0 && e.plan.persistent != 1) continue;
-    if (e.plan.smooth_rows != 8 && e.plan.smooth_rows != 16 && e.plan.smooth_rows != -1) continue;
+    if (e.plan.smooth_rows != 8 && e.plan.smooth_rows != 16 && (e.plan.smooth_rows < -3 || e.plan.smooth_rows > -1))
+      continue;
     if (e.plan.cc_chunks < 0 || e.plan.cc_chunks > 4096) continue;
     g_table.push_back(e);
   }

@@ -304,7 +304,7 @@ class SyNParams:
     persistent_max_voxels: int = 0  # largest level it runs (0: automatic)
     test_inject: int = 0  # SYNX_INJECT_* (failure-detection tests)
     histogram_match: bool = False  # --use-histogram-matching 1: the moving image matched to the fixed one
-    smooth_tile_rows: int = 0  # 3-D update smoothing: 8/16 slab tiles, -1 two kernels, 0 tuned table / model
+    smooth_tile_rows: int = 0  # 3-D smoothing: 8/16 slab, -1 two kernels, -2/-3 pipelined xy, 0 table / model
     cc_z_chunks: int = 0  # CC kernel z chunks, 0 tuned table / model
     tuning: int = 0  # 0: per-level plans from the tuning table; 1: built-in cost models only
 

@@ -91,7 +91,9 @@ typedef struct synx_params {
    * smoothing choice not at all).  0 = the tuning table's entry for the level grid (see
    * synx_tuning_load), or the built-in cost models when the table has none. */
   int32_t smooth_tile_rows;      /* 3-D update smoothing: 8 or 16 = fused slab kernel with 32 x rows
-                                    column tiles; -1 = xy kernel + z kernel through a temporary */
+                                    column tiles; -1 = xy kernel + z kernel through a temporary;
+                                    -2 / -3 = the same with the pipelined xy kernel (double-buffered
+                                    32 x 32 / 32 x 64 tiles over chunks of slices) */
   int32_t cc_z_chunks;           /* z chunks of the CC kernel's column walks (>= 1), 0 = table/model */
   int32_t tuning;                /* 0: use the tuning table; 1: built-in cost models only */
   int32_t reserved[1];

@@ -225,3 +225,24 @@ def test_single_pass_inverse_matches_two_pass_bit_for_bit(cuda, dim, size, graph
     np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
     assert outs[0][1] == outs[1][1]
     assert max(k for _, k in outs[0][1]) > 4  # some inversions iterate more than once
+
+
+@pytest.mark.parametrize("rows", [-2, -3])
+@pytest.mark.parametrize("uvar", [3.0, 0.3])
+def test_pipelined_xy_smoothing_matches_bit_for_bit(cuda, uvar, rows):
+    # the pipelined xy kernel (double-buffered halo tiles over chunks of slices) does the xy kernel's
+    # arithmetic: whole registrations agree bit for bit with the plain xy kernel
+    f, m = make_pair(3, (43, 71, 29), seed=23)
+    g = Geom((43, 71, 29))
+    outs = []
+    for tile_rows in (rows, -1):
+        P = SyNParams(dim=3, cc_radius=3, update_variance=uvar, iterations=(5, 3), shrink_factors=(2, 1),
+                      smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12, smooth_tile_rows=tile_rows,
+                      flags=SYNX_F_USE_GRAPHS | SYNX_F_NO_PERSISTENT)
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.run()
+            outs.append((st.fields(), [r.metric for r in st.log()]))
+    np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
+    np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
+    assert outs[0][1] == outs[1][1]

@@ -13,10 +13,11 @@ def test_table_loads_and_skips_malformed_lines(tmp_path):
                  "3 182 218 182 4 6  0 16 7  1.2 1.5\n"
                  "2 256 256 1 2 6  1 8 0  0.1 0.1\n"
                  "3 10 10 10 4 6  5 8 0  1 1\n"      # persistent must be 0 or 1
-                 "3 10 10 10 4 6  0 12 0  1 1\n"     # tile rows must be 8, 16 or -1
+                 "3 10 10 10 4 6  0 12 0  1 1\n"     # tile rows must be 8, 16, -1, -2 or -3
+                 "3 12 10 10 4 6  0 -2 4  1 1\n"
                  "garbage\n")
     try:
-        assert synx.tuning_load(str(p)) == 2
+        assert synx.tuning_load(str(p)) == 3
         assert synx.tuning_path() == str(p)
     finally:
         synx.tuning_load(None)
