@@ -127,6 +127,8 @@ def tune(names, reps=2, log=print):
                 results[name] = time_levels(f, m, g, dim, stage, over, reps)
             except S.SynxError as e:  # a candidate the device cannot run (e.g. too large for the level kernel)
                 log(f"  {label}: {name} skipped: {e}")
+        for name, (ms, _) in results.items():
+            log(f"    {label} {name}: " + " ".join(f"{x:.4f}" for x in ms) + " ms/iteration per level")
         for lv, factor in enumerate(stage["shrink_factors"]):
             key = level_key(g, factor, dim, stage["cc_radius"], 3.0)
             default_ms = results["models"][0][lv]
