@@ -364,7 +364,15 @@ def run_batched(args) -> int:
     with ClockSampler(local) as clk:
         t_bat = timed(batched)
     launches = (S.launch_count() - launches0) // max(args.warmup + args.steps, 1) * args.steps
+    for st in seq:
+        st.reset_profile()
     t_seq = timed(sequential)
+    # the sequential arm's time per pyramid level (all pairs, per step): what batching can remove is
+    # bounded by the share of the levels whose launches leave the GPU idle
+    seq_level_ms = [0.0] * len(BATCH_STAGE["iterations"])
+    for st in seq:
+        for lv in st.level_profile():
+            seq_level_ms[lv["level"]] += lv["iterate_ms"] / (args.warmup + args.steps)
     # the two arms compute the same fields (each pair's result does not depend on the batch)
     same = all(bool(torch.equal(torch.from_numpy(x.fields()[0]), torch.from_numpy(y.fields()[0])))
                for x, y in zip(seq, bat))
@@ -387,6 +395,7 @@ def run_batched(args) -> int:
                            "l2": "flushed between steps (256 MB)", "parallelism": f"replicas x{ws}",
                            "sequential_pairs_per_hour": pph_seq, "speedup_vs_sequential": pph / pph_seq,
                            "sequential_ms_per_step": 1000.0 * t_seq_all / args.steps,
+                           "sequential_level_ms_per_step": [round(x, 2) for x in seq_level_ms],
                            "fields_identical_to_sequential": same},
                 "clocks": clk.summary(), "gpu_launches": int(launches)}
         print(json.dumps(line), flush=True)
