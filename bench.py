@@ -61,8 +61,8 @@ BYTES_PER_ITER_VOXEL = 176
 BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel: read psi, gather phi, write psi
 ROOF_LEVEL = 3  # the 182x218x182 level: one iteration graph per replay
 # DRAM bytes (read + write) of one replay of that iteration graph, from the ncu capture summarised
-# in profiles/iteration_graph_182x218x182.md
-ITER_GRAPH_TRAFFIC_BYTES = 3.820e9  # 2.419 GB read + 1.401 GB written (mean of two replays)
+# in profiles/iteration_graph_182x218x182.md (one pass per graph, every replay of two registrations)
+ITER_GRAPH_TRAFFIC_BYTES = 2.902e9  # 1.786 GB read + 1.116 GB written (mean of 40 replays)
 
 
 DATA = "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field"
