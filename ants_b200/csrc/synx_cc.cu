@@ -69,10 +69,10 @@ static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, flo
 }
 
 // z-chunk of one CC block.  Each block first fills its z window (2R slices, column updates only,
-// about a third of a full slice's work each), then marches its chunk; 3 blocks are resident per
-// SM at R = 4.  The chunk count minimises waves x (chunk + warm-up cost), so the last wave is not
-// mostly empty.  A tile plan may fix the number of chunks instead (at most nz / R, chunks of at
-// least R slices).
+// about a third of a full slice's work each), then marches its chunk; 2 blocks are resident per
+// SM.  The chunk count minimises waves x (chunk + warm-up cost), so the last wave is not mostly
+// empty (e.g. 182 slices over 6 x 28 tiles: 7 chunks, 1176 blocks = 3.97 waves of 296).  A tile
+// plan may fix the number of chunks instead (at most nz / R, chunks of at least R slices).
 static int cc_max_chunks(const GridInfo& g, int radius) {
   return g.d.dim == 2 ? 1 : std::max(1, g.d.nz / std::max(radius, 1));
 }
@@ -86,9 +86,7 @@ static int cc_zchunk(const GridInfo& g, int radius, int chunks = 0) {
     return (nz + chunks - 1) / chunks;
   }
   const int bxy = ((g.d.nx + 31) / 32) * ((g.d.ny + 7) / 8);
-  // resident blocks: shared memory (the tile's, plus 1 KB the SM reserves per block) and 64 registers
-  const int per_sm = std::max(1, std::min(4, (int)((228 * 1024) / (cc_smem_bytes(3, radius, false) + 1024))));
-  const int slots = per_sm * 148;
+  const int slots = 2 * 148;
   int best_zc = nz;
   double best = 1e30;
   for (int c = 1; c <= max_chunks; ++c) {
@@ -116,10 +114,10 @@ int cc_blocks_max(const GridInfo& g, int radius) {
 
 size_t cc_smem_bytes(int dim, int radius, bool masked) {
   // CCShape<R, DIM, double, masked>::smem for a run-time radius
-  const size_t TX = 32, TY = 8, HX = TX + 2 * radius, HY = TY + 2 * radius;
-  const size_t GR = dim == 3 ? radius + 2 : 1, GC = (TX + 2) * (TY + 2);
+  const size_t TX = 32, TY = 8, HX = TX + 2 * radius, HY = TY + 2 * radius, HC = HX * HY;
+  const size_t RD = dim == 3 ? 2 * radius + 1 : 1;
   const size_t nq = masked ? 6 : 5;
-  return GR * GC * 8 + nq * HY * (HX | 1) * 8 + nq * HY * (TX + 1) * 8 + nq * TY * TX * 8 + (masked ? GR * GC : 0);
+  return RD * HC * 8 + nq * HY * (HX | 1) * 8 + nq * HY * (TX + 1) * 8 + (masked ? RD * HC : 0);
 }
 
 template <int R, int DIM>

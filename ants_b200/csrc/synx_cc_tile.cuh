@@ -13,9 +13,9 @@ namespace synx {
 // Neighbourhood cross-correlation: value and both update directions.
 //
 // A block owns a 32 x 8 tile of output columns and marches along z over a chunk of ZC
-// slices.  FP64 running z-window sums of F, M, F^2, M^2, FM per halo column live in shared
-// memory (each thread updates its own columns); the slice leaving the window is read again
-// (an L2 hit) and subtracted, the entering one added.  Per slice the column sums
+// slices.  Each thread keeps FP64 running z-window sums of F, M, F^2, M^2, FM for up to CPT
+// halo columns; the raw (F, M) values of the last 2R+1 slices sit in a shared-memory ring so
+// the leaving slice is subtracted without a second global read.  Per slice the column sums
 // are box-summed along x and then y in shared memory (FP64) with sliding windows: along x one
 // thread per (quantity, halo row, half of the 32 outputs), along y one thread per (quantity,
 // output column) walking the 8 output rows; the rows of both staging arrays have an odd pitch,
@@ -50,28 +50,18 @@ __device__ __forceinline__ float grad1(float vm, float v0, float vp, int pos, in
 
 // With metric masks (MASKED) a sixth quantity, the count of valid voxels, is box-summed beside the
 // five sums, and a byte ring holds the validity of the ring's slices.
-// Shared memory of one tile.  The running z-window column sums live in shared memory (cs,
-// persistent across the slices of the chunk), so they cost no registers; the value leaving the z
-// window is read again from global memory (an L2 hit: the block loaded it 2R + 1 slices earlier)
-// instead of being kept in a ring.  Only the values the centre differences and the centre itself
-// need, slices z - 1 .. z + R of the tile's interior and a one-voxel rim, stay in a small ring.
-// With metric masks (MASKED) a sixth quantity, the count of valid voxels, is box-summed beside the
-// five sums, and a byte ring holds the centre validity.
 template <int R, int DIM, typename T = double, bool MASKED = false>
 struct CCShape {
   static constexpr int TX = 32, TY = 8;
   static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HC = HX * HY;
   static constexpr int RZ = DIM == 3 ? R : 0;
-  static constexpr int GR = DIM == 3 ? RZ + 2 : 1;   // ring slots: slices z - 1 .. z + RZ
-  static constexpr int GX = TX + 2, GY = TY + 2;      // ring columns: interior and a one-voxel rim
-  static constexpr int GC = GX * GY;
+  static constexpr int RD = 2 * RZ + 1;
   static constexpr int CPT = (HC + 255) / 256;
   static constexpr int NQ = MASKED ? 6 : 5;
   static constexpr int CSP = HX | 1;   // row pitch of the column sums (odd)
   static constexpr int XSP = TX + 1;   // row pitch of the x box sums (odd)
-  static constexpr size_t smem = (size_t)GR * GC * sizeof(float2) + (size_t)NQ * HY * CSP * sizeof(T) +
-                                 (size_t)NQ * HY * XSP * sizeof(T) + (size_t)NQ * TY * TX * sizeof(T) +
-                                 (MASKED ? (size_t)GR * GC : 0);
+  static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)NQ * HY * CSP * sizeof(T) +
+                                 (size_t)NQ * HY * XSP * sizeof(T) + (MASKED ? (size_t)RD * HC : 0);
 };
 
 // One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
@@ -94,13 +84,13 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
                                           float* __restrict__ cc_out, int bx, int by, int bz,
                                           unsigned char* smem_raw, double* red, double* valid_count = nullptr) {
   using S = CCShape<R, DIM, T, MASKED>;
-  constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, CPT = S::CPT;
-  constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY, NQ = S::NQ, GR = S::GR, GX = S::GX, GC = S::GC;
-  float2* ring = reinterpret_cast<float2*>(smem_raw);  // [GR][GC]
-  T* cs = reinterpret_cast<T*>(ring + GR * GC);       // [NQ][HY][CSP] running column sums
-  T* xs = cs + NQ * HY * CSP;                          // [NQ][HY][XSP]
-  T* ys = xs + NQ * HY * XSP;                          // [NQ][TY][TX]
-  unsigned char* vring = reinterpret_cast<unsigned char*>(ys + NQ * TY * TX);  // [GR][GC] (MASKED)
+  constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
+  constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY, NQ = S::NQ;
+  float2* ring = reinterpret_cast<float2*>(smem_raw);
+  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [NQ][HY][CSP]; reused as ys [NQ][TY][TX] after the x pass
+  T* xs = cs + NQ * HY * CSP;                     // [NQ][HY][XSP]
+  T* ys = cs;
+  unsigned char* vring = reinterpret_cast<unsigned char*>(xs + NQ * HY * XSP);  // [RD][HC] (MASKED)
   const unsigned char* __restrict__ valid = P.valid;
 
   const int tid = threadIdx.x;
@@ -110,8 +100,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   const int z0 = bz * P.ZC;
   const int z1 = min(z0 + P.ZC, nz);
 
-  // owned halo columns: global offset, column-sum slot, ring slot (-1: outside the ring's region)
-  int gofs[CPT], sofs[CPT], rofs[CPT];
+  // owned halo columns
+  int gofs[CPT], sofs[CPT];
   bool gval[CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) {
@@ -121,17 +111,18 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     gval[c] = col < HC && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
     gofs[c] = gval[c] ? gy * nx + gx : 0;
     sofs[c] = hy * CSP + hx;
-    const int rx = hx - (R - 1), ry = hy - (R - 1);
-    rofs[c] = (col < HC && rx >= 0 && rx < GX && ry >= 0 && ry < S::GY) ? ry * GX + rx : -1;
-    if (col < HC)
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) cs[q * HY * CSP + sofs[c]] = T(0);
   }
+  // sliding-window tasks: x pass (quantity, half, halo row), y pass (quantity, output column)
+  T acc[CPT][NQ];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[c][q] = T(0);
 
   // warm-up: slices z0-RZ .. z0+RZ-1
   for (int zs = z0 - RZ; zs < z0 + RZ; ++zs) {
     const bool zin = zs >= 0 && zs < nz;
-    const int slot = pmod(zs, GR);
+    const int slot = pmod(zs, RD);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
       int col = tid + c * 256;
@@ -145,19 +136,16 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
           vb = MASKED ? __ldg(valid + o) : 1;
           if (vb) {
             const T f = v.x, m = v.y;
-            T* q = cs + sofs[c];
-            q[0] += f;
-            q[HY * CSP] += m;
-            q[2 * HY * CSP] += f * f;
-            q[3 * HY * CSP] += m * m;
-            q[4 * HY * CSP] += f * m;
-            if (MASKED) q[(NQ - 1) * HY * CSP] += T(1);
+            acc[c][0] += f;
+            acc[c][1] += m;
+            acc[c][2] += f * f;
+            acc[c][3] += m * m;
+            acc[c][4] += f * m;
+            if (MASKED) acc[c][NQ - 1] += T(1);
           }
         }
-        if (rofs[c] >= 0) {
-          ring[slot * GC + rofs[c]] = v;
-          if (MASKED) vring[slot * GC + rofs[c]] = vb;
-        }
+        ring[slot * HC + col] = v;
+        if (MASKED) vring[slot * HC + col] = vb;
       }
     }
   }
@@ -186,7 +174,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   for (int zc = z0; zc < z1; ++zc) {
     // slide the z window: subtract slice zc-RZ-1 (if it was added), add slice zc+RZ
     const int ze = zc + RZ, zl = zc - RZ - 1;
-    const int slot = pmod(ze, GR);
+    const int slot = pmod(ze, RD);
     const bool sub = zc > z0 && zl >= 0;
     const bool zin = ze < nz;
     const bool znext = zc + 1 < z1 && ze + 1 < nz;
@@ -194,34 +182,31 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     for (int c = 0; c < CPT; ++c) {
       int col = tid + c * 256;
       if (col < HC) {
-        T* q = cs + sofs[c];
-        if (sub && gval[c]) {
-          const long long o = (long long)zl * nxy + gofs[c];
-          if (!MASKED || __ldg(valid + o)) {
-            const T f = __ldg(Ft + o), m = __ldg(Mt + o);
-            q[0] -= f;
-            q[HY * CSP] -= m;
-            q[2 * HY * CSP] -= f * f;
-            q[3 * HY * CSP] -= m * m;
-            q[4 * HY * CSP] -= f * m;
-            if (MASKED) q[(NQ - 1) * HY * CSP] -= T(1);
-          }
+        if (sub && gval[c] && (!MASKED || vring[slot * HC + col])) {
+          float2 o = ring[slot * HC + col];
+          const T f = o.x, m = o.y;
+          acc[c][0] -= f;
+          acc[c][1] -= m;
+          acc[c][2] -= f * f;
+          acc[c][3] -= m * m;
+          acc[c][4] -= f * m;
+          if (MASKED) acc[c][NQ - 1] -= T(1);
         }
         const float2 v = nv[c];  // zero outside the volume
         const unsigned char vb = MASKED ? nvb[c] : 1;
         if (zin && gval[c] && vb) {
           const T f = v.x, m = v.y;
-          q[0] += f;
-          q[HY * CSP] += m;
-          q[2 * HY * CSP] += f * f;
-          q[3 * HY * CSP] += m * m;
-          q[4 * HY * CSP] += f * m;
-          if (MASKED) q[(NQ - 1) * HY * CSP] += T(1);
+          acc[c][0] += f;
+          acc[c][1] += m;
+          acc[c][2] += f * f;
+          acc[c][3] += m * m;
+          acc[c][4] += f * m;
+          if (MASKED) acc[c][NQ - 1] += T(1);
         }
-        if (rofs[c] >= 0) {
-          ring[slot * GC + rofs[c]] = v;
-          if (MASKED) vring[slot * GC + rofs[c]] = (zin && gval[c]) ? vb : 0;
-        }
+        ring[slot * HC + col] = v;
+        if (MASKED) vring[slot * HC + col] = (zin && gval[c]) ? vb : 0;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) cs[q * HY * CSP + sofs[c]] = acc[c][q];
         nv[c] = make_float2(0.0f, 0.0f);
         if (MASKED) nvb[c] = 0;
         if (znext && gval[c]) {
@@ -268,9 +253,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       }
     }
     __syncthreads();
-    const int cidx = (ty + 1) * GX + (tx + 1);
-    const int cslot = pmod(zc, GR);
-    const bool center_ok = out_ok && (!MASKED || vring[cslot * GC + cidx]);
+    const int cidx = (ty + R) * HX + (tx + R);
+    const bool center_ok = out_ok && (!MASKED || vring[pmod(zc, RD) * HC + cidx]);
     if (MASKED && out_ok && !center_ok) {  // a masked-out voxel: no value, no update
       const long long oi = (long long)zc * nxy + (long long)oy * nx + ox;
 #pragma unroll
@@ -289,7 +273,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       const T sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
       const T sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
       const T sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
-      const float2* rc = ring + cslot * GC;
+      const float2* rc = ring + pmod(zc, RD) * HC;
       const float2 v0 = rc[cidx];
       const T fh = (T)v0.x - mF, mh = (T)v0.y - mM;
       T cc = T(1), aF = T(0), aM = T(0);
@@ -308,12 +292,12 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         const float2 xm = rc[cidx - 1], xp = rc[cidx + 1];
         gMi[0] = grad1(xm.y, v0.y, xp.y, ox, nx, P.h[0]);
         gFi[0] = grad1(xm.x, v0.x, xp.x, ox, nx, P.h[0]);
-        const float2 ym = rc[cidx - GX], yp = rc[cidx + GX];
+        const float2 ym = rc[cidx - HX], yp = rc[cidx + HX];
         gMi[1] = grad1(ym.y, v0.y, yp.y, oy, ny, P.h[1]);
         gFi[1] = grad1(ym.x, v0.x, yp.x, oy, ny, P.h[1]);
         gMi[2] = gFi[2] = 0.0f;
         if (DIM == 3) {
-          const float2 zm = ring[pmod(zc - 1, GR) * GC + cidx], zp = ring[pmod(zc + 1, GR) * GC + cidx];
+          const float2 zm = ring[pmod(zc - 1, RD) * HC + cidx], zp = ring[pmod(zc + 1, RD) * HC + cidx];
           gMi[2] = grad1(zm.y, v0.y, zp.y, zc, nz, P.h[2]);
           gFi[2] = grad1(zm.x, v0.x, zp.x, zc, nz, P.h[2]);
         }
@@ -342,8 +326,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     __syncthreads();
   }
   if (MASKED) {
-    const double nv_ = block_sum_d(n_valid, red);
-    if (tid == 0 && valid_count) *valid_count = nv_;
+    const double nv = block_sum_d(n_valid, red);
+    if (tid == 0 && valid_count) *valid_count = nv;
     __syncthreads();  // red is reused below
   }
   return block_sum_d(cc_acc, red);
