@@ -16,6 +16,7 @@ template <int R, int DIM, typename T, bool MASKED = false>
 __global__ void __launch_bounds__(256)
     k_cc(const float* __restrict__ Ft, const float* __restrict__ Mt, Dims d, CCParams P, float* __restrict__ gF,
          float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
@@ -59,12 +60,12 @@ template <int R, int DIM>
 static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, float* gF, float* gM, double* partials,
                         IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P, bool fp32) {
   if (P.valid != nullptr)
-    k_cc<R, DIM, double, true><<<grid, 256, CCShape<R, DIM, double, true>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials,
+    launch_k(k_cc<R, DIM, double, true>, grid, 256, CCShape<R, DIM, double, true>::smem, s, Ft, Mt, g.d, P, gF, gM, partials,
                                                                                      ctl, cc_out);
   else if (fp32)
-    k_cc<R, DIM, float><<<grid, 256, CCShape<R, DIM, float>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
+    launch_k(k_cc<R, DIM, float>, grid, 256, CCShape<R, DIM, float>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
   else
-    k_cc<R, DIM, double><<<grid, 256, CCShape<R, DIM, double>::smem, s>>>(Ft, Mt, g.d, P, gF, gM, partials, ctl,
+    launch_k(k_cc<R, DIM, double>, grid, 256, CCShape<R, DIM, double>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl,
                                                                           cc_out);
 }
 

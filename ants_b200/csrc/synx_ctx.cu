@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/synx.h"
@@ -166,6 +167,7 @@ struct synx_ctx {
   bool own_stream = false;
   cudaStream_t aux = nullptr;        // captures the inverse loop bodies of the level graphs
   bool loop_graphs_failed = false;   // the driver refused conditional nodes: graphs use plain launches
+  bool pdl_failed = false;           // the driver refused programmatic edges in a captured graph
   std::string err;
   bool images_set = false;
   synx_geom geF{}, geM{};
@@ -631,9 +633,23 @@ void smooth_halves(synx_ctx* c, const float* const* in, float* const* out, const
 // graph): each fixed-point inverse becomes its k = 0 launch followed by a conditional WHILE node
 // whose body is one sub-iteration launch plus the loop-control kernel, instead of all
 // max_iter + 1 launches of which the converged tail does nothing.
-cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
+// Scope in which the library's launches use programmatic dependent launch (see launch_k).
+struct PdlScope {
+  int saved;
+  explicit PdlScope(bool on) : saved(t_pdl) {
+    t_pdl = on ? 1 : 0;
+    t_pdl_skip = 1;  // the first launch follows whatever came before the iteration
+  }
+  ~PdlScope() {
+    t_pdl = saved;
+    t_pdl_skip = 0;
+  }
+};
+
+cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false, bool with_pdl = true) {
   const GridInfo& g = c->cur_grid;
   cudaStream_t s = c->stream;
+  PdlScope pdl(with_pdl && !profile && !c->pdl_failed && (c->P.flags & SYNX_F_NO_PDL) == 0);
   auto ev = [&](void) -> int {
     if (c->ev_used >= c->ev_pool.size()) {
       cudaEvent_t e;
@@ -742,10 +758,13 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false) {
     if ((e = cudaStreamBeginCaptureToGraph(c->aux, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                            cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return e;
+    t_pdl_skip = 1;  // the body's first kernel has no kernel before it
     sub(-1, c->aux);
     control(h, false, c->aux);
     cudaGraph_t body = nullptr;
-    return cudaStreamEndCapture(c->aux, &body);
+    e = cudaStreamEndCapture(c->aux, &body);
+    t_pdl_skip = 1;  // the next launch on s follows the conditional node
+    return e;
   };
   {
     const float* phi[2] = {c->phiF, c->phiM};
@@ -983,10 +1002,17 @@ int level_iterate(synx_ctx* c, int level) {
       }
       // with the inverse loops as conditional nodes first; if the driver refuses them, again
       // with plain launches
-      for (bool loops : {!c->loop_graphs_failed, false}) {
+      // attempts: conditional loops with programmatic dependent launch, then without PDL (a driver
+      // that refuses programmatic edges in captured graphs), then plain launches
+      const bool pdl0 = !c->pdl_failed && (c->P.flags & SYNX_F_NO_PDL) == 0;
+      const bool loops0 = !c->loop_graphs_failed;
+      const std::pair<bool, bool> tries[3] = {{loops0, pdl0}, {loops0, false}, {false, false}};
+      for (int tr = 0; tr < 3; ++tr) {
+        const bool loops = tries[tr].first, with_pdl = tries[tr].second;
+        if (tr > 0 && tries[tr] == tries[tr - 1]) continue;
         const long long before = launch_count();
         CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t eq = enqueue_iteration(c, false, loops);
+        const cudaError_t eq = enqueue_iteration(c, false, loops, with_pdl);
         cudaGraph_t graph = nullptr;
         const cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
         c->graph_nodes[level] = launch_count() - before;
@@ -1005,8 +1031,9 @@ int level_iterate(synx_ctx* c, int level) {
           }
         }
         cudaGetLastError();
-        if (!loops) return set_err(c, SYNX_E_CUDA, std::string("level graph: ") + cudaGetErrorString(e));
-        c->loop_graphs_failed = true;
+        if (!loops && !with_pdl) return set_err(c, SYNX_E_CUDA, std::string("level graph: ") + cudaGetErrorString(e));
+        if (with_pdl) c->pdl_failed = true;
+        else c->loop_graphs_failed = true;
       }
     }
     for (int k = 0; k < iters; ++k) CUDA_TRY(c, cudaGraphLaunch(c->gexec_lv[level], c->stream));

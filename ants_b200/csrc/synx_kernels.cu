@@ -21,6 +21,9 @@
 
 namespace synx {
 
+thread_local int t_pdl = 0;
+thread_local int t_pdl_skip = 0;
+
 // Process-wide count of kernel launches issued by this library (instrumentation).
 std::atomic<long long> g_launches{0};
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -229,6 +232,7 @@ void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s) {
 // ------------------------------------------------------------------------------------------
 template <int DIM, bool DIAG>
 __global__ void __launch_bounds__(256) k_warp_pair(const WarpArgs a, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && ctl != nullptr) {
     ctl->maxnorm[0] = 0u;  // the update scaling of this iteration starts from zero
@@ -245,11 +249,11 @@ void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, con
   a.zb = m.zb;
   const bool dg = affine_diag(a.mF) && affine_diag(a.mM);
   if (gv.d.dim == 3) {
-    if (dg) k_warp_pair<3, true><<<m.grid, 256, 0, s>>>(a, ctl);
-    else k_warp_pair<3, false><<<m.grid, 256, 0, s>>>(a, ctl);
+    if (dg) launch_k(k_warp_pair<3, true>, m.grid, 256, 0, s, a, ctl);
+    else launch_k(k_warp_pair<3, false>, m.grid, 256, 0, s, a, ctl);
   } else {
-    if (dg) k_warp_pair<2, true><<<m.grid, 256, 0, s>>>(a, ctl);
-    else k_warp_pair<2, false><<<m.grid, 256, 0, s>>>(a, ctl);
+    if (dg) launch_k(k_warp_pair<2, true>, m.grid, 256, 0, s, a, ctl);
+    else launch_k(k_warp_pair<2, false>, m.grid, 256, 0, s, a, ctl);
   }
 }
 
@@ -424,6 +428,7 @@ __global__ void __launch_bounds__(256) k_mask_validity(const unsigned char* __re
                                                        const unsigned char* __restrict__ mM, Dims dM, Affine aM,
                                                        const float* __restrict__ psiM, Dims dv, int zb,
                                                        unsigned char* __restrict__ valid, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   const Coord3 c = coord3(dv, zb, 1);
   if (!c.ok) return;
@@ -451,9 +456,9 @@ void launch_mask_validity(const unsigned char* mF, const GridInfo& gmF, const fl
   const Affine aF = make_affine(gv, gmF), aM = make_affine(gv, gmM);
   const Map3 m = map3(gv.d);
   if (gv.d.dim == 3)
-    k_mask_validity<3><<<m.grid, 256, 0, s>>>(mF, gmF.d, aF, psiF, mM, gmM.d, aM, psiM, gv.d, m.zb, valid, ctl);
+    launch_k(k_mask_validity<3>, m.grid, 256, 0, s, mF, gmF.d, aF, psiF, mM, gmM.d, aM, psiM, gv.d, m.zb, valid, ctl);
   else
-    k_mask_validity<2><<<m.grid, 256, 0, s>>>(mF, gmF.d, aF, psiF, mM, gmM.d, aM, psiM, gv.d, m.zb, valid, ctl);
+    launch_k(k_mask_validity<2>, m.grid, 256, 0, s, mF, gmF.d, aF, psiF, mM, gmM.d, aM, psiM, gv.d, m.zb, valid, ctl);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -467,6 +472,7 @@ constexpr int kSmoothTileY = 64;
 
 template <int DIM, int R>
 __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ __align__(16) float sm3[];
   __shared__ float red[32];
@@ -485,6 +491,7 @@ __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, 
 // xy-smoothed fields for the z kernel; the arithmetic is k_smooth_xy's (the same bits).
 template <int R, int TY>
 __global__ void __launch_bounds__(256) k_smooth_xy_pipe(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R, RPT = TY / 8;
   constexpr int TILE = 3 * HY * HXP;
@@ -535,6 +542,7 @@ template <int R>
 // the ring lives in shared memory ((2R+1) x 3 x 256 floats, smooth_z_smem_bytes), so few registers
 // are needed: 5 resident blocks per SM up to R = 6 (40 KB of ring each), 3 up to R = 12
 __global__ void __launch_bounds__(256, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ float zring[];
   __shared__ float red[32];
@@ -558,6 +566,7 @@ __global__ void __launch_bounds__(256, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth
 // slices of each chunk.  The arithmetic and its order are those of the two-kernel path: the same bits.
 template <int R, int TY>
 __global__ void __launch_bounds__(256) k_smooth_slab(const Smooth3Args a, Dims d, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   constexpr int K = 2 * R + 1, RPT = TY / 8;
   extern __shared__ __align__(16) float sms[];
@@ -751,9 +760,9 @@ static void launch_smooth_slab(const Smooth3Args& a0, const GridInfo& g, int RR,
 #define SYNX_SSLAB(RV)                                                              \
   case RV:                                                                          \
     if (TY == 16)                                                                   \
-      k_smooth_slab<RV, 16><<<grid, 256, smooth_slab_smem_bytes(RV, 16), s>>>(a, g.d, ctl); \
+      launch_k(k_smooth_slab<RV, 16>, grid, 256, smooth_slab_smem_bytes(RV, 16), s, a, g.d, ctl); \
     else                                                                            \
-      k_smooth_slab<RV, 8><<<grid, 256, smooth_slab_smem_bytes(RV, 8), s>>>(a, g.d, ctl);   \
+      launch_k(k_smooth_slab<RV, 8>, grid, 256, smooth_slab_smem_bytes(RV, 8), s, a, g.d, ctl);   \
     break;
   (void)smem;
   switch (RR) {
@@ -819,9 +828,9 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
 #define SYNX_SXYP(RV)                                                                           \
   case RV:                                                                                      \
     if (TY == 64)                                                                               \
-      k_smooth_xy_pipe<RV, 64><<<gp, 256, smooth_xy_pipe_smem_bytes(RV, 64), s>>>(ap, g.d, ctl); \
+      launch_k(k_smooth_xy_pipe<RV, 64>, gp, 256, smooth_xy_pipe_smem_bytes(RV, 64), s, ap, g.d, ctl); \
     else                                                                                        \
-      k_smooth_xy_pipe<RV, 32><<<gp, 256, smooth_xy_pipe_smem_bytes(RV, 32), s>>>(ap, g.d, ctl); \
+      launch_k(k_smooth_xy_pipe<RV, 32>, gp, 256, smooth_xy_pipe_smem_bytes(RV, 32), s, ap, g.d, ctl); \
     break;
     switch (RR) {
       SYNX_SXYP(1)
@@ -847,9 +856,9 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
 #define SYNX_SXY(RV)                                             \
   case RV:                                                       \
     if (dim == 3)                                                \
-      k_smooth_xy<3, RV><<<gxy, 256, smem, s>>>(a, g.d, ctl);    \
+      launch_k(k_smooth_xy<3, RV>, gxy, 256, smem, s, a, g.d, ctl);    \
     else                                                         \
-      k_smooth_xy<2, RV><<<gxy, 256, smem, s>>>(a, g.d, ctl);    \
+      launch_k(k_smooth_xy<2, RV>, gxy, 256, smem, s, a, g.d, ctl);    \
     break;
   switch (RR) {
     SYNX_SXY(1)
@@ -883,7 +892,7 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   count_launch();
 #define SYNX_SZ(RV)                                    \
   case RV:                                             \
-    k_smooth_z<RV><<<gz, 256, smooth_z_smem_bytes(RV), s>>>(a, g.d, ctl);    \
+    launch_k(k_smooth_z<RV>, gz, 256, smooth_z_smem_bytes(RV), s, a, g.d, ctl);    \
     break;
   switch (RR) {
     SYNX_SZ(1)
@@ -910,6 +919,7 @@ template <int DIM>
 __global__ void __launch_bounds__(256)
     k_smooth_pass(Ptr2c in, Ptr2 out, Ptr2c orig, Dims d, int zb, int axis, const float* __restrict__ coeffs, int R,
                   int last, float w1, float w2, int do_max, float ihx, float ihy, float ihz, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   __shared__ float red[32];
   const Coord3 c3 = coord3(d, zb, gridDim.z / ((d.nz + zb - 1) / zb));
@@ -966,10 +976,10 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
   const Map3 m = map3(g.d, halves);
   float ih[3] = {(float)(1.0 / g.sp[0]), (float)(1.0 / g.sp[1]), (float)(1.0 / g.sp[2])};
   if (g.d.dim == 3)
-    k_smooth_pass<3><<<m.grid, 256, 0, s>>>(pi, po, pg, g.d, m.zb, axis, coeffs, R, last ? 1 : 0, w1, w2,
+    launch_k(k_smooth_pass<3>, m.grid, 256, 0, s, pi, po, pg, g.d, m.zb, axis, coeffs, R, last ? 1 : 0, w1, w2,
                                             maxnorm ? 1 : 0, ih[0], ih[1], ih[2], ctl);
   else
-    k_smooth_pass<2><<<m.grid, 256, 0, s>>>(pi, po, pg, g.d, m.zb, axis, coeffs, R, last ? 1 : 0, w1, w2,
+    launch_k(k_smooth_pass<2>, m.grid, 256, 0, s, pi, po, pg, g.d, m.zb, axis, coeffs, R, last ? 1 : 0, w1, w2,
                                             maxnorm ? 1 : 0, ih[0], ih[1], ih[2], ctl);
 }
 
@@ -979,6 +989,7 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
 // ------------------------------------------------------------------------------------------
 template <int DIM, bool DIAG>
 __global__ void __launch_bounds__(256) k_compose(const ComposeArgs a, int halves, IterCtl* ctl) {
+  griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   const int gz = gridDim.z / halves;
   const int h = blockIdx.z / gz;
@@ -999,11 +1010,11 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
   a.zb = m.zb;
   const bool dg = affine_diag(a.m);
   if (g.d.dim == 3) {
-    if (dg) k_compose<3, true><<<m.grid, 256, 0, s>>>(a, halves, ctl);
-    else k_compose<3, false><<<m.grid, 256, 0, s>>>(a, halves, ctl);
+    if (dg) launch_k(k_compose<3, true>, m.grid, 256, 0, s, a, halves, ctl);
+    else launch_k(k_compose<3, false>, m.grid, 256, 0, s, a, halves, ctl);
   } else {
-    if (dg) k_compose<2, true><<<m.grid, 256, 0, s>>>(a, halves, ctl);
-    else k_compose<2, false><<<m.grid, 256, 0, s>>>(a, halves, ctl);
+    if (dg) launch_k(k_compose<2, true>, m.grid, 256, 0, s, a, halves, ctl);
+    else launch_k(k_compose<2, false>, m.grid, 256, 0, s, a, halves, ctl);
   }
 }
 
@@ -1024,6 +1035,7 @@ template <int DIM, bool DIAG>
 __global__ void __launch_bounds__(256, 4) k_invert_step(const InvArgs a, InvLaunch L, IterCtl* ctl,
                                                         double* __restrict__ psum, float* __restrict__ pmax,
                                                         int pcap) {
+  griddep_wait();
   if (L.stop_aware && ctl->stop) return;
   __shared__ double redd[32];
   __shared__ float redf[32];
@@ -1127,11 +1139,11 @@ void launch_invert_step(const float* const* phi, float* const* psi, int halves, 
   const bool dg = affine_diag(am);
   const dim3 grid((unsigned)(nb * halves));
   if (g.d.dim == 3) {
-    if (dg) k_invert_step<3, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
-    else k_invert_step<3, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    if (dg) launch_k(k_invert_step<3, true>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    else launch_k(k_invert_step<3, false>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   } else {
-    if (dg) k_invert_step<2, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
-    else k_invert_step<2, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    if (dg) launch_k(k_invert_step<2, true>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity);
+    else launch_k(k_invert_step<2, false>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity);
   }
 }
 
@@ -1234,6 +1246,7 @@ template <int DIM, bool DIAG>
 __global__ void __launch_bounds__(256, 4) k_invert_spec(const InvArgs a, InvLaunch L, IterCtl* ctl,
                                                         double* __restrict__ psum, float* __restrict__ pmax, int pcap,
                                                         InvList list) {
+  griddep_wait();
   if (L.stop_aware && ctl->stop) return;
   __shared__ double redd[32];
   __shared__ float redf[32];
@@ -1291,6 +1304,7 @@ __global__ void __launch_bounds__(256, 4) k_invert_spec(const InvArgs a, InvLaun
 // block to finish clears the list and the running bound for the next sub-iteration.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_invert_fix(const InvArgs a, InvLaunch L, IterCtl* ctl, InvList list) {
+  griddep_wait();
   if (L.stop_aware && ctl->stop) return;
   __shared__ int am_last;
   const int nb = gridDim.x / L.halves;
@@ -1356,11 +1370,11 @@ void launch_invert_spec(const float* const* phi, float* const* psi, int halves, 
   const bool dg = affine_diag(make_affine(g, g));
   const dim3 grid((unsigned)(nb * halves));
   if (g.d.dim == 3) {
-    if (dg) k_invert_spec<3, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
-    else k_invert_spec<3, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+    if (dg) launch_k(k_invert_spec<3, true>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+    else launch_k(k_invert_spec<3, false>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
   } else {
-    if (dg) k_invert_spec<2, true><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
-    else k_invert_spec<2, false><<<grid, 256, 0, s>>>(a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+    if (dg) launch_k(k_invert_spec<2, true>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
+    else launch_k(k_invert_spec<2, false>, grid, 256, 0, s, a, L, ctl, pb.sum, pb.maxv, pb.capacity, il);
   }
 }
 
@@ -1375,12 +1389,13 @@ void launch_invert_fix(const float* const* phi, float* const* psi, int halves, c
   const InvList il{{list[0], halves > 1 ? list[1] : list[0]}};
   const dim3 grid((unsigned)(kInvFixBlocksPerHalf * halves));
   if (g.d.dim == 3)
-    k_invert_fix<3><<<grid, 256, 0, s>>>(a, L, ctl, il);
+    launch_k(k_invert_fix<3>, grid, 256, 0, s, a, L, ctl, il);
   else
-    k_invert_fix<2><<<grid, 256, 0, s>>>(a, L, ctl, il);
+    launch_k(k_invert_fix<2>, grid, 256, 0, s, a, L, ctl, il);
 }
 
 __global__ void k_inv_spec_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, int init) {
+  griddep_wait();
   InvCtl* C = ctl->inv[phase];
   const int next = init ? 1 : C[0].kdev + 1;
   const int s = next & 1;
@@ -1392,11 +1407,12 @@ __global__ void k_inv_spec_control(IterCtl* ctl, int phase, cudaGraphConditional
 void launch_inv_spec_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, bool init,
                              cudaStream_t s) {
   count_launch();
-  k_inv_spec_control<<<1, 1, 0, s>>>(ctl, phase, handle, max_iter, init ? 1 : 0);
+  launch_k(k_inv_spec_control, 1, 1, 0, s, ctl, phase, handle, max_iter, init ? 1 : 0);
 }
 
 __global__ void k_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter,
                                    int init) {
+  griddep_wait();
   InvCtl* C = ctl->inv[phase];
   unsigned go = 0;
   if (init) {
@@ -1414,20 +1430,21 @@ __global__ void k_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditional
 void launch_inv_loop_control(IterCtl* ctl, int phase, cudaGraphConditionalHandle handle, int max_iter, bool init,
                              cudaStream_t s) {
   count_launch();
-  k_inv_loop_control<<<1, 1, 0, s>>>(ctl, phase, handle, max_iter, init ? 1 : 0);
+  launch_k(k_inv_loop_control, 1, 1, 0, s, ctl, phase, handle, max_iter, init ? 1 : 0);
 }
 
 // ------------------------------------------------------------------------------------------
 // Convergence monitor and per-iteration log (one warp).
 // ------------------------------------------------------------------------------------------
 __global__ void k_converge(IterCtl* ctl, LogDev log, double threshold, int window) {
+  griddep_wait();
   if (ctl->stop) return;
   converge_step(ctl, log, threshold, window);
 }
 
 void launch_converge(IterCtl* ctl, LogDev log, double threshold, int window, cudaStream_t s) {
   count_launch();
-  k_converge<<<1, 32, 0, s>>>(ctl, log, threshold, window);
+  launch_k(k_converge, 1, 32, 0, s, ctl, log, threshold, window);
 }
 
 
@@ -1505,6 +1522,7 @@ __global__ void __launch_bounds__(256) k_resample(Ptr4c in, Dims di, Ptr4 out, D
 }
 
 __global__ void __launch_bounds__(256) k_round_half(Ptr4 f, int nf, long long n) {
+  griddep_wait();
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     for (int k = 0; k < nf; ++k) f.p[k][i] = __half2float(__float2half_rn(f.p[k][i]));
@@ -1515,7 +1533,7 @@ void launch_round_half(float* const* f, int nf, long long n, cudaStream_t s) {
   Ptr4 p{};
   for (int k = 0; k < nf && k < 4; ++k) p.p[k] = f[k];
   const long long blocks = std::min<long long>((n + 255) / 256, 148 * 16);
-  k_round_half<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(p, std::min(nf, 4), n);
+  launch_k(k_round_half, (unsigned)std::max<long long>(blocks, 1), 256, 0, s, p, std::min(nf, 4), n);
 }
 
 void launch_resample_fields(const float* const* in, const GridInfo& gi, float* const* out, const GridInfo& go,

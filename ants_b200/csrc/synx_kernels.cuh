@@ -8,6 +8,32 @@
 
 namespace synx {
 
+// Programmatic dependent launch.  The kernels of one SyN iteration are launched with programmatic
+// stream serialisation when t_pdl is set (the stage sets it while it enqueues an iteration), so a
+// kernel's launch and block scheduling overlap the end of the kernel before it; each such kernel
+// waits at its start (griddep_wait, before touching global memory) until its predecessor has
+// completed and its writes are visible.  Without the attribute the wait returns at once.
+extern thread_local int t_pdl;       // launches from this host thread use the attribute
+extern thread_local int t_pdl_skip;  // the next launch does not (it follows a graph node that is not a kernel)
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  const bool pdl = t_pdl && !t_pdl_skip;
+  t_pdl_skip = 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Fixed-point inverse control block, one per (phase, half).  Slot k%2 holds the decision
 // and statistics consumed by launch k; launch k writes slot (k+1)%2.
 struct InvCtl {

@@ -27,6 +27,7 @@ SYNX_F_CC_FP32_SUMS = 0x8
 SYNX_F_FIELDS_FP16 = 0x10
 SYNX_F_SMOOTH_TWO_PASS = 0x20
 SYNX_F_INV_TWO_PASS = 0x40
+SYNX_F_NO_PDL = 0x80
 SYNX_INJECT_BARRIER_TIMEOUT = 1
 SYNX_INJECT_ALLOC_FAILURE = 2
 

@@ -110,6 +110,8 @@ typedef struct synx_params {
                                        kernel (same results) */
 #define SYNX_F_INV_TWO_PASS 0x40    /* fixed-point inverse with a statistics pass and an update pass per
                                        sub-iteration instead of the single-pass form (same results) */
+#define SYNX_F_NO_PDL 0x80          /* launch an iteration's kernels without programmatic dependent launch
+                                       (same results) */
 
 /* Failure injection for tests (host-side; nothing faults): the level kernel's grid barrier waits for
  * one block more than it launched, with a short poll limit, so the wait runs out, the kernel ends

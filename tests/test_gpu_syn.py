@@ -14,8 +14,8 @@ import pytest
 
 import oracle as O
 from ants_b200 import phantoms
-from ants_b200.synx import (SYNX_F_INV_TWO_PASS, SYNX_F_NO_PERSISTENT, SYNX_F_SMOOTH_TWO_PASS, SYNX_F_USE_GRAPHS, Geom,
-                            SyNParams, SyNStage)
+from ants_b200.synx import (SYNX_F_INV_TWO_PASS, SYNX_F_NO_PDL, SYNX_F_NO_PERSISTENT, SYNX_F_SMOOTH_TWO_PASS,
+                            SYNX_F_USE_GRAPHS, Geom, SyNParams, SyNStage)
 
 pytestmark = pytest.mark.gpu
 
@@ -243,6 +243,26 @@ def test_pipelined_xy_smoothing_matches_bit_for_bit(cuda, uvar, rows):
             st.set_images(f, g, m, g)
             st.run()
             outs.append((st.fields(), [r.metric for r in st.log()]))
+    np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
+    np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
+    assert outs[0][1] == outs[1][1]
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_programmatic_dependent_launch_changes_nothing(cuda, graphs):
+    # an iteration's kernels launched with programmatic dependent launch (the default) and without it
+    # give the same bits, in captured graphs (inverse loops as conditional nodes) and in plain launches
+    f, m = make_pair(3, (44, 39, 35), seed=29)
+    g = Geom((44, 39, 35))
+    outs = []
+    for extra in (0, SYNX_F_NO_PDL):
+        P = SyNParams(dim=3, cc_radius=3, iterations=(6, 4), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0),
+                      convergence_threshold=1e-12,
+                      flags=(SYNX_F_USE_GRAPHS if graphs else 0) | SYNX_F_NO_PERSISTENT | extra)
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.run()
+            outs.append((st.fields(), [(r.metric, r.inverse_iterations) for r in st.log()]))
     np.testing.assert_array_equal(outs[0][0][0], outs[1][0][0])
     np.testing.assert_array_equal(outs[0][0][1], outs[1][0][1])
     assert outs[0][1] == outs[1][1]
