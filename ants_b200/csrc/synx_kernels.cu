@@ -1261,27 +1261,34 @@ __global__ void __launch_bounds__(256, 4) k_invert_spec(const InvArgs a, InvLaun
     return;
   }
   const float eps = k == 0 ? 0.75f : 0.5f;
-  // Seed the running bound before the tiles: every thread evaluates the residual norm of the current
-  // iterate at one voxel of a sample spread over the whole half-field (a multiplicative hash of its
-  // index), exactly as the pass computes it, so the block's maximum of these is a lower bound of the
-  // field's maximum.  Without it the first tiles, before any bound is known, defer most voxels.
+  // Seed the running bound before the tiles: one lane per warp evaluates the residual norm of the
+  // current iterate at one voxel of a sample spread over the whole half-field (a multiplicative hash of
+  // the warp's index; ~4700 voxels at full resolution), exactly as the pass computes it, so the maximum
+  // of these is a lower bound of the field's maximum.  Without it the first tiles, before any bound is
+  // known, defer most of their voxels; with one sample per thread the scattered gathers cost more DRAM
+  // traffic than the deferrals they save.
   {
-    const Dims& d = a.g;
-    const long long N = d.N;
-    const long long j = ((long long)(bid * blockDim.x + threadIdx.x) * 2654435761LL) % N;
-    const int x = (int)(j % d.nx), y = (int)((j / d.nx) % d.ny), z = (int)(j / ((long long)d.nx * d.ny));
-    const float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
-    const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
-    float p[3] = {psi[j], psi[N + j], DIM == 3 ? psi[2 * N + j] : 0.0f};
-    float e[3];
-    inv_residual<DIM, DIAG>(phi, d, a.A, (float)x, (float)y, (float)z, p, e);
-    float s2 = 0.0f;
+    float nrm = 0.0f;
+    if ((threadIdx.x & 31) == 0) {
+      const Dims& d = a.g;
+      const long long N = d.N;
+      const long long w = (long long)bid * (blockDim.x >> 5) + (threadIdx.x >> 5);
+      const long long j = (w * 2654435761LL) % N;
+      const int x = (int)(j % d.nx), y = (int)((j / d.nx) % d.ny), z = (int)(j / ((long long)d.nx * d.ny));
+      const float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
+      const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
+      float p[3] = {psi[j], psi[N + j], DIM == 3 ? psi[2 * N + j] : 0.0f};
+      float e[3];
+      inv_residual<DIM, DIAG>(phi, d, a.A, (float)x, (float)y, (float)z, p, e);
+      float s2 = 0.0f;
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      const float v = e[c] * a.ih[c];
-      s2 += v * v;
+      for (int c = 0; c < DIM; ++c) {
+        const float v = e[c] * a.ih[c];
+        s2 += v * v;
+      }
+      nrm = sqrtf(s2);
     }
-    const float bm = block_max_f(sqrtf(s2), redf);
+    const float bm = block_max_f(nrm, redf);
     if (threadIdx.x == 0) atomicMax(&C.mrun, __float_as_uint(bm));
     __syncthreads();  // redf is reused by the reductions below
   }
