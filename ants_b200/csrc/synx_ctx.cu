@@ -594,8 +594,8 @@ int smooth_images_for_level(synx_ctx* c, int level) {
       launch_conv_image_axis(src, out, g, axis, c->coeff_img + axis * c->coeff_cap, R[axis], c->stream);
       src = out;
     }
-    // the host kernel buffer must outlive the async copy: synchronise before reuse
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    // no synchronisation: a copy from pageable host memory has taken its data when it returns, and the
+    // next image's coefficient upload is ordered after these passes on the stream
   }
   return SYNX_OK;
 }

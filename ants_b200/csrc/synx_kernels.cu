@@ -1600,6 +1600,9 @@ __global__ void __launch_bounds__(256) k_conv_image_axis(const float* __restrict
     const int pos = axis == 0 ? c3.x : (axis == 1 ? c3.y : z);
     const float* line = in + i - pos * astride;
     double s = 0.0;
+    // unrolled so that the taps' loads are issued ahead of the accumulation chain (the order of the
+    // additions, j ascending, is unchanged)
+#pragma unroll 8
     for (int j = 0; j <= 2 * R; ++j) {
       const int q = min(max(pos + j - R, 0), len - 1);
       s += __ldg(coeffs + j) * (double)__ldg(line + q * astride);
