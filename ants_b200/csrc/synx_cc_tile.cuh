@@ -16,12 +16,14 @@ namespace synx {
 // slices.  Each thread keeps FP64 running z-window sums of F, M, F^2, M^2, FM for up to CPT
 // halo columns; the raw (F, M) values of the last 2R+1 slices sit in a shared-memory ring so
 // the leaving slice is subtracted without a second global read.  Per slice the column sums
-// are box-summed along x and then y in shared memory (FP64) with sliding windows: along x one
-// thread per (quantity, halo row, half of the 32 outputs), along y one thread per (quantity,
-// output column) walking the 8 output rows; the rows of both staging arrays have an odd pitch,
-// so the threads of a half-warp, which differ in row, hit distinct banks.  This gives the five
-// window sums of each output voxel, from which the CC terms and derivatives follow.  The
-// in-bounds count is separable (cx*cy*cz) and computed analytically.
+// are box-summed along y and then x in shared memory (FP64) with sliding windows: along y one
+// thread per (quantity, halo column) walking down the 8 output rows, along x one thread per
+// (quantity, output row, 8-output segment); the x pass reads and writes rows of an odd pitch,
+// so the threads of a half-warp, which differ in row, hit distinct banks.  (y first: the x pass
+// then runs over the 8 output rows only, not the 8 + 2R halo rows, and both sliding chains are
+// 2R+1 + 14 additions long.)  This gives the five window sums of each output voxel, from which
+// the CC terms and derivatives follow.  The in-bounds count is separable (cx*cy*cz) and computed
+// analytically.
 //
 // T is the type of the window sums and of the variance terms formed from them: double (the
 // default; the sums of F^2 and M^2 cancel badly in float when the window is nearly flat) or
@@ -58,10 +60,13 @@ struct CCShape {
   static constexpr int RD = 2 * RZ + 1;
   static constexpr int CPT = (HC + 255) / 256;
   static constexpr int NQ = MASKED ? 6 : 5;
-  static constexpr int CSP = HX | 1;   // row pitch of the column sums (odd)
-  static constexpr int XSP = TX + 1;   // row pitch of the x box sums (odd)
+  static constexpr int CSP = HX | 1;   // row pitch of the column sums and of the y box sums (odd)
+  static constexpr int XSP = TX + 1;   // row pitch of the window sums (odd)
+  static constexpr int XSEG = 8;       // outputs per x-pass task
+  static_assert(TX % XSEG == 0, "x segments tile the output row");
+  static_assert(NQ * TY * XSP <= NQ * HY * CSP, "window sums fit in the column sums' space");
   static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)NQ * HY * CSP * sizeof(T) +
-                                 (size_t)NQ * HY * XSP * sizeof(T) + (MASKED ? (size_t)RD * HC : 0);
+                                 (size_t)NQ * TY * CSP * sizeof(T) + (MASKED ? (size_t)RD * HC : 0);
 };
 
 // One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
@@ -87,10 +92,10 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
   constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY, NQ = S::NQ;
   float2* ring = reinterpret_cast<float2*>(smem_raw);
-  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [NQ][HY][CSP]; reused as ys [NQ][TY][TX] after the x pass
-  T* xs = cs + NQ * HY * CSP;                     // [NQ][HY][XSP]
-  T* ys = cs;
-  unsigned char* vring = reinterpret_cast<unsigned char*>(xs + NQ * HY * XSP);  // [RD][HC] (MASKED)
+  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [NQ][HY][CSP] column sums; reused as ws after the y pass
+  T* ys = cs + NQ * HY * CSP;                     // [NQ][TY][CSP] y box sums of the halo columns
+  T* ws = cs;                                     // [NQ][TY][XSP] window sums of the output voxels
+  unsigned char* vring = reinterpret_cast<unsigned char*>(ys + NQ * TY * CSP);  // [RD][HC] (MASKED)
   const unsigned char* __restrict__ valid = P.valid;
 
   const int tid = threadIdx.x;
@@ -217,39 +222,39 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       }
     }
     __syncthreads();
-    // x box sums, sliding along the row: outputs 16 h .. 16 h + 15 of one halo row (one task per
-    // quantity, half and halo row)
-    for (int task = tid; task < NQ * 2 * HY; task += 256) {
-      const int xrow = task % HY, xhalf = (task / HY) & 1, xq = task / (2 * HY);
-      const T* src = cs + xq * HY * CSP + xrow * CSP + 16 * xhalf;
-      T* dst = xs + xq * HY * XSP + xrow * XSP + 16 * xhalf;
+    // y box sums, sliding down one halo column over the TY output rows (one task per quantity and
+    // halo column)
+    for (int task = tid; task < NQ * HX; task += 256) {
+      const int yq = task / HX, ycol = task - yq * HX;
+      const T* src = cs + yq * HY * CSP + ycol;
+      T* dst = ys + yq * TY * CSP + ycol;
+      T s = T(0);
+#pragma unroll
+      for (int j = 0; j <= 2 * R; ++j) s += src[j * CSP];
+      dst[0] = s;
+#pragma unroll
+      for (int y = 1; y < TY; ++y) {
+        s += src[(y + 2 * R) * CSP];
+        s -= src[(y - 1) * CSP];
+        dst[y * CSP] = s;
+      }
+    }
+    __syncthreads();
+    // x box sums, sliding along an output row: outputs XSEG k .. XSEG k + XSEG-1 (one task per
+    // quantity, output row and segment; consecutive threads take consecutive rows)
+    for (int task = tid; task < NQ * TY * (TX / S::XSEG); task += 256) {
+      const int row = task % (NQ * TY), seg = task / (NQ * TY);
+      const T* src = ys + row * CSP + S::XSEG * seg;
+      T* dst = ws + row * XSP + S::XSEG * seg;
       T s = T(0);
 #pragma unroll
       for (int j = 0; j <= 2 * R; ++j) s += src[j];
       dst[0] = s;
 #pragma unroll
-      for (int x = 1; x < 16; ++x) {
+      for (int x = 1; x < S::XSEG; ++x) {
         s += src[x + 2 * R];
         s -= src[x - 1];
         dst[x] = s;
-      }
-    }
-    __syncthreads();
-    // y box sums, sliding down one output column over the TY output rows (one task per quantity
-    // and output column)
-    for (int task = tid; task < NQ * 32; task += 256) {
-      const int ycol = task & 31, yq = task >> 5;
-      const T* src = xs + yq * HY * XSP + ycol;
-      T* dst = ys + yq * TY * TX + ycol;
-      T s = T(0);
-#pragma unroll
-      for (int j = 0; j <= 2 * R; ++j) s += src[j * XSP];
-      dst[0] = s;
-#pragma unroll
-      for (int y = 1; y < TY; ++y) {
-        s += src[(y + 2 * R) * XSP];
-        s -= src[(y - 1) * XSP];
-        dst[y * TX] = s;
       }
     }
     __syncthreads();
@@ -264,7 +269,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     if (center_ok) {
       T Sq[NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) Sq[q] = ys[q * TY * TX + ty * TX + tx];
+      for (int q = 0; q < NQ; ++q) Sq[q] = ws[(q * TY + ty) * XSP + tx];
       const T czn = (T)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
       const T n = MASKED ? Sq[NQ - 1] : cxn * cyn * czn;
       if (MASKED) n_valid += 1.0;
