@@ -12,8 +12,13 @@ namespace synx {
 // the last block sums them in order).
 // With metric masks (MASKED) the partials hold each block's cc sum and, after them, its count of
 // valid voxels; the value is -sum / count.
+// Threads per standalone CC block: 320 = 10 warps own the 640 halo columns of a radius-4 tile two
+// each (256 threads would leave a third column to half of the warps), and the register cap keeps two
+// blocks per SM.
+constexpr int CC_THREADS = 320;
+
 template <int R, int DIM, typename T, bool MASKED = false>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(CC_THREADS, 2)
     k_cc(const float* __restrict__ Ft, const float* __restrict__ Mt, Dims d, CCParams P, float* __restrict__ gF,
          float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out) {
   griddep_wait();
@@ -23,8 +28,8 @@ __global__ void __launch_bounds__(256)
   __shared__ double vcount;
   __shared__ int am_last;
   const int tid = threadIdx.x;
-  const double bs = cc_tile<R, DIM, T, MASKED>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y, blockIdx.z,
-                                               smem_raw, red, &vcount);
+  const double bs = cc_tile<R, DIM, T, MASKED, CC_THREADS>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y,
+                                                           blockIdx.z, smem_raw, red, &vcount);
   const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
   const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (tid == 0) {
@@ -38,7 +43,7 @@ __global__ void __launch_bounds__(256)
   if (am_last) {
     __threadfence();
     double s = 0.0, n = 0.0;
-    for (unsigned b = tid; b < nblocks; b += 256) {
+    for (unsigned b = tid; b < nblocks; b += CC_THREADS) {
       s += __ldcg(partials + b);
       if (MASKED) n += __ldcg(partials + nblocks + b);
     }
@@ -60,12 +65,12 @@ template <int R, int DIM>
 static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, float* gF, float* gM, double* partials,
                         IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P, bool fp32) {
   if (P.valid != nullptr)
-    launch_k(k_cc<R, DIM, double, true>, grid, 256, CCShape<R, DIM, double, true>::smem, s, Ft, Mt, g.d, P, gF, gM, partials,
+    launch_k(k_cc<R, DIM, double, true>, grid, CC_THREADS, CCShape<R, DIM, double, true>::smem, s, Ft, Mt, g.d, P, gF, gM, partials,
                                                                                      ctl, cc_out);
   else if (fp32)
-    launch_k(k_cc<R, DIM, float>, grid, 256, CCShape<R, DIM, float>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
+    launch_k(k_cc<R, DIM, float>, grid, CC_THREADS, CCShape<R, DIM, float>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
   else
-    launch_k(k_cc<R, DIM, double>, grid, 256, CCShape<R, DIM, double>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl,
+    launch_k(k_cc<R, DIM, double>, grid, CC_THREADS, CCShape<R, DIM, double>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl,
                                                                           cc_out);
 }
 

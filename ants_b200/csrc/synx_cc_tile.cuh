@@ -20,10 +20,11 @@ namespace synx {
 // thread per (quantity, halo column) walking down the 8 output rows, along x one thread per
 // (quantity, output row, 8-output segment); the x pass reads and writes rows of an odd pitch,
 // so the threads of a half-warp, which differ in row, hit distinct banks.  (y first: the x pass
-// then runs over the 8 output rows only, not the 8 + 2R halo rows, and both sliding chains are
-// 2R+1 + 14 additions long.)  This gives the five window sums of each output voxel, from which
-// the CC terms and derivatives follow.  The in-bounds count is separable (cx*cy*cz) and computed
-// analytically.
+// then runs over the 8 output rows only, not the 8 + 2R halo rows.  Each task's first window is
+// summed pairwise and each slide adds the difference of the entering and leaving values, so a
+// task's chain of dependent additions is ceil(log2(2R+1)) + 7 long.)  This gives the five
+// window sums of each output voxel, from which the CC terms and derivatives follow.  The
+// in-bounds count is separable (cx*cy*cz) and computed analytically.
 //
 // T is the type of the window sums and of the variance terms formed from them: double (the
 // default; the sums of F^2 and M^2 cancel badly in float when the window is nearly flat) or
@@ -52,13 +53,14 @@ __device__ __forceinline__ float grad1(float vm, float v0, float vp, int pos, in
 
 // With metric masks (MASKED) a sixth quantity, the count of valid voxels, is box-summed beside the
 // five sums, and a byte ring holds the validity of the ring's slices.
-template <int R, int DIM, typename T = double, bool MASKED = false>
+template <int R, int DIM, typename T = double, bool MASKED = false, int NT = 256>
 struct CCShape {
   static constexpr int TX = 32, TY = 8;
   static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HC = HX * HY;
   static constexpr int RZ = DIM == 3 ? R : 0;
   static constexpr int RD = 2 * RZ + 1;
-  static constexpr int CPT = (HC + 255) / 256;
+  static constexpr int CPT = (HC + NT - 1) / NT;  // halo columns per thread
+  static_assert(NT % 32 == 0 && NT >= TX * TY, "a thread per output voxel");
   static constexpr int NQ = MASKED ? 6 : 5;
   static constexpr int CSP = HX | 1;   // row pitch of the column sums and of the y box sums (odd)
   static constexpr int XSP = TX + 1;   // row pitch of the window sums (odd)
@@ -69,9 +71,21 @@ struct CCShape {
                                  (size_t)NQ * TY * CSP * sizeof(T) + (MASKED ? (size_t)RD * HC : 0);
 };
 
-// One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
-// Returns the tile's sum of local cc (valid in thread 0).  All threads of the block must call
-// it; `smem_raw` holds CCShape<R, DIM>::smem bytes and `red` 32 doubles.
+// Sum of the K values src[0], src[stride], ..., src[(K-1) stride], added pairwise (a tree of depth
+// ceil(log2 K)) so that the first window of a sliding pass is not a chain of K dependent additions.
+// The sliding steps that follow add (entering - leaving), one dependent addition per output.
+template <int K, typename T>
+__device__ __forceinline__ T window_sum(const T* src, int stride) {
+  T v[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) v[j] = src[j * stride];
+#pragma unroll
+  for (int w = 1; w < K; w *= 2)
+#pragma unroll
+    for (int j = 0; j + w < K; j += 2 * w) v[j] += v[j + w];
+  return v[0];
+}
+
 template <typename T>
 __device__ __forceinline__ T rcp_rn(T x);
 template <>
@@ -83,12 +97,15 @@ __device__ __forceinline__ float rcp_rn<float>(float x) {
   return __frcp_rn(x);
 }
 
-template <int R, int DIM, typename T = double, bool MASKED = false>
+// One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
+// Returns the tile's sum of local cc (valid in thread 0).  All NT threads of the block must call
+// it; `smem_raw` holds CCShape<R, DIM, T, MASKED>::smem bytes and `red` 32 doubles.
+template <int R, int DIM, typename T = double, bool MASKED = false, int NT = 256>
 __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const float* __restrict__ Mt, const Dims& d,
                                           const CCParams& P, float* __restrict__ gF, float* __restrict__ gM,
                                           float* __restrict__ cc_out, int bx, int by, int bz,
                                           unsigned char* smem_raw, double* red, double* valid_count = nullptr) {
-  using S = CCShape<R, DIM, T, MASKED>;
+  using S = CCShape<R, DIM, T, MASKED, NT>;
   constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
   constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY, NQ = S::NQ;
   float2* ring = reinterpret_cast<float2*>(smem_raw);
@@ -110,7 +127,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   bool gval[CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) {
-    int col = tid + c * 256;
+    int col = tid + c * NT;
     int hx = col % HX, hy = col / HX;
     int gx = x0 - R + hx, gy = y0 - R + hy;
     gval[c] = col < HC && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
@@ -130,7 +147,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     const int slot = pmod(zs, RD);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
-      int col = tid + c * 256;
+      int col = tid + c * NT;
       if (col < HC) {
         float2 v = make_float2(0.0f, 0.0f);
         unsigned char vb = 0;
@@ -158,7 +175,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   double cc_acc = 0.0, n_valid = 0.0;
   const int tx = tid & 31, ty = tid >> 5;
   const int ox = x0 + tx, oy = y0 + ty;
-  const bool out_ok = ox < nx && oy < ny;
+  const bool out_ok = ty < TY && ox < nx && oy < ny;  // threads past the 32 x 8 outputs only sum
   const T cxn = (T)(min(ox + R, nx - 1) - max(ox - R, 0) + 1);
   const T cyn = (T)(min(oy + R, ny - 1) - max(oy - R, 0) + 1);
 
@@ -185,7 +202,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     const bool znext = zc + 1 < z1 && ze + 1 < nz;
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
-      int col = tid + c * 256;
+      int col = tid + c * NT;
       if (col < HC) {
         if (sub && gval[c] && (!MASKED || vring[slot * HC + col])) {
           float2 o = ring[slot * HC + col];
@@ -224,36 +241,30 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     __syncthreads();
     // y box sums, sliding down one halo column over the TY output rows (one task per quantity and
     // halo column)
-    for (int task = tid; task < NQ * HX; task += 256) {
+    for (int task = tid; task < NQ * HX; task += NT) {
       const int yq = task / HX, ycol = task - yq * HX;
       const T* src = cs + yq * HY * CSP + ycol;
       T* dst = ys + yq * TY * CSP + ycol;
-      T s = T(0);
-#pragma unroll
-      for (int j = 0; j <= 2 * R; ++j) s += src[j * CSP];
+      T s = window_sum<2 * R + 1>(src, CSP);
       dst[0] = s;
 #pragma unroll
       for (int y = 1; y < TY; ++y) {
-        s += src[(y + 2 * R) * CSP];
-        s -= src[(y - 1) * CSP];
+        s += src[(y + 2 * R) * CSP] - src[(y - 1) * CSP];
         dst[y * CSP] = s;
       }
     }
     __syncthreads();
     // x box sums, sliding along an output row: outputs XSEG k .. XSEG k + XSEG-1 (one task per
     // quantity, output row and segment; consecutive threads take consecutive rows)
-    for (int task = tid; task < NQ * TY * (TX / S::XSEG); task += 256) {
+    for (int task = tid; task < NQ * TY * (TX / S::XSEG); task += NT) {
       const int row = task % (NQ * TY), seg = task / (NQ * TY);
       const T* src = ys + row * CSP + S::XSEG * seg;
       T* dst = ws + row * XSP + S::XSEG * seg;
-      T s = T(0);
-#pragma unroll
-      for (int j = 0; j <= 2 * R; ++j) s += src[j];
+      T s = window_sum<2 * R + 1>(src, 1);
       dst[0] = s;
 #pragma unroll
       for (int x = 1; x < S::XSEG; ++x) {
-        s += src[x + 2 * R];
-        s -= src[x - 1];
+        s += src[x + 2 * R] - src[x - 1];
         dst[x] = s;
       }
     }
