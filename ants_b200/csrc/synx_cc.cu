@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdint>
 
 #include "synx_cc_tile.cuh"
 #include "synx_level.cuh"
@@ -118,12 +119,29 @@ int cc_blocks_max(const GridInfo& g, int radius) {
   return cc_blocks(g, radius, cc_max_chunks(g, radius));
 }
 
+template <int R, int DIM>
+static size_t cc_smem_t(bool masked) {
+  return masked ? CCShape<R, DIM, double, true>::smem : CCShape<R, DIM, double>::smem;
+}
+
 size_t cc_smem_bytes(int dim, int radius, bool masked) {
-  // CCShape<R, DIM, double, masked>::smem for a run-time radius
-  const size_t TX = 32, TY = 8, HX = TX + 2 * radius, HY = TY + 2 * radius, HC = HX * HY;
-  const size_t RD = dim == 3 ? 2 * radius + 1 : 1;
-  const size_t nq = masked ? 6 : 5;
-  return RD * HC * 8 + nq * HY * (HX | 1) * 8 + nq * HY * (TX + 1) * 8 + (masked ? RD * HC : 0);
+  // CCShape<R, DIM, double, masked>::smem for a run-time radius (the tile's own layout, so the
+  // persistent level kernel's allocation cannot fall behind it); radii without a kernel: SIZE_MAX
+#define SYNX_CC_SMEM(RR) \
+  case RR:               \
+    return dim == 3 ? cc_smem_t<RR, 3>(masked) : cc_smem_t<RR, 2>(masked);
+  switch (radius) {
+    SYNX_CC_SMEM(1)
+    SYNX_CC_SMEM(2)
+    SYNX_CC_SMEM(3)
+    SYNX_CC_SMEM(4)
+    SYNX_CC_SMEM(5)
+    SYNX_CC_SMEM(6)
+    SYNX_CC_SMEM(7)
+    default:
+      return SIZE_MAX;
+  }
+#undef SYNX_CC_SMEM
 }
 
 template <int R, int DIM>

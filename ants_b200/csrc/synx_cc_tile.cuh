@@ -66,9 +66,14 @@ struct CCShape {
   static constexpr int XSP = TX + 1;   // row pitch of the window sums (odd)
   static constexpr int XSEG = 8;       // outputs per x-pass task
   static_assert(TX % XSEG == 0, "x segments tile the output row");
-  static_assert(NQ * TY * XSP <= NQ * HY * CSP, "window sums fit in the column sums' space");
   static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)NQ * HY * CSP * sizeof(T) +
-                                 (size_t)NQ * TY * CSP * sizeof(T) + (MASKED ? (size_t)RD * HC : 0);
+                                 (size_t)NQ * TY * CSP * sizeof(T) + (size_t)NQ * TY * XSP * sizeof(T) +
+                                 (MASKED ? (size_t)RD * HC : 0);
+  // The next slice's column update writes the column sums and ring slot (z + 1 + R) mod (2R + 1)
+  // while slower warps may still be in this slice's epilogue, which reads the window sums (their
+  // own array) and ring slots z - 1, z, z + 1.  Those slots differ from the written one unless
+  // R = 1, so only then does a slice end with a barrier.
+  static constexpr bool END_BARRIER = DIM == 3 && R < 2;
 };
 
 // Sum of the K values src[0], src[stride], ..., src[(K-1) stride], added pairwise (a tree of depth
@@ -109,10 +114,10 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
   constexpr int CSP = S::CSP, XSP = S::XSP, TY = S::TY, NQ = S::NQ;
   float2* ring = reinterpret_cast<float2*>(smem_raw);
-  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [NQ][HY][CSP] column sums; reused as ws after the y pass
+  T* cs = reinterpret_cast<T*>(ring + RD * HC);  // [NQ][HY][CSP] column sums
   T* ys = cs + NQ * HY * CSP;                     // [NQ][TY][CSP] y box sums of the halo columns
-  T* ws = cs;                                     // [NQ][TY][XSP] window sums of the output voxels
-  unsigned char* vring = reinterpret_cast<unsigned char*>(ys + NQ * TY * CSP);  // [RD][HC] (MASKED)
+  T* ws = ys + NQ * TY * CSP;                     // [NQ][TY][XSP] window sums of the output voxels
+  unsigned char* vring = reinterpret_cast<unsigned char*>(ws + NQ * TY * XSP);  // [RD][HC] (MASKED)
   const unsigned char* __restrict__ valid = P.valid;
 
   const int tid = threadIdx.x;
@@ -339,7 +344,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       }
       if (cc_out != nullptr) cc_out[oi] = (float)cc;
     }
-    __syncthreads();
+    if (S::END_BARRIER) __syncthreads();
   }
   if (MASKED) {
     const double nv = block_sum_d(n_valid, red);

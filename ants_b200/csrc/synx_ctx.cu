@@ -1072,6 +1072,9 @@ int level_finish(synx_ctx* c, int level) {
   const std::vector<double>& lm = c->h_lm;
   const std::vector<double>& lc = c->h_lc;
   const std::vector<int>& li = c->h_li;
+  if (hctl.bar_err == 2)
+    return set_err(c, SYNX_E_CUDA, "level " + std::to_string(level) +
+                                       ": the level kernel was launched with less shared memory than its tiles use");
   if (hctl.bar_err)
     return set_err(c, SYNX_E_CUDA, "level " + std::to_string(level) + ": a grid barrier of the level kernel timed out");
   const int done = std::min(hctl.iter, iters);

@@ -70,7 +70,8 @@ struct IterCtl {
   InvCtl inv[2][2];           // [phase A (psi), phase B (phi)][half]
   unsigned bar_count;         // grid barrier of the persistent level kernel: arrivals,
   unsigned bar_gen;           // generation,
-  int bar_err;                // and 1 if a wait gave up (the kernel then returns)
+  int bar_err;                // and 1 if a wait gave up, 2 if the launch's shared memory was too
+                              // small (the kernel then returns)
   int pad1;
 };
 

@@ -284,11 +284,26 @@ __device__ void level_body(const LevelArgs& A, const Grp& gp, unsigned char* sme
   }
 }
 
+// The level's phases carve the dynamic shared memory as the CC tile and the xy smoothing tile lay
+// it out; a launch that provides less records IterCtl::bar_err = 2 and every block returns, so a
+// host-side sizing mistake is reported by the run instead of reaching outside the allocation.
+template <int DIM, int RCC>
+__device__ __forceinline__ bool level_smem_ok(const LevelArgs& A) {
+  unsigned have;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(have));
+  const size_t need_cc = CCShape<RCC, DIM>::smem;
+  const size_t need_xy = smooth3_smem_floats(DIM, A.r_smooth, kLevelSmoothTY) * sizeof(float);
+  if (have >= need_cc && have >= need_xy) return true;
+  if (threadIdx.x == 0) atomicExch(&A.ctl->bar_err, 2);
+  return false;
+}
+
 template <int DIM, int RCC>
 __global__ void __launch_bounds__(256, 2) k_level(const __grid_constant__ LevelArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double redd[32];
   __shared__ float redf[32];
+  if (!level_smem_ok<DIM, RCC>(A)) return;
   const Grp gp{(int)blockIdx.x, (int)gridDim.x};
   if (A.diag) level_body<DIM, RCC, true>(A, gp, smem, redd, redf);
   else level_body<DIM, RCC, false>(A, gp, smem, redd, redf);
@@ -317,6 +332,7 @@ __global__ void __launch_bounds__(256, 2) k_level_batch(const __grid_constant__ 
   for (int i = threadIdx.x; i < (int)(sizeof(LevelArgs) / 8); i += blockDim.x) a_raw[i] = src[i];
   __syncthreads();
   const LevelArgs& A = *reinterpret_cast<const LevelArgs*>(a_raw);
+  if (!level_smem_ok<DIM, RCC>(A)) return;
   const Grp gp{(int)blockIdx.x - B.first_block[p], B.first_block[p + 1] - B.first_block[p]};
   if (A.diag) level_body<DIM, RCC, true>(A, gp, smem, redd, redf);
   else level_body<DIM, RCC, false>(A, gp, smem, redd, redf);
