@@ -91,6 +91,67 @@ __device__ __forceinline__ float lerp_at(const float* __restrict__ a, const Cell
   return fmaf(b1 - b0, c.wz, b0);
 }
 
+// Cell of a point whose every axis has both neighbours inside the grid (0 <= floor(c) < n - 1), so
+// that no clamp applies: the upper neighbours sit at +1, +nx and +nx*ny, the weights are c - floor(c).
+// Returns false for a point that needs the clamp-to-edge cell (make_cell); the offset and weights it
+// computes are then not meant to be used.  Where it returns true, the corners and weights are exactly
+// make_cell's, so lerp_interior gives lerp_at's value bit for bit.
+template <int DIM>
+__device__ __forceinline__ bool interior_cell(const Dims& d, float cx, float cy, float cz, int& o, float& wx,
+                                              float& wy, float& wz) {
+  const float fx = floorf(cx), fy = floorf(cy), fz = DIM == 3 ? floorf(cz) : 0.0f;
+  const int bx = (int)fx, by = (int)fy, bz = (int)fz;
+  wx = cx - fx;
+  wy = cy - fy;
+  wz = DIM == 3 ? cz - fz : 0.0f;
+  o = (bz * d.ny + by) * d.nx + bx;
+  bool in = (unsigned)bx < (unsigned)(d.nx - 1) && (unsigned)by < (unsigned)(d.ny - 1);
+  if (DIM == 3) in = in && (unsigned)bz < (unsigned)(d.nz - 1);
+  return in;
+}
+
+// lerp_at for an interior cell: p = plane + offset of the lower corner; sy = nx, sz = nx * ny.
+template <int DIM>
+__device__ __forceinline__ float lerp_interior(const float* __restrict__ p, int sy, int sz, float wx, float wy,
+                                               float wz) {
+  const float* py = p + sy;
+  float v00 = __ldg(p), v10 = __ldg(p + 1);
+  float v01 = __ldg(py), v11 = __ldg(py + 1);
+  float a0 = fmaf(v10 - v00, wx, v00);
+  float a1 = fmaf(v11 - v01, wx, v01);
+  float b0 = fmaf(a1 - a0, wy, a0);
+  if (DIM == 2) return b0;
+  const float* q = p + sz;
+  const float* qy = q + sy;
+  float u00 = __ldg(q), u10 = __ldg(q + 1);
+  float u01 = __ldg(qy), u11 = __ldg(qy + 1);
+  float c0 = fmaf(u10 - u00, wx, u00);
+  float c1 = fmaf(u11 - u01, wx, u01);
+  float b1 = fmaf(c1 - c0, wy, c0);
+  return fmaf(b1 - b0, wz, b0);
+}
+
+// Multilinear interpolation of NC planes (plane c at a + c * N) at one point inside the buffer.  A
+// warp whose active lanes all have interior cells takes the interior cell's short form; otherwise
+// every lane takes the clamp-to-edge cell, so lanes near the edges do not split the warp into both
+// forms (on small grids most warps have such a lane).  Either form gives the same value.
+template <int DIM, int NC>
+__device__ __forceinline__ void lerp_planes(const float* __restrict__ a, int N, const Dims& d, float cx, float cy,
+                                            float cz, float out[NC]) {
+  int o;
+  float wx, wy, wz;
+  const bool in = interior_cell<DIM>(d, cx, cy, cz, o, wx, wy, wz);
+  if (__all_sync(__activemask(), in)) {
+    const int sy = d.nx, sz = d.nx * d.ny;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c] = lerp_interior<DIM>(a + c * N + o, sy, sz, wx, wy, wz);
+  } else {
+    const Cell cl = make_cell<DIM>(d, cx, cy, cz);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c] = lerp_at<DIM>(a + c * N, cl);
+  }
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -44,7 +44,9 @@ __device__ __forceinline__ float sample(const float* __restrict__ img, const Dim
   float cx, cy, cz;
   map_point<DIM, DIAG>(m, fx, fy, fz, ux, uy, uz, cx, cy, cz);
   if (!inside_buffer<DIM>(di, cx, cy, cz)) return 0.0f;
-  return lerp_at<DIM>(img, make_cell<DIM>(di, cx, cy, cz));
+  float v;
+  lerp_planes<DIM, 1>(img, 0, di, cx, cy, cz, &v);
+  return v;
 }
 
 // ---- warp of both images through their inverse half-fields -----------------------------------
@@ -143,10 +145,11 @@ __device__ __forceinline__ void compose_tile(const ComposeArgs& a, const IterCtl
     float cx, cy, cz;
     map_point<DIM, DIAG>(a.m, fx, fy, (float)z, w0, w1, w2, cx, cy, cz);
     if (inside_buffer<DIM>(d, cx, cy, cz)) {
-      const Cell c = make_cell<DIM>(d, cx, cy, cz);
-      O[i] = fmaf(scale, lerp_at<DIM>(D, c), w0);
-      O[N + i] = fmaf(scale, lerp_at<DIM>(D + N, c), w1);
-      if (DIM == 3) O[2 * N + i] = fmaf(scale, lerp_at<DIM>(D + 2 * N, c), w2);
+      float v[DIM];
+      lerp_planes<DIM, DIM>(D, N, d, cx, cy, cz, v);
+      O[i] = fmaf(scale, v[0], w0);
+      O[N + i] = fmaf(scale, v[1], w1);
+      if (DIM == 3) O[2 * N + i] = fmaf(scale, v[DIM - 1], w2);
     } else {
       O[i] = w0;
       O[N + i] = w1;
@@ -189,11 +192,11 @@ __device__ __forceinline__ void inv_residual(const float* __restrict__ phi, cons
   e[1] = p[1];
   e[2] = DIM == 3 ? p[2] : 0.0f;
   if (inside_buffer<DIM>(d, cx, cy, cz)) {
-    const Cell c = make_cell<DIM>(d, cx, cy, cz);
-    const int N = (int)d.N;
-    e[0] += lerp_at<DIM>(phi, c);
-    e[1] += lerp_at<DIM>(phi + N, c);
-    if (DIM == 3) e[2] += lerp_at<DIM>(phi + 2 * N, c);
+    float v[DIM];
+    lerp_planes<DIM, DIM>(phi, (int)d.N, d, cx, cy, cz, v);
+    e[0] += v[0];
+    e[1] += v[1];
+    if (DIM == 3) e[2] += v[DIM - 1];
   }
 }
 

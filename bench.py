@@ -795,6 +795,74 @@ def run_apply(args) -> int:
     return 0
 
 
+def run_kernels(args) -> int:
+    """Each full-resolution step of a SyN iteration once per step through the C ABI, on the
+    182x218x182 phantom pair and a smooth synthetic field (about 3 voxels at most): image warp, CC
+    value + both update directions (r = 4), update smoothing (variance 3 voxels^2), composition, and
+    a field inversion from a zero start.  Few launches and a few hundred MB on the device, so a
+    profiler capture of one of these kernels stays short.  Prints one JSON line with the mean time
+    of each call (CUDA events on the launching stream around the call, L2 flushed before each; the
+    calls that return a value or allocate scratch synchronise inside, which the times include)."""
+    import torch
+    from ants_b200 import phantoms, replicas
+    from ants_b200 import synx as S
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = S.Geom(SIZE)
+    N = g.count
+    fixed, moving = phantoms.pair_3d(SIZE, seed=replicas.pair_seed(0))
+    rng = np.random.default_rng(0x5EED0000 + 6000)
+    u = np.ascontiguousarray(np.moveaxis(phantoms.smooth_field(g.shape, 6.0, 3.0, rng), -1, 0).astype(np.float32))
+    F, M = torch.from_numpy(fixed).to(dev), torch.from_numpy(moving).to(dev)
+    U = torch.from_numpy(u).to(dev)
+    W = 0.5 * U
+    out1 = torch.empty(g.shape, device=dev)
+    gF, gM, out3 = (torch.empty((3,) + g.shape, device=dev) for _ in range(3))
+    psi = torch.zeros_like(U)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+    calls = {
+        "warp_image": (lambda: S.warp_image(F, g, U, g, out1, stream=stream.cuda_stream), 20),
+        "cc_metric_r4": (lambda: S.cc_metric(F, M, g, 4, gF, gM, stream=stream.cuda_stream), 32),
+        "smooth_field_var3": (lambda: S.smooth_field(U, out3, g, 3.0, stream=stream.cuda_stream), 48),
+        "compose": (lambda: S.compose(U, W, g, out3, 0.5, stream=stream.cuda_stream), 72),
+        "invert_field": (lambda: (psi.zero_(), S.invert_field(U, psi, g, stream=stream.cuda_stream)), None),
+    }
+    for _ in range(max(args.warmup, 0)):
+        for fn, _b in calls.values():
+            fn()
+    torch.cuda.synchronize()
+    launches0 = S.launch_count()
+    res = {}
+    with ClockSampler(0) as clk:
+        for name, (fn, bytes_per_voxel) in calls.items():
+            ms = []
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+            t = sum(ms) / len(ms)
+            res[name] = {"call_us": 1000.0 * t}
+            if bytes_per_voxel:
+                res[name]["algorithmic_gbs"] = bytes_per_voxel * N / (t / 1000.0) / 1e9
+    launches = S.launch_count() - launches0
+    peak, peak_kind = measured_peak_hbm()
+    line = {"metric": "per-call time at 182x218x182", "value": res["cc_metric_r4"]["call_us"], "unit": "us",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic: seeded phantom pair, smooth field",
+            "config": {"workload": "one call of each full-resolution step (182x218x182) through the C ABI",
+                       "l2": "flushed before each call (256 MB)"},
+            "kernels": res, "peak_hbm_gbs": peak, "peak_source": peak_kind, "clocks": clk.summary(),
+            "gpu_launches": int(launches)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------------------------
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
@@ -806,10 +874,12 @@ def main(argv=None) -> int:
     ap.add_argument("--plain-launches", action="store_true",
                     help="launch every kernel directly instead of replaying per-level CUDA graphs (the same "
                          "work; profilers see each kernel, which they do not inside graphs with conditional nodes)")
-    ap.add_argument("--config", default="single", choices=["single", "batched", "serving", "precision", "apply"],
+    ap.add_argument("--config", default="single",
+                    choices=["single", "batched", "serving", "precision", "apply", "kernels"],
                     help="single: the 182x218x182 pair (default); batched: 32 pairs of uneven sizes, "
                          "batched vs sequential pairs/hour; serving: Poisson arrivals of a 2-D/3-D mix, "
-                         "p50/p99 latency; precision: the error study; apply: antsApplyTransforms warp + affine")
+                         "p50/p99 latency; precision: the error study; apply: antsApplyTransforms warp + affine; "
+                         "kernels: each full-resolution step once (short profiler captures)")
     ap.add_argument("--rates", default="0.5,2,5,10,20", help="serving: arrival rates (requests/s)")
     ap.add_argument("--window", type=float, default=12.0, help="serving: seconds of arrivals per rate")
     args = ap.parse_args(argv)
@@ -821,6 +891,8 @@ def main(argv=None) -> int:
         return run_precision(args)
     if args.config == "apply":
         return run_apply(args)
+    if args.config == "kernels":
+        return run_kernels(args)
 
     ws, rank, local = dist_env()
     from ants_b200 import phantoms, replicas
