@@ -122,7 +122,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
 
   const int tid = threadIdx.x;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const long long nxy = (long long)nx * ny, N = d.N;
+  const int nxy = nx * ny, N = (int)d.N;  // 32-bit offsets: the host keeps 3 N below 2^31
   const int x0 = bx * TX, y0 = by * S::TY;
   const int z0 = bz * P.ZC;
   const int z1 = min(z0 + P.ZC, nz);
@@ -157,7 +157,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         float2 v = make_float2(0.0f, 0.0f);
         unsigned char vb = 0;
         if (zin && gval[c]) {
-          long long o = (long long)zs * nxy + gofs[c];
+          const int o = zs * nxy + gofs[c];
           v.x = __ldg(Ft + o);
           v.y = __ldg(Mt + o);
           vb = MASKED ? __ldg(valid + o) : 1;
@@ -193,15 +193,19 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     nv[c] = make_float2(0.0f, 0.0f);
     nvb[c] = 0;
     if (z0 < z1 && z0 + RZ < nz && gval[c]) {
-      const long long o = (long long)(z0 + RZ) * nxy + gofs[c];
+      const int o = (z0 + RZ) * nxy + gofs[c];
       nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
       if (MASKED) nvb[c] = __ldg(valid + o);
     }
   }
+  // ring slots of slices zc (sc), zc - 1 (sm), zc + 1 (sp) and zc + RZ (slot), advanced per slice
+  int sc = pmod(z0, RD);
+  const int pofs = oy * nx + ox;
   for (int zc = z0; zc < z1; ++zc) {
+    const int sp = sc + 1 == RD ? 0 : sc + 1, sm = sc == 0 ? RD - 1 : sc - 1;
+    const int slot = sc + RZ >= RD ? sc + RZ - RD : sc + RZ;
     // slide the z window: subtract slice zc-RZ-1 (if it was added), add slice zc+RZ
     const int ze = zc + RZ, zl = zc - RZ - 1;
-    const int slot = pmod(ze, RD);
     const bool sub = zc > z0 && zl >= 0;
     const bool zin = ze < nz;
     const bool znext = zc + 1 < z1 && ze + 1 < nz;
@@ -237,7 +241,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         nv[c] = make_float2(0.0f, 0.0f);
         if (MASKED) nvb[c] = 0;
         if (znext && gval[c]) {
-          const long long o = (long long)(ze + 1) * nxy + gofs[c];
+          const int o = (ze + 1) * nxy + gofs[c];
           nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
           if (MASKED) nvb[c] = __ldg(valid + o);
         }
@@ -275,9 +279,9 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     }
     __syncthreads();
     const int cidx = (ty + R) * HX + (tx + R);
-    const bool center_ok = out_ok && (!MASKED || vring[pmod(zc, RD) * HC + cidx]);
+    const bool center_ok = out_ok && (!MASKED || vring[sc * HC + cidx]);
     if (MASKED && out_ok && !center_ok) {  // a masked-out voxel: no value, no update
-      const long long oi = (long long)zc * nxy + (long long)oy * nx + ox;
+      const int oi = zc * nxy + pofs;
 #pragma unroll
       for (int dd = 0; dd < DIM; ++dd) gF[dd * N + oi] = gM[dd * N + oi] = 0.0f;
       if (cc_out != nullptr) cc_out[oi] = 0.0f;
@@ -294,7 +298,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       const T sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
       const T sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
       const T sFM = Sq[4] - mM * Sq[0] - mF * Sq[1] + n * mM * mF;
-      const float2* rc = ring + pmod(zc, RD) * HC;
+      const float2* rc = ring + sc * HC;
       const float2 v0 = rc[cidx];
       const T fh = (T)v0.x - mF, mh = (T)v0.y - mM;
       T cc = T(1), aF = T(0), aM = T(0);
@@ -318,12 +322,12 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         gFi[1] = grad1(ym.x, v0.x, yp.x, oy, ny, P.h[1]);
         gMi[2] = gFi[2] = 0.0f;
         if (DIM == 3) {
-          const float2 zm = ring[pmod(zc - 1, RD) * HC + cidx], zp = ring[pmod(zc + 1, RD) * HC + cidx];
+          const float2 zm = ring[sm * HC + cidx], zp = ring[sp * HC + cidx];
           gMi[2] = grad1(zm.y, v0.y, zp.y, zc, nz, P.h[2]);
           gFi[2] = grad1(zm.x, v0.x, zp.x, zc, nz, P.h[2]);
         }
       }
-      const long long oi = (long long)zc * nxy + (long long)oy * nx + ox;
+      const int oi = zc * nxy + pofs;
 #pragma unroll
       for (int dd = 0; dd < DIM; ++dd) {
         float pm, pf;
@@ -345,6 +349,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       if (cc_out != nullptr) cc_out[oi] = (float)cc;
     }
     if (S::END_BARRIER) __syncthreads();
+    sc = sp;
   }
   if (MASKED) {
     const double nv = block_sum_d(n_valid, red);

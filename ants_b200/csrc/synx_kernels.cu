@@ -541,7 +541,7 @@ size_t smooth_xy_pipe_smem_bytes(int R, int TY) {
 template <int R>
 // the ring lives in shared memory ((2R+1) x 3 x 256 floats, smooth_z_smem_bytes), so few registers
 // are needed: 5 resident blocks per SM up to R = 6 (40 KB of ring each), 3 up to R = 12
-__global__ void __launch_bounds__(256, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
+__global__ void __launch_bounds__(kSmoothZThreads, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
   griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ float zring[];
@@ -640,7 +640,7 @@ static int smooth3_radius(int dim, const int R[3]) {
 
 bool smooth3_supported(int dim, const int R[3]) { return smooth3_radius(dim, R) <= kSmoothRMax; }
 
-static size_t smooth_z_smem_bytes(int R) { return (size_t)(2 * R + 1) * 3 * 256 * sizeof(float); }
+static size_t smooth_z_smem_bytes(int R) { return (size_t)(2 * R + 1) * 3 * kSmoothZThreads * sizeof(float); }
 
 template <int R>
 static cudaError_t smooth3_attr_both() {
@@ -892,7 +892,7 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   count_launch();
 #define SYNX_SZ(RV)                                    \
   case RV:                                             \
-    launch_k(k_smooth_z<RV>, gz, 256, smooth_z_smem_bytes(RV), s, a, g.d, ctl);    \
+    launch_k(k_smooth_z<RV>, gz, kSmoothZThreads, smooth_z_smem_bytes(RV), s, a, g.d, ctl);    \
     break;
   switch (RR) {
     SYNX_SZ(1)

@@ -319,23 +319,29 @@ template <int DIM, int R, int TY, bool ASYNC>
 __device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
                                                     float* tile) {
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
+  static_assert(HX <= 64, "two columns per lane cover a halo row");
   const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
   const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const int x0 = bx * 32, y0 = by * TY;
-  const float* plane = src + z * nxy;
-  for (int row = ty; row < DIM * HY; row += 8) {
-    const int c = row / HY, hy = row - c * HY;
-    const int gy = min(max(y0 - R + hy, 0), ny - 1);
-    const float* line = plane + c * N + gy * nx;
-    float* trow = tile + row * HXP;
+  // the halo columns this lane copies (replicate-edge indices) are the same in every row
+  const int gx0 = min(max(x0 - R + tx, 0), nx - 1);
+  const int gx1 = min(max(x0 - R + 32 + tx, 0), nx - 1);
+  const bool second = tx < HX - 32;
 #pragma unroll
-    for (int hx = tx; hx < HX; hx += 32) {
-      const float* g = line + min(max(x0 - R + hx, 0), nx - 1);
-      if (ASYNC)
-        cp_async4(trow + hx, g);
-      else
-        trow[hx] = __ldg(g);
+  for (int c = 0; c < DIM; ++c) {
+    const float* cplane = src + c * N + z * nxy;
+    float* ctile = tile + c * HY * HXP;
+    for (int hy = ty; hy < HY; hy += 8) {
+      const float* line = cplane + min(max(y0 - R + hy, 0), ny - 1) * nx;
+      float* trow = ctile + hy * HXP;
+      if (ASYNC) {
+        cp_async4(trow + tx, line + gx0);
+        if (second) cp_async4(trow + 32 + tx, line + gx1);
+      } else {
+        trow[tx] = __ldg(line + gx0);
+        if (second) trow[32 + tx] = __ldg(line + gx1);
+      }
     }
   }
 }
@@ -503,8 +509,11 @@ __device__ __forceinline__ float smooth_z_column(const Smooth3Args& a, const Dim
   return mx;
 }
 
-// The same z part with the ring in shared memory (`ring` holds (2R+1) x 3 x blockDim floats, slot-
-// major, thread-minor: each thread touches only its own column, so no barrier is needed and the
+// Threads of a block of the standalone z smoothing kernel.
+constexpr int kSmoothZThreads = 256;
+
+// The same z part with the ring in shared memory (`ring` holds (2R+1) x 3 x kSmoothZThreads floats,
+// slot-major, thread-minor: each thread touches only its own column, so no barrier is needed and the
 // accesses are conflict-free).  Far fewer registers than the register ring, so more blocks fit on
 // an SM; the arithmetic and its order are the same, so the results have the same bits.
 template <int R>
@@ -519,8 +528,10 @@ __device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, cons
   const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
   float mx = 0.0f;
   if (ox >= nx || oy >= ny) return mx;
-  const int T = blockDim.x, t = threadIdx.x;
-  auto slot = [&](int s, int c) -> float& { return ring[(s * 3 + c) * T + t]; };
+  // a compile-time row length (the kernel's block), so every slot's offset is an immediate
+  constexpr int T = kSmoothZThreads;
+  float* rt = ring + threadIdx.x;
+  auto slot = [&](int s, int c) -> float& { return rt[(s * 3 + c) * T]; };
   const float* col = src + oy * nx + ox;
 #pragma unroll
   for (int u = 0; u < 2 * R; ++u) {
