@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, 
   __shared__ float red[32];
   const int h = blockIdx.z / d.nz;
   const int z = blockIdx.z - h * d.nz;
-  const float mx = smooth_xy_tile<DIM, R, kSmoothTileY>(a, d, blockIdx.x, blockIdx.y, z, h, sm3);
+  const float mx = smooth_xy_tile<DIM, R, kSmoothTileY, TileLoad::Batched>(a, d, blockIdx.x, blockIdx.y, z, h, sm3);
   if (DIM == 2 && a.do_max) {
     const float bm = block_max_f(mx, red);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
@@ -505,13 +505,13 @@ __global__ void __launch_bounds__(256) k_smooth_xy_pipe(const Smooth3Args a, Dim
   float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int ox = blockIdx.x * 32 + tx, oy0 = blockIdx.y * TY + ty * RPT;
-  smooth_xy_load_tile<3, R, TY, true>(a, d, blockIdx.x, blockIdx.y, z0, h, smp);
+  smooth_xy_load_tile<3, R, TY, TileLoad::Async>(a, d, blockIdx.x, blockIdx.y, z0, h, smp);
   cp_async_commit();
   for (int z = z0; z < z1; ++z) {
     const int k = z - z0;
     if (z + 1 < z1) {
       // buffer (k + 1) & 1 was last read by the convolution of slice z - 1, which ended in a barrier
-      smooth_xy_load_tile<3, R, TY, true>(a, d, blockIdx.x, blockIdx.y, z + 1, h, smp + ((k + 1) & 1) * TILE);
+      smooth_xy_load_tile<3, R, TY, TileLoad::Async>(a, d, blockIdx.x, blockIdx.y, z + 1, h, smp + ((k + 1) & 1) * TILE);
       cp_async_commit();
       cp_async_wait<1>();
     } else {

@@ -301,10 +301,6 @@ __host__ __device__ inline size_t smooth3_smem_floats(int dim, int R, int TY = 8
 // consecutive outputs from float4 loads) and then along y (each thread makes TY/8 consecutive rows
 // of one column from registers).  Taller tiles convolve fewer halo rows along x per output (TY + 2R
 // rows for TY outputs).
-// The xy convolution of one (32 x TY tile, slice z, field h): thread (tx, ty) gets the outputs at
-// x = bx*32 + tx, y = by*TY + ty*(TY/8) + r in y[c][r].  All threads of the block must call it.
-// Halo tile of one (32 x TY tile, slice z, field h) into shared memory (replicate-edge indices):
-// plain loads, or with ASYNC cp.async copies that the caller commits and waits for.
 __device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -315,7 +311,14 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(NPENDING) : "memory");
 }
 
-template <int DIM, int R, int TY, bool ASYNC>
+// How a halo tile reaches shared memory: a loop of plain loads and stores (few registers: the
+// persistent level kernel), all of a warp's rows of a component loaded into registers before they
+// are stored (the loads in flight together: the standalone xy kernel), or cp.async copies that the
+// caller commits and waits for.
+enum class TileLoad { Loop, Batched, Async };
+
+// Halo tile of one (32 x TY tile, slice z, field h) into shared memory (replicate-edge indices).
+template <int DIM, int R, int TY, TileLoad LOAD>
 __device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
                                                     float* tile) {
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
@@ -328,19 +331,42 @@ __device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const 
   const int gx0 = min(max(x0 - R + tx, 0), nx - 1);
   const int gx1 = min(max(x0 - R + 32 + tx, 0), nx - 1);
   const bool second = tx < HX - 32;
+  constexpr int RPW = (HY + 7) / 8;  // halo rows per warp and component
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
     const float* cplane = src + c * N + z * nxy;
     float* ctile = tile + c * HY * HXP;
-    for (int hy = ty; hy < HY; hy += 8) {
-      const float* line = cplane + min(max(y0 - R + hy, 0), ny - 1) * nx;
-      float* trow = ctile + hy * HXP;
-      if (ASYNC) {
-        cp_async4(trow + tx, line + gx0);
-        if (second) cp_async4(trow + 32 + tx, line + gx1);
-      } else {
-        trow[tx] = __ldg(line + gx0);
-        if (second) trow[32 + tx] = __ldg(line + gx1);
+    if (LOAD != TileLoad::Batched) {
+      for (int hy = ty; hy < HY; hy += 8) {
+        const float* line = cplane + min(max(y0 - R + hy, 0), ny - 1) * nx;
+        float* trow = ctile + hy * HXP;
+        if (LOAD == TileLoad::Async) {
+          cp_async4(trow + tx, line + gx0);
+          if (second) cp_async4(trow + 32 + tx, line + gx1);
+        } else {
+          trow[tx] = __ldg(line + gx0);
+          if (second) trow[32 + tx] = __ldg(line + gx1);
+        }
+      }
+    } else {
+      float v0[RPW], v1[RPW];
+#pragma unroll
+      for (int k = 0; k < RPW; ++k) {
+        const int hy = ty + 8 * k;
+        if (hy < HY) {
+          const float* line = cplane + min(max(y0 - R + hy, 0), ny - 1) * nx;
+          v0[k] = __ldg(line + gx0);
+          v1[k] = second ? __ldg(line + gx1) : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < RPW; ++k) {
+        const int hy = ty + 8 * k;
+        if (hy < HY) {
+          float* trow = ctile + hy * HXP;
+          trow[tx] = v0[k];
+          if (second) trow[32 + tx] = v1[k];
+        }
       }
     }
   }
@@ -398,13 +424,14 @@ __device__ __forceinline__ void smooth_xy_convolve(const Smooth3Args& a, const f
   __syncthreads();  // the tile and xsum may be reused by the caller's next tile
 }
 
-template <int DIM, int R, int TY>
+template <int DIM, int R, int TY, TileLoad LOAD = TileLoad::Loop>
 __device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
                                                   float* sm, float (&y)[DIM][TY / 8]) {
+  static_assert(LOAD != TileLoad::Async, "the caller waits for cp.async copies");
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
   float* tile = sm;                     // [DIM][HY][HXP]
   float* xsum = tile + DIM * HY * HXP;  // [DIM][HY][32]
-  smooth_xy_load_tile<DIM, R, TY, false>(a, d, bx, by, z, h, tile);
+  smooth_xy_load_tile<DIM, R, TY, LOAD>(a, d, bx, by, z, h, tile);
   __syncthreads();
   smooth_xy_convolve<DIM, R, TY>(a, tile, xsum, y);
 }
@@ -413,12 +440,12 @@ __device__ __forceinline__ void smooth_xy_compute(const Smooth3Args& a, const Di
 // to `out` for the z part; in 2-D this is the whole filter and the SyN epilogue runs here (max norm
 // returned).  All threads of the block must call it; `sm` holds smooth3_smem_floats(DIM, R, TY)
 // floats.
-template <int DIM, int R, int TY = 8>
+template <int DIM, int R, int TY = 8, TileLoad LOAD = TileLoad::Loop>
 __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims& d, int bx, int by, int z, int h,
                                                 float* sm) {
   constexpr int RPT = TY / 8;
   float y[DIM][RPT];
-  smooth_xy_compute<DIM, R, TY>(a, d, bx, by, z, h, sm, y);
+  smooth_xy_compute<DIM, R, TY, LOAD>(a, d, bx, by, z, h, sm, y);
   const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
   float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
