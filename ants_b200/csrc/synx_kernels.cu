@@ -1242,8 +1242,14 @@ __device__ __forceinline__ void invert_spec_tile(const InvArgs& a, int h, int bx
   if (lane == leader && wmax > seen) atomicMax(gbound, wmax);
 }
 
+// Resident blocks per SM of the single-pass inverse; a launch is one wave of them, shared by the two
+// halves.  (3 blocks with up to 80 registers measured the same; staging the corner gathers in shared
+// memory with cp.async, two voxels in flight per thread, took 328 instead of 224 us per full-resolution
+// launch: more instructions per voxel and no gain in latency hiding.)
+constexpr int kInvSpecBlocksPerSM = 4;
+
 template <int DIM, bool DIAG>
-__global__ void __launch_bounds__(256, 4) k_invert_spec(const InvArgs a, InvLaunch L, IterCtl* ctl,
+__global__ void __launch_bounds__(256, kInvSpecBlocksPerSM) k_invert_spec(const InvArgs a, InvLaunch L, IterCtl* ctl,
                                                         double* __restrict__ psum, float* __restrict__ pmax, int pcap,
                                                         InvList list) {
   griddep_wait();
@@ -1394,7 +1400,7 @@ void launch_invert_spec(const float* const* phi, float* const* psi, int halves, 
   const Map3 m2 = map3(g.d, 2, kInvTarget);
   const int tz = (int)m2.grid.z / 2;
   const int ntiles = (int)m2.grid.x * (int)m2.grid.y * tz;
-  const int nb = std::max(1, std::min({ntiles, kInvBlocksPerHalf, pb.capacity}));
+  const int nb = std::max(1, std::min({ntiles, 148 * kInvSpecBlocksPerSM / 2, pb.capacity}));
   const InvArgs a = make_inv_args(phi, psi, halves, g, m2.zb, ecache);
   InvLaunch L{k, max_iter, phase, stop_aware ? 1 : 0, halves, (int)m2.grid.x, (int)m2.grid.y, tz, mean_tol, max_tol};
   const InvList il{{list[0], halves > 1 ? list[1] : list[0]}};

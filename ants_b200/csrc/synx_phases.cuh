@@ -170,10 +170,10 @@ struct InvArgs {
   int zb;
 };
 
+// Continuous index of voxel (fx, fy, fz) displaced by p (physical): (fx, fy, fz) + A p.
 template <int DIM, bool DIAG>
-__device__ __forceinline__ void inv_residual(const float* __restrict__ phi, const Dims& d, const float* A, float fx,
-                                             float fy, float fz, const float p[3], float e[3]) {
-  float cx, cy, cz;
+__device__ __forceinline__ void inv_map(const float* A, float fx, float fy, float fz, const float p[3], float& cx,
+                                        float& cy, float& cz) {
   if (DIAG) {
     cx = fmaf(A[0], p[0], fx);
     cy = fmaf(A[4], p[1], fy);
@@ -188,6 +188,13 @@ __device__ __forceinline__ void inv_residual(const float* __restrict__ phi, cons
       cz = fz + A[6] * p[0] + A[7] * p[1] + A[8] * p[2];
     }
   }
+}
+
+template <int DIM, bool DIAG>
+__device__ __forceinline__ void inv_residual(const float* __restrict__ phi, const Dims& d, const float* A, float fx,
+                                             float fy, float fz, const float p[3], float e[3]) {
+  float cx, cy, cz;
+  inv_map<DIM, DIAG>(A, fx, fy, fz, p, cx, cy, cz);
   e[0] = p[0];
   e[1] = p[1];
   e[2] = DIM == 3 ? p[2] : 0.0f;
