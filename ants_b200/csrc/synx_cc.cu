@@ -21,7 +21,7 @@ constexpr int CC_THREADS = 320;
 template <int R, int DIM, typename T, bool MASKED = false>
 __global__ void __launch_bounds__(CC_THREADS, 2)
     k_cc(const float* __restrict__ Ft, const float* __restrict__ Mt, Dims d, CCParams P, float* __restrict__ gF,
-         float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out) {
+         float* __restrict__ gM, double* __restrict__ partials, IterCtl* ctl, float* __restrict__ cc_out, int rev) {
   griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -29,10 +29,11 @@ __global__ void __launch_bounds__(CC_THREADS, 2)
   __shared__ double vcount;
   __shared__ int am_last;
   const int tid = threadIdx.x;
-  const double bs = cc_tile<R, DIM, T, MASKED, CC_THREADS>(Ft, Mt, d, P, gF, gM, cc_out, blockIdx.x, blockIdx.y,
-                                                           blockIdx.z, smem_raw, red, &vcount);
+  const uint3 b = sweep_block(rev);
+  const double bs = cc_tile<R, DIM, T, MASKED, CC_THREADS>(Ft, Mt, d, P, gF, gM, cc_out, b.x, b.y, b.z, smem_raw, red,
+                                                           &vcount);
   const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
-  const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  const unsigned bid = b.x + gridDim.x * (b.y + gridDim.y * b.z);  // the tile's partial slot
   if (tid == 0) {
     partials[bid] = bs;
     if (MASKED) partials[nblocks + bid] = vcount;
@@ -67,12 +68,13 @@ static void cc_launch_t(const float* Ft, const float* Mt, const GridInfo& g, flo
                         IterCtl* ctl, cudaStream_t s, float* cc_out, dim3 grid, const CCParams& P, bool fp32) {
   if (P.valid != nullptr)
     launch_k(k_cc<R, DIM, double, true>, grid, CC_THREADS, CCShape<R, DIM, double, true>::smem, s, Ft, Mt, g.d, P, gF, gM, partials,
-                                                                                     ctl, cc_out);
+                                                                                     ctl, cc_out, t_rev);
   else if (fp32)
-    launch_k(k_cc<R, DIM, float>, grid, CC_THREADS, CCShape<R, DIM, float>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl, cc_out);
+    launch_k(k_cc<R, DIM, float>, grid, CC_THREADS, CCShape<R, DIM, float>::smem, s, Ft, Mt, g.d, P, gF, gM, partials,
+             ctl, cc_out, t_rev);
   else
     launch_k(k_cc<R, DIM, double>, grid, CC_THREADS, CCShape<R, DIM, double>::smem, s, Ft, Mt, g.d, P, gF, gM, partials, ctl,
-                                                                          cc_out);
+                                                                          cc_out, t_rev);
 }
 
 // z-chunk of one CC block.  Each block first fills its z window (2R slices, column updates only,

@@ -660,7 +660,16 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false, boo
     cudaEventRecord(c->ev_pool[idx], s);
     return idx;
   };
+  // Sweep orders: each kernel walks its grid opposite to the kernel whose output it reads, so it
+  // starts on that kernel's last-written tiles while they are in L2 (warp backwards after the
+  // inversions' forward walks, CC forwards, xy smoothing backwards, z smoothing forwards, composition
+  // backwards, the inversions forwards).  Only the order of the tiles changes, not any result.
+  struct SweepReset {
+    ~SweepReset() { t_rev = 0; }
+  } sweep_reset;
+  t_rev = 1;
   launch_warp_pair(c->Fs, c->gF, c->psiF, c->Ms, c->gM, c->psiM, g, c->Ft, c->Mt, c->ctl, s);
+  t_rev = 0;
   const bool masked = c->maskF != nullptr || c->maskM != nullptr;
   if (masked) launch_mask_validity(c->maskF, c->gmF, c->psiF, c->maskM, c->gmM, c->psiM, g, c->valid, c->ctl, s);
   int e0 = profile ? ev() : -1;
@@ -670,6 +679,7 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false, boo
   // update-field smoothing, SyN epilogue (boundary zero, blend) and max ||u/spacing||
   const float* upd[2] = {c->t1F, c->t1M};
   const double var = c->P.update_variance;
+  t_rev = 1;  // xy pass backwards, z pass forwards
   {
     const float* in[2] = {c->gFu, c->gMu};
     float* out[2] = {c->t1F, c->t1M};
@@ -685,6 +695,7 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false, boo
   }
   // scale + compose into the forward half-fields (in place), or into t2 followed by the
   // total-field smoothing back into the half-fields when its variance is positive
+  t_rev = 1;  // composition backwards
   if (c->P.total_variance > 0.0) {
     const double vt = c->P.total_variance;
     const float w1 = vt < 0.5 ? (float)(1.0 - vt / 0.5) : 1.0f;
@@ -694,12 +705,14 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false, boo
     const float* in[2] = {c->t2F, c->t2M};
     float* out[2] = {c->phiF, c->phiM};
     float* tmp[2] = {c->gFu, c->gMu};
+    t_rev = 0;
     smooth_halves(c, in, out, in, tmp, c->coeff_tot, c->h_coeff_tot.data(), c->R_tot, true, w1, 1.0f - w1, false);
   } else {
     const float* w[2] = {c->phiF, c->phiM};
     float* o[2] = {c->phiF, c->phiM};
     launch_compose(upd, w, o, 2, g, (float)c->P.learning_rate, c->ctl, s);
   }
+  t_rev = 0;
   // precision study: half-fields stored in half precision (rounded after every step that writes them)
   const bool fp16 = (c->P.flags & SYNX_F_FIELDS_FP16) != 0;
   auto round_pair = [&](float* a, float* b) {

@@ -152,6 +152,19 @@ __device__ __forceinline__ void lerp_planes(const float* __restrict__ a, int N, 
   }
 }
 
+// This block's tile coordinates, in reverse order of the grid when `rev` (block 0 takes the last
+// tile).  Blocks start roughly in index order, so a kernel walking the grid backwards begins on the
+// tiles that the kernel before it (walking forwards) wrote last, while they are still in L2.
+__device__ __forceinline__ uint3 sweep_block(int rev) {
+  uint3 b = blockIdx;
+  if (rev) {
+    b.x = gridDim.x - 1 - b.x;
+    b.y = gridDim.y - 1 - b.y;
+    b.z = gridDim.z - 1 - b.z;
+  }
+  return b;
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -23,6 +23,7 @@ namespace synx {
 
 thread_local int t_pdl = 0;
 thread_local int t_pdl_skip = 0;
+thread_local int t_rev = 0;
 
 // Process-wide count of kernel launches issued by this library (instrumentation).
 std::atomic<long long> g_launches{0};
@@ -231,14 +232,15 @@ void launch_zero_ctl_level(IterCtl* ctl, cudaStream_t s) {
 // Warps (one tile per block).
 // ------------------------------------------------------------------------------------------
 template <int DIM, bool DIAG>
-__global__ void __launch_bounds__(256) k_warp_pair(const WarpArgs a, IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_warp_pair(const WarpArgs a, IterCtl* ctl, int rev) {
   griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && ctl != nullptr) {
     ctl->maxnorm[0] = 0u;  // the update scaling of this iteration starts from zero
     ctl->maxnorm[1] = 0u;
   }
-  warp_pair_tile<DIM, DIAG>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  const uint3 b = sweep_block(rev);
+  warp_pair_tile<DIM, DIAG>(a, b.x, b.y, b.z);
 }
 
 void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, const float* M, const GridInfo& gM,
@@ -249,11 +251,11 @@ void launch_warp_pair(const float* F, const GridInfo& gF, const float* psiF, con
   a.zb = m.zb;
   const bool dg = affine_diag(a.mF) && affine_diag(a.mM);
   if (gv.d.dim == 3) {
-    if (dg) launch_k(k_warp_pair<3, true>, m.grid, 256, 0, s, a, ctl);
-    else launch_k(k_warp_pair<3, false>, m.grid, 256, 0, s, a, ctl);
+    if (dg) launch_k(k_warp_pair<3, true>, m.grid, 256, 0, s, a, ctl, t_rev);
+    else launch_k(k_warp_pair<3, false>, m.grid, 256, 0, s, a, ctl, t_rev);
   } else {
-    if (dg) launch_k(k_warp_pair<2, true>, m.grid, 256, 0, s, a, ctl);
-    else launch_k(k_warp_pair<2, false>, m.grid, 256, 0, s, a, ctl);
+    if (dg) launch_k(k_warp_pair<2, true>, m.grid, 256, 0, s, a, ctl, t_rev);
+    else launch_k(k_warp_pair<2, false>, m.grid, 256, 0, s, a, ctl, t_rev);
   }
 }
 
@@ -471,14 +473,15 @@ void launch_mask_validity(const unsigned char* mF, const GridInfo& gmF, const fl
 constexpr int kSmoothTileY = 64;
 
 template <int DIM, int R>
-__global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_smooth_xy(const Smooth3Args a, Dims d, IterCtl* ctl, int rev) {
   griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ __align__(16) float sm3[];
   __shared__ float red[32];
-  const int h = blockIdx.z / d.nz;
-  const int z = blockIdx.z - h * d.nz;
-  const float mx = smooth_xy_tile<DIM, R, kSmoothTileY, TileLoad::Batched>(a, d, blockIdx.x, blockIdx.y, z, h, sm3);
+  const uint3 b = sweep_block(rev);
+  const int h = b.z / d.nz;
+  const int z = b.z - h * d.nz;
+  const float mx = smooth_xy_tile<DIM, R, kSmoothTileY, TileLoad::Batched>(a, d, b.x, b.y, z, h, sm3);
   if (DIM == 2 && a.do_max) {
     const float bm = block_max_f(mx, red);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
@@ -541,15 +544,17 @@ size_t smooth_xy_pipe_smem_bytes(int R, int TY) {
 template <int R>
 // the ring lives in shared memory ((2R+1) x 3 x 256 floats, smooth_z_smem_bytes), so few registers
 // are needed: 5 resident blocks per SM up to R = 6 (40 KB of ring each), 3 up to R = 12
-__global__ void __launch_bounds__(kSmoothZThreads, (R <= 6 ? 5 : 3)) k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl) {
+__global__ void __launch_bounds__(kSmoothZThreads, (R <= 6 ? 5 : 3))
+    k_smooth_z(const Smooth3Args a, Dims d, IterCtl* ctl, int rev) {
   griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
   extern __shared__ float zring[];
   __shared__ float red[32];
+  const uint3 b = sweep_block(rev);
   const int nzc = gridDim.z / a.halves;
-  const int h = blockIdx.z / nzc;
-  const int zc = blockIdx.z - h * nzc;
-  const float mx = smooth_z_column_smem<R>(a, d, blockIdx.x, blockIdx.y, zc, h, zring);
+  const int h = b.z / nzc;
+  const int zc = b.z - h * nzc;
+  const float mx = smooth_z_column_smem<R>(a, d, b.x, b.y, zc, h, zring);
   if (a.do_max) {
     const float bm = block_max_f(mx, red);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxnorm[h], bm);
@@ -856,9 +861,9 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
 #define SYNX_SXY(RV)                                             \
   case RV:                                                       \
     if (dim == 3)                                                \
-      launch_k(k_smooth_xy<3, RV>, gxy, 256, smem, s, a, g.d, ctl);    \
+      launch_k(k_smooth_xy<3, RV>, gxy, 256, smem, s, a, g.d, ctl, t_rev);    \
     else                                                         \
-      launch_k(k_smooth_xy<2, RV>, gxy, 256, smem, s, a, g.d, ctl);    \
+      launch_k(k_smooth_xy<2, RV>, gxy, 256, smem, s, a, g.d, ctl, t_rev);    \
     break;
   switch (RR) {
     SYNX_SXY(1)
@@ -892,7 +897,7 @@ void launch_smooth_field(const float* const* in, float* const* out, const float*
   count_launch();
 #define SYNX_SZ(RV)                                    \
   case RV:                                             \
-    launch_k(k_smooth_z<RV>, gz, kSmoothZThreads, smooth_z_smem_bytes(RV), s, a, g.d, ctl);    \
+    launch_k(k_smooth_z<RV>, gz, kSmoothZThreads, smooth_z_smem_bytes(RV), s, a, g.d, ctl, t_rev ^ 1); \
     break;
   switch (RR) {
     SYNX_SZ(1)
@@ -988,12 +993,13 @@ void launch_smooth_field_pass(const float* const* in, float* const* out, const f
 // Composition (one tile per block, both halves by blockIdx.z).
 // ------------------------------------------------------------------------------------------
 template <int DIM, bool DIAG>
-__global__ void __launch_bounds__(256) k_compose(const ComposeArgs a, int halves, IterCtl* ctl) {
+__global__ void __launch_bounds__(256) k_compose(const ComposeArgs a, int halves, IterCtl* ctl, int rev) {
   griddep_wait();
   if (ctl != nullptr && ctl->stop) return;
+  const uint3 b = sweep_block(rev);
   const int gz = gridDim.z / halves;
-  const int h = blockIdx.z / gz;
-  compose_tile<DIM, DIAG>(a, ctl, h, blockIdx.x, blockIdx.y, blockIdx.z - h * gz);
+  const int h = b.z / gz;
+  compose_tile<DIM, DIAG>(a, ctl, h, b.x, b.y, b.z - h * gz);
 }
 
 void launch_compose(const float* const* d, const float* const* w, float* const* out, int halves, const GridInfo& g,
@@ -1010,11 +1016,11 @@ void launch_compose(const float* const* d, const float* const* w, float* const* 
   a.zb = m.zb;
   const bool dg = affine_diag(a.m);
   if (g.d.dim == 3) {
-    if (dg) launch_k(k_compose<3, true>, m.grid, 256, 0, s, a, halves, ctl);
-    else launch_k(k_compose<3, false>, m.grid, 256, 0, s, a, halves, ctl);
+    if (dg) launch_k(k_compose<3, true>, m.grid, 256, 0, s, a, halves, ctl, t_rev);
+    else launch_k(k_compose<3, false>, m.grid, 256, 0, s, a, halves, ctl, t_rev);
   } else {
-    if (dg) launch_k(k_compose<2, true>, m.grid, 256, 0, s, a, halves, ctl);
-    else launch_k(k_compose<2, false>, m.grid, 256, 0, s, a, halves, ctl);
+    if (dg) launch_k(k_compose<2, true>, m.grid, 256, 0, s, a, halves, ctl, t_rev);
+    else launch_k(k_compose<2, false>, m.grid, 256, 0, s, a, halves, ctl, t_rev);
   }
 }
 

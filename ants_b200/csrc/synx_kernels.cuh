@@ -15,6 +15,10 @@ namespace synx {
 // completed and its writes are visible.  Without the attribute the wait returns at once.
 extern thread_local int t_pdl;       // launches from this host thread use the attribute
 extern thread_local int t_pdl_skip;  // the next launch does not (it follows a graph node that is not a kernel)
+// Sweep order of the launches from this host thread that take one (warp, CC, xy and z smoothing,
+// composition): 1 = the grid in reverse (see sweep_block).  The z smoothing pass takes the
+// opposite of its xy pass.
+extern thread_local int t_rev;
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 template <typename... KArgs, typename... Args>
