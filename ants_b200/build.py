@@ -35,7 +35,7 @@ LIB_HEADERS = ["synx_device.cuh", "synx_kernels.cuh", "synx_phases.cuh", "synx_c
                "synx_level_body.cuh", "synx_host.h", "synx_nvtx.h"]
 CLI_SOURCES = ["ants_registration.cpp", "nifti_io.cpp"]
 APPLY_SOURCES = ["ants_apply_transforms.cpp", "nifti_io.cpp"]
-CLI_HEADERS = ["nifti_io.h", "ants_registration.h", "ants_apply_transforms.h", "cli_common.h"]
+CLI_HEADERS = ["nifti_io.h", "ants_registration.h", "ants_apply_transforms.h", "cli_common.h", "composite_txt.h"]
 
 
 def _nvcc() -> str:

@@ -15,7 +15,17 @@
 //   -r/--initial-moving-transform file | [file,useInverse] | identity | [fixed,moving,feature]
 //       (repeatable, the first given acting first; linear .mat/.txt files, or the translation derived
 //       from two images: feature 0 geometric centers, 1 centers of mass, 2 origins)
-//   -z/--collapse-output-transforms 0|1 (default 1)   -a/--write-composite-transform 0
+//   -z/--collapse-output-transforms 0|1 (default 1)
+//   -a/--write-composite-transform 0|1: prefixComposite.txt and prefixInverseComposite.txt instead of
+//       the separate files, in ITK's text transform form (the reference writes .h5; HDF5 is not
+//       available here)
+//   -i/--initialize-transforms-per-stage 0|1 (needs -a 1 and -z 0)
+//   -j/--save-state file.txt: the registration state (initial transforms, then the SyN stage's
+//       fixed-to-middle and moving-to-middle fields each followed by its inverse; needs -a 1)
+//   -k/--restore-state file.txt: a saved state; its linear transforms act as the initial moving
+//       transform and, with -i 1, its four fields start the SyN stage (without -i the reference
+//       makes the composed fields an initial displacement-field transform, which this stage does
+//       not take: refused)
 //   -x/--masks [fixedMask,movingMask] | fixedMask (metric masks; a name that is not a file = no mask)
 // Output: prefix0Warp.nii.gz and prefix0InverseWarp.nii.gz (antsRegistrationTemplateHeader.cxx:74-90
 // names for SyN); with initial transforms, prefix0GenericAffine.mat (them, collapsed) and
@@ -24,7 +34,7 @@
 // moving image's geometry (an index <-> physical map the device functions take in general form),
 // which samples the moving image at Init(x + psi_M(x)) exactly.  With -z 0, derived translations are
 // written as prefix<n>DerivedInitialMovingTranslation.mat.  Other stages, metrics, initial fixed
-// transforms and HDF5 composite output are rejected with EXIT_FAILURE.
+// transforms and HDF5 transform files are rejected with EXIT_FAILURE.
 #include "ants_registration.h"
 
 #include <cuda_runtime.h>
@@ -44,6 +54,7 @@
 #include <vector>
 
 #include "cli_common.h"
+#include "composite_txt.h"
 #include "nifti_io.h"
 #include "synx.h"
 
@@ -66,7 +77,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       {"-f", "shrink-factors"}, {"-s", "smoothing-sigmas"}, {"-o", "output"}, {"-v", "verbose"},
       {"-w", "winsorize-image-intensities"}, {"-u", "use-histogram-matching"}, {"-x", "masks"},
       {"-r", "initial-moving-transform"}, {"-q", "initial-fixed-transform"}, {"-n", "interpolation"},
-      {"-a", "write-composite-transform"}, {"-z", "collapse-output-transforms"}, {"-h", "help"}};
+      {"-a", "write-composite-transform"}, {"-z", "collapse-output-transforms"}, {"-h", "help"},
+      {"-i", "initialize-transforms-per-stage"}, {"-j", "save-state"}, {"-k", "restore-state"}};
   for (size_t i = 0; i < args.size(); ++i) {
     std::string k = args[i];
     std::string name;
@@ -84,16 +96,28 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     auto it = opt.find(n);
     return it == opt.end() ? def : it->second.back();
   };
-  for (const char* bad : {"initial-fixed-transform", "restore-state", "save-state", "restrict-deformation"})
+  for (const char* bad : {"initial-fixed-transform", "restrict-deformation"})
     if (opt.count(bad)) throw std::runtime_error(std::string("option --") + bad + " is not supported by this SyN+CC stage");
   auto flag = [&](const std::string& n, bool def) {
     if (!opt.count(n)) return def;
     const std::string v = lower(one(n, ""));
     return !(v == "0" || v == "false");
   };
-  if (flag("write-composite-transform", false))
-    throw std::runtime_error("option --write-composite-transform 1 (HDF5 composite output) is not supported");
+  // the reference's option checks (Examples/antsRegistration.cxx:629-655,
+  // Examples/antsRegistrationTemplateHeader.h:154-172, :293-305)
+  const bool composite_out = flag("write-composite-transform", false);
   const bool collapse = flag("collapse-output-transforms", true);
+  const bool init_per_stage = flag("initialize-transforms-per-stage", false);
+  const std::string save_state = opt.count("save-state") ? one("save-state", "") : "";
+  const std::string restore_state = opt.count("restore-state") ? one("restore-state", "") : "";
+  if (init_per_stage && !composite_out)
+    throw std::runtime_error("--initialize-transforms-per-stage requires --write-composite-transform");
+  if (!save_state.empty() && !composite_out) throw std::runtime_error("--save-state requires --write-composite-transform");
+  if (init_per_stage && collapse)
+    throw std::runtime_error("initialize-transforms-per-stage & collapse-output-transforms options are mutually exclusive");
+  if (!restore_state.empty() && opt.count("initial-moving-transform"))
+    throw std::runtime_error("restore-state option is mutually exclusive with initial-moving-transform & "
+                             "initial-fixed-transform options");
   const bool histogram_matching = flag("use-histogram-matching", false);
   if (opt.count("interpolation") && lower(one("interpolation", "Linear")) != "linear")
     throw std::runtime_error("only Linear interpolation is supported for the warped outputs");
@@ -155,6 +179,30 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       throw std::runtime_error("initial moving transform '" + file +
                                "': only linear transform files (.mat/.txt) are supported");
     for (const LinearItem& li : read_linear_file(file, dim, invert)) init.push_back(li);
+  }
+  // --restore-state: [linear..., fixedToMiddle, its inverse, movingToMiddle, its inverse]
+  // (itkantsRegistrationHelper.hxx:3637-3725); a composite lists first the transform that acts last
+  std::vector<composite::Item> state_fields;
+  if (!restore_state.empty()) {
+    std::vector<composite::Item> items = composite::read(restore_state);
+    const size_t n = items.size();
+    if (n >= 4 && items[n - 1].is_field() && items[n - 2].is_field() && items[n - 3].is_field() &&
+        items[n - 4].is_field()) {
+      if (!init_per_stage)
+        throw std::runtime_error("--restore-state with SyN fields needs --initialize-transforms-per-stage 1 here: "
+                                 "without it the reference starts from the composed fields as an initial "
+                                 "displacement-field transform, which this stage does not take");
+      state_fields.assign(items.end() - 4, items.end());
+      items.resize(n - 4);
+    }
+    for (auto it = items.rbegin(); it != items.rend(); ++it) {
+      if (it->is_field())
+        throw std::runtime_error("--restore-state: displacement fields other than a SyN state are not supported");
+      LinearItem li;
+      li.linear = composite::to_linear(*it, dim);
+      li.map = map_of(li.linear, false);
+      init.push_back(li);
+    }
   }
   Map init_map;
   double init_center[3] = {0.0, 0.0, 0.0};
@@ -290,6 +338,20 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   auto t0 = std::chrono::steady_clock::now();
   if (synx_set_images(ctx, fixed.data.data(), &gf, moving.data.data(), &gm) != 0)
     throw std::runtime_error(std::string("synx_set_images: ") + synx_last_error(ctx));
+  if (!state_fields.empty()) {
+    // the SyN stage starts from the restored fixed-to-middle and moving-to-middle fields
+    // (itkantsRegistrationHelper.hxx:2093-2125)
+    const synx_geom gs = composite::field_geom(state_fields[0], dim);
+    for (int k = 1; k < 4; ++k) {
+      const synx_geom gk = composite::field_geom(state_fields[k], dim);
+      if (std::memcmp(gk.size, gs.size, sizeof(gs.size)) != 0)
+        throw std::runtime_error("--restore-state: the four SyN fields do not share one grid");
+    }
+    if (synx_set_initial_half_fields(ctx, state_fields[0].field.data(), state_fields[1].field.data(),
+                                     state_fields[2].field.data(), state_fields[3].field.data(), &gs) != 0)
+      throw std::runtime_error(std::string("synx_set_initial_half_fields: ") + synx_last_error(ctx));
+    if (verbose) out << "  SyN stage initialized from the restored registration state" << std::endl;
+  }
   int64_t printed = 0;
   for (int l = 0; l < L; ++l) {
     auto tl = std::chrono::steady_clock::now();
@@ -323,13 +385,61 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   std::vector<float> fwd((size_t)No * dim), inv((size_t)No * dim);
   if (synx_get_fields(ctx, fwd.data(), inv.data()) != 0)
     throw std::runtime_error(std::string("synx_get_fields: ") + synx_last_error(ctx));
+  // output files in the precision the reference writes them: float with --float 1, double by default
+  // (antsRegistration.cxx:488-491); the values are computed in float either way
+  const int out_type = use_float ? 16 : 64;
+  auto typed = [out_type](nifti::Image im) {
+    im.out_datatype = out_type;
+    return im;
+  };
+  // the initial transforms in composite order (the one acting last first), collapsed to one affine
+  // transform when the output transforms are collapsed
+  std::vector<synx_linear> queue;
+  for (auto it = init.rbegin(); it != init.rend(); ++it) queue.push_back(it->linear);
+  std::vector<synx_linear> out_queue = queue;
+  if (collapse && !init.empty()) out_queue.assign(1, linear_of(init_map, dim, init_center));
+  if (!save_state.empty()) {
+    // the registration state (antsRegistrationTemplateHeader.h:1307-1346): the initial transforms,
+    // then fixed-to-middle, its inverse, moving-to-middle, its inverse
+    std::vector<float> hf[4];
+    for (auto& h : hf) h.resize((size_t)No * dim);
+    if (synx_get_half_fields(ctx, hf[0].data(), hf[1].data(), hf[2].data(), hf[3].data()) != 0)
+      throw std::runtime_error(std::string("synx_get_half_fields: ") + synx_last_error(ctx));
+    std::vector<composite::Item> items;
+    for (const synx_linear& t : queue) items.push_back(composite::linear_item(t, dim));
+    for (const auto& h : hf) items.push_back(composite::field_item(go, h, !use_float));
+    composite::write(save_state, dim, items);
+  }
+  if (composite_out) {
+    // prefixComposite and prefixInverseComposite (antsRegistrationTemplateHeader.h:1394-1424): the
+    // initial transforms then the SyN field; the inverse lists the inverses in reverse order
+    std::vector<composite::Item> fw, iv;
+    for (const synx_linear& t : out_queue) fw.push_back(composite::linear_item(t, dim));
+    fw.push_back(composite::field_item(go, fwd, !use_float));
+    iv.push_back(composite::field_item(go, inv, !use_float));
+    for (auto it = out_queue.rbegin(); it != out_queue.rend(); ++it) {
+      Map mi;
+      if (!inverse(map_of(*it, false), mi)) throw std::runtime_error("an initial transform is singular");
+      iv.push_back(composite::linear_item(linear_of(mi, dim, it->center), dim));
+    }
+    composite::write(prefix + "Composite.txt", dim, fw);
+    composite::write(prefix + "InverseComposite.txt", dim, iv);
+  }
   // file names as antsRegistrationTemplateHeader.h:1436-1458 numbers them: with initial transforms
   // and collapsing, prefix0GenericAffine.mat holds them and the SyN fields are transform 1; without
-  // collapsing the initial transforms are not rewritten and the SyN fields follow them
+  // collapsing the initial transforms are not rewritten and the SyN fields follow them, except those
+  // a restored state brought, which are written one by one (the numbering starts after the -r
+  // options, :1434, and a restored state has none)
   int warp_index = 0;
-  if (!init.empty()) {
-    warp_index = collapse ? 1 : n_init;
-    if (collapse) {
+  if (!composite_out && !init.empty()) {
+    warp_index = collapse ? 1 : (restore_state.empty() ? n_init : (int)queue.size());
+    if (!collapse && !restore_state.empty()) {
+      for (size_t k = 0; k < queue.size(); ++k) {
+        const std::string name = prefix + std::to_string(k) + "GenericAffine.mat";
+        if (synx_write_linear_transform(name.c_str(), &queue[k]) != 0)
+          throw std::runtime_error(std::string("synx_write_linear_transform: ") + synx_last_error(nullptr));
+      }
+    } else if (collapse) {
       const synx_linear total = linear_of(init_map, dim, init_center);
       if (synx_write_linear_transform((prefix + "0GenericAffine.mat").c_str(), &total) != 0)
         throw std::runtime_error(std::string("synx_write_linear_transform: ") + synx_last_error(nullptr));
@@ -342,16 +452,11 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       }
     }
   }
-  // output files in the precision the reference writes them: float with --float 1, double by default
-  // (antsRegistration.cxx:488-491); the values are computed in float either way
-  const int out_type = use_float ? 16 : 64;
-  auto typed = [out_type](nifti::Image im) {
-    im.out_datatype = out_type;
-    return im;
-  };
   const std::string wi = std::to_string(warp_index);
-  nifti::write(prefix + wi + "Warp.nii.gz", typed(field_image(go, fwd)));
-  nifti::write(prefix + wi + "InverseWarp.nii.gz", typed(field_image(go, inv)));
+  if (!composite_out) {
+    nifti::write(prefix + wi + "Warp.nii.gz", typed(field_image(go, fwd)));
+    nifti::write(prefix + wi + "InverseWarp.nii.gz", typed(field_image(go, inv)));
+  }
   if (!warped.empty()) nifti::write(warped, typed(like(fixed, warp_on_device(moving, gm, fwd, go))));
   if (!inv_warped.empty()) {
     std::vector<float> inv_on_moving = resample_on_device(inv, go, gm);

@@ -1,0 +1,211 @@
+// A composite transform in ITK's text transform-file form, for the files antsRegistration writes with
+// --write-composite-transform 1 (Examples/antsRegistrationTemplateHeader.h:1394-1424) and
+// --save-state (:1307-1346) and reads with --restore-state (:293-328).  The reference writes these
+// as HDF5 (.h5), which needs a library this build does not have; ITK's text form carries the same
+// transforms and is what ITK's transform reader takes for a .txt/.tfm name:
+//
+//   #Insight Transform File V1.0
+//   #Transform 0
+//   Transform: CompositeTransform_double_3_3
+//   #Transform 1
+//   Transform: AffineTransform_double_3_3
+//   Parameters: <A row-major, then t>
+//   FixedParameters: <center>
+//   #Transform 2
+//   Transform: DisplacementFieldTransform_float_3_3
+//   Parameters: <the field's vectors, voxel by voxel with x fastest, D components each>
+//   FixedParameters: <size, origin, spacing, direction row-major>
+//
+// The first transform of the composite acts last on a point (ITK's composite queue order), as in
+// antsApplyTransforms' -t list.  Field values are written in the shortest form that reads back to
+// the same float.
+#pragma once
+
+#include <cctype>
+#include <charconv>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "synx.h"
+
+namespace ants_b200 {
+namespace composite {
+
+struct Item {
+  std::string type;             // e.g. "AffineTransform_double_3_3"
+  std::vector<double> params;   // linear transforms
+  std::vector<float> field;     // displacement fields (interleaved vectors)
+  std::vector<double> fixed;    // fixed parameters
+  bool is_field() const { return type.rfind("DisplacementFieldTransform_", 0) == 0; }
+};
+
+inline std::string suffix(const char* scalar, int dim) {
+  return std::string("_") + scalar + "_" + std::to_string(dim) + "_" + std::to_string(dim);
+}
+
+inline Item linear_item(const synx_linear& t, int dim) {
+  Item it;
+  it.type = "AffineTransform" + suffix("double", dim);
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) it.params.push_back(t.matrix[r * 3 + c]);
+  for (int r = 0; r < dim; ++r) it.params.push_back(t.translation[r]);
+  for (int r = 0; r < dim; ++r) it.fixed.push_back(t.center[r]);
+  return it;
+}
+
+// A displacement field on grid g (interleaved vectors, D per voxel).
+inline Item field_item(const synx_geom& g, const std::vector<float>& v, bool double_type) {
+  Item it;
+  const int dim = g.dim;
+  it.type = "DisplacementFieldTransform" + suffix(double_type ? "double" : "float", dim);
+  it.field = v;
+  for (int k = 0; k < dim; ++k) it.fixed.push_back((double)g.size[k]);
+  for (int k = 0; k < dim; ++k) it.fixed.push_back(g.origin[k]);
+  for (int k = 0; k < dim; ++k) it.fixed.push_back(g.spacing[k]);
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) it.fixed.push_back(g.direction[r * 3 + c]);
+  return it;
+}
+
+inline synx_linear to_linear(const Item& it, int dim) {
+  const bool known = it.type.rfind("AffineTransform_", 0) == 0 || it.type.rfind("MatrixOffsetTransformBase_", 0) == 0;
+  if (!known || (int)it.params.size() != dim * dim + dim || (int)it.fixed.size() != dim)
+    throw std::runtime_error("composite transform: unsupported linear entry '" + it.type + "'");
+  synx_linear t;
+  std::memset(&t, 0, sizeof(t));
+  t.dim = dim;
+  t.has_center = 1;
+  t.matrix[8] = 1.0;
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) t.matrix[r * 3 + c] = it.params[r * dim + c];
+  for (int r = 0; r < dim; ++r) {
+    t.translation[r] = it.params[dim * dim + r];
+    t.center[r] = it.fixed[r];
+  }
+  return t;
+}
+
+inline synx_geom field_geom(const Item& it, int dim) {
+  if ((int)it.fixed.size() != dim * (3 + dim)) throw std::runtime_error("composite transform: bad field geometry");
+  synx_geom g;
+  std::memset(&g, 0, sizeof(g));
+  g.dim = dim;
+  g.size[0] = g.size[1] = g.size[2] = 1;
+  g.spacing[0] = g.spacing[1] = g.spacing[2] = 1.0;
+  g.direction[0] = g.direction[4] = g.direction[8] = 1.0;
+  for (int k = 0; k < dim; ++k) {
+    g.size[k] = (int64_t)it.fixed[k];
+    g.origin[k] = it.fixed[dim + k];
+    g.spacing[k] = it.fixed[2 * dim + k];
+  }
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) g.direction[r * 3 + c] = it.fixed[3 * dim + r * dim + c];
+  const long long n = g.size[0] * g.size[1] * g.size[2];
+  if ((long long)it.field.size() != n * dim)
+    throw std::runtime_error("composite transform: field parameters do not match its size");
+  return g;
+}
+
+inline bool text_name(const std::string& path) {
+  auto ends = [&](const char* e) {
+    const size_t n = std::strlen(e);
+    if (path.size() < n) return false;
+    for (size_t i = 0; i < n; ++i)
+      if (std::tolower((unsigned char)path[path.size() - n + i]) != e[i]) return false;
+    return true;
+  };
+  return ends(".txt") || ends(".tfm");
+}
+
+template <class V>
+inline void write_numbers(std::FILE* f, const char* key, const V& v) {
+  std::fputs(key, f);
+  char buf[64];
+  for (auto x : v) {
+    buf[0] = ' ';
+    auto r = std::to_chars(buf + 1, buf + sizeof(buf), x);
+    std::fwrite(buf, 1, (size_t)(r.ptr - buf), f);
+  }
+  std::fputc('\n', f);
+}
+
+inline void write(const std::string& path, int dim, const std::vector<Item>& items) {
+  if (!text_name(path))
+    throw std::runtime_error("'" + path + "': composite transforms are written in ITK's text form (.txt or .tfm); "
+                             "HDF5 (.h5) is not available in this build");
+  std::FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) throw std::runtime_error("cannot write '" + path + "'");
+  std::fprintf(f, "#Insight Transform File V1.0\n#Transform 0\nTransform: CompositeTransform%s\n",
+               suffix("double", dim).c_str());
+  for (size_t k = 0; k < items.size(); ++k) {
+    std::fprintf(f, "#Transform %zu\nTransform: %s\n", k + 1, items[k].type.c_str());
+    if (items[k].is_field()) write_numbers(f, "Parameters:", items[k].field);
+    else write_numbers(f, "Parameters:", items[k].params);
+    write_numbers(f, "FixedParameters:", items[k].fixed);
+  }
+  const bool ok = std::ferror(f) == 0;
+  if (std::fclose(f) != 0 || !ok) throw std::runtime_error("error writing '" + path + "'");
+}
+
+template <class T>
+inline std::vector<T> parse_numbers(const std::string& s, size_t from, const std::string& path) {
+  std::vector<T> v;
+  const char* p = s.data() + from;
+  const char* e = s.data() + s.size();
+  while (true) {
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+    if (p >= e) break;
+    T x{};
+    auto r = std::from_chars(p, e, x);
+    if (r.ec != std::errc()) throw std::runtime_error("'" + path + "': bad number in a parameter line");
+    v.push_back(x);
+    p = r.ptr;
+  }
+  return v;
+}
+
+// The transforms of a composite file, in its order (the composite's own entry left out).  A file
+// holding a single transform reads as a composite of one.
+inline std::vector<Item> read(const std::string& path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw std::runtime_error("cannot read '" + path + "'");
+  std::vector<Item> items;
+  std::string line;
+  bool header = false;
+  while (std::getline(in, line)) {
+    if (line.rfind("#Insight Transform File", 0) == 0) {
+      header = true;
+      continue;
+    }
+    if (line.empty() || line[0] == '#') continue;
+    const size_t colon = line.find(':');
+    if (colon == std::string::npos) throw std::runtime_error("'" + path + "': unexpected line");
+    const std::string key = line.substr(0, colon);
+    if (key == "Transform") {
+      size_t b = colon + 1;
+      while (b < line.size() && line[b] == ' ') ++b;
+      size_t e = line.size();
+      while (e > b && (line[e - 1] == ' ' || line[e - 1] == '\r')) --e;
+      const std::string type = line.substr(b, e - b);
+      if (type.rfind("CompositeTransform_", 0) == 0) continue;
+      items.push_back(Item{type, {}, {}, {}});
+    } else if (key == "Parameters" || key == "FixedParameters") {
+      if (items.empty()) throw std::runtime_error("'" + path + "': parameters before any transform");
+      Item& it = items.back();
+      if (key == "FixedParameters") it.fixed = parse_numbers<double>(line, colon + 1, path);
+      else if (it.is_field()) it.field = parse_numbers<float>(line, colon + 1, path);
+      else it.params = parse_numbers<double>(line, colon + 1, path);
+    } else {
+      throw std::runtime_error("'" + path + "': unexpected key '" + key + "'");
+    }
+  }
+  if (!header) throw std::runtime_error("'" + path + "' is not an ITK text transform file");
+  return items;
+}
+
+}  // namespace composite
+}  // namespace ants_b200

@@ -216,6 +216,10 @@ struct synx_ctx {
   unsigned char* maskM = nullptr;
   GridInfo gmF{}, gmM{};
   unsigned char* valid = nullptr;
+  // initial half-fields phiF, psiF, phiM, psiM (component planes, one after the other, on init_grid),
+  // resampled to the first level's grid when it starts, or null: zero fields
+  float* init_half = nullptr;
+  GridInfo init_grid{};
   int* inv_list[2] = {nullptr, nullptr};  // deferred voxels of the single-pass inverse, per half
   // canonical buffer assignment (level changes swap field and work buffers)
   float* canon[8] = {};
@@ -960,7 +964,13 @@ int level_begin(synx_ctx* c, int level) {
   rc = upload_level_kernels(c, level);
   if (rc) return rc;
   c->plan[level] = resolve_plan(c, level);
-  if (level == 0) {
+  if (level == 0 && c->init_half) {
+    const size_t n = (size_t)D * c->init_grid.d.N;
+    const float* in[4] = {c->init_half, c->init_half + n, c->init_half + 2 * n, c->init_half + 3 * n};
+    float* out[4] = {c->phiF, c->psiF, c->phiM, c->psiM};
+    launch_resample_fields(in, c->init_grid, out, gl, 4, c->stream);
+    if (c->P.flags & SYNX_F_FIELDS_FP16) launch_round_half(out, 4, (long long)D * gl.d.N, c->stream);
+  } else if (level == 0) {
     for (float* f : {c->phiF, c->psiF, c->phiM, c->psiM})
       CUDA_TRY(c, cudaMemsetAsync(f, 0, 4 * (size_t)D * gl.d.N, c->stream));
   } else {
@@ -1461,6 +1471,7 @@ int synx_destroy(synx_ctx* ctx) {
   free_arena(ctx);
   if (ctx->maskF) cudaFree(ctx->maskF);
   if (ctx->maskM) cudaFree(ctx->maskM);
+  if (ctx->init_half) cudaFree(ctx->init_half);
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   for (auto e : ctx->lev_ev)
     if (e) cudaEventDestroy(e);
@@ -1541,6 +1552,51 @@ int synx_set_masks(synx_ctx* c, const float* fixed_mask, const synx_geom* gfm, c
   if (!rc) rc = upload(moving_mask, gmm, &c->maskM, &c->gmM);
   drop_graphs(c);  // the iteration's launches change with the masks
   return rc;
+}
+
+int synx_set_initial_half_fields(synx_ctx* c, const float* phi_f, const float* psi_f, const float* phi_m,
+                                 const float* psi_m, const synx_geom* grid) {
+  if (!valid_ctx(c)) return set_err(nullptr, SYNX_E_ARG, "null context");
+  const int given = (phi_f != nullptr) + (psi_f != nullptr) + (phi_m != nullptr) + (psi_m != nullptr);
+  if (given != 0 && given != 4)
+    return set_err(c, SYNX_E_ARG, "synx_set_initial_half_fields: give all four half-fields or none");
+  if (given == 4 && !check_geom(grid, c->D))
+    return set_err(c, SYNX_E_ARG, "synx_set_initial_half_fields: grid does not match the stage dimension or is invalid");
+  if (c->cur_level >= 0 && c->cur_level + 1 < c->P.n_levels)
+    return set_err(c, SYNX_E_STATE, "synx_set_initial_half_fields: a run is in progress");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (c->init_half) {
+    cudaFree(c->init_half);
+    c->init_half = nullptr;
+  }
+  if (given == 0) return SYNX_OK;
+  geom_to_grid(*grid, c->init_grid);
+  const size_t n = (size_t)c->D * c->init_grid.d.N;
+  float* inter = nullptr;
+  cudaError_t e = cudaMalloc((void**)&c->init_half, 4 * 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&inter, 4 * n);
+  if (e != cudaSuccess) {
+    if (c->init_half) cudaFree(c->init_half);
+    c->init_half = nullptr;
+    cudaGetLastError();
+    return set_err(c, SYNX_E_NOMEM, std::string("synx_set_initial_half_fields: ") + cudaGetErrorString(e));
+  }
+  const float* src[4] = {phi_f, psi_f, phi_m, psi_m};
+  for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+    e = cudaMemcpy(inter, src[k], 4 * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      launch_deinterleave(inter, c->init_half + k * n, c->init_grid.d.N, c->D, c->stream);
+      e = cudaStreamSynchronize(c->stream);
+    }
+  }
+  cudaFree(inter);
+  if (e != cudaSuccess) {
+    cudaFree(c->init_half);
+    c->init_half = nullptr;
+    return set_err(c, SYNX_E_CUDA, std::string("synx_set_initial_half_fields: ") + cudaGetErrorString(e));
+  }
+  return SYNX_OK;
 }
 
 int synx_set_images(synx_ctx* c, const float* F, const synx_geom* gf, const float* M, const synx_geom* gm) {

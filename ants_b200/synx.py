@@ -188,6 +188,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_get_fields_device": (I, [V, V, V]),
         "synx_get_half_fields": (I, [V, V, V, V, V]),
         "synx_set_half_fields": (I, [V, V, V, V, V, P(SynxGeom)]),
+        "synx_set_initial_half_fields": (I, [V, V, V, V, V, P(SynxGeom)]),
         "synx_get_log": (I, [V, V, V, V, V, V, C.c_int64, P(C.c_int64)]),
         "synx_get_profile": (I, [V, P(D), P(C.c_int64), P(C.c_int64), P(D), P(C.c_int64), P(C.c_int64)]),
         "synx_reset_profile": (I, [V]),
@@ -605,6 +606,19 @@ class SyNStage:
         arrs = [_host(a, grid.dim * grid.count, "half field") for a in (phi_f, psi_f, phi_m, psi_m)]
         g = grid.to_c()
         self._ck(self.lib.synx_set_half_fields(self.h, *[_ptr(a) for a in arrs], C.byref(g)))
+
+    def set_initial_half_fields(self, phi_f=None, psi_f=None, phi_m=None, psi_m=None, grid: Geom | None = None) -> None:
+        """The stage's starting half-fields (interleaved host arrays on `grid`, as half_fields()
+        returns them), resampled to the first level's grid instead of zero fields: a stage resumed
+        from a saved registration state.  All None clears them."""
+        if phi_f is None and psi_f is None and phi_m is None and psi_m is None:
+            self._ck(self.lib.synx_set_initial_half_fields(self.h, None, None, None, None, None))
+            return
+        if grid is None:
+            raise SynxError("initial half-fields need their grid")
+        arrs = [_host(a, grid.dim * grid.count, "initial half field") for a in (phi_f, psi_f, phi_m, psi_m)]
+        g = grid.to_c()
+        self._ck(self.lib.synx_set_initial_half_fields(self.h, *[_ptr(a) for a in arrs], C.byref(g)))
 
     def log(self) -> list[LogRecord]:
         n = C.c_int64()

@@ -309,6 +309,17 @@ int synx_histogram_match(const float* src_dev, int64_t n_src, const float* ref_d
 int synx_set_masks(synx_ctx* ctx, const float* fixed_mask, const synx_geom* fixed_mask_geom,
                    const float* moving_mask, const synx_geom* moving_mask_geom);
 
+/* Initial half-fields of the stage: a SyN stage initialized from a saved registration state
+ * (antsRegistration --restore-state with --initialize-transforms-per-stage 1; the restored
+ * FixedToMiddle and MovingToMiddle transforms are set on the SyN method at
+ * Examples/itkantsRegistrationHelper.hxx:2093-2125, and its per-level initialization resamples their
+ * fields to each level's domain).  Host arrays, interleaved like synx_get_half_fields' (phiF = fixed
+ * to middle, psiF its inverse, phiM = moving to middle, psiM its inverse), on `grid`; all NULL
+ * clears them.  The first level resamples them to its grid instead of starting from zero fields.
+ * They stay set across runs and synx_set_images; refused while a run is between levels. */
+int synx_set_initial_half_fields(synx_ctx* ctx, const float* phi_f, const float* psi_f, const float* phi_m,
+                                 const float* psi_m, const synx_geom* grid);
+
 /* Tile plans chosen by the project's autotuner (python -m ants_b200.autotune): a text table of
  * measured winners per level grid, one line per (dim, nx, ny, nz, CC radius, smoothing radius) with
  * the chosen persistent-kernel use, smoothing tile rows and CC z chunks.  Loaded once per process at

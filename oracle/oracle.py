@@ -74,6 +74,8 @@ def load() -> C.CDLL:
             f"oracle_resample_field_{suf}": (None, [V, P(G), V, P(G)]),
             f"oracle_syn_iteration_{suf}": (D, [V, P(G), V, P(G), P(Pm), P(G), V, V, V, V, P(I)]),
             f"oracle_syn_register_{suf}": (I, [V, P(G), V, P(G), P(Pm), V, V, P(G), V, V, V, V, V, I]),
+            f"oracle_syn_register_full_{suf}": (I, [V, P(G), V, P(G), P(Pm), V, P(G), V, P(G), V, V, V, V, P(G), V,
+                                                      V, V, P(G), V, V, V, V, V, I]),
         })
     for n, (r, a) in sigs.items():
         f = getattr(lib, n)
@@ -232,9 +234,12 @@ def syn_iteration(Fs, gF, Ms, gM, params, g, phiF, psiF, phiM, psiM, dtype=np.fl
 
 
 def syn_register(F, gF, M, gM, params, dtype=np.float32, fixed_mask=None, fixed_mask_geom=None, moving_mask=None,
-                 moving_mask_geom=None):
+                 moving_mask_geom=None, initial_half_fields=None, initial_geom=None, return_half_fields=False):
     """Full stage: returns (forward, inverse, out_geom, log) with fields as component planes.  Metric
-    masks (nonzero = inside) on their own grids (default: the image's grid) are optional."""
+    masks (nonzero = inside) on their own grids (default: the image's grid) are optional.
+    initial_half_fields: (phiF, psiF, phiM, psiM) as component planes on initial_geom, the stage's
+    starting half-fields (resampled to the first level's grid), or None for zero fields.  With
+    return_half_fields the final half-fields are returned as a fifth item."""
     from ants_b200.synx import Geom, SynxGeom
     f, m = _c(F, dtype), _c(M, dtype)
     g_last = gF
@@ -242,6 +247,7 @@ def syn_register(F, gF, M, gM, params, dtype=np.float32, fixed_mask=None, fixed_
         g_last = shrink_geom(gF, s)
     fwd = np.empty((g_last.dim,) + g_last.shape, dtype)
     inv = np.empty_like(fwd)
+    half = np.empty((4, g_last.dim) + g_last.shape, dtype) if return_half_fields else None
     cap = int(sum(params.iterations)) + 1
     lv = np.zeros(cap, np.int32)
     it = np.zeros(cap, np.int32)
@@ -251,22 +257,25 @@ def syn_register(F, gF, M, gM, params, dtype=np.float32, fixed_mask=None, fixed_
     go = SynxGeom()
     pc = params.to_c()
     ga, gb = gF.to_c(), gM.to_c()
-    if fixed_mask is None and moving_mask is None:
-        n = getattr(load(), f"oracle_syn_register_{_suf(dtype)}")(_p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc),
-                                                                  _p(fwd), _p(inv), C.byref(go), _p(lv), _p(it),
-                                                                  _p(me), _p(cv), _p(ki), cap)
-    else:
-        mf = _c(fixed_mask, dtype) if fixed_mask is not None else None
-        mm = _c(moving_mask, dtype) if moving_mask is not None else None
-        gmf = (fixed_mask_geom or gF).to_c() if mf is not None else None
-        gmm = (moving_mask_geom or gM).to_c() if mm is not None else None
-        n = getattr(load(), f"oracle_syn_register_masked_{_suf(dtype)}")(
-            _p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc), _p(mf) if mf is not None else None,
-            C.byref(gmf) if gmf is not None else None, _p(mm) if mm is not None else None,
-            C.byref(gmm) if gmm is not None else None, _p(fwd), _p(inv), C.byref(go), _p(lv), _p(it), _p(me),
-            _p(cv), _p(ki), cap)
+    mf = _c(fixed_mask, dtype) if fixed_mask is not None else None
+    mm = _c(moving_mask, dtype) if moving_mask is not None else None
+    gmf = (fixed_mask_geom or gF).to_c() if mf is not None else None
+    gmm = (moving_mask_geom or gM).to_c() if mm is not None else None
+    ini = [None] * 4
+    gi = None
+    if initial_half_fields is not None:
+        ini = [_c(a, dtype) for a in initial_half_fields]
+        gi = (initial_geom or gF).to_c()
+    n = getattr(load(), f"oracle_syn_register_full_{_suf(dtype)}")(
+        _p(f), C.byref(ga), _p(m), C.byref(gb), C.byref(pc), _p(mf) if mf is not None else None,
+        C.byref(gmf) if gmf is not None else None, _p(mm) if mm is not None else None,
+        C.byref(gmm) if gmm is not None else None, *[(_p(a) if a is not None else None) for a in ini],
+        C.byref(gi) if gi is not None else None, _p(fwd), _p(inv), _p(half) if half is not None else None,
+        C.byref(go), _p(lv), _p(it), _p(me), _p(cv), _p(ki), cap)
     log = [dict(level=int(lv[i]), iteration=int(it[i]), metric=float(me[i]), convergence=float(cv[i]),
                 inverse_iterations=int(ki[i])) for i in range(min(n, cap))]
+    if return_half_fields:
+        return fwd, inv, Geom.from_c(go), log, half
     return fwd, inv, Geom.from_c(go), log
 
 

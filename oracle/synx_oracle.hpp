@@ -1160,6 +1160,21 @@ struct SynRun {
   std::vector<double> level_seconds;
 
   std::vector<T> maskF, maskM;
+  // Initial half-fields phiF, psiF, phiM, psiM (component planes on grid gI), or none: a SyN stage
+  // initialized from a saved registration state (Examples/itkantsRegistrationHelper.hxx:2093-2125
+  // sets the restored FixedToMiddle and MovingToMiddle transforms on the SyN method, whose per-level
+  // initialization resamples their fields to each level's domain, the first level's included).
+  std::vector<T> init[4];
+  Geom gI;
+  bool have_init = false;
+
+  void set_initial_half_fields(const T* phiF0, const T* psiF0, const T* phiM0, const T* psiM0, const Geom& g) {
+    const T* src[4] = {phiF0, psiF0, phiM0, psiM0};
+    const size_t n = (size_t)g.count() * g.dim;
+    for (int k = 0; k < 4; ++k) init[k].assign(src[k], src[k] + n);
+    gI = g;
+    have_init = true;
+  }
 
   // Metric masks (nonzero = inside) on their own grids; null for none.  Call before advancing.
   void set_masks(const T* mF, const Geom* gmF, const T* mM, const Geom* gmM) {
@@ -1204,10 +1219,11 @@ struct SynRun {
     smooth_image(M.data(), Ms.data(), gM, P.sigma[l], P.sigma_mm);
     if (l == 0) {
       S.g = gl;
-      S.phiF.assign((size_t)N * D, (T)0);
-      S.psiF.assign((size_t)N * D, (T)0);
-      S.phiM.assign((size_t)N * D, (T)0);
-      S.psiM.assign((size_t)N * D, (T)0);
+      std::vector<T>* fl[4] = {&S.phiF, &S.psiF, &S.phiM, &S.psiM};
+      for (int q = 0; q < 4; ++q) {
+        fl[q]->assign((size_t)N * D, (T)0);
+        if (have_init) resample_field(init[q].data(), gI, fl[q]->data(), gl);
+      }
     } else {
       std::vector<T>* fl[4] = {&S.phiF, &S.psiF, &S.phiM, &S.psiM};
       for (auto* v : fl) {
@@ -1274,18 +1290,32 @@ struct SynRun {
   }
 };
 
+// Initial half-fields of a stage (component planes on grid g), or all null.
+template <class T>
+struct SynInit {
+  const T* f[4] = {nullptr, nullptr, nullptr, nullptr};  // phiF, psiF, phiM, psiM
+  Geom g;
+};
+
 template <class T>
 inline void syn_register(const T* F_in, const Geom& gF, const T* M_in, const Geom& gM, const SynParams& P,
                          std::vector<T>& fwd, std::vector<T>& inv, Geom& gOut, SynLog* log = nullptr,
                          const T* maskF = nullptr, const Geom* gmF = nullptr, const T* maskM = nullptr,
-                         const Geom* gmM = nullptr) {
+                         const Geom* gmM = nullptr, const SynInit<T>* init = nullptr,
+                         std::vector<T>* half_out = nullptr) {
   SynRun<T> R(F_in, gF, M_in, gM, P);
   R.set_masks(maskF, gmF, maskM, gmM);
+  if (init && init->f[0]) R.set_initial_half_fields(init->f[0], init->f[1], init->f[2], init->f[3], init->g);
   while (!R.done) R.advance(INT64_MAX);
   fwd.swap(R.fwd);
   inv.swap(R.inv);
   gOut = R.S.g;
   if (log) *log = R.log;
+  if (half_out) {  // the final half-fields phiF, psiF, phiM, psiM, one after the other
+    half_out->clear();
+    for (const std::vector<T>* v : {&R.S.phiF, &R.S.psiF, &R.S.phiM, &R.S.psiM})
+      half_out->insert(half_out->end(), v->begin(), v->end());
+  }
 }
 
 }  // namespace synx_oracle

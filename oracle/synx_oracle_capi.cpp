@@ -171,6 +171,13 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
                                        synx_geom* gout, int32_t* log_level, int32_t* log_iter,       \
                                        double* log_metric, double* log_conv, int32_t* log_inv,       \
                                        int log_cap);                                                 \
+  int oracle_syn_register_full_##SUF(const T* F, const synx_geom* gF, const T* M, const synx_geom* gM, \
+                                     const synx_params* p, const T* maskF, const synx_geom* gmF,     \
+                                     const T* maskM, const synx_geom* gmM, const T* iphiF,           \
+                                     const T* ipsiF, const T* iphiM, const T* ipsiM,                 \
+                                     const synx_geom* gI, T* fwd, T* inv, T* half, synx_geom* gout,  \
+                                     int32_t* log_level, int32_t* log_iter, double* log_metric,      \
+                                     double* log_conv, int32_t* log_inv, int log_cap);               \
   int oracle_syn_register_##SUF(const T* F, const synx_geom* gF, const T* M, const synx_geom* gM,    \
                                 const synx_params* p, T* fwd, T* inv, synx_geom* gout,               \
                                 int32_t* log_level, int32_t* log_iter, double* log_metric,           \
@@ -186,17 +193,40 @@ void oracle_shrink_geom(const synx_geom* in, unsigned factor, synx_geom* out) {
                                        synx_geom* gout, int32_t* log_level, int32_t* log_iter,       \
                                        double* log_metric, double* log_conv, int32_t* log_inv,       \
                                        int log_cap) {                                                \
+    return oracle_syn_register_full_##SUF(F, gF, M, gM, p, maskF, gmF, maskM, gmM, nullptr, nullptr, \
+                                          nullptr, nullptr, nullptr, fwd, inv, nullptr, gout,        \
+                                          log_level, log_iter, log_metric, log_conv, log_inv, log_cap); \
+  }                                                                                                  \
+  /* The same, also with initial half-fields phiF, psiF, phiM, psiM (component planes on grid gI; \
+     null for none) and the final half-fields written one after the other to `half` (4 x D x N of  \
+     the last level grid; null: not wanted). */                                                      \
+  int oracle_syn_register_full_##SUF(const T* F, const synx_geom* gF, const T* M, const synx_geom* gM, \
+                                     const synx_params* p, const T* maskF, const synx_geom* gmF,     \
+                                     const T* maskM, const synx_geom* gmM, const T* iphiF,           \
+                                     const T* ipsiF, const T* iphiM, const T* ipsiM,                 \
+                                     const synx_geom* gI, T* fwd, T* inv, T* half, synx_geom* gout,  \
+                                     int32_t* log_level, int32_t* log_iter, double* log_metric,      \
+                                     double* log_conv, int32_t* log_inv, int log_cap) {              \
     SynParams P = to_params(p);                                                                      \
-    std::vector<T> f, v;                                                                             \
+    std::vector<T> f, v, hv;                                                                         \
     Geom go;                                                                                         \
     SynLog L;                                                                                        \
     Geom a, b;                                                                                       \
     if (gmF) a = to_geom(gmF);                                                                       \
     if (gmM) b = to_geom(gmM);                                                                       \
+    SynInit<T> init;                                                                                 \
+    if (iphiF && ipsiF && iphiM && ipsiM && gI) {                                                    \
+      init.f[0] = iphiF;                                                                             \
+      init.f[1] = ipsiF;                                                                             \
+      init.f[2] = iphiM;                                                                             \
+      init.f[3] = ipsiM;                                                                             \
+      init.g = to_geom(gI);                                                                          \
+    }                                                                                                \
     syn_register(F, to_geom(gF), M, to_geom(gM), P, f, v, go, &L, maskF, gmF ? &a : nullptr, maskM,  \
-                 gmM ? &b : nullptr);                                                                \
+                 gmM ? &b : nullptr, &init, half ? &hv : nullptr);                                   \
     std::copy(f.begin(), f.end(), fwd);                                                              \
     std::copy(v.begin(), v.end(), inv);                                                              \
+    if (half) std::copy(hv.begin(), hv.end(), half);                                                 \
     from_geom(go, gout);                                                                             \
     int nrec = (int)L.metric.size();                                                                 \
     for (int i = 0; i < nrec && i < log_cap; ++i) {                                                  \

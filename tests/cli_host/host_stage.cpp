@@ -7,10 +7,11 @@
 #include <string>
 #include <vector>
 #include "synx.h"
-extern "C" int oracle_syn_register_masked_f32(const float*, const synx_geom*, const float*, const synx_geom*,
-                                              const synx_params*, const float*, const synx_geom*, const float*,
-                                              const synx_geom*, float*, float*, synx_geom*, int32_t*, int32_t*,
-                                              double*, double*, int32_t*, int);
+extern "C" int oracle_syn_register_full_f32(const float*, const synx_geom*, const float*, const synx_geom*,
+                                            const synx_params*, const float*, const synx_geom*, const float*,
+                                            const synx_geom*, const float*, const float*, const float*, const float*,
+                                            const synx_geom*, float*, float*, float*, synx_geom*, int32_t*, int32_t*,
+                                            double*, double*, int32_t*, int);
 extern "C" void oracle_shrink_geom(const synx_geom*, unsigned, synx_geom*);
 struct synx_ctx {
   synx_params p;
@@ -18,6 +19,9 @@ struct synx_ctx {
   synx_geom gf, gm, go;
   std::vector<float> mF, mM;  // metric masks (empty: none)
   synx_geom gmF, gmM;
+  std::vector<float> init[4];  // initial half-fields, component planes (empty: none)
+  synx_geom gI;
+  std::vector<float> half;     // final half-fields, component planes one after the other
   std::vector<int32_t> lv, it, ki;
   std::vector<double> me, cv;
   bool done = false;
@@ -58,6 +62,20 @@ int synx_set_masks(synx_ctx* c, const float* mf, const synx_geom* gmf, const flo
   if (mm) { c->gmM = *gmm; c->mM.assign(mm, mm + gmm->size[0] * gmm->size[1] * gmm->size[2]); }
   return 0;
 }
+int synx_set_initial_half_fields(synx_ctx* c, const float* a, const float* b, const float* d, const float* e,
+                                 const synx_geom* g) {
+  for (auto& v : c->init) v.clear();
+  if (!a) return 0;
+  c->gI = *g;
+  const size_t N = g->size[0] * g->size[1] * g->size[2], D = g->dim;
+  const float* src[4] = {a, b, d, e};
+  for (int k = 0; k < 4; ++k) {
+    c->init[k].resize(N * D);
+    for (size_t i = 0; i < N; ++i)
+      for (size_t q = 0; q < D; ++q) c->init[k][q * N + i] = src[k][i * D + q];
+  }
+  return 0;
+}
 int synx_run_level(synx_ctx* c, int level) {
   if (c->done || level != c->p.n_levels - 1) return 0;  // the whole stage runs at the last level
   synx_geom go;
@@ -66,11 +84,15 @@ int synx_run_level(synx_ctx* c, int level) {
   std::vector<float> f(N * D), v(N * D);
   const int cap = 100000;
   c->lv.resize(cap); c->it.resize(cap); c->ki.resize(cap); c->me.resize(cap); c->cv.resize(cap);
-  int n = oracle_syn_register_masked_f32(c->F.data(), &c->gf, c->M.data(), &c->gm, &c->p,
-                                         c->mF.empty() ? nullptr : c->mF.data(), c->mF.empty() ? nullptr : &c->gmF,
-                                         c->mM.empty() ? nullptr : c->mM.data(), c->mM.empty() ? nullptr : &c->gmM,
-                                         f.data(), v.data(), &c->go, c->lv.data(), c->it.data(), c->me.data(),
-                                         c->cv.data(), c->ki.data(), cap);
+  const bool ini = !c->init[0].empty();
+  c->half.resize(4 * N * D);
+  int n = oracle_syn_register_full_f32(c->F.data(), &c->gf, c->M.data(), &c->gm, &c->p,
+                                       c->mF.empty() ? nullptr : c->mF.data(), c->mF.empty() ? nullptr : &c->gmF,
+                                       c->mM.empty() ? nullptr : c->mM.data(), c->mM.empty() ? nullptr : &c->gmM,
+                                       ini ? c->init[0].data() : nullptr, ini ? c->init[1].data() : nullptr,
+                                       ini ? c->init[2].data() : nullptr, ini ? c->init[3].data() : nullptr,
+                                       ini ? &c->gI : nullptr, f.data(), v.data(), c->half.data(), &c->go,
+                                       c->lv.data(), c->it.data(), c->me.data(), c->cv.data(), c->ki.data(), cap);
   for (auto* a : {&c->lv, &c->it, &c->ki}) a->resize(n);
   c->me.resize(n); c->cv.resize(n);
   c->fwd.resize(N * D); c->inv.resize(N * D);
@@ -80,6 +102,15 @@ int synx_run_level(synx_ctx* c, int level) {
   return 0;
 }
 int synx_get_output_geom(const synx_ctx* c, synx_geom* g) { *g = c->go; return 0; }
+int synx_get_half_fields(synx_ctx* c, float* a, float* b, float* d, float* e) {
+  const size_t N = c->go.size[0] * c->go.size[1] * c->go.size[2], D = c->p.dim;
+  float* dst[4] = {a, b, d, e};
+  for (int k = 0; k < 4; ++k)
+    if (dst[k])
+      for (size_t i = 0; i < N; ++i)
+        for (size_t q = 0; q < D; ++q) dst[k][i * D + q] = c->half[(k * D + q) * N + i];
+  return 0;
+}
 int synx_get_fields(synx_ctx* c, float* fw, float* iv) {
   std::memcpy(fw, c->fwd.data(), 4 * c->fwd.size()); std::memcpy(iv, c->inv.data(), 4 * c->inv.size()); return 0; }
 int synx_get_log(synx_ctx* c, int32_t* level, int32_t* iter, double* metric, double* conv, int32_t* inv, int64_t cap, int64_t* count) {

@@ -46,7 +46,9 @@ def test_nifti_roundtrip_scalar_and_vector(tmp_path):
      "must match the levels"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-f", "1", "-s", "0", "-o", "x"], "no convergence"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
-      "--restore-state", "state.h5"], "not supported"),
+      "--restore-state", "/nonexistent/state.txt"], "cannot read"),
+    (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
+      "--save-state", "state.txt"], "--save-state requires --write-composite-transform"),
     (["-d", "4", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x"],
      "dimensionality"),
     (["-d", "3", "-m", "CC[/nonexistent/f.nii.gz,/nonexistent/m.nii.gz,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10",
@@ -58,7 +60,9 @@ def test_nifti_roundtrip_scalar_and_vector(tmp_path):
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
       "-r", "/nonexistent/a.mat"], "cannot open transform file"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
-      "-a", "1"], "write-composite-transform"),
+      "-i", "1"], "--initialize-transforms-per-stage requires --write-composite-transform"),
+    (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
+      "-a", "1", "-i", "1"], "mutually exclusive"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
       "-q", "a.mat"], "initial-fixed-transform"),
 ])

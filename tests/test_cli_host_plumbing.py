@@ -111,3 +111,17 @@ def test_masks(host_cli, tmp_path):
         return np.moveaxis(fwd, 0, -1), np.moveaxis(inv, 0, -1)
 
     X.check_cli_masks(host_cli["reg"], tmp_path, stage_fields)
+
+
+def test_state_and_composite(host_cli, tmp_path):
+    import oracle as O
+    import test_zz_u_state as U
+
+    def stage(f, gf, m, gm, P, init):
+        kw = {}
+        if init is not None:
+            kw = dict(initial_half_fields=[U.planes(a) for a in init], initial_geom=gf)
+        fwd, inv, _, _, half = O.syn_register(f, gf, m, gm, P, return_half_fields=True, **kw)
+        return U.interleaved(fwd), U.interleaved(inv), [U.interleaved(h) for h in half]
+
+    U.check_cli_state(host_cli["reg"], tmp_path, stage)
