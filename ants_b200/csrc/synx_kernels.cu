@@ -1623,9 +1623,118 @@ __global__ void __launch_bounds__(256) k_conv_image_axis(const float* __restrict
   }
 }
 
+// The same pass with the radius a compile-time constant, in two forms whose sums are the generic
+// kernel's (coefficient j times the replicate-edge sample pos - R + j, j ascending, in FP64 FMAs):
+//  * along x, each warp converts its row segment and halo to double once into shared memory and sums
+//    from there (the taps are immediate offsets);
+//  * along y or z, each thread walks a chunk of its line with the last 2R+1 samples in registers
+//    (unrolled by 2R+1 so every ring index is a compile-time constant): one load and one conversion
+//    per output instead of 2R+1.
+constexpr int kConvImageMaxR = 16;
+
+template <int R>
+__global__ void __launch_bounds__(256) k_conv_image_x(const float* __restrict__ in, float* __restrict__ out, Dims d,
+                                                      const double* __restrict__ coeffs) {
+  constexpr int K = 2 * R + 1, W = 32 + 2 * R;
+  __shared__ double buf[8][W];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x0 = blockIdx.x * 32, y = blockIdx.y * 8 + w, z = blockIdx.z;
+  if (y >= d.ny) return;  // the whole warp; no block-wide barrier below
+  double c[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) c[j] = __ldg(coeffs + j);
+  const long long row = ((long long)z * d.ny + y) * d.nx;
+  const float* line = in + row;
+  for (int k = lane; k < W; k += 32) buf[w][k] = (double)__ldg(line + min(max(x0 - R + k, 0), d.nx - 1));
+  __syncwarp();
+  const int x = x0 + lane;
+  if (x >= d.nx) return;
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < K; ++j) acc = fma(c[j], buf[w][lane + j], acc);
+  out[row + x] = (float)acc;
+}
+
+template <int R, int AXIS>
+__global__ void __launch_bounds__(256) k_conv_image_walk(const float* __restrict__ in, float* __restrict__ out, Dims d,
+                                                         const double* __restrict__ coeffs, int chunk) {
+  constexpr int K = 2 * R + 1;
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int o = blockIdx.y * 8 + (threadIdx.x >> 5);  // z for a y walk, y for a z walk
+  const int len = AXIS == 1 ? d.ny : d.nz;
+  if (x >= d.nx || o >= (AXIS == 1 ? d.nz : d.ny)) return;
+  const long long stride = AXIS == 1 ? (long long)d.nx : (long long)d.nx * d.ny;
+  const long long base = AXIS == 1 ? (long long)o * d.nx * d.ny + x : (long long)o * d.nx + x;
+  const int p0 = blockIdx.z * chunk, p1 = min(p0 + chunk, len);
+  double c[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) c[j] = __ldg(coeffs + j);
+  double ring[K];
+#pragma unroll
+  for (int u = 0; u < 2 * R; ++u) ring[u] = (double)__ldg(in + base + min(max(p0 - R + u, 0), len - 1) * stride);
+  for (int pb = p0; pb < p1; pb += K) {
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+      const int p = pb + u;
+      if (p < p1) {
+        ring[(u + 2 * R) % K] = (double)__ldg(in + base + min(p + R, len - 1) * stride);
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc = fma(c[j], ring[(u + j) % K], acc);
+        out[base + p * stride] = (float)acc;
+      }
+    }
+  }
+}
+
+template <int R>
+static void conv_image_axis_t(const float* in, float* out, const GridInfo& g, int axis, const double* coeffs,
+                              cudaStream_t s) {
+  const Dims& d = g.d;
+  const int gx = (d.nx + 31) / 32;
+  if (axis == 0) {
+    k_conv_image_x<R><<<dim3(gx, (d.ny + 7) / 8, d.nz), 256, 0, s>>>(in, out, d, coeffs);
+    return;
+  }
+  const int other = axis == 1 ? d.nz : d.ny, len = axis == 1 ? d.ny : d.nz;
+  const int cols = gx * ((other + 7) / 8);
+  // about 8 walking warps per SM; a chunk is at least 2R + 1 long, its warm-up being 2R loads
+  const int chunks = std::max(1, std::min(len, (148 * 8 + cols - 1) / cols));
+  const int chunk = std::min(len, std::max((len + chunks - 1) / chunks, 2 * R + 1));
+  const dim3 grid(gx, (other + 7) / 8, (len + chunk - 1) / chunk);
+  if (axis == 1) k_conv_image_walk<R, 1><<<grid, 256, 0, s>>>(in, out, d, coeffs, chunk);
+  else k_conv_image_walk<R, 2><<<grid, 256, 0, s>>>(in, out, d, coeffs, chunk);
+}
+
 void launch_conv_image_axis(const float* in, float* out, const GridInfo& g, int axis, const double* coeffs, int R,
                             cudaStream_t s) {
   count_launch();
+  switch (R) {
+#define SYNX_CONV_IMG(RV)                                   \
+  case RV:                                                  \
+    conv_image_axis_t<RV>(in, out, g, axis, coeffs, s);     \
+    return;
+    SYNX_CONV_IMG(1)
+    SYNX_CONV_IMG(2)
+    SYNX_CONV_IMG(3)
+    SYNX_CONV_IMG(4)
+    SYNX_CONV_IMG(5)
+    SYNX_CONV_IMG(6)
+    SYNX_CONV_IMG(7)
+    SYNX_CONV_IMG(8)
+    SYNX_CONV_IMG(9)
+    SYNX_CONV_IMG(10)
+    SYNX_CONV_IMG(11)
+    SYNX_CONV_IMG(12)
+    SYNX_CONV_IMG(13)
+    SYNX_CONV_IMG(14)
+    SYNX_CONV_IMG(15)
+    SYNX_CONV_IMG(16)
+#undef SYNX_CONV_IMG
+    default:
+      break;
+  }
+  static_assert(kConvImageMaxR == 16, "the switch covers 1..kConvImageMaxR");
   const Map3 m = map3(g.d);
   k_conv_image_axis<<<m.grid, 256, 0, s>>>(in, out, g.d, m.zb, axis, coeffs, R);
 }
