@@ -3,11 +3,40 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "synx_cc_tile.cuh"
 #include "synx_level.cuh"
 
 namespace synx {
+
+// The window counts' reciprocals (CCParams::rcp), one table per device in a file-scope device array
+// (no allocation): filled from the host's IEEE divisions, which round correctly like the device's
+// reciprocal, by cc_prepare before any launch that reads it; its address is cached per device.
+__device__ double g_cc_rcp[kCCRcpMax + 1];
+
+static const double* cc_rcp_table(bool fill) {
+  static std::mutex mu;
+  static std::map<int, const double*> addr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = addr.find(dev);
+  if (it != addr.end()) return it->second;
+  if (!fill) return nullptr;
+  std::vector<double> h(kCCRcpMax + 1, 0.0);
+  for (int n = 1; n <= kCCRcpMax; ++n) h[n] = 1.0 / (double)n;
+  void* p = nullptr;
+  if (cudaMemcpyToSymbol(g_cc_rcp, h.data(), sizeof(double) * h.size()) != cudaSuccess ||
+      cudaGetSymbolAddress(&p, g_cc_rcp) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  addr[dev] = static_cast<const double*>(p);
+  return addr[dev];
+}
 
 // Standalone CC kernel: one tile per block, deterministic metric reduction (block partials,
 // the last block sums them in order).
@@ -159,6 +188,7 @@ static cudaError_t cc_prepare_t() {
 }
 
 cudaError_t cc_prepare(int dim, int radius) {
+  if (cc_rcp_table(true) == nullptr) return cudaErrorInitializationError;
 #define SYNX_CC_PREP(RR) \
   case RR:               \
     return dim == 3 ? cc_prepare_t<RR, 3>() : cc_prepare_t<RR, 2>();
@@ -191,6 +221,8 @@ CCParams make_cc_params(const GridInfo& g, int radius, int chunks) {
   P.identity_dir = ident ? 1 : 0;
   P.eps = 1.1920928955078125e-07;  // FLT_EPSILON: the reference metric's float guard
   P.valid = nullptr;
+  P.rcp = cc_rcp_table(false);  // set up by cc_prepare, which every entry point calls first (else null:
+                                // the tile computes the reciprocals)
   P.ZC = cc_zchunk(g, radius, chunks);
   return P;
 }

@@ -38,7 +38,12 @@ struct CCParams {
   double eps;
   int ZC;          // z-chunk per block
   const unsigned char* valid;  // metric masks: nonzero = valid voxel (MASKED tiles only)
+  // 1/n for n = 0..kCCRcpMax, each the correctly rounded double (the window's voxel count n is an
+  // integer, so a table lookup replaces the reciprocal sequence; entry 0 is unused)
+  const double* rcp;
 };
+
+constexpr int kCCRcpMax = 15 * 15 * 15;  // the largest window, radius 7 in 3-D
 
 __device__ __forceinline__ int pmod(int a, int m) {
   int r = a % m;
@@ -66,6 +71,7 @@ struct CCShape {
   static constexpr int XSP = TX + 1;   // row pitch of the window sums (odd)
   static constexpr int XSEG = 8;       // outputs per x-pass task
   static_assert(TX % XSEG == 0, "x segments tile the output row");
+  static constexpr bool EXACT = CPT * NT == HC;  // every thread owns exactly CPT halo columns
   static constexpr size_t smem = (size_t)RD * HC * sizeof(float2) + (size_t)NQ * HY * CSP * sizeof(T) +
                                  (size_t)NQ * TY * CSP * sizeof(T) + (size_t)NQ * TY * XSP * sizeof(T) +
                                  (MASKED ? (size_t)RD * HC : 0);
@@ -135,7 +141,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     int col = tid + c * NT;
     int hx = col % HX, hy = col / HX;
     int gx = x0 - R + hx, gy = y0 - R + hy;
-    gval[c] = col < HC && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+    gval[c] = (S::EXACT || col < HC) && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
     gofs[c] = gval[c] ? gy * nx + gx : 0;
     sofs[c] = hy * CSP + hx;
   }
@@ -153,7 +159,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
       int col = tid + c * NT;
-      if (col < HC) {
+      if (S::EXACT || col < HC) {
         float2 v = make_float2(0.0f, 0.0f);
         unsigned char vb = 0;
         if (zin && gval[c]) {
@@ -212,7 +218,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
       int col = tid + c * NT;
-      if (col < HC) {
+      if (S::EXACT || col < HC) {
         if (sub && gval[c] && (!MASKED || vring[slot * HC + col])) {
           float2 o = ring[slot * HC + col];
           const T f = o.x, m = o.y;
@@ -250,7 +256,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     __syncthreads();
     // y box sums, sliding down one halo column over the TY output rows (one task per quantity and
     // halo column)
-    for (int task = tid; task < NQ * HX; task += NT) {
+    for (int task = tid; task < NQ * HX; task += NT) {  // one pass when the tasks fit the block
       const int yq = task / HX, ycol = task - yq * HX;
       const T* src = cs + yq * HY * CSP + ycol;
       T* dst = ys + yq * TY * CSP + ycol;
@@ -261,6 +267,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         s += src[(y + 2 * R) * CSP] - src[(y - 1) * CSP];
         dst[y * CSP] = s;
       }
+      if (NQ * HX <= NT) break;
     }
     __syncthreads();
     // x box sums, sliding along an output row: outputs XSEG k .. XSEG k + XSEG-1 (one task per
@@ -276,6 +283,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         s += src[x + 2 * R] - src[x - 1];
         dst[x] = s;
       }
+      if (NQ * TY * (TX / S::XSEG) <= NT) break;
     }
     __syncthreads();
     const int cidx = (ty + R) * HX + (tx + R);
@@ -293,7 +301,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       const T czn = (T)(min(zc + RZ, nz - 1) - max(zc - RZ, 0) + 1);
       const T n = MASKED ? Sq[NQ - 1] : cxn * cyn * czn;
       if (MASKED) n_valid += 1.0;
-      const T inv_n = rcp_rn(n);
+      // the same bits either way; the table saves the reciprocal sequence
+      const T inv_n = (sizeof(T) == 8 && P.rcp != nullptr) ? (T)__ldg(P.rcp + (int)n) : rcp_rn(n);
       const T mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
       const T sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
       const T sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;
