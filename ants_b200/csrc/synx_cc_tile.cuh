@@ -82,21 +82,6 @@ struct CCShape {
   static constexpr bool END_BARRIER = DIM == 3 && R < 2;
 };
 
-// Sum of the K values src[0], src[stride], ..., src[(K-1) stride], added pairwise (a tree of depth
-// ceil(log2 K)) so that the first window of a sliding pass is not a chain of K dependent additions.
-// The sliding steps that follow add (entering - leaving), one dependent addition per output.
-template <int K, typename T>
-__device__ __forceinline__ T window_sum(const T* src, int stride) {
-  T v[K];
-#pragma unroll
-  for (int j = 0; j < K; ++j) v[j] = src[j * stride];
-#pragma unroll
-  for (int w = 1; w < K; w *= 2)
-#pragma unroll
-    for (int j = 0; j + w < K; j += 2 * w) v[j] += v[j + w];
-  return v[0];
-}
-
 template <typename T>
 __device__ __forceinline__ T rcp_rn(T x);
 template <>
@@ -106,6 +91,33 @@ __device__ __forceinline__ double rcp_rn<double>(double x) {
 template <>
 __device__ __forceinline__ float rcp_rn<float>(float x) {
   return __frcp_rn(x);
+}
+
+// One sliding pass of a task: dst[y * dstride] = sum of src[(y + j) * stride], j = 0..2R, for
+// y = 0..NOUT-1.  The first window is summed pairwise (a tree of depth ceil(log2(2R+1)), not a
+// chain of 2R+1 dependent additions) and each slide adds (entering - leaving), one dependent
+// addition per output.  The 2R + NOUT inputs are loaded once into registers (the slides reuse the
+// window's values instead of reloading them past the stores).
+template <int R, int NOUT, typename T>
+__device__ __forceinline__ void slide_sums(const T* src, int stride, T* dst, int dstride) {
+  constexpr int K = 2 * R + 1, L = K + NOUT - 1;
+  T v[L];
+#pragma unroll
+  for (int j = 0; j < L; ++j) v[j] = src[j * stride];
+  T w[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) w[j] = v[j];
+#pragma unroll
+  for (int m = 1; m < K; m *= 2)
+#pragma unroll
+    for (int j = 0; j + m < K; j += 2 * m) w[j] += w[j + m];
+  T s = w[0];
+  dst[0] = s;
+#pragma unroll
+  for (int y = 1; y < NOUT; ++y) {
+    s += v[y + 2 * R] - v[y - 1];
+    dst[y * dstride] = s;
+  }
 }
 
 // One CC tile: output columns x in [32 bx, 32 bx + 32), y in [8 by, 8 by + 8), z chunk bz.
@@ -258,15 +270,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     // halo column)
     for (int task = tid; task < NQ * HX; task += NT) {  // one pass when the tasks fit the block
       const int yq = task / HX, ycol = task - yq * HX;
-      const T* src = cs + yq * HY * CSP + ycol;
-      T* dst = ys + yq * TY * CSP + ycol;
-      T s = window_sum<2 * R + 1>(src, CSP);
-      dst[0] = s;
-#pragma unroll
-      for (int y = 1; y < TY; ++y) {
-        s += src[(y + 2 * R) * CSP] - src[(y - 1) * CSP];
-        dst[y * CSP] = s;
-      }
+      slide_sums<R, TY>(cs + yq * HY * CSP + ycol, CSP, ys + yq * TY * CSP + ycol, CSP);
       if (NQ * HX <= NT) break;
     }
     __syncthreads();
@@ -274,15 +278,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     // quantity, output row and segment; consecutive threads take consecutive rows)
     for (int task = tid; task < NQ * TY * (TX / S::XSEG); task += NT) {
       const int row = task % (NQ * TY), seg = task / (NQ * TY);
-      const T* src = ys + row * CSP + S::XSEG * seg;
-      T* dst = ws + row * XSP + S::XSEG * seg;
-      T s = window_sum<2 * R + 1>(src, 1);
-      dst[0] = s;
-#pragma unroll
-      for (int x = 1; x < S::XSEG; ++x) {
-        s += src[x + 2 * R] - src[x - 1];
-        dst[x] = s;
-      }
+      slide_sums<R, S::XSEG>(ys + row * CSP + S::XSEG * seg, 1, ws + row * XSP + S::XSEG * seg, 1);
       if (NQ * TY * (TX / S::XSEG) <= NT) break;
     }
     __syncthreads();
