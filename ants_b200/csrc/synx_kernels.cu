@@ -1632,27 +1632,34 @@ __global__ void __launch_bounds__(256) k_conv_image_axis(const float* __restrict
 //    per output instead of 2R+1.
 constexpr int kConvImageMaxR = 16;
 
+constexpr int kConvImageXSlices = 8;  // rows of consecutive slices per warp of the x pass
+
 template <int R>
 __global__ void __launch_bounds__(256) k_conv_image_x(const float* __restrict__ in, float* __restrict__ out, Dims d,
                                                       const double* __restrict__ coeffs) {
   constexpr int K = 2 * R + 1, W = 32 + 2 * R;
   __shared__ double buf[8][W];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int x0 = blockIdx.x * 32, y = blockIdx.y * 8 + w, z = blockIdx.z;
+  const int x0 = blockIdx.x * 32, y = blockIdx.y * 8 + w;
   if (y >= d.ny) return;  // the whole warp; no block-wide barrier below
   double c[K];
 #pragma unroll
   for (int j = 0; j < K; ++j) c[j] = __ldg(coeffs + j);
-  const long long row = ((long long)z * d.ny + y) * d.nx;
-  const float* line = in + row;
-  for (int k = lane; k < W; k += 32) buf[w][k] = (double)__ldg(line + min(max(x0 - R + k, 0), d.nx - 1));
-  __syncwarp();
   const int x = x0 + lane;
-  if (x >= d.nx) return;
-  double acc = 0.0;
+  const int z0 = blockIdx.z * kConvImageXSlices, z1 = min(z0 + kConvImageXSlices, d.nz);
+  for (int z = z0; z < z1; ++z) {
+    const long long row = ((long long)z * d.ny + y) * d.nx;
+    const float* line = in + row;
+    __syncwarp();  // the previous row's reads of buf are done
+    for (int k = lane; k < W; k += 32) buf[w][k] = (double)__ldg(line + min(max(x0 - R + k, 0), d.nx - 1));
+    __syncwarp();
+    if (x < d.nx) {
+      double acc = 0.0;
 #pragma unroll
-  for (int j = 0; j < K; ++j) acc = fma(c[j], buf[w][lane + j], acc);
-  out[row + x] = (float)acc;
+      for (int j = 0; j < K; ++j) acc = fma(c[j], buf[w][lane + j], acc);
+      out[row + x] = (float)acc;
+    }
+  }
 }
 
 template <int R, int AXIS>
@@ -1693,7 +1700,8 @@ static void conv_image_axis_t(const float* in, float* out, const GridInfo& g, in
   const Dims& d = g.d;
   const int gx = (d.nx + 31) / 32;
   if (axis == 0) {
-    k_conv_image_x<R><<<dim3(gx, (d.ny + 7) / 8, d.nz), 256, 0, s>>>(in, out, d, coeffs);
+    k_conv_image_x<R><<<dim3(gx, (d.ny + 7) / 8, (d.nz + kConvImageXSlices - 1) / kConvImageXSlices), 256, 0, s>>>(
+        in, out, d, coeffs);
     return;
   }
   const int other = axis == 1 ? d.nz : d.ny, len = axis == 1 ? d.ny : d.nz;

@@ -62,7 +62,7 @@ BYTES_PER_INV_VOXEL = 36  # one fixed-point sub-iteration, one half-field voxel:
 ROOF_LEVEL = 3  # the 182x218x182 level: one iteration graph per replay
 # DRAM bytes (read + write) of one replay of that iteration graph, from the ncu capture summarised
 # in profiles/iteration_graph_182x218x182.md (one pass per graph, every replay of two registrations)
-ITER_GRAPH_TRAFFIC_BYTES = 2.784e9  # 1.722 GB read + 1.063 GB written (mean of 40 replays)
+ITER_GRAPH_TRAFFIC_BYTES = 2.665e9  # 1.607 GB read + 1.058 GB written (mean of 40 replays)
 
 
 DATA = "synthetic: seeded layered-ellipsoid phantom pair, moving = fixed warped by a smooth field"
