@@ -305,7 +305,8 @@ ArenaPlan arena_plan(const synx_ctx* c) {
     invb = std::max(invb, inv_blocks(g));
   }
   invb = std::max(invb, 2048);
-  for (auto& g : c->lv) invb = (int)std::max<long long>(invb, level_inv_units(g));  // level kernel: one slot per tile
+  // level kernel: two slots per tile (its sub-iterations alternate between them)
+  for (auto& g : c->lv) invb = (int)std::max<long long>(invb, 2 * level_inv_units(g));
   // step entry points on arbitrary grids reuse nothing from here
   const int coeff_cap = 1024;
   int max_iters = 1;
@@ -810,7 +811,7 @@ cudaError_t enqueue_iteration(synx_ctx* c, bool profile, bool loops = false, boo
 // kernels; 0.9 M voxels 16.0 ms vs 14.3 ms.
 constexpr long long kPersistentMaxVoxels = 400000;
 
-// Inversion tiles per half-field of the level kernel on grid g (one residual partial slot each).
+// Inversion tiles per half-field of the level kernel on grid g (two residual partial slots each).
 long long level_inv_units(const GridInfo& g) {
   const int zb = level_zb(g.d, 2);
   return (long long)((g.d.nx + 31) / 32) * ((g.d.ny + 7) / 8) * ((g.d.nz + zb - 1) / zb);
@@ -827,7 +828,7 @@ bool persistent_capable(synx_ctx* c, const GridInfo& g, bool profile) {
   for (int a = 0; a < c->D; ++a) rs = std::max(rs, c->R_upd[a]);
   if (rs > kLevelMaxSmoothRadius) return false;
   if (c->P.cc_radius < 1 || c->P.cc_radius > 7) return false;
-  return level_inv_units(g) <= c->inv_cap;
+  return 2 * level_inv_units(g) <= c->inv_cap;
 }
 
 bool persistent_eligible(synx_ctx* c, const GridInfo& g, bool profile) {

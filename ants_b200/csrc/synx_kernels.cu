@@ -1274,31 +1274,41 @@ __global__ void __launch_bounds__(256, kInvSpecBlocksPerSM) k_invert_spec(const 
   }
   const float eps = k == 0 ? 0.75f : 0.5f;
   // Seed the running bound before the tiles: one lane per warp evaluates the residual norm of the
-  // current iterate at one voxel of a sample spread over the whole half-field (a multiplicative hash of
-  // the warp's index; ~4700 voxels at full resolution), exactly as the pass computes it, so the maximum
-  // of these is a lower bound of the field's maximum.  Without it the first tiles, before any bound is
-  // known, defer most of their voxels; with one sample per thread the scattered gathers cost more DRAM
-  // traffic than the deferrals they save.
+  // current iterate at one voxel, exactly as the pass computes it, so the maximum of these is a lower
+  // bound of the field's maximum.  The voxels lie in this block's own tiles (warp w samples the tile
+  // w/8 of the way through the block's walk), which no other block writes and this one has not
+  // started, so each sample is the residual of the iterate the pass starts from; a voxel of another
+  // block's tile could already hold its update.  The blocks' walks interleave over the whole grid, so
+  // the samples (~4700 at full resolution) spread over the field.  Without them the first tiles,
+  // before any bound is known, defer most of their voxels; with one sample per thread the scattered
+  // gathers cost more DRAM traffic than the deferrals they save.
   {
     float nrm = 0.0f;
-    if ((threadIdx.x & 31) == 0) {
+    const int ntiles = L.tx * L.ty * L.tz;
+    const int nw = blockDim.x >> 5, w = threadIdx.x >> 5;
+    const int J = bid < ntiles ? (ntiles - 1 - bid) / nb + 1 : 0;  // tiles of this block's walk
+    if ((threadIdx.x & 31) == 0 && J > 0) {
       const Dims& d = a.g;
-      const long long N = d.N;
-      const long long w = (long long)bid * (blockDim.x >> 5) + (threadIdx.x >> 5);
-      const long long j = (w * 2654435761LL) % N;
-      const int x = (int)(j % d.nx), y = (int)((j / d.nx) % d.ny), z = (int)(j / ((long long)d.nx * d.ny));
-      const float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
-      const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
-      float p[3] = {psi[j], psi[N + j], DIM == 3 ? psi[2 * N + j] : 0.0f};
-      float e[3];
-      inv_residual<DIM, DIAG>(phi, d, a.A, (float)x, (float)y, (float)z, p, e);
-      float s2 = 0.0f;
+      const int t = bid + (w * J / nw) * nb;
+      const int bx = t % L.tx, r = t / L.tx, by = r % L.ty, bz = r / L.ty;
+      const int x = bx * 32 + ((w * 13 + 5) & 31), y = by * 8 + (w & 7);
+      const int z = bz * a.zb + (w * 3) % a.zb;
+      if (x < d.nx && y < d.ny && z < d.nz) {
+        const long long N = d.N;
+        const long long j = ((long long)z * d.ny + y) * d.nx + x;
+        const float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
+        const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
+        float p[3] = {psi[j], psi[N + j], DIM == 3 ? psi[2 * N + j] : 0.0f};
+        float e[3];
+        inv_residual<DIM, DIAG>(phi, d, a.A, (float)x, (float)y, (float)z, p, e);
+        float s2 = 0.0f;
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        const float v = e[c] * a.ih[c];
-        s2 += v * v;
+        for (int c = 0; c < DIM; ++c) {
+          const float v = e[c] * a.ih[c];
+          s2 += v * v;
+        }
+        nrm = sqrtf(s2);
       }
-      nrm = sqrtf(s2);
     }
     const float bm = block_max_f(nrm, redf);
     if (threadIdx.x == 0) atomicMax(&C.mrun, __float_as_uint(bm));

@@ -22,7 +22,7 @@ struct LevelArgs {
   double* cc_partials;
   double* inv_psum;
   float* inv_pmax;
-  int pcap;             // partial slots per half (>= inversion tiles per half)
+  int pcap;             // partial slots per half (>= 2 x inversion tiles per half)
   int iters;            // iterations of the level
   int r_smooth;         // update-field smoothing radius (1..8)
   int cc_gx, cc_gy, cc_gz;

@@ -117,9 +117,9 @@ __device__ float smooth_z_dispatch(const LevelArgs& A, int bx, int by, int zc, i
   }
 }
 
-// Deterministic reduction of the per-tile partials (n per half; sum and max per half): every
-// block that runs it gets bit-identical results.
-__device__ void reduce_partials(const LevelArgs& A, int n, double out_sum[2], float out_max[2], double* redd,
+// Deterministic reduction of the per-tile partials (n per half, starting at slot `off` of each
+// half; sum and max per half): every block that runs it gets bit-identical results.
+__device__ void reduce_partials(const LevelArgs& A, int n, int off, double out_sum[2], float out_max[2], double* redd,
                                 float* redf) {
   __shared__ double s_sum[2];
   __shared__ float s_max[2];
@@ -127,8 +127,8 @@ __device__ void reduce_partials(const LevelArgs& A, int n, double out_sum[2], fl
     double s = 0.0;
     float m = 0.0f;
     for (int b = threadIdx.x; b < n; b += blockDim.x) {
-      s += __ldcg(A.inv_psum + h * A.pcap + b);
-      m = fmaxf(m, __ldcg(A.inv_pmax + h * A.pcap + b));
+      s += __ldcg(A.inv_psum + h * A.pcap + off + b);
+      m = fmaxf(m, __ldcg(A.inv_pmax + h * A.pcap + off + b));
     }
     block_sum_max(s, m, redd, redf);
     if (threadIdx.x == 0) {
@@ -144,7 +144,11 @@ __device__ void reduce_partials(const LevelArgs& A, int n, double out_sum[2], fl
 }
 
 // One fixed-point inversion of both halves (psi <- inv(phi), warm-started from psi).  Each tile
-// writes its own residual partials, so the statistics do not depend on the group size.
+// writes its own residual partials, so the statistics do not depend on the group size.  After the
+// barrier that ends a sub-iteration every block reads all of that sub-iteration's partials, while
+// faster blocks may already write the next one's: consecutive sub-iterations use the two halves of
+// each half-field's slots in turn (nh slots each), and two sub-iterations apart a barrier lies between
+// the last read and the next write.
 template <int DIM, bool DIAG>
 __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, const Grp& gp, double* redd,
                               float* redf) {
@@ -161,14 +165,14 @@ __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, c
     invert_tile<DIM, DIAG>(I, h, bx, by, bz, false, true, 0.0f, 0.0f, acc, mx);
     block_sum_max(acc, mx, redd, redf);
     if (threadIdx.x == 0) {
-      A.inv_psum[h * A.pcap + (u - h * nh)] = acc;
+      A.inv_psum[h * A.pcap + (u - h * nh)] = acc;  // sub-iteration 0: first slot set
       A.inv_pmax[h * A.pcap + (u - h * nh)] = mx;
     }
   }
   if (!grid_barrier(ctl, gp.G + A.bar_extra, A.bar_spins)) return false;
   double sum[2];
   float mxv[2];
-  reduce_partials(A, nh, sum, mxv, redd, redf);
+  reduce_partials(A, nh, 0, sum, mxv, redd, redf);
   bool exec[2] = {true, true};
   int iters[2] = {0, 0};
   for (int k = 1; k <= A.inv_max_iter; ++k) {
@@ -192,13 +196,13 @@ __device__ bool inverse_phase(const LevelArgs& A, const InvArgs& I, int phase, c
       if (st[h]) {
         block_sum_max(acc, mx, redd, redf);
         if (threadIdx.x == 0) {
-          A.inv_psum[h * A.pcap + (u - h * nh)] = acc;
-          A.inv_pmax[h * A.pcap + (u - h * nh)] = mx;
+          A.inv_psum[h * A.pcap + (k & 1) * nh + (u - h * nh)] = acc;
+          A.inv_pmax[h * A.pcap + (k & 1) * nh + (u - h * nh)] = mx;
         }
       }
     }
     if (!grid_barrier(ctl, gp.G + A.bar_extra, A.bar_spins)) return false;
-    if (st[0] || st[1]) reduce_partials(A, nh, sum, mxv, redd, redf);
+    if (st[0] || st[1]) reduce_partials(A, nh, (k & 1) * nh, sum, mxv, redd, redf);
     exec[0] = st[0];
     exec[1] = st[1];
   }
