@@ -124,9 +124,9 @@ __device__ __forceinline__ void slide_sums(const T* src, int stride, T* dst, int
 // Returns the tile's sum of local cc (valid in thread 0).  All NT threads of the block must call
 // it; `smem_raw` holds CCShape<R, DIM, T, MASKED>::smem bytes and `red` 32 doubles.
 template <int R, int DIM, typename T = double, bool MASKED = false, int NT = 256>
-__device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const float* __restrict__ Mt, const Dims& d,
-                                          const CCParams& P, float* __restrict__ gF, float* __restrict__ gM,
-                                          float* __restrict__ cc_out, int bx, int by, int bz,
+__device__ __forceinline__ double cc_tile(const float* SYNX_RESTRICT Ft, const float* SYNX_RESTRICT Mt, const Dims& d,
+                                          const CCParams& P, float* SYNX_RESTRICT gF, float* SYNX_RESTRICT gM,
+                                          float* SYNX_RESTRICT cc_out, int bx, int by, int bz,
                                           unsigned char* smem_raw, double* red, double* valid_count = nullptr) {
   using S = CCShape<R, DIM, T, MASKED, NT>;
   constexpr int TX = S::TX, HX = S::HX, HY = S::HY, HC = S::HC, RZ = S::RZ, RD = S::RD, CPT = S::CPT;
@@ -136,7 +136,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
   T* ys = cs + NQ * HY * CSP;                     // [NQ][TY][CSP] y box sums of the halo columns
   T* ws = ys + NQ * TY * CSP;                     // [NQ][TY][XSP] window sums of the output voxels
   unsigned char* vring = reinterpret_cast<unsigned char*>(ws + NQ * TY * XSP);  // [RD][HC] (MASKED)
-  const unsigned char* __restrict__ valid = P.valid;
+  const unsigned char* SYNX_RESTRICT valid = P.valid;
 
   const int tid = threadIdx.x;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
@@ -176,9 +176,9 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         unsigned char vb = 0;
         if (zin && gval[c]) {
           const int o = zs * nxy + gofs[c];
-          v.x = __ldg(Ft + o);
-          v.y = __ldg(Mt + o);
-          vb = MASKED ? __ldg(valid + o) : 1;
+          v.x = SYNX_LDG(Ft + o);
+          v.y = SYNX_LDG(Mt + o);
+          vb = MASKED ? SYNX_LDG(valid + o) : 1;
           if (vb) {
             const T f = v.x, m = v.y;
             acc[c][0] += f;
@@ -212,8 +212,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
     nvb[c] = 0;
     if (z0 < z1 && z0 + RZ < nz && gval[c]) {
       const int o = (z0 + RZ) * nxy + gofs[c];
-      nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
-      if (MASKED) nvb[c] = __ldg(valid + o);
+      nv[c] = make_float2(SYNX_LDG(Ft + o), SYNX_LDG(Mt + o));
+      if (MASKED) nvb[c] = SYNX_LDG(valid + o);
     }
   }
   // ring slots of slices zc (sc), zc - 1 (sm), zc + 1 (sp) and zc + RZ (slot), advanced per slice
@@ -260,8 +260,8 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
         if (MASKED) nvb[c] = 0;
         if (znext && gval[c]) {
           const int o = (ze + 1) * nxy + gofs[c];
-          nv[c] = make_float2(__ldg(Ft + o), __ldg(Mt + o));
-          if (MASKED) nvb[c] = __ldg(valid + o);
+          nv[c] = make_float2(SYNX_LDG(Ft + o), SYNX_LDG(Mt + o));
+          if (MASKED) nvb[c] = SYNX_LDG(valid + o);
         }
       }
     }
@@ -298,7 +298,7 @@ __device__ __forceinline__ double cc_tile(const float* __restrict__ Ft, const fl
       const T n = MASKED ? Sq[NQ - 1] : cxn * cyn * czn;
       if (MASKED) n_valid += 1.0;
       // the same bits either way; the table saves the reciprocal sequence
-      const T inv_n = (sizeof(T) == 8 && P.rcp != nullptr) ? (T)__ldg(P.rcp + (int)n) : rcp_rn(n);
+      const T inv_n = (sizeof(T) == 8 && P.rcp != nullptr) ? (T)SYNX_LDG(P.rcp + (int)n) : rcp_rn(n);
       const T mF = Sq[0] * inv_n, mM = Sq[1] * inv_n;
       const T sFF = Sq[2] - mF * Sq[0] - mF * Sq[0] + n * mF * mF;
       const T sMM = Sq[3] - mM * Sq[1] - mM * Sq[1] + n * mM * mM;

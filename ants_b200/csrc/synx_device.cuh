@@ -5,6 +5,20 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Loads in the device functions that the per-kernel launches and the persistent level kernel share.
+// A per-kernel launch only reads data that earlier launches wrote, so the read-only (non-coherent)
+// path and restrict-qualified pointers apply.  The level kernel reads, after a grid barrier, data that
+// other blocks wrote earlier in the same launch, which the read-only path may serve stale: its
+// translation unit defines SYNX_COHERENT_LOADS, so these are plain (coherent) global loads there and
+// no pointer is restrict-qualified (which would let the compiler choose the read-only path itself).
+#ifdef SYNX_COHERENT_LOADS
+#define SYNX_LDG(p) (*(p))
+#define SYNX_RESTRICT
+#else
+#define SYNX_LDG(p) __ldg(p)
+#define SYNX_RESTRICT __restrict__
+#endif
+
 namespace synx {
 
 // Voxel counts of one grid.  nz = 1 for 2-D.
@@ -74,17 +88,17 @@ __device__ __forceinline__ Cell make_cell(const Dims& d, float cx, float cy, flo
 
 // Multilinear interpolation in the lerp form a + (b - a) w, x then y then z.
 template <int DIM>
-__device__ __forceinline__ float lerp_at(const float* __restrict__ a, const Cell& c) {
+__device__ __forceinline__ float lerp_at(const float* SYNX_RESTRICT a, const Cell& c) {
   const float* p = a + c.o000;
-  float v00 = __ldg(p), v10 = __ldg(p + c.dx);
-  float v01 = __ldg(p + c.dy), v11 = __ldg(p + c.dy + c.dx);
+  float v00 = SYNX_LDG(p), v10 = SYNX_LDG(p + c.dx);
+  float v01 = SYNX_LDG(p + c.dy), v11 = SYNX_LDG(p + c.dy + c.dx);
   float a0 = fmaf(v10 - v00, c.wx, v00);
   float a1 = fmaf(v11 - v01, c.wx, v01);
   float b0 = fmaf(a1 - a0, c.wy, a0);
   if (DIM == 2) return b0;
   const float* q = p + c.dz;
-  float u00 = __ldg(q), u10 = __ldg(q + c.dx);
-  float u01 = __ldg(q + c.dy), u11 = __ldg(q + c.dy + c.dx);
+  float u00 = SYNX_LDG(q), u10 = SYNX_LDG(q + c.dx);
+  float u01 = SYNX_LDG(q + c.dy), u11 = SYNX_LDG(q + c.dy + c.dx);
   float c0 = fmaf(u10 - u00, c.wx, u00);
   float c1 = fmaf(u11 - u01, c.wx, u01);
   float b1 = fmaf(c1 - c0, c.wy, c0);
@@ -112,19 +126,19 @@ __device__ __forceinline__ bool interior_cell(const Dims& d, float cx, float cy,
 
 // lerp_at for an interior cell: p = plane + offset of the lower corner; sy = nx, sz = nx * ny.
 template <int DIM>
-__device__ __forceinline__ float lerp_interior(const float* __restrict__ p, int sy, int sz, float wx, float wy,
+__device__ __forceinline__ float lerp_interior(const float* SYNX_RESTRICT p, int sy, int sz, float wx, float wy,
                                                float wz) {
   const float* py = p + sy;
-  float v00 = __ldg(p), v10 = __ldg(p + 1);
-  float v01 = __ldg(py), v11 = __ldg(py + 1);
+  float v00 = SYNX_LDG(p), v10 = SYNX_LDG(p + 1);
+  float v01 = SYNX_LDG(py), v11 = SYNX_LDG(py + 1);
   float a0 = fmaf(v10 - v00, wx, v00);
   float a1 = fmaf(v11 - v01, wx, v01);
   float b0 = fmaf(a1 - a0, wy, a0);
   if (DIM == 2) return b0;
   const float* q = p + sz;
   const float* qy = q + sy;
-  float u00 = __ldg(q), u10 = __ldg(q + 1);
-  float u01 = __ldg(qy), u11 = __ldg(qy + 1);
+  float u00 = SYNX_LDG(q), u10 = SYNX_LDG(q + 1);
+  float u01 = SYNX_LDG(qy), u11 = SYNX_LDG(qy + 1);
   float c0 = fmaf(u10 - u00, wx, u00);
   float c1 = fmaf(u11 - u01, wx, u01);
   float b1 = fmaf(c1 - c0, wy, c0);
@@ -136,7 +150,7 @@ __device__ __forceinline__ float lerp_interior(const float* __restrict__ p, int 
 // every lane takes the clamp-to-edge cell, so lanes near the edges do not split the warp into both
 // forms (on small grids most warps have such a lane).  Either form gives the same value.
 template <int DIM, int NC>
-__device__ __forceinline__ void lerp_planes(const float* __restrict__ a, int N, const Dims& d, float cx, float cy,
+__device__ __forceinline__ void lerp_planes(const float* SYNX_RESTRICT a, int N, const Dims& d, float cx, float cy,
                                             float cz, float out[NC]) {
   int o;
   float wx, wy, wz;

@@ -1,5 +1,7 @@
 // One translation unit per CC radius of the persistent level kernel (the build compiles this
 // file once per radius with -DSYNX_RCC=r, so the instantiations compile in parallel).
+// the level kernel reads data its own blocks wrote earlier in the launch: coherent loads throughout
+#define SYNX_COHERENT_LOADS 1
 #include "synx_level_body.cuh"
 
 #ifndef SYNX_RCC

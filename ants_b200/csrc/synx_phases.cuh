@@ -39,7 +39,7 @@ __device__ __forceinline__ void map_point(const Affine& m, float fx, float fy, f
 }
 
 template <int DIM, bool DIAG>
-__device__ __forceinline__ float sample(const float* __restrict__ img, const Dims& di, const Affine& m, float fx,
+__device__ __forceinline__ float sample(const float* SYNX_RESTRICT img, const Dims& di, const Affine& m, float fx,
                                         float fy, float fz, float ux, float uy, float uz) {
   float cx, cy, cz;
   map_point<DIM, DIAG>(m, fx, fy, fz, ux, uy, uz, cx, cy, cz);
@@ -69,8 +69,8 @@ __device__ __forceinline__ void warp_pair_tile(const WarpArgs& a, int bx, int by
   if (x >= dv.nx || y >= dv.ny) return;
   const int z0 = bz * a.zb, z1 = min(z0 + a.zb, dv.nz);
   const int N = (int)dv.N, nxy = dv.nx * dv.ny;
-  const float* __restrict__ psiF = a.psiF;
-  const float* __restrict__ psiM = a.psiM;
+  const float* SYNX_RESTRICT psiF = a.psiF;
+  const float* SYNX_RESTRICT psiM = a.psiM;
   const float fx = (float)x, fy = (float)y;
   const int i0 = z0 * nxy + y * dv.nx + x;
   float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
@@ -116,7 +116,7 @@ __device__ __forceinline__ void compose_tile(const ComposeArgs& a, const IterCtl
   const Dims& d = a.g;
   const int x = bx * 32 + (threadIdx.x & 31), y = by * 8 + (threadIdx.x >> 5);
   if (x >= d.nx || y >= d.ny) return;
-  const float* __restrict__ D = h ? a.d.p[1] : a.d.p[0];
+  const float* SYNX_RESTRICT D = h ? a.d.p[1] : a.d.p[0];
   const float* W = h ? a.w.p[1] : a.w.p[0];
   float* O = h ? a.o.p[1] : a.o.p[0];
   float scale = 1.0f;
@@ -191,7 +191,7 @@ __device__ __forceinline__ void inv_map(const float* A, float fx, float fy, floa
 }
 
 template <int DIM, bool DIAG>
-__device__ __forceinline__ void inv_residual(const float* __restrict__ phi, const Dims& d, const float* A, float fx,
+__device__ __forceinline__ void inv_residual(const float* SYNX_RESTRICT phi, const Dims& d, const float* A, float fx,
                                              float fy, float fz, const float p[3], float e[3]) {
   float cx, cy, cz;
   inv_map<DIM, DIAG>(A, fx, fy, fz, p, cx, cy, cz);
@@ -217,9 +217,9 @@ __device__ __forceinline__ void invert_tile(const InvArgs& a, int h, int bx, int
   const Dims& d = a.g;
   const int x = bx * 32 + (threadIdx.x & 31), y = by * 8 + (threadIdx.x >> 5);
   if (x >= d.nx || y >= d.ny) return;
-  const float* __restrict__ phi = h ? a.phi.p[1] : a.phi.p[0];
-  float* __restrict__ psi = h ? a.psi.p[1] : a.psi.p[0];
-  float* __restrict__ ec = h ? a.ecache.p[1] : a.ecache.p[0];
+  const float* SYNX_RESTRICT phi = h ? a.phi.p[1] : a.phi.p[0];
+  float* SYNX_RESTRICT psi = h ? a.psi.p[1] : a.psi.p[0];
+  float* SYNX_RESTRICT ec = h ? a.ecache.p[1] : a.ecache.p[0];
   const int z0 = bz * a.zb, z1 = min(z0 + a.zb, d.nz);
   const int N = (int)d.N, nxy = d.nx * d.ny;
   const float fx = (float)x, fy = (float)y;
@@ -331,7 +331,7 @@ __device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const 
   constexpr int HX = 32 + 2 * R, HXP = (HX + 3) & ~3, HY = TY + 2 * R;
   static_assert(HX <= 64, "two columns per lane cover a halo row");
   const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
-  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
+  const float* SYNX_RESTRICT src = h ? a.in.p[1] : a.in.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const int x0 = bx * 32, y0 = by * TY;
   // the halo columns this lane copies (replicate-edge indices) are the same in every row
@@ -351,8 +351,8 @@ __device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const 
           cp_async4(trow + tx, line + gx0);
           if (second) cp_async4(trow + 32 + tx, line + gx1);
         } else {
-          trow[tx] = __ldg(line + gx0);
-          if (second) trow[32 + tx] = __ldg(line + gx1);
+          trow[tx] = SYNX_LDG(line + gx0);
+          if (second) trow[32 + tx] = SYNX_LDG(line + gx1);
         }
       }
     } else {
@@ -362,8 +362,8 @@ __device__ __forceinline__ void smooth_xy_load_tile(const Smooth3Args& a, const 
         const int hy = ty + 8 * k;
         if (hy < HY) {
           const float* line = cplane + min(max(y0 - R + hy, 0), ny - 1) * nx;
-          v0[k] = __ldg(line + gx0);
-          v1[k] = second ? __ldg(line + gx1) : 0.0f;
+          v0[k] = SYNX_LDG(line + gx0);
+          v1[k] = second ? SYNX_LDG(line + gx1) : 0.0f;
         }
       }
 #pragma unroll
@@ -454,13 +454,13 @@ __device__ __forceinline__ float smooth_xy_tile(const Smooth3Args& a, const Dims
   float y[DIM][RPT];
   smooth_xy_compute<DIM, R, TY, LOAD>(a, d, bx, by, z, h, sm, y);
   const int nx = d.nx, ny = d.ny, nxy = nx * ny, N = (int)d.N;
-  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
+  float* SYNX_RESTRICT dst = h ? a.out.p[1] : a.out.p[0];
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const int x0 = bx * 32, y0 = by * TY;
   const int ox = x0 + tx, ty0 = ty * RPT;
   float mx = 0.0f;
   if (ox >= nx) return mx;
-  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+  const float* SYNX_RESTRICT org = h ? a.orig.p[1] : a.orig.p[0];
 #pragma unroll
   for (int r = 0; r < RPT; ++r) {
     const int oy = y0 + ty0 + r;
@@ -496,9 +496,9 @@ template <int R>
 __device__ __forceinline__ float smooth_z_column(const Smooth3Args& a, const Dims& d, int bx, int by, int zc, int h) {
   constexpr int K = 2 * R + 1, RD = K;
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
-  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
-  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
-  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+  const float* SYNX_RESTRICT src = h ? a.in.p[1] : a.in.p[0];
+  float* SYNX_RESTRICT dst = h ? a.out.p[1] : a.out.p[0];
+  const float* SYNX_RESTRICT org = h ? a.orig.p[1] : a.orig.p[0];
   const int ox = bx * 32 + (threadIdx.x & 31), oy = by * 8 + (threadIdx.x >> 5);
   const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
   float mx = 0.0f;
@@ -509,7 +509,7 @@ __device__ __forceinline__ float smooth_z_column(const Smooth3Args& a, const Dim
   for (int u = 0; u < 2 * R; ++u) {
     const int zs = min(max(z0 - R + u, 0), nz - 1);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) ring[c][u] = __ldg(col + c * N + zs * nxy);
+    for (int c = 0; c < 3; ++c) ring[c][u] = SYNX_LDG(col + c * N + zs * nxy);
   }
   const bool xyedge = ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1;
   for (int zb = z0; zb < z1; zb += RD) {
@@ -519,7 +519,7 @@ __device__ __forceinline__ float smooth_z_column(const Smooth3Args& a, const Dim
       if (z < z1) {
         const int zs = min(z + R, nz - 1);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) ring[c][(u + 2 * R) % RD] = __ldg(col + c * N + zs * nxy);
+        for (int c = 0; c < 3; ++c) ring[c][(u + 2 * R) % RD] = SYNX_LDG(col + c * N + zs * nxy);
         const int i = z * nxy + oy * nx + ox;
         const bool edge = a.epilogue && (xyedge || z == 0 || z == nz - 1);
         float nrm2 = 0.0f;
@@ -555,9 +555,9 @@ __device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, cons
                                                       int h, float* ring) {
   constexpr int K = 2 * R + 1, RD = K;
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxy = nx * ny, N = (int)d.N;
-  const float* __restrict__ src = h ? a.in.p[1] : a.in.p[0];
-  float* __restrict__ dst = h ? a.out.p[1] : a.out.p[0];
-  const float* __restrict__ org = h ? a.orig.p[1] : a.orig.p[0];
+  const float* SYNX_RESTRICT src = h ? a.in.p[1] : a.in.p[0];
+  float* SYNX_RESTRICT dst = h ? a.out.p[1] : a.out.p[0];
+  const float* SYNX_RESTRICT org = h ? a.orig.p[1] : a.orig.p[0];
   const int ox = bx * 32 + (threadIdx.x & 31), oy = by * 8 + (threadIdx.x >> 5);
   const int z0 = zc * a.ZC, z1 = min(z0 + a.ZC, nz);
   float mx = 0.0f;
@@ -571,7 +571,7 @@ __device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, cons
   for (int u = 0; u < 2 * R; ++u) {
     const int zs = min(max(z0 - R + u, 0), nz - 1);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) slot(u, c) = __ldg(col + c * N + zs * nxy);
+    for (int c = 0; c < 3; ++c) slot(u, c) = SYNX_LDG(col + c * N + zs * nxy);
   }
   const bool xyedge = ox == 0 || ox == nx - 1 || oy == 0 || oy == ny - 1;
   // the slices entering the window are loaded two outputs ahead (q0: slice z + R, q1: z + R + 1),
@@ -579,8 +579,8 @@ __device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, cons
   float q0[3], q1[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    q0[c] = z0 < z1 ? __ldg(col + c * N + min(z0 + R, nz - 1) * nxy) : 0.0f;
-    q1[c] = z0 + 1 < z1 ? __ldg(col + c * N + min(z0 + 1 + R, nz - 1) * nxy) : 0.0f;
+    q0[c] = z0 < z1 ? SYNX_LDG(col + c * N + min(z0 + R, nz - 1) * nxy) : 0.0f;
+    q1[c] = z0 + 1 < z1 ? SYNX_LDG(col + c * N + min(z0 + 1 + R, nz - 1) * nxy) : 0.0f;
   }
   for (int zb = z0; zb < z1; zb += RD) {
 #pragma unroll
@@ -591,7 +591,7 @@ __device__ __forceinline__ float smooth_z_column_smem(const Smooth3Args& a, cons
         for (int c = 0; c < 3; ++c) {
           slot((u + 2 * R) % RD, c) = q0[c];
           q0[c] = q1[c];
-          if (z + 2 < z1) q1[c] = __ldg(col + c * N + min(z + 2 + R, nz - 1) * nxy);
+          if (z + 2 < z1) q1[c] = SYNX_LDG(col + c * N + min(z + 2 + R, nz - 1) * nxy);
         }
         const int i = z * nxy + oy * nx + ox;
         const bool edge = a.epilogue && (xyedge || z == 0 || z == nz - 1);
