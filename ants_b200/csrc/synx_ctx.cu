@@ -1546,7 +1546,10 @@ int synx_set_masks(synx_ctx* c, const float* fixed_mask, const synx_geom* gfm, c
       cudaGetLastError();
       return set_err(c, SYNX_E_NOMEM, std::string("synx_set_masks: ") + cudaGetErrorString(e));
     }
-    CUDA_TRY(c, cudaMemcpy(*dst, b.data(), n, cudaMemcpyHostToDevice));
+    // on the context's stream, which does not synchronise with the legacy default stream: a plain
+    // cudaMemcpy from pageable memory may return before its data reach the device
+    CUDA_TRY(c, cudaMemcpyAsync(*dst, b.data(), n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));  // b is released on return
     return SYNX_OK;
   };
   int rc = upload(fixed_mask, gfm, &c->maskF, &c->gmF);
@@ -1585,7 +1588,10 @@ int synx_set_initial_half_fields(synx_ctx* c, const float* phi_f, const float* p
   }
   const float* src[4] = {phi_f, psi_f, phi_m, psi_m};
   for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
-    e = cudaMemcpy(inter, src[k], 4 * n, cudaMemcpyHostToDevice);
+    // the copy on the context's stream, ordered before the kernel that reads it (a plain cudaMemcpy from
+    // pageable memory may return before its data reach the device, and this stream does not
+    // synchronise with the legacy default stream)
+    e = cudaMemcpyAsync(inter, src[k], 4 * n, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
       launch_deinterleave(inter, c->init_half + k * n, c->init_grid.d.N, c->D, c->stream);
       e = cudaStreamSynchronize(c->stream);
