@@ -96,6 +96,30 @@ def test_stage_from_initial_half_fields_matches_oracle(cuda, dim):
     assert rms_vox(fwd, rf, go.spacing) < 0.5 * rms_vox(fwd, zf, go.spacing)
 
 
+@pytest.mark.gpu
+def test_seeded_stage_repeats_bit_for_bit(cuda):
+    # four unrelated smooth fields make every inversion run its full 20 sub-iterations; the uploaded
+    # fields (about 760 KB each) must reach the device before the first level resamples them
+    size = (40, 44, 36)
+    f, m = phantoms.pair_3d(size, seed=61)
+    g = Geom(size, (1.0, 1.125, 0.875))
+    rng = np.random.default_rng(66)
+    sp = np.asarray(g.spacing).reshape((-1, 1, 1, 1))
+    init = [np.ascontiguousarray(np.moveaxis((np.moveaxis(phantoms.smooth_field(f.shape, 6.0, 1.5, rng), -1, 0) * sp)
+                                             .astype(np.float32), 0, -1)) for _ in range(4)]
+    P = SyNParams(dim=3, cc_radius=3, iterations=(8, 5), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0),
+                  convergence_threshold=1e-12, flags=SYNX_F_USE_GRAPHS)
+    runs = []
+    for _ in range(2):
+        with SyNStage(P) as st:
+            st.set_images(f, g, m, g)
+            st.set_initial_half_fields(*init, grid=g)
+            st.run()
+            runs.append(st.fields())
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+
+
 def check_cli_state(reg, tmp_path, stage):
     """--save-state, --restore-state, -a 1 and their option rules on a 2-D pair.
     stage(f, g, m, g, P, init) -> (forward, inverse, (phiF, psiF, phiM, psiM)), interleaved, where
