@@ -125,3 +125,53 @@ def test_state_and_composite(host_cli, tmp_path):
         return U.interleaved(fwd), U.interleaved(inv), [U.interleaved(h) for h in half]
 
     U.check_cli_state(host_cli["reg"], tmp_path, stage)
+
+
+def test_state_with_initial_transform(host_cli, tmp_path):
+    # -r init.mat with --save-state: the state and the composite list the initial transform first
+    # (ITK's composite order: it acts last); --restore-state makes it the initial moving transform again
+    # and starts the stage from the saved fields
+    import numpy as np
+
+    import oracle as O
+    import test_zz_stack_apply as S
+    import test_zz_u_state as U
+    from ants_b200 import nifti, phantoms
+    from ants_b200.synx import Geom, SyNParams
+    size = (64, 60)
+    f, m = phantoms.pair_2d(size, seed=33)
+    g = Geom(size)
+    A = S.Affine([[1.02, 0.03], [-0.02, 0.99]], [0.8, -0.6], [32.0, 30.0])
+    A.write_mat(tmp_path / "init.mat")
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    base = [host_cli["reg"], "-d", "2", "--float", "1", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]",
+            "-t", "SyN[0.2,3,0]", "-c", "[8x4,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-a", "1", "-z", "0", "-i", "1"]
+    state = str(tmp_path / "state.txt")
+    r = subprocess.run(base + ["-r", f"{tmp_path}/init.mat", "-j", state, "-o", str(tmp_path / "A_")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    items = U.read_composite(state)
+    assert [t for t, _, _ in items] == ["AffineTransform_double_2_2"] + ["DisplacementFieldTransform_float_2_2"] * 4
+    np.testing.assert_allclose(items[0][1], np.r_[A.A.ravel(), A.t], atol=1e-12)
+    np.testing.assert_allclose(items[0][2], A.c, atol=1e-12)
+    comp = U.read_composite(tmp_path / "A_Composite.txt")
+    icomp = U.read_composite(tmp_path / "A_InverseComposite.txt")
+    assert [t for t, _, _ in comp] == ["AffineTransform_double_2_2", "DisplacementFieldTransform_float_2_2"]
+    assert [t for t, _, _ in icomp] == ["DisplacementFieldTransform_float_2_2", "AffineTransform_double_2_2"]
+    Ai = np.linalg.inv(A.A)
+    np.testing.assert_allclose(icomp[1][1][:4].reshape(2, 2), Ai, atol=1e-12)
+    np.testing.assert_allclose(icomp[1][1][4:], -Ai @ A.t, atol=1e-9)  # same center, inverted map
+    # restore: the initial transform comes back from the state, the stage starts from its fields
+    r = subprocess.run(base + ["-k", state, "-o", str(tmp_path / "B_")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    comp_b = U.read_composite(tmp_path / "B_Composite.txt")
+    np.testing.assert_allclose(comp_b[0][1], items[0][1], atol=1e-12)
+    half = [np.ascontiguousarray(it[1].astype(np.float32).reshape(size[1], size[0], 2).transpose(2, 0, 1))
+            for it in items[1:]]
+    P = SyNParams(dim=2, learning_rate=0.2, cc_radius=2, iterations=(8, 4), shrink_factors=(2, 1),
+                  smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12)
+    rf, _, go, _ = O.syn_register(f, g, m, S.push_forward(g, A.inverse()), P, initial_half_fields=half,
+                                  initial_geom=g)
+    got = comp_b[1][1].astype(np.float32).reshape(size[1], size[0], 2).transpose(2, 0, 1)
+    assert float(np.sqrt(((got - rf) ** 2).sum(0).mean())) <= 1e-3
