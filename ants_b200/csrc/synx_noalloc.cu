@@ -85,12 +85,19 @@ int synx_cc_metric_noalloc(const float* fixed_dev, const float* moving_dev, cons
     return fail(SYNX_E_ARG, "synx_cc_metric_noalloc: this grid needs " + std::to_string(blocks) +
                                 " CC blocks; the fixed scratch holds at most " + std::to_string(kMaxCCBlocks) +
                                 " (for example 8192 x 1024 voxels per slice); use synx_cc_metric");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (value_host) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+    if (ce != cudaSuccess) return fail(SYNX_E_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(SYNX_E_ARG, "synx_cc_metric_noalloc: value_host must be NULL while the stream is being captured");
+  }
   void* base = nullptr;
   int rc = scratch_on_current_device(&base);
   if (rc) return rc;
   cudaError_t e = synx::cc_prepare(g->dim, radius);
   if (e != cudaSuccess) return fail(SYNX_E_CUDA, std::string("CC kernel setup: ") + cudaGetErrorString(e));
-  cudaStream_t s = (cudaStream_t)stream;
   synx::IterCtl* ctl = reinterpret_cast<synx::IterCtl*>(base);
   double* partials = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + kCtlBytes);
   // the previous call's control block is still there: the arrival counter must start at zero

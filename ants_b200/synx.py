@@ -764,20 +764,21 @@ def cc_metric_masked(F, M, valid, g: Geom, radius: int, gF, gM, stream=None) -> 
     return v.value
 
 
-def cc_metric_noalloc(F, M, g: Geom, radius: int, gF, gM, stream=None) -> float:
+def cc_metric_noalloc(F, M, g: Geom, radius: int, gF, gM, stream=None, read_value: bool = True):
     """cc_metric without any device allocation: the kernel's scratch is a fixed device array
     inside libsynx (for callers that cannot allocate, e.g. inside graph capture).  Calls on one
-    device share that array, so calls that overlap on the GPU race."""
+    device share that array, so calls that overlap on the GPU race.  With read_value=False the call
+    does not wait for its stream and returns None (the form a stream capture takes)."""
     lib = load_library()
     gc = g.to_c()
     v = C.c_double()
     n = g.count
     rc = lib.synx_cc_metric_noalloc(_dev(F, n, "F"), _dev(M, n, "M"), C.byref(gc), radius, _dev(gF, g.dim * n, "gF"),
-                                    _dev(gM, g.dim * n, "gM"), C.byref(v),
+                                    _dev(gM, g.dim * n, "gM"), C.byref(v) if read_value else None,
                                     _stream(stream))
     if rc != 0:
         raise SynxError(f"synx error {rc} ({ERRORS.get(rc, '?')}): {lib.synx_noalloc_last_error().decode()}")
-    return v.value
+    return v.value if read_value else None
 
 
 def smooth_field(u, out, g: Geom, variance: float, stream=None) -> float:

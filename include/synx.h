@@ -362,7 +362,10 @@ int synx_cc_metric_ex(const float* fixed_dev, const float* moving_dev, const syn
  * calls on a device share the array and find the previous call's contents in it (the control
  * block is cleared before each launch): calls that overlap on the GPU (other streams, other
  * host threads) race.  value_host may be NULL; otherwise the call waits for its stream to read
- * the value.  Errors are reported by synx_noalloc_last_error(). */
+ * the value.  While the stream is being captured into a CUDA graph value_host must be NULL (a
+ * capture cannot wait for its stream; the call returns SYNX_E_ARG otherwise): the gradients are
+ * written on each replay, and the value stays in the shared array until the next call.  Errors are
+ * reported by synx_noalloc_last_error(). */
 int synx_cc_metric_noalloc(const float* fixed_dev, const float* moving_dev, const synx_geom* g, int radius,
                            float* grad_fixed_dev, float* grad_moving_dev, double* value_host, void* stream);
 const char* synx_noalloc_last_error(void);

@@ -4,8 +4,9 @@ It serves callers that must not allocate device memory themselves: a plug-in who
 application (a viewer, a deep-learning framework with its own caching allocator, a serving process)
 owns the GPU's memory and its budget, or a latency-bound loop that cannot afford the device-wide
 synchronisation a cudaMalloc/cudaFree pair can cause.  It keeps the CC kernel's scratch in a fixed
-array inside libsynx instead.  The GPU test calls it twice in a row through the C ABI and checks each
-result against synx_cc_metric on the same inputs, with the tolerances of the CC parity tests.  The
+array inside libsynx instead.  The GPU tests call it twice in a row through the C ABI, and inside a
+CUDA graph capture replayed on new inputs, and check each result against synx_cc_metric on the same
+inputs, with the tolerances of the CC parity tests.  The
 file name sorts after every other test file, so pytest collects it last and a run which stops at the
 first failure has already run every other test.
 """
@@ -59,3 +60,49 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda):
                 a, b = a.cpu().numpy(), b.cpu().numpy()
                 scale = max(np.abs(b).max(), 1e-20)
                 np.testing.assert_allclose(a, b, atol=1e-6 * scale, rtol=1e-5)
+
+
+@pytest.mark.gpu
+def test_noalloc_inside_graph_capture(cuda):
+    # captured into a CUDA graph (value not read), each replay recomputes both gradients from the
+    # inputs' current contents; a call that asks for the value while the stream captures is refused
+    # before it touches the stream, and the capture goes on
+    import torch
+
+    g = Geom((37, 29, 23), (1.0, 1.2, 0.9))
+    radius = 3
+    rng = np.random.default_rng(13)
+
+    def pair():
+        F = rng.uniform(0, 1, g.shape).astype(np.float32)
+        M = (0.6 * np.roll(F, 1, axis=-1) + 0.1 * rng.standard_normal(g.shape)).astype(np.float32)
+        return torch.from_numpy(F).to(cuda), torch.from_numpy(M).to(cuda)
+
+    Fd, Md = pair()
+    shape = (g.dim,) + g.shape
+    out_f = torch.empty(shape, device=cuda)
+    out_m = torch.empty(shape, device=cuda)
+    synx.cc_metric_noalloc(Fd, Md, g, radius, out_f, out_m)  # first call on the device: before any capture
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        s = torch.cuda.current_stream().cuda_stream
+        with pytest.raises(synx.SynxError, match="must be NULL while the stream is being captured"):
+            synx.cc_metric_noalloc(Fd, Md, g, radius, out_f, out_m, stream=s)
+        assert synx.cc_metric_noalloc(Fd, Md, g, radius, out_f, out_m, stream=s, read_value=False) is None
+    ref_f = torch.empty(shape, device=cuda)
+    ref_m = torch.empty(shape, device=cuda)
+    for _ in range(2):
+        F2, M2 = pair()
+        Fd.copy_(F2)
+        Md.copy_(M2)
+        out_f.fill_(float("nan"))
+        out_m.fill_(float("nan"))
+        graph.replay()
+        synx.cc_metric(Fd, Md, g, radius, ref_f, ref_m)
+        torch.cuda.synchronize()
+        for a, b in ((out_f, ref_f), (out_m, ref_m)):
+            a, b = a.cpu().numpy(), b.cpu().numpy()
+            scale = max(np.abs(b).max(), 1e-20)
+            np.testing.assert_allclose(a, b, atol=1e-6 * scale, rtol=1e-5)
+    del graph
