@@ -343,8 +343,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     // (itkantsRegistrationHelper.hxx:2093-2125)
     const synx_geom gs = composite::field_geom(state_fields[0], dim);
     for (int k = 1; k < 4; ++k) {
-      const synx_geom gk = composite::field_geom(state_fields[k], dim);
-      if (std::memcmp(gk.size, gs.size, sizeof(gs.size)) != 0)
+      composite::field_geom(state_fields[k], dim);
+      if (state_fields[k].fixed != state_fields[0].fixed)
         throw std::runtime_error("--restore-state: the four SyN fields do not share one grid");
     }
     if (synx_set_initial_half_fields(ctx, state_fields[0].field.data(), state_fields[1].field.data(),

@@ -98,7 +98,10 @@ inline synx_geom field_geom(const Item& it, int dim) {
   g.spacing[0] = g.spacing[1] = g.spacing[2] = 1.0;
   g.direction[0] = g.direction[4] = g.direction[8] = 1.0;
   for (int k = 0; k < dim; ++k) {
-    g.size[k] = (int64_t)it.fixed[k];
+    const double sz = it.fixed[k];
+    if (!(sz >= 1.0 && sz <= 1e9 && sz == (double)(int64_t)sz) || !(it.fixed[2 * dim + k] > 0.0))
+      throw std::runtime_error("composite transform: field sizes must be positive integers and spacings positive");
+    g.size[k] = (int64_t)sz;
     g.origin[k] = it.fixed[dim + k];
     g.spacing[k] = it.fixed[2 * dim + k];
   }

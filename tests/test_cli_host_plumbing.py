@@ -175,3 +175,58 @@ def test_state_with_initial_transform(host_cli, tmp_path):
                                   initial_geom=g)
     got = comp_b[1][1].astype(np.float32).reshape(size[1], size[0], 2).transpose(2, 0, 1)
     assert float(np.sqrt(((got - rf) ** 2).sum(0).mean())) <= 1e-3
+
+
+def test_restore_rejects_malformed_state(host_cli, tmp_path):
+    # a saved state edited by hand: each defect is refused with its own message before the stage runs
+    from ants_b200 import nifti, phantoms
+    from ants_b200.synx import Geom
+    size = (40, 36)
+    f, m = phantoms.pair_2d(size, seed=34)
+    g = Geom(size)
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    base = [host_cli["reg"], "-d", "2", "--float", "1", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]",
+            "-t", "SyN[0.2,3,0]", "-c", "[2x1,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-a", "1", "-z", "0", "-i", "1"]
+    state = tmp_path / "state.txt"
+    r = subprocess.run(base + ["-j", str(state), "-o", str(tmp_path / "A_")], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = state.read_text().splitlines()
+    par = [i for i, s in enumerate(lines) if s.startswith("Parameters:")]
+    fix = [i for i, s in enumerate(lines) if s.startswith("FixedParameters:")]
+    assert len(par) == len(fix) == 4
+
+    def edited(line, fn):
+        out = list(lines)
+        out[line] = fn(out[line])
+        return out
+
+    def replace_token(k, value):
+        def fn(s):
+            key, vals = s.split(":", 1)
+            t = vals.split()
+            t[k] = value
+            return key + ": " + " ".join(t)
+        return fn
+
+    cases = {
+        "not an ITK text transform file": lines[1:],
+        "bad number": edited(par[3], replace_token(0, "x1")),
+        "positive integers": edited(fix[0], replace_token(0, "0")),
+        "do not match its size": edited(par[0], lambda s: s.rsplit(" ", 1)[0]),
+        "do not share one grid": edited(fix[3], replace_token(2, "1.5")),
+        "other than a SyN state": lines[:par[3] - 2],
+        "unexpected key": lines + ["Offset: 1 2"],
+    }
+    for k, (msg, text) in enumerate(cases.items()):
+        bad = tmp_path / f"bad{k}.txt"
+        bad.write_text("\n".join(text) + "\n")
+        r = subprocess.run(base + ["-k", str(bad), "-o", str(tmp_path / f"B{k}_")], capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode != 0 and msg in r.stderr, (msg, r.stderr)
+        assert not (tmp_path / f"B{k}_Composite.txt").exists()
+    # the unedited state restores
+    r = subprocess.run(base + ["-k", str(state), "-o", str(tmp_path / "C_")], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
