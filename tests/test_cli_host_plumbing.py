@@ -230,3 +230,54 @@ def test_restore_rejects_malformed_state(host_cli, tmp_path):
     r = subprocess.run(base + ["-k", str(state), "-o", str(tmp_path / "C_")], capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stderr
+
+
+def test_collapsed_composite(host_cli, tmp_path):
+    # -a 1 with collapsing (the default -z 1) and two -r transforms: the composite holds one affine
+    # transform, the same one prefix0GenericAffine.mat holds without -a, then the SyN field (the same
+    # values as prefix1Warp); the inverse composite lists the field's inverse, then the affine's inverse
+    import numpy as np
+
+    import test_zz_stack_apply as S
+    import test_zz_u_state as U
+    from ants_b200 import nifti, phantoms, synx
+    from ants_b200.synx import Geom
+    size = (48, 44)
+    f, m = phantoms.pair_2d(size, seed=35)
+    g = Geom(size)
+    A = S.Affine([[1.01, 0.02], [-0.01, 0.98]], [0.5, -0.4], [24.0, 22.0])
+    B = S.Affine([[0.99, -0.015], [0.01, 1.02]], [-0.3, 0.2], [20.0, 21.0])
+    A.write_mat(tmp_path / "a.mat")
+    B.write_mat(tmp_path / "b.mat")
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    base = [host_cli["reg"], "-d", "2", "--float", "1", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]",
+            "-t", "SyN[0.2,3,0]", "-c", "[4x2,1e-12,10]", "-f", "2x1", "-s", "1x0vox",
+            "-r", f"{tmp_path}/a.mat", "-r", f"{tmp_path}/b.mat"]
+    for extra in (["-o", str(tmp_path / "A_")], ["-a", "1", "-o", str(tmp_path / "B_")]):
+        r = subprocess.run(base + extra, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+    assert not (tmp_path / "B_0GenericAffine.mat").exists() and not (tmp_path / "B_1Warp.nii.gz").exists()
+    comp = U.read_composite(tmp_path / "B_Composite.txt")
+    icomp = U.read_composite(tmp_path / "B_InverseComposite.txt")
+    assert [t for t, _, _ in comp] == ["AffineTransform_double_2_2", "DisplacementFieldTransform_float_2_2"]
+    assert [t for t, _, _ in icomp] == ["DisplacementFieldTransform_float_2_2", "AffineTransform_double_2_2"]
+    mat = synx.read_linear_transform(str(tmp_path / "A_0GenericAffine.mat"), 2)
+    np.testing.assert_allclose(comp[0][1][:4].reshape(2, 2), mat.matrix, atol=1e-12)
+    np.testing.assert_allclose(comp[0][1][4:], mat.translation, atol=1e-9)
+    np.testing.assert_allclose(comp[0][2], mat.center, atol=1e-12)
+    fwd, _ = nifti.read(tmp_path / "A_1Warp.nii.gz", 2)
+    inv, _ = nifti.read(tmp_path / "A_1InverseWarp.nii.gz", 2)
+    np.testing.assert_array_equal(comp[1][1].astype(np.float32), fwd.astype(np.float32).reshape(-1))
+    np.testing.assert_array_equal(icomp[0][1].astype(np.float32), inv.astype(np.float32).reshape(-1))
+    # the inverse composite's affine undoes the collapsed one
+    Cf = S.Affine(comp[0][1][:4].reshape(2, 2), comp[0][1][4:], comp[0][2])
+    Ci = S.Affine(icomp[1][1][:4].reshape(2, 2), icomp[1][1][4:], icomp[1][2])
+    np.testing.assert_allclose(Ci.M @ Cf.M, np.eye(2), atol=1e-12)
+    np.testing.assert_allclose(Ci.M @ Cf.b + Ci.b, 0.0, atol=1e-9)
+    # and the collapsed affine is the two -r transforms composed: the reference stores repeated options
+    # newest first and adds them to the composite in that order, which applies the last one added (the
+    # first given) first to a point; the center is that of the transform acting first
+    np.testing.assert_allclose(Cf.M, B.M @ A.M, atol=1e-12)
+    np.testing.assert_allclose(Cf.b, B.M @ A.b + B.b, atol=1e-9)
+    np.testing.assert_allclose(comp[0][2], A.c, atol=1e-12)
