@@ -71,21 +71,13 @@ inline Item field_item(const synx_geom& g, const std::vector<float>& v, bool dou
   return it;
 }
 
+// A linear entry (any type synx_read_linear_transform reads: affine, translation, identity, the
+// rigid and similarity families) in matrix-offset form.
 inline synx_linear to_linear(const Item& it, int dim) {
-  const bool known = it.type.rfind("AffineTransform_", 0) == 0 || it.type.rfind("MatrixOffsetTransformBase_", 0) == 0;
-  if (!known || (int)it.params.size() != dim * dim + dim || (int)it.fixed.size() != dim)
-    throw std::runtime_error("composite transform: unsupported linear entry '" + it.type + "'");
   synx_linear t;
-  std::memset(&t, 0, sizeof(t));
-  t.dim = dim;
-  t.has_center = 1;
-  t.matrix[8] = 1.0;
-  for (int r = 0; r < dim; ++r)
-    for (int c = 0; c < dim; ++c) t.matrix[r * 3 + c] = it.params[r * dim + c];
-  for (int r = 0; r < dim; ++r) {
-    t.translation[r] = it.params[dim * dim + r];
-    t.center[r] = it.fixed[r];
-  }
+  if (synx_linear_from_parameters(it.type.c_str(), it.params.data(), (int)it.params.size(), it.fixed.data(),
+                                  (int)it.fixed.size(), dim, &t) != SYNX_OK)
+    throw std::runtime_error(std::string("composite transform: ") + synx_last_error(nullptr));
   return t;
 }
 

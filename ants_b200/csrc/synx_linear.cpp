@@ -351,6 +351,25 @@ int synx_read_linear_transform(const char* path, int dim, int index, synx_linear
   }
 }
 
+int synx_linear_from_parameters(const char* type, const double* params, int n_params, const double* fixed,
+                                int n_fixed, int dim, synx_linear* out) {
+  const char* fn = "synx_linear_from_parameters: ";
+  if (!type || !out || n_params < 0 || n_fixed < 0 || (n_params > 0 && !params) || (n_fixed > 0 && !fixed))
+    return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "null pointer or negative count");
+  if (dim != 2 && dim != 3) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "dim must be 2 or 3");
+  try {
+    RawTransform r{type, std::vector<double>(params, params + n_params), std::vector<double>(fixed, fixed + n_fixed)};
+    synx_linear L;
+    if (!to_linear(r, dim, L, r.type)) fail(SYNX_E_ARG, "'" + r.type + "': a composite is not a linear transform");
+    *out = L;
+    return SYNX_OK;
+  } catch (const ReadError& e) {
+    return synx::set_global_error(e.code, fn + e.msg);
+  } catch (const std::exception& e) {
+    return synx::set_global_error(SYNX_E_ARG, fn + std::string(e.what()));
+  }
+}
+
 int synx_linear_field(const synx_linear* t, int invert, const synx_geom* g, float* field) {
   const char* fn = "synx_linear_field: ";
   if (!t || !g || !field) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "null argument");

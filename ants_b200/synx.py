@@ -223,6 +223,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "synx_server_wait": (I, [V, C.c_int64, D, P(SynxRequestInfo)]),
         "synx_server_get_stats": (I, [V, P(SynxServerStats)]),
         "synx_read_linear_transform": (I, [C.c_char_p, I, I, P(SynxLinear)]),
+        "synx_linear_from_parameters": (I, [C.c_char_p, P(D), I, P(D), I, I, P(SynxLinear)]),
         "synx_linear_field": (I, [P(SynxLinear), I, P(SynxGeom), V]),
         "synx_write_linear_transform": (I, [C.c_char_p, P(SynxLinear)]),
         "synx_initial_translation": (I, [V, P(SynxGeom), V, P(SynxGeom), I, P(SynxLinear)]),
@@ -871,6 +872,19 @@ def read_linear_transform(path, dim: int, index: int = 0) -> LinearTransform:
     rc = load_library().synx_read_linear_transform(os.fsencode(str(path)), dim, index, C.byref(t))
     if rc < 0:
         _check(rc)
+    m = np.array(list(t.matrix), dtype=np.float64).reshape(3, 3)[:dim, :dim]
+    return LinearTransform(m, np.array(list(t.translation)[:dim]), np.array(list(t.center)[:dim]))
+
+
+def linear_from_parameters(type_name: str, params, fixed, dim: int) -> LinearTransform:
+    """A linear transform from its ITK type name, parameters and fixed parameters (the entries of
+    a transform file), in matrix-offset form."""
+    p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+    f = np.ascontiguousarray(fixed, dtype=np.float64).reshape(-1)
+    t = SynxLinear()
+    dp = C.POINTER(C.c_double)
+    _check(load_library().synx_linear_from_parameters(type_name.encode(), p.ctypes.data_as(dp), p.size,
+                                                      f.ctypes.data_as(dp), f.size, dim, C.byref(t)))
     m = np.array(list(t.matrix), dtype=np.float64).reshape(3, 3)[:dim, :dim]
     return LinearTransform(m, np.array(list(t.translation)[:dim]), np.array(list(t.center)[:dim]))
 

@@ -429,6 +429,15 @@ typedef struct synx_linear {
  * type); synx_last_error(NULL) names the reason. */
 int synx_read_linear_transform(const char* path, int dim, int index, synx_linear* out);
 
+/* The same conversion for one transform given by its type name ("<Base>_<double|float>_<D>_<D>",
+ * a type listed above) and its parameters and fixed parameters as an ITK transform file holds them
+ * (the entries of a composite transform read elsewhere, e.g. a saved registration state).  The
+ * counterpart of ITK's transform factory for these types.  `params`/`fixed` may be NULL when their
+ * count is 0.  SYNX_OK, or SYNX_E_ARG (malformed name, wrong counts, dimension mismatch, a
+ * CompositeTransform) / SYNX_E_UNSUPPORTED (another type). */
+int synx_linear_from_parameters(const char* type, const double* params, int n_params, const double* fixed,
+                                int n_fixed, int dim, synx_linear* out);
+
 /* Displacement field of a linear transform on `grid`, in host memory, as component planes
  * (component c of voxel i at field[c*N + i], the layout of the step entry points, ready to copy
  * to the device for synx_compose / synx_warp_image): u(p) = T(p) - p at every voxel centre p,

@@ -281,3 +281,53 @@ def test_collapsed_composite(host_cli, tmp_path):
     np.testing.assert_allclose(Cf.M, B.M @ A.M, atol=1e-12)
     np.testing.assert_allclose(Cf.b, B.M @ A.b + B.b, atol=1e-9)
     np.testing.assert_allclose(comp[0][2], A.c, atol=1e-12)
+
+
+def test_restore_state_with_a_rigid_entry(host_cli, tmp_path):
+    # a state whose linear part is a rigid transform (the type a rigid stage saves, here Euler2D): it
+    # becomes the initial moving transform in matrix-offset form, written back as an affine entry, and
+    # the stage starts from the saved fields with the moving image read through it
+    import numpy as np
+
+    import oracle as O
+    import test_zz_stack_apply as S
+    import test_zz_u_state as U
+    from ants_b200 import nifti, phantoms, synx
+    from ants_b200.synx import Geom, SyNParams
+    size = (48, 44)
+    f, m = phantoms.pair_2d(size, seed=36)
+    g = Geom(size)
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    base = [host_cli["reg"], "-d", "2", "--float", "1", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]",
+            "-t", "SyN[0.2,3,0]", "-c", "[4x2,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-a", "1", "-z", "0", "-i", "1"]
+    state = tmp_path / "state.txt"
+    r = subprocess.run(base + ["-j", str(state), "-o", str(tmp_path / "A_")], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = state.read_text().splitlines()
+    assert lines[2].startswith("Transform: CompositeTransform_")
+    euler = ("Euler2DTransform_double_2_2", [0.05, 0.7, -0.4], [20.0, 18.0])
+    lines[3:3] = ["#Transform 1", f"Transform: {euler[0]}", "Parameters: 0.05 0.7 -0.4", "FixedParameters: 20 18"]
+    rigid = tmp_path / "rigid_state.txt"
+    rigid.write_text("\n".join(lines) + "\n")
+    r = subprocess.run(base + ["-k", str(rigid), "-o", str(tmp_path / "B_")], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    L = synx.linear_from_parameters(*euler, 2)
+    th = 0.05
+    np.testing.assert_allclose(L.matrix, [[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]], atol=1e-15)
+    comp = U.read_composite(tmp_path / "B_Composite.txt")
+    assert [t for t, _, _ in comp] == ["AffineTransform_double_2_2", "DisplacementFieldTransform_float_2_2"]
+    np.testing.assert_allclose(comp[0][1], np.r_[L.matrix.ravel(), L.translation], atol=1e-15)
+    np.testing.assert_allclose(comp[0][2], L.center, atol=1e-15)
+    items = U.read_composite(state)
+    half = [np.ascontiguousarray(it[1].astype(np.float32).reshape(size[1], size[0], 2).transpose(2, 0, 1))
+            for it in items]
+    A = S.Affine(L.matrix, L.translation, L.center)
+    P = SyNParams(dim=2, learning_rate=0.2, cc_radius=2, iterations=(4, 2), shrink_factors=(2, 1),
+                  smoothing_sigmas=(1.0, 0.0), convergence_threshold=1e-12)
+    rf, _, _, _ = O.syn_register(f, g, m, S.push_forward(g, A.inverse()), P, initial_half_fields=half,
+                                 initial_geom=g)
+    got = comp[1][1].astype(np.float32).reshape(size[1], size[0], 2).transpose(2, 0, 1)
+    assert float(np.sqrt(((got - rf) ** 2).sum(0).mean())) <= 1e-3

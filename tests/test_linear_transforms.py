@@ -3,6 +3,7 @@ fields (synx_linear_field): host-only entry points of the C ABI, checked on the 
 numpy and scipy's rotation conventions.  The files are written here in the two forms ITK's
 transform IO uses: MATLAB v4 binary (.mat) and Insight text (.txt, the layout of
 Scripts/ANTSAverage3DAffine.sh:94-98)."""
+import ctypes as C
 import os
 import struct
 import subprocess
@@ -348,3 +349,47 @@ def test_fold_moving_geometry_reads_the_image_at_init():
     for q in rng.uniform(-10, 20, (10, 3)):
         init_q = apply(T2, apply(T1, q))
         np.testing.assert_allclose(index_of(gf, q), index_of(g, init_q), atol=1e-9)
+
+
+def test_from_parameters_matches_the_file_reader(tmp_path):
+    # synx_linear_from_parameters converts one (type, parameters, fixed parameters) entry exactly as
+    # synx_read_linear_transform converts that entry of a file
+    v = [0.1, -0.2, 0.15]
+    cases = [
+        (3, "AffineTransform_double_3_3", list(AFFINE3) + list(TRANS3), list(CENTER3)),
+        (3, "MatrixOffsetTransformBase_float_3_3", list(AFFINE3) + list(TRANS3), list(CENTER3)),
+        (3, "Euler3DTransform_double_3_3", [0.3, -0.2, 0.45, 1, 2, 3], [1.0, 2.0, 3.0]),
+        (3, "Euler3DTransform_double_3_3", [0.3, -0.2, 0.45, 1, 2, 3], [1.0, 2.0, 3.0, 1.0]),
+        (3, "VersorRigid3DTransform_double_3_3", v + [1, 2, 3], [1.0, 2.0, 3.0]),
+        (3, "Similarity3DTransform_double_3_3", v + [1, 2, 3, 1.3], [1.0, 2.0, 3.0]),
+        (3, "TranslationTransform_double_3_3", [1, 2, 3], []),
+        (3, "IdentityTransform_double_3_3", [], []),
+        (2, "AffineTransform_double_2_2", [1.1, 0.2, -0.1, 0.9, 4, 5], [3.0, 4.0]),
+        (2, "Euler2DTransform_double_2_2", [0.4, 5, -6], [3.0, 4.0]),
+        (2, "Rigid2DTransform_double_2_2", [0.4, 5, -6], [3.0, 4.0]),
+        (2, "Similarity2DTransform_double_2_2", [0.8, 0.4, 5, -6], [3.0, 4.0]),
+    ]
+    for i, (dim, name, params, fixed) in enumerate(cases):
+        p = tmp_path / f"t{i}.txt"
+        write_txt(p, [(name, params, fixed)])
+        want = synx.read_linear_transform(p, dim)
+        got = synx.linear_from_parameters(name, params, fixed, dim)
+        for a, b in ((got.matrix, want.matrix), (got.translation, want.translation), (got.center, want.center)):
+            np.testing.assert_array_equal(a, b, err_msg=name)
+    lib = synx.load_library()
+    for name, params, fixed, dim, code, needle in [
+        ("CompositeTransform_double_3_3", [], [], 3, -1, "composite is not a linear transform"),
+        ("Euler3DTransform_double_3_3", [0.1, 0.2, 0.3, 1, 2], [0, 0, 0], 3, -1, "expected 6"),
+        ("AffineTransform_double_2_2", [1, 0, 0, 1, 0, 0], [0, 0], 3, -1, "is not a 3-D transform"),
+        ("BSplineTransform_double_3_3", [0.0] * 6, [0, 0, 0], 3, -5, "is not supported"),
+        ("Affine", [1, 0, 0, 1, 0, 0], [0, 0], 2, -1, "unrecognised transform type"),
+    ]:
+        with pytest.raises(SynxError, match=needle):
+            synx.linear_from_parameters(name, params, fixed, dim)
+        t = synx.SynxLinear()
+        arr = (C.c_double * max(len(params), 1))(*params)
+        fx = (C.c_double * max(len(fixed), 1))(*fixed)
+        assert lib.synx_linear_from_parameters(name.encode(), arr, len(params), fx, len(fixed), dim, C.byref(t)) == code
+    assert lib.synx_linear_from_parameters(b"IdentityTransform_double_2_2", None, 0, None, 0, 2, None) == -1
+    assert lib.synx_linear_from_parameters(b"IdentityTransform_double_2_2", None, 1, None, 0, 2,
+                                           C.byref(synx.SynxLinear())) == -1
