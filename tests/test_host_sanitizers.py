@@ -1,7 +1,7 @@
 """Host code under AddressSanitizer and UndefinedBehaviorSanitizer, and the command lines' --help.
 
-The readers of user files -- the ITK transform-file parsers (synx_linear.cpp) and the NIfTI reader
-(nifti_io.cpp) -- are compiled with -fsanitize=address,undefined and fed seeded mutations of valid
+The readers of user files -- the ITK transform-file parsers (synx_linear.cpp), the composite and
+registration-state reader (composite_txt.h) and the NIfTI reader (nifti_io.cpp) -- are compiled with -fsanitize=address,undefined and fed seeded mutations of valid
 files (truncations, byte flips, insertions, random bytes).  Each case must either parse or fail with
 an error; any sanitizer report fails the test.  The reference has no sanitizer builds; its smoke tests
 run every program's --help (Examples/TestSuite/CMakeLists.txt:1038-1044), mirrored at the end.
@@ -23,10 +23,13 @@ DRIVER = r"""
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include "composite_txt.h"
 #include "nifti_io.h"
 #include "synx.h"
 #include "synx_host.h"
-namespace synx { int set_global_error(int code, const std::string&) { return code; } }
+static std::string g_msg;
+namespace synx { int set_global_error(int code, const std::string& m) { g_msg = m; return code; } }
+extern "C" const char* synx_last_error(const synx_ctx*) { return g_msg.c_str(); }
 
 static std::vector<unsigned char> mutate(std::vector<unsigned char> b, std::mt19937& rng) {
   switch (rng() % 4) {
@@ -46,7 +49,8 @@ int main(int argc, char** argv) {
   const std::string dir = argv[1];
   const int cases = atoi(argv[2]);
   std::mt19937 rng(7);
-  // seeds: a MATLAB v4 affine, an Insight text affine, a NIfTI-1 image
+  // seeds: a MATLAB v4 affine, an Insight text affine, a NIfTI-1 image, a composite (rigid entry and a
+  // 2 x 2 displacement field, the form of a saved registration state)
   std::vector<unsigned char> mat;
   auto add = [&](const void* p, size_t n) { auto* c = (const unsigned char*)p; mat.insert(mat.end(), c, c + n); };
   auto var = [&](const char* name, int n) {
@@ -63,9 +67,35 @@ int main(int argc, char** argv) {
   { FILE* f = fopen((dir + "/seed.nii").c_str(), "rb"); unsigned char buf[4096]; size_t n;
     while ((n = fread(buf, 1, sizeof buf, f)) > 0) nii.insert(nii.end(), buf, buf + n); fclose(f); }
   const std::vector<unsigned char> txtb(txt.begin(), txt.end());
-  long parsed = 0, rejected = 0;
+  const std::string comp = "#Insight Transform File V1.0\n#Transform 0\nTransform: CompositeTransform_double_2_2\n"
+                           "#Transform 1\nTransform: Euler2DTransform_double_2_2\nParameters: 0.1 1 2\n"
+                           "FixedParameters: 3 4\n#Transform 2\nTransform: DisplacementFieldTransform_float_2_2\n"
+                           "Parameters: 0.5 -0.25 0 1 2 3 4 5\nFixedParameters: 2 2 0 0 1 1 1 0 0 1\n";
+  const std::vector<unsigned char> compb(comp.begin(), comp.end());
+  long parsed = 0, rejected = 0, cparsed = 0, crejected = 0;
   for (int it = 0; it < cases; ++it) {
-    const int which = it % 3;
+    const int which = it % 4;
+    if (which == 3) {
+      const std::string path = dir + "/c.txt";
+      put(path, mutate(compb, rng));
+      try {
+        std::vector<ants_b200::composite::Item> items = ants_b200::composite::read(path);
+        for (const auto& item : items)
+          for (int dim = 2; dim <= 3; ++dim) {
+            try {
+              if (item.is_field()) ants_b200::composite::field_geom(item, dim);
+              else ants_b200::composite::to_linear(item, dim);
+            } catch (const std::exception&) {
+            }
+          }
+        ants_b200::composite::write(dir + "/rt.txt", 2, items);
+        if (ants_b200::composite::read(dir + "/rt.txt").size() != items.size()) return 3;
+        ++cparsed;
+      } catch (const std::exception&) {
+        ++crejected;
+      }
+      continue;
+    }
     const std::string path = dir + (which == 0 ? "/x.mat" : which == 1 ? "/x.txt" : "/x.nii");
     put(path, mutate(which == 0 ? mat : which == 1 ? txtb : nii, rng));
     if (which < 2) {
@@ -86,7 +116,7 @@ int main(int argc, char** argv) {
       try { nifti::read(path); ++parsed; } catch (const std::exception&) { ++rejected; }
     }
   }
-  printf("parsed %ld rejected %ld\n", parsed, rejected);
+  printf("parsed %ld rejected %ld cparsed %ld crejected %ld\n", parsed, rejected, cparsed, crejected);
   return 0;
 }
 """
@@ -102,11 +132,11 @@ def test_file_readers_under_sanitizers(tmp_path):
                             os.path.join(CSRC, "nifti_io.cpp"), "-lz"], capture_output=True, text=True, timeout=300)
     assert build.returncode == 0, build.stderr[-2000:]
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:allocator_may_return_null=1", UBSAN_OPTIONS="print_stacktrace=1")
-    r = subprocess.run([str(exe), str(tmp_path), "3000"], capture_output=True, text=True, timeout=300, env=env)
+    r = subprocess.run([str(exe), str(tmp_path), "4000"], capture_output=True, text=True, timeout=300, env=env)
     assert r.returncode == 0, (r.stdout + r.stderr)[-3000:]
     assert "runtime error" not in r.stderr and "AddressSanitizer" not in r.stderr, r.stderr[-3000:]
-    parsed, rejected = (int(x) for x in r.stdout.split()[1::2])
-    assert parsed > 0 and rejected > 0
+    parsed, rejected, cparsed, crejected = (int(x) for x in r.stdout.split()[1::2])
+    assert parsed > 0 and rejected > 0 and cparsed > 0 and crejected > 0, r.stdout
 
 
 @pytest.mark.parametrize("exe", ["antsRegistrationSyN_b200", "antsApplyTransforms_b200"])
