@@ -281,6 +281,13 @@ def test_collapsed_composite(host_cli, tmp_path):
     np.testing.assert_allclose(Cf.M, B.M @ A.M, atol=1e-12)
     np.testing.assert_allclose(Cf.b, B.M @ A.b + B.b, atol=1e-9)
     np.testing.assert_allclose(comp[0][2], A.c, atol=1e-12)
+    # without --float 1 the reference's fields are double: the entries say so, and carry the same values
+    r = subprocess.run([a for a in base if a not in ("--float", "1")] + ["-a", "1", "-o", str(tmp_path / "D_")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    dcomp = U.read_composite(tmp_path / "D_Composite.txt")
+    assert [t for t, _, _ in dcomp] == ["AffineTransform_double_2_2", "DisplacementFieldTransform_double_2_2"]
+    np.testing.assert_array_equal(dcomp[1][1].astype(np.float32), comp[1][1].astype(np.float32))
 
 
 def test_restore_state_with_a_rigid_entry(host_cli, tmp_path):
