@@ -20,7 +20,10 @@
 //       A linear transform file (.mat / .txt; the types synx_read_linear_transform reads): [file,1]
 //       applies its inverse.  The transforms of one file act as the composite the file holds: the
 //       last one first, or for [file,1] the inverse of the first one first (:1440-1451).
-//       HDF5 composite files (.h5) are not supported.
+//       A composite transform in ITK's text form (.txt holding displacement fields, as
+//       antsRegistration_b200 -a 1 writes prefixComposite.txt) acts as its entries, the last one
+//       first; [composite,1] is rejected when it holds fields.  HDF5 composite files (.h5) are not
+//       supported.
 //   -n/--interpolation Linear (the default) | NearestNeighbor | GenericLabel[Linear] (label images;
 //       others are rejected)
 //   -f/--default-value v (0): value where the point maps outside the input image
@@ -65,6 +68,7 @@
 #include <vector>
 
 #include "cli_common.h"
+#include "composite_txt.h"
 #include "nifti_io.h"
 #include "synx.h"
 
@@ -106,7 +110,47 @@ struct ChainItem {
   Map map;  // linear transforms
   synx_linear linear{};
   bool invert = false;
+  // a displacement field read from a composite file: component planes on its own grid (a field
+  // given as an image file is read when its turn comes)
+  bool in_memory = false;
+  std::vector<float> planes;
+  synx_geom grid{};
 };
+
+// The entries of a text composite file in application order (the last entry first), or an empty
+// list when the file holds no displacement field (a linear file, read by the linear reader) or is
+// not a composite the text reader takes.
+std::vector<ChainItem> composite_chain(const std::string& file, int dim, bool invert) {
+  std::vector<composite::Item> items;
+  try {
+    items = composite::read(file);
+  } catch (const std::exception&) {
+    return {};
+  }
+  if (std::none_of(items.begin(), items.end(), [](const composite::Item& it) { return it.is_field(); })) return {};
+  if (invert)
+    throw std::runtime_error("the inverse of composite transform '" + file +
+                             "' is not available: it holds displacement fields (use the inverse composite)");
+  std::vector<ChainItem> chain;
+  for (auto it = items.rbegin(); it != items.rend(); ++it) {
+    ChainItem c;
+    c.file = file;
+    if (it->is_field()) {
+      c.grid = composite::field_geom(*it, dim);
+      const size_t n = it->field.size() / (size_t)dim;
+      c.planes.resize(it->field.size());
+      for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < dim; ++k) c.planes[(size_t)k * n + i] = it->field[i * (size_t)dim + (size_t)k];
+      c.in_memory = true;
+    } else {
+      c.is_linear = true;
+      c.linear = composite::to_linear(*it, dim);
+      c.map = map_of(c.linear, false);
+    }
+    chain.push_back(std::move(c));
+  }
+  return chain;
+}
 
 int run(const std::vector<std::string>& args, std::ostream& out) {
   std::map<std::string, std::vector<std::string>> opt;
@@ -203,6 +247,13 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     const std::string lf = lower(file);
     if (ends_with(lf, ".h5") || ends_with(lf, ".hdf5") || ends_with(lf, ".xfm"))
       throw std::runtime_error("transform '" + file + "': HDF5/composite transform files are not supported");
+    if (ends_with(lf, ".txt")) {
+      std::vector<ChainItem> cc = composite_chain(file, dim, invert);
+      if (!cc.empty()) {
+        for (ChainItem& c : cc) chain.push_back(std::move(c));
+        continue;
+      }
+    }
     if (ends_with(lf, ".mat") || ends_with(lf, ".txt")) {
       for (const LinearItem& li : read_linear_file(file, dim, invert)) {
         ChainItem c;
@@ -293,18 +344,27 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       step_ok(synx_field_affine_update(tmp.p, w.p, &ge, c.map.M, w.p, nullptr), "synx_field_affine_update");
       note = c.invert ? " (linear, inverse)" : " (linear)";
     } else {
-      const nifti::Image f = nifti::read(c.file);
-      if (f.components != dim || f.dim != dim || f.time_series)
-        throw std::runtime_error("'" + c.file + "' is not a " + std::to_string(dim) + "-D displacement field");
-      const synx_geom gf = to_geom(f, dim);
-      const long long Nf = f.voxels();
+      nifti::Image f;
+      synx_geom gf;
+      const float* fdata = nullptr;
+      if (c.in_memory) {
+        gf = c.grid;
+        fdata = c.planes.data();
+      } else {
+        f = nifti::read(c.file);
+        if (f.components != dim || f.dim != dim || f.time_series)
+          throw std::runtime_error("'" + c.file + "' is not a " + std::to_string(dim) + "-D displacement field");
+        gf = to_geom(f, dim);
+        fdata = f.data.data();
+      }
+      const long long Nf = gf.size[0] * gf.size[1] * gf.size[2];
       if (same_grid(gf, ge)) {
         // on the evaluation grid: the first field is copied, a later one composed (w + d(x + w))
-        CLI_CK(cudaMemcpy(k == first_field ? w.p : tmp.p, f.data.data(), 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
+        CLI_CK(cudaMemcpy(k == first_field ? w.p : tmp.p, fdata, 4 * (size_t)N * dim, cudaMemcpyHostToDevice));
         if (k != first_field) step_ok(synx_compose(tmp.p, w.p, &ge, 1.0f, w.p, nullptr), "synx_compose");
       } else {
         DeviceBuffer src((size_t)Nf * dim);
-        CLI_CK(cudaMemcpy(src.p, f.data.data(), 4 * (size_t)Nf * dim, cudaMemcpyHostToDevice));
+        CLI_CK(cudaMemcpy(src.p, fdata, 4 * (size_t)Nf * dim, cudaMemcpyHostToDevice));
         if (k == first_field) {
           // sampled on its own grid at the evaluation grid's points
           step_ok(synx_resample_field(src.p, &gf, w.p, &ge, nullptr), "synx_resample_field");

@@ -338,3 +338,51 @@ def test_restore_state_with_a_rigid_entry(host_cli, tmp_path):
                                  initial_geom=g)
     got = comp[1][1].astype(np.float32).reshape(size[1], size[0], 2).transpose(2, 0, 1)
     assert float(np.sqrt(((got - rf) ** 2).sum(0).mean())) <= 1e-3
+
+
+def test_apply_reads_the_composite(host_cli, tmp_path):
+    # antsApplyTransforms -t prefixComposite.txt acts as the separate files of the same registration:
+    # the composite's last entry (the SyN field) first, then the affine; the inverse composite as
+    # -t [prefix0GenericAffine.mat,1] -t prefix1InverseWarp; and [composite,1] is refused
+    import numpy as np
+
+    import test_zz_stack_apply as S
+    from ants_b200 import nifti, phantoms
+    from ants_b200.synx import Geom
+    size = (48, 44)
+    f, m = phantoms.pair_2d(size, seed=37)
+    g = Geom(size, (1.0, 0.9))
+    A = S.Affine([[1.01, 0.02], [-0.01, 0.98]], [0.5, -0.4], [24.0, 20.0])
+    A.write_mat(tmp_path / "a.mat")
+    nifti.write(tmp_path / "f.nii.gz", f, g)
+    nifti.write(tmp_path / "m.nii.gz", m, g)
+    base = [host_cli["reg"], "-d", "2", "--float", "1", "-m", f"CC[{tmp_path}/f.nii.gz,{tmp_path}/m.nii.gz,1,2]",
+            "-t", "SyN[0.2,3,0]", "-c", "[4x2,1e-12,10]", "-f", "2x1", "-s", "1x0vox", "-r", f"{tmp_path}/a.mat"]
+    for extra in (["-o", str(tmp_path / "A_")], ["-a", "1", "-o", str(tmp_path / "B_")]):
+        r = subprocess.run(base + extra, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+
+    def apply(ref, inp, ts, out, collapse=False):
+        o = f"[{tmp_path / out},1]" if collapse else str(tmp_path / out)
+        args = [host_cli["apply"], "-d", "2", "--float", "1", "-i", f"{tmp_path}/{inp}.nii.gz",
+                "-r", f"{tmp_path}/{ref}.nii.gz"] + sum((["-t", t] for t in ts), []) + ["-o", o]
+        r = subprocess.run(args, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        return nifti.read(tmp_path / out, 2)[0]
+
+    p, q = str(tmp_path / "A_"), str(tmp_path / "B_")
+    want = apply("f", "m", [f"{p}1Warp.nii.gz", f"{p}0GenericAffine.mat"], "w_files.nii.gz")
+    got = apply("f", "m", [f"{q}Composite.txt"], "w_comp.nii.gz")
+    np.testing.assert_array_equal(got, want)
+    want = apply("m", "f", [f"[{p}0GenericAffine.mat,1]", f"{p}1InverseWarp.nii.gz"], "i_files.nii.gz")
+    got = apply("m", "f", [f"{q}InverseComposite.txt"], "i_comp.nii.gz")
+    bad = np.abs(got - want) > 1e-5  # the inverse affine is stored re-centred: rounding-level changes
+    assert bad.mean() < 1e-3, int(bad.sum())
+    # the collapsed field through the composite equals the one through the files
+    cf = apply("f", "m", [f"{q}Composite.txt"], "c_comp.nii.gz", collapse=True)
+    ff = apply("f", "m", [f"{p}1Warp.nii.gz", f"{p}0GenericAffine.mat"], "c_files.nii.gz", collapse=True)
+    np.testing.assert_array_equal(cf, ff)
+    r = subprocess.run([host_cli["apply"], "-d", "2", "-i", f"{tmp_path}/m.nii.gz", "-r", f"{tmp_path}/f.nii.gz",
+                        "-t", f"[{q}Composite.txt,1]", "-o", str(tmp_path / "x.nii.gz")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0 and "use the inverse composite" in r.stderr, r.stderr
