@@ -28,6 +28,8 @@ CLI = os.path.join(HERE, "antsRegistrationSyN_b200")
 # the C++ library entry `ants::antsRegistration(std::vector<std::string>, std::ostream*)`
 REG_LIB = os.path.join(HERE, "libantsRegistration_b200.so")
 APPLY_CLI = os.path.join(HERE, "antsApplyTransforms_b200")
+# the C++ library entry `ants::antsApplyTransforms(std::vector<std::string>, std::ostream*)`
+APPLY_LIB = os.path.join(HERE, "libantsApplyTransforms_b200.so")
 
 LIB_SOURCES = ["synx_kernels.cu", "synx_cc.cu", "synx_level.cu", "synx_ctx.cu", "synx_noalloc.cu", "synx_server.cpp",
                "synx_linear.cpp", "synx_tune.cpp"]
@@ -108,23 +110,34 @@ def _build_exe(target: str, sources: list[str], force: bool) -> str | None:
     return target
 
 
-def build_reg_lib(force: bool = False) -> str | None:
-    """libantsRegistration_b200.so: the command line without its main(), exporting the reference's
-    library symbol ants::antsRegistration for wrappers."""
-    srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES]
+def _build_entry_lib(target: str, sources: list[str], force: bool) -> str:
+    """A command line without its main(), as a shared library exporting its ants:: entry symbol."""
+    srcs = [os.path.join(CSRC, s) for s in sources]
     deps = srcs + [os.path.join(CSRC, h) for h in CLI_HEADERS] + [LIB]
-    if not force and not _stale(REG_LIB, deps):
-        return REG_LIB
+    if not force and not _stale(target, deps):
+        return target
     cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", "-fPIC", "-shared", "-DSYNX_CLI_NO_MAIN", "-I", INCLUDE,
-           "-I", "/usr/local/cuda/include", "-o", REG_LIB, *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN",
+           "-I", "/usr/local/cuda/include", "-o", target, *srcs, "-L", HERE, "-lsynx", "-Wl,-rpath,$ORIGIN",
            "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,/usr/local/cuda/lib64", "-lz"]
     _run(cmd)
-    return REG_LIB
+    return target
+
+
+def build_reg_lib(force: bool = False) -> str | None:
+    """libantsRegistration_b200.so: the registration command line without its main(), exporting the
+    reference's library symbol ants::antsRegistration for wrappers."""
+    return _build_entry_lib(REG_LIB, CLI_SOURCES, force)
+
+
+def build_apply_lib(force: bool = False) -> str | None:
+    """libantsApplyTransforms_b200.so: the same for ants::antsApplyTransforms."""
+    return _build_entry_lib(APPLY_LIB, APPLY_SOURCES, force)
 
 
 def build_cli(force: bool = False) -> str | None:
-    """antsRegistrationSyN_b200, antsApplyTransforms_b200 and libantsRegistration_b200.so."""
+    """antsRegistrationSyN_b200, antsApplyTransforms_b200 and the two entry-symbol libraries."""
     _build_exe(APPLY_CLI, APPLY_SOURCES, force)
+    build_apply_lib(force)
     build_reg_lib(force)
     return _build_exe(CLI, CLI_SOURCES, force)
 

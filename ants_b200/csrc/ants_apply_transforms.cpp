@@ -54,6 +54,7 @@
 // outside a field's grid (no displacement), as ITK's composite applies them.  The collapsed field,
 // L_post(x_G + w) - p, is assembled on the host while it is written.
 #include "ants_apply_transforms.h"
+#include "antsApplyTransforms.h"  // the exported ants::antsApplyTransforms
 
 #include <cuda_runtime.h>
 
@@ -474,7 +475,17 @@ int antsApplyTransforms(std::vector<std::string> args, std::ostream* out) {
 
 }  // namespace ants_b200
 
+namespace ants {
+
+int antsApplyTransforms(std::vector<std::string> args, std::ostream* out_stream) {
+  return ants_b200::antsApplyTransforms(std::move(args), out_stream);
+}
+
+}  // namespace ants
+
+#ifndef SYNX_CLI_NO_MAIN
 int main(int argc, char** argv) {
   std::vector<std::string> args(argv + 1, argv + argc);
-  return ants_b200::antsApplyTransforms(args, &std::cout);
+  return ants::antsApplyTransforms(args, &std::cout);
 }
+#endif

@@ -36,6 +36,7 @@
 // written as prefix<n>DerivedInitialMovingTranslation.mat.  Other stages, metrics, initial fixed
 // transforms and HDF5 transform files are rejected with EXIT_FAILURE.
 #include "ants_registration.h"
+#include "antsRegistration.h"  // the exported ants::antsRegistration
 
 #include <cuda_runtime.h>
 

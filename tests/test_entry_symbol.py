@@ -1,9 +1,11 @@
-"""The reference's C++ library entry, ants::antsRegistration, links and behaves like the reference's.
+"""The reference's C++ library entries, ants::antsRegistration and ants::antsApplyTransforms, link and
+behave like the reference's.
 
 A wrapper that binds the reference declares `int ants::antsRegistration(std::vector<std::string>,
-std::ostream*)` (Examples/include/antsRegistration.h:7-9).  The caller below is compiled against that
-declaration alone and linked against libantsRegistration_b200.so; the calls it makes end before any
-device work (help, option errors), so this runs without a GPU.
+std::ostream*)` (Examples/include/antsRegistration.h:7-9) and `int ants::antsApplyTransforms(...)` of the
+same shape (Examples/include/antsApplyTransforms.h:4-10).  The callers below are compiled against those
+declarations alone and linked against libantsRegistration_b200.so / libantsApplyTransforms_b200.so; the
+calls they make end before any device work (help, option errors), so this runs without a GPU.
 """
 import os
 import subprocess
@@ -79,3 +81,31 @@ def test_double_precision_request_warns(caller):
     assert "WARNING: double precision requested" in err0
     assert "WARNING: double precision requested" in err_default
     assert "WARNING" not in err1
+
+
+APPLY_CALLER = CALLER.replace("antsRegistration", "antsApplyTransforms")
+
+
+@pytest.fixture(scope="module")
+def apply_caller(tmp_path_factory):
+    from ants_b200 import build
+    build.build_lib()
+    build.build_apply_lib()
+    d = tmp_path_factory.mktemp("apply_entry")
+    src = d / "caller.cpp"
+    src.write_text(APPLY_CALLER)
+    exe = d / "caller"
+    subprocess.run(["g++", "-std=c++17", "-o", str(exe), str(src), "-L", LIBDIR, "-lantsApplyTransforms_b200",
+                    f"-Wl,-rpath,{LIBDIR}"], check=True)
+    return str(exe)
+
+
+def test_apply_entry_symbol(apply_caller, tmp_path):
+    rc, out, _ = run(apply_caller, ["--help"])
+    assert rc == 0 and "antsApplyTransforms_b200" in out
+    rc, _, err = run(apply_caller, ["-Q", "1"])
+    assert rc == 1 and "unexpected argument '-Q'" in err
+    # a missing input file fails inside the call, before any device work, without an exception escaping
+    rc, _, err = run(apply_caller, ["-d", "3", "-i", str(tmp_path / "none.nii.gz"), "-r", str(tmp_path / "none.nii.gz"),
+                                    "-t", "[" + str(tmp_path / "w.nii.gz") + ",1]", "-o", str(tmp_path / "o.nii.gz")])
+    assert rc == 1 and "inverse of displacement field" in err
