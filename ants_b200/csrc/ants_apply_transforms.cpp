@@ -17,7 +17,7 @@
 //       maps p to A(p + u(p)), as the registration's own composite does.
 //       A displacement field image: [field,0] is accepted; [field,1] is rejected (a displacement
 //       field has no closed-form inverse: pass the InverseWarp field instead).
-//       A linear transform file (.mat / .txt; the types synx_read_linear_transform reads): [file,1]
+//       A linear transform file (.mat / .txt / .tfm; the types synx_read_linear_transform reads): [file,1]
 //       applies its inverse.  The transforms of one file act as the composite the file holds: the
 //       last one first, or for [file,1] the inverse of the first one first (:1440-1451).
 //       A composite transform in ITK's text form (.txt holding displacement fields, as
@@ -248,14 +248,14 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     const std::string lf = lower(file);
     if (ends_with(lf, ".h5") || ends_with(lf, ".hdf5") || ends_with(lf, ".xfm"))
       throw std::runtime_error("transform '" + file + "': HDF5/composite transform files are not supported");
-    if (ends_with(lf, ".txt")) {
+    if (ends_with(lf, ".txt") || ends_with(lf, ".tfm")) {
       std::vector<ChainItem> cc = composite_chain(file, dim, invert);
       if (!cc.empty()) {
         for (ChainItem& c : cc) chain.push_back(std::move(c));
         continue;
       }
     }
-    if (ends_with(lf, ".mat") || ends_with(lf, ".txt")) {
+    if (ends_with(lf, ".mat") || ends_with(lf, ".txt") || ends_with(lf, ".tfm")) {
       for (const LinearItem& li : read_linear_file(file, dim, invert)) {
         ChainItem c;
         c.file = file;

@@ -13,7 +13,7 @@
 //   -v/--verbose 0|1   --random-seed N (accepted, no effect: the stage is deterministic)
 //   --gpu N (device index; not a reference option)
 //   -r/--initial-moving-transform file | [file,useInverse] | identity | [fixed,moving,feature]
-//       (repeatable, the first given acting first; linear .mat/.txt files, or the translation derived
+//       (repeatable, the first given acting first; linear .mat/.txt/.tfm files, or the translation derived
 //       from two images: feature 0 geometric centers, 1 centers of mass, 2 origins)
 //   -z/--collapse-output-transforms 0|1 (default 1)
 //   -a/--write-composite-transform 0|1: prefixComposite.txt and prefixInverseComposite.txt instead of
@@ -175,10 +175,11 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     }
     const std::string lf = lower(file);
     const bool is_linear_file = lf.size() > 4 && (lf.compare(lf.size() - 4, 4, ".mat") == 0 ||
-                                                  lf.compare(lf.size() - 4, 4, ".txt") == 0);
+                                                  lf.compare(lf.size() - 4, 4, ".txt") == 0 ||
+                                                  lf.compare(lf.size() - 4, 4, ".tfm") == 0);
     if (!is_linear_file)
       throw std::runtime_error("initial moving transform '" + file +
-                               "': only linear transform files (.mat/.txt) are supported");
+                               "': only linear transform files (.mat/.txt/.tfm) are supported");
     for (const LinearItem& li : read_linear_file(file, dim, invert)) init.push_back(li);
   }
   // --restore-state: [linear..., fixedToMiddle, its inverse, movingToMiddle, its inverse]

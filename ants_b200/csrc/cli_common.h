@@ -178,7 +178,7 @@ inline synx_geom push_forward(const synx_geom& g, const Map& L) {
   return r;
 }
 
-// One linear transform of a .mat/.txt file, in application order.
+// One linear transform of a .mat/.txt/.tfm file, in application order.
 struct LinearItem {
   synx_linear linear;
   Map map;  // the map applied (already inverted for [file,1])

@@ -10,7 +10,8 @@
 //    writes either, a vector reads the same both ways), P element type (0 double, 1 float) and
 //    T = 0 (a full numeric matrix).  A variable named after a transform type holds that
 //    transform's parameters; the variable "fixed" after it holds its fixed parameters.
-//  * Insight text (.txt): "#Insight Transform File V1.0", then per transform a "Transform: <type>"
+//  * Insight text (.txt, or .tfm, the other name ITK's text transform IO takes): "#Insight Transform
+//    File V1.0", then per transform a "Transform: <type>"
 //    line, a "Parameters:" line and a "FixedParameters:" line (the form
 //    Scripts/ANTSAverage3DAffine.sh:94-98 writes).
 // Type names are <Base>_<double|float>_<D>_<D>.  Every supported type is reduced to the
@@ -328,8 +329,8 @@ int synx_read_linear_transform(const char* path, int dim, int index, synx_linear
   try {
     const std::string p(path);
     const std::string ext = lower_ext(p);
-    if (ext != ".mat" && ext != ".txt")
-      fail(SYNX_E_UNSUPPORTED, "'" + p + "': linear transforms are read from .mat or .txt files");
+    if (ext != ".mat" && ext != ".txt" && ext != ".tfm")
+      fail(SYNX_E_UNSUPPORTED, "'" + p + "': linear transforms are read from .mat, .txt or .tfm files");
     const std::vector<char> buf = slurp(p);
     const std::vector<RawTransform> raw = ext == ".mat" ? parse_mat(buf, p) : parse_txt(buf, p);
     std::vector<synx_linear> lin;
@@ -494,8 +495,8 @@ int synx_write_linear_transform(const char* path, const synx_linear* t) {
   const int D = t->dim;
   if (D != 2 && D != 3) return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "dim must be 2 or 3");
   const std::string p(path), ext = lower_ext(p);
-  if (ext != ".mat" && ext != ".txt")
-    return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "'" + p + "': write a .mat or .txt file");
+  if (ext != ".mat" && ext != ".txt" && ext != ".tfm")
+    return synx::set_global_error(SYNX_E_ARG, std::string(fn) + "'" + p + "': write a .mat, .txt or .tfm file");
   std::vector<double> params, fixed;
   for (int i = 0; i < D; ++i)
     for (int j = 0; j < D; ++j) params.push_back(t->matrix[i * 3 + j]);

@@ -419,7 +419,7 @@ typedef struct synx_linear {
 
 /* Reads linear transform `index` (0-based, file order) of an ITK transform file: the MATLAB v4
  * binary form (.mat; a parameter variable named after the transform type, then "fixed") or the
- * Insight text form (.txt: "Transform:", "Parameters:", "FixedParameters:" lines).  Types, double
+ * Insight text form (.txt or .tfm: "Transform:", "Parameters:", "FixedParameters:" lines).  Types, double
  * or float, `dim` x `dim`: AffineTransform, MatrixOffsetTransformBase, TranslationTransform,
  * IdentityTransform, Euler2DTransform, Rigid2DTransform, Similarity2DTransform, Euler3DTransform,
  * VersorRigid3DTransform, Similarity3DTransform; a CompositeTransform entry is skipped (its
@@ -458,7 +458,7 @@ int synx_initial_translation(const float* fixed_host, const synx_geom* fixed_geo
 /* Writes `transform` as an ITK AffineTransform_double_<dim>_<dim> file: MATLAB v4 (.mat,
  * little-endian double column vectors "AffineTransform_double_D_D" = A row-major then t, and
  * "fixed" = c), the form antsRegistration writes prefix0GenericAffine.mat in, or Insight text
- * (.txt).  SYNX_E_ARG for another extension or a file that cannot be written. */
+ * (.txt or .tfm).  SYNX_E_ARG for another extension or a file that cannot be written. */
 int synx_write_linear_transform(const char* path, const synx_linear* transform);
 
 #ifdef __cplusplus

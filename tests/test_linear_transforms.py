@@ -228,7 +228,7 @@ def test_linear_field_rejects_singular_inverse_and_bad_grids():
         synx.linear_field(t, Geom((4, 4)))
 
 
-@pytest.mark.parametrize("ext", [".mat", ".txt"])
+@pytest.mark.parametrize("ext", [".mat", ".txt", ".tfm"])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_write_round_trip(tmp_path, ext, dim):
     if dim == 3:
