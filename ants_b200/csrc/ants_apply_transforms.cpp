@@ -27,8 +27,10 @@
 //   -n/--interpolation Linear (the default) | NearestNeighbor | GenericLabel[Linear] (label images;
 //       others are rejected)
 //   -f/--default-value v (0): value where the point maps outside the input image
-//   -o/--output warped | [collapsed,1] | DisplacementField[collapsed]  (the collapsed form writes
-//       the single displacement field equivalent to the stack, on the reference grid, :1115-1131)
+//   -o/--output warped | [warped,0] | [collapsed,1] | DisplacementField[collapsed]  (the collapsed
+//       form writes the single displacement field equivalent to the stack, on the reference grid,
+//       :1115-1131) | CompositeTransform[file.txt]  (the stack uncollapsed, in ITK's text form; no
+//       reference image needed)
 //       | Linear[collapsed.mat,invert]  (an all-linear stack as one affine transform file)
 //   -u/--output-data-type char|uchar|short|int|float|double|default (a cast of the float result)
 //   --float 0|1 (computation is float32 either way; output files, the collapsed field and the
@@ -194,8 +196,11 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     throw std::runtime_error("GenericLabel supports the Linear interpolator only");
   const bool nearest = interp == "nearestneighbor", label = interp == "genericlabel";
   if (!opt.count("output")) throw std::runtime_error("an output (-o) is required");
-  const bool linear_out = lower(parse_call(one("output", "")).name) == "linear";
-  if (!linear_out && !opt.count("reference-image")) throw std::runtime_error("a reference image (-r) is required");
+  const std::string out_form = lower(parse_call(one("output", "")).name);
+  const bool linear_out = out_form == "linear";
+  // Linear[...] and CompositeTransform[...] write transforms only (:436-460)
+  if (!linear_out && out_form != "compositetransform" && !opt.count("reference-image"))
+    throw std::runtime_error("a reference image (-r) is required");
   const bool verbose = one("verbose", "0") == "1" || lower(one("verbose", "0")) == "true";
   const int gpu = std::atoi(one("gpu", "0").c_str());
   const float defval = (float)std::atof(one("default-value", "0").c_str());
@@ -213,7 +218,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
 
   // output form
   OptionCall o = parse_call(one("output", ""));
-  bool collapse = false;
+  bool collapse = false, composite_out = false;
   std::string out_path;
   if (lower(o.name) == "displacementfield") {
     if (o.params.size() != 1) throw std::runtime_error("DisplacementField[file] needs one file name");
@@ -221,17 +226,21 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     out_path = o.params[0];
   } else if (o.name.empty() && !o.params.empty()) {
     out_path = o.params[0];
+    // [file,1]: the collapsed field; [file,0]: the warped image, as a plain name (:404-421)
     collapse = o.params.size() > 1 && (o.params[1] == "1" || lower(o.params[1]) == "true");
-    if (!collapse) throw std::runtime_error("-o [file,0] is not a supported output form");
   } else if (linear_out) {
     if (o.params.empty() || o.params.size() > 2) throw std::runtime_error("Linear[file.mat,invert] needs a file name");
     out_path = o.params[0];
   } else if (lower(o.name) == "compositetransform") {
-    throw std::runtime_error("-o " + o.name + "[...] is not supported (displacement fields only)");
+    // the stack as one composite transform file, uncollapsed (:444-460, :690-701)
+    if (o.params.size() != 1) throw std::runtime_error("CompositeTransform[file] needs one file name");
+    composite_out = true;
+    out_path = o.params[0];
   } else {
     out_path = o.name;
   }
-  if (!collapse && !linear_out && !opt.count("input")) throw std::runtime_error("an input image (-i) is required");
+  if (!collapse && !linear_out && !composite_out && !opt.count("input"))
+    throw std::runtime_error("an input image (-i) is required");
 
   // the chain in application order: command-line order, each file's transforms as its composite
   std::vector<ChainItem> chain;
@@ -303,6 +312,40 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     }
     step_ok(synx_write_linear_transform(out_path.c_str(), &t), "synx_write_linear_transform");
     if (verbose) out << "wrote the collapsed linear transform " << out_path << "\n";
+    return EXIT_SUCCESS;
+  }
+
+  if (composite_out) {
+    // ITK's queue order: the transform acting last first.  Linear entries in matrix-offset form
+    // (AffineTransform: a rigid or similarity entry keeps its map, not its type); an inverted one as
+    // its inverse map about the same center; fields with their own grids.  Text form only.
+    std::vector<composite::Item> items;
+    for (auto it = chain.rbegin(); it != chain.rend(); ++it) {
+      const ChainItem& c = *it;
+      if (c.is_linear) {
+        items.push_back(composite::linear_item(c.invert ? linear_of(c.map, dim, c.linear.center) : c.linear, dim));
+        continue;
+      }
+      synx_geom gf;
+      std::vector<float> planes;
+      if (c.in_memory) {
+        gf = c.grid;
+        planes = c.planes;
+      } else {
+        nifti::Image f = nifti::read(c.file);
+        if (f.components != dim || f.dim != dim || f.time_series)
+          throw std::runtime_error("'" + c.file + "' is not a " + std::to_string(dim) + "-D displacement field");
+        gf = to_geom(f, dim);
+        planes = std::move(f.data);
+      }
+      const size_t n = planes.size() / (size_t)dim;
+      std::vector<float> v(planes.size());
+      for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < dim; ++k) v[i * (size_t)dim + (size_t)k] = planes[(size_t)k * n + i];
+      items.push_back(composite::field_item(gf, v, real_type == 64));
+    }
+    composite::write(out_path, dim, items);
+    if (verbose) out << "wrote the composite transform " << out_path << "\n";
     return EXIT_SUCCESS;
   }
 

@@ -34,7 +34,7 @@ def run(exe, args):
     (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz", "-n", "BSpline[3]"], "NearestNeighbor"),
     (["-d", "5", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz"], "dimensionality"),
     (["-d", "3", "-e", "2", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "x.nii.gz"], "multichannel (4)"),
-    (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "CompositeTransform[x.h5]"], "not supported"),
+    (["-d", "3", "-i", "a.nii.gz", "-r", "a.nii.gz", "-o", "CompositeTransform[x.h5]"], "HDF5 (.h5) is not available"),
     (["-d", "3", "-i", "a.nii.gz", "-r", "/nonexistent/r.nii.gz", "-o", "x.nii.gz"], "cannot open"),
 ])
 def test_rejects_bad_input(exe, args, needle):

@@ -386,3 +386,35 @@ def test_apply_reads_the_composite(host_cli, tmp_path):
                         "-t", f"[{q}Composite.txt,1]", "-o", str(tmp_path / "x.nii.gz")],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode != 0 and "use the inverse composite" in r.stderr, r.stderr
+
+    # -o CompositeTransform[file] writes the stack uncollapsed (no input or reference image needed): the
+    # same composite antsRegistration -a 1 wrote, and it applies as the files do
+    def write_composite(ts, out):
+        args = [host_cli["apply"], "-d", "2", "--float", "1"] + sum((["-t", t] for t in ts), [])
+        r = subprocess.run(args + ["-o", f"CompositeTransform[{tmp_path / out}]"], capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr
+        return U.read_composite(tmp_path / out)
+
+    import test_zz_u_state as U
+    fw = write_composite([f"{p}1Warp.nii.gz", f"{p}0GenericAffine.mat"], "fw.txt")
+    reg = U.read_composite(tmp_path / "B_Composite.txt")
+    assert [t for t, _, _ in fw] == [t for t, _, _ in reg]
+    for (_, a, fa), (_, b, fb) in zip(fw, reg):
+        np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(fa, fb)
+    np.testing.assert_array_equal(apply("f", "m", [str(tmp_path / "fw.txt")], "w_fw.nii.gz"),
+                                  apply("f", "m", [f"{p}1Warp.nii.gz", f"{p}0GenericAffine.mat"], "w_files2.nii.gz"))
+    iv = write_composite([f"[{p}0GenericAffine.mat,1]", f"{p}1InverseWarp.nii.gz"], "iv.txt")
+    assert [t for t, _, _ in iv] == ["DisplacementFieldTransform_float_2_2", "AffineTransform_double_2_2"]
+    got = apply("m", "f", [str(tmp_path / "iv.txt")], "i_iv.nii.gz")
+    bad = np.abs(got - want) > 1e-5
+    assert bad.mean() < 1e-3, int(bad.sum())
+    # -o [warped,0] is the plain warped output
+    np.testing.assert_array_equal(apply("f", "m", [f"{q}Composite.txt"], "w0.nii.gz"),
+                                  nifti.read(tmp_path / "w_comp.nii.gz", 2)[0])
+    r = subprocess.run([host_cli["apply"], "-d", "2", "--float", "1", "-i", f"{tmp_path}/m.nii.gz", "-r",
+                        f"{tmp_path}/f.nii.gz", "-t", f"{q}Composite.txt", "-o", f"[{tmp_path / 'w0b.nii.gz'},0]"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    np.testing.assert_array_equal(nifti.read(tmp_path / "w0b.nii.gz", 2)[0], nifti.read(tmp_path / "w_comp.nii.gz", 2)[0])
