@@ -11,6 +11,10 @@
 //   -o/--output prefix | [prefix,warpedImage,inverseWarpedImage]
 //   -w/--winsorize-image-intensities [lower,upper]   -u/--use-histogram-matching 0|1
 //   -v/--verbose 0|1   --random-seed N (accepted, no effect: the stage is deterministic)
+//   -p/--print-similarity-measure-interval N, --write-interval-volumes N, -l/--use-estimate-learning-
+//       rate-once (accepted; non-zero intervals are not implemented and draw a warning)
+//   --minc 0 (1 is refused: NIfTI output only)   --version
+//   Unknown options are accepted with a warning, as the reference's parser keeps and ignores them.
 //   --gpu N (device index; not a reference option)
 //   -r/--initial-moving-transform file | [file,useInverse] | identity | [fixed,moving,feature]
 //       (repeatable, the first given acting first; linear .mat/.txt/.tfm files, or the translation derived
@@ -79,7 +83,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
       {"-w", "winsorize-image-intensities"}, {"-u", "use-histogram-matching"}, {"-x", "masks"},
       {"-r", "initial-moving-transform"}, {"-q", "initial-fixed-transform"}, {"-n", "interpolation"},
       {"-a", "write-composite-transform"}, {"-z", "collapse-output-transforms"}, {"-h", "help"},
-      {"-i", "initialize-transforms-per-stage"}, {"-j", "save-state"}, {"-k", "restore-state"}};
+      {"-i", "initialize-transforms-per-stage"}, {"-j", "save-state"}, {"-k", "restore-state"},
+      {"-p", "print-similarity-measure-interval"}, {"-l", "use-estimate-learning-rate-once"}};
   for (size_t i = 0; i < args.size(); ++i) {
     std::string k = args[i];
     std::string name;
@@ -88,6 +93,10 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     else throw std::runtime_error("unexpected argument '" + k + "'");
     if (name == "help") {
       out << "antsRegistrationSyN_b200: antsRegistration options for one SyN + CC stage on a B200\n";
+      return EXIT_SUCCESS;
+    }
+    if (name == "version") {
+      out << "antsRegistrationSyN_b200: the antsRegistration SyN + CC stage on the synx C ABI (sm_100a)\n";
       return EXIT_SUCCESS;
     }
     if (i + 1 >= args.size()) throw std::runtime_error("option --" + name + " needs a value");
@@ -99,6 +108,32 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   };
   for (const char* bad : {"initial-fixed-transform", "restrict-deformation"})
     if (opt.count(bad)) throw std::runtime_error(std::string("option --") + bad + " is not supported by this SyN+CC stage");
+  // The reference's parser keeps options it does not know and goes on (Utilities/antsCommandLineParser
+  // .cxx:124-160); so does this one, with a warning, since a misspelt option would otherwise pass unseen.
+  // Options of the reference this stage does not implement: MINC output is refused (only NIfTI is
+  // written); the full-scale metric printout (-p) and the interval volumes are ignored with a warning.
+  static const char* const known[] = {
+      "dimensionality", "output", "save-state", "restore-state", "write-composite-transform",
+      "print-similarity-measure-interval", "write-interval-volumes", "collapse-output-transforms",
+      "initialize-transforms-per-stage", "interpolation", "initial-moving-transform", "metric", "transform",
+      "convergence", "smoothing-sigmas", "shrink-factors", "use-histogram-matching", "use-estimate-learning-rate-once",
+      "winsorize-image-intensities", "masks", "float", "minc", "random-seed", "verbose", "gpu"};
+  for (const auto& kv : opt) {
+    if (std::find_if(std::begin(known), std::end(known), [&](const char* k) { return kv.first == k; }) ==
+        std::end(known))
+      std::cerr << "antsRegistrationSyN_b200: WARNING: unknown option --" << kv.first << " ignored" << std::endl;
+  }
+  for (const char* ignored : {"print-similarity-measure-interval", "write-interval-volumes"}) {
+    if (!opt.count(ignored)) continue;
+    const std::string v = opt[ignored].back();
+    if (!(v == "0" || v.empty()))
+      std::cerr << "antsRegistrationSyN_b200: WARNING: --" << ignored << " " << v << " is not implemented; ignored"
+                << std::endl;
+  }
+  if (opt.count("minc")) {
+    const std::string v = lower(opt["minc"].back());
+    if (!(v == "0" || v == "false")) throw std::runtime_error("MINC output (--minc 1) is not supported: NIfTI only");
+  }
   auto flag = [&](const std::string& n, bool def) {
     if (!opt.count(n)) return def;
     const std::string v = lower(one(n, ""));

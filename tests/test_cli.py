@@ -65,11 +65,32 @@ def test_nifti_roundtrip_scalar_and_vector(tmp_path):
       "-a", "1", "-i", "1"], "mutually exclusive"),
     (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
       "-q", "a.mat"], "initial-fixed-transform"),
+    (["-d", "3", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x",
+      "--minc", "1"], "MINC output"),
 ])
 def test_cli_rejects_bad_input(cli, args, needle):
     r = run(cli, args)
     assert r.returncode == 1
     assert needle in r.stderr
+
+
+def test_cli_options_it_keeps_but_does_not_implement(cli):
+    # the reference's parser keeps unknown options and goes on; this one does too, and says so. Its
+    # other options are accepted (-p, -l, --write-interval-volumes, --minc 0, --random-seed, --version);
+    # the non-zero intervals draw a warning. The run then stops at the missing images, before device work.
+    r = run(cli, ["--version"])
+    assert r.returncode == 0 and "antsRegistrationSyN_b200" in r.stdout
+    base = ["-d", "3", "--float", "1", "-m", "CC[/nonexistent/f.nii.gz,/nonexistent/m.nii.gz,1,4]",
+            "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0", "-o", "x"]
+    r = run(cli, base + ["--convergance", "[5,1e-6,10]", "-p", "5", "--write-interval-volumes", "3", "-l", "1",
+                         "--minc", "0", "--random-seed", "7"])
+    assert r.returncode == 1 and "cannot open" in r.stderr, r.stderr
+    assert "unknown option --convergance ignored" in r.stderr
+    assert "--print-similarity-measure-interval 5 is not implemented" in r.stderr
+    assert "--write-interval-volumes 3 is not implemented" in r.stderr
+    assert "unexpected argument" not in r.stderr and "--use-estimate" not in r.stderr
+    r = run(cli, base + ["-p", "0", "--write-interval-volumes", "0"])
+    assert "WARNING" not in r.stderr, r.stderr
 
 
 @pytest.mark.gpu
