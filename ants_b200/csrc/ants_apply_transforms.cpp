@@ -6,6 +6,8 @@
 // transforms before them (prefix0GenericAffine.mat).  Options follow
 // Examples/antsApplyTransforms.cxx:1063-1240:
 //   -d/--dimensionality 2|3      -i/--input image     -r/--reference-image image
+//   --time-index t (with -e 3: volume t alone, into a 3-D image)   -z/--static-cast-for-R (accepted)
+//   Unknown options are accepted with a warning, as the reference's parser keeps and ignores them.
 //   -e/--input-image-type 0|scalar (default) | 3|time-series | 4|multichannel (each volume or channel
 //       resampled in turn)
 //   -t/--transform file  (repeatable).  Order: a reference point is moved by the FIRST transform
@@ -160,7 +162,7 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   const std::map<std::string, std::string> alias = {
       {"-d", "dimensionality"}, {"-i", "input"},         {"-r", "reference-image"}, {"-t", "transform"},
       {"-n", "interpolation"},  {"-f", "default-value"}, {"-o", "output"},          {"-v", "verbose"},
-      {"-e", "input-image-type"}, {"-u", "output-data-type"}, {"-h", "help"}};
+      {"-e", "input-image-type"}, {"-u", "output-data-type"}, {"-h", "help"}, {"-z", "static-cast-for-R"}};
   for (size_t i = 0; i < args.size(); ++i) {
     const std::string& k = args[i];
     std::string name;
@@ -184,10 +186,30 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
   // are resampled one by one (:516-535, :903-981); vector and tensor inputs are rejected
   const std::string itype = lower(one("input-image-type", "0"));
   const bool multichannel = itype == "4" || itype == "multichannel";
-  const bool series = itype == "3" || itype == "time-series";
+  bool series = itype == "3" || itype == "time-series";
   if (!(itype == "0" || itype == "scalar" || multichannel || series))
     throw std::runtime_error("only scalar (0), time-series (3) and multichannel (4) input images are supported");
   if (series && dim != 3) throw std::runtime_error("time-series input (-e 3) needs -d 3");
+  // --time-index t with -e 3: only volume t is resampled, into a 3-D image (:242-249, :283-317); the
+  // reference reads it for time series only
+  long long time_index = -1;
+  if (series && opt.count("time-index")) {
+    const std::string v = one("time-index", "0");
+    char* end = nullptr;
+    time_index = std::strtoll(v.c_str(), &end, 10);
+    if (end == v.c_str() || *end != '\0' || time_index < 0)
+      throw std::runtime_error("--time-index must be a non-negative integer");
+  }
+  // options of the reference this front end keeps without using (-z only changes how R reads
+  // transforms) or does not know: the reference's parser keeps unknown options and goes on
+  // (Utilities/antsCommandLineParser.cxx:124-160); this one names them on stderr
+  static const char* const known[] = {"dimensionality", "input-image-type", "time-index", "input", "reference-image",
+                                      "output", "interpolation", "output-data-type", "transform", "default-value",
+                                      "static-cast-for-R", "float", "verbose", "gpu"};
+  for (const auto& kv : opt)
+    if (std::find_if(std::begin(known), std::end(known), [&](const char* k) { return kv.first == k; }) ==
+        std::end(known))
+      std::cerr << "antsApplyTransforms_b200: WARNING: unknown option --" << kv.first << " ignored" << std::endl;
   const OptionCall icall = parse_call(one("interpolation", "Linear"));
   const std::string interp = lower(icall.name);
   if (interp != "linear" && interp != "nearestneighbor" && interp != "genericlabel")
@@ -470,6 +492,16 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     throw std::runtime_error(series ? "the input is not a time series (-e 3)"
                              : multichannel ? "the input is a time series (use -e 3)"
                              : "the input must be a scalar image (-e 3 resamples a time series, -e 4 a multichannel image)");
+  if (time_index >= 0) {
+    if (time_index >= in.components)
+      throw std::runtime_error("time index to extract is out of range [0, " + std::to_string(in.components - 1) + "]");
+    const long long nv = in.voxels();
+    in.data.erase(in.data.begin() + (time_index + 1) * nv, in.data.end());
+    in.data.erase(in.data.begin(), in.data.begin() + time_index * nv);
+    in.components = 1;
+    in.time_series = false;
+    series = false;
+  }
   const int channels = in.components;
   synx_geom gi = to_geom(in, dim);
   if (tail_begin < chain.size()) {

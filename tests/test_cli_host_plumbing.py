@@ -78,6 +78,10 @@ def test_time_series(host_cli, tmp_path):
     S.check_time_series(host_cli["apply"], tmp_path)
 
 
+def test_time_index(host_cli, tmp_path):
+    S.check_time_index(host_cli["apply"], tmp_path)
+
+
 def test_output_types(host_cli, tmp_path):
     S.check_output_types(host_cli["apply"], tmp_path)
 

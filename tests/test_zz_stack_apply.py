@@ -336,6 +336,38 @@ def check_time_series(exe, tmp_path):
         assert r.returncode == 1 and needle in r.stderr, (args, r.stderr)
 
 
+def check_time_index(exe, tmp_path):
+    """--time-index t with -e 3 (antsApplyTransforms.cxx:242-249, :283-317): volume t alone, resampled into
+    a 3-D image, the same values as volume t of the whole series; out of range and without -e 3 as the
+    reference treats them; -z and unknown options kept (the latter named on stderr)."""
+    cs, parts = cases(3)
+    g = parts["g"]
+    nifti.write(tmp_path / "a.nii.gz", np.ascontiguousarray(np.moveaxis(parts["a"], 0, -1)), g, vector=True)
+    parts["A"].write_mat(tmp_path / "A.mat")
+    nifti.write(tmp_path / "fixed.nii.gz", np.zeros(g.shape, np.float32), g)
+    gi = Geom((40, 36, 32), (0.8,) * 3, (-3.0,) * 3)
+    vols = np.random.default_rng(99).uniform(0, 1, gi.shape + (3,)).astype(np.float32)
+    nifti.write(tmp_path / "ts.nii", vols, gi, time_series=True, time_step=2.5)
+    base = ["-d", "3", "-r", f"{tmp_path}/fixed.nii.gz", "-t", f"{tmp_path}/a.nii.gz", "-t", f"{tmp_path}/A.mat"]
+    r = run(exe, base + ["-e", "3", "-i", f"{tmp_path}/ts.nii", "-o", f"{tmp_path}/all.nii"])
+    assert r.returncode == 0, r.stderr
+    whole, _ = nifti.read(tmp_path / "all.nii", 3)
+    r = run(exe, base + ["-e", "3", "--time-index", "1", "-z", "1", "--bogus-option", "7", "-i", f"{tmp_path}/ts.nii",
+                         "-o", f"{tmp_path}/t1.nii"])
+    assert r.returncode == 0, r.stderr
+    assert "unknown option --bogus-option ignored" in r.stderr and "static-cast" not in r.stderr
+    one, go = nifti.read(tmp_path / "t1.nii", 3)
+    assert one.shape == g.shape and go.size == g.size
+    np.testing.assert_array_equal(one, whole[..., 1])
+    r = run(exe, base + ["-e", "3", "--time-index", "3", "-i", f"{tmp_path}/ts.nii", "-o", f"{tmp_path}/t3.nii"])
+    assert r.returncode == 1 and "out of range [0, 2]" in r.stderr, r.stderr
+    # without -e 3 the reference does not read --time-index: a scalar input is resampled as usual
+    nifti.write(tmp_path / "s.nii", np.ascontiguousarray(vols[..., 0]), gi)
+    r = run(exe, base + ["--time-index", "2", "-i", f"{tmp_path}/s.nii", "-o", f"{tmp_path}/s_out.nii"])
+    assert r.returncode == 0, r.stderr
+    np.testing.assert_array_equal(nifti.read(tmp_path / "s_out.nii", 3)[0], whole[..., 0])
+
+
 def check_multichannel(exe, tmp_path, dim=3):
     """-e 4: every channel of a multichannel image resampled through `-t field -t affine.mat`, written
     back as a multichannel image on the reference grid."""
