@@ -66,7 +66,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <iostream>
+#include <iterator>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -130,6 +132,11 @@ std::vector<ChainItem> composite_chain(const std::string& file, int dim, bool in
   try {
     items = composite::read(file);
   } catch (const std::exception&) {
+    // not a composite the text reader takes: the linear reader reports on it, unless it names a
+    // displacement field, whose own error is the one to report
+    std::ifstream in(file, std::ios::binary);
+    const std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    if (text.find("DisplacementFieldTransform_") != std::string::npos) throw;
     return {};
   }
   if (std::none_of(items.begin(), items.end(), [](const composite::Item& it) { return it.is_field(); })) return {};

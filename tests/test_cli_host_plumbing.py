@@ -390,6 +390,21 @@ def test_apply_reads_the_composite(host_cli, tmp_path):
                         "-t", f"[{q}Composite.txt,1]", "-o", str(tmp_path / "x.nii.gz")],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode != 0 and "use the inverse composite" in r.stderr, r.stderr
+    # a damaged composite is reported as such, not as an unsupported linear type
+    lines = (tmp_path / "B_Composite.txt").read_text().splitlines()
+    par = [i for i, ln in enumerate(lines) if ln.startswith("Parameters:")][-1]
+    lines[par] = lines[par].rsplit(" ", 1)[0]
+    (tmp_path / "bad_comp.txt").write_text("\n".join(lines) + "\n")
+    r = subprocess.run([host_cli["apply"], "-d", "2", "-i", f"{tmp_path}/m.nii.gz", "-r", f"{tmp_path}/f.nii.gz",
+                        "-t", str(tmp_path / "bad_comp.txt"), "-o", str(tmp_path / "x.nii.gz")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0 and "do not match its size" in r.stderr, r.stderr
+    lines[par] = lines[par] + " abc"
+    (tmp_path / "bad_comp2.txt").write_text("\n".join(lines) + "\n")
+    r = subprocess.run([host_cli["apply"], "-d", "2", "-i", f"{tmp_path}/m.nii.gz", "-r", f"{tmp_path}/f.nii.gz",
+                        "-t", str(tmp_path / "bad_comp2.txt"), "-o", str(tmp_path / "x.nii.gz")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0 and "bad number" in r.stderr, r.stderr
 
     # -o CompositeTransform[file] writes the stack uncollapsed (no input or reference image needed): the
     # same composite antsRegistration -a 1 wrote, and it applies as the files do
