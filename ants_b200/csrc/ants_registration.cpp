@@ -215,6 +215,19 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     if (!is_linear_file)
       throw std::runtime_error("initial moving transform '" + file +
                                "': only linear transform files (.mat/.txt/.tfm) are supported");
+    if (lf.compare(lf.size() - 4, 4, ".mat") != 0) {
+      // a text composite holding displacement fields (prefixComposite.txt): the stage samples the moving
+      // image through linear initial transforms only
+      bool has_field = false;
+      try {
+        for (const composite::Item& it : composite::read(file)) has_field = has_field || it.is_field();
+      } catch (const std::exception&) {
+        // not a composite the text reader takes: the linear reader reports on it
+      }
+      if (has_field)
+        throw std::runtime_error("initial moving transform '" + file +
+                                 "' holds a displacement field: only linear initial transforms are supported");
+    }
     for (const LinearItem& li : read_linear_file(file, dim, invert)) init.push_back(li);
   }
   // --restore-state: [linear..., fixedToMiddle, its inverse, movingToMiddle, its inverse]

@@ -74,6 +74,16 @@ def test_cli_rejects_bad_input(cli, args, needle):
     assert needle in r.stderr
 
 
+def test_cli_rejects_an_initial_transform_with_a_field(cli, tmp_path):
+    comp = tmp_path / "c.txt"
+    comp.write_text("#Insight Transform File V1.0\n#Transform 0\nTransform: CompositeTransform_double_2_2\n"
+                    "#Transform 1\nTransform: DisplacementFieldTransform_float_2_2\nParameters: 0 0 0 0 0 0 0 0\n"
+                    "FixedParameters: 2 2 0 0 1 1 1 0 0 1\n")
+    r = run(cli, ["-d", "2", "--float", "1", "-m", "CC[a,b,1,4]", "-t", "SyN[0.1,3,0]", "-c", "10", "-f", "1", "-s", "0",
+                  "-o", "x", "-r", str(comp)])
+    assert r.returncode == 1 and "holds a displacement field" in r.stderr, r.stderr
+
+
 def test_cli_options_it_keeps_but_does_not_implement(cli):
     # the reference's parser keeps unknown options and goes on; this one does too, and says so. Its
     # other options are accepted (-p, -l, --write-interval-volumes, --minc 0, --random-seed, --version);
