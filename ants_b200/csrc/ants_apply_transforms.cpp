@@ -285,7 +285,8 @@ int run(const std::vector<std::string>& args, std::ostream& out) {
     if (lower(file) == "identity") continue;
     const std::string lf = lower(file);
     if (ends_with(lf, ".h5") || ends_with(lf, ".hdf5") || ends_with(lf, ".xfm"))
-      throw std::runtime_error("transform '" + file + "': HDF5/composite transform files are not supported");
+      throw std::runtime_error("transform '" + file +
+                               "': HDF5 and MINC transform files are not supported (text composites .txt/.tfm are)");
     if (ends_with(lf, ".txt") || ends_with(lf, ".tfm")) {
       std::vector<ChainItem> cc = composite_chain(file, dim, invert);
       if (!cc.empty()) {
