@@ -21,6 +21,7 @@
 // the same float.
 #pragma once
 
+#include <algorithm>
 #include <cctype>
 #include <charconv>
 #include <cstdio>
@@ -28,6 +29,8 @@
 #include <fstream>
 #include <stdexcept>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "synx.h"
@@ -116,14 +119,47 @@ inline bool text_name(const std::string& path) {
   return ends(".txt") || ends(".tfm");
 }
 
+// " v_i0 v_i0+1 ... v_i1-1" into s (shortest round-trip forms).
+template <class V>
+inline void format_numbers(const V& v, size_t i0, size_t i1, std::string& s) {
+  constexpr size_t kMaxNumber = 32;  // a sign, 17 digits, a point and a 5-character exponent fit
+  s.resize((i1 - i0) * (kMaxNumber + 1));
+  char* p = &s[0];
+  char* const e = p + s.size();
+  for (size_t i = i0; i < i1; ++i) {
+    *p++ = ' ';
+    p = std::to_chars(p, e, v[i]).ptr;
+  }
+  s.resize((size_t)(p - s.data()));
+}
+
+// One "key: v0 v1 ..." line.  A displacement field holds tens of millions of numbers: they are
+// formatted in blocks of 4 M, each block split over the host's threads, and written in order, so the
+// bytes are those of a sequential pass and the text held at once stays near 150 MB.
 template <class V>
 inline void write_numbers(std::FILE* f, const char* key, const V& v) {
   std::fputs(key, f);
-  char buf[64];
-  for (auto x : v) {
-    buf[0] = ' ';
-    auto r = std::to_chars(buf + 1, buf + sizeof(buf), x);
-    std::fwrite(buf, 1, (size_t)(r.ptr - buf), f);
+  const size_t n = v.size();
+  constexpr size_t kBlock = size_t(1) << 22, kSerial = size_t(1) << 16;
+  const unsigned hw = n < kSerial ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::string> parts(hw);
+  for (size_t b0 = 0; b0 < n; b0 += kBlock) {
+    const size_t b1 = std::min(n, b0 + kBlock), per = (b1 - b0 + hw - 1) / hw;
+    auto part = [&](unsigned t) {
+      const size_t i0 = std::min(b1, b0 + t * per), i1 = std::min(b1, i0 + per);
+      format_numbers(v, i0, i1, parts[t]);
+    };
+    std::vector<std::thread> pool;
+    unsigned started = 1;
+    try {
+      for (; started < hw; ++started) pool.emplace_back(part, started);
+    } catch (const std::system_error&) {
+      // no more threads: the parts not started are formatted here
+    }
+    part(0);
+    for (unsigned t = started; t < hw; ++t) part(t);
+    for (std::thread& th : pool) th.join();
+    for (const std::string& s : parts) std::fwrite(s.data(), 1, s.size(), f);
   }
   std::fputc('\n', f);
 }
@@ -146,20 +182,60 @@ inline void write(const std::string& path, int dim, const std::vector<Item>& ite
   if (std::fclose(f) != 0 || !ok) throw std::runtime_error("error writing '" + path + "'");
 }
 
+inline bool blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
+
+// The numbers of [p, e) appended to v; false at the first text that is not a number.
 template <class T>
-inline std::vector<T> parse_numbers(const std::string& s, size_t from, const std::string& path) {
-  std::vector<T> v;
-  const char* p = s.data() + from;
-  const char* e = s.data() + s.size();
+inline bool parse_span(const char* p, const char* e, std::vector<T>& v) {
   while (true) {
-    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
-    if (p >= e) break;
+    while (p < e && blank(*p)) ++p;
+    if (p >= e) return true;
     T x{};
     auto r = std::from_chars(p, e, x);
-    if (r.ec != std::errc()) throw std::runtime_error("'" + path + "': bad number in a parameter line");
+    if (r.ec != std::errc()) return false;
     v.push_back(x);
     p = r.ptr;
   }
+}
+
+// The numbers of a parameter line from offset `from`.  A long line (a displacement field's) is cut at
+// blanks into one span per host thread, the spans parsed at once and joined in order: cutting only at
+// blanks keeps every number whole, so the result is that of one pass.
+template <class T>
+inline std::vector<T> parse_numbers(const std::string& s, size_t from, const std::string& path) {
+  const char* const p = s.data() + from;
+  const char* const e = s.data() + s.size();
+  const size_t len = (size_t)(e - p);
+  const unsigned hw =
+      len < (size_t(1) << 20) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<const char*> cut(hw + 1, e);
+  cut[0] = p;
+  for (unsigned t = 1; t < hw; ++t) {
+    const char* c = std::max(cut[t - 1], p + len / hw * t);
+    while (c < e && !blank(*c)) ++c;
+    cut[t] = c;
+  }
+  std::vector<std::vector<T>> parts(hw);
+  std::vector<char> ok(hw, 0);
+  auto part = [&](unsigned t) { ok[t] = parse_span(cut[t], cut[t + 1], parts[t]) ? 1 : 0; };
+  std::vector<std::thread> pool;
+  unsigned started = 1;
+  try {
+    for (; started < hw; ++started) pool.emplace_back(part, started);
+  } catch (const std::system_error&) {
+    // no more threads: the spans not started are parsed here
+  }
+  part(0);
+  for (unsigned t = started; t < hw; ++t) part(t);
+  for (std::thread& th : pool) th.join();
+  if (std::find(ok.begin(), ok.end(), 0) != ok.end())
+    throw std::runtime_error("'" + path + "': bad number in a parameter line");
+  if (hw == 1) return std::move(parts[0]);
+  size_t total = 0;
+  for (const auto& v : parts) total += v.size();
+  std::vector<T> v;
+  v.reserve(total);
+  for (const auto& q : parts) v.insert(v.end(), q.begin(), q.end());
   return v;
 }
 

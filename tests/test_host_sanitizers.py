@@ -139,6 +139,52 @@ def test_file_readers_under_sanitizers(tmp_path):
     assert parsed > 0 and rejected > 0 and cparsed > 0 and crejected > 0, r.stdout
 
 
+ROUND_TRIP = r"""
+#include <cstdio>
+#include <random>
+#include <string>
+#include <vector>
+#include "composite_txt.h"
+static std::string g_msg;
+namespace synx { int set_global_error(int code, const std::string& m) { g_msg = m; return code; } }
+extern "C" const char* synx_last_error(const synx_ctx*) { return g_msg.c_str(); }
+int main(int argc, char** argv) {
+  // a field large enough for the threaded formatting (> 64 K numbers) and parsing (> 1 MB of text)
+  synx_geom g{}; g.dim = 2; g.size[0] = 611; g.size[1] = 467; g.size[2] = 1;
+  g.spacing[0] = 0.7; g.spacing[1] = 1.3; g.spacing[2] = 1.0;
+  g.direction[0] = g.direction[4] = g.direction[8] = 1.0;
+  std::vector<float> v(2 * 611 * 467);
+  std::mt19937 rng(3); std::normal_distribution<float> nd(0.f, 3.f);
+  for (auto& x : v) x = nd(rng);
+  const std::string path = std::string(argv[1]) + "/big.txt";
+  ants_b200::composite::write(path, 2, {ants_b200::composite::field_item(g, v, false)});
+  const auto back = ants_b200::composite::read(path);
+  if (back.size() != 1 || back[0].field != v) return 2;
+  const synx_geom gb = ants_b200::composite::field_geom(back[0], 2);
+  if (gb.size[0] != 611 || gb.size[1] != 467 || gb.spacing[0] != 0.7) return 3;
+  std::printf("round trip ok\n");
+  return 0;
+}
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+@pytest.mark.parametrize("sanitizer", ["address,undefined", "thread"])
+def test_large_composite_round_trip(tmp_path, sanitizer):
+    # the threaded number formatting and parsing of a large field: values back bit for bit, with no
+    # sanitizer finding (memory errors, undefined behaviour, data races)
+    src = tmp_path / "rt.cpp"
+    src.write_text(ROUND_TRIP)
+    exe = tmp_path / "rt"
+    build = subprocess.run(["g++", "-std=c++17", "-O1", "-g", f"-fsanitize={sanitizer}", "-fno-sanitize-recover=all",
+                            "-I", INCLUDE, "-I", CSRC, "-o", str(exe), str(src), os.path.join(CSRC, "synx_linear.cpp")],
+                           capture_output=True, text=True, timeout=300)
+    assert build.returncode == 0, build.stderr[-2000:]
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "round trip ok" in r.stdout, (r.stdout + r.stderr)[-3000:]
+    assert "WARNING: ThreadSanitizer" not in r.stderr and "AddressSanitizer" not in r.stderr, r.stderr[-3000:]
+
+
 @pytest.mark.parametrize("exe", ["antsRegistrationSyN_b200", "antsApplyTransforms_b200"])
 def test_help(exe):
     from ants_b200 import build
