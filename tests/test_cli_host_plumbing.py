@@ -437,3 +437,41 @@ def test_apply_reads_the_composite(host_cli, tmp_path):
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     np.testing.assert_array_equal(nifti.read(tmp_path / "w0b.nii.gz", 2)[0], nifti.read(tmp_path / "w_comp.nii.gz", 2)[0])
+
+
+def test_large_gzip_output(host_cli, tmp_path):
+    # a collapsed field of 3 x 160 x 150 x 100 floats (29 MB) is written as several gzip members; the
+    # Python reader (gzip) and the C++ reader (zlib gzread, here as a -t input) both see the bytes of the
+    # uncompressed file
+    import gzip
+
+    import numpy as np
+
+    from ants_b200 import nifti
+    from ants_b200.synx import Geom
+    g = Geom((160, 150, 100), (1.0, 1.1, 1.2))
+    nifti.write(tmp_path / "ref.nii.gz", np.zeros(g.shape, np.float32), g)
+    rng = np.random.default_rng(5)
+    small = Geom((20, 19, 13), (8.0, 8.7, 9.3))
+    u = rng.normal(0, 1.5, small.shape + (3,)).astype(np.float32)
+    nifti.write(tmp_path / "u.nii.gz", u, small, vector=True)
+    for out in ("c.nii.gz", "c.nii"):
+        r = subprocess.run([host_cli["apply"], "-d", "3", "--float", "1", "-r", f"{tmp_path}/ref.nii.gz",
+                            "-t", f"{tmp_path}/u.nii.gz", "-o", f"[{tmp_path / out},1]"],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+    raw = (tmp_path / "c.nii").read_bytes()
+    assert len(raw) > (8 << 20) * 3
+    assert gzip.open(tmp_path / "c.nii.gz").read() == raw
+    members = (tmp_path / "c.nii.gz").read_bytes().count(b"\x1f\x8b\x08")
+    assert members >= 3
+    a, _ = nifti.read(tmp_path / "c.nii.gz", 3)
+    b, _ = nifti.read(tmp_path / "c.nii", 3)
+    np.testing.assert_array_equal(a, b)
+    # the C++ reader: the compressed field as a transform gives the same collapsed field as the plain one
+    for src, out in (("c.nii.gz", "d1.nii"), ("c.nii", "d2.nii")):
+        r = subprocess.run([host_cli["apply"], "-d", "3", "--float", "1", "-r", f"{tmp_path}/ref.nii.gz",
+                            "-t", f"{tmp_path}/{src}", "-o", f"[{tmp_path / out},1]"],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+    assert (tmp_path / "d1.nii").read_bytes() == (tmp_path / "d2.nii").read_bytes()
