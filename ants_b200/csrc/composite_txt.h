@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <system_error>
@@ -145,9 +146,14 @@ inline void write_numbers(std::FILE* f, const char* key, const V& v) {
   std::vector<std::string> parts(hw);
   for (size_t b0 = 0; b0 < n; b0 += kBlock) {
     const size_t b1 = std::min(n, b0 + kBlock), per = (b1 - b0 + hw - 1) / hw;
+    std::vector<char> ok(hw, 1);
     auto part = [&](unsigned t) {
       const size_t i0 = std::min(b1, b0 + t * per), i1 = std::min(b1, i0 + per);
-      format_numbers(v, i0, i1, parts[t]);
+      try {
+        format_numbers(v, i0, i1, parts[t]);
+      } catch (const std::bad_alloc&) {
+        ok[t] = 0;  // thrown below, not across the thread
+      }
     };
     std::vector<std::thread> pool;
     unsigned started = 1;
@@ -159,6 +165,7 @@ inline void write_numbers(std::FILE* f, const char* key, const V& v) {
     part(0);
     for (unsigned t = started; t < hw; ++t) part(t);
     for (std::thread& th : pool) th.join();
+    if (std::find(ok.begin(), ok.end(), 0) != ok.end()) throw std::bad_alloc();
     for (const std::string& s : parts) std::fwrite(s.data(), 1, s.size(), f);
   }
   std::fputc('\n', f);
@@ -217,7 +224,14 @@ inline std::vector<T> parse_numbers(const std::string& s, size_t from, const std
   }
   std::vector<std::vector<T>> parts(hw);
   std::vector<char> ok(hw, 0);
-  auto part = [&](unsigned t) { ok[t] = parse_span(cut[t], cut[t + 1], parts[t]) ? 1 : 0; };
+  std::vector<char> oom(hw, 0);
+  auto part = [&](unsigned t) {
+    try {
+      ok[t] = parse_span(cut[t], cut[t + 1], parts[t]) ? 1 : 0;
+    } catch (const std::bad_alloc&) {
+      oom[t] = 1;  // thrown below, not across the thread
+    }
+  };
   std::vector<std::thread> pool;
   unsigned started = 1;
   try {
@@ -228,6 +242,7 @@ inline std::vector<T> parse_numbers(const std::string& s, size_t from, const std
   part(0);
   for (unsigned t = started; t < hw; ++t) part(t);
   for (std::thread& th : pool) th.join();
+  if (std::find(oom.begin(), oom.end(), 1) != oom.end()) throw std::bad_alloc();
   if (std::find(ok.begin(), ok.end(), 0) != ok.end())
     throw std::runtime_error("'" + path + "': bad number in a parameter line");
   if (hw == 1) return std::move(parts[0]);

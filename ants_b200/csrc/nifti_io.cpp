@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <stdexcept>
 #include <system_error>
 #include <thread>
@@ -144,7 +145,11 @@ void write_gzip_members(const std::string& path, const std::vector<unsigned char
     const unsigned wave = (unsigned)std::min<size_t>(hw, chunks - c0);
     auto part = [&](unsigned t) {
       const size_t b = (c0 + t) * kChunk, e = std::min(all.size(), b + kChunk);
-      done[t] = gzip_member(all.data() + b, e - b, out[t]) ? 1 : 0;
+      try {
+        done[t] = gzip_member(all.data() + b, e - b, out[t]) ? 1 : 0;
+      } catch (const std::bad_alloc&) {
+        done[t] = 0;  // reported as a failed write, not thrown across the thread
+      }
     };
     std::vector<std::thread> pool;
     unsigned started = 1;
