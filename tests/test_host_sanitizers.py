@@ -145,10 +145,18 @@ ROUND_TRIP = r"""
 #include <string>
 #include <vector>
 #include "composite_txt.h"
+#include "nifti_io.h"
 static std::string g_msg;
 namespace synx { int set_global_error(int code, const std::string& m) { g_msg = m; return code; } }
 extern "C" const char* synx_last_error(const synx_ctx*) { return g_msg.c_str(); }
 int main(int argc, char** argv) {
+  // a .nii.gz large enough for several gzip members compressed on separate threads
+  nifti::Image im; im.dim = 3; im.components = 3; im.size[0] = 131; im.size[1] = 97; im.size[2] = 83;
+  im.data.resize(3ull * 131 * 97 * 83);
+  std::mt19937 r0(5); std::normal_distribution<float> n0(0.f, 1.f);
+  for (auto& x : im.data) x = n0(r0);
+  nifti::write(std::string(argv[1]) + "/big.nii.gz", im);
+  if (nifti::read(std::string(argv[1]) + "/big.nii.gz").data != im.data) return 4;
   // a field large enough for the threaded formatting (> 64 K numbers) and parsing (> 1 MB of text)
   synx_geom g{}; g.dim = 2; g.size[0] = 611; g.size[1] = 467; g.size[2] = 1;
   g.spacing[0] = 0.7; g.spacing[1] = 1.3; g.spacing[2] = 1.0;
@@ -171,14 +179,15 @@ int main(int argc, char** argv) {
 @pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
 @pytest.mark.parametrize("sanitizer", ["address,undefined", "thread"])
 def test_large_composite_round_trip(tmp_path, sanitizer):
-    # the threaded number formatting and parsing of a large field: values back bit for bit, with no
-    # sanitizer finding (memory errors, undefined behaviour, data races)
+    # the threaded number formatting and parsing of a large field, and the threaded gzip members of a
+    # large .nii.gz: values back bit for bit, with no sanitizer finding (memory errors, undefined
+    # behaviour, data races)
     src = tmp_path / "rt.cpp"
     src.write_text(ROUND_TRIP)
     exe = tmp_path / "rt"
     build = subprocess.run(["g++", "-std=c++17", "-O1", "-g", f"-fsanitize={sanitizer}", "-fno-sanitize-recover=all",
-                            "-I", INCLUDE, "-I", CSRC, "-o", str(exe), str(src), os.path.join(CSRC, "synx_linear.cpp")],
-                           capture_output=True, text=True, timeout=300)
+                            "-I", INCLUDE, "-I", CSRC, "-o", str(exe), str(src), os.path.join(CSRC, "synx_linear.cpp"),
+                            os.path.join(CSRC, "nifti_io.cpp"), "-lz"], capture_output=True, text=True, timeout=300)
     assert build.returncode == 0, build.stderr[-2000:]
     r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "round trip ok" in r.stdout, (r.stdout + r.stderr)[-3000:]
